@@ -1,0 +1,309 @@
+#!/usr/bin/env python
+"""Benchmark of the DG wave-equation RK3 step on B200 (one JSON line on rank 0).
+
+Workload (the reference's 256 x 256, N = 8 configuration): uniform periodic
+quad mesh of [-1, 1]^2, Legendre-Gauss N = 8, the reference plane-wave
+initial condition, CFL 0.5, FP64. One benchmark step is one low-storage RK3
+time step (three stages) over the whole mesh.
+
+Metric: DOF-stage updates/s = DOF x 3 x steps / seconds, DOF = 3 K (N+1)^2
+(p, u, v). `value` is device-resident (inputs already in HBM); `e2e` is the
+same metric through the C ABI with host buffers: every e2e step uploads the
+state from pinned host memory, runs the configuration's 2000 RK3 steps and
+downloads the state. The working set (q, RK register, trace buffers:
+~370 MB) is larger than the 126 MB L2, so no L2 flush is inserted.
+
+`--impl reference` times the reference's own CPU path (oracle/_ref) on the
+host cores on the same configuration, a bounded number of steps.
+
+Multi-GPU (torchrun): the path runs as independent replicas, one per GPU
+(no data-path collective); value sums the ranks' DOF-stages over the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RES, ORDER, CFL, CONFIG_STEPS = 256, 8, 0.5, 2000
+BYTES_PER_DOF_STAGE = 32  # read + write of q and of the RK register, FP64
+
+
+def workload_zone():
+    from tests import meshgen
+    return meshgen.uniform_zone(RES, x_periodic=True, y_periodic=True)
+
+
+def dof_count() -> int:
+    return 3 * RES * RES * (ORDER + 1) ** 2
+
+
+def config(extra: dict | None = None) -> dict:
+    c = {"workload": f"dg_wave_rk3_periodic_{RES}x{RES}_N{ORDER}_plane_wave", "mesh": f"{RES}x{RES} uniform periodic quads on [-1,1]^2",
+         "order_N": ORDER, "dof": dof_count(), "cfl": CFL, "rk_stages_per_step": 3, "precision_form": "fp64",
+         "l2_policy": "working set > L2 (126 MB): q+k 255 MB, traces 113 MB; no flush", "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# Clocks during the timed region.
+class ClockSampler:
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100", "-i", str(self.index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def physical_gpu_index(local: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local < len(ids) and ids[local].isdigit():
+            return int(ids[local])
+    return local
+
+
+def measured_hbm_peak() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic() -> float | None:
+    """DRAM bytes per stage-kernel launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d[f"N{ORDER}_res{RES}"]["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(budget_s: float, max_steps: int, warmup: int) -> dict:
+    """The reference's own CPU path (oracle/_ref/libndgref.so; the plain-C
+    oracle when it is absent) on the workload, timed on this host."""
+    from oracle import pyoracle
+    zone = workload_zone()
+    kind = "reference" if pyoracle.ref_available() else "port"
+    solver = pyoracle.RefSolver(zone, ORDER, cfl=CFL) if kind == "reference" else pyoracle.OracleSolver(zone, ORDER, cfl=CFL)
+    solver.initial_conditions()
+    t = 0.0
+    for _ in range(warmup):
+        t = solver.run(1, t)
+    done, start = 0, time.perf_counter()
+    while done < max_steps:
+        t = solver.run(1, t)
+        done += 1
+        if time.perf_counter() - start > budget_s:
+            break
+    elapsed = time.perf_counter() - start
+    rate = dof_count() * 3 * done / elapsed
+    return {"value": rate, "unit": "DOF-stage updates/s", "cores": 1, "kind": kind, "steps": done, "seconds": elapsed,
+            "sample": f"{done} RK3 steps of the {RES}x{RES} N={ORDER} workload on 1 host core (the reference CPU path is single-threaded)"}
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    budget = float(os.environ.get("NDG_REF_BUDGET_S", "90"))
+    base = cpu_reference_rate(budget, max(args.steps, 1), min(args.warmup, 1))
+    line = {"impl": "reference", "metric": "DOF-stage updates/s", "value": base["value"], "unit": "DOF-stage updates/s",
+            "n_gpus": args.gpus, "steps": base["steps"], "warmup": min(args.warmup, 1),
+            "ms_per_step": 1e3 * base["seconds"] / base["steps"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference plane-wave initial condition)",
+            "config": config({"sample": base["sample"]}),
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": base["value"], "unit": "DOF-stage updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import ndg_cuda_b200 as ndg
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    stream = torch.cuda.Stream()
+    zone = workload_zone()
+    mesh = ndg.Mesh2D_t(zone, ORDER, cfl=CFL, device=local, stream=stream.cuda_stream)
+    mesh.initial_conditions()
+    dof = ndg.dof_count(mesh)
+    assert dof == dof_count()
+
+    ndg.Solver2D_t.run(mesh, args.warmup)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(physical_gpu_index(local)) as clocks:
+        barrier()
+        launches0 = mesh.launches()
+        start.record(stream)
+        ndg.Solver2D_t.run(mesh, args.steps)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        launches = mesh.launches() - launches0
+        barrier()
+    ms = start.elapsed_time(stop)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * dof * 3 * args.steps / (ms_max / 1e3)
+
+    # Roofline of the dominant kernel: the fused stage kernel, timed per launch.
+    stage_ms = mesh.time_stage(1, 30)
+    achieved = BYTES_PER_DOF_STAGE * dof / (stage_ms / 1e3) / 1e9
+    peak, peak_kind = measured_hbm_peak()
+    traffic = profiled_traffic()
+
+    # End to end through the C ABI with pinned host buffers.
+    e2e_steps = 2
+    host = {f: torch.empty(mesh.field_size, dtype=torch.float64, pin_memory=True) for f in ("p", "u", "v")}
+    for f in host:
+        host[f].copy_(torch.from_numpy(mesh.get_field(f)))
+    L = ndg.lib()
+
+    def e2e_call():
+        for i, f in enumerate(("p", "u", "v")):
+            ndg._check(L.ndg_set_field(mesh.handle, 0, i, host[f].data_ptr()))
+        ndg.Solver2D_t.run(mesh, CONFIG_STEPS)
+        for i, f in enumerate(("p", "u", "v")):
+            ndg._check(L.ndg_get_field(mesh.handle, 0, i, host[f].data_ptr()))
+
+    e2e_call()  # warm-up
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    wall0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * dof * 3 * CONFIG_STEPS * e2e_steps / (float(e2e_t.item()) / 1e3)
+    state_bytes = 3 * mesh.field_size * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_rate(float(os.environ.get("NDG_CPU_BUDGET_S", "15")), 1000, 1)
+
+    if rank == 0:
+        line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (reference plane-wave initial condition on a generated mesh)",
+                "config": config(),
+                "e2e": {"value": e2e_value, "unit": "DOF-stage updates/s", "h2d_bytes_per_step": state_bytes,
+                        "d2h_bytes_per_step": state_bytes, "rk3_steps_per_e2e_step": CONFIG_STEPS, "e2e_steps": e2e_steps,
+                        "host_wall_s": wall},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "traffic": traffic, "kernel": f"stage_kernel<{ORDER}, false>", "kernel_ms": stage_ms,
+                             "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof, "peak_source": peak_kind},
+                "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "gpu_launches": launches,
+                "clocks": clocks.summary()}
+        print(json.dumps(line), flush=True)
+    mesh.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=CONFIG_STEPS)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
+

@@ -1,0 +1,202 @@
+/* ndg_b200: C ABI of the B200 (sm_100a) DG spectral-element wave solver.
+ *
+ * Drop-in for the GPU path of NDG_cuda's 2D wave-equation time step. Every
+ * entry point takes plain pointers and sizes; device memory, streams and
+ * kernels stay inside the library. Each declaration names the reference
+ * interface it replaces (paths inside the NDG_cuda repository).
+ *
+ * Conventions
+ *  - Every call returns an ndg_status; on failure ndg_last_error() returns a
+ *    message for the calling thread. Nothing calls exit().
+ *  - One context per host thread; calls on one context are not thread-safe.
+ *    All device work is ordered on the context's stream; calls that return
+ *    host data synchronise that stream.
+ *  - Element fields are laid out as the reference's Element2D_t arrays:
+ *    element after element, (N+1)^2 values each, node index i*(N+1)+j with i
+ *    along xi and j along eta (include/entities/Element2D_t.h:36-38).
+ *  - Several independent instances (same mesh, different fields) can share
+ *    one context; instance fields follow each other in the field arrays.
+ */
+#ifndef NDG_B200_H
+#define NDG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ndg_status {
+    NDG_OK = 0,
+    NDG_ERR_INVALID_ARG = 1,
+    NDG_ERR_MESH = 2,
+    NDG_ERR_CUDA = 3,
+    NDG_ERR_NONFINITE = 4,
+    NDG_ERR_OOM = 5,
+    NDG_ERR_TIMEOUT = 6,
+    NDG_ERR_UNSUPPORTED = 7
+} ndg_status;
+
+/* Opaque solver context. */
+typedef struct ndg_ctx ndg_ctx;
+
+/* Arithmetic of the stage kernels.
+ * NDG_FP64: FP64 with fused multiply-adds and reciprocal multiplies.
+ * NDG_FP64_STRICT: FP64 rounded operation by operation in the reference's
+ *   order (no contraction, true divisions): bit-identical to the reference's
+ *   CPU path on the same inputs.
+ * NDG_FP32: volume, surface and flux arithmetic in FP32, solution and RK
+ *   register kept in FP64. */
+typedef enum ndg_precision { NDG_FP64 = 0, NDG_FP64_STRICT = 1, NDG_FP32 = 2 } ndg_precision;
+
+/* Tables of NDG_t (include/entities/NDG_t.cuh:11-29). */
+typedef enum ndg_table {
+    NDG_TABLE_NODES = 0,
+    NDG_TABLE_WEIGHTS = 1,
+    NDG_TABLE_BARYCENTRIC_WEIGHTS = 2,
+    NDG_TABLE_LAGRANGE_LEFT = 3,
+    NDG_TABLE_LAGRANGE_RIGHT = 4,
+    NDG_TABLE_LAGRANGE_DERIVATIVE_LEFT = 5,
+    NDG_TABLE_LAGRANGE_DERIVATIVE_RIGHT = 6,
+    NDG_TABLE_DERIVATIVE_MATRICES = 7,
+    NDG_TABLE_G_HAT_DERIVATIVE_MATRICES = 8,
+    NDG_TABLE_DERIVATIVE_MATRICES_HAT = 9,
+    NDG_TABLE_INTERPOLATION_MATRICES = 10,
+    NDG_TABLE_POLYNOMIALS = 11
+} ndg_table;
+
+typedef enum ndg_field {
+    NDG_FIELD_P = 0, NDG_FIELD_U = 1, NDG_FIELD_V = 2,          /* Element2D_t::p_, u_, v_ */
+    NDG_FIELD_G_P = 3, NDG_FIELD_G_U = 4, NDG_FIELD_G_V = 5,    /* Element2D_t::G_p_ ... (last stage's time derivative) */
+    NDG_FIELD_K_P = 6, NDG_FIELD_K_U = 7, NDG_FIELD_K_V = 8     /* Element2D_t::p_intermediate_ ... (RK register) */
+} ndg_field;
+
+/* Boundary condition codes of the zone description (CGNS BCType_t subset read by
+ * Mesh2D_t::read_cgns, src/meshes/Mesh2D_t.cpp:725-816). */
+typedef enum ndg_bc { NDG_BC_WALL = 0, NDG_BC_SYMMETRY = 1, NDG_BC_INFLOW = 2, NDG_BC_OUTFLOW = 3, NDG_BC_NULL = 4 } ndg_bc;
+
+/* Boundary lists of ndg_mesh_get_boundary (Mesh2D_t::wall_boundaries_ ...,
+ * interfaces_origin_ ..., include/meshes/Mesh2D_t.h:29-38). */
+typedef enum ndg_boundary_list {
+    NDG_LIST_WALL = 0, NDG_LIST_SYMMETRY = 1, NDG_LIST_INFLOW = 2, NDG_LIST_OUTFLOW = 3,
+    NDG_LIST_INTERFACE_ORIGIN = 4, NDG_LIST_INTERFACE_ORIGIN_SIDE = 5, NDG_LIST_INTERFACE_DESTINATION = 6
+} ndg_boundary_list;
+
+/* One unstructured 2D zone in CGNS terms: what Mesh2D_t::read_cgns reads from
+ * a file (src/meshes/Mesh2D_t.cpp:422-645), as arrays.
+ *  - section_type: 0 = QUAD_4 (domain), 1 = BAR_2 (ghost/boundary elements);
+ *    section_start/end: 1-based element numbers; section_connectivity:
+ *    1-based node numbers, 4 per quad and 2 per bar, sections concatenated.
+ *  - boco_type: ndg_bc; boco_points: 1-based element numbers, concatenated.
+ *  - conn_*: Abutting1to1 self connectivity (periodic), 1-based element
+ *    numbers of the receiving ghost and of its donor ghost. */
+typedef struct ndg_zone {
+    int64_t n_nodes;
+    const double* x;
+    const double* y;
+    int32_t n_sections;
+    const int32_t* section_type;
+    const int64_t* section_start;
+    const int64_t* section_end;
+    const int64_t* section_connectivity;
+    int32_t n_bocos;
+    const int32_t* boco_type;
+    const int64_t* boco_count;
+    const int64_t* boco_points;
+    int32_t n_conns;
+    const int64_t* conn_count;
+    const int64_t* conn_points;
+    const int64_t* conn_donors;
+} ndg_zone;
+
+/* Constructor arguments of Mesh2D_t (include/meshes/Mesh2D_t.cuh:25) and
+ * the CFL of Solver2D_t (include/solvers/Solver2D_t.cuh:16). */
+typedef struct ndg_mesh_params {
+    int32_t initial_N;
+    int32_t maximum_N;
+    int64_t n_interpolation_points;
+    int32_t max_split_level;
+    int64_t adaptivity_interval;
+    double tolerance_min;
+    double tolerance_max;
+    double cfl;
+} ndg_mesh_params;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* ndg_last_error(void);
+const char* ndg_version(void);
+
+/* Context: owns device memory and the stream of one solver.
+ * device < 0 makes a host-only context (tables and mesh topology, no GPU).
+ * stream is a cudaStream_t (NULL = a stream created by the context).
+ * Replaces the stream/ownership plumbing of Mesh2D_t (include/meshes/Mesh2D_t.cuh:163). */
+ndg_status ndg_ctx_create(int32_t device, void* stream, ndg_ctx** out);
+ndg_status ndg_ctx_destroy(ndg_ctx* ctx);
+ndg_status ndg_ctx_set_precision(ndg_ctx* ctx, int32_t precision);
+ndg_status ndg_ctx_synchronize(ndg_ctx* ctx);
+/* Keep a copy of each stage's time derivative G (Element2D_t::G_p_ ...) so
+ * that ndg_get_field can return it; off by default (it costs HBM traffic). */
+ndg_status ndg_ctx_keep_derivative(ndg_ctx* ctx, int32_t enable);
+
+/* NDG_t<LegendrePolynomial_t>(N_max, n_interpolation_points, stream)
+ * (include/entities/NDG_t.cuh:11, include/entities/NDG_t.tcu:13-72). */
+ndg_status ndg_tables_build(ndg_ctx* ctx, int32_t N_max, int64_t n_interpolation_points);
+/* One table of order N into out[capacity]; *count = number of values. */
+ndg_status ndg_tables_get(const ndg_ctx* ctx, int32_t table, int32_t N, double* out, int64_t capacity, int64_t* count);
+/* The same without a context (host FP64, no GPU). */
+ndg_status ndg_tables_compute(int32_t N_max, int64_t n_interpolation_points, int32_t table, int32_t N, double* out, int64_t capacity, int64_t* count);
+
+/* Mesh2D_t(filename, initial_N, maximum_N, ...) for a zone given as arrays
+ * (include/meshes/Mesh2D_t.cuh:25, src/meshes/Mesh2D_t.cu:32-82). Builds the
+ * reference's element, face, boundary and interface numbering, then the
+ * device layout. n_instances independent solutions share the mesh. */
+ndg_status ndg_mesh_load_zone(ndg_ctx* ctx, const ndg_zone* zone, const ndg_mesh_params* params, int32_t n_instances);
+/* Same, from a mesh file: .su2 (Mesh2D_t::read_su2, src/meshes/Mesh2D_t.cpp:78-421). */
+ndg_status ndg_mesh_load_file(ndg_ctx* ctx, const char* path, const ndg_mesh_params* params, int32_t n_instances);
+ndg_status ndg_mesh_counts(const ndg_ctx* ctx, int64_t* n_elements, int64_t* n_elements_total, int64_t* n_faces, int64_t* n_nodes);
+/* Topology views with the reference's numbering (Face2D_t fields,
+ * include/entities/Face2D_t.h:37-58; Element2D_t nodes_/faces_/N_). */
+ndg_status ndg_mesh_get_faces(const ndg_ctx* ctx, int64_t* nodes, int64_t* elements, int64_t* sides, int32_t* N,
+                              double* normal, double* tangent, double* offset, double* scale);
+ndg_status ndg_mesh_get_elements(const ndg_ctx* ctx, int64_t* nodes, int32_t* N, double* delta_xy_min, int64_t* first_face);
+ndg_status ndg_mesh_get_boundary(const ndg_ctx* ctx, int32_t list, int64_t* out, int64_t capacity, int64_t* count);
+ndg_status ndg_mesh_get_nodes(const ndg_ctx* ctx, double* xy);
+/* Degrees of freedom per field and instance: sum over elements of (N+1)^2. */
+ndg_status ndg_mesh_field_size(const ndg_ctx* ctx, int64_t* n_values);
+
+/* Mesh2D_t::initial_conditions (src/meshes/Mesh2D_t.cu:5030): the reference
+ * plane wave g(x, 0) in every instance; G and the RK register are zeroed. */
+ndg_status ndg_initial_conditions(ndg_ctx* ctx);
+/* Copies one field of one instance from/to host memory (field_size values).
+ * instance < 0 addresses all instances back to back. */
+ndg_status ndg_set_field(ndg_ctx* ctx, int32_t instance, int32_t field, const double* values);
+ndg_status ndg_get_field(ndg_ctx* ctx, int32_t instance, int32_t field, double* values);
+
+/* Solver2D_t::get_delta_t (src/solvers/Solver2D_t.cu:17-31): min over
+ * elements of CFL * delta_xy_min / (N^2 c), reduced on the device. */
+ndg_status ndg_get_delta_t(ndg_ctx* ctx, double* delta_t);
+/* One low-storage RK3 stage m in {0,1,2} at step start `time` with step dt:
+ * interpolate_to_boundaries, boundary_conditions, project_to_faces,
+ * calculate_wave_fluxes, project_to_elements, compute_dg_wave_derivative,
+ * rk3_(first_)step (include/solvers/Solver2D_t.tcu:46-70), fused. */
+ndg_status ndg_stage(ndg_ctx* ctx, int32_t m, double time, double dt);
+/* n_steps RK3 steps, each with dt = get_delta_t; *time advances by dt per step. */
+ndg_status ndg_run(ndg_ctx* ctx, int64_t n_steps, double* time);
+/* The reference's time loop to t_end (include/solvers/Solver2D_t.tcu:7-135
+ * without output or adaptivity): the last step is shortened to land on
+ * t_end. *time is the start time in and the end time out. */
+ndg_status ndg_solve(ndg_ctx* ctx, double t_end, double* time, int64_t* n_steps);
+
+/* Benchmark aid: launches stage m n_launches times back to back (the state
+ * advances), timing each launch with CUDA events on the context's stream;
+ * *avg_ms = mean kernel duration. */
+ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* avg_ms);
+
+/* Kernel launches issued by this context so far (for launch accounting). */
+ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

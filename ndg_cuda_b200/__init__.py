@@ -1,0 +1,349 @@
+"""ndg_cuda_b200: B200-native DG spectral-element solver for the 2D wave equation.
+
+Python host side of the library. It mirrors the reference's host API for the
+hot path -- NDG_t (polynomial tables), Mesh2D_t (mesh, initial conditions,
+fields) and Solver2D_t (CFL step, RK3 stepping, solve) -- over the C ABI of
+include/ndg_b200.h, which ctypes binds from the in-tree
+ndg_cuda_b200/libndg_b200.so. There is no fallback: if the library is missing
+or a call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["NdgError", "lib", "NDG_t", "Mesh2D_t", "Solver2D_t", "Zone", "LIB_PATH",
+           "FP64", "FP64_STRICT", "FP32", "tables_compute"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libndg_b200.so")
+
+FP64, FP64_STRICT, FP32 = 0, 1, 2
+_STATUS = {0: "OK", 1: "INVALID_ARG", 2: "MESH", 3: "CUDA", 4: "NONFINITE", 5: "OOM", 6: "TIMEOUT", 7: "UNSUPPORTED"}
+FIELDS = {"p": 0, "u": 1, "v": 2, "G_p": 3, "G_u": 4, "G_v": 5, "k_p": 6, "k_u": 7, "k_v": 8}
+TABLES = ["nodes", "weights", "barycentric_weights", "lagrange_interpolant_left", "lagrange_interpolant_right",
+          "lagrange_interpolant_derivative_left", "lagrange_interpolant_derivative_right", "derivative_matrices",
+          "g_hat_derivative_matrices", "derivative_matrices_hat", "interpolation_matrices", "polynomials"]
+
+
+class NdgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class _Zone(C.Structure):
+    _fields_ = [("n_nodes", C.c_int64), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("n_sections", C.c_int32), ("section_type", C.c_void_p), ("section_start", C.c_void_p),
+                ("section_end", C.c_void_p), ("section_connectivity", C.c_void_p),
+                ("n_bocos", C.c_int32), ("boco_type", C.c_void_p), ("boco_count", C.c_void_p), ("boco_points", C.c_void_p),
+                ("n_conns", C.c_int32), ("conn_count", C.c_void_p), ("conn_points", C.c_void_p), ("conn_donors", C.c_void_p)]
+
+
+class _Params(C.Structure):
+    _fields_ = [("initial_N", C.c_int32), ("maximum_N", C.c_int32), ("n_interpolation_points", C.c_int64),
+                ("max_split_level", C.c_int32), ("adaptivity_interval", C.c_int64),
+                ("tolerance_min", C.c_double), ("tolerance_max", C.c_double), ("cfl", C.c_double)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libndg_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise NdgError(3, f"{LIB_PATH} is missing; build it with python -m ndg_cuda_b200.build")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    sigs = {
+        "ndg_last_error": ([], C.c_char_p), "ndg_version": ([], C.c_char_p),
+        "ndg_ctx_create": ([i32, vp, C.POINTER(vp)], C.c_int),
+        "ndg_ctx_destroy": ([vp], C.c_int),
+        "ndg_ctx_set_precision": ([vp, i32], C.c_int),
+        "ndg_ctx_keep_derivative": ([vp, i32], C.c_int),
+        "ndg_ctx_synchronize": ([vp], C.c_int),
+        "ndg_tables_build": ([vp, i32, i64], C.c_int),
+        "ndg_tables_get": ([vp, i32, i32, vp, i64, C.POINTER(i64)], C.c_int),
+        "ndg_tables_compute": ([i32, i64, i32, i32, vp, i64, C.POINTER(i64)], C.c_int),
+        "ndg_mesh_load_zone": ([vp, C.POINTER(_Zone), C.POINTER(_Params), i32], C.c_int),
+        "ndg_mesh_load_file": ([vp, C.c_char_p, C.POINTER(_Params), i32], C.c_int),
+        "ndg_mesh_counts": ([vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)], C.c_int),
+        "ndg_mesh_get_faces": ([vp] * 9, C.c_int),
+        "ndg_mesh_get_elements": ([vp] * 5, C.c_int),
+        "ndg_mesh_get_boundary": ([vp, i32, vp, i64, C.POINTER(i64)], C.c_int),
+        "ndg_mesh_get_nodes": ([vp, vp], C.c_int),
+        "ndg_mesh_field_size": ([vp, C.POINTER(i64)], C.c_int),
+        "ndg_initial_conditions": ([vp], C.c_int),
+        "ndg_set_field": ([vp, i32, i32, vp], C.c_int),
+        "ndg_get_field": ([vp, i32, i32, vp], C.c_int),
+        "ndg_get_delta_t": ([vp, C.POINTER(dbl)], C.c_int),
+        "ndg_stage": ([vp, i32, dbl, dbl], C.c_int),
+        "ndg_run": ([vp, i64, C.POINTER(dbl)], C.c_int),
+        "ndg_solve": ([vp, dbl, C.POINTER(dbl), C.POINTER(i64)], C.c_int),
+        "ndg_launch_count": ([vp, C.POINTER(i64)], C.c_int),
+        "ndg_time_stage": ([vp, i32, i32, C.POINTER(dbl)], C.c_int),
+    }
+    for name, (args, res) in sigs.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise NdgError(status, lib().ndg_last_error().decode())
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def tables_compute(N_max: int, n_interpolation_points: int, table: str | int, N: int) -> np.ndarray:
+    """One NDG_t table computed on the host (no GPU needed)."""
+    t = TABLES.index(table) if isinstance(table, str) else table
+    count = C.c_int64()
+    _check(lib().ndg_tables_compute(N_max, n_interpolation_points, t, N, None, 0, C.byref(count)))
+    out = np.empty(count.value)
+    _check(lib().ndg_tables_compute(N_max, n_interpolation_points, t, N, _ptr(out), out.size, C.byref(count)))
+    return out
+
+
+class Zone:
+    """One unstructured 2D zone in CGNS terms (the input of Mesh2D_t).
+
+    `sections` are (name, type, start, end, connectivity) with type 0 = QUAD_4
+    and 1 = BAR_2; `bocos` are (name, bc, points); `conns` are
+    (name, points, donor_points); all element and node numbers 1-based.
+    """
+
+    def __init__(self, x, y, sections, bocos=(), conns=()):
+        self.x = np.ascontiguousarray(x, dtype=np.float64)
+        self.y = np.ascontiguousarray(y, dtype=np.float64)
+        self.sections = list(sections)
+        self.bocos = list(bocos)
+        self.conns = list(conns)
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "Zone":
+        return cls(d["x"], d["y"], d["sections"], d["bocos"], d["conns"])
+
+    def _struct(self) -> tuple[_Zone, list]:
+        keep = []
+
+        def arr(values, dtype):
+            a = np.ascontiguousarray(np.asarray(values, dtype=dtype)) if len(values) else np.zeros(1, dtype=dtype)
+            keep.append(a)
+            return _ptr(a)
+
+        z = _Zone()
+        z.n_nodes = self.x.size
+        z.x, z.y = _ptr(self.x), _ptr(self.y)
+        z.n_sections = len(self.sections)
+        z.section_type = arr([s[1] for s in self.sections], np.int32)
+        z.section_start = arr([s[2] for s in self.sections], np.int64)
+        z.section_end = arr([s[3] for s in self.sections], np.int64)
+        z.section_connectivity = arr(np.concatenate([np.asarray(s[4], np.int64) for s in self.sections]), np.int64)
+        z.n_bocos = len(self.bocos)
+        z.boco_type = arr([b[1] for b in self.bocos], np.int32)
+        z.boco_count = arr([len(b[2]) for b in self.bocos], np.int64)
+        z.boco_points = arr(np.concatenate([np.asarray(b[2], np.int64) for b in self.bocos]) if self.bocos else [], np.int64)
+        z.n_conns = len(self.conns)
+        z.conn_count = arr([len(c[1]) for c in self.conns], np.int64)
+        z.conn_points = arr(np.concatenate([np.asarray(c[1], np.int64) for c in self.conns]) if self.conns else [], np.int64)
+        z.conn_donors = arr(np.concatenate([np.asarray(c[2], np.int64) for c in self.conns]) if self.conns else [], np.int64)
+        return z, keep
+
+
+class _Context:
+    def __init__(self, device: int, stream: int | None = None):
+        h = C.c_void_p()
+        _check(lib().ndg_ctx_create(device, stream, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ndg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NDG_t:
+    """Polynomial tables of NDG_t<LegendrePolynomial_t>(N_max, n_interpolation_points)
+    (include/entities/NDG_t.cuh:11-29), one numpy array per order."""
+
+    def __init__(self, N_max: int, n_interpolation_points: int, device: int = 0):
+        self.N_max_ = N_max
+        self.N_interpolation_points_ = n_interpolation_points
+        self._ctx = _Context(device)
+        _check(lib().ndg_tables_build(self._ctx.h, N_max, n_interpolation_points))
+        for i, name in enumerate(TABLES):
+            setattr(self, name + "_", [self._get(i, N) for N in range(N_max + 1)])
+
+    def _get(self, table: int, N: int) -> np.ndarray:
+        count = C.c_int64()
+        _check(lib().ndg_tables_get(self._ctx.h, table, N, None, 0, C.byref(count)))
+        out = np.empty(count.value)
+        _check(lib().ndg_tables_get(self._ctx.h, table, N, _ptr(out), out.size, C.byref(count)))
+        return out
+
+
+class Mesh2D_t:
+    """Mesh2D_t(zone, initial_N, maximum_N, ...) on one GPU
+    (include/meshes/Mesh2D_t.cuh:23-182): reference numbering of elements,
+    faces, ghosts and boundaries; device fields p, u, v, G and the RK register.
+
+    `mesh` is a Zone, a zone dict (tests/meshgen.py layout) or a .su2 path.
+    `n_instances` independent solutions share the mesh (batched runs).
+    device < 0 builds the topology only (no GPU).
+    """
+
+    def __init__(self, mesh, initial_N: int, maximum_N: int | None = None, n_interpolation_points: int = 2,
+                 max_split_level: int = 0, adaptivity_interval: int = 0, tolerance_min: float = 1e-6,
+                 tolerance_max: float = 1e-14, cfl: float = 0.5, n_instances: int = 1, device: int = 0,
+                 precision: int = FP64, keep_derivative: bool = False, stream: int | None = None):
+        self.initial_N_ = initial_N
+        self.maximum_N_ = maximum_N if maximum_N is not None else initial_N
+        self.adaptivity_interval_ = adaptivity_interval
+        self.n_instances = n_instances
+        self._ctx = _Context(device, stream)
+        h = self._ctx.h
+        if precision != FP64:
+            _check(lib().ndg_ctx_set_precision(h, precision))
+        if keep_derivative:
+            _check(lib().ndg_ctx_keep_derivative(h, 1))
+        p = _Params(initial_N, self.maximum_N_, n_interpolation_points, max_split_level, adaptivity_interval,
+                    tolerance_min, tolerance_max, cfl)
+        if isinstance(mesh, (str, os.PathLike)):
+            _check(lib().ndg_mesh_load_file(h, os.fspath(mesh).encode(), C.byref(p), n_instances))
+        else:
+            zone = mesh if isinstance(mesh, Zone) else Zone.from_dict(mesh)
+            z, keep = zone._struct()
+            _check(lib().ndg_mesh_load_zone(h, C.byref(z), C.byref(p), n_instances))
+            del keep
+        counts = [C.c_int64() for _ in range(4)]
+        _check(lib().ndg_mesh_counts(h, *[C.byref(c) for c in counts]))
+        self.n_elements_, self.n_elements_total_, self.n_faces_, self.n_nodes_ = (c.value for c in counts)
+        fs = C.c_int64()
+        _check(lib().ndg_mesh_field_size(h, C.byref(fs)))
+        self.field_size = fs.value
+
+    @property
+    def handle(self):
+        return self._ctx.h
+
+    def set_precision(self, precision: int) -> None:
+        _check(lib().ndg_ctx_set_precision(self._ctx.h, precision))
+
+    # Mesh2D_t::initial_conditions (src/meshes/Mesh2D_t.cu:5030)
+    def initial_conditions(self) -> None:
+        _check(lib().ndg_initial_conditions(self._ctx.h))
+
+    def set_field(self, name: str, values: np.ndarray, instance: int = -1) -> None:
+        values = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        expected = self.field_size * (self.n_instances if instance < 0 else 1)
+        if values.size != expected:
+            raise ValueError(f"expected {expected} values, got {values.size}")
+        _check(lib().ndg_set_field(self._ctx.h, instance, FIELDS[name], _ptr(values)))
+
+    def get_field(self, name: str, instance: int = -1) -> np.ndarray:
+        out = np.empty(self.field_size * (self.n_instances if instance < 0 else 1))
+        _check(lib().ndg_get_field(self._ctx.h, instance, FIELDS[name], _ptr(out)))
+        return out
+
+    def synchronize(self) -> None:
+        _check(lib().ndg_ctx_synchronize(self._ctx.h))
+
+    def time_stage(self, m: int, n_launches: int) -> float:
+        """Mean duration in ms of the stage-m kernel over n_launches launches (advances the state)."""
+        ms = C.c_double()
+        _check(lib().ndg_time_stage(self._ctx.h, m, n_launches, C.byref(ms)))
+        return ms.value
+
+    def launches(self) -> int:
+        n = C.c_int64()
+        _check(lib().ndg_launch_count(self._ctx.h, C.byref(n)))
+        return n.value
+
+    # Topology views with the reference's numbering.
+    def faces(self) -> dict:
+        F = self.n_faces_
+        d = {k: np.empty(2 * F, dtype=np.int64) for k in ("nodes", "elements", "sides")}
+        d["N"] = np.empty(F, dtype=np.int32)
+        for k in ("normal", "tangent", "offset", "scale"):
+            d[k] = np.empty(2 * F)
+        _check(lib().ndg_mesh_get_faces(self._ctx.h, *[_ptr(d[k]) for k in ("nodes", "elements", "sides", "N", "normal", "tangent", "offset", "scale")]))
+        return d
+
+    def elements(self) -> dict:
+        E = self.n_elements_total_
+        d = {"nodes": np.empty(4 * E, dtype=np.int64), "N": np.empty(E, dtype=np.int32), "delta_xy_min": np.empty(E),
+             "first_face": np.empty(4 * E, dtype=np.int64)}
+        _check(lib().ndg_mesh_get_elements(self._ctx.h, *[_ptr(d[k]) for k in ("nodes", "N", "delta_xy_min", "first_face")]))
+        return d
+
+    def boundary(self, kind: int) -> np.ndarray:
+        cnt = C.c_int64()
+        _check(lib().ndg_mesh_get_boundary(self._ctx.h, kind, None, 0, C.byref(cnt)))
+        out = np.empty(max(cnt.value, 1), dtype=np.int64)
+        _check(lib().ndg_mesh_get_boundary(self._ctx.h, kind, _ptr(out), out.size, C.byref(cnt)))
+        return out[:cnt.value]
+
+    def nodes(self) -> np.ndarray:
+        out = np.empty(2 * self.n_nodes_)
+        _check(lib().ndg_mesh_get_nodes(self._ctx.h, _ptr(out)))
+        return out.reshape(-1, 2)
+
+    def close(self) -> None:
+        self._ctx.close()
+
+
+class Solver2D_t:
+    """Solver2D_t(CFL, output_times, viscosity) (include/solvers/Solver2D_t.cuh:14-65):
+    the CFL step and the low-storage RK3 time loop on the GPU."""
+
+    def __init__(self, CFL: float = 0.5, output_times=(1.0,), viscosity: float = 0.0):
+        self.CFL_ = CFL
+        self.output_times_ = list(output_times)
+        self.viscosity_ = viscosity
+
+    @staticmethod
+    def get_delta_t(mesh: Mesh2D_t) -> float:
+        dt = C.c_double()
+        _check(lib().ndg_get_delta_t(mesh.handle, C.byref(dt)))
+        return dt.value
+
+    @staticmethod
+    def stage(mesh: Mesh2D_t, m: int, time: float, dt: float) -> None:
+        _check(lib().ndg_stage(mesh.handle, m, time, dt))
+
+    @staticmethod
+    def run(mesh: Mesh2D_t, n_steps: int, time: float = 0.0) -> float:
+        t = C.c_double(time)
+        _check(lib().ndg_run(mesh.handle, n_steps, C.byref(t)))
+        return t.value
+
+    def solve(self, mesh: Mesh2D_t, time: float = 0.0) -> tuple[float, int]:
+        """Steps to output_times_[-1] with the reference's shortened last step."""
+        t = C.c_double(time)
+        n = C.c_int64()
+        _check(lib().ndg_solve(mesh.handle, float(self.output_times_[-1]), C.byref(t), C.byref(n)))
+        return t.value, n.value
+
+
+def dof_count(mesh: Mesh2D_t) -> int:
+    """Degrees of freedom 3 * sum (N+1)^2 over elements and instances."""
+    return 3 * mesh.field_size * mesh.n_instances
+
+

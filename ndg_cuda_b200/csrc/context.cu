@@ -1,0 +1,658 @@
+// C ABI of the library (include/ndg_b200.h): contexts, tables, meshes,
+// fields and time stepping. Host orchestration only; the arithmetic is in
+// stage_kernels.cu.
+#include "ndg_internal.hpp"
+#include "stage_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace ndg {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& message) { g_last_error = message; }
+
+[[noreturn]] void fail(ndg_status status, const std::string& message) { throw Error{status, message}; }
+
+namespace {
+
+void check_cuda(cudaError_t err, const char* what) {
+    if (err != cudaSuccess) {
+        const ndg_status st = (err == cudaErrorMemoryAllocation) ? NDG_ERR_OOM : NDG_ERR_CUDA;
+        fail(st, std::string(what) + ": " + cudaGetErrorString(err));
+    }
+}
+
+template <typename T>
+struct DeviceBuffer {
+    T* ptr = nullptr;
+    size_t count = 0;
+    void allocate(size_t n) {
+        release();
+        if (n == 0) return;
+        check_cuda(cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)), "cudaMalloc");
+        count = n;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    ~DeviceBuffer() { release(); }
+};
+
+// Williamson low-storage RK3 coefficients (include/solvers/Solver2D_t.tpp:16-18).
+constexpr double kRkA[3] = {0, -5.0 / 9.0, -153.0 / 128.0};
+constexpr double kRkB[3] = {0, 1.0 / 3.0, 0.75};
+constexpr double kRkG[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+
+}  // namespace
+}  // namespace ndg
+
+struct ndg_ctx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int precision = NDG_FP64;
+    bool keep_derivative = false;
+
+    bool has_tables = false;
+    ndg::Tables tables;
+
+    bool has_mesh = false;
+    ndg::Topology topo;
+    ndg_mesh_params params{};
+    int n_instances = 1;
+    int N = 0;
+    int64_t K = 0;
+    int64_t field_size = 0;  // per field and instance
+
+    ndg::DeviceBuffer<double> q, k, G, tr[2], corners, normal, gscale, inflow, dxy, step, scratch;
+    ndg::DeviceBuffer<int32_t> link, elem_N;
+    int cur = 0;
+    bool traces_valid = false;
+    double dt_mesh = 0.0;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int64_t launches = 0;
+
+    ~ndg_ctx() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace ndg {
+namespace {
+
+bool strict(const ndg_ctx* c) { return c->precision == NDG_FP64_STRICT; }
+
+void require_device(const ndg_ctx* c) {
+    if (c->device < 0) fail(NDG_ERR_INVALID_ARG, "this call needs a GPU context (device >= 0)");
+}
+
+void require_mesh(const ndg_ctx* c) {
+    if (!c->has_mesh) fail(NDG_ERR_INVALID_ARG, "no mesh loaded");
+}
+
+void make_current(const ndg_ctx* c) {
+    if (c->device >= 0) check_cuda(cudaSetDevice(c->device), "cudaSetDevice");
+}
+
+void drop_graphs(ndg_ctx* c) {
+    for (auto& g : c->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+dev::StageArgs stage_args(ndg_ctx* c, int m, int in) {
+    dev::StageArgs a{};
+    a.q = c->q.ptr;
+    a.k = c->k.ptr;
+    a.trace_in = c->tr[in].ptr;
+    a.trace_out = c->tr[1 - in].ptr;
+    a.G_out = c->keep_derivative ? c->G.ptr : nullptr;
+    a.corners = c->corners.ptr;
+    a.link = reinterpret_cast<const int2*>(c->link.ptr);
+    a.normal = reinterpret_cast<const double2*>(c->normal.ptr);
+    a.gscale = c->gscale.ptr;
+    a.inflow = reinterpret_cast<const double4*>(c->inflow.ptr);
+    a.step = c->step.ptr;
+    a.rk_a = kRkA[m];
+    a.rk_b = kRkB[m];
+    a.rk_g = kRkG[m];
+    a.first = m == 0;
+    a.n_elements = c->K;
+    a.n_instances = c->n_instances;
+    return a;
+}
+
+void launch_stage(ndg_ctx* c, int m) {
+    const dev::StageArgs a = stage_args(c, m, c->cur);
+    check_cuda(dev::launch_stage(c->N, strict(c), a, c->stream), "stage kernel launch");
+    c->cur = 1 - c->cur;
+    ++c->launches;
+}
+
+void ensure_traces(ndg_ctx* c) {
+    if (c->traces_valid) return;
+    dev::TraceArgs a{c->q.ptr, c->tr[c->cur].ptr, c->K, c->n_instances};
+    check_cuda(dev::launch_traces(c->N, strict(c), a, c->stream), "trace kernel launch");
+    ++c->launches;
+    c->traces_valid = true;
+}
+
+void set_step(ndg_ctx* c, double time, double dt, double t_end) {
+    const double host[4] = {time, dt, c->dt_mesh, t_end};
+    check_cuda(cudaMemcpyAsync(c->step.ptr, host, sizeof(host), cudaMemcpyHostToDevice, c->stream), "step upload");
+    check_cuda(cudaStreamSynchronize(c->stream), "step upload");
+}
+
+// One RK3 step as a CUDA graph: three stage kernels and the time update,
+// for each parity of the trace double buffer.
+void ensure_graphs(ndg_ctx* c) {
+    if (c->graph[0] && c->graph[1]) return;
+    for (int parity = 0; parity < 2; ++parity) {
+        cudaGraph_t g = nullptr;
+        check_cuda(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+        cudaError_t err = cudaSuccess;
+        for (int m = 0; m < 3 && err == cudaSuccess; ++m) {
+            const dev::StageArgs a = stage_args(c, m, (parity + m) & 1);
+            err = dev::launch_stage(c->N, strict(c), a, c->stream);
+        }
+        if (err == cudaSuccess) err = dev::launch_end_step(c->step.ptr, c->stream);
+        cudaError_t end = cudaStreamEndCapture(c->stream, &g);
+        check_cuda(err, "graph capture launch");
+        check_cuda(end, "graph capture end");
+        cudaGraphExec_t exec = nullptr;
+        err = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        check_cuda(err, "graph instantiate");
+        c->graph[parity] = exec;
+    }
+}
+
+void run_steps(ndg_ctx* c, int64_t n_steps) {
+    ensure_traces(c);
+    ensure_graphs(c);
+    for (int64_t s = 0; s < n_steps; ++s) {
+        check_cuda(cudaGraphLaunch(c->graph[c->cur], c->stream), "graph launch");
+        c->cur = 1 - c->cur;  // three stages flip the trace buffer an odd number of times
+        c->launches += 4;
+    }
+}
+
+double* field_ptr(ndg_ctx* c, int32_t field, int instance) {
+    const int64_t per_inst = 3 * c->field_size;
+    if (field >= NDG_FIELD_P && field <= NDG_FIELD_V) return c->q.ptr + instance * per_inst + field * c->field_size;
+    if (field >= NDG_FIELD_K_P && field <= NDG_FIELD_K_V) return c->k.ptr + instance * per_inst + (field - NDG_FIELD_K_P) * c->field_size;
+    if (field >= NDG_FIELD_G_P && field <= NDG_FIELD_G_V) {
+        if (!c->keep_derivative) fail(NDG_ERR_INVALID_ARG, "time derivative fields need ndg_ctx_keep_derivative(ctx, 1) before stepping");
+        return c->G.ptr + instance * per_inst + (field - NDG_FIELD_G_P) * c->field_size;
+    }
+    fail(NDG_ERR_INVALID_ARG, "unknown field");
+}
+
+void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_instances) {
+    if (n_instances < 1) fail(NDG_ERR_INVALID_ARG, "n_instances must be >= 1");
+    if (p.initial_N < 1 || p.initial_N > p.maximum_N) fail(NDG_ERR_INVALID_ARG, "need 1 <= initial_N <= maximum_N");
+    if (!(p.cfl > 0.0)) fail(NDG_ERR_INVALID_ARG, "cfl must be positive");
+    if (!c->has_tables || c->tables.N_max < p.maximum_N) {
+        c->tables = build_tables(p.maximum_N, p.n_interpolation_points > 1 ? p.n_interpolation_points : 2);
+        c->has_tables = true;
+        if (c->device >= 0) check_cuda(dev::upload_tables(c->tables), "table upload");
+    }
+    compute_geometry(topo, c->tables);
+    c->topo = std::move(topo);
+    c->params = p;
+    c->n_instances = n_instances;
+    c->N = p.initial_N;
+    c->K = c->topo.n_domain;
+    c->field_size = c->K * (c->N + 1) * (c->N + 1);
+    c->has_mesh = true;
+    c->traces_valid = false;
+    c->cur = 0;
+    drop_graphs(c);
+    if (c->device < 0) return;
+
+    if (c->N > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "orders above 16 have no compiled kernel");
+    const SidePlan plan = build_side_plan(c->topo, c->tables);
+    const size_t per_field = static_cast<size_t>(c->field_size);
+    const size_t n = static_cast<size_t>(c->N + 1);
+    const size_t K = static_cast<size_t>(c->K);
+    const size_t inst = static_cast<size_t>(n_instances);
+    c->q.allocate(inst * 3 * per_field);
+    c->k.allocate(inst * 3 * per_field);
+    c->G.release();
+    if (c->keep_derivative) c->G.allocate(inst * 3 * per_field);
+    c->tr[0].allocate(inst * 3 * K * 4 * n);
+    c->tr[1].allocate(inst * 3 * K * 4 * n);
+    c->corners.allocate(plan.corners.size());
+    c->normal.allocate(plan.normal.size());
+    c->gscale.allocate(plan.gscale.size());
+    c->inflow.allocate(plan.inflow_xy.size());
+    c->link.allocate(plan.link.size());
+    c->dxy.allocate(K);
+    c->elem_N.allocate(K);
+    c->step.allocate(4);
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream), "mesh upload");
+    };
+    up(c->corners.ptr, plan.corners.data(), plan.corners.size() * sizeof(double));
+    up(c->normal.ptr, plan.normal.data(), plan.normal.size() * sizeof(double));
+    up(c->gscale.ptr, plan.gscale.data(), plan.gscale.size() * sizeof(double));
+    up(c->inflow.ptr, plan.inflow_xy.data(), plan.inflow_xy.size() * sizeof(double));
+    up(c->link.ptr, plan.link.data(), plan.link.size() * sizeof(int32_t));
+    up(c->dxy.ptr, c->topo.delta_xy_min.data(), K * sizeof(double));
+    std::vector<int32_t> eN(c->topo.elem_N.begin(), c->topo.elem_N.begin() + static_cast<std::ptrdiff_t>(K));
+    up(c->elem_N.ptr, eN.data(), K * sizeof(int32_t));
+    check_cuda(cudaMemsetAsync(c->q.ptr, 0, c->q.count * sizeof(double), c->stream), "memset");
+    check_cuda(cudaMemsetAsync(c->k.ptr, 0, c->k.count * sizeof(double), c->stream), "memset");
+    check_cuda(dev::prepare_kernels(c->N, false), "kernel attributes");
+    check_cuda(dev::prepare_kernels(c->N, true), "kernel attributes");
+    // CFL step of the fixed mesh, reduced on the device (Solver2D_t.cu:17-31).
+    check_cuda(dev::launch_delta_t(c->dxy.ptr, c->elem_N.ptr, c->K, p.cfl, c->step.ptr + 2, c->stream), "delta_t kernel");
+    ++c->launches;
+    check_cuda(cudaMemcpyAsync(&c->dt_mesh, c->step.ptr + 2, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "delta_t readback");
+    check_cuda(cudaStreamSynchronize(c->stream), "mesh load");
+}
+
+template <typename F>
+ndg_status guarded(F&& f) {
+    try {
+        f();
+        set_last_error("");
+        return NDG_OK;
+    } catch (const Error& e) {
+        set_last_error(e.message);
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return NDG_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return NDG_ERR_INVALID_ARG;
+    }
+}
+
+void copy_table(const Tables& t, int32_t table, int32_t N, double* out, int64_t capacity, int64_t* count) {
+    if (table < 0 || table > 11) fail(NDG_ERR_INVALID_ARG, "unknown table");
+    if (N < 0 || N > t.N_max) fail(NDG_ERR_INVALID_ARG, "order outside the tables");
+    const auto& v = t.get(static_cast<ndg_table>(table), N);
+    if (count) *count = static_cast<int64_t>(v.size());
+    if (out) {
+        if (capacity < static_cast<int64_t>(v.size())) fail(NDG_ERR_INVALID_ARG, "output buffer too small");
+        std::memcpy(out, v.data(), v.size() * sizeof(double));
+    }
+}
+
+}  // namespace
+}  // namespace ndg
+
+using namespace ndg;
+
+extern "C" {
+
+const char* ndg_last_error(void) { return g_last_error.c_str(); }
+
+const char* ndg_version(void) { return "ndg_b200 0.1.0 (sm_100a)"; }
+
+ndg_status ndg_ctx_create(int32_t device, void* stream, ndg_ctx** out) {
+    return guarded([&] {
+        if (!out) fail(NDG_ERR_INVALID_ARG, "out is NULL");
+        auto c = std::make_unique<ndg_ctx>();
+        c->device = device;
+        if (device >= 0) {
+            int count = 0;
+            check_cuda(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+            if (device >= count) fail(NDG_ERR_INVALID_ARG, "no such device");
+            check_cuda(cudaSetDevice(device), "cudaSetDevice");
+            if (stream) {
+                c->stream = static_cast<cudaStream_t>(stream);
+            } else {
+                check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+                c->own_stream = true;
+            }
+        }
+        *out = c.release();
+    });
+}
+
+ndg_status ndg_ctx_destroy(ndg_ctx* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        if (ctx->device >= 0) {
+            cudaSetDevice(ctx->device);
+            cudaStreamSynchronize(ctx->stream);
+        }
+        delete ctx;
+    });
+}
+
+ndg_status ndg_ctx_set_precision(ndg_ctx* ctx, int32_t precision) {
+    return guarded([&] {
+        if (!ctx) fail(NDG_ERR_INVALID_ARG, "ctx is NULL");
+        if (precision == NDG_FP32) fail(NDG_ERR_UNSUPPORTED, "the FP32 form is not built yet");
+        if (precision != NDG_FP64 && precision != NDG_FP64_STRICT) fail(NDG_ERR_INVALID_ARG, "unknown precision");
+        if (ctx->precision != precision) drop_graphs(ctx);
+        ctx->precision = precision;
+    });
+}
+
+ndg_status ndg_ctx_keep_derivative(ndg_ctx* ctx, int32_t enable) {
+    return guarded([&] {
+        if (!ctx) fail(NDG_ERR_INVALID_ARG, "ctx is NULL");
+        make_current(ctx);
+        ctx->keep_derivative = enable != 0;
+        drop_graphs(ctx);
+        if (ctx->has_mesh && ctx->device >= 0) {
+            if (ctx->keep_derivative) {
+                ctx->G.allocate(static_cast<size_t>(3 * ctx->field_size * ctx->n_instances));
+                check_cuda(cudaMemsetAsync(ctx->G.ptr, 0, ctx->G.count * sizeof(double), ctx->stream), "memset");
+            } else {
+                ctx->G.release();
+            }
+        }
+    });
+}
+
+ndg_status ndg_ctx_synchronize(ndg_ctx* ctx) {
+    return guarded([&] {
+        if (!ctx) fail(NDG_ERR_INVALID_ARG, "ctx is NULL");
+        if (ctx->device >= 0) {
+            make_current(ctx);
+            check_cuda(cudaStreamSynchronize(ctx->stream), "synchronize");
+        }
+    });
+}
+
+ndg_status ndg_tables_build(ndg_ctx* ctx, int32_t N_max, int64_t n_interp) {
+    return guarded([&] {
+        if (!ctx) fail(NDG_ERR_INVALID_ARG, "ctx is NULL");
+        make_current(ctx);
+        ctx->tables = build_tables(N_max, n_interp);
+        ctx->has_tables = true;
+        if (ctx->device >= 0) check_cuda(dev::upload_tables(ctx->tables), "table upload");
+    });
+}
+
+ndg_status ndg_tables_get(const ndg_ctx* ctx, int32_t table, int32_t N, double* out, int64_t capacity, int64_t* count) {
+    return guarded([&] {
+        if (!ctx || !ctx->has_tables) fail(NDG_ERR_INVALID_ARG, "no tables built");
+        copy_table(ctx->tables, table, N, out, capacity, count);
+    });
+}
+
+ndg_status ndg_tables_compute(int32_t N_max, int64_t n_interp, int32_t table, int32_t N, double* out, int64_t capacity, int64_t* count) {
+    return guarded([&] {
+        const Tables t = build_tables(N_max, n_interp);
+        copy_table(t, table, N, out, capacity, count);
+    });
+}
+
+ndg_status ndg_mesh_load_zone(ndg_ctx* ctx, const ndg_zone* zone, const ndg_mesh_params* params, int32_t n_instances) {
+    return guarded([&] {
+        if (!ctx || !zone || !params) fail(NDG_ERR_INVALID_ARG, "NULL argument");
+        make_current(ctx);
+        load_mesh(ctx, build_topology(*zone, params->initial_N), *params, n_instances);
+    });
+}
+
+ndg_status ndg_mesh_load_file(ndg_ctx* ctx, const char* path, const ndg_mesh_params* params, int32_t n_instances) {
+    return guarded([&] {
+        if (!ctx || !path || !params) fail(NDG_ERR_INVALID_ARG, "NULL argument");
+        make_current(ctx);
+        std::string p(path);
+        std::string ext = p.size() >= 4 ? p.substr(p.size() - 4) : "";
+        for (auto& ch : ext) ch = static_cast<char>(std::tolower(static_cast<unsigned char>(ch)));
+        if (ext == ".su2") {
+            load_mesh(ctx, read_su2(p, params->initial_N), *params, n_instances);
+        } else if (p.size() >= 5 && (p.substr(p.size() - 5) == ".cgns" || p.substr(p.size() - 5) == ".CGNS")) {
+            fail(NDG_ERR_UNSUPPORTED, "this build has no CGNS library; pass the zone arrays to ndg_mesh_load_zone");
+        } else {
+            fail(NDG_ERR_INVALID_ARG, "extension not recognised (.su2 or .cgns)");
+        }
+    });
+}
+
+ndg_status ndg_mesh_counts(const ndg_ctx* ctx, int64_t* n_elements, int64_t* n_elements_total, int64_t* n_faces, int64_t* n_nodes) {
+    return guarded([&] {
+        require_mesh(ctx);
+        if (n_elements) *n_elements = ctx->topo.n_domain;
+        if (n_elements_total) *n_elements_total = static_cast<int64_t>(ctx->topo.elem_nodes.size());
+        if (n_faces) *n_faces = static_cast<int64_t>(ctx->topo.face_nodes.size());
+        if (n_nodes) *n_nodes = static_cast<int64_t>(ctx->topo.node_x.size());
+    });
+}
+
+ndg_status ndg_mesh_get_faces(const ndg_ctx* ctx, int64_t* nodes, int64_t* elements, int64_t* sides, int32_t* N, double* normal, double* tangent, double* offset, double* scale) {
+    return guarded([&] {
+        require_mesh(ctx);
+        const auto& t = ctx->topo;
+        for (size_t f = 0; f < t.face_nodes.size(); ++f) {
+            for (size_t k = 0; k < 2; ++k) {
+                if (nodes) nodes[2 * f + k] = t.face_nodes[f][k];
+                if (elements) elements[2 * f + k] = t.face_elems[f][k];
+                if (sides) sides[2 * f + k] = t.face_sides[f][k];
+                if (normal) normal[2 * f + k] = t.face_normal[f][k];
+                if (tangent) tangent[2 * f + k] = t.face_tangent[f][k];
+                if (offset) offset[2 * f + k] = t.face_offset[f][k];
+                if (scale) scale[2 * f + k] = t.face_scale[f][k];
+            }
+            if (N) N[f] = t.face_N[f];
+        }
+    });
+}
+
+ndg_status ndg_mesh_get_elements(const ndg_ctx* ctx, int64_t* nodes, int32_t* N, double* delta_xy_min, int64_t* first_face) {
+    return guarded([&] {
+        require_mesh(ctx);
+        const auto& t = ctx->topo;
+        for (size_t e = 0; e < t.elem_nodes.size(); ++e) {
+            for (size_t k = 0; k < 4; ++k) {
+                if (nodes) nodes[4 * e + k] = t.elem_nodes[e][k];
+                if (first_face) first_face[4 * e + k] = t.elem_face[e][k];
+            }
+            if (N) N[e] = t.elem_N[e];
+            if (delta_xy_min) delta_xy_min[e] = t.delta_xy_min[e];
+        }
+    });
+}
+
+ndg_status ndg_mesh_get_boundary(const ndg_ctx* ctx, int32_t list, int64_t* out, int64_t capacity, int64_t* count) {
+    return guarded([&] {
+        require_mesh(ctx);
+        const auto& t = ctx->topo;
+        const std::vector<int64_t>* v = nullptr;
+        switch (list) {
+            case NDG_LIST_WALL: v = &t.boundary[kWall]; break;
+            case NDG_LIST_SYMMETRY: v = &t.boundary[kSymmetry]; break;
+            case NDG_LIST_INFLOW: v = &t.boundary[kInflow]; break;
+            case NDG_LIST_OUTFLOW: v = &t.boundary[kOutflow]; break;
+            case NDG_LIST_INTERFACE_ORIGIN: v = &t.if_origin; break;
+            case NDG_LIST_INTERFACE_ORIGIN_SIDE: v = &t.if_origin_side; break;
+            case NDG_LIST_INTERFACE_DESTINATION: v = &t.if_destination; break;
+            default: fail(NDG_ERR_INVALID_ARG, "unknown boundary list");
+        }
+        if (count) *count = static_cast<int64_t>(v->size());
+        if (out) {
+            if (capacity < static_cast<int64_t>(v->size())) fail(NDG_ERR_INVALID_ARG, "output buffer too small");
+            std::memcpy(out, v->data(), v->size() * sizeof(int64_t));
+        }
+    });
+}
+
+ndg_status ndg_mesh_get_nodes(const ndg_ctx* ctx, double* xy) {
+    return guarded([&] {
+        require_mesh(ctx);
+        for (size_t i = 0; i < ctx->topo.node_x.size(); ++i) {
+            xy[2 * i] = ctx->topo.node_x[i];
+            xy[2 * i + 1] = ctx->topo.node_y[i];
+        }
+    });
+}
+
+ndg_status ndg_mesh_field_size(const ndg_ctx* ctx, int64_t* n_values) {
+    return guarded([&] {
+        require_mesh(ctx);
+        *n_values = ctx->field_size;
+    });
+}
+
+ndg_status ndg_initial_conditions(ndg_ctx* ctx) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        make_current(ctx);
+        check_cuda(dev::launch_initial_conditions(ctx->q.ptr, ctx->k.ptr, ctx->corners.ptr, ctx->N, ctx->K, ctx->n_instances, ctx->stream), "initial condition kernel");
+        ++ctx->launches;
+        if (ctx->keep_derivative) check_cuda(cudaMemsetAsync(ctx->G.ptr, 0, ctx->G.count * sizeof(double), ctx->stream), "memset");
+        ctx->traces_valid = false;
+    });
+}
+
+ndg_status ndg_set_field(ndg_ctx* ctx, int32_t instance, int32_t field, const double* values) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (!values) fail(NDG_ERR_INVALID_ARG, "values is NULL");
+        if (instance >= ctx->n_instances) fail(NDG_ERR_INVALID_ARG, "instance out of range");
+        make_current(ctx);
+        const int first = instance < 0 ? 0 : instance;
+        const int last = instance < 0 ? ctx->n_instances : instance + 1;
+        for (int i = first; i < last; ++i) {
+            double* dst = field_ptr(ctx, field, i);
+            check_cuda(cudaMemcpyAsync(dst, values + (i - first) * ctx->field_size, static_cast<size_t>(ctx->field_size) * sizeof(double),
+                                       cudaMemcpyHostToDevice, ctx->stream),
+                       "field upload");
+        }
+        if (field <= NDG_FIELD_V) ctx->traces_valid = false;
+    });
+}
+
+ndg_status ndg_get_field(ndg_ctx* ctx, int32_t instance, int32_t field, double* values) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (!values) fail(NDG_ERR_INVALID_ARG, "values is NULL");
+        if (instance >= ctx->n_instances) fail(NDG_ERR_INVALID_ARG, "instance out of range");
+        make_current(ctx);
+        const int first = instance < 0 ? 0 : instance;
+        const int last = instance < 0 ? ctx->n_instances : instance + 1;
+        for (int i = first; i < last; ++i) {
+            const double* src = field_ptr(ctx, field, i);
+            check_cuda(cudaMemcpyAsync(values + (i - first) * ctx->field_size, src, static_cast<size_t>(ctx->field_size) * sizeof(double),
+                                       cudaMemcpyDeviceToHost, ctx->stream),
+                       "field download");
+        }
+        check_cuda(cudaStreamSynchronize(ctx->stream), "field download");
+    });
+}
+
+ndg_status ndg_get_delta_t(ndg_ctx* ctx, double* delta_t) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (!delta_t) fail(NDG_ERR_INVALID_ARG, "delta_t is NULL");
+        *delta_t = ctx->dt_mesh;
+    });
+}
+
+ndg_status ndg_stage(ndg_ctx* ctx, int32_t m, double time, double dt) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (m < 0 || m > 2) fail(NDG_ERR_INVALID_ARG, "stage index must be 0, 1 or 2");
+        make_current(ctx);
+        set_step(ctx, time, dt, std::numeric_limits<double>::infinity());
+        ensure_traces(ctx);
+        launch_stage(ctx, m);
+    });
+}
+
+ndg_status ndg_run(ndg_ctx* ctx, int64_t n_steps, double* time) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (n_steps < 0) fail(NDG_ERR_INVALID_ARG, "n_steps must be >= 0");
+        make_current(ctx);
+        const double t0 = time ? *time : 0.0;
+        set_step(ctx, t0, ctx->dt_mesh, std::numeric_limits<double>::infinity());
+        run_steps(ctx, n_steps);
+        // The device advances time by the same FP64 additions.
+        double t = t0;
+        for (int64_t s = 0; s < n_steps; ++s) t += ctx->dt_mesh;
+        if (time) *time = t;
+    });
+}
+
+ndg_status ndg_solve(ndg_ctx* ctx, double t_end, double* time, int64_t* n_steps) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        make_current(ctx);
+        const double t0 = time ? *time : 0.0;
+        // Step count of the reference loop (Solver2D_t.tcu:35-42): the last
+        // step is shortened to land on t_end.
+        int64_t steps = 0;
+        double t = t0;
+        while (t < t_end) {
+            double dt = ctx->dt_mesh;
+            if (t + dt > t_end) dt = t_end - t;
+            t += dt;
+            ++steps;
+        }
+        const double dt0 = (t0 + ctx->dt_mesh > t_end) ? t_end - t0 : ctx->dt_mesh;
+        set_step(ctx, t0, dt0, t_end);
+        run_steps(ctx, steps);
+        if (time) *time = t;
+        if (n_steps) *n_steps = steps;
+    });
+}
+
+ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* avg_ms) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (m < 0 || m > 2 || n_launches < 1 || !avg_ms) fail(NDG_ERR_INVALID_ARG, "bad stage timing request");
+        make_current(ctx);
+        ensure_traces(ctx);
+        std::vector<cudaEvent_t> ev(static_cast<size_t>(2 * n_launches));
+        for (auto& e : ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+        for (int i = 0; i < n_launches; ++i) {
+            check_cuda(cudaEventRecord(ev[static_cast<size_t>(2 * i)], ctx->stream), "cudaEventRecord");
+            launch_stage(ctx, m);
+            check_cuda(cudaEventRecord(ev[static_cast<size_t>(2 * i + 1)], ctx->stream), "cudaEventRecord");
+        }
+        check_cuda(cudaStreamSynchronize(ctx->stream), "stage timing");
+        double total = 0.0;
+        for (int i = 0; i < n_launches; ++i) {
+            float ms = 0.0f;
+            check_cuda(cudaEventElapsedTime(&ms, ev[static_cast<size_t>(2 * i)], ev[static_cast<size_t>(2 * i + 1)]), "cudaEventElapsedTime");
+            total += ms;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        *avg_ms = total / n_launches;
+    });
+}
+
+ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches) {
+    return guarded([&] {
+        if (!ctx || !launches) fail(NDG_ERR_INVALID_ARG, "NULL argument");
+        *launches = ctx->launches;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// Internal types shared by the host (C++) and device (CUDA) parts of the
+// library. Not installed; the public surface is include/ndg_b200.h.
+#pragma once
+
+#include "../../include/ndg_b200.h"
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ndg {
+
+constexpr int kMaxOrder = 16;  // highest polynomial order with a compiled kernel
+
+// ---------------------------------------------------------------------------
+// Errors: every C entry point converts an ndg::Error into a status and a
+// thread-local message.
+struct Error {
+    ndg_status status;
+    std::string message;
+};
+[[noreturn]] void fail(ndg_status status, const std::string& message);
+void set_last_error(const std::string& message);
+
+// ---------------------------------------------------------------------------
+// Polynomial tables of NDG_t<LegendrePolynomial_t>, one vector per order.
+struct Tables {
+    int N_max = -1;
+    int64_t n_interp = 0;
+    // [table][N] with table in ndg_table order.
+    std::array<std::vector<std::vector<double>>, 12> t;
+    const std::vector<double>& get(ndg_table table, int N) const { return t[table][static_cast<size_t>(N)]; }
+};
+Tables build_tables(int N_max, int64_t n_interp);
+bool almost_equal(double x, double y);
+
+// ---------------------------------------------------------------------------
+// Mesh topology with the reference's numbering.
+enum BoundaryKind : int { kWall = 0, kSymmetry = 1, kInflow = 2, kOutflow = 3 };
+
+struct Topology {
+    std::vector<double> node_x, node_y;
+    int64_t n_domain = 0;                 // domain elements come first
+    std::vector<int> elem_N;              // all elements
+    std::vector<std::array<int64_t, 4>> elem_nodes;
+    std::vector<std::array<int64_t, 4>> elem_face;  // face of each side, -1 when none
+    // faces
+    std::vector<int> face_N;
+    std::vector<std::array<int64_t, 2>> face_nodes, face_elems, face_sides;
+    std::vector<std::array<double, 2>> face_normal, face_tangent, face_offset, face_scale;
+    std::vector<double> face_length;
+    // boundaries and self interfaces
+    std::array<std::vector<int64_t>, 4> boundary;
+    std::vector<int64_t> if_origin, if_origin_side, if_destination;
+    // geometry
+    std::vector<double> delta_xy_min;
+    std::vector<std::array<double, 2>> center;
+    std::vector<std::array<double, 4>> ghost_scale;  // scaling_factor_[s] (constant along a straight side)
+};
+
+Topology build_topology(const ndg_zone& zone, int initial_N);
+Topology read_su2(const std::string& path, int initial_N);
+void compute_geometry(Topology& topo, const Tables& tables);
+
+// ---------------------------------------------------------------------------
+// Device plan of one mesh for the fused stage kernels (uniform order N,
+// conforming faces). Per domain element side:
+//   link.x = neighbour element whose side trace feeds the face (-1: none),
+//   link.y = neighbour side | kind << 2 | role << 5,
+// where kind is a SideKind and role is 1 when the element is the face's
+// right (second) element.
+enum SideKind : int { kInterior = 0, kMirror = 1, kCopy = 2, kAnalytic = 3, kZero = 4 };
+
+struct SidePlan {
+    std::vector<int32_t> link;      // 2 per side, 8 per element
+    std::vector<double> normal;     // 2 per side, 8 per element
+    std::vector<double> gscale;     // ghost scaling factor per side (kMirror/kCopy), 4 per element
+    std::vector<double> inflow_xy;  // 4 per side (ghost end points, kAnalytic), 16 per element
+    std::vector<double> corners;    // 8 per element: x0, y0, x1, y1, x2, y2, x3, y3
+};
+SidePlan build_side_plan(const Topology& topo, const Tables& tables);
+
+}  // namespace ndg

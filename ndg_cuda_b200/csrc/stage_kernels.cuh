@@ -1,0 +1,51 @@
+// Device entry points of the fused stage kernels (stage_kernels.cu).
+#pragma once
+
+#include "ndg_internal.hpp"
+
+#include <cuda_runtime.h>
+
+namespace ndg {
+namespace dev {
+
+// Arguments of one RK3 stage over all elements and instances.
+// Layouts (FP64): q, k, G_out: [instance][field p,u,v][element][(N+1)^2];
+// traces: [instance][field][element][side][N+1]; per element side: link,
+// normal, gscale, inflow ([element][side]); corners: [element][8].
+struct StageArgs {
+    double* q;
+    double* k;
+    const double* trace_in;
+    double* trace_out;
+    double* G_out;  // optional copy of the stage's time derivative
+    const double* corners;
+    const int2* link;
+    const double2* normal;
+    const double* gscale;
+    const double4* inflow;
+    const double* step;  // {time, dt, dt_mesh, t_end}
+    double rk_a, rk_b, rk_g;
+    int first;
+    int64_t n_elements;
+    int n_instances;
+};
+
+struct TraceArgs {
+    const double* q;
+    double* trace_out;
+    int64_t n_elements;
+    int n_instances;
+};
+
+cudaError_t prepare_kernels(int N, bool strict);
+cudaError_t launch_stage(int N, bool strict, const StageArgs& a, cudaStream_t stream);
+cudaError_t launch_traces(int N, bool strict, const TraceArgs& a, cudaStream_t stream);
+cudaError_t launch_initial_conditions(double* q, double* k, const double* corners, int N, int64_t K, int n_instances, cudaStream_t stream);
+cudaError_t launch_delta_t(const double* delta_xy_min, const int* elem_N, int64_t K, double cfl, double* out, cudaStream_t stream);
+cudaError_t launch_begin_step(double* step, cudaStream_t stream);
+cudaError_t launch_end_step(double* step, cudaStream_t stream);
+cudaError_t upload_tables(const Tables& t);
+int elements_per_block(int N);
+
+}  // namespace dev
+}  // namespace ndg

@@ -52,6 +52,7 @@ def _load_ref():
         lib.ndgref_zone_add_boco.argtypes = [C.c_char_p, C.c_int, _lp, C.c_long]
         lib.ndgref_zone_add_conn.argtypes = [C.c_char_p, _lp, _lp, C.c_long]
         lib.ndgref_create.argtypes = [C.c_int, C.c_int, C.c_long, C.c_int, C.c_long, C.c_double, C.c_double, C.c_double]
+        lib.ndgref_create_file.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_long, C.c_double]
         lib.ndgref_table.argtypes = [C.c_int, C.c_long, C.c_int, C.c_int, _dp]
         lib.ndgref_counts.argtypes = [C.POINTER(C.c_long)] * 4
         lib.ndgref_get_delta_t.restype = C.c_double
@@ -128,11 +129,15 @@ class _Base:
 class RefSolver(_Base):
     """The reference's own SEM::Host path (one process holds one instance)."""
 
-    def __init__(self, zone: dict, N: int, N_max: int | None = None, cfl: float = 0.5, n_interp: int = 2,
+    def __init__(self, zone: dict | str, N: int, N_max: int | None = None, cfl: float = 0.5, n_interp: int = 2,
                  max_split_level: int = 0, adaptivity_interval: int = 0,
                  tolerance_min: float = 1e-6, tolerance_max: float = 1e-14):
         lib = _load_ref()
         self.lib = lib
+        if isinstance(zone, str):
+            lib.ndgref_create_file(zone.encode(), N, N_max if N_max is not None else N, n_interp, cfl)
+            self._refresh_counts()
+            return
         lib.ndgref_zone_reset(len(zone["x"]), np.ascontiguousarray(zone["x"]), np.ascontiguousarray(zone["y"]))
         for name, typ, start, end, conn in zone["sections"]:
             conn = np.ascontiguousarray(conn, dtype=np.int64)

@@ -113,6 +113,16 @@ int ndgref_create(int initial_N, int maximum_N, long n_interpolation_points, int
     return 0;
 }
 
+// Same, reading a mesh file through the reference's own readers
+// (Mesh2D_t::read_su2 for .su2).
+int ndgref_create_file(const char* path, int initial_N, int maximum_N, long n_interpolation_points, double cfl) {
+    g_ref.mesh.reset();
+    g_ref.ndg = std::make_unique<NDG>(maximum_N, static_cast<size_t>(n_interpolation_points));
+    g_ref.mesh = std::make_unique<Mesh2D_t>(path, initial_N, maximum_N, static_cast<size_t>(n_interpolation_points), 0, 0, 0, 1e-6, 1e-14, 0.0, g_ref.ndg->nodes_, std::vector<double>{1.0});
+    g_ref.solver = std::make_unique<Solver2D_t>(cfl, std::vector<double>{1.0}, 0.0);
+    return 0;
+}
+
 void ndgref_destroy() {
     g_ref.mesh.reset();
     g_ref.solver.reset();
