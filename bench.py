@@ -232,7 +232,7 @@ def run_ours(args) -> None:
     traffic = profiled_traffic()
 
     # End to end through the C ABI with pinned host buffers.
-    e2e_steps = 2
+    e2e_steps = 0 if args.no_e2e else 2
     host = {f: torch.empty(mesh.field_size, dtype=torch.float64, pin_memory=True) for f in ("p", "u", "v")}
     for f in host:
         host[f].copy_(torch.from_numpy(mesh.get_field(f)))
@@ -245,7 +245,8 @@ def run_ours(args) -> None:
         for i, f in enumerate(("p", "u", "v")):
             ndg._check(L.ndg_get_field(mesh.handle, 0, i, host[f].data_ptr()))
 
-    e2e_call()  # warm-up
+    if e2e_steps:
+        e2e_call()  # warm-up
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     wall0 = time.perf_counter()
@@ -259,7 +260,7 @@ def run_ours(args) -> None:
     e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * dof * 3 * CONFIG_STEPS * e2e_steps / (float(e2e_t.item()) / 1e3)
+    e2e_value = world * dof * 3 * CONFIG_STEPS * e2e_steps / (float(e2e_t.item()) / 1e3) if e2e_steps else None
     state_bytes = 3 * mesh.field_size * 8
 
     cpu = None
@@ -294,7 +295,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=CONFIG_STEPS)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference timing (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -75,10 +75,13 @@ struct ndg_ctx {
     int n_instances = 1;
     int N = 0;
     int64_t K = 0;
-    int64_t field_size = 0;  // per field and instance
+    int64_t field_size = 0;  // values per field and instance seen through the API: K (N+1)^2
+    int64_t Kp = 0;          // elements per device field block: K rounded up to even
+    int64_t block = 0;       // values per device field block: Kp (N+1)^2
 
     ndg::DeviceBuffer<double> q, k, G, tr[2], corners, normal, gscale, inflow, dxy, step, scratch;
     ndg::DeviceBuffer<int32_t> link, elem_N;
+    ndg::DeviceBuffer<unsigned> error;
     int cur = 0;
     bool traces_valid = false;
     double dt_mesh = 0.0;
@@ -117,6 +120,19 @@ void drop_graphs(ndg_ctx* c) {
     }
 }
 
+// Reads the kernels' error word (set when a bounded wait in a stage kernel
+// gave up); synchronises the stream.
+void check_device_error(ndg_ctx* c) {
+    if (!c->error.ptr) return;
+    unsigned err = 0;
+    check_cuda(cudaMemcpyAsync(&err, c->error.ptr, sizeof(err), cudaMemcpyDeviceToHost, c->stream), "error word readback");
+    check_cuda(cudaStreamSynchronize(c->stream), "error word readback");
+    if (err) {
+        check_cuda(cudaMemsetAsync(c->error.ptr, 0, sizeof(unsigned), c->stream), "memset");
+        fail(NDG_ERR_TIMEOUT, "a stage kernel gave up waiting for its tile copies; the state is not valid");
+    }
+}
+
 dev::StageArgs stage_args(ndg_ctx* c, int m, int in) {
     dev::StageArgs a{};
     a.q = c->q.ptr;
@@ -135,7 +151,9 @@ dev::StageArgs stage_args(ndg_ctx* c, int m, int in) {
     a.rk_g = kRkG[m];
     a.first = m == 0;
     a.n_elements = c->K;
+    a.field_stride = c->Kp;
     a.n_instances = c->n_instances;
+    a.error = c->error.ptr;
     return a;
 }
 
@@ -148,7 +166,7 @@ void launch_stage(ndg_ctx* c, int m) {
 
 void ensure_traces(ndg_ctx* c) {
     if (c->traces_valid) return;
-    dev::TraceArgs a{c->q.ptr, c->tr[c->cur].ptr, c->K, c->n_instances};
+    dev::TraceArgs a{c->q.ptr, c->tr[c->cur].ptr, c->K, c->Kp, c->n_instances};
     check_cuda(dev::launch_traces(c->N, strict(c), a, c->stream), "trace kernel launch");
     ++c->launches;
     c->traces_valid = true;
@@ -195,12 +213,12 @@ void run_steps(ndg_ctx* c, int64_t n_steps) {
 }
 
 double* field_ptr(ndg_ctx* c, int32_t field, int instance) {
-    const int64_t per_inst = 3 * c->field_size;
-    if (field >= NDG_FIELD_P && field <= NDG_FIELD_V) return c->q.ptr + instance * per_inst + field * c->field_size;
-    if (field >= NDG_FIELD_K_P && field <= NDG_FIELD_K_V) return c->k.ptr + instance * per_inst + (field - NDG_FIELD_K_P) * c->field_size;
+    const int64_t per_inst = 3 * c->block;
+    if (field >= NDG_FIELD_P && field <= NDG_FIELD_V) return c->q.ptr + instance * per_inst + field * c->block;
+    if (field >= NDG_FIELD_K_P && field <= NDG_FIELD_K_V) return c->k.ptr + instance * per_inst + (field - NDG_FIELD_K_P) * c->block;
     if (field >= NDG_FIELD_G_P && field <= NDG_FIELD_G_V) {
         if (!c->keep_derivative) fail(NDG_ERR_INVALID_ARG, "time derivative fields need ndg_ctx_keep_derivative(ctx, 1) before stepping");
-        return c->G.ptr + instance * per_inst + (field - NDG_FIELD_G_P) * c->field_size;
+        return c->G.ptr + instance * per_inst + (field - NDG_FIELD_G_P) * c->block;
     }
     fail(NDG_ERR_INVALID_ARG, "unknown field");
 }
@@ -221,6 +239,8 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     c->N = p.initial_N;
     c->K = c->topo.n_domain;
     c->field_size = c->K * (c->N + 1) * (c->N + 1);
+    c->Kp = c->K + (c->K & 1);
+    c->block = c->Kp * (c->N + 1) * (c->N + 1);
     c->has_mesh = true;
     c->traces_valid = false;
     c->cur = 0;
@@ -229,7 +249,7 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
 
     if (c->N > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "orders above 16 have no compiled kernel");
     const SidePlan plan = build_side_plan(c->topo, c->tables);
-    const size_t per_field = static_cast<size_t>(c->field_size);
+    const size_t per_field = static_cast<size_t>(c->block);
     const size_t n = static_cast<size_t>(c->N + 1);
     const size_t K = static_cast<size_t>(c->K);
     const size_t inst = static_cast<size_t>(n_instances);
@@ -237,8 +257,10 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     c->k.allocate(inst * 3 * per_field);
     c->G.release();
     if (c->keep_derivative) c->G.allocate(inst * 3 * per_field);
-    c->tr[0].allocate(inst * 3 * K * 4 * n);
-    c->tr[1].allocate(inst * 3 * K * 4 * n);
+    const size_t Kp = static_cast<size_t>(c->Kp);
+    c->tr[0].allocate(inst * 3 * Kp * 4 * n);
+    c->tr[1].allocate(inst * 3 * Kp * 4 * n);
+    c->error.allocate(1);
     c->corners.allocate(plan.corners.size());
     c->normal.allocate(plan.normal.size());
     c->gscale.allocate(plan.gscale.size());
@@ -260,6 +282,9 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     up(c->elem_N.ptr, eN.data(), K * sizeof(int32_t));
     check_cuda(cudaMemsetAsync(c->q.ptr, 0, c->q.count * sizeof(double), c->stream), "memset");
     check_cuda(cudaMemsetAsync(c->k.ptr, 0, c->k.count * sizeof(double), c->stream), "memset");
+    check_cuda(cudaMemsetAsync(c->tr[0].ptr, 0, c->tr[0].count * sizeof(double), c->stream), "memset");
+    check_cuda(cudaMemsetAsync(c->tr[1].ptr, 0, c->tr[1].count * sizeof(double), c->stream), "memset");
+    check_cuda(cudaMemsetAsync(c->error.ptr, 0, sizeof(unsigned), c->stream), "memset");
     check_cuda(dev::prepare_kernels(c->N, false), "kernel attributes");
     check_cuda(dev::prepare_kernels(c->N, true), "kernel attributes");
     // CFL step of the fixed mesh, reduced on the device (Solver2D_t.cu:17-31).
@@ -359,7 +384,7 @@ ndg_status ndg_ctx_keep_derivative(ndg_ctx* ctx, int32_t enable) {
         drop_graphs(ctx);
         if (ctx->has_mesh && ctx->device >= 0) {
             if (ctx->keep_derivative) {
-                ctx->G.allocate(static_cast<size_t>(3 * ctx->field_size * ctx->n_instances));
+                ctx->G.allocate(static_cast<size_t>(3 * ctx->block * ctx->n_instances));
                 check_cuda(cudaMemsetAsync(ctx->G.ptr, 0, ctx->G.count * sizeof(double), ctx->stream), "memset");
             } else {
                 ctx->G.release();
@@ -374,6 +399,7 @@ ndg_status ndg_ctx_synchronize(ndg_ctx* ctx) {
         if (ctx->device >= 0) {
             make_current(ctx);
             check_cuda(cudaStreamSynchronize(ctx->stream), "synchronize");
+            check_device_error(ctx);
         }
     });
 }
@@ -516,7 +542,7 @@ ndg_status ndg_initial_conditions(ndg_ctx* ctx) {
         require_mesh(ctx);
         require_device(ctx);
         make_current(ctx);
-        check_cuda(dev::launch_initial_conditions(ctx->q.ptr, ctx->k.ptr, ctx->corners.ptr, ctx->N, ctx->K, ctx->n_instances, ctx->stream), "initial condition kernel");
+        check_cuda(dev::launch_initial_conditions(ctx->q.ptr, ctx->k.ptr, ctx->corners.ptr, ctx->N, ctx->K, ctx->Kp, ctx->n_instances, ctx->stream), "initial condition kernel");
         ++ctx->launches;
         if (ctx->keep_derivative) check_cuda(cudaMemsetAsync(ctx->G.ptr, 0, ctx->G.count * sizeof(double), ctx->stream), "memset");
         ctx->traces_valid = false;
@@ -558,6 +584,7 @@ ndg_status ndg_get_field(ndg_ctx* ctx, int32_t instance, int32_t field, double* 
                        "field download");
         }
         check_cuda(cudaStreamSynchronize(ctx->stream), "field download");
+        check_device_error(ctx);
     });
 }
 
@@ -637,6 +664,7 @@ ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* a
             check_cuda(cudaEventRecord(ev[static_cast<size_t>(2 * i + 1)], ctx->stream), "cudaEventRecord");
         }
         check_cuda(cudaStreamSynchronize(ctx->stream), "stage timing");
+        check_device_error(ctx);
         double total = 0.0;
         for (int i = 0; i < n_launches; ++i) {
             float ms = 0.0f;

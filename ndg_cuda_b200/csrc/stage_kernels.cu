@@ -5,34 +5,47 @@
 // boundary_conditions, project_to_faces, calculate_wave_fluxes,
 // project_to_elements, compute_dg_wave_derivative, rk3_step;
 // include/solvers/Solver2D_t.tcu:46-70) become the phases of one CTA that
-// holds a tile of EPB elements in shared memory:
+// owns a tile of EPB consecutive elements:
 //
-//   P1  stream q = (p, u, v) of the tile into shared memory (coalesced);
-//       build the per-element metric vectors from the four corners
-//   P2  per element side node: own trace (l(+-1) . q line), the far-side
-//       trace (neighbour's stored trace or a boundary rule), upwind flux,
-//       times the side's edge metric -> element side flux
-//   P3  xi lines:  Dhat . (y_eta F - x_eta G) + lift           -> G
-//   P4  eta lines: Dhat . (-y_xi F + x_xi G) + lift, then /J   -> G
-//   P5  k = a k + G, q += g dt k (FP64), streamed back to HBM
-//   P6  side traces of the new q -> trace buffer for the next stage
+//   prologue  one thread starts TMA bulk copies (cp.async.bulk) of the tile's
+//             q = (p, u, v) and RK register k into shared memory, each group
+//             signalling its own mbarrier; meanwhile every thread prefetches
+//             the far-side traces of its side nodes (neighbour traces of the
+//             previous stage) and builds metric vectors and 1/J from the
+//             four corners
+//   P2a       own side traces l(+-1) . q-line          (after q has landed)
+//   P2b       upwind flux of every side node, times the edge metric
+//   P3        xi lines:  Dhat . (y_eta F - x_eta G) + lift      -> G
+//   P4        eta lines: Dhat . (-y_xi F + x_xi G) + lift, /J, then the RK
+//             update k = a k + G, q += g dt k in place (after k has landed);
+//             bottom and top traces of the new q straight from registers
+//   epilogue  one thread starts TMA bulk stores of q and k; the right and
+//             left traces of the new q go to the trace buffer
 //
-// HBM traffic per element and stage: q and k read and written (the
-// algorithmic 32 B per degree of freedom) plus one trace write and one
-// neighbour-trace read of 4(N+1) values per field. Geometry is 8 corner
-// coordinates per element; metrics, Jacobians and edge metrics are
-// recomputed in registers, because on straight-sided quads x_xi, y_xi depend
-// only on eta and x_eta, y_eta only on xi (quad_metrics,
+// Work is spread as one thread per (field, element, line), 3 EPB (N+1)
+// threads per CTA. HBM traffic per element and stage: q and k read and
+// written (the algorithmic 32 B per degree of freedom), one trace write and
+// one neighbour-trace read of 4(N+1) values per field, and 8 corner
+// coordinates. Metrics are recomputed: on straight-sided quads x_xi, y_xi
+// depend only on eta and x_eta, y_eta only on xi (quad_metrics,
 // include/functions/quad_metrics.tpp:2-7).
+//
+// Field blocks hold an even number of elements (one unused element when K is
+// odd) and tiles start on even elements, so every tile copy starts on a
+// 16-byte boundary and moves a multiple of 16 bytes, as cp.async.bulk needs.
 //
 // STRICT instantiations round every operation in the reference's order
 // (__dmul_rn/__dadd_rn, true divisions) and reproduce its CPU results bit
 // for bit; the default instantiations contract to FMAs and multiply by
-// reciprocal weights.
+// reciprocals.
 #include "ndg_internal.hpp"
 #include "stage_kernels.cuh"
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
 
 namespace ndg {
 namespace dev {
@@ -59,19 +72,81 @@ template <bool S> __device__ __forceinline__ double sub(double a, double b) { re
 // s + a*b: two roundings in strict mode, one FMA otherwise.
 template <bool S> __device__ __forceinline__ double madd(double s, double a, double b) { return S ? __dadd_rn(s, __dmul_rn(a, b)) : fma(a, b, s); }
 
+// ---------------------------------------------------------------------------
+// TMA bulk copies and mbarriers (PTX ISA: cp.async.bulk, mbarrier).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase 0 of an mbarrier, giving up after `limit_ns`: the error
+// word is then set and false returned so that the CTA stops.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned* error, uint64_t limit_ns) {
+    const uint32_t a = smem_addr(bar);
+    uint32_t done = 0;
+    const uint64_t t0 = global_ns();
+    while (true) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a)
+            : "memory");
+        if (done) return true;
+        if (global_ns() - t0 > limit_ns) {
+            atomicOr(error, 1u);
+            return false;
+        }
+    }
+}
+
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+
+// ---------------------------------------------------------------------------
 template <int N>
 struct Tile {
     static constexpr int n = N + 1;
     static constexpr int NN = n * n;
-    static constexpr int kThreads = 256;
-    static constexpr int EPB = (kThreads / (3 * n)) > 0 ? (kThreads / (3 * n)) : 1;
-    // shared memory layout, in doubles
-    static constexpr int kQ = 0;                        // [3][EPB][NN]
-    static constexpr int kG = kQ + 3 * EPB * NN;        // [3][EPB][NN]
-    static constexpr int kF = kG + 3 * EPB * NN;        // [3][EPB][4][n] element side fluxes
-    static constexpr int kM = kF + 3 * EPB * 4 * n;     // [EPB][4][n] x_xi(eta), y_xi(eta), x_eta(xi), y_eta(xi)
-    static constexpr int kS = kM + EPB * 4 * n;         // [EPB][4] edge metric per side
-    static constexpr int kDoubles = kS + EPB * 4;
+    // Elements per CTA: even (aligned tile copies), at most ~60 KB of shared
+    // memory so that several CTAs share an SM, at most 256 threads.
+    static constexpr int per_element_doubles = 3 * NN * 3 + 3 * 4 * n * 3 + 4 * n + NN + 4;
+    static constexpr int by_smem = (60 * 1024 / 8) / per_element_doubles;
+    static constexpr int by_threads = 256 / (3 * n);
+    static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
+    static constexpr int EPB = raw >= 2 ? (raw & ~1) : 2;
+    static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
+    // shared memory layout (doubles); the tile buffers first, 16-byte aligned
+    static constexpr int kQ = 0;                         // [3][EPB][NN]
+    static constexpr int kK = kQ + 3 * EPB * NN;         // [3][EPB][NN]
+    static constexpr int kG = kK + 3 * EPB * NN;         // [3][EPB][NN]
+    static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n] own side traces
+    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far side traces
+    static constexpr int kF = kFar + 3 * EPB * 4 * n;    // [3][EPB][4][n] element side fluxes
+    static constexpr int kM = kF + 3 * EPB * 4 * n;      // [EPB][4][n] x_xi, y_xi (of eta), x_eta, y_eta (of xi)
+    static constexpr int kJ = kM + EPB * 4 * n;          // [EPB][NN] 1/J (J in strict mode)
+    static constexpr int kS = kJ + EPB * NN;             // [EPB][4] edge metric per side
+    static constexpr int kBar = kS + EPB * 4;            // two mbarriers (8 bytes each)
+    static constexpr int kDoubles = kBar + 2;
     static constexpr size_t kBytes = sizeof(double) * kDoubles;
 };
 
@@ -81,23 +156,13 @@ struct Tile {
 template <int N, bool S>
 __device__ __forceinline__ double side_trace(const double* __restrict__ q, int s, int m) {
     constexpr int n = N + 1;
-    const double* lm = c_lagrange_left + vec_offset(N);
-    const double* lp = c_lagrange_right + vec_offset(N);
+    const double* l = (s == 0 || s == 3) ? c_lagrange_left + vec_offset(N) : c_lagrange_right + vec_offset(N);
     const int line = (s < 2) ? m : N - m;
+    const int base = (s == 0 || s == 2) ? line * n : line;
+    const int stride = (s == 0 || s == 2) ? 1 : n;
     double acc = 0.0;
-    if (s == 0) {
 #pragma unroll
-        for (int j = 0; j < n; ++j) acc = madd<S>(acc, lm[j], q[line * n + j]);
-    } else if (s == 2) {
-#pragma unroll
-        for (int j = 0; j < n; ++j) acc = madd<S>(acc, lp[j], q[line * n + j]);
-    } else if (s == 1) {
-#pragma unroll
-        for (int j = 0; j < n; ++j) acc = madd<S>(acc, lp[j], q[j * n + line]);
-    } else {
-#pragma unroll
-        for (int j = 0; j < n; ++j) acc = madd<S>(acc, lm[j], q[j * n + line]);
-    }
+    for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], q[base + j * stride]);
     return acc;
 }
 
@@ -111,131 +176,190 @@ __device__ __forceinline__ void plane_wave(double x, double y, double t, double&
     v = __dmul_rn(p, ky);
 }
 
+// Bilinear metric term ((1 - t) a + (1 + t) b) / 4 of quad_metrics.
+template <bool S>
+__device__ __forceinline__ double metric(double t, double a, double b) {
+    return mul<S>(add<S>(mul<S>(sub<S>(1.0, t), a), mul<S>(add<S>(1.0, t), b)), 0.25);
+}
+
 template <int N, bool S>
-__global__ void __launch_bounds__(256) stage_kernel(StageArgs a) {
+__global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
     using T = Tile<N>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(128) double smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + T::kBar);
     double* qs = smem + T::kQ;
+    double* ks = smem + T::kK;
     double* gs = smem + T::kG;
+    double* own_s = smem + T::kOwn;
+    double* far_s = smem + T::kFar;
     double* fs = smem + T::kF;
     double* ms = smem + T::kM;
+    double* js = smem + T::kJ;
     double* ss = smem + T::kS;
 
     const int tid = threadIdx.x;
     const int64_t K = a.n_elements;
+    const int64_t Kp = a.field_stride;  // elements per field block (K rounded up to even)
     const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
     const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
+    const int ne_copy = (ne + 1) & ~1;  // tile copies move an even number of elements
     const int64_t inst = blockIdx.y;
-    double* q = a.q + inst * 3 * K * NN;
-    double* k = a.k + inst * 3 * K * NN;
-    const double* tr_in = a.trace_in + inst * 3 * K * 4 * n;
-    double* tr_out = a.trace_out + inst * 3 * K * 4 * n;
+    double* q = a.q + inst * 3 * Kp * NN;
+    double* k = a.k + inst * 3 * Kp * NN;
+    const double* tr_in = a.trace_in + inst * 3 * Kp * 4 * n;
+    double* tr_out = a.trace_out + inst * 3 * Kp * 4 * n;
     const double* xn = c_nodes + vec_offset(N);
     const double time = a.step[0];
     const double dt = a.step[1];
 
-    // P1: q tile and metric vectors.
-    const int tile_vals = ne * NN;
-    for (int idx = tid; idx < 3 * tile_vals; idx += T::kThreads) {
-        const int f = idx / tile_vals;
-        const int r = idx - f * tile_vals;
-        qs[f * EPB * NN + r] = q[(f * K + e0) * NN + r];
-    }
-    for (int idx = tid; idx < ne * n; idx += T::kThreads) {
-        const int e = idx / n, i = idx - e * n;
-        const double* c = a.corners + 8 * (e0 + e);
-        const double x0 = c[0], y0 = c[1], x1 = c[2], y1 = c[3], x2 = c[4], y2 = c[5], x3 = c[6], y3 = c[7];
-        const double t = xn[i];
-        const double lo = sub<S>(1.0, t), hi = add<S>(1.0, t);
-        double* m = ms + e * 4 * n;
-        m[0 * n + i] = mul<S>(add<S>(mul<S>(lo, sub<S>(x1, x0)), mul<S>(hi, sub<S>(x2, x3))), 0.25);  // x_xi at eta = t
-        m[1 * n + i] = mul<S>(add<S>(mul<S>(lo, sub<S>(y1, y0)), mul<S>(hi, sub<S>(y2, y3))), 0.25);  // y_xi at eta = t
-        m[2 * n + i] = mul<S>(add<S>(mul<S>(lo, sub<S>(x3, x0)), mul<S>(hi, sub<S>(x2, x1))), 0.25);  // x_eta at xi = t
-        m[3 * n + i] = mul<S>(add<S>(mul<S>(lo, sub<S>(y3, y0)), mul<S>(hi, sub<S>(y2, y1))), 0.25);  // y_eta at xi = t
-    }
-    for (int idx = tid; idx < ne * 4; idx += T::kThreads) {
-        // Edge metric of side s, constant along a straight side
-        // (Element2D_t.cpp:756-769): |d(x,y)/dxi| at eta = -1, +1 for sides
-        // 0, 2 and |d(x,y)/deta| at xi = +1, -1 for sides 1, 3.
-        const int e = idx >> 2, sd = idx & 3;
-        const double* c = a.corners + 8 * (e0 + e);
-        const double x0 = c[0], y0 = c[1], x1 = c[2], y1 = c[3], x2 = c[4], y2 = c[5], x3 = c[6], y3 = c[7];
-        const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
-        const double l2 = sub<S>(1.0, at), h2 = add<S>(1.0, at);
-        double dx, dy;
-        if (sd == 0 || sd == 2) {
-            dx = mul<S>(add<S>(mul<S>(l2, sub<S>(x1, x0)), mul<S>(h2, sub<S>(x2, x3))), 0.25);
-            dy = mul<S>(add<S>(mul<S>(l2, sub<S>(y1, y0)), mul<S>(h2, sub<S>(y2, y3))), 0.25);
-        } else {
-            dx = mul<S>(add<S>(mul<S>(l2, sub<S>(x3, x0)), mul<S>(h2, sub<S>(x2, x1))), 0.25);
-            dy = mul<S>(add<S>(mul<S>(l2, sub<S>(y3, y0)), mul<S>(h2, sub<S>(y2, y1))), 0.25);
+    // Thread -> (field f, element e of the tile, line or node index m).
+    const int f = tid / (EPB * n);
+    const int r = tid - f * (EPB * n);
+    const int e = r / n;
+    const int m = r - e * n;
+    const bool active = f < 3 && e < ne;
+    const int64_t ge = e0 + e;
+
+    // Prologue: bulk copies of q and k.
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+        const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
+        mbar_expect_tx(&bars[0], 3 * bytes);
+        for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, &bars[0]);
+        if (!a.first) {
+            mbar_expect_tx(&bars[1], 3 * bytes);
+            for (int ff = 0; ff < 3; ++ff) bulk_load(ks + ff * EPB * NN, k + (ff * Kp + e0) * NN, bytes, &bars[1]);
         }
-        ss[idx] = sqrt(add<S>(mul<S>(dx, dx), mul<S>(dy, dy)));
+    }
+
+    // Prefetch of the far-side traces of this thread's side nodes: interior
+    // and periodic sides read the neighbour's trace of the previous stage.
+    double far_pref[4] = {0.0, 0.0, 0.0, 0.0};
+    if (active) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int2 lk = a.link[4 * ge + s];
+            if (((lk.y >> 2) & 7) == kInterior) far_pref[s] = tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)];
+        }
+        // Metric vectors, edge metrics and 1/J of the element, from its corners.
+        const double* c = a.corners + 8 * ge;
+        const double x0 = c[0], y0 = c[1], x1 = c[2], y1 = c[3], x2 = c[4], y2 = c[5], x3 = c[6], y3 = c[7];
+        double* mv = ms + e * 4 * n;
+        const double t = xn[m];
+        const double x_eta = metric<S>(t, sub<S>(x3, x0), sub<S>(x2, x1));  // at xi = t
+        const double y_eta = metric<S>(t, sub<S>(y3, y0), sub<S>(y2, y1));
+        if (f == 0) {
+            mv[0 * n + m] = metric<S>(t, sub<S>(x1, x0), sub<S>(x2, x3));  // x_xi at eta = t
+            mv[1 * n + m] = metric<S>(t, sub<S>(y1, y0), sub<S>(y2, y3));  // y_xi at eta = t
+        } else if (f == 1) {
+            mv[2 * n + m] = x_eta;
+            mv[3 * n + m] = y_eta;
+        } else {
+            // Edge metric of side sd, constant along a straight side
+            // (Element2D_t.cpp:756-769): |d(x,y)/dxi| at eta = -1, +1 for
+            // sides 0, 2 and |d(x,y)/deta| at xi = +1, -1 for sides 1, 3.
+            for (int sd = m; sd < 4; sd += n) {
+                const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
+                double dx, dy;
+                if (sd == 0 || sd == 2) {
+                    dx = metric<S>(at, sub<S>(x1, x0), sub<S>(x2, x3));
+                    dy = metric<S>(at, sub<S>(y1, y0), sub<S>(y2, y3));
+                } else {
+                    dx = metric<S>(at, sub<S>(x3, x0), sub<S>(x2, x1));
+                    dy = metric<S>(at, sub<S>(y3, y0), sub<S>(y2, y1));
+                }
+                ss[e * 4 + sd] = sqrt(add<S>(mul<S>(dx, dx), mul<S>(dy, dy)));
+            }
+        }
+        // J at nodes (m, j), j = f, f + 3, ...: x_xi(eta_j) y_eta(xi_m) - x_eta(xi_m) y_xi(eta_j).
+        for (int j = f; j < n; j += 3) {
+            const double tj = xn[j];
+            const double x_xi = metric<S>(tj, sub<S>(x1, x0), sub<S>(x2, x3));
+            const double y_xi = metric<S>(tj, sub<S>(y1, y0), sub<S>(y2, y3));
+            const double jac = sub<S>(mul<S>(x_xi, y_eta), mul<S>(x_eta, y_xi));
+            js[e * NN + m * n + j] = S ? jac : __drcp_rn(jac);
+        }
+    }
+    __syncthreads();  // mbarrier init, metrics, J
+
+    if (!mbar_wait(&bars[0], a.error, kWaitLimitNs)) return;
+
+    // P2a: own side traces of this thread's field at node m of each side,
+    // and the prefetched far traces.
+    if (active) {
+        const double* qf = qs + (f * EPB + e) * NN;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            own_s[((f * EPB + e) * 4 + s) * n + m] = side_trace<N, S>(qf, s, m);
+            far_s[((f * EPB + e) * 4 + s) * n + m] = far_pref[s];
+        }
     }
     __syncthreads();
 
-    // P2: element side fluxes.
+    // P2b: far traces of boundary sides, upwind flux (Solver2D_t.cpp:48-63)
+    // in the face's own left/right order, then the element's view of it
+    // (Mesh2D_t.cpp:3895-3929): times the edge metric, negated for the
+    // face's right element.
     for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
-        const int e = idx / (4 * n);
+        const int ee = idx / (4 * n);
         const int s = (idx / n) & 3;
-        const int m = idx - (idx / n) * n;
-        const int64_t ge = e0 + e;
-        double own[3], far[3];
-#pragma unroll
-        for (int f = 0; f < 3; ++f) own[f] = side_trace<N, S>(qs + (f * EPB + e) * NN, s, m);
-        const int2 link = a.link[4 * ge + s];
-        const double2 nrm = a.normal[4 * ge + s];
-        const int kind = (link.y >> 2) & 7;
-        const int role = (link.y >> 5) & 1;
+        const int mm = idx - (idx / n) * n;
+        const int64_t g = e0 + ee;
+        const int2 lk = a.link[4 * g + s];
+        const double2 nrm = a.normal[4 * g + s];
+        const int kind = (lk.y >> 2) & 7;
+        const int role = (lk.y >> 5) & 1;
+        const int o = (ee * 4 + s) * n + mm;
+        constexpr int fstride = EPB * 4 * n;
+        const double op = own_s[o], ou = own_s[fstride + o], ov = own_s[2 * fstride + o];
+        double fp_, fu_, fv_;
         if (kind == kInterior) {
-            const int nb_side = link.y & 3;
-#pragma unroll
-            for (int f = 0; f < 3; ++f) far[f] = tr_in[((f * K + link.x) * 4 + nb_side) * n + (N - m)];
+            fp_ = far_s[o];
+            fu_ = far_s[fstride + o];
+            fv_ = far_s[2 * fstride + o];
         } else if (kind == kMirror || kind == kCopy) {
-            // Ghost trace: the element's own trace reversed and scaled by the
-            // ghost's edge metric; walls and symmetry planes then mirror the
-            // normal velocity (Mesh2D_t.cpp:4366-4434, 4601-4710).
-            const double gsc = a.gscale[4 * ge + s];
-            far[0] = mul<S>(own[0], gsc);
-            const double gu = mul<S>(own[1], gsc), gv = mul<S>(own[2], gsc);
+            // Ghost trace: the own trace reversed and scaled by the ghost's
+            // edge metric; walls and symmetry planes then mirror the normal
+            // velocity (Mesh2D_t.cpp:4366-4434, 4601-4710).
+            const double gsc = a.gscale[4 * g + s];
+            fp_ = mul<S>(op, gsc);
+            const double gu = mul<S>(ou, gsc), gv = mul<S>(ov, gsc);
             if (kind == kMirror) {
                 const double tx = -nrm.y, ty = nrm.x;
                 const double l0 = -add<S>(mul<S>(gu, nrm.x), mul<S>(gv, nrm.y));
                 const double l1 = add<S>(mul<S>(gu, tx), mul<S>(gv, ty));
-                far[1] = add<S>(mul<S>(nrm.x, l0), mul<S>(tx, l1));
-                far[2] = add<S>(mul<S>(nrm.y, l0), mul<S>(ty, l1));
+                fu_ = add<S>(mul<S>(nrm.x, l0), mul<S>(tx, l1));
+                fv_ = add<S>(mul<S>(nrm.y, l0), mul<S>(ty, l1));
             } else {
-                far[1] = gu;
-                far[2] = gv;
+                fu_ = gu;
+                fv_ = gv;
             }
         } else if (kind == kAnalytic) {
             // Inflow: the analytic wave on the ghost edge at the stage time
             // (Mesh2D_t.cpp:4575-4599); the face reads ghost node N - m.
-            const double4 g = a.inflow[4 * ge + s];
-            const double r = mul<S>(add<S>(xn[N - m], 1.0), 0.5);
-            const double gx = add<S>(mul<S>(g.z, r), mul<S>(g.x, sub<S>(1.0, r)));
-            const double gy = add<S>(mul<S>(g.w, r), mul<S>(g.y, sub<S>(1.0, r)));
-            plane_wave(gx, gy, add<S>(time, mul<S>(a.rk_b, dt)), far[0], far[1], far[2]);
+            const double4 gq = a.inflow[4 * g + s];
+            const double rr = mul<S>(add<S>(xn[N - mm], 1.0), 0.5);
+            const double gx = add<S>(mul<S>(gq.z, rr), mul<S>(gq.x, sub<S>(1.0, rr)));
+            const double gy = add<S>(mul<S>(gq.w, rr), mul<S>(gq.y, sub<S>(1.0, rr)));
+            plane_wave(gx, gy, add<S>(time, mul<S>(a.rk_b, dt)), fp_, fu_, fv_);
         } else {
-            far[0] = far[1] = far[2] = 0.0;
+            fp_ = fu_ = fv_ = 0.0;
         }
-        // Upwind flux of the face (Solver2D_t.cpp:48-63) with the face's own
-        // left/right order, then the element's view of it
-        // (Mesh2D_t.cpp:3895-3929): scaled by the edge metric, and negated
-        // for the face's right element.
-        const double Lp = role ? far[0] : own[0], Lu = role ? far[1] : own[1], Lv = role ? far[2] : own[2];
-        const double Rp = role ? own[0] : far[0], Ru = role ? own[1] : far[1], Rv = role ? own[2] : far[2];
+        const double Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
+        const double Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
         const double wL = add<S>(Lp, add<S>(mul<S>(Lu, nrm.x), mul<S>(Lv, nrm.y)));
         const double wR = sub<S>(Rp, add<S>(mul<S>(Ru, nrm.x), mul<S>(Rv, nrm.y)));
-        const double fp = mul<S>(sub<S>(wL, wR), 0.5);
+        const double flp = mul<S>(sub<S>(wL, wR), 0.5);
         const double sum = add<S>(wL, wR);
-        const double fu = mul<S>(mul<S>(nrm.x, sum), 0.5);
-        const double fv = mul<S>(mul<S>(nrm.y, sum), 0.5);
-        const double sf = ss[e * 4 + s];
-        fs[((0 * EPB + e) * 4 + s) * n + m] = mul<S>(role ? -fp : fp, sf);
-        fs[((1 * EPB + e) * 4 + s) * n + m] = mul<S>(role ? -fu : fu, sf);
-        fs[((2 * EPB + e) * 4 + s) * n + m] = mul<S>(role ? -fv : fv, sf);
+        const double flu = mul<S>(mul<S>(nrm.x, sum), 0.5);
+        const double flv = mul<S>(mul<S>(nrm.y, sum), 0.5);
+        const double sf = ss[ee * 4 + s];
+        fs[o] = mul<S>(role ? -flp : flp, sf);
+        fs[fstride + o] = mul<S>(role ? -flu : flu, sf);
+        fs[2 * fstride + o] = mul<S>(role ? -flv : flv, sf);
     }
     __syncthreads();
 
@@ -245,19 +369,17 @@ __global__ void __launch_bounds__(256) stage_kernel(StageArgs a) {
     const double* w = c_weights + vec_offset(N);
     const double* iw = c_inv_weights + vec_offset(N);
 
-    // P3: xi lines (fixed eta index j), Solver2D_t.cpp:71-101.
-    for (int idx = tid; idx < 3 * ne * n; idx += T::kThreads) {
-        const int f = idx / (ne * n);
-        const int r = idx - f * ne * n;
-        const int e = r / n, j = r - (r / n) * n;
+    // P3: xi lines (eta index j = m), Solver2D_t.cpp:71-101.
+    if (active) {
+        const int j = m;
         const double* P = qs + (0 * EPB + e) * NN;
         const double* U = qs + (1 * EPB + e) * NN;
         const double* V = qs + (2 * EPB + e) * NN;
-        const double* m = ms + e * 4 * n;
+        const double* mv = ms + e * 4 * n;
         double fl[n];
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-            const double x_eta = m[2 * n + i], y_eta = m[3 * n + i];
+            const double x_eta = mv[2 * n + i], y_eta = mv[3 * n + i];
             if (f == 0) fl[i] = sub<S>(mul<S>(y_eta, U[i * n + j]), mul<S>(x_eta, V[i * n + j]));
             else if (f == 1) fl[i] = mul<S>(y_eta, P[i * n + j]);
             else fl[i] = -mul<S>(x_eta, P[i * n + j]);
@@ -270,105 +392,101 @@ __global__ void __launch_bounds__(256) stage_kernel(StageArgs a) {
             double acc = 0.0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[i * n + mm], fl[mm]);
-            const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i])
-                                  : (fr * lp[i] + fl3 * lm[i]) * iw[i];
+            const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
             G[i * n + j] = -add<S>(acc, lift);
         }
     }
     __syncthreads();
 
-    // P4: eta lines (fixed xi index i), Solver2D_t.cpp:103-134, then /J.
-    for (int idx = tid; idx < 3 * ne * n; idx += T::kThreads) {
-        const int f = idx / (ne * n);
-        const int r = idx - f * ne * n;
-        const int e = r / n, i = r - (r / n) * n;
+    // P4: eta lines (xi index i = m), Solver2D_t.cpp:103-134, the division
+    // by J, and the low-storage RK3 update (Solver2D_t.cpp:138-172).
+    double line[n];  // contravariant flux of this thread's field along eta, from q before the update
+    if (active) {
+        const int i = m;
         const double* P = qs + (0 * EPB + e) * NN + i * n;
         const double* U = qs + (1 * EPB + e) * NN + i * n;
         const double* V = qs + (2 * EPB + e) * NN + i * n;
-        const double* m = ms + e * 4 * n;
-        double fl[n];
+        const double* mv = ms + e * 4 * n;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            const double x_xi = m[0 * n + j], y_xi = m[1 * n + j];
-            if (f == 0) fl[j] = add<S>(mul<S>(-y_xi, U[j]), mul<S>(x_xi, V[j]));
-            else if (f == 1) fl[j] = mul<S>(-y_xi, P[j]);
-            else fl[j] = mul<S>(x_xi, P[j]);
+            const double x_xi = mv[0 * n + j], y_xi = mv[1 * n + j];
+            if (f == 0) line[j] = add<S>(mul<S>(-y_xi, U[j]), mul<S>(x_xi, V[j]));
+            else if (f == 1) line[j] = mul<S>(-y_xi, P[j]);
+            else line[j] = mul<S>(x_xi, P[j]);
         }
+    }
+    __syncthreads();  // every thread holds its inputs: rows of q may now be overwritten
+    if (!a.first && !mbar_wait(&bars[1], a.error, kWaitLimitNs)) return;
+    if (active) {
+        const int i = m;
         const double ft = fs[((f * EPB + e) * 4 + 2) * n + (N - i)];
         const double fb = fs[((f * EPB + e) * 4 + 0) * n + i];
-        const double x_eta = m[2 * n + i], y_eta = m[3 * n + i];
-        double* G = gs + (f * EPB + e) * NN + i * n;
+        const double* G = gs + (f * EPB + e) * NN + i * n;
+        const double* jrow = js + e * NN + i * n;
+        double* qrow = qs + (f * EPB + e) * NN + i * n;
+        double* krow = ks + (f * EPB + e) * NN + i * n;
+        const double gdt = mul<S>(a.rk_g, dt);
+        double bottom = 0.0, top = 0.0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             double acc = 0.0;
 #pragma unroll
-            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[j * n + mm], fl[mm]);
-            const double lift = S ? __ddiv_rn(add<S>(mul<S>(ft, lp[j]), mul<S>(fb, lm[j])), w[j])
-                                  : (ft * lp[j] + fb * lm[j]) * iw[j];
-            const double jac = sub<S>(mul<S>(m[0 * n + j], y_eta), mul<S>(x_eta, m[1 * n + j]));
+            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[j * n + mm], line[mm]);
+            const double lift = S ? __ddiv_rn(add<S>(mul<S>(ft, lp[j]), mul<S>(fb, lm[j])), w[j]) : (ft * lp[j] + fb * lm[j]) * iw[j];
             const double num = sub<S>(G[j], add<S>(acc, lift));
-            G[j] = S ? __ddiv_rn(num, jac) : num * __drcp_rn(jac);
+            const double Gn = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
+            const double kn = a.first ? Gn : add<S>(mul<S>(a.rk_a, krow[j]), Gn);
+            const double qn = add<S>(qrow[j], mul<S>(gdt, kn));
+            krow[j] = kn;
+            qrow[j] = qn;
+            if (a.G_out) a.G_out[inst * 3 * Kp * NN + (f * Kp + ge) * NN + i * n + j] = Gn;
+            bottom = madd<S>(bottom, lm[j], qn);
+            top = madd<S>(top, lp[j], qn);
         }
+        // Bottom and top traces of the new solution (Element2D_t.cpp:86-125).
+        tr_out[((f * Kp + ge) * 4 + 0) * n + i] = bottom;
+        tr_out[((f * Kp + ge) * 4 + 2) * n + (N - i)] = top;
     }
+    fence_proxy_async();
     __syncthreads();
 
-    // P5: low-storage RK3 update (Solver2D_t.cpp:138-172), FP64.
-    const double gdt = mul<S>(a.rk_g, dt);
-    for (int idx = tid; idx < 3 * tile_vals; idx += T::kThreads) {
-        const int f = idx / tile_vals;
-        const int r = idx - f * tile_vals;
-        const int64_t gi = (f * K + e0) * NN + r;
-        const double G = gs[f * EPB * NN + r];
-        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, k[gi]), G);
-        const double qn = add<S>(qs[f * EPB * NN + r], mul<S>(gdt, kn));
-        k[gi] = kn;
-        q[gi] = qn;
-        qs[f * EPB * NN + r] = qn;
-        if (a.G_out) a.G_out[inst * 3 * K * NN + gi] = G;
+    // Epilogue: bulk stores of the tile, and the right and left traces.
+    if (tid == 0) {
+        const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
+        for (int ff = 0; ff < 3; ++ff) {
+            bulk_store(q + (ff * Kp + e0) * NN, qs + ff * EPB * NN, bytes);
+            bulk_store(k + (ff * Kp + e0) * NN, ks + ff * EPB * NN, bytes);
+        }
+        bulk_commit();
     }
-    __syncthreads();
-
-    // P6: side traces of the new solution for the next stage.
-    for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
-        const int e = idx / (4 * n);
-        const int s = (idx / n) & 3;
-        const int m = idx - (idx / n) * n;
-#pragma unroll
-        for (int f = 0; f < 3; ++f) tr_out[((f * K + e0 + e) * 4 + s) * n + m] = side_trace<N, S>(qs + (f * EPB + e) * NN, s, m);
+    if (active) {
+        const double* qf = qs + (f * EPB + e) * NN;
+        tr_out[((f * Kp + ge) * 4 + 1) * n + m] = side_trace<N, S>(qf, 1, m);
+        tr_out[((f * Kp + ge) * 4 + 3) * n + m] = side_trace<N, S>(qf, 3, m);
     }
+    if (tid == 0) bulk_wait_read();
 }
 
 // Side traces only (start of a run, or after the host changed q).
 template <int N, bool S>
 __global__ void __launch_bounds__(256) trace_kernel(TraceArgs a) {
-    using T = Tile<N>;
-    constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
-    extern __shared__ double smem[];
-    const int64_t K = a.n_elements;
-    const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
-    const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
-    const int64_t inst = blockIdx.y;
-    const double* q = a.q + inst * 3 * K * NN;
-    double* tr_out = a.trace_out + inst * 3 * K * 4 * n;
-    const int tile_vals = ne * NN;
-    for (int idx = threadIdx.x; idx < 3 * tile_vals; idx += T::kThreads) {
-        const int f = idx / tile_vals;
-        const int r = idx - f * tile_vals;
-        smem[f * EPB * NN + r] = q[(f * K + e0) * NN + r];
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < ne * 4 * n; idx += T::kThreads) {
-        const int e = idx / (4 * n);
-        const int s = (idx / n) & 3;
-        const int m = idx - (idx / n) * n;
-#pragma unroll
-        for (int f = 0; f < 3; ++f) tr_out[((f * K + e0 + e) * 4 + s) * n + m] = side_trace<N, S>(smem + (f * EPB + e) * NN, s, m);
+    constexpr int n = N + 1, NN = n * n;
+    const int64_t K = a.n_elements, Kp = a.field_stride;
+    const int64_t total = static_cast<int64_t>(a.n_instances) * 3 * K * 4 * n;
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total; idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int m = static_cast<int>(idx % n);
+        const int s = static_cast<int>((idx / n) % 4);
+        const int64_t e = (idx / (4 * n)) % K;
+        const int64_t fi = idx / (4 * n * K);  // instance * 3 + field
+        const double* qf = a.q + (fi * Kp + e) * NN;
+        a.trace_out[((fi * Kp + e) * 4 + s) * n + m] = side_trace<N, S>(qf, s, m);
     }
 }
 
 // Reference plane-wave initial condition (Mesh2D_t.cpp:1192-1216) on every
-// node of every instance, bilinear map of include/functions/quad_map.tpp:2-7.
-__global__ void initial_condition_kernel(double* q, double* k, const double* corners, int N, int64_t K, int n_instances) {
+// node of every instance, through the bilinear map of
+// include/functions/quad_map.tpp:2-7 in the reference's operation order.
+__global__ void initial_condition_kernel(double* q, double* k, const double* corners, int N, int64_t K, int64_t Kp, int n_instances) {
     const int n = N + 1, NN = n * n;
     const int64_t total = K * NN;
     const double* xn = c_nodes + vec_offset(N);
@@ -378,27 +496,24 @@ __global__ void initial_condition_kernel(double* q, double* k, const double* cor
         const int i = node / n, j = node - (node / n) * n;
         const double* c = corners + 8 * e;
         const double xi = xn[i], eta = xn[j];
-        const double gx = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(c[0], __dsub_rn(1.0, xi)), __dsub_rn(1.0, eta)),
-                                                                  __dmul_rn(__dmul_rn(c[2], __dadd_rn(xi, 1.0)), __dsub_rn(1.0, eta))),
-                                                        __dmul_rn(__dmul_rn(c[4], __dadd_rn(xi, 1.0)), __dadd_rn(eta, 1.0))),
-                                              __dmul_rn(__dmul_rn(c[6], __dsub_rn(1.0, xi)), __dadd_rn(eta, 1.0))),
+        const double a = __dsub_rn(1.0, xi), b = __dadd_rn(xi, 1.0), cc = __dsub_rn(1.0, eta), d = __dadd_rn(eta, 1.0);
+        const double gx = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(c[0], a), cc), __dmul_rn(__dmul_rn(c[2], b), cc)), __dmul_rn(__dmul_rn(c[4], b), d)),
+                                              __dmul_rn(__dmul_rn(c[6], a), d)),
                                     0.25);
-        const double gy = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(c[1], __dsub_rn(1.0, xi)), __dsub_rn(1.0, eta)),
-                                                                  __dmul_rn(__dmul_rn(c[3], __dadd_rn(xi, 1.0)), __dsub_rn(1.0, eta))),
-                                                        __dmul_rn(__dmul_rn(c[5], __dadd_rn(xi, 1.0)), __dadd_rn(eta, 1.0))),
-                                              __dmul_rn(__dmul_rn(c[7], __dsub_rn(1.0, xi)), __dadd_rn(eta, 1.0))),
+        const double gy = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(c[1], a), cc), __dmul_rn(__dmul_rn(c[3], b), cc)), __dmul_rn(__dmul_rn(c[5], b), d)),
+                                              __dmul_rn(__dmul_rn(c[7], a), d)),
                                     0.25);
         double p, u, v;
         plane_wave(gx, gy, 0.0, p, u, v);
         for (int inst = 0; inst < n_instances; ++inst) {
-            double* qi = q + static_cast<int64_t>(inst) * 3 * total;
-            double* ki = k + static_cast<int64_t>(inst) * 3 * total;
+            double* qi = q + static_cast<int64_t>(inst) * 3 * Kp * NN;
+            double* ki = k + static_cast<int64_t>(inst) * 3 * Kp * NN;
             qi[idx] = p;
-            qi[total + idx] = u;
-            qi[2 * total + idx] = v;
+            qi[Kp * NN + idx] = u;
+            qi[2 * Kp * NN + idx] = v;
             ki[idx] = 0.0;
-            ki[total + idx] = 0.0;
-            ki[2 * total + idx] = 0.0;
+            ki[Kp * NN + idx] = 0.0;
+            ki[2 * Kp * NN + idx] = 0.0;
         }
     }
 }
@@ -421,12 +536,9 @@ __global__ void delta_t_kernel(const double* delta_xy_min, const int* elem_N, in
     if (threadIdx.x == 0) *out = red[0];
 }
 
-// Step bookkeeping of the reference's time loop (Solver2D_t.tcu:37-42, 72):
-// step = {time, dt, dt_mesh, t_end}.
-__global__ void begin_step_kernel(double* step) {
-    const double time = step[0], dt_mesh = step[2], t_end = step[3];
-    step[1] = (time + dt_mesh > t_end) ? t_end - time : dt_mesh;
-}
+// Time update of the reference's loop (Solver2D_t.tcu:37-42, 72) with
+// step = {time, dt, dt_mesh, t_end}: advance, then the next step's dt,
+// shortened to land on t_end.
 __global__ void end_step_kernel(double* step) {
     const double time = step[0] + step[1];
     step[0] = time;
@@ -446,27 +558,27 @@ static cudaError_t launch_stage_t(const StageArgs& a, cudaStream_t stream) {
 
 template <int N, bool S>
 static cudaError_t launch_trace_t(const TraceArgs& a, cudaStream_t stream) {
-    using T = Tile<N>;
-    const size_t bytes = sizeof(double) * 3 * T::EPB * T::NN;
-    const dim3 grid(static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
-    trace_kernel<N, S><<<grid, T::kThreads, bytes, stream>>>(a);
+    const int64_t total = static_cast<int64_t>(a.n_instances) * 3 * a.n_elements * 4 * (N + 1);
+    const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 32));
+    trace_kernel<N, S><<<blocks, 256, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
-// Opts the kernels of one order into more than 48 KB of dynamic shared memory
-// on the current device. Called once per device and order, before any launch
-// or stream capture.
+// Opts the stage kernel of one order into more than 48 KB of dynamic shared
+// memory on the current device. Called once per device and order, before
+// any launch or stream capture.
 template <int N, bool S>
 static cudaError_t prepare_t() {
-    using T = Tile<N>;
-    cudaError_t err = cudaFuncSetAttribute(stage_kernel<N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(T::kBytes));
-    if (err != cudaSuccess) return err;
-    return cudaFuncSetAttribute(trace_kernel<N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(sizeof(double) * 3 * T::EPB * T::NN));
+    return cudaFuncSetAttribute(stage_kernel<N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
 }
 
-#define NDG_DISPATCH_ORDER(FN, N_, STRICT_, ...)                  \
-    switch (N_) {                                                 \
+template <int N, bool S>
+static int epb_t() {
+    return Tile<N>::EPB;
+}
+
+#define NDG_DISPATCH_ORDER(FN, N_, STRICT_, ...)                                          \
+    switch (N_) {                                                                         \
         case 1: return STRICT_ ? FN<1, true>(__VA_ARGS__) : FN<1, false>(__VA_ARGS__);    \
         case 2: return STRICT_ ? FN<2, true>(__VA_ARGS__) : FN<2, false>(__VA_ARGS__);    \
         case 3: return STRICT_ ? FN<3, true>(__VA_ARGS__) : FN<3, false>(__VA_ARGS__);    \
@@ -483,40 +595,38 @@ static cudaError_t prepare_t() {
         case 14: return STRICT_ ? FN<14, true>(__VA_ARGS__) : FN<14, false>(__VA_ARGS__); \
         case 15: return STRICT_ ? FN<15, true>(__VA_ARGS__) : FN<15, false>(__VA_ARGS__); \
         case 16: return STRICT_ ? FN<16, true>(__VA_ARGS__) : FN<16, false>(__VA_ARGS__); \
-        default: return cudaErrorInvalidValue;                    \
+        default: break;                                                                   \
     }
 
 cudaError_t prepare_kernels(int N, bool strict) {
     NDG_DISPATCH_ORDER(prepare_t, N, strict)
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_stage(int N, bool strict, const StageArgs& a, cudaStream_t stream) {
     NDG_DISPATCH_ORDER(launch_stage_t, N, strict, a, stream)
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_traces(int N, bool strict, const TraceArgs& a, cudaStream_t stream) {
     NDG_DISPATCH_ORDER(launch_trace_t, N, strict, a, stream)
+    return cudaErrorInvalidValue;
 }
 
 int elements_per_block(int N) {
-    const int n = N + 1;
-    return (256 / (3 * n)) > 0 ? 256 / (3 * n) : 1;
+    NDG_DISPATCH_ORDER(epb_t, N, false)
+    return 0;
 }
 
-cudaError_t launch_initial_conditions(double* q, double* k, const double* corners, int N, int64_t K, int n_instances, cudaStream_t stream) {
+cudaError_t launch_initial_conditions(double* q, double* k, const double* corners, int N, int64_t K, int64_t Kp, int n_instances, cudaStream_t stream) {
     const int64_t total = K * (N + 1) * (N + 1);
     const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 16));
-    initial_condition_kernel<<<blocks, 256, 0, stream>>>(q, k, corners, N, K, n_instances);
+    initial_condition_kernel<<<blocks, 256, 0, stream>>>(q, k, corners, N, K, Kp, n_instances);
     return cudaGetLastError();
 }
 
 cudaError_t launch_delta_t(const double* delta_xy_min, const int* elem_N, int64_t K, double cfl, double* out, cudaStream_t stream) {
     delta_t_kernel<<<1, 1024, 0, stream>>>(delta_xy_min, elem_N, K, cfl, out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_begin_step(double* step, cudaStream_t stream) {
-    begin_step_kernel<<<1, 1, 0, stream>>>(step);
     return cudaGetLastError();
 }
 
@@ -532,11 +642,12 @@ cudaError_t upload_tables(const Tables& t) {
     for (int N = 0; N <= std::min(t.N_max, kMaxOrder); ++N) {
         const int n = N + 1;
         for (int i = 0; i < n; ++i) {
-            nodes[static_cast<size_t>(vec_offset(N) + i)] = t.get(NDG_TABLE_NODES, N)[static_cast<size_t>(i)];
-            weights[static_cast<size_t>(vec_offset(N) + i)] = t.get(NDG_TABLE_WEIGHTS, N)[static_cast<size_t>(i)];
-            inv_w[static_cast<size_t>(vec_offset(N) + i)] = 1.0 / t.get(NDG_TABLE_WEIGHTS, N)[static_cast<size_t>(i)];
-            ll[static_cast<size_t>(vec_offset(N) + i)] = t.get(NDG_TABLE_LAGRANGE_LEFT, N)[static_cast<size_t>(i)];
-            lr[static_cast<size_t>(vec_offset(N) + i)] = t.get(NDG_TABLE_LAGRANGE_RIGHT, N)[static_cast<size_t>(i)];
+            const size_t at = static_cast<size_t>(vec_offset(N) + i);
+            nodes[at] = t.get(NDG_TABLE_NODES, N)[static_cast<size_t>(i)];
+            weights[at] = t.get(NDG_TABLE_WEIGHTS, N)[static_cast<size_t>(i)];
+            inv_w[at] = 1.0 / t.get(NDG_TABLE_WEIGHTS, N)[static_cast<size_t>(i)];
+            ll[at] = t.get(NDG_TABLE_LAGRANGE_LEFT, N)[static_cast<size_t>(i)];
+            lr[at] = t.get(NDG_TABLE_LAGRANGE_RIGHT, N)[static_cast<size_t>(i)];
         }
         for (int i = 0; i < n * n; ++i) dhat[static_cast<size_t>(mat_offset(N) + i)] = t.get(NDG_TABLE_DERIVATIVE_MATRICES_HAT, N)[static_cast<size_t>(i)];
     }

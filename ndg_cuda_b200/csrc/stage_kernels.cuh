@@ -9,9 +9,10 @@ namespace ndg {
 namespace dev {
 
 // Arguments of one RK3 stage over all elements and instances.
-// Layouts (FP64): q, k, G_out: [instance][field p,u,v][element][(N+1)^2];
-// traces: [instance][field][element][side][N+1]; per element side: link,
-// normal, gscale, inflow ([element][side]); corners: [element][8].
+// Layouts (FP64): q, k, G_out: [instance][field p,u,v][field_stride][(N+1)^2];
+// traces: [instance][field][field_stride][side][N+1], where field_stride is
+// the element count rounded up to even; per element side: link, normal,
+// gscale, inflow ([element][side]); corners: [element][8].
 struct StageArgs {
     double* q;
     double* k;
@@ -24,9 +25,11 @@ struct StageArgs {
     const double* gscale;
     const double4* inflow;
     const double* step;  // {time, dt, dt_mesh, t_end}
+    unsigned* error;     // set when a bounded wait gives up
     double rk_a, rk_b, rk_g;
     int first;
     int64_t n_elements;
+    int64_t field_stride;
     int n_instances;
 };
 
@@ -34,15 +37,15 @@ struct TraceArgs {
     const double* q;
     double* trace_out;
     int64_t n_elements;
+    int64_t field_stride;
     int n_instances;
 };
 
 cudaError_t prepare_kernels(int N, bool strict);
 cudaError_t launch_stage(int N, bool strict, const StageArgs& a, cudaStream_t stream);
 cudaError_t launch_traces(int N, bool strict, const TraceArgs& a, cudaStream_t stream);
-cudaError_t launch_initial_conditions(double* q, double* k, const double* corners, int N, int64_t K, int n_instances, cudaStream_t stream);
+cudaError_t launch_initial_conditions(double* q, double* k, const double* corners, int N, int64_t K, int64_t Kp, int n_instances, cudaStream_t stream);
 cudaError_t launch_delta_t(const double* delta_xy_min, const int* elem_N, int64_t K, double cfl, double* out, cudaStream_t stream);
-cudaError_t launch_begin_step(double* step, cudaStream_t stream);
 cudaError_t launch_end_step(double* step, cudaStream_t stream);
 cudaError_t upload_tables(const Tables& t);
 int elements_per_block(int N);
