@@ -4,31 +4,30 @@
 // instance: the reference's seven stage calls (interpolate_to_boundaries,
 // boundary_conditions, project_to_faces, calculate_wave_fluxes,
 // project_to_elements, compute_dg_wave_derivative, rk3_step;
-// include/solvers/Solver2D_t.tcu:46-70) become the phases of one CTA that
+// include/solvers/Solver2D_t.tcu:46-70) become the passes of one CTA that
 // owns a tile of EPB consecutive elements:
 //
-//   prologue  one thread starts TMA bulk copies (cp.async.bulk) of the tile's
-//             q = (p, u, v) and RK register k into shared memory, each group
-//             signalling its own mbarrier; meanwhile every thread prefetches
-//             the far-side traces of its side nodes (neighbour traces of the
-//             previous stage) and builds metric vectors and 1/J from the
-//             four corners
-//   P2a       own side traces l(+-1) . q-line          (after q has landed)
-//   P2b       upwind flux of every side node, times the edge metric
-//   P3        xi lines:  Dhat . (y_eta F - x_eta G) + lift      -> G
-//   P4        eta lines: Dhat . (-y_xi F + x_xi G) + lift, /J, then the RK
-//             update k = a k + G, q += g dt k in place (after k has landed);
-//             bottom and top traces of the new q straight from registers
-//   epilogue  one thread starts TMA bulk stores of q and k; the right and
-//             left traces of the new q go to the trace buffer
+//   prologue  one thread starts a TMA bulk copy (cp.async.bulk + mbarrier)
+//             of the tile's q = (p, u, v) into shared memory; meanwhile all
+//             threads prefetch the far-side traces of their side nodes (the
+//             neighbours' traces of the previous stage) and build J and edge
+//             metrics from the four corners
+//   rows      bottom/top own traces
+//   columns   xi-direction flux lines (kept in registers), right/left own traces
+//   flux      upwind flux of every side node, times the edge metric
+//   xi pass   Dhat . line + lift                       -> G (columns)
+//   eta pass  eta-direction flux lines, Dhat . line + lift, then /J -> G (rows)
+//   RK        k = a k + G, q += g dt k in FP64, node by node, coalesced
+//   traces    four side traces of the new q for the next stage
 //
 // Work is spread as one thread per (field, element, line), 3 EPB (N+1)
-// threads per CTA. HBM traffic per element and stage: q and k read and
-// written (the algorithmic 32 B per degree of freedom), one trace write and
-// one neighbour-trace read of 4(N+1) values per field, and 8 corner
-// coordinates. Metrics are recomputed: on straight-sided quads x_xi, y_xi
-// depend only on eta and x_eta, y_eta only on xi (quad_metrics,
-// include/functions/quad_metrics.tpp:2-7).
+// threads per CTA; shared memory carries only the q tile, G, J and the side
+// data. HBM traffic per
+// element and stage: q and k read and written (the algorithmic 32 B per
+// degree of freedom), one trace write and one neighbour-trace read of 4(N+1)
+// values per field, and 8 corner coordinates. Metrics are recomputed in
+// registers: on straight-sided quads x_xi, y_xi depend only on eta and
+// x_eta, y_eta only on xi (quad_metrics, include/functions/quad_metrics.tpp:2-7).
 //
 // Field blocks hold an even number of elements (one unused element when K is
 // odd) and tiles start on even elements, so every tile copy starts on a
@@ -73,7 +72,7 @@ template <bool S> __device__ __forceinline__ double sub(double a, double b) { re
 template <bool S> __device__ __forceinline__ double madd(double s, double a, double b) { return S ? __dadd_rn(s, __dmul_rn(a, b)) : fma(a, b, s); }
 
 // ---------------------------------------------------------------------------
-// TMA bulk copies and mbarriers (PTX ISA: cp.async.bulk, mbarrier).
+// TMA bulk copy and mbarrier (PTX ISA: cp.async.bulk, mbarrier).
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -88,12 +87,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                  "l"(src), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
-__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -129,23 +122,22 @@ struct Tile {
     static constexpr int NN = n * n;
     // Elements per CTA: even (aligned tile copies), at most ~60 KB of shared
     // memory so that several CTAs share an SM, at most 256 threads.
-    static constexpr int per_element_doubles = 3 * NN * 3 + 3 * 4 * n * 3 + 4 * n + NN + 4;
+    static constexpr int per_element_doubles = 2 * 3 * NN + 2 * 3 * 4 * n + NN + 4;
     static constexpr int by_smem = (60 * 1024 / 8) / per_element_doubles;
     static constexpr int by_threads = 256 / (3 * n);
     static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
     static constexpr int EPB = raw >= 2 ? (raw & ~1) : 2;
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
-    // shared memory layout (doubles); the tile buffers first, 16-byte aligned
-    static constexpr int kQ = 0;                         // [3][EPB][NN]
-    static constexpr int kK = kQ + 3 * EPB * NN;         // [3][EPB][NN]
-    static constexpr int kG = kK + 3 * EPB * NN;         // [3][EPB][NN]
+    // Node-wise work per thread in the RK phase: ceil(3 EPB NN / threads).
+    static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;
+    // shared memory layout (doubles); the bulk-copied q tile first
+    static constexpr int kQ = 0;                         // [3][EPB][NN] q, then q of the next stage
+    static constexpr int kG = kQ + 3 * EPB * NN;         // [3][EPB][NN] time derivative G
     static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n] own side traces
-    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far side traces
-    static constexpr int kF = kFar + 3 * EPB * 4 * n;    // [3][EPB][4][n] element side fluxes
-    static constexpr int kM = kF + 3 * EPB * 4 * n;      // [EPB][4][n] x_xi, y_xi (of eta), x_eta, y_eta (of xi)
-    static constexpr int kJ = kM + EPB * 4 * n;          // [EPB][NN] 1/J (J in strict mode)
+    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far side traces, then side fluxes
+    static constexpr int kJ = kFar + 3 * EPB * 4 * n;    // [EPB][NN] 1/J (J in strict mode)
     static constexpr int kS = kJ + EPB * NN;             // [EPB][4] edge metric per side
-    static constexpr int kBar = kS + EPB * 4;            // two mbarriers (8 bytes each)
+    static constexpr int kBar = kS + EPB * 4;            // mbarrier (8 bytes)
     static constexpr int kDoubles = kBar + 2;
     static constexpr size_t kBytes = sizeof(double) * kDoubles;
 };
@@ -182,251 +174,273 @@ __device__ __forceinline__ double metric(double t, double a, double b) {
     return mul<S>(add<S>(mul<S>(sub<S>(1.0, t), a), mul<S>(add<S>(1.0, t), b)), 0.25);
 }
 
+// Linear-in-t metric term of quad_metrics: ((1 - t) d0 + (1 + t) d1) / 4.
+// Strict mode evaluates the reference's expression; the default mode the
+// equivalent fma(t, (d1 - d0) / 4, (d0 + d1) / 4).
+template <bool S>
+struct MetricLine {
+    double d0, d1, a, b;
+    __device__ __forceinline__ MetricLine(double d0_, double d1_) : d0(d0_), d1(d1_), a(0.25 * (d0_ + d1_)), b(0.25 * (d1_ - d0_)) {}
+    __device__ __forceinline__ double operator()(double t) const { return S ? metric<S>(t, d0, d1) : fma(t, b, a); }
+};
+
 template <int N, bool S>
 __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
     using T = Tile<N>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     extern __shared__ __align__(128) double smem[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + T::kBar);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T::kBar);
     double* qs = smem + T::kQ;
-    double* ks = smem + T::kK;
     double* gs = smem + T::kG;
     double* own_s = smem + T::kOwn;
-    double* far_s = smem + T::kFar;
-    double* fs = smem + T::kF;
-    double* ms = smem + T::kM;
+    double* far_s = smem + T::kFar;  // far traces, then element side fluxes in place
     double* js = smem + T::kJ;
     double* ss = smem + T::kS;
+    constexpr int FS = EPB * 4 * n;  // field stride of own_s / far_s
 
     const int tid = threadIdx.x;
     const int64_t K = a.n_elements;
     const int64_t Kp = a.field_stride;  // elements per field block (K rounded up to even)
     const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
     const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
-    const int ne_copy = (ne + 1) & ~1;  // tile copies move an even number of elements
+    const int ne_copy = (ne + 1) & ~1;  // the tile copy moves an even number of elements
     const int64_t inst = blockIdx.y;
     double* q = a.q + inst * 3 * Kp * NN;
     double* k = a.k + inst * 3 * Kp * NN;
     const double* tr_in = a.trace_in + inst * 3 * Kp * 4 * n;
     double* tr_out = a.trace_out + inst * 3 * Kp * 4 * n;
     const double* xn = c_nodes + vec_offset(N);
+    const double* lm = c_lagrange_left + vec_offset(N);
+    const double* lp = c_lagrange_right + vec_offset(N);
     const double time = a.step[0];
     const double dt = a.step[1];
 
-    // Thread -> (field f, element e of the tile, line or node index m).
+    // Line threads: (field f, element e of the tile, line or node index m).
     const int f = tid / (EPB * n);
-    const int r = tid - f * (EPB * n);
-    const int e = r / n;
-    const int m = r - e * n;
+    const int rr = tid - f * (EPB * n);
+    const int e = rr / n;
+    const int m = rr - e * n;
     const bool active = f < 3 && e < ne;
     const int64_t ge = e0 + e;
 
-    // Prologue: bulk copies of q and k.
+    // Prologue: one bulk copy per field brings the q tile into shared memory.
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        mbar_init(bar, 1);
         mbar_fence_init();
         const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
-        mbar_expect_tx(&bars[0], 3 * bytes);
-        for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, &bars[0]);
-        if (!a.first) {
-            mbar_expect_tx(&bars[1], 3 * bytes);
-            for (int ff = 0; ff < 3; ++ff) bulk_load(ks + ff * EPB * NN, k + (ff * Kp + e0) * NN, bytes, &bars[1]);
-        }
+        mbar_expect_tx(bar, 3 * bytes);
+        for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
     }
-
-    // Prefetch of the far-side traces of this thread's side nodes: interior
-    // and periodic sides read the neighbour's trace of the previous stage.
-    double far_pref[4] = {0.0, 0.0, 0.0, 0.0};
+    // Far traces of this thread's field at node m of the four sides (the
+    // neighbour's trace of the previous stage), element metrics, edge
+    // metrics and J.
+    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const int2 lk = a.link[4 * ge + s];
-            if (((lk.y >> 2) & 7) == kInterior) far_pref[s] = tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)];
+            const double v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0;
+            far_s[f * FS + (e * 4 + s) * n + m] = v;
         }
-        // Metric vectors, edge metrics and 1/J of the element, from its corners.
         const double* c = a.corners + 8 * ge;
-        const double x0 = c[0], y0 = c[1], x1 = c[2], y1 = c[3], x2 = c[4], y2 = c[5], x3 = c[6], y3 = c[7];
-        double* mv = ms + e * 4 * n;
-        const double t = xn[m];
-        const double x_eta = metric<S>(t, sub<S>(x3, x0), sub<S>(x2, x1));  // at xi = t
-        const double y_eta = metric<S>(t, sub<S>(y3, y0), sub<S>(y2, y1));
-        if (f == 0) {
-            mv[0 * n + m] = metric<S>(t, sub<S>(x1, x0), sub<S>(x2, x3));  // x_xi at eta = t
-            mv[1 * n + m] = metric<S>(t, sub<S>(y1, y0), sub<S>(y2, y3));  // y_xi at eta = t
-        } else if (f == 1) {
-            mv[2 * n + m] = x_eta;
-            mv[3 * n + m] = y_eta;
-        } else {
+        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
+    }
+    // x_xi, y_xi are functions of eta; x_eta, y_eta functions of xi.
+    const MetricLine<S> x_xi(sub<S>(x1, x0), sub<S>(x2, x3)), y_xi(sub<S>(y1, y0), sub<S>(y2, y3));
+    const MetricLine<S> x_eta(sub<S>(x3, x0), sub<S>(x2, x1)), y_eta(sub<S>(y3, y0), sub<S>(y2, y1));
+    if (active) {
+        const double tm = xn[m];
+        if (f == 2) {
             // Edge metric of side sd, constant along a straight side
             // (Element2D_t.cpp:756-769): |d(x,y)/dxi| at eta = -1, +1 for
             // sides 0, 2 and |d(x,y)/deta| at xi = +1, -1 for sides 1, 3.
             for (int sd = m; sd < 4; sd += n) {
                 const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
-                double dx, dy;
-                if (sd == 0 || sd == 2) {
-                    dx = metric<S>(at, sub<S>(x1, x0), sub<S>(x2, x3));
-                    dy = metric<S>(at, sub<S>(y1, y0), sub<S>(y2, y3));
-                } else {
-                    dx = metric<S>(at, sub<S>(x3, x0), sub<S>(x2, x1));
-                    dy = metric<S>(at, sub<S>(y3, y0), sub<S>(y2, y1));
-                }
+                const double dx = (sd == 0 || sd == 2) ? metric<S>(at, x_xi.d0, x_xi.d1) : metric<S>(at, x_eta.d0, x_eta.d1);
+                const double dy = (sd == 0 || sd == 2) ? metric<S>(at, y_xi.d0, y_xi.d1) : metric<S>(at, y_eta.d0, y_eta.d1);
                 ss[e * 4 + sd] = sqrt(add<S>(mul<S>(dx, dx), mul<S>(dy, dy)));
             }
         }
-        // J at nodes (m, j), j = f, f + 3, ...: x_xi(eta_j) y_eta(xi_m) - x_eta(xi_m) y_xi(eta_j).
+        // J at nodes (m, j), j = f, f + 3, ...: x_xi(eta_j) y_eta(xi_m) - x_eta(xi_m) y_xi(eta_j)
+        // (Element2D_t.cpp:752).
+        const double xe = x_eta(tm), ye = y_eta(tm);
         for (int j = f; j < n; j += 3) {
             const double tj = xn[j];
-            const double x_xi = metric<S>(tj, sub<S>(x1, x0), sub<S>(x2, x3));
-            const double y_xi = metric<S>(tj, sub<S>(y1, y0), sub<S>(y2, y3));
-            const double jac = sub<S>(mul<S>(x_xi, y_eta), mul<S>(x_eta, y_xi));
+            const double jac = sub<S>(mul<S>(x_xi(tj), ye), mul<S>(xe, y_xi(tj)));
             js[e * NN + m * n + j] = S ? jac : __drcp_rn(jac);
         }
     }
-    __syncthreads();  // mbarrier init, metrics, J
+    __syncthreads();  // mbarrier init, far traces, edge metrics, J
+    if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
 
-    if (!mbar_wait(&bars[0], a.error, kWaitLimitNs)) return;
-
-    // P2a: own side traces of this thread's field at node m of each side,
-    // and the prefetched far traces.
-    if (active) {
-        const double* qf = qs + (f * EPB + e) * NN;
+    // Row pass (xi index i = m): bottom and top traces (Element2D_t.cpp:86-125)
+    // of the rows; field 0's threads take u and v, field 1's take p.
+    if (active && f < 2) {
+        const int i = m;
+        const double* R0 = qs + ((f == 0 ? 1 : 0) * EPB + e) * NN + i * n;
+        const double* R1 = qs + (2 * EPB + e) * NN + i * n;
+        double b0 = 0.0, t0 = 0.0, b1 = 0.0, t1 = 0.0;
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            own_s[((f * EPB + e) * 4 + s) * n + m] = side_trace<N, S>(qf, s, m);
-            far_s[((f * EPB + e) * 4 + s) * n + m] = far_pref[s];
+        for (int j = 0; j < n; ++j) {
+            b0 = madd<S>(b0, lm[j], R0[j]);
+            t0 = madd<S>(t0, lp[j], R0[j]);
+            if (f == 0) {
+                b1 = madd<S>(b1, lm[j], R1[j]);
+                t1 = madd<S>(t1, lp[j], R1[j]);
+            }
+        }
+        const int fa = f == 0 ? 1 : 0;
+        own_s[fa * FS + (e * 4 + 0) * n + i] = b0;
+        own_s[fa * FS + (e * 4 + 2) * n + (N - i)] = t0;
+        if (f == 0) {
+            own_s[2 * FS + (e * 4 + 0) * n + i] = b1;
+            own_s[2 * FS + (e * 4 + 2) * n + (N - i)] = t1;
+        }
+    }
+    // Column pass (eta index j = m): the xi-direction flux line
+    // (Solver2D_t.cpp:72-80), and the right and left traces.
+    double col[n];
+    if (active) {
+        const int j = m;
+        const double* P = qs + (0 * EPB + e) * NN + j;
+        const double* U = qs + (1 * EPB + e) * NN + j;
+        const double* V = qs + (2 * EPB + e) * NN + j;
+        if (f == 0) {
+            double ru = 0.0, lu = 0.0, rv = 0.0, lv = 0.0;
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                const double u = U[i * n], v = V[i * n];
+                col[i] = sub<S>(mul<S>(y_eta(xn[i]), u), mul<S>(x_eta(xn[i]), v));
+                ru = madd<S>(ru, lp[i], u);
+                lu = madd<S>(lu, lm[i], u);
+                rv = madd<S>(rv, lp[i], v);
+                lv = madd<S>(lv, lm[i], v);
+            }
+            own_s[1 * FS + (e * 4 + 1) * n + j] = ru;
+            own_s[1 * FS + (e * 4 + 3) * n + (N - j)] = lu;
+            own_s[2 * FS + (e * 4 + 1) * n + j] = rv;
+            own_s[2 * FS + (e * 4 + 3) * n + (N - j)] = lv;
+        } else {
+            double rp = 0.0, lp_ = 0.0;
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                const double p = P[i * n];
+                col[i] = (f == 1) ? mul<S>(y_eta(xn[i]), p) : -mul<S>(x_eta(xn[i]), p);
+                rp = madd<S>(rp, lp[i], p);
+                lp_ = madd<S>(lp_, lm[i], p);
+            }
+            if (f == 1) {
+                own_s[0 * FS + (e * 4 + 1) * n + j] = rp;
+                own_s[0 * FS + (e * 4 + 3) * n + (N - j)] = lp_;
+            }
         }
     }
     __syncthreads();
 
-    // P2b: far traces of boundary sides, upwind flux (Solver2D_t.cpp:48-63)
-    // in the face's own left/right order, then the element's view of it
-    // (Mesh2D_t.cpp:3895-3929): times the edge metric, negated for the
-    // face's right element.
-    for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
-        const int ee = idx / (4 * n);
-        const int s = (idx / n) & 3;
-        const int mm = idx - (idx / n) * n;
-        const int64_t g = e0 + ee;
-        const int2 lk = a.link[4 * g + s];
-        const double2 nrm = a.normal[4 * g + s];
-        const int kind = (lk.y >> 2) & 7;
-        const int role = (lk.y >> 5) & 1;
-        const int o = (ee * 4 + s) * n + mm;
-        constexpr int fstride = EPB * 4 * n;
-        const double op = own_s[o], ou = own_s[fstride + o], ov = own_s[2 * fstride + o];
-        double fp_, fu_, fv_;
-        if (kind == kInterior) {
-            fp_ = far_s[o];
-            fu_ = far_s[fstride + o];
-            fv_ = far_s[2 * fstride + o];
-        } else if (kind == kMirror || kind == kCopy) {
-            // Ghost trace: the own trace reversed and scaled by the ghost's
-            // edge metric; walls and symmetry planes then mirror the normal
-            // velocity (Mesh2D_t.cpp:4366-4434, 4601-4710).
-            const double gsc = a.gscale[4 * g + s];
-            fp_ = mul<S>(op, gsc);
-            const double gu = mul<S>(ou, gsc), gv = mul<S>(ov, gsc);
-            if (kind == kMirror) {
-                const double tx = -nrm.y, ty = nrm.x;
-                const double l0 = -add<S>(mul<S>(gu, nrm.x), mul<S>(gv, nrm.y));
-                const double l1 = add<S>(mul<S>(gu, tx), mul<S>(gv, ty));
-                fu_ = add<S>(mul<S>(nrm.x, l0), mul<S>(tx, l1));
-                fv_ = add<S>(mul<S>(nrm.y, l0), mul<S>(ty, l1));
+    // Flux pass: side nodes of sides {0, 3} (f = 0), {1} (f = 1), {2} (f = 2)
+    // at index m. Far traces of boundary sides, the upwind flux
+    // (Solver2D_t.cpp:48-63) in the face's own left/right order, then the
+    // element's view of it (Mesh2D_t.cpp:3895-3929): times the edge metric,
+    // negated for the face's right element.
+    if (active) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (!((f == 0 && (s == 0 || s == 3)) || (f == 1 && s == 1) || (f == 2 && s == 2))) continue;
+            const int2 lk = a.link[4 * ge + s];
+            const int kind = (lk.y >> 2) & 7;
+            const int role = (lk.y >> 5) & 1;
+            const double2 nv = a.normal[4 * ge + s];
+            const int o = (e * 4 + s) * n + m;
+            const double op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
+            double fp_, fu_, fv_;
+            if (kind == kInterior) {
+                fp_ = far_s[o];
+                fu_ = far_s[FS + o];
+                fv_ = far_s[2 * FS + o];
+            } else if (kind == kMirror || kind == kCopy) {
+                // Ghost trace: the own trace reversed and scaled by the ghost's
+                // edge metric; walls and symmetry planes then mirror the normal
+                // velocity (Mesh2D_t.cpp:4366-4434, 4601-4710).
+                const double gsc = a.gscale[4 * ge + s];
+                fp_ = mul<S>(op, gsc);
+                const double gu = mul<S>(ou, gsc), gv = mul<S>(ov, gsc);
+                if (kind == kMirror) {
+                    const double tx = -nv.y, ty = nv.x;
+                    const double l0 = -add<S>(mul<S>(gu, nv.x), mul<S>(gv, nv.y));
+                    const double l1 = add<S>(mul<S>(gu, tx), mul<S>(gv, ty));
+                    fu_ = add<S>(mul<S>(nv.x, l0), mul<S>(tx, l1));
+                    fv_ = add<S>(mul<S>(nv.y, l0), mul<S>(ty, l1));
+                } else {
+                    fu_ = gu;
+                    fv_ = gv;
+                }
+            } else if (kind == kAnalytic) {
+                // Inflow: the analytic wave on the ghost edge at the stage time
+                // (Mesh2D_t.cpp:4575-4599); the face reads ghost node N - m.
+                const double4 gq = a.inflow[4 * ge + s];
+                const double r = mul<S>(add<S>(xn[N - m], 1.0), 0.5);
+                const double gx = add<S>(mul<S>(gq.z, r), mul<S>(gq.x, sub<S>(1.0, r)));
+                const double gy = add<S>(mul<S>(gq.w, r), mul<S>(gq.y, sub<S>(1.0, r)));
+                plane_wave(gx, gy, add<S>(time, mul<S>(a.rk_b, dt)), fp_, fu_, fv_);
             } else {
-                fu_ = gu;
-                fv_ = gv;
+                fp_ = fu_ = fv_ = 0.0;
             }
-        } else if (kind == kAnalytic) {
-            // Inflow: the analytic wave on the ghost edge at the stage time
-            // (Mesh2D_t.cpp:4575-4599); the face reads ghost node N - m.
-            const double4 gq = a.inflow[4 * g + s];
-            const double rr = mul<S>(add<S>(xn[N - mm], 1.0), 0.5);
-            const double gx = add<S>(mul<S>(gq.z, rr), mul<S>(gq.x, sub<S>(1.0, rr)));
-            const double gy = add<S>(mul<S>(gq.w, rr), mul<S>(gq.y, sub<S>(1.0, rr)));
-            plane_wave(gx, gy, add<S>(time, mul<S>(a.rk_b, dt)), fp_, fu_, fv_);
-        } else {
-            fp_ = fu_ = fv_ = 0.0;
+            const double Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
+            const double Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
+            const double wL = add<S>(Lp, add<S>(mul<S>(Lu, nv.x), mul<S>(Lv, nv.y)));
+            const double wR = sub<S>(Rp, add<S>(mul<S>(Ru, nv.x), mul<S>(Rv, nv.y)));
+            const double flp = mul<S>(sub<S>(wL, wR), 0.5);
+            const double sum = add<S>(wL, wR);
+            const double flu = mul<S>(mul<S>(nv.x, sum), 0.5);
+            const double flv = mul<S>(mul<S>(nv.y, sum), 0.5);
+            const double sf = ss[e * 4 + s];
+            far_s[o] = mul<S>(role ? -flp : flp, sf);
+            far_s[FS + o] = mul<S>(role ? -flu : flu, sf);
+            far_s[2 * FS + o] = mul<S>(role ? -flv : flv, sf);
         }
-        const double Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
-        const double Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
-        const double wL = add<S>(Lp, add<S>(mul<S>(Lu, nrm.x), mul<S>(Lv, nrm.y)));
-        const double wR = sub<S>(Rp, add<S>(mul<S>(Ru, nrm.x), mul<S>(Rv, nrm.y)));
-        const double flp = mul<S>(sub<S>(wL, wR), 0.5);
-        const double sum = add<S>(wL, wR);
-        const double flu = mul<S>(mul<S>(nrm.x, sum), 0.5);
-        const double flv = mul<S>(mul<S>(nrm.y, sum), 0.5);
-        const double sf = ss[ee * 4 + s];
-        fs[o] = mul<S>(role ? -flp : flp, sf);
-        fs[fstride + o] = mul<S>(role ? -flu : flu, sf);
-        fs[2 * fstride + o] = mul<S>(role ? -flv : flv, sf);
     }
     __syncthreads();
 
     const double* Dh = c_dhat + mat_offset(N);
-    const double* lm = c_lagrange_left + vec_offset(N);
-    const double* lp = c_lagrange_right + vec_offset(N);
     const double* w = c_weights + vec_offset(N);
     const double* iw = c_inv_weights + vec_offset(N);
+    const double* F = far_s + f * FS + e * 4 * n;  // this thread's field, element side fluxes
 
-    // P3: xi lines (eta index j = m), Solver2D_t.cpp:71-101.
+    // xi pass (eta index j = m): Dhat . line + lift, G = -(...)
+    // (Solver2D_t.cpp:82-101); G column j.
     if (active) {
         const int j = m;
-        const double* P = qs + (0 * EPB + e) * NN;
-        const double* U = qs + (1 * EPB + e) * NN;
-        const double* V = qs + (2 * EPB + e) * NN;
-        const double* mv = ms + e * 4 * n;
-        double fl[n];
-#pragma unroll
-        for (int i = 0; i < n; ++i) {
-            const double x_eta = mv[2 * n + i], y_eta = mv[3 * n + i];
-            if (f == 0) fl[i] = sub<S>(mul<S>(y_eta, U[i * n + j]), mul<S>(x_eta, V[i * n + j]));
-            else if (f == 1) fl[i] = mul<S>(y_eta, P[i * n + j]);
-            else fl[i] = -mul<S>(x_eta, P[i * n + j]);
-        }
-        const double fr = fs[((f * EPB + e) * 4 + 1) * n + j];
-        const double fl3 = fs[((f * EPB + e) * 4 + 3) * n + (N - j)];
-        double* G = gs + (f * EPB + e) * NN;
+        const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
+        double* G = gs + (f * EPB + e) * NN + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             double acc = 0.0;
 #pragma unroll
-            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[i * n + mm], fl[mm]);
+            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[i * n + mm], col[mm]);
             const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
-            G[i * n + j] = -add<S>(acc, lift);
+            G[i * n] = -add<S>(acc, lift);
         }
     }
     __syncthreads();
 
-    // P4: eta lines (xi index i = m), Solver2D_t.cpp:103-134, the division
-    // by J, and the low-storage RK3 update (Solver2D_t.cpp:138-172).
-    double line[n];  // contravariant flux of this thread's field along eta, from q before the update
+    // eta pass (xi index i = m): G = (G - (Dhat . line + lift)) / J
+    // (Solver2D_t.cpp:114-133); G row i.
     if (active) {
         const int i = m;
+        // eta-direction contravariant flux line of this thread's field (Solver2D_t.cpp:103-113).
+        double line[n];
         const double* P = qs + (0 * EPB + e) * NN + i * n;
         const double* U = qs + (1 * EPB + e) * NN + i * n;
         const double* V = qs + (2 * EPB + e) * NN + i * n;
-        const double* mv = ms + e * 4 * n;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            const double x_xi = mv[0 * n + j], y_xi = mv[1 * n + j];
-            if (f == 0) line[j] = add<S>(mul<S>(-y_xi, U[j]), mul<S>(x_xi, V[j]));
-            else if (f == 1) line[j] = mul<S>(-y_xi, P[j]);
-            else line[j] = mul<S>(x_xi, P[j]);
+            if (f == 0) line[j] = add<S>(mul<S>(-y_xi(xn[j]), U[j]), mul<S>(x_xi(xn[j]), V[j]));
+            else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), P[j]);
+            else line[j] = mul<S>(x_xi(xn[j]), P[j]);
         }
-    }
-    __syncthreads();  // every thread holds its inputs: rows of q may now be overwritten
-    if (!a.first && !mbar_wait(&bars[1], a.error, kWaitLimitNs)) return;
-    if (active) {
-        const int i = m;
-        const double ft = fs[((f * EPB + e) * 4 + 2) * n + (N - i)];
-        const double fb = fs[((f * EPB + e) * 4 + 0) * n + i];
-        const double* G = gs + (f * EPB + e) * NN + i * n;
+        const double ft = F[2 * n + (N - i)], fb = F[0 * n + i];
+        double* G = gs + (f * EPB + e) * NN + i * n;
         const double* jrow = js + e * NN + i * n;
-        double* qrow = qs + (f * EPB + e) * NN + i * n;
-        double* krow = ks + (f * EPB + e) * NN + i * n;
-        const double gdt = mul<S>(a.rk_g, dt);
-        double bottom = 0.0, top = 0.0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             double acc = 0.0;
@@ -434,37 +448,57 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
             for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[j * n + mm], line[mm]);
             const double lift = S ? __ddiv_rn(add<S>(mul<S>(ft, lp[j]), mul<S>(fb, lm[j])), w[j]) : (ft * lp[j] + fb * lm[j]) * iw[j];
             const double num = sub<S>(G[j], add<S>(acc, lift));
-            const double Gn = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
-            const double kn = a.first ? Gn : add<S>(mul<S>(a.rk_a, krow[j]), Gn);
-            const double qn = add<S>(qrow[j], mul<S>(gdt, kn));
-            krow[j] = kn;
-            qrow[j] = qn;
-            if (a.G_out) a.G_out[inst * 3 * Kp * NN + (f * Kp + ge) * NN + i * n + j] = Gn;
-            bottom = madd<S>(bottom, lm[j], qn);
-            top = madd<S>(top, lp[j], qn);
+            G[j] = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
         }
-        // Bottom and top traces of the new solution (Element2D_t.cpp:86-125).
-        tr_out[((f * Kp + ge) * 4 + 0) * n + i] = bottom;
-        tr_out[((f * Kp + ge) * 4 + 2) * n + (N - i)] = top;
     }
-    fence_proxy_async();
     __syncthreads();
 
-    // Epilogue: bulk stores of the tile, and the right and left traces.
-    if (tid == 0) {
-        const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
-        for (int ff = 0; ff < 3; ++ff) {
-            bulk_store(q + (ff * Kp + e0) * NN, qs + ff * EPB * NN, bytes);
-            bulk_store(k + (ff * Kp + e0) * NN, ks + ff * EPB * NN, bytes);
+    // Low-storage RK3 update (Solver2D_t.cpp:138-172), node by node:
+    // coalesced reads of k (prefetched) and writes of k and q.
+    const double gdt = mul<S>(a.rk_g, dt);
+    double kold[T::kNodeIters];
+#pragma unroll
+    for (int c = 0; c < T::kNodeIters; ++c) {
+        const int idx = tid + c * T::kThreads;
+        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
+        kold[c] = (!a.first && ff < 3 && r < ne * NN) ? k[(ff * Kp + e0) * NN + r] : 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < T::kNodeIters; ++c) {
+        const int idx = tid + c * T::kThreads;
+        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
+        if (ff < 3 && r < ne * NN) {
+            const double G = gs[ff * EPB * NN + r];
+            const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, kold[c]), G);
+            const double qn = add<S>(qs[ff * EPB * NN + r], mul<S>(gdt, kn));
+            const int64_t gi = (ff * Kp + e0) * NN + r;
+            k[gi] = kn;
+            q[gi] = qn;
+            qs[ff * EPB * NN + r] = qn;
+            if (a.G_out) a.G_out[inst * 3 * Kp * NN + gi] = G;
         }
-        bulk_commit();
     }
+    __syncthreads();
+
+    // Side traces of the new solution for the next stage: bottom/top from
+    // row m, right/left from column m (Element2D_t.cpp:86-125).
     if (active) {
-        const double* qf = qs + (f * EPB + e) * NN;
-        tr_out[((f * Kp + ge) * 4 + 1) * n + m] = side_trace<N, S>(qf, 1, m);
-        tr_out[((f * Kp + ge) * 4 + 3) * n + m] = side_trace<N, S>(qf, 3, m);
+        const double* row = qs + (f * EPB + e) * NN + m * n;
+        const double* cl = qs + (f * EPB + e) * NN + m;
+        double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            b = madd<S>(b, lm[j], row[j]);
+            t = madd<S>(t, lp[j], row[j]);
+            r = madd<S>(r, lp[j], cl[j * n]);
+            l = madd<S>(l, lm[j], cl[j * n]);
+        }
+        double* to = tr_out + (f * Kp + ge) * 4 * n;
+        to[0 * n + m] = b;
+        to[2 * n + (N - m)] = t;
+        to[1 * n + m] = r;
+        to[3 * n + (N - m)] = l;
     }
-    if (tid == 0) bulk_wait_read();
 }
 
 // Side traces only (start of a run, or after the host changed q).
