@@ -131,13 +131,16 @@ def measured_hbm_peak() -> tuple[float, str]:
 
 def profiled_traffic() -> float | None:
     """DRAM bytes per stage-kernel launch from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.txt")
     try:
         with open(path) as f:
-            d = json.load(f)
-        return float(d[f"N{ORDER}_res{RES}"]["dram_bytes_per_launch"])
-    except (OSError, KeyError, ValueError):
-        return None
+            for line in f:
+                parts = line.split()
+                if len(parts) == 2 and parts[0] == f"N{ORDER}_res{RES}":
+                    return float(parts[1])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 # ---------------------------------------------------------------------------

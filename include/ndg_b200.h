@@ -187,6 +187,14 @@ ndg_status ndg_run(ndg_ctx* ctx, int64_t n_steps, double* time);
  * t_end. *time is the start time in and the end time out. */
 ndg_status ndg_solve(ndg_ctx* ctx, double t_end, double* time, int64_t* n_steps);
 
+/* Mesh2D_t::estimate_error (src/meshes/Mesh2D_t.cu:5158, Element2D_t::estimate_p_error,
+ * src/entities/Element2D_t.cpp:274-343): Legendre-coefficient decay of the
+ * pressure in every element of every instance, on the device. */
+ndg_status ndg_estimate_error(ndg_ctx* ctx);
+/* Per element of one instance: p_error_, p_sigma_, refine_ (error >
+ * tolerance_min), coarsen_ (error < tolerance_max). Any pointer may be NULL. */
+ndg_status ndg_get_error(ndg_ctx* ctx, int32_t instance, double* p_error, double* p_sigma, int32_t* refine, int32_t* coarsen);
+
 /* Benchmark aid: launches stage m n_launches times back to back (the state
  * advances), timing each launch with CUDA events on the context's stream;
  * *avg_ms = mean kernel duration. */

@@ -86,6 +86,8 @@ def lib() -> C.CDLL:
         "ndg_solve": ([vp, dbl, C.POINTER(dbl), C.POINTER(i64)], C.c_int),
         "ndg_launch_count": ([vp, C.POINTER(i64)], C.c_int),
         "ndg_time_stage": ([vp, i32, i32, C.POINTER(dbl)], C.c_int),
+        "ndg_estimate_error": ([vp], C.c_int),
+        "ndg_get_error": ([vp, i32, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
@@ -261,6 +263,18 @@ class Mesh2D_t:
         out = np.empty(self.field_size * (self.n_instances if instance < 0 else 1))
         _check(lib().ndg_get_field(self._ctx.h, instance, FIELDS[name], _ptr(out)))
         return out
+
+    # Mesh2D_t::estimate_error (src/meshes/Mesh2D_t.cu:5158)
+    def estimate_error(self) -> None:
+        _check(lib().ndg_estimate_error(self._ctx.h))
+
+    def error(self, instance: int = 0) -> dict:
+        """p_error_, p_sigma_, refine_, coarsen_ of every element of one instance."""
+        K = self.n_elements_
+        d = {"p_error": np.empty(K), "p_sigma": np.empty(K), "refine": np.empty(K, dtype=np.int32),
+             "coarsen": np.empty(K, dtype=np.int32)}
+        _check(lib().ndg_get_error(self._ctx.h, instance, *[_ptr(d[k]) for k in ("p_error", "p_sigma", "refine", "coarsen")]))
+        return d
 
     def synchronize(self) -> None:
         _check(lib().ndg_ctx_synchronize(self._ctx.h))

@@ -2,6 +2,7 @@
 // fields and time stepping. Host orchestration only; the arithmetic is in
 // stage_kernels.cu.
 #include "ndg_internal.hpp"
+#include "estimator.cuh"
 #include "stage_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -82,6 +83,9 @@ struct ndg_ctx {
     ndg::DeviceBuffer<double> q, k, G, tr[2], corners, normal, gscale, inflow, dxy, step, scratch;
     ndg::DeviceBuffer<int32_t> link, elem_N;
     ndg::DeviceBuffer<unsigned> error;
+    ndg::DeviceBuffer<double> p_error, p_sigma;
+    ndg::DeviceBuffer<int32_t> refine, coarsen;
+    bool has_error_estimate = false;
     int cur = 0;
     bool traces_valid = false;
     double dt_mesh = 0.0;
@@ -230,7 +234,10 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     if (!c->has_tables || c->tables.N_max < p.maximum_N) {
         c->tables = build_tables(p.maximum_N, p.n_interpolation_points > 1 ? p.n_interpolation_points : 2);
         c->has_tables = true;
-        if (c->device >= 0) check_cuda(dev::upload_tables(c->tables), "table upload");
+        if (c->device >= 0) {
+            check_cuda(dev::upload_tables(c->tables), "table upload");
+            check_cuda(dev::upload_polynomials(c->tables), "table upload");
+        }
     }
     compute_geometry(topo, c->tables);
     c->topo = std::move(topo);
@@ -261,6 +268,11 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     c->tr[0].allocate(inst * 3 * Kp * 4 * n);
     c->tr[1].allocate(inst * 3 * Kp * 4 * n);
     c->error.allocate(1);
+    c->p_error.allocate(inst * K);
+    c->p_sigma.allocate(inst * K);
+    c->refine.allocate(inst * K);
+    c->coarsen.allocate(inst * K);
+    c->has_error_estimate = false;
     c->corners.allocate(plan.corners.size());
     c->normal.allocate(plan.normal.size());
     c->gscale.allocate(plan.gscale.size());
@@ -410,7 +422,10 @@ ndg_status ndg_tables_build(ndg_ctx* ctx, int32_t N_max, int64_t n_interp) {
         make_current(ctx);
         ctx->tables = build_tables(N_max, n_interp);
         ctx->has_tables = true;
-        if (ctx->device >= 0) check_cuda(dev::upload_tables(ctx->tables), "table upload");
+        if (ctx->device >= 0) {
+            check_cuda(dev::upload_tables(ctx->tables), "table upload");
+            check_cuda(dev::upload_polynomials(ctx->tables), "table upload");
+        }
     });
 }
 
@@ -673,6 +688,46 @@ ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* a
         }
         for (auto& e : ev) cudaEventDestroy(e);
         *avg_ms = total / n_launches;
+    });
+}
+
+ndg_status ndg_estimate_error(ndg_ctx* ctx) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        make_current(ctx);
+        dev::EstimatorArgs a{};
+        a.q = ctx->q.ptr;
+        a.p_error = ctx->p_error.ptr;
+        a.p_sigma = ctx->p_sigma.ptr;
+        a.refine = ctx->refine.ptr;
+        a.coarsen = ctx->coarsen.ptr;
+        a.tolerance_min = ctx->params.tolerance_min;
+        a.tolerance_max = ctx->params.tolerance_max;
+        a.n_elements = ctx->K;
+        a.field_stride = ctx->Kp;
+        a.n_instances = ctx->n_instances;
+        a.N = ctx->N;
+        check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
+        ++ctx->launches;
+        ctx->has_error_estimate = true;
+    });
+}
+
+ndg_status ndg_get_error(ndg_ctx* ctx, int32_t instance, double* p_error, double* p_sigma, int32_t* refine, int32_t* coarsen) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (!ctx->has_error_estimate) fail(NDG_ERR_INVALID_ARG, "call ndg_estimate_error first");
+        if (instance < 0 || instance >= ctx->n_instances) fail(NDG_ERR_INVALID_ARG, "instance out of range");
+        make_current(ctx);
+        const size_t off = static_cast<size_t>(instance) * static_cast<size_t>(ctx->K);
+        const size_t K = static_cast<size_t>(ctx->K);
+        if (p_error) check_cuda(cudaMemcpyAsync(p_error, ctx->p_error.ptr + off, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "error download");
+        if (p_sigma) check_cuda(cudaMemcpyAsync(p_sigma, ctx->p_sigma.ptr + off, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "error download");
+        if (refine) check_cuda(cudaMemcpyAsync(refine, ctx->refine.ptr + off, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "error download");
+        if (coarsen) check_cuda(cudaMemcpyAsync(coarsen, ctx->coarsen.ptr + off, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "error download");
+        check_cuda(cudaStreamSynchronize(ctx->stream), "error download");
     });
 }
 
