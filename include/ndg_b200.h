@@ -175,6 +175,10 @@ ndg_status ndg_get_field(ndg_ctx* ctx, int32_t instance, int32_t field, double* 
 /* Solver2D_t::get_delta_t (src/solvers/Solver2D_t.cu:17-31): min over
  * elements of CFL * delta_xy_min / (N^2 c), reduced on the device. */
 ndg_status ndg_get_delta_t(ndg_ctx* ctx, double* delta_t);
+/* The CFL of Solver2D_t(CFL, ...) (include/solvers/Solver2D_t.cuh:16):
+ * recomputes the mesh's step for a new CFL (the load used
+ * ndg_mesh_params.cfl); later ndg_run/ndg_solve steps use it. */
+ndg_status ndg_set_cfl(ndg_ctx* ctx, double cfl);
 /* One low-storage RK3 stage m in {0,1,2} at step start `time` with step dt:
  * interpolate_to_boundaries, boundary_conditions, project_to_faces,
  * calculate_wave_fluxes, project_to_elements, compute_dg_wave_derivative,

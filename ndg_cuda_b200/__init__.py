@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
         "ndg_set_field": ([vp, i32, i32, vp], C.c_int),
         "ndg_get_field": ([vp, i32, i32, vp], C.c_int),
         "ndg_get_delta_t": ([vp, C.POINTER(dbl)], C.c_int),
+        "ndg_set_cfl": ([vp, dbl], C.c_int),
         "ndg_stage": ([vp, i32, dbl, dbl], C.c_int),
         "ndg_run": ([vp, i64, C.POINTER(dbl)], C.c_int),
         "ndg_solve": ([vp, dbl, C.POINTER(dbl), C.POINTER(i64)], C.c_int),
@@ -349,9 +350,11 @@ class Solver2D_t:
         return t.value
 
     def solve(self, mesh: Mesh2D_t, time: float = 0.0) -> tuple[float, int]:
-        """Steps to output_times_[-1] with the reference's shortened last step."""
+        """Steps to output_times_[-1] with the reference's shortened last step,
+        at this solver's CFL."""
         t = C.c_double(time)
         n = C.c_int64()
+        _check(lib().ndg_set_cfl(mesh.handle, float(self.CFL_)))
         _check(lib().ndg_solve(mesh.handle, float(self.output_times_[-1]), C.byref(t), C.byref(n)))
         return t.value, n.value
 

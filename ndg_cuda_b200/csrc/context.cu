@@ -227,6 +227,15 @@ double* field_ptr(ndg_ctx* c, int32_t field, int instance) {
     fail(NDG_ERR_INVALID_ARG, "unknown field");
 }
 
+// CFL step of the fixed mesh, reduced on the device (Solver2D_t.cu:17-31).
+void compute_dt_mesh(ndg_ctx* c, double cfl) {
+    check_cuda(dev::launch_delta_t(c->dxy.ptr, c->elem_N.ptr, c->K, cfl, c->step.ptr + 2, c->stream), "delta_t kernel");
+    ++c->launches;
+    check_cuda(cudaMemcpyAsync(&c->dt_mesh, c->step.ptr + 2, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "delta_t readback");
+    check_cuda(cudaStreamSynchronize(c->stream), "delta_t");
+    c->params.cfl = cfl;
+}
+
 void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_instances) {
     if (n_instances < 1) fail(NDG_ERR_INVALID_ARG, "n_instances must be >= 1");
     if (p.initial_N < 1 || p.initial_N > p.maximum_N) fail(NDG_ERR_INVALID_ARG, "need 1 <= initial_N <= maximum_N");
@@ -299,11 +308,7 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     check_cuda(cudaMemsetAsync(c->error.ptr, 0, sizeof(unsigned), c->stream), "memset");
     check_cuda(dev::prepare_kernels(c->N, false), "kernel attributes");
     check_cuda(dev::prepare_kernels(c->N, true), "kernel attributes");
-    // CFL step of the fixed mesh, reduced on the device (Solver2D_t.cu:17-31).
-    check_cuda(dev::launch_delta_t(c->dxy.ptr, c->elem_N.ptr, c->K, p.cfl, c->step.ptr + 2, c->stream), "delta_t kernel");
-    ++c->launches;
-    check_cuda(cudaMemcpyAsync(&c->dt_mesh, c->step.ptr + 2, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "delta_t readback");
-    check_cuda(cudaStreamSynchronize(c->stream), "mesh load");
+    compute_dt_mesh(c, p.cfl);
 }
 
 template <typename F>
@@ -609,6 +614,16 @@ ndg_status ndg_get_delta_t(ndg_ctx* ctx, double* delta_t) {
         require_device(ctx);
         if (!delta_t) fail(NDG_ERR_INVALID_ARG, "delta_t is NULL");
         *delta_t = ctx->dt_mesh;
+    });
+}
+
+ndg_status ndg_set_cfl(ndg_ctx* ctx, double cfl) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (!(cfl > 0.0) || !std::isfinite(cfl)) fail(NDG_ERR_INVALID_ARG, "cfl must be positive and finite");
+        make_current(ctx);
+        compute_dt_mesh(ctx, cfl);
     });
 }
 

@@ -14,6 +14,7 @@ import pytest
 import ndg_cuda_b200 as ndg
 from oracle.pyoracle import OracleSolver, oracle_table
 from tests import meshgen
+from tests.meshgen import su2_markers, write_su2
 
 HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "ndg_b200.h")
 
@@ -67,27 +68,6 @@ def test_topology_bitwise_vs_oracle(name, res, kw):
     assert np.array_equal(m.nodes(), o.nodes())
 
 
-def write_su2(path, zone: dict, markers: dict) -> None:
-    """Writes the zone's quads and the given {tag: bar sections} as SU2 (0-based)."""
-    quads = zone["sections"][0][4].reshape(-1, 4) - 1
-    with open(path, "w") as f:
-        f.write("NDIME= 2\n")
-        f.write(f"NPOIN= {zone['x'].size}\n")
-        for x, y in zip(zone["x"], zone["y"]):
-            f.write(f"{x:.17g} {y:.17g}\n")
-        f.write(f"NELEM= {len(quads)}\n")
-        for q in quads:
-            f.write("9 " + " ".join(str(v) for v in q) + "\n")
-        f.write(f"NMARK= {len(markers)}\n")
-        for tag, bars in markers.items():
-            f.write(f"MARKER_TAG= {tag}\nMARKER_ELEMS= {len(bars)}\n")
-            for b in bars:
-                f.write(f"3 {b[0]} {b[1]}\n")
-
-
-def su2_markers(zone: dict) -> dict:
-    bars = [s[4].reshape(-1, 2) - 1 for s in zone["sections"][1:]]  # bottom, right, top, left
-    return {"wall": bars[0], "farfield": bars[1], "symmetry": bars[2], "inlet": bars[3]}
 
 
 def test_su2_reader_bitwise_vs_reference_reader(tmp_path, ref_available):
