@@ -207,6 +207,22 @@ ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* a
 /* Kernel launches issued by this context so far (for launch accounting). */
 ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches);
 
+/* No counterpart in the reference. The CFL time step of ndg_get_delta_t,
+ * min over elements of cfl * delta_xy_min / N^2 (bit-identical), computed
+ * from caller-owned device arrays of n_elements values on the current device
+ * and returned in *delta_t (host memory) after the stream has been
+ * synchronised. It allocates no device memory (no cudaMalloc/cudaFree, no
+ * allocating library routine) and needs no context: for callers that manage
+ * all device memory through their own pool, or whose time loop cannot afford
+ * the device-wide synchronisation of cudaMalloc/cudaFree. The partial minima go to one fixed 33 KB scratch array
+ * per device, so n_elements is at most 4,194,304 (NDG_ERR_INVALID_ARG
+ * beyond), and calls that overlap in time on one device race on that array:
+ * serialise them. The first call on each device looks up the array's
+ * address; make it before any stream capture begins. stream is a
+ * cudaStream_t of the current device (NULL: the default stream). */
+ndg_status ndg_delta_t_from_device(const double* delta_xy_min, const int32_t* elem_N, int64_t n_elements,
+                                   double cfl, void* stream, double* delta_t);
+
 #ifdef __cplusplus
 }
 #endif

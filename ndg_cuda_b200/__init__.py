@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
         "ndg_time_stage": ([vp, i32, i32, C.POINTER(dbl)], C.c_int),
         "ndg_estimate_error": ([vp], C.c_int),
         "ndg_get_error": ([vp, i32, vp, vp, vp, vp], C.c_int),
+        "ndg_delta_t_from_device": ([vp, vp, i64, dbl, vp, C.POINTER(dbl)], C.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
@@ -357,6 +358,14 @@ class Solver2D_t:
         _check(lib().ndg_set_cfl(mesh.handle, float(self.CFL_)))
         _check(lib().ndg_solve(mesh.handle, float(self.output_times_[-1]), C.byref(t), C.byref(n)))
         return t.value, n.value
+
+
+def delta_t_from_device(delta_xy_min: int, elem_N: int, n_elements: int, cfl: float, stream: int = 0) -> float:
+    """CFL step from device arrays (float64 delta_xy_min, int32 N per element)
+    given by address, without allocating: ndg_delta_t_from_device."""
+    dt = C.c_double()
+    _check(lib().ndg_delta_t_from_device(delta_xy_min, elem_N, n_elements, cfl, stream or None, C.byref(dt)))
+    return dt.value
 
 
 def dof_count(mesh: Mesh2D_t) -> int:
