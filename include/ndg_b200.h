@@ -199,6 +199,17 @@ ndg_status ndg_estimate_error(ndg_ctx* ctx);
  * tolerance_min), coarsen_ (error < tolerance_max). Any pointer may be NULL. */
 ndg_status ndg_get_error(ndg_ctx* ctx, int32_t instance, double* p_error, double* p_sigma, int32_t* refine, int32_t* coarsen);
 
+/* Mesh2D_t::adapt(N_max, nodes, barycentric_weights) (src/meshes/Mesh2D_t.cpp:1644-2268)
+ * from the last ndg_estimate_error: elements with refine_ and p_sigma_ >= 1
+ * below maximum_N gain 2 orders (p_adapt, :5026) with their solution
+ * interpolated (Element2D_t::interpolate_from, src/entities/Element2D_t.cpp:464-579);
+ * boundary and interface ghosts and faces take their neighbours' orders
+ * (adjust_boundaries, adjust_interfaces, adjust_faces, :7482-7538). Later
+ * steps run the mixed-order (mortar) stage path. Needs one instance.
+ * Element splitting (h-refinement, max_split_level > 0 with p_sigma_ < 1)
+ * returns NDG_ERR_UNSUPPORTED. The estimate is consumed. */
+ndg_status ndg_adapt(ndg_ctx* ctx);
+
 /* Benchmark aid: launches stage m n_launches times back to back (the state
  * advances), timing each launch with CUDA events on the context's stream;
  * *avg_ms = mean kernel duration. */

@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
         "ndg_time_stage": ([vp, i32, i32, C.POINTER(dbl)], C.c_int),
         "ndg_estimate_error": ([vp], C.c_int),
         "ndg_get_error": ([vp, i32, vp, vp, vp, vp], C.c_int),
+        "ndg_adapt": ([vp], C.c_int),
         "ndg_delta_t_from_device": ([vp, vp, i64, dbl, vp, C.POINTER(dbl)], C.c_int),
     }
     for name, (args, res) in sigs.items():
@@ -277,6 +278,16 @@ class Mesh2D_t:
              "coarsen": np.empty(K, dtype=np.int32)}
         _check(lib().ndg_get_error(self._ctx.h, instance, *[_ptr(d[k]) for k in ("p_error", "p_sigma", "refine", "coarsen")]))
         return d
+
+    def adapt(self) -> None:
+        """Mesh2D_t::adapt from the last error estimate (p-refinement)."""
+        _check(lib().ndg_adapt(self._ctx.h))
+        counts = [C.c_int64() for _ in range(4)]
+        _check(lib().ndg_mesh_counts(self._ctx.h, *[C.byref(c) for c in counts]))
+        self.n_elements_, self.n_elements_total_, self.n_faces_, self.n_nodes_ = (c.value for c in counts)
+        fs = C.c_int64()
+        _check(lib().ndg_mesh_field_size(self._ctx.h, C.byref(fs)))
+        self.field_size = fs.value
 
     def synchronize(self) -> None:
         _check(lib().ndg_ctx_synchronize(self._ctx.h))

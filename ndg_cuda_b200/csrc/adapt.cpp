@@ -1,0 +1,186 @@
+// Host side of mixed-order meshes: the device plan of the general stage
+// path, and p-adaptation of the topology with the reference's rules.
+#include "ndg_internal.hpp"
+
+#include <algorithm>
+#include <map>
+
+namespace ndg {
+
+bool fused_path_applies(const Topology& t) {
+    if (t.n_domain <= 0) return false;
+    const int N = t.elem_N[0];
+    for (int Ne : t.elem_N)
+        if (Ne != N) return false;
+    for (int Nf : t.face_N)
+        if (Nf != N) return false;
+    for (int64_t e = 0; e < t.n_domain; ++e) {
+        const auto& nd = t.elem_nodes[static_cast<size_t>(e)];
+        for (int s = 0; s < 4; ++s) {
+            const int64_t f = t.elem_face[static_cast<size_t>(e)][static_cast<size_t>(s)];
+            if (f < 0) return false;
+            const auto& fe = t.face_elems[static_cast<size_t>(f)];
+            const auto& fn = t.face_nodes[static_cast<size_t>(f)];
+            const int64_t a = nd[static_cast<size_t>(s)], b = nd[static_cast<size_t>((s + 1) % 4)];
+            const bool conforming = fe[0] == e ? (fn[0] == a && fn[1] == b) : (fn[0] == b && fn[1] == a);
+            if (!conforming) return false;
+            const int64_t other = fe[0] == e ? fe[1] : fe[0];
+            if (other >= t.n_domain && (t.face_scale[static_cast<size_t>(f)][1] != 1.0 || t.face_offset[static_cast<size_t>(f)][1] != 0.0))
+                return false;
+        }
+    }
+    return true;
+}
+
+GeneralPlan build_general_plan(const Topology& t) {
+    GeneralPlan p;
+    const int64_t K = t.n_domain;
+    const int64_t total = static_cast<int64_t>(t.elem_N.size());
+    const int64_t F = static_cast<int64_t>(t.face_N.size());
+    p.n_domain = K;
+    p.n_total = total;
+    p.n_faces = F;
+    p.eN.assign(t.elem_N.begin(), t.elem_N.end());
+    p.off2.resize(static_cast<size_t>(K));
+    p.off1.resize(static_cast<size_t>(total));
+    int64_t o2 = 0, o1 = 0;
+    for (int64_t e = 0; e < total; ++e) {
+        const int64_t n = t.elem_N[static_cast<size_t>(e)] + 1;
+        if (e < K) {
+            p.off2[static_cast<size_t>(e)] = o2;
+            o2 += n * n;
+            p.off1[static_cast<size_t>(e)] = o1;
+            o1 += 4 * n;
+        } else {
+            p.off1[static_cast<size_t>(e)] = o1;
+            o1 += n;
+        }
+    }
+    p.block = o2 + (o2 & 1);
+    p.trace_total = o1;
+    p.enodes.resize(static_cast<size_t>(4 * total));
+    p.sface_start.assign(static_cast<size_t>(4 * total + 1), 0);
+    for (int64_t e = 0; e < total; ++e) {
+        for (int s = 0; s < 4; ++s) {
+            p.enodes[static_cast<size_t>(4 * e + s)] = t.elem_nodes[static_cast<size_t>(e)][static_cast<size_t>(s)];
+            const int64_t f = t.elem_face[static_cast<size_t>(e)][static_cast<size_t>(s)];
+            const bool has = e < K ? f >= 0 : (s == 0 && f >= 0);
+            p.sface_start[static_cast<size_t>(4 * e + s + 1)] = p.sface_start[static_cast<size_t>(4 * e + s)] + (has ? 1 : 0);
+            if (has) p.sface.push_back(f);
+        }
+    }
+    p.corners.resize(static_cast<size_t>(8 * K));
+    for (int64_t e = 0; e < K; ++e)
+        for (int k = 0; k < 4; ++k) {
+            const size_t nd = static_cast<size_t>(t.elem_nodes[static_cast<size_t>(e)][static_cast<size_t>(k)]);
+            p.corners[static_cast<size_t>(8 * e + 2 * k)] = t.node_x[nd];
+            p.corners[static_cast<size_t>(8 * e + 2 * k + 1)] = t.node_y[nd];
+        }
+    p.node_xy.resize(2 * t.node_x.size());
+    for (size_t i = 0; i < t.node_x.size(); ++i) {
+        p.node_xy[2 * i] = t.node_x[i];
+        p.node_xy[2 * i + 1] = t.node_y[i];
+    }
+    p.fN.assign(t.face_N.begin(), t.face_N.end());
+    p.foff.resize(static_cast<size_t>(F));
+    int64_t of = 0;
+    for (int64_t f = 0; f < F; ++f) {
+        p.foff[static_cast<size_t>(f)] = of;
+        of += t.face_N[static_cast<size_t>(f)] + 1;
+    }
+    p.face_total = of;
+    auto put2 = [F](const auto& src, auto& dst) {
+        dst.resize(static_cast<size_t>(2 * F));
+        for (int64_t f = 0; f < F; ++f) {
+            dst[static_cast<size_t>(2 * f)] = src[static_cast<size_t>(f)][0];
+            dst[static_cast<size_t>(2 * f + 1)] = src[static_cast<size_t>(f)][1];
+        }
+    };
+    put2(t.face_nodes, p.fnodes);
+    put2(t.face_elems, p.felem);
+    put2(t.face_sides, p.fside);
+    put2(t.face_normal, p.fnormal);
+    put2(t.face_tangent, p.ftangent);
+    put2(t.face_offset, p.foffset);
+    put2(t.face_scale, p.fscale);
+
+    // What fills each ghost's side-0 trace (Mesh2D_t::boundary_conditions
+    // runs walls, symmetry, inflow, outflow, then interfaces: last writer wins).
+    const int64_t G = total - K;
+    p.gkind.assign(static_cast<size_t>(G), 4);
+    p.gscale.assign(static_cast<size_t>(G), 0.0);
+    p.gsrc.assign(static_cast<size_t>(G), 0);
+    p.gsrc_side.assign(static_cast<size_t>(G), 0);
+    const int kinds[4] = {0, 0, 1, 2};  // wall, symmetry: mirror; inflow: analytic; outflow: copy
+    for (int b = 0; b < 4; ++b)
+        for (int64_t g : t.boundary[static_cast<size_t>(b)]) p.gkind[static_cast<size_t>(g - K)] = kinds[b];
+    for (size_t i = 0; i < t.if_destination.size(); ++i) {
+        const size_t g = static_cast<size_t>(t.if_destination[i] - K);
+        p.gkind[g] = 3;
+        p.gsrc[g] = t.if_origin[i];
+        p.gsrc_side[g] = static_cast<int32_t>(t.if_origin_side[i]);
+    }
+    for (int64_t g = K; g < total; ++g) p.gscale[static_cast<size_t>(g - K)] = t.ghost_scale[static_cast<size_t>(g)][0];
+
+    std::map<int, std::vector<int64_t>> by_order;
+    for (int64_t e = 0; e < K; ++e) by_order[t.elem_N[static_cast<size_t>(e)]].push_back(e);
+    for (auto& kv : by_order) p.groups.emplace_back(kv.first, std::move(kv.second));
+    return p;
+}
+
+// Mesh2D_t::adapt when no element splits (src/meshes/Mesh2D_t.cpp:1644-1700):
+// p_adapt (:5026-5049; Element2D_t::would_p_refine, Element2D_t.cpp:802-806),
+// then adjust_boundaries for walls, symmetry, inflow and outflow
+// (:7482-7504), adjust_interfaces (:7506-7520) and adjust_faces (:7522-7538).
+// A ghost whose order changes gets new, zeroed boundary storage in the
+// reference (Element2D_t::resize_boundary_storage, Element2D_t.cpp:735-741),
+// scaling factor included; that is kept.
+bool p_adapt(Topology& t, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level) {
+    const int64_t K = t.n_domain;
+    for (int64_t e = 0; e < K; ++e) {
+        const bool h = refine[e] && p_sigma[e] < 1.0 && 0 < max_split_level;
+        if (h) fail(NDG_ERR_UNSUPPORTED, "h-adaptation (element splitting) is not available yet; set max_split_level to 0");
+    }
+    bool changed = false;
+    for (int64_t e = 0; e < K; ++e) {
+        int& N = t.elem_N[static_cast<size_t>(e)];
+        if (refine[e] && p_sigma[e] >= 1.0 && N + 2 <= N_max) {
+            N += 2;
+            changed = true;
+        }
+    }
+    for (int b = 0; b < 4; ++b)
+        for (int64_t g : t.boundary[static_cast<size_t>(b)]) {
+            int N_el = t.elem_N[static_cast<size_t>(g)];
+            const int64_t f = t.elem_face[static_cast<size_t>(g)][0];
+            if (f >= 0) {
+                const auto& fe = t.face_elems[static_cast<size_t>(f)];
+                const int64_t src = fe[fe[0] == g ? 1 : 0];
+                N_el = std::max(N_el, t.elem_N[static_cast<size_t>(src)]);
+            }
+            if (t.elem_N[static_cast<size_t>(g)] != N_el) {
+                t.elem_N[static_cast<size_t>(g)] = N_el;
+                t.ghost_scale[static_cast<size_t>(g)][0] = 0.0;
+                changed = true;
+            }
+        }
+    for (size_t i = 0; i < t.if_origin.size(); ++i) {
+        const int Ns = t.elem_N[static_cast<size_t>(t.if_origin[i])];
+        int& Nd = t.elem_N[static_cast<size_t>(t.if_destination[i])];
+        if (Nd != Ns) {
+            Nd = Ns;
+            t.ghost_scale[static_cast<size_t>(t.if_destination[i])][0] = 0.0;
+            changed = true;
+        }
+    }
+    for (size_t f = 0; f < t.face_N.size(); ++f) {
+        const int Nf = std::max(t.elem_N[static_cast<size_t>(t.face_elems[f][0])], t.elem_N[static_cast<size_t>(t.face_elems[f][1])]);
+        if (t.face_N[f] != Nf) {
+            t.face_N[f] = Nf;
+            changed = true;
+        }
+    }
+    return changed;
+}
+
+}  // namespace ndg

@@ -3,10 +3,12 @@
 // stage_kernels.cu.
 #include "ndg_internal.hpp"
 #include "estimator.cuh"
+#include "general_kernels.cuh"
 #include "stage_kernels.cuh"
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -38,6 +40,17 @@ template <typename T>
 struct DeviceBuffer {
     T* ptr = nullptr;
     size_t count = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    void swap(DeviceBuffer& o) noexcept {
+        std::swap(ptr, o.ptr);
+        std::swap(count, o.count);
+    }
+    void upload(const std::vector<T>& v, cudaStream_t stream) {
+        allocate(std::max<size_t>(v.size(), 1));
+        if (!v.empty()) check_cuda(cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "mesh upload");
+    }
     void allocate(size_t n) {
         release();
         if (n == 0) return;
@@ -89,6 +102,15 @@ struct ndg_ctx {
     int cur = 0;
     bool traces_valid = false;
     double dt_mesh = 0.0;
+
+    // Mixed-order meshes (after adaptation) run the general stage path.
+    bool general = false;
+    ndg::GeneralPlan gplan;
+    ndg::DeviceBuffer<int32_t> g_eN, g_fN, g_gkind, g_gsrc_side;
+    ndg::DeviceBuffer<int64_t> g_off2, g_off1, g_enodes, g_sface_start, g_sface, g_foff, g_fnodes, g_felem, g_fside, g_gsrc, g_ids;
+    ndg::DeviceBuffer<double> g_corners, g_node_xy, g_fnormal, g_ftangent, g_foffset, g_fscale, g_gscale, etr, ffl;
+    std::vector<ndg::dev::OrderGroup> groups;
+    ndg::dev::GeneralMesh gmesh;
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t launches = 0;
@@ -161,15 +183,47 @@ dev::StageArgs stage_args(ndg_ctx* c, int m, int in) {
     return a;
 }
 
+dev::GeneralStage general_args(ndg_ctx* c, int m) {
+    dev::GeneralStage a{};
+    a.m = c->gmesh;
+    a.q = c->q.ptr;
+    a.k = c->k.ptr;
+    a.G_out = c->keep_derivative ? c->G.ptr : nullptr;
+    a.etr = c->etr.ptr;
+    a.ffl = c->ffl.ptr;
+    a.step = c->step.ptr;
+    a.rk_a = kRkA[m];
+    a.rk_b = kRkB[m];
+    a.rk_g = kRkG[m];
+    a.first = m == 0;
+    a.n_instances = c->n_instances;
+    return a;
+}
+
+// Kernel launches of one stage of the general path: side traces and volume
+// per order group, ghost traces, face fluxes.
+int64_t general_stage_launches(const ndg_ctx* c) {
+    const int64_t ghosts = c->gmesh.n_total > c->gmesh.n_domain ? 1 : 0;
+    return 2 * static_cast<int64_t>(c->groups.size()) + ghosts + 1;
+}
+
+cudaError_t issue_stage(ndg_ctx* c, int m, int in) {
+    if (c->general) return dev::launch_general_stage(general_args(c, m), c->groups.data(), static_cast<int>(c->groups.size()), strict(c), c->stream);
+    return dev::launch_stage(c->N, strict(c), stage_args(c, m, in), c->stream);
+}
+
 void launch_stage(ndg_ctx* c, int m) {
-    const dev::StageArgs a = stage_args(c, m, c->cur);
-    check_cuda(dev::launch_stage(c->N, strict(c), a, c->stream), "stage kernel launch");
-    c->cur = 1 - c->cur;
-    ++c->launches;
+    check_cuda(issue_stage(c, m, c->cur), "stage kernel launch");
+    if (c->general) {
+        c->launches += general_stage_launches(c);
+    } else {
+        c->cur = 1 - c->cur;
+        ++c->launches;
+    }
 }
 
 void ensure_traces(ndg_ctx* c) {
-    if (c->traces_valid) return;
+    if (c->traces_valid || c->general) return;
     dev::TraceArgs a{c->q.ptr, c->tr[c->cur].ptr, c->K, c->Kp, c->n_instances};
     check_cuda(dev::launch_traces(c->N, strict(c), a, c->stream), "trace kernel launch");
     ++c->launches;
@@ -182,18 +236,17 @@ void set_step(ndg_ctx* c, double time, double dt, double t_end) {
     check_cuda(cudaStreamSynchronize(c->stream), "step upload");
 }
 
-// One RK3 step as a CUDA graph: three stage kernels and the time update,
-// for each parity of the trace double buffer.
+// One RK3 step as a CUDA graph: the three stages and the time update. The
+// uniform path alternates two trace buffers, so it has one graph per parity;
+// the general path has one.
 void ensure_graphs(ndg_ctx* c) {
-    if (c->graph[0] && c->graph[1]) return;
-    for (int parity = 0; parity < 2; ++parity) {
+    const int n_graphs = c->general ? 1 : 2;
+    if (c->graph[0] && (n_graphs == 1 || c->graph[1])) return;
+    for (int parity = 0; parity < n_graphs; ++parity) {
         cudaGraph_t g = nullptr;
         check_cuda(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
         cudaError_t err = cudaSuccess;
-        for (int m = 0; m < 3 && err == cudaSuccess; ++m) {
-            const dev::StageArgs a = stage_args(c, m, (parity + m) & 1);
-            err = dev::launch_stage(c->N, strict(c), a, c->stream);
-        }
+        for (int m = 0; m < 3 && err == cudaSuccess; ++m) err = issue_stage(c, m, (parity + m) & 1);
         if (err == cudaSuccess) err = dev::launch_end_step(c->step.ptr, c->stream);
         cudaError_t end = cudaStreamEndCapture(c->stream, &g);
         check_cuda(err, "graph capture launch");
@@ -210,9 +263,14 @@ void run_steps(ndg_ctx* c, int64_t n_steps) {
     ensure_traces(c);
     ensure_graphs(c);
     for (int64_t s = 0; s < n_steps; ++s) {
-        check_cuda(cudaGraphLaunch(c->graph[c->cur], c->stream), "graph launch");
-        c->cur = 1 - c->cur;  // three stages flip the trace buffer an odd number of times
-        c->launches += 4;
+        if (c->general) {
+            check_cuda(cudaGraphLaunch(c->graph[0], c->stream), "graph launch");
+            c->launches += 3 * general_stage_launches(c) + 1;
+        } else {
+            check_cuda(cudaGraphLaunch(c->graph[c->cur], c->stream), "graph launch");
+            c->cur = 1 - c->cur;  // three stages flip the trace buffer an odd number of times
+            c->launches += 4;
+        }
     }
 }
 
@@ -236,6 +294,157 @@ void compute_dt_mesh(ndg_ctx* c, double cfl) {
     c->params.cfl = cfl;
 }
 
+// Field layout of a topology: per domain element its order and first
+// value within a field block, the block size and the values per field seen
+// through the API. The uniform path pads the element count to even.
+struct Layout {
+    bool general = false;
+    int64_t block = 0, field_size = 0;
+    std::vector<int32_t> N;
+    std::vector<int64_t> off2;
+};
+
+Layout layout_of(const Topology& t) {
+    Layout l;
+    l.general = !fused_path_applies(t);
+    const int64_t K = t.n_domain;
+    l.N.assign(t.elem_N.begin(), t.elem_N.begin() + static_cast<std::ptrdiff_t>(K));
+    l.off2.resize(static_cast<size_t>(K));
+    int64_t o = 0;
+    for (int64_t e = 0; e < K; ++e) {
+        l.off2[static_cast<size_t>(e)] = o;
+        o += static_cast<int64_t>(l.N[static_cast<size_t>(e)] + 1) * (l.N[static_cast<size_t>(e)] + 1);
+    }
+    l.field_size = o;
+    if (l.general) {
+        l.block = o + (o & 1);
+    } else {
+        const int64_t NN = static_cast<int64_t>(l.N[0] + 1) * (l.N[0] + 1);
+        l.block = (K + (K & 1)) * NN;
+    }
+    return l;
+}
+
+// Uploads what the stage kernels of the current topology read: the side
+// plan of the uniform path or the arrays of the general path.
+void upload_plan(ndg_ctx* c, const Layout& l) {
+    const size_t inst = static_cast<size_t>(c->n_instances);
+    c->general = l.general;
+    c->block = l.block;
+    c->field_size = l.field_size;
+    c->K = c->topo.n_domain;
+    c->Kp = c->K + (c->K & 1);
+    c->N = *std::max_element(l.N.begin(), l.N.end());
+    const size_t K = static_cast<size_t>(c->K);
+    if (!l.general) {
+        if (c->N > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "orders above 16 have no compiled kernel");
+        const SidePlan plan = build_side_plan(c->topo, c->tables);
+        const size_t n = static_cast<size_t>(c->N + 1);
+        c->tr[0].allocate(inst * 3 * static_cast<size_t>(c->Kp) * 4 * n);
+        c->tr[1].allocate(inst * 3 * static_cast<size_t>(c->Kp) * 4 * n);
+        check_cuda(cudaMemsetAsync(c->tr[0].ptr, 0, c->tr[0].count * sizeof(double), c->stream), "memset");
+        check_cuda(cudaMemsetAsync(c->tr[1].ptr, 0, c->tr[1].count * sizeof(double), c->stream), "memset");
+        c->corners.upload(plan.corners, c->stream);
+        c->normal.upload(plan.normal, c->stream);
+        c->gscale.upload(plan.gscale, c->stream);
+        c->inflow.upload(plan.inflow_xy, c->stream);
+        c->link.upload(plan.link, c->stream);
+        check_cuda(dev::prepare_kernels(c->N, false), "kernel attributes");
+        check_cuda(dev::prepare_kernels(c->N, true), "kernel attributes");
+        c->groups.clear();
+    } else {
+        for (int Ne : c->topo.elem_N)
+            if (Ne < 1 || Ne > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "element orders must lie in 1..16");
+        c->tr[0].release();
+        c->tr[1].release();
+        c->gplan = build_general_plan(c->topo);
+        const GeneralPlan& g = c->gplan;
+        c->g_eN.upload(g.eN, c->stream);
+        c->g_off2.upload(g.off2, c->stream);
+        c->g_off1.upload(g.off1, c->stream);
+        c->g_enodes.upload(g.enodes, c->stream);
+        c->g_sface_start.upload(g.sface_start, c->stream);
+        c->g_sface.upload(g.sface, c->stream);
+        c->g_corners.upload(g.corners, c->stream);
+        c->g_node_xy.upload(g.node_xy, c->stream);
+        c->g_fN.upload(g.fN, c->stream);
+        c->g_foff.upload(g.foff, c->stream);
+        c->g_fnodes.upload(g.fnodes, c->stream);
+        c->g_felem.upload(g.felem, c->stream);
+        c->g_fside.upload(g.fside, c->stream);
+        c->g_fnormal.upload(g.fnormal, c->stream);
+        c->g_ftangent.upload(g.ftangent, c->stream);
+        c->g_foffset.upload(g.foffset, c->stream);
+        c->g_fscale.upload(g.fscale, c->stream);
+        c->g_gkind.upload(g.gkind, c->stream);
+        c->g_gscale.upload(g.gscale, c->stream);
+        c->g_gsrc.upload(g.gsrc, c->stream);
+        c->g_gsrc_side.upload(g.gsrc_side, c->stream);
+        std::vector<int64_t> ids;
+        for (const auto& grp : g.groups) ids.insert(ids.end(), grp.second.begin(), grp.second.end());
+        c->g_ids.upload(ids, c->stream);
+        c->groups.clear();
+        int64_t at = 0;
+        for (const auto& grp : g.groups) {
+            dev::OrderGroup og;
+            og.N = grp.first;
+            og.count = static_cast<int64_t>(grp.second.size());
+            og.ids = c->g_ids.ptr + at;
+            at += og.count;
+            c->groups.push_back(og);
+            check_cuda(dev::prepare_general_kernels(og.N), "kernel attributes");
+        }
+        c->etr.allocate(inst * 3 * static_cast<size_t>(g.trace_total));
+        c->ffl.allocate(inst * 3 * static_cast<size_t>(std::max<int64_t>(g.face_total, 1)));
+        dev::GeneralMesh& M = c->gmesh;
+        M = dev::GeneralMesh{};
+        M.n_domain = g.n_domain;
+        M.n_total = g.n_total;
+        M.n_faces = g.n_faces;
+        M.trace_total = g.trace_total;
+        M.face_total = g.face_total;
+        M.block = g.block;
+        M.max_n = 1;
+        for (int Ne : g.eN) M.max_n = std::max(M.max_n, Ne + 1);
+        for (int Nf : g.fN) M.max_n = std::max(M.max_n, Nf + 1);
+        M.eN = c->g_eN.ptr;
+        M.off2 = c->g_off2.ptr;
+        M.off1 = c->g_off1.ptr;
+        M.enodes = c->g_enodes.ptr;
+        M.sface_start = c->g_sface_start.ptr;
+        M.sface = c->g_sface.ptr;
+        M.corners = c->g_corners.ptr;
+        M.node_xy = c->g_node_xy.ptr;
+        M.fN = c->g_fN.ptr;
+        M.foff = c->g_foff.ptr;
+        M.fnodes = c->g_fnodes.ptr;
+        M.felem = c->g_felem.ptr;
+        M.fside = c->g_fside.ptr;
+        M.fnormal = c->g_fnormal.ptr;
+        M.ftangent = c->g_ftangent.ptr;
+        M.foffset = c->g_foffset.ptr;
+        M.fscale = c->g_fscale.ptr;
+        M.gkind = c->g_gkind.ptr;
+        M.gscale = c->g_gscale.ptr;
+        M.gsrc = c->g_gsrc.ptr;
+        M.gsrc_side = c->g_gsrc_side.ptr;
+        // The uniform-path corners also serve the initial condition of a
+        // general mesh.
+        c->corners.upload(g.corners, c->stream);
+    }
+    std::vector<double> dxy(c->topo.delta_xy_min.begin(), c->topo.delta_xy_min.begin() + static_cast<std::ptrdiff_t>(K));
+    c->dxy.upload(dxy, c->stream);
+    c->elem_N.upload(l.N, c->stream);
+    c->p_error.allocate(inst * K);
+    c->p_sigma.allocate(inst * K);
+    c->refine.allocate(inst * K);
+    c->coarsen.allocate(inst * K);
+    c->has_error_estimate = false;
+    c->traces_valid = false;
+    c->cur = 0;
+    drop_graphs(c);
+}
+
 void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_instances) {
     if (n_instances < 1) fail(NDG_ERR_INVALID_ARG, "n_instances must be >= 1");
     if (p.initial_N < 1 || p.initial_N > p.maximum_N) fail(NDG_ERR_INVALID_ARG, "need 1 <= initial_N <= maximum_N");
@@ -245,6 +454,7 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
         c->has_tables = true;
         if (c->device >= 0) {
             check_cuda(dev::upload_tables(c->tables), "table upload");
+            check_cuda(dev::upload_general_tables(c->tables), "table upload");
             check_cuda(dev::upload_polynomials(c->tables), "table upload");
         }
     }
@@ -252,62 +462,29 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     c->topo = std::move(topo);
     c->params = p;
     c->n_instances = n_instances;
+    const Layout l = layout_of(c->topo);
     c->N = p.initial_N;
     c->K = c->topo.n_domain;
-    c->field_size = c->K * (c->N + 1) * (c->N + 1);
+    c->field_size = l.field_size;
     c->Kp = c->K + (c->K & 1);
-    c->block = c->Kp * (c->N + 1) * (c->N + 1);
+    c->block = l.block;
     c->has_mesh = true;
     c->traces_valid = false;
     c->cur = 0;
     drop_graphs(c);
     if (c->device < 0) return;
 
-    if (c->N > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "orders above 16 have no compiled kernel");
-    const SidePlan plan = build_side_plan(c->topo, c->tables);
-    const size_t per_field = static_cast<size_t>(c->block);
-    const size_t n = static_cast<size_t>(c->N + 1);
-    const size_t K = static_cast<size_t>(c->K);
     const size_t inst = static_cast<size_t>(n_instances);
-    c->q.allocate(inst * 3 * per_field);
-    c->k.allocate(inst * 3 * per_field);
+    c->q.allocate(inst * 3 * static_cast<size_t>(l.block));
+    c->k.allocate(inst * 3 * static_cast<size_t>(l.block));
     c->G.release();
-    if (c->keep_derivative) c->G.allocate(inst * 3 * per_field);
-    const size_t Kp = static_cast<size_t>(c->Kp);
-    c->tr[0].allocate(inst * 3 * Kp * 4 * n);
-    c->tr[1].allocate(inst * 3 * Kp * 4 * n);
+    if (c->keep_derivative) c->G.allocate(inst * 3 * static_cast<size_t>(l.block));
     c->error.allocate(1);
-    c->p_error.allocate(inst * K);
-    c->p_sigma.allocate(inst * K);
-    c->refine.allocate(inst * K);
-    c->coarsen.allocate(inst * K);
-    c->has_error_estimate = false;
-    c->corners.allocate(plan.corners.size());
-    c->normal.allocate(plan.normal.size());
-    c->gscale.allocate(plan.gscale.size());
-    c->inflow.allocate(plan.inflow_xy.size());
-    c->link.allocate(plan.link.size());
-    c->dxy.allocate(K);
-    c->elem_N.allocate(K);
     c->step.allocate(4);
-    auto up = [&](void* dst, const void* src, size_t bytes) {
-        check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream), "mesh upload");
-    };
-    up(c->corners.ptr, plan.corners.data(), plan.corners.size() * sizeof(double));
-    up(c->normal.ptr, plan.normal.data(), plan.normal.size() * sizeof(double));
-    up(c->gscale.ptr, plan.gscale.data(), plan.gscale.size() * sizeof(double));
-    up(c->inflow.ptr, plan.inflow_xy.data(), plan.inflow_xy.size() * sizeof(double));
-    up(c->link.ptr, plan.link.data(), plan.link.size() * sizeof(int32_t));
-    up(c->dxy.ptr, c->topo.delta_xy_min.data(), K * sizeof(double));
-    std::vector<int32_t> eN(c->topo.elem_N.begin(), c->topo.elem_N.begin() + static_cast<std::ptrdiff_t>(K));
-    up(c->elem_N.ptr, eN.data(), K * sizeof(int32_t));
     check_cuda(cudaMemsetAsync(c->q.ptr, 0, c->q.count * sizeof(double), c->stream), "memset");
     check_cuda(cudaMemsetAsync(c->k.ptr, 0, c->k.count * sizeof(double), c->stream), "memset");
-    check_cuda(cudaMemsetAsync(c->tr[0].ptr, 0, c->tr[0].count * sizeof(double), c->stream), "memset");
-    check_cuda(cudaMemsetAsync(c->tr[1].ptr, 0, c->tr[1].count * sizeof(double), c->stream), "memset");
     check_cuda(cudaMemsetAsync(c->error.ptr, 0, sizeof(unsigned), c->stream), "memset");
-    check_cuda(dev::prepare_kernels(c->N, false), "kernel attributes");
-    check_cuda(dev::prepare_kernels(c->N, true), "kernel attributes");
+    upload_plan(c, l);
     compute_dt_mesh(c, p.cfl);
 }
 
@@ -562,8 +739,15 @@ ndg_status ndg_initial_conditions(ndg_ctx* ctx) {
         require_mesh(ctx);
         require_device(ctx);
         make_current(ctx);
-        check_cuda(dev::launch_initial_conditions(ctx->q.ptr, ctx->k.ptr, ctx->corners.ptr, ctx->N, ctx->K, ctx->Kp, ctx->n_instances, ctx->stream), "initial condition kernel");
-        ++ctx->launches;
+        if (ctx->general) {
+            check_cuda(dev::launch_general_initial_conditions(general_args(ctx, 0), ctx->groups.data(), static_cast<int>(ctx->groups.size()), ctx->stream),
+                       "initial condition kernel");
+            ctx->launches += static_cast<int64_t>(ctx->groups.size());
+        } else {
+            check_cuda(dev::launch_initial_conditions(ctx->q.ptr, ctx->k.ptr, ctx->corners.ptr, ctx->N, ctx->K, ctx->Kp, ctx->n_instances, ctx->stream),
+                       "initial condition kernel");
+            ++ctx->launches;
+        }
         if (ctx->keep_derivative) check_cuda(cudaMemsetAsync(ctx->G.ptr, 0, ctx->G.count * sizeof(double), ctx->stream), "memset");
         ctx->traces_valid = false;
     });
@@ -720,11 +904,23 @@ ndg_status ndg_estimate_error(ndg_ctx* ctx) {
         a.tolerance_min = ctx->params.tolerance_min;
         a.tolerance_max = ctx->params.tolerance_max;
         a.n_elements = ctx->K;
-        a.field_stride = ctx->Kp;
+        a.block = ctx->block;
         a.n_instances = ctx->n_instances;
-        a.N = ctx->N;
-        check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
-        ++ctx->launches;
+        if (ctx->general) {
+            a.off2 = ctx->g_off2.ptr;
+            for (const auto& g : ctx->groups) {
+                a.N = g.N;
+                a.count = g.count;
+                a.ids = g.ids;
+                check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
+                ++ctx->launches;
+            }
+        } else {
+            a.N = ctx->N;
+            a.count = ctx->K;
+            check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
+            ++ctx->launches;
+        }
         ctx->has_error_estimate = true;
     });
 }
@@ -743,6 +939,77 @@ ndg_status ndg_get_error(ndg_ctx* ctx, int32_t instance, double* p_error, double
         if (refine) check_cuda(cudaMemcpyAsync(refine, ctx->refine.ptr + off, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "error download");
         if (coarsen) check_cuda(cudaMemcpyAsync(coarsen, ctx->coarsen.ptr + off, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "error download");
         check_cuda(cudaStreamSynchronize(ctx->stream), "error download");
+    });
+}
+
+ndg_status ndg_adapt(ndg_ctx* ctx) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (!ctx->has_error_estimate) fail(NDG_ERR_INVALID_ARG, "call ndg_estimate_error first");
+        if (ctx->n_instances != 1) fail(NDG_ERR_UNSUPPORTED, "adaptation needs a single instance (the mesh is shared)");
+        make_current(ctx);
+        const size_t K = static_cast<size_t>(ctx->K);
+        std::vector<int32_t> refine(K);
+        std::vector<double> sigma(K);
+        check_cuda(cudaMemcpyAsync(refine.data(), ctx->refine.ptr, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
+        check_cuda(cudaMemcpyAsync(sigma.data(), ctx->p_sigma.ptr, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
+        check_cuda(cudaStreamSynchronize(ctx->stream), "flag download");
+        const Layout before = layout_of(ctx->topo);
+        Topology topo = ctx->topo;
+        if (!p_adapt(topo, refine.data(), sigma.data(), ctx->params.maximum_N, ctx->params.max_split_level)) {
+            ctx->has_error_estimate = false;
+            return;
+        }
+        const Layout after = layout_of(topo);
+        // Transfer the fields to the new orders (same element points), then
+        // switch the topology and the device plan.
+        DeviceBuffer<int32_t> oN, nN;
+        DeviceBuffer<int64_t> oOff, nOff;
+        oN.upload(before.N, ctx->stream);
+        nN.upload(after.N, ctx->stream);
+        oOff.upload(before.off2, ctx->stream);
+        nOff.upload(after.off2, ctx->stream);
+        dev::Transfer t{};
+        t.old_block = before.block;
+        t.new_block = after.block;
+        t.n_fields = 3;
+        t.n_instances = ctx->n_instances;
+        t.n_elements = ctx->K;
+        t.old_N = oN.ptr;
+        t.new_N = nN.ptr;
+        t.old_off2 = oOff.ptr;
+        t.new_off2 = nOff.ptr;
+        const size_t values = static_cast<size_t>(ctx->n_instances) * 3 * static_cast<size_t>(after.block);
+        DeviceBuffer<double> q2, k2, G2;
+        q2.allocate(values);
+        k2.allocate(values);
+        check_cuda(cudaMemsetAsync(q2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
+        check_cuda(cudaMemsetAsync(k2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
+        t.src = ctx->q.ptr;
+        t.dst = q2.ptr;
+        check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
+        t.src = ctx->k.ptr;
+        t.dst = k2.ptr;
+        t.zero_changed = 1;
+        check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
+        ctx->launches += 2;
+        if (ctx->keep_derivative) {
+            G2.allocate(values);
+            check_cuda(cudaMemsetAsync(G2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
+            t.src = ctx->G.ptr;
+            t.dst = G2.ptr;
+            t.zero_changed = 0;
+            check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
+            ++ctx->launches;
+        }
+        check_cuda(cudaStreamSynchronize(ctx->stream), "transfer");
+        ctx->q.swap(q2);
+        ctx->k.swap(k2);
+        if (ctx->keep_derivative) ctx->G.swap(G2);
+        ctx->topo = std::move(topo);
+        upload_plan(ctx, after);
+        compute_dt_mesh(ctx, ctx->params.cfl);
     });
 }
 

@@ -39,13 +39,15 @@ __constant__ double c_poly[kPolyTotal];
 
 __global__ void estimate_error_kernel(EstimatorArgs a) {
     const int N = a.N, n = N + 1, NN = n * n;
-    const int64_t total = a.n_elements * a.n_instances;
+    const int64_t total = a.count * a.n_instances;
     const double* poly = c_poly + poly_offset(N);
     const int npl = (N + 1 < 4) ? N + 1 : 4;  // n_points_least_squares_max (include/helpers/constants.h:19)
     for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total; idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t inst = idx / a.n_elements;
-        const int64_t e = idx - inst * a.n_elements;
-        const double* P = a.q + inst * 3 * a.field_stride * NN + e * NN;
+        const int64_t inst = idx / a.count;
+        const int64_t le = idx - inst * a.count;
+        const int64_t e = a.ids ? a.ids[le] : le;
+        const double* P = a.q + inst * 3 * a.block + (a.off2 ? a.off2[e] : e * NN);
+        const int64_t out = inst * a.n_elements + e;
         double spectrum[4];
         for (int ni = 0; ni < npl; ++ni) {
             const int p = N + ni + 1 - npl;
@@ -85,10 +87,10 @@ __global__ void estimate_error_kernel(EstimatorArgs a) {
         const double tail = __dmul_rn(__ddiv_rn(__dmul_rn(__dmul_rn(C, C), 0.5), sigma), exp(__dmul_rn(__dmul_rn(-2.0, sigma), static_cast<double>(N + 1))));
         const double last = spectrum[npl - 1];
         const double err = __dsqrt_rn(__dadd_rn(__dmul_rn(last, last), tail));
-        a.p_error[idx] = err;
-        a.p_sigma[idx] = sigma;
-        a.refine[idx] = err > a.tolerance_min ? 1 : 0;
-        a.coarsen[idx] = err < a.tolerance_max ? 1 : 0;
+        a.p_error[out] = err;
+        a.p_sigma[out] = sigma;
+        a.refine[out] = err > a.tolerance_min ? 1 : 0;
+        a.coarsen[out] = err < a.tolerance_max ? 1 : 0;
     }
 }
 
@@ -103,7 +105,8 @@ cudaError_t upload_polynomials(const Tables& t) {
 
 cudaError_t launch_estimate_error(const EstimatorArgs& a, cudaStream_t stream) {
     if (a.N < 0 || a.N > kMaxPoly) return cudaErrorInvalidValue;
-    const int64_t total = a.n_elements * a.n_instances;
+    const int64_t total = a.count * a.n_instances;
+    if (total == 0) return cudaSuccess;
     const int blocks = static_cast<int>(std::min<int64_t>((total + 127) / 128, 148 * 16));
     estimate_error_kernel<<<blocks, 128, 0, stream>>>(a);
     return cudaGetLastError();

@@ -8,8 +8,10 @@
 namespace ndg {
 namespace dev {
 
-// Layouts: q as in StageArgs ([instance][field][field_stride][(N+1)^2]);
-// outputs [instance][element].
+// One launch covers `count` elements of order N. q: [instance][field][block]
+// with element e at off2[e] (e (N+1)^2 when off2 is null); outputs
+// [instance][n_elements] at the element numbers ids[] (0 .. count-1 when
+// ids is null).
 struct EstimatorArgs {
     const double* q;
     double* p_error;
@@ -18,8 +20,11 @@ struct EstimatorArgs {
     int* coarsen;
     double tolerance_min;
     double tolerance_max;
+    int64_t count;
     int64_t n_elements;
-    int64_t field_stride;
+    int64_t block;
+    const int64_t* ids;
+    const int64_t* off2;
     int n_instances;
     int N;
 };

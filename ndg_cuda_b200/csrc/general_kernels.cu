@@ -1,0 +1,758 @@
+// Stage kernels for mixed-order meshes with nonconforming faces (sm_100a).
+//
+// After adaptation elements differ in order and faces carry mortar offsets
+// and scales, so the stage runs in the reference's own steps
+// (include/solvers/Solver2D_t.tcu:46-70), each a kernel over device arrays:
+//
+//   side traces    every domain element side, order-templated per group
+//                  (Element2D_t::interpolate_to_boundaries, Element2D_t.cpp:86-125)
+//   ghost traces   walls, symmetry planes, outflow: the neighbours' traces
+//                  projected onto the ghost; inflow: the plane wave; periodic
+//                  interfaces: the origin's side trace
+//                  (Mesh2D_t.cpp:4298-4730)
+//   face fluxes    both traces brought to the face order (copy when conforming,
+//                  barycentric interpolation otherwise), then the upwind flux
+//                  (Mesh2D_t.cpp:3803-3893, Solver2D_t.cpp:48-63)
+//   volume         per order group: the element's side fluxes gathered from
+//                  its faces (mortar projection, Mesh2D_t.cpp:3895-4006), the
+//                  derivative (Solver2D_t.cpp:66-136) and the RK3 update
+//                  (Solver2D_t.cpp:138-172), one CTA per tile of elements
+//
+// STRICT instantiations round every operation in the reference's order and
+// reproduce its CPU results bit for bit; node matching (almost_equal) is
+// always evaluated exactly as the reference does, since it is a decision.
+#include "general_kernels.cuh"
+#include "stage_common.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <vector>
+
+namespace ndg {
+namespace dev {
+
+namespace {
+
+constexpr int kGVecTotal = (kMaxOrder + 1) * (kMaxOrder + 2) / 2;
+constexpr int kGMatTotal = (kMaxOrder + 1) * (kMaxOrder + 2) * (2 * kMaxOrder + 3) / 6;
+__host__ __device__ constexpr int gvec(int N) { return N * (N + 1) / 2; }
+__host__ __device__ constexpr int gmat(int N) { return N * (N + 1) * (2 * N + 1) / 6; }
+
+__constant__ double g_nodes[kGVecTotal];
+__constant__ double g_weights[kGVecTotal];
+__constant__ double g_inv_weights[kGVecTotal];
+__constant__ double g_bary[kGVecTotal];
+__constant__ double g_lagrange_left[kGVecTotal];
+__constant__ double g_lagrange_right[kGVecTotal];
+__constant__ double g_dhat[kGMatTotal];
+
+// Mesh2D_t::almost_equal (src/meshes/Mesh2D_t.cpp:3785-3792): 2 ulp relative,
+// or an absolute difference below DBL_MIN.
+__device__ __forceinline__ bool almost_equal(double x, double y) {
+    const double d = fabs(__dsub_rn(x, y));
+    return d <= __dmul_rn(__dmul_rn(DBL_EPSILON, fabs(__dadd_rn(x, y))), 2.0) || d < DBL_MIN;
+}
+
+// Reference coordinate on an element side of face node coordinate xf:
+// (xf + 1) scale + 2 offset - 1 (Mesh2D_t.cpp:3847, 3954).
+__device__ __forceinline__ double mortar_coord(double xf, double scale, double offset) {
+    return __dsub_rn(__dadd_rn(__dmul_rn(__dadd_rn(xf, 1.0), scale), __dmul_rn(2.0, offset)), 1.0);
+}
+
+// ---------------------------------------------------------------------------
+// Side traces of the domain elements of one order group: thread per
+// (element, side, node), three fields each.
+template <int N, bool S>
+__global__ void __launch_bounds__(256) general_traces_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
+    constexpr int n = N + 1;
+    const double* lm = g_lagrange_left + gvec(N);
+    const double* lp = g_lagrange_right + gvec(N);
+    const int64_t total = count * 4 * n;
+    const int64_t fb = a.m.block, ft = a.m.trace_total;
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total * a.n_instances;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t inst = idx / total;
+        const int64_t r = idx - inst * total;
+        const int64_t le = r / (4 * n);
+        const int sm = static_cast<int>(r - le * 4 * n);
+        const int s = sm / n, m = sm - s * n;
+        const int64_t e = ids[le];
+        const double* l = (s == 0 || s == 3) ? lm : lp;
+        const int line = (s < 2) ? m : N - m;
+        const int base = (s == 0 || s == 2) ? line * n : line;
+        const int stride = (s == 0 || s == 2) ? 1 : n;
+        const double* q = a.q + inst * 3 * fb + a.m.off2[e] + base;
+        double* out = a.etr + inst * 3 * ft + a.m.off1[e] + s * n + m;
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], q[f * fb + j * stride]);
+            out[f * ft] = acc;
+        }
+    }
+}
+
+// Ghost traces: thread per (instance, ghost element).
+template <bool S>
+__global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
+    const GeneralMesh& M = a.m;
+    const int64_t n_ghosts = M.n_total - M.n_domain;
+    const int64_t ft = M.trace_total;
+    const double t = add<S>(a.step[0], mul<S>(a.rk_b, a.step[1]));
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n_ghosts * a.n_instances;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t inst = idx / n_ghosts;
+        const int64_t gi = idx - inst * n_ghosts;
+        const int64_t ge = M.n_domain + gi;
+        const int N = M.eN[ge];
+        const double* xe = g_nodes + gvec(N);
+        double* tr = a.etr + inst * 3 * ft;
+        double* gp = tr + M.off1[ge];
+        double* gu = gp + ft;
+        double* gv = gu + ft;
+        const int kind = M.gkind[gi];
+        if (kind == kGhostMirror || kind == kGhostCopy) {
+            // Mesh2D_t.cpp:4366-4434 (multi-face branch) and 4601-4710.
+            const double* we = g_weights + gvec(N);
+            const double* bwe = g_bary + gvec(N);
+            const double sf = M.gscale[gi];
+            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = 0.0;
+            for (int64_t q = M.sface_start[4 * ge]; q < M.sface_start[4 * ge + 1]; ++q) {
+                const int64_t f = M.sface[q];
+                const int fs = M.felem[2 * f] == ge ? 1 : 0;
+                const int64_t nb = M.felem[2 * f + fs];
+                const int64_t nbs = M.fside[2 * f + fs];
+                const int Nn = M.eN[nb];
+                const double* xnb = g_nodes + gvec(Nn);
+                const double* wnb = g_weights + gvec(Nn);
+                const double* np_ = tr + M.off1[nb] + nbs * (Nn + 1);
+                const double* nu_ = np_ + ft;
+                const double* nv_ = nu_ + ft;
+                const double scale = M.fscale[2 * f + fs], offset = M.foffset[2 * f + fs];
+                for (int j = 0; j <= Nn; ++j) {
+                    const double coord = mortar_coord(xnb[Nn - j], scale, offset);
+                    int found = -1;
+                    for (int i = 0; i <= N; ++i)
+                        if (almost_equal(coord, xe[i])) {
+                            found = i;
+                            break;
+                        }
+                    if (found >= 0) {
+                        const int i = found;
+                        const double w = S ? __ddiv_rn(wnb[j], we[i]) : wnb[j] / we[i];
+                        gp[i] = add<S>(gp[i], mul<S>(mul<S>(w, np_[j]), sf));
+                        gu[i] = add<S>(gu[i], mul<S>(mul<S>(w, nu_[j]), sf));
+                        gv[i] = add<S>(gv[i], mul<S>(mul<S>(w, nv_[j]), sf));
+                    } else {
+                        double s = 0.0;
+                        for (int i = 0; i <= N; ++i) s = add<S>(s, S ? __ddiv_rn(bwe[i], __dsub_rn(coord, xe[i])) : bwe[i] / (coord - xe[i]));
+                        for (int i = 0; i <= N; ++i) {
+                            const double T = S ? __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), s)) : bwe[i] / ((coord - xe[i]) * s);
+                            const double w = S ? __ddiv_rn(__dmul_rn(T, wnb[j]), we[i]) : T * wnb[j] / we[i];
+                            gp[i] = add<S>(gp[i], mul<S>(mul<S>(w, np_[j]), sf));
+                            gu[i] = add<S>(gu[i], mul<S>(mul<S>(w, nu_[j]), sf));
+                            gv[i] = add<S>(gv[i], mul<S>(mul<S>(w, nv_[j]), sf));
+                        }
+                    }
+                }
+            }
+            if (kind == kGhostMirror && M.sface_start[4 * ge + 1] > M.sface_start[4 * ge]) {
+                const int64_t f = M.sface[M.sface_start[4 * ge]];
+                const double nx = M.fnormal[2 * f], ny = M.fnormal[2 * f + 1];
+                const double tx = M.ftangent[2 * f], ty = M.ftangent[2 * f + 1];
+                for (int i = 0; i <= N; ++i) {
+                    const double Vx = gu[i], Vy = gv[i];
+                    const double l0 = -add<S>(mul<S>(Vx, nx), mul<S>(Vy, ny));
+                    const double l1 = add<S>(mul<S>(Vx, tx), mul<S>(Vy, ty));
+                    gu[i] = add<S>(mul<S>(nx, l0), mul<S>(tx, l1));
+                    gv[i] = add<S>(mul<S>(ny, l0), mul<S>(ty, l1));
+                }
+            }
+        } else if (kind == kGhostAnalytic) {
+            // Mesh2D_t.cpp:4575-4599.
+            const int64_t n0 = M.enodes[4 * ge], n1 = M.enodes[4 * ge + 1];
+            const double p0x = M.node_xy[2 * n0], p0y = M.node_xy[2 * n0 + 1];
+            const double p1x = M.node_xy[2 * n1], p1y = M.node_xy[2 * n1 + 1];
+            for (int i = 0; i <= N; ++i) {
+                const double r = __dmul_rn(__dadd_rn(xe[i], 1.0), 0.5);
+                const double gx = __dadd_rn(__dmul_rn(p1x, r), __dmul_rn(p0x, __dsub_rn(1.0, r)));
+                const double gy = __dadd_rn(__dmul_rn(p1y, r), __dmul_rn(p0y, __dsub_rn(1.0, r)));
+                plane_wave(gx, gy, t, gp[i], gu[i], gv[i]);
+            }
+        } else if (kind == kGhostInterface) {
+            // Mesh2D_t.cpp:4712-4730.
+            const int64_t src = M.gsrc[gi];
+            const int Ns = M.eN[src];
+            const double* sp = tr + M.off1[src] + M.gsrc_side[gi] * (Ns + 1);
+            for (int i = 0; i <= Ns && i <= N; ++i) {
+                gp[i] = sp[i];
+                gu[i] = sp[i + ft];
+                gv[i] = sp[i + 2 * ft];
+            }
+        } else {
+            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = 0.0;
+        }
+    }
+}
+
+// Face fluxes: thread per (instance, face, face node).
+template <bool S>
+__global__ void __launch_bounds__(256) general_faces_kernel(GeneralStage a, int max_n) {
+    const GeneralMesh& M = a.m;
+    const int64_t ft = M.trace_total, ff = M.face_total;
+    const int64_t per_inst = M.n_faces * max_n;
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < per_inst * a.n_instances;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t inst = idx / per_inst;
+        const int64_t r = idx - inst * per_inst;
+        const int64_t f = r / max_n;
+        const int i = static_cast<int>(r - f * max_n);
+        const int Nf = M.fN[f];
+        if (i > Nf) continue;
+        const double* xf = g_nodes + gvec(Nf);
+        const double* tr = a.etr + inst * 3 * ft;
+        double val[2][3];
+        for (int side = 0; side < 2; ++side) {
+            const int64_t e = M.felem[2 * f + side];
+            const int64_t es = M.fside[2 * f + side];
+            const int Ne = M.eN[e];
+            const double* ep = tr + M.off1[e] + es * (Ne + 1);
+            const int64_t en0 = M.enodes[4 * e + es];
+            const int64_t en1 = M.enodes[4 * e + ((es + 1) & 3)];
+            const bool conforming = side == 0 ? (Nf == Ne && M.fnodes[2 * f] == en0 && M.fnodes[2 * f + 1] == en1)
+                                              : (Nf == Ne && M.fnodes[2 * f + 1] == en0 && M.fnodes[2 * f] == en1);
+            if (conforming) {
+                const int src = side == 0 ? i : Nf - i;
+                val[side][0] = ep[src];
+                val[side][1] = ep[src + ft];
+                val[side][2] = ep[src + 2 * ft];
+            } else {
+                const double* xe = g_nodes + gvec(Ne);
+                const double* bwe = g_bary + gvec(Ne);
+                const double coord = mortar_coord(xf[side == 0 ? i : Nf - i], M.fscale[2 * f + side], M.foffset[2 * f + side]);
+                double pn = 0.0, un = 0.0, vn = 0.0, den = 0.0;
+                for (int j = 0; j <= Ne; ++j) {
+                    if (almost_equal(coord, xe[j])) {
+                        pn = ep[j];
+                        un = ep[j + ft];
+                        vn = ep[j + 2 * ft];
+                        den = 1.0;
+                        break;
+                    }
+                    const double tj = S ? __ddiv_rn(bwe[j], __dsub_rn(coord, xe[j])) : bwe[j] / (coord - xe[j]);
+                    pn = madd<S>(pn, tj, ep[j]);
+                    un = madd<S>(un, tj, ep[j + ft]);
+                    vn = madd<S>(vn, tj, ep[j + 2 * ft]);
+                    den = add<S>(den, tj);
+                }
+                val[side][0] = S ? __ddiv_rn(pn, den) : pn / den;
+                val[side][1] = S ? __ddiv_rn(un, den) : un / den;
+                val[side][2] = S ? __ddiv_rn(vn, den) : vn / den;
+            }
+        }
+        // Upwind flux with c = 1 (Solver2D_t.cpp:48-63).
+        const double nx = M.fnormal[2 * f], ny = M.fnormal[2 * f + 1];
+        const double wL = add<S>(val[0][0], add<S>(mul<S>(val[0][1], nx), mul<S>(val[0][2], ny)));
+        const double wR = sub<S>(val[1][0], add<S>(mul<S>(val[1][1], nx), mul<S>(val[1][2], ny)));
+        const double sum = add<S>(wL, wR);
+        double* out = a.ffl + inst * 3 * ff + M.foff[f] + i;
+        out[0] = mul<S>(sub<S>(wL, wR), 0.5);
+        out[ff] = mul<S>(mul<S>(nx, sum), 0.5);
+        out[2 * ff] = mul<S>(mul<S>(ny, sum), 0.5);
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Volume kernel tiles: EPB elements of one order per CTA, one thread per
+// (field, element, line) as in the uniform kernel.
+template <int N>
+struct GenTile {
+    static constexpr int n = N + 1;
+    static constexpr int NN = n * n;
+    static constexpr int raw = 256 / (3 * n);
+    static constexpr int EPB = raw >= 1 ? raw : 1;
+    static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
+    static constexpr int kQ = 0;                        // [3][EPB][NN] q
+    static constexpr int kG = kQ + 3 * EPB * NN;        // [3][EPB][NN] G
+    static constexpr int kF = kG + 3 * EPB * NN;        // [3][EPB][4][n] element side fluxes
+    static constexpr int kJ = kF + 3 * EPB * 4 * n;     // [EPB][NN] J (1/J in the default mode)
+    static constexpr int kS = kJ + EPB * NN;            // [EPB][4] edge metric per side
+    static constexpr int kDoubles = kS + EPB * 4;
+    static constexpr size_t kBytes = sizeof(double) * kDoubles;
+};
+
+// Element side flux of node i of side s of element e (Mesh2D_t.cpp:3895-4006):
+// the face flux times the edge metric when one face of the same order
+// covers the side (reversed and negated for the face's right element),
+// otherwise the mortar projection of every face on the side.
+template <bool S>
+__device__ __forceinline__ void element_side_flux(const GeneralStage& a, const double* __restrict__ ffl, int64_t e, int s, int i, int N,
+                                                  double sfv, double out[3]) {
+    const GeneralMesh& M = a.m;
+    const int64_t ff = M.face_total;
+    const int64_t q0 = M.sface_start[4 * e + s], q1 = M.sface_start[4 * e + s + 1];
+    if (q1 == q0) {
+        out[0] = out[1] = out[2] = 0.0;
+        return;
+    }
+    const int64_t f0 = M.sface[q0];
+    const int64_t en0 = M.enodes[4 * e + s], en1 = M.enodes[4 * e + ((s + 1) & 3)];
+    if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0] == en0 && M.fnodes[2 * f0 + 1] == en1) {
+        const double* fl = ffl + M.foff[f0] + i;
+        out[0] = mul<S>(fl[0], sfv);
+        out[1] = mul<S>(fl[ff], sfv);
+        out[2] = mul<S>(fl[2 * ff], sfv);
+        return;
+    }
+    if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0 + 1] == en0 && M.fnodes[2 * f0] == en1) {
+        const double* fl = ffl + M.foff[f0] + (N - i);
+        out[0] = mul<S>(-fl[0], sfv);
+        out[1] = mul<S>(-fl[ff], sfv);
+        out[2] = mul<S>(-fl[2 * ff], sfv);
+        return;
+    }
+    const double* xe = g_nodes + gvec(N);
+    const double* we = g_weights + gvec(N);
+    const double* bwe = g_bary + gvec(N);
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int64_t q = q0; q < q1; ++q) {
+        const int64_t f = M.sface[q];
+        const int Nf = M.fN[f];
+        const double* xf = g_nodes + gvec(Nf);
+        const double* wf = g_weights + gvec(Nf);
+        const bool fwd = e == M.felem[2 * f];
+        const int fs = fwd ? 0 : 1;
+        const double sgn = fwd ? 1.0 : -1.0;
+        const double scale = M.fscale[2 * f + fs], offset = M.foffset[2 * f + fs];
+        for (int j = 0; j <= Nf; ++j) {
+            const double coord = mortar_coord(xf[fwd ? j : Nf - j], scale, offset);
+            const double* fl = ffl + M.foff[f] + j;
+            int found = -1;
+            for (int ii = 0; ii <= N; ++ii)
+                if (almost_equal(coord, xe[ii])) {
+                    found = ii;
+                    break;
+                }
+            double w;
+            if (found >= 0) {
+                if (found != i) continue;
+                w = S ? __ddiv_rn(__dmul_rn(sgn, wf[j]), we[i]) : sgn * wf[j] / we[i];
+            } else {
+                double sb = 0.0;
+                for (int ii = 0; ii <= N; ++ii) sb = add<S>(sb, S ? __ddiv_rn(bwe[ii], __dsub_rn(coord, xe[ii])) : bwe[ii] / (coord - xe[ii]));
+                const double T = S ? __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), sb)) : bwe[i] / ((coord - xe[i]) * sb);
+                w = S ? __ddiv_rn(__dmul_rn(__dmul_rn(sgn, T), wf[j]), we[i]) : sgn * T * wf[j] / we[i];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[c] = add<S>(acc[c], mul<S>(mul<S>(mul<S>(w, fl[c * ff]), sfv), scale));
+        }
+    }
+    out[0] = acc[0];
+    out[1] = acc[1];
+    out[2] = acc[2];
+}
+
+template <int N, bool S>
+__global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
+    using T = GenTile<N>;
+    constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
+    extern __shared__ __align__(128) double smem[];
+    double* qs = smem + T::kQ;
+    double* gs = smem + T::kG;
+    double* fs = smem + T::kF;
+    double* js = smem + T::kJ;
+    double* ss = smem + T::kS;
+    constexpr int FS = EPB * 4 * n;
+    const GeneralMesh& M = a.m;
+    const int tid = threadIdx.x;
+    const int64_t base = static_cast<int64_t>(blockIdx.x) * EPB;
+    const int ne = static_cast<int>((count - base) < EPB ? (count - base) : EPB);
+    const int64_t inst = blockIdx.y;
+    const int64_t fb = M.block;
+    double* q = a.q + inst * 3 * fb;
+    double* k = a.k + inst * 3 * fb;
+    const double* ffl = a.ffl + inst * 3 * M.face_total;
+    const double* xn = g_nodes + gvec(N);
+    const double* lm = g_lagrange_left + gvec(N);
+    const double* lp = g_lagrange_right + gvec(N);
+    const double dt = a.step[1];
+
+    // q tile: coalesced within each element's blocks.
+    for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
+        const int f = idx / (ne * NN), r = idx - f * (ne * NN);
+        const int e = r / NN, node = r - e * NN;
+        qs[(f * EPB + e) * NN + node] = q[f * fb + M.off2[ids[base + e]] + node];
+    }
+
+    const int f = tid / (EPB * n);
+    const int rr = tid - f * (EPB * n);
+    const int e = rr / n;
+    const int m = rr - e * n;
+    const bool active = f < 3 && e < ne;
+    const int64_t ge = active ? ids[base + e] : 0;
+    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    if (active) {
+        const double* c = M.corners + 8 * ge;
+        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
+    }
+    const MetricLine<S> x_xi(sub<S>(x1, x0), sub<S>(x2, x3)), y_xi(sub<S>(y1, y0), sub<S>(y2, y3));
+    const MetricLine<S> x_eta(sub<S>(x3, x0), sub<S>(x2, x1)), y_eta(sub<S>(y3, y0), sub<S>(y2, y1));
+    if (active) {
+        const double tm = xn[m];
+        if (f == 2) {
+            for (int sd = m; sd < 4; sd += n) {
+                const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
+                const double dx = (sd == 0 || sd == 2) ? metric<S>(at, x_xi.d0, x_xi.d1) : metric<S>(at, x_eta.d0, x_eta.d1);
+                const double dy = (sd == 0 || sd == 2) ? metric<S>(at, y_xi.d0, y_xi.d1) : metric<S>(at, y_eta.d0, y_eta.d1);
+                ss[e * 4 + sd] = sqrt(add<S>(mul<S>(dx, dx), mul<S>(dy, dy)));
+            }
+        }
+        const double xe = x_eta(tm), ye = y_eta(tm);
+        for (int j = f; j < n; j += 3) {
+            const double tj = xn[j];
+            const double jac = sub<S>(mul<S>(x_xi(tj), ye), mul<S>(xe, y_xi(tj)));
+            js[e * NN + m * n + j] = S ? jac : __drcp_rn(jac);
+        }
+    }
+    __syncthreads();  // q tile, J, edge metrics
+
+    // Element side fluxes: item (element, side, node), three fields each.
+    for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
+        const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
+        const int s = sm / n, i = sm - s * n;
+        double out[3];
+        element_side_flux<S>(a, ffl, ids[base + ee], s, i, N, ss[ee * 4 + s], out);
+        fs[0 * FS + idx] = out[0];
+        fs[1 * FS + idx] = out[1];
+        fs[2 * FS + idx] = out[2];
+    }
+    __syncthreads();
+
+    const double* Dh = g_dhat + gmat(N);
+    const double* w = g_weights + gvec(N);
+    const double* iw = g_inv_weights + gvec(N);
+    const double* F = fs + f * FS + e * 4 * n;
+
+    // xi pass (eta index j = m): Dhat . line + lift, G = -(...) (Solver2D_t.cpp:82-101).
+    if (active) {
+        const int j = m;
+        double col[n];
+        const double* P = qs + (0 * EPB + e) * NN + j;
+        const double* U = qs + (1 * EPB + e) * NN + j;
+        const double* V = qs + (2 * EPB + e) * NN + j;
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            if (f == 0) col[i] = sub<S>(mul<S>(y_eta(xn[i]), U[i * n]), mul<S>(x_eta(xn[i]), V[i * n]));
+            else if (f == 1) col[i] = mul<S>(y_eta(xn[i]), P[i * n]);
+            else col[i] = -mul<S>(x_eta(xn[i]), P[i * n]);
+        }
+        const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
+        double* G = gs + (f * EPB + e) * NN + j;
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+#pragma unroll
+            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[i * n + mm], col[mm]);
+            const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
+            G[i * n] = -add<S>(acc, lift);
+        }
+    }
+    __syncthreads();
+
+    // eta pass (xi index i = m): G = (G - (Dhat . line + lift)) / J (Solver2D_t.cpp:103-133).
+    if (active) {
+        const int i = m;
+        double line[n];
+        const double* P = qs + (0 * EPB + e) * NN + i * n;
+        const double* U = qs + (1 * EPB + e) * NN + i * n;
+        const double* V = qs + (2 * EPB + e) * NN + i * n;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            if (f == 0) line[j] = add<S>(mul<S>(-y_xi(xn[j]), U[j]), mul<S>(x_xi(xn[j]), V[j]));
+            else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), P[j]);
+            else line[j] = mul<S>(x_xi(xn[j]), P[j]);
+        }
+        const double ft = F[2 * n + (N - i)], fbm = F[0 * n + i];
+        double* G = gs + (f * EPB + e) * NN + i * n;
+        const double* jrow = js + e * NN + i * n;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            double acc = 0.0;
+#pragma unroll
+            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[j * n + mm], line[mm]);
+            const double lift = S ? __ddiv_rn(add<S>(mul<S>(ft, lp[j]), mul<S>(fbm, lm[j])), w[j]) : (ft * lp[j] + fbm * lm[j]) * iw[j];
+            const double num = sub<S>(G[j], add<S>(acc, lift));
+            G[j] = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
+        }
+    }
+    __syncthreads();
+
+    // Low-storage RK3 update (Solver2D_t.cpp:138-172), node by node.
+    const double gdt = mul<S>(a.rk_g, dt);
+    for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
+        const int ff = idx / (ne * NN), r = idx - ff * (ne * NN);
+        const int ee = r / NN, node = r - ee * NN;
+        const int64_t gi = ff * fb + M.off2[ids[base + ee]] + node;
+        const double G = gs[(ff * EPB + ee) * NN + node];
+        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, k[gi]), G);
+        k[gi] = kn;
+        q[gi] = add<S>(qs[(ff * EPB + ee) * NN + node], mul<S>(gdt, kn));
+        if (a.G_out) a.G_out[inst * 3 * fb + gi] = G;
+    }
+}
+
+// Plane-wave initial condition at every node of a group (Mesh2D_t.cpp:1192-1216).
+template <int N>
+__global__ void __launch_bounds__(256) general_ic_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
+    constexpr int n = N + 1, NN = n * n;
+    const double* xn = g_nodes + gvec(N);
+    const int64_t fb = a.m.block;
+    const int64_t total = count * NN;
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total * a.n_instances;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t inst = idx / total;
+        const int64_t r = idx - inst * total;
+        const int64_t le = r / NN;
+        const int node = static_cast<int>(r - le * NN);
+        const int i = node / n, j = node - i * n;
+        const int64_t e = ids[le];
+        const double* c = a.m.corners + 8 * e;
+        // quad_map (include/functions/quad_map.tpp): bilinear map of (xi_i, eta_j).
+        const double xi = xn[i], eta = xn[j];
+        const double am = __dsub_rn(1.0, xi), bp = __dadd_rn(xi, 1.0), cm = __dsub_rn(1.0, eta), dp = __dadd_rn(eta, 1.0);
+        const double x = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(c[0], am), cm), __dmul_rn(__dmul_rn(c[2], bp), cm)), __dmul_rn(__dmul_rn(c[4], bp), dp)),
+                                             __dmul_rn(__dmul_rn(c[6], am), dp)),
+                                   0.25);
+        const double y = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(c[1], am), cm), __dmul_rn(__dmul_rn(c[3], bp), cm)), __dmul_rn(__dmul_rn(c[5], bp), dp)),
+                                             __dmul_rn(__dmul_rn(c[7], am), dp)),
+                                   0.25);
+        double p, u, v;
+        plane_wave(x, y, 0.0, p, u, v);
+        const int64_t gi = inst * 3 * fb + a.m.off2[e] + node;
+        a.q[gi] = p;
+        a.q[gi + fb] = u;
+        a.q[gi + 2 * fb] = v;
+        a.k[gi] = 0.0;
+        a.k[gi + fb] = 0.0;
+        a.k[gi + 2 * fb] = 0.0;
+    }
+}
+
+// Field transfer, one thread per (instance, field, new element, node)
+// (Element2D_t::interpolate_from, same points; Element2D_t.cpp:464-579),
+// always rounded as the reference rounds.
+__global__ void __launch_bounds__(256) transfer_kernel(Transfer t, int max_nn) {
+    const int64_t per_field = t.n_elements * max_nn;
+    const int64_t total = per_field * t.n_fields * t.n_instances;
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total; idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t fi = idx / per_field;  // instance * n_fields + field
+        const int64_t r = idx - fi * per_field;
+        const int64_t e = r / max_nn;
+        const int node = static_cast<int>(r - e * max_nn);
+        const int Nn = t.new_N[e], No = t.old_N[e];
+        const int nn = Nn + 1, no = No + 1;
+        if (node >= nn * nn) continue;
+        const double* src = t.src + fi * t.old_block + t.old_off2[e];
+        double* dst = t.dst + fi * t.new_block + t.new_off2[e] + node;
+        if (Nn == No) {
+            *dst = src[node];
+            continue;
+        }
+        if (t.zero_changed) {
+            *dst = 0.0;
+            continue;
+        }
+        const int i = node / nn, j = node - i * nn;
+        const double x = g_nodes[gvec(Nn) + i], y = g_nodes[gvec(Nn) + j];
+        const double* xo = g_nodes + gvec(No);
+        const double* bo = g_bary + gvec(No);
+        int row = -1, col = -1;
+        for (int mm = 0; mm <= No; ++mm) {
+            if (almost_equal(x, xo[mm])) col = mm;
+            if (almost_equal(y, xo[mm])) row = mm;
+        }
+        double v;
+        if (row != -1 && col != -1) {
+            v = src[col * no + row];
+        } else if (row != -1) {
+            double num = 0.0, den = 0.0;
+            for (int mm = 0; mm <= No; ++mm) {
+                const double tt = __ddiv_rn(bo[mm], __dsub_rn(x, xo[mm]));
+                num = __dadd_rn(num, __dmul_rn(tt, src[mm * no + row]));
+                den = __dadd_rn(den, tt);
+            }
+            v = __ddiv_rn(num, den);
+        } else if (col != -1) {
+            double num = 0.0, den = 0.0;
+            for (int mm = 0; mm <= No; ++mm) {
+                const double tt = __ddiv_rn(bo[mm], __dsub_rn(y, xo[mm]));
+                num = __dadd_rn(num, __dmul_rn(tt, src[col * no + mm]));
+                den = __dadd_rn(den, tt);
+            }
+            v = __ddiv_rn(num, den);
+        } else {
+            double dx = 0.0, dy = 0.0;
+            for (int kk = 0; kk <= No; ++kk) {
+                dx = __dadd_rn(dx, __ddiv_rn(bo[kk], __dsub_rn(x, xo[kk])));
+                dy = __dadd_rn(dy, __ddiv_rn(bo[kk], __dsub_rn(y, xo[kk])));
+            }
+            v = 0.0;
+            for (int mm = 0; mm <= No; ++mm) {
+                const double tx = __ddiv_rn(bo[mm], __dmul_rn(__dsub_rn(x, xo[mm]), dx));
+                for (int nn2 = 0; nn2 <= No; ++nn2) {
+                    const double ty = __ddiv_rn(bo[nn2], __dmul_rn(__dsub_rn(y, xo[nn2]), dy));
+                    v = __dadd_rn(v, __dmul_rn(__dmul_rn(src[mm * no + nn2], tx), ty));
+                }
+            }
+        }
+        *dst = v;
+    }
+}
+
+int grid_for(int64_t items, int threads) {
+    const int64_t b = (items + threads - 1) / threads;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32)));
+}
+
+template <int N, bool S>
+cudaError_t launch_group(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
+    using T = GenTile<N>;
+    general_traces_kernel<N, S><<<grid_for(g.count * 4 * (N + 1) * a.n_instances, 256), 256, 0, stream>>>(a, g.ids, g.count);
+    return cudaGetLastError();
+}
+
+template <int N, bool S>
+cudaError_t launch_volume(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
+    using T = GenTile<N>;
+    const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
+    general_volume_kernel<N, S><<<grid, T::kThreads, T::kBytes, stream>>>(a, g.ids, g.count);
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t set_attrs() {
+    cudaError_t err = cudaFuncSetAttribute(general_volume_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(GenTile<N>::kBytes));
+    if (err != cudaSuccess) return err;
+    return cudaFuncSetAttribute(general_volume_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(GenTile<N>::kBytes));
+}
+
+template <int N>
+cudaError_t launch_ic(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
+    general_ic_kernel<N><<<grid_for(g.count * (N + 1) * (N + 1) * a.n_instances, 256), 256, 0, stream>>>(a, g.ids, g.count);
+    return cudaGetLastError();
+}
+
+// Calls fn.template operator()<N>() for a runtime order 1..16.
+template <typename F>
+cudaError_t by_order(int N, F&& fn) {
+    switch (N) {
+        case 1: return fn(std::integral_constant<int, 1>{});
+        case 2: return fn(std::integral_constant<int, 2>{});
+        case 3: return fn(std::integral_constant<int, 3>{});
+        case 4: return fn(std::integral_constant<int, 4>{});
+        case 5: return fn(std::integral_constant<int, 5>{});
+        case 6: return fn(std::integral_constant<int, 6>{});
+        case 7: return fn(std::integral_constant<int, 7>{});
+        case 8: return fn(std::integral_constant<int, 8>{});
+        case 9: return fn(std::integral_constant<int, 9>{});
+        case 10: return fn(std::integral_constant<int, 10>{});
+        case 11: return fn(std::integral_constant<int, 11>{});
+        case 12: return fn(std::integral_constant<int, 12>{});
+        case 13: return fn(std::integral_constant<int, 13>{});
+        case 14: return fn(std::integral_constant<int, 14>{});
+        case 15: return fn(std::integral_constant<int, 15>{});
+        case 16: return fn(std::integral_constant<int, 16>{});
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t upload_general_tables(const Tables& t) {
+    if (t.N_max < 1) return cudaSuccess;
+    std::vector<double> nodes(kGVecTotal, 0.0), weights(kGVecTotal, 0.0), inv_w(kGVecTotal, 0.0), bary(kGVecTotal, 0.0), ll(kGVecTotal, 0.0),
+        lr(kGVecTotal, 0.0), dhat(kGMatTotal, 0.0);
+    for (int N = 0; N <= std::min(t.N_max, kMaxOrder); ++N) {
+        for (int i = 0; i <= N; ++i) {
+            const size_t at = static_cast<size_t>(gvec(N) + i);
+            nodes[at] = t.get(NDG_TABLE_NODES, N)[static_cast<size_t>(i)];
+            weights[at] = t.get(NDG_TABLE_WEIGHTS, N)[static_cast<size_t>(i)];
+            inv_w[at] = 1.0 / weights[at];
+            bary[at] = t.get(NDG_TABLE_BARYCENTRIC_WEIGHTS, N)[static_cast<size_t>(i)];
+            ll[at] = t.get(NDG_TABLE_LAGRANGE_LEFT, N)[static_cast<size_t>(i)];
+            lr[at] = t.get(NDG_TABLE_LAGRANGE_RIGHT, N)[static_cast<size_t>(i)];
+        }
+        const auto& d = t.get(NDG_TABLE_DERIVATIVE_MATRICES_HAT, N);
+        std::copy(d.begin(), d.end(), dhat.begin() + gmat(N));
+    }
+    cudaError_t err;
+    if ((err = cudaMemcpyToSymbol(g_nodes, nodes.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(g_weights, weights.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(g_inv_weights, inv_w.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(g_bary, bary.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(g_lagrange_left, ll.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(g_lagrange_right, lr.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
+    return cudaMemcpyToSymbol(g_dhat, dhat.data(), sizeof(double) * kGMatTotal);
+}
+
+cudaError_t prepare_general_kernels(int N) {
+    return by_order(N, [](auto c) { return set_attrs<decltype(c)::value>(); });
+}
+
+cudaError_t launch_general_stage(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream) {
+    cudaError_t err = cudaSuccess;
+    const int max_n = a.m.max_n;
+    for (int g = 0; g < n_groups && err == cudaSuccess; ++g) {
+        if (groups[g].count == 0) continue;
+        err = by_order(groups[g].N, [&](auto c) {
+            constexpr int N = decltype(c)::value;
+            return strict ? launch_group<N, true>(a, groups[g], stream) : launch_group<N, false>(a, groups[g], stream);
+        });
+    }
+    if (err != cudaSuccess) return err;
+    const int64_t n_ghosts = a.m.n_total - a.m.n_domain;
+    if (n_ghosts > 0) {
+        if (strict) general_ghosts_kernel<true><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
+        else general_ghosts_kernel<false><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
+        if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    }
+    // max_n covers the largest face order.
+    const int64_t face_items = a.m.n_faces * max_n * a.n_instances;
+    if (strict) general_faces_kernel<true><<<grid_for(face_items, 256), 256, 0, stream>>>(a, max_n);
+    else general_faces_kernel<false><<<grid_for(face_items, 256), 256, 0, stream>>>(a, max_n);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    for (int g = 0; g < n_groups && err == cudaSuccess; ++g) {
+        if (groups[g].count == 0) continue;
+        err = by_order(groups[g].N, [&](auto c) {
+            constexpr int N = decltype(c)::value;
+            return strict ? launch_volume<N, true>(a, groups[g], stream) : launch_volume<N, false>(a, groups[g], stream);
+        });
+    }
+    return err;
+}
+
+cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream) {
+    cudaError_t err = cudaSuccess;
+    for (int g = 0; g < n_groups && err == cudaSuccess; ++g) {
+        if (groups[g].count == 0) continue;
+        err = by_order(groups[g].N, [&](auto c) { return launch_ic<decltype(c)::value>(a, groups[g], stream); });
+    }
+    return err;
+}
+
+cudaError_t launch_transfer(const Transfer& t, cudaStream_t stream) {
+    if (t.n_elements == 0) return cudaSuccess;
+    constexpr int max_nn = (kMaxOrder + 1) * (kMaxOrder + 1);
+    transfer_kernel<<<grid_for(t.n_elements * max_nn * t.n_fields * t.n_instances, 256), 256, 0, stream>>>(t, max_nn);
+    return cudaGetLastError();
+}
+
+}  // namespace dev
+}  // namespace ndg

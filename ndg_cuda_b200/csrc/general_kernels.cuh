@@ -1,0 +1,106 @@
+// Stage kernels for meshes of mixed order and nonconforming faces
+// (general_kernels.cu): the state after p- or h-adaptation.
+#pragma once
+
+#include "ndg_internal.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ndg {
+namespace dev {
+
+// What a ghost element's side-0 trace is made of at each stage
+// (Mesh2D_t::boundary_conditions, src/meshes/Mesh2D_t.cpp:3731-3782).
+enum GhostKind : int {
+    kGhostMirror = 0,     // wall and symmetry: projected neighbour trace, normal velocity mirrored
+    kGhostAnalytic = 1,   // inflow: the plane wave on the ghost's edge
+    kGhostCopy = 2,       // outflow: projected neighbour trace
+    kGhostInterface = 3,  // periodic destination: the origin element's side trace
+    kGhostNone = 4
+};
+
+// Device view of a mixed-order mesh, in the reference's numbering:
+// elements 0 .. n_domain-1 are the domain, the rest ghosts.
+struct GeneralMesh {
+    int64_t n_domain = 0, n_total = 0, n_faces = 0;
+    int64_t trace_total = 0;  // values per field of the element side-trace array
+    int64_t face_total = 0;   // values per field of the face flux array
+    int64_t block = 0;        // values per field block of q, k and G
+    int max_n = 1;            // largest order + 1 over elements and faces
+    const int* eN = nullptr;            // [n_total] order
+    const int64_t* off2 = nullptr;      // [n_domain] first value of the element in a field block
+    const int64_t* off1 = nullptr;      // [n_total] first side-trace value (4 (N+1) domain, N+1 ghost)
+    const int64_t* enodes = nullptr;    // [4 n_total]
+    const int64_t* sface_start = nullptr;  // [4 n_total + 1] faces of side s of element e:
+    const int64_t* sface = nullptr;        //   sface[sface_start[4e+s] .. sface_start[4e+s+1])
+    const double* corners = nullptr;    // [8 n_domain]
+    const double* node_xy = nullptr;    // [2 n_nodes]
+    const int* fN = nullptr;            // [n_faces]
+    const int64_t* foff = nullptr;      // [n_faces] first flux value of the face
+    const int64_t* fnodes = nullptr;    // [2 n_faces]
+    const int64_t* felem = nullptr;     // [2 n_faces]
+    const int64_t* fside = nullptr;     // [2 n_faces]
+    const double* fnormal = nullptr;    // [2 n_faces]
+    const double* ftangent = nullptr;   // [2 n_faces]
+    const double* foffset = nullptr;    // [2 n_faces]
+    const double* fscale = nullptr;     // [2 n_faces]
+    const int* gkind = nullptr;         // [n_total - n_domain] GhostKind
+    const double* gscale = nullptr;     // [n_total - n_domain] side-0 scaling factor
+    const int64_t* gsrc = nullptr;      // [n_total - n_domain] interface origin element
+    const int* gsrc_side = nullptr;     // [n_total - n_domain] interface origin side
+};
+
+// One RK3 stage on a mixed-order mesh.
+struct GeneralStage {
+    GeneralMesh m;
+    double* q = nullptr;      // [instance][field][block]
+    double* k = nullptr;
+    double* G_out = nullptr;  // optional copy of the stage's time derivative
+    double* etr = nullptr;    // [instance][field][trace_total] element side traces
+    double* ffl = nullptr;    // [instance][field][face_total] face fluxes
+    const double* step = nullptr;  // {time, dt, dt_mesh, t_end}
+    double rk_a = 0, rk_b = 0, rk_g = 0;
+    int first = 0;
+    int n_instances = 1;
+};
+
+// Elements of one order, processed by one launch of the order's kernels.
+struct OrderGroup {
+    int N = 0;
+    int64_t count = 0;
+    const int64_t* ids = nullptr;  // device, element numbers
+};
+
+cudaError_t upload_general_tables(const Tables& t);
+cudaError_t prepare_general_kernels(int N);
+// Side traces, ghost traces, face fluxes, then per order group the
+// element fluxes, volume term and RK update.
+cudaError_t launch_general_stage(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream);
+// The plane-wave initial condition at every node of a mixed-order mesh.
+cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream);
+
+// Field transfer to a re-ordered mesh (Element2D_t::interpolate_from, same
+// element points; src/entities/Element2D_t.cpp:464-579): for new element e,
+// old order old_N[e] at old offset old_off2[e]; equal orders copy, others
+// interpolate, or write zeros when zero_changed is set (the RK register of a
+// re-ordered element starts at zero). Fields: n_fields blocks of old_block /
+// new_block values per instance.
+struct Transfer {
+    const double* src = nullptr;
+    double* dst = nullptr;
+    int64_t old_block = 0, new_block = 0;
+    int n_fields = 3;
+    int n_instances = 1;
+    int64_t n_elements = 0;
+    const int* old_N = nullptr;
+    const int64_t* old_off2 = nullptr;
+    const int* new_N = nullptr;
+    const int64_t* new_off2 = nullptr;
+    int zero_changed = 0;  // 1: write zeros where the order changed (RK register)
+};
+cudaError_t launch_transfer(const Transfer& t, cudaStream_t stream);
+
+}  // namespace dev
+}  // namespace ndg

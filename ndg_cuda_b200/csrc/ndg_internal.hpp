@@ -81,4 +81,30 @@ struct SidePlan {
 };
 SidePlan build_side_plan(const Topology& topo, const Tables& tables);
 
+// True when every element and face has one order and every face is
+// conforming, so the fused uniform-order kernels apply.
+bool fused_path_applies(const Topology& t);
+
+// Host arrays of the general (mixed-order, mortar) stage path; the field
+// names match dev::GeneralMesh.
+struct GeneralPlan {
+    int64_t n_domain = 0, n_total = 0, n_faces = 0, trace_total = 0, face_total = 0, block = 0;
+    std::vector<int32_t> eN;
+    std::vector<int64_t> off2, off1, enodes, sface_start, sface;
+    std::vector<double> corners, node_xy;
+    std::vector<int32_t> fN;
+    std::vector<int64_t> foff, fnodes, felem, fside;
+    std::vector<double> fnormal, ftangent, foffset, fscale;
+    std::vector<int32_t> gkind;
+    std::vector<double> gscale;
+    std::vector<int64_t> gsrc;
+    std::vector<int32_t> gsrc_side;
+    std::vector<std::pair<int, std::vector<int64_t>>> groups;  // order, its domain elements
+};
+GeneralPlan build_general_plan(const Topology& t);
+
+// p-adaptation of the topology (orders of elements, ghosts and faces) from
+// per-element refine flags and decay rates. Returns whether an order changed.
+bool p_adapt(Topology& t, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level);
+
 }  // namespace ndg
