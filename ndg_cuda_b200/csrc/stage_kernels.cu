@@ -130,7 +130,8 @@ struct Tile {
     static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far side traces, then side fluxes
     static constexpr int kJ = kFar + 3 * EPB * 4 * n;    // [EPB][NN] 1/J (J in strict mode)
     static constexpr int kS = kJ + EPB * NN;             // [EPB][4] edge metric per side
-    static constexpr int kBar = kS + EPB * 4;            // mbarrier (8 bytes)
+    static constexpr int kZ = kS + EPB * 4;              // [NN] zeros: the absent flux component
+    static constexpr int kBar = kZ + NN;                 // mbarrier (8 bytes)
     static constexpr int kDoubles = kBar + 2;
     static constexpr size_t kBytes = sizeof(double) * kDoubles;
 };
@@ -151,8 +152,16 @@ __device__ __forceinline__ double side_trace(const double* __restrict__ q, int s
     return acc;
 }
 
+// Coefficients of order N, passed by value as a kernel parameter so that
+// every use is a constant-bank operand with a compile-time offset.
+template <int N>
+struct Coeffs {
+    double dhat[(N + 1) * (N + 1)];
+    double xn[N + 1], lm[N + 1], lp[N + 1], w[N + 1], iw[N + 1];
+};
+
 template <int N, bool S>
-__global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
+__global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a, const __grid_constant__ Coeffs<N> cf) {
     using T = Tile<N>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     extern __shared__ __align__(128) double smem[];
@@ -163,6 +172,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
     double* far_s = smem + T::kFar;  // far traces, then element side fluxes in place
     double* js = smem + T::kJ;
     double* ss = smem + T::kS;
+    double* zs = smem + T::kZ;
     constexpr int FS = EPB * 4 * n;  // field stride of own_s / far_s
 
     const int tid = threadIdx.x;
@@ -176,9 +186,9 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
     double* k = a.k + inst * 3 * Kp * NN;
     const double* tr_in = a.trace_in + inst * 3 * Kp * 4 * n;
     double* tr_out = a.trace_out + inst * 3 * Kp * 4 * n;
-    const double* xn = c_nodes + vec_offset(N);
-    const double* lm = c_lagrange_left + vec_offset(N);
-    const double* lp = c_lagrange_right + vec_offset(N);
+    const double* xn = cf.xn;
+    const double* lm = cf.lm;
+    const double* lp = cf.lp;
     const double time = a.step[0];
     const double dt = a.step[1];
 
@@ -198,6 +208,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
         mbar_expect_tx(bar, 3 * bytes);
         for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
     }
+    for (int i = tid; i < NN; i += T::kThreads) zs[i] = 0.0;
     // Far traces of this thread's field at node m of the four sides (the
     // neighbour's trace of the previous stage), element metrics, edge
     // metrics and J.
@@ -237,82 +248,44 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
             js[e * NN + m * n + j] = S ? jac : __drcp_rn(jac);
         }
     }
-    __syncthreads();  // mbarrier init, far traces, edge metrics, J
+    __syncthreads();  // mbarrier init, zeros, far traces, edge metrics, J
     if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
 
-    // Row pass (xi index i = m): bottom and top traces (Element2D_t.cpp:86-125)
-    // of the rows; field 0's threads take u and v, field 1's take p.
-    if (active && f < 2) {
-        const int i = m;
-        const double* R0 = qs + ((f == 0 ? 1 : 0) * EPB + e) * NN + i * n;
-        const double* R1 = qs + (2 * EPB + e) * NN + i * n;
-        double b0 = 0.0, t0 = 0.0, b1 = 0.0, t1 = 0.0;
+    // Own side traces of this thread's field (Element2D_t.cpp:86-125):
+    // bottom and top from row m, right and left from column m.
+    // The flux lines take (X, Y) = (u, v), (p, 0), (0, p) for f = 0, 1, 2:
+    // x_flux = (c u, p, 0), y_flux = (c v, 0, p) (Solver2D_t.cpp:31-37).
+    const double* Qe = qs + e * NN;
+    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : (f == 1 ? Qe : zs);
+    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : (f == 1 ? zs : Qe);
+    if (active) {
+        const double* Qf = Qe + f * EPB * NN;
+        double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            b0 = madd<S>(b0, lm[j], R0[j]);
-            t0 = madd<S>(t0, lp[j], R0[j]);
-            if (f == 0) {
-                b1 = madd<S>(b1, lm[j], R1[j]);
-                t1 = madd<S>(t1, lp[j], R1[j]);
-            }
+            const double qr = Qf[m * n + j], qc = Qf[j * n + m];
+            b = madd<S>(b, lm[j], qr);
+            t = madd<S>(t, lp[j], qr);
+            r = madd<S>(r, lp[j], qc);
+            l = madd<S>(l, lm[j], qc);
         }
-        const int fa = f == 0 ? 1 : 0;
-        own_s[fa * FS + (e * 4 + 0) * n + i] = b0;
-        own_s[fa * FS + (e * 4 + 2) * n + (N - i)] = t0;
-        if (f == 0) {
-            own_s[2 * FS + (e * 4 + 0) * n + i] = b1;
-            own_s[2 * FS + (e * 4 + 2) * n + (N - i)] = t1;
-        }
-    }
-    // Column pass (eta index j = m): the xi-direction flux line
-    // (Solver2D_t.cpp:72-80), and the right and left traces.
-    double col[n];
-    if (active) {
-        const int j = m;
-        const double* P = qs + (0 * EPB + e) * NN + j;
-        const double* U = qs + (1 * EPB + e) * NN + j;
-        const double* V = qs + (2 * EPB + e) * NN + j;
-        if (f == 0) {
-            double ru = 0.0, lu = 0.0, rv = 0.0, lv = 0.0;
-#pragma unroll
-            for (int i = 0; i < n; ++i) {
-                const double u = U[i * n], v = V[i * n];
-                col[i] = sub<S>(mul<S>(y_eta(xn[i]), u), mul<S>(x_eta(xn[i]), v));
-                ru = madd<S>(ru, lp[i], u);
-                lu = madd<S>(lu, lm[i], u);
-                rv = madd<S>(rv, lp[i], v);
-                lv = madd<S>(lv, lm[i], v);
-            }
-            own_s[1 * FS + (e * 4 + 1) * n + j] = ru;
-            own_s[1 * FS + (e * 4 + 3) * n + (N - j)] = lu;
-            own_s[2 * FS + (e * 4 + 1) * n + j] = rv;
-            own_s[2 * FS + (e * 4 + 3) * n + (N - j)] = lv;
-        } else {
-            double rp = 0.0, lp_ = 0.0;
-#pragma unroll
-            for (int i = 0; i < n; ++i) {
-                const double p = P[i * n];
-                col[i] = (f == 1) ? mul<S>(y_eta(xn[i]), p) : -mul<S>(x_eta(xn[i]), p);
-                rp = madd<S>(rp, lp[i], p);
-                lp_ = madd<S>(lp_, lm[i], p);
-            }
-            if (f == 1) {
-                own_s[0 * FS + (e * 4 + 1) * n + j] = rp;
-                own_s[0 * FS + (e * 4 + 3) * n + (N - j)] = lp_;
-            }
-        }
+        double* o = own_s + f * FS + e * 4 * n;
+        o[0 * n + m] = b;
+        o[2 * n + (N - m)] = t;
+        o[1 * n + m] = r;
+        o[3 * n + (N - m)] = l;
     }
     __syncthreads();
 
-    // Flux pass: side nodes of sides {0, 3} (f = 0), {1} (f = 1), {2} (f = 2)
-    // at index m. Far traces of boundary sides, the upwind flux
-    // (Solver2D_t.cpp:48-63) in the face's own left/right order, then the
-    // element's view of it (Mesh2D_t.cpp:3895-3929): times the edge metric,
-    // negated for the face's right element.
+    // Flux pass: side nodes m of side f, and of side 3 for f = 0. Far traces
+    // of boundary sides, the upwind flux (Solver2D_t.cpp:48-63) in the face's
+    // own left/right order, then the element's view of it
+    // (Mesh2D_t.cpp:3895-3929): times the edge metric, negated for the face's
+    // right element.
     if (active) {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            if (!((f == 0 && (s == 0 || s == 3)) || (f == 1 && s == 1) || (f == 2 && s == 2))) continue;
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1 && f != 0) break;
+            const int s = pass == 0 ? f : 3;
             const int2 lk = a.link[4 * ge + s];
             const int kind = (lk.y >> 2) & 7;
             const int role = (lk.y >> 5) & 1;
@@ -368,15 +341,18 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
     }
     __syncthreads();
 
-    const double* Dh = c_dhat + mat_offset(N);
-    const double* w = c_weights + vec_offset(N);
-    const double* iw = c_inv_weights + vec_offset(N);
+    const double* Dh = cf.dhat;
+    const double* w = cf.w;
+    const double* iw = cf.iw;
     const double* F = far_s + f * FS + e * 4 * n;  // this thread's field, element side fluxes
 
-    // xi pass (eta index j = m): Dhat . line + lift, G = -(...)
-    // (Solver2D_t.cpp:82-101); G column j.
+    // xi pass (eta index j = m): contravariant flux line eta_y X - eta_x Y
+    // (Solver2D_t.cpp:72-80), Dhat . line + lift, G = -(...) (:82-101); G column j.
     if (active) {
         const int j = m;
+        double col[n];
+#pragma unroll
+        for (int i = 0; i < n; ++i) col[i] = sub<S>(mul<S>(y_eta(xn[i]), Xe[i * n + j]), mul<S>(x_eta(xn[i]), Ye[i * n + j]));
         const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
         double* G = gs + (f * EPB + e) * NN + j;
 #pragma unroll
@@ -390,21 +366,13 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a) {
     }
     __syncthreads();
 
-    // eta pass (xi index i = m): G = (G - (Dhat . line + lift)) / J
-    // (Solver2D_t.cpp:114-133); G row i.
+    // eta pass (xi index i = m): line -xi_y X + xi_x Y (Solver2D_t.cpp:103-113),
+    // G = (G - (Dhat . line + lift)) / J (:114-133); G row i.
     if (active) {
         const int i = m;
-        // eta-direction contravariant flux line of this thread's field (Solver2D_t.cpp:103-113).
         double line[n];
-        const double* P = qs + (0 * EPB + e) * NN + i * n;
-        const double* U = qs + (1 * EPB + e) * NN + i * n;
-        const double* V = qs + (2 * EPB + e) * NN + i * n;
 #pragma unroll
-        for (int j = 0; j < n; ++j) {
-            if (f == 0) line[j] = add<S>(mul<S>(-y_xi(xn[j]), U[j]), mul<S>(x_xi(xn[j]), V[j]));
-            else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), P[j]);
-            else line[j] = mul<S>(x_xi(xn[j]), P[j]);
-        }
+        for (int j = 0; j < n; ++j) line[j] = add<S>(mul<S>(-y_xi(xn[j]), Xe[i * n + j]), mul<S>(x_xi(xn[j]), Ye[i * n + j]));
         const double ft = F[2 * n + (N - i)], fb = F[0 * n + i];
         double* G = gs + (f * EPB + e) * NN + i * n;
         const double* jrow = js + e * NN + i * n;
@@ -547,13 +515,35 @@ __global__ void end_step_kernel(double* step) {
 }
 
 // ---------------------------------------------------------------------------
+// Host copies of the packed tables (set by upload_tables): the stage kernels
+// take their order's coefficients as a by-value parameter.
+namespace {
+std::vector<double> h_nodes(kVecTotal), h_weights(kVecTotal), h_inv_weights(kVecTotal), h_ll(kVecTotal), h_lr(kVecTotal), h_dhat(kMatTotal);
+}
+
+template <int N>
+Coeffs<N> make_coeffs() {
+    Coeffs<N> c;
+    constexpr int n = N + 1;
+    for (int i = 0; i < n; ++i) {
+        c.xn[i] = h_nodes[static_cast<size_t>(vec_offset(N) + i)];
+        c.lm[i] = h_ll[static_cast<size_t>(vec_offset(N) + i)];
+        c.lp[i] = h_lr[static_cast<size_t>(vec_offset(N) + i)];
+        c.w[i] = h_weights[static_cast<size_t>(vec_offset(N) + i)];
+        c.iw[i] = h_inv_weights[static_cast<size_t>(vec_offset(N) + i)];
+    }
+    for (int i = 0; i < n * n; ++i) c.dhat[i] = h_dhat[static_cast<size_t>(mat_offset(N) + i)];
+    return c;
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers.
 
 template <int N, bool S>
 static cudaError_t launch_stage_t(const StageArgs& a, cudaStream_t stream) {
     using T = Tile<N>;
     const dim3 grid(static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
-    stage_kernel<N, S><<<grid, T::kThreads, T::kBytes, stream>>>(a);
+    stage_kernel<N, S><<<grid, T::kThreads, T::kBytes, stream>>>(a, make_coeffs<N>());
     return cudaGetLastError();
 }
 
@@ -652,6 +642,12 @@ cudaError_t upload_tables(const Tables& t) {
         }
         for (int i = 0; i < n * n; ++i) dhat[static_cast<size_t>(mat_offset(N) + i)] = t.get(NDG_TABLE_DERIVATIVE_MATRICES_HAT, N)[static_cast<size_t>(i)];
     }
+    h_nodes = nodes;
+    h_weights = weights;
+    h_inv_weights = inv_w;
+    h_ll = ll;
+    h_lr = lr;
+    h_dhat = dhat;
     cudaError_t err;
     if ((err = cudaMemcpyToSymbol(c_nodes, nodes.data(), sizeof(double) * kVecTotal)) != cudaSuccess) return err;
     if ((err = cudaMemcpyToSymbol(c_weights, weights.data(), sizeof(double) * kVecTotal)) != cudaSuccess) return err;
