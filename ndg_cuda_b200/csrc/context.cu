@@ -338,7 +338,15 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
     const size_t K = static_cast<size_t>(c->K);
     if (!l.general) {
         if (c->N > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "orders above 16 have no compiled kernel");
-        const SidePlan plan = build_side_plan(c->topo, c->tables);
+        SidePlan plan = build_side_plan(c->topo, c->tables);
+        // Tiles copy an even number of elements: pad the per-element arrays
+        // to the even element count (the pad element has no sides).
+        const size_t Kpad = static_cast<size_t>(c->Kp);
+        plan.corners.resize(8 * Kpad, 0.0);
+        plan.link.resize(8 * Kpad, static_cast<int32_t>(kZero << 2));
+        plan.normal.resize(8 * Kpad, 0.0);
+        plan.gscale.resize(4 * Kpad, 0.0);
+        plan.inflow_xy.resize(16 * Kpad, 0.0);
         const size_t n = static_cast<size_t>(c->N + 1);
         c->tr[0].allocate(inst * 3 * static_cast<size_t>(c->Kp) * 4 * n);
         c->tr[1].allocate(inst * 3 * static_cast<size_t>(c->Kp) * 4 * n);
