@@ -266,6 +266,39 @@ def run_ours(args) -> None:
     e2e_value = world * dof * 3 * CONFIG_STEPS * e2e_steps / (float(e2e_t.item()) / 1e3) if e2e_steps else None
     state_bytes = 3 * mesh.field_size * 8
 
+    # FP32 form on the same workload: throughput, kernel time, and its error
+    # against this FP64 run after the configuration's 2000 steps from the
+    # same initial condition.
+    fp32 = None
+    if not args.no_fp32:
+        m32 = ndg.Mesh2D_t(zone, ORDER, cfl=CFL, device=local, stream=stream.cuda_stream, precision=ndg.FP32)
+        m32.initial_conditions()
+        ndg.Solver2D_t.run(m32, args.warmup)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        ndg.Solver2D_t.run(m32, args.steps)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        f_ms = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(f_ms, op=dist.ReduceOp.MAX)
+        stage32_ms = m32.time_stage(1, 30)
+        m32.initial_conditions()
+        mesh.initial_conditions()
+        ndg.Solver2D_t.run(m32, CONFIG_STEPS)
+        ndg.Solver2D_t.run(mesh, CONFIG_STEPS)
+        err = {}
+        for f in ("p", "u", "v"):
+            a64, a32 = mesh.get_field(f), m32.get_field(f)
+            err[f] = float(((a32 - a64) ** 2).sum() ** 0.5 / max((a64 ** 2).sum() ** 0.5, 1e-300))
+        fp32 = {"value": world * dof * 3 * args.steps / (float(f_ms.item()) / 1e3), "unit": "DOF-stage updates/s",
+                "ms_per_step": float(f_ms.item()) / args.steps, "kernel": f"stage_kernel_f32<{ORDER}>", "kernel_ms": stage32_ms,
+                "roofline_frac": BYTES_PER_DOF_STAGE * dof / (stage32_ms / 1e3) / 1e9 / peak,
+                "rel_l2_vs_fp64": err, "steps_compared": CONFIG_STEPS,
+                "arithmetic": "traces, fluxes, metrics and volume term in FP32; q, k and the RK update in FP64"}
+        m32.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(float(os.environ.get("NDG_CPU_BUDGET_S", "15")), 1000, 1)
@@ -283,6 +316,7 @@ def run_ours(args) -> None:
                              "traffic": traffic, "kernel": f"stage_kernel<{ORDER}, false>", "kernel_ms": stage_ms,
                              "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof, "peak_source": peak_kind},
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "fp32": fp32,
                 "gpu_launches": launches,
                 "clocks": clocks.summary()}
         print(json.dumps(line), flush=True)
@@ -300,6 +334,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference timing (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg (profiling runs)")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-form leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

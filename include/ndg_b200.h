@@ -45,8 +45,10 @@ typedef struct ndg_ctx ndg_ctx;
  * NDG_FP64_STRICT: FP64 rounded operation by operation in the reference's
  *   order (no contraction, true divisions): bit-identical to the reference's
  *   CPU path on the same inputs.
- * NDG_FP32: volume, surface and flux arithmetic in FP32, solution and RK
- *   register kept in FP64. */
+ * NDG_FP32: traces, fluxes, metrics and the volume term in FP32 (traces
+ *   stored in FP32); the solution, the RK register and the RK update stay
+ *   FP64. Meshes of one order; after adaptation stepping returns
+ *   NDG_ERR_UNSUPPORTED. */
 typedef enum ndg_precision { NDG_FP64 = 0, NDG_FP64_STRICT = 1, NDG_FP32 = 2 } ndg_precision;
 
 /* Tables of NDG_t (include/entities/NDG_t.cuh:11-29). */

@@ -94,6 +94,7 @@ struct ndg_ctx {
     int64_t block = 0;       // values per device field block: Kp (N+1)^2
 
     ndg::DeviceBuffer<double> q, k, G, tr[2], corners, normal, gscale, inflow, dxy, step, scratch;
+    ndg::DeviceBuffer<float> tr32[2];  // traces of the FP32 form
     ndg::DeviceBuffer<int32_t> link, elem_N;
     ndg::DeviceBuffer<unsigned> error;
     ndg::DeviceBuffer<double> p_error, p_sigma;
@@ -165,6 +166,8 @@ dev::StageArgs stage_args(ndg_ctx* c, int m, int in) {
     a.k = c->k.ptr;
     a.trace_in = c->tr[in].ptr;
     a.trace_out = c->tr[1 - in].ptr;
+    a.trace_in_f = c->tr32[in].ptr;
+    a.trace_out_f = c->tr32[1 - in].ptr;
     a.G_out = c->keep_derivative ? c->G.ptr : nullptr;
     a.corners = c->corners.ptr;
     a.link = reinterpret_cast<const int2*>(c->link.ptr);
@@ -207,12 +210,24 @@ int64_t general_stage_launches(const ndg_ctx* c) {
     return 2 * static_cast<int64_t>(c->groups.size()) + ghosts + 1;
 }
 
+bool fp32(const ndg_ctx* c) { return c->precision == NDG_FP32; }
+
 cudaError_t issue_stage(ndg_ctx* c, int m, int in) {
-    if (c->general) return dev::launch_general_stage(general_args(c, m), c->groups.data(), static_cast<int>(c->groups.size()), strict(c), c->stream);
+    if (c->general) {
+        if (fp32(c)) return cudaErrorNotSupported;  // rejected by require_form before any capture
+        return dev::launch_general_stage(general_args(c, m), c->groups.data(), static_cast<int>(c->groups.size()), strict(c), c->stream);
+    }
+    if (fp32(c)) return dev::launch_stage_f32(c->N, stage_args(c, m, in), c->stream);
     return dev::launch_stage(c->N, strict(c), stage_args(c, m, in), c->stream);
 }
 
+// The FP32 form runs the uniform-order kernels only.
+void require_form(const ndg_ctx* c) {
+    if (c->general && fp32(c)) fail(NDG_ERR_UNSUPPORTED, "the FP32 form covers meshes of one order; this mesh has been adapted");
+}
+
 void launch_stage(ndg_ctx* c, int m) {
+    require_form(c);
     check_cuda(issue_stage(c, m, c->cur), "stage kernel launch");
     if (c->general) {
         c->launches += general_stage_launches(c);
@@ -224,8 +239,23 @@ void launch_stage(ndg_ctx* c, int m) {
 
 void ensure_traces(ndg_ctx* c) {
     if (c->traces_valid || c->general) return;
-    dev::TraceArgs a{c->q.ptr, c->tr[c->cur].ptr, c->K, c->Kp, c->n_instances};
-    check_cuda(dev::launch_traces(c->N, strict(c), a, c->stream), "trace kernel launch");
+    dev::TraceArgs a{};
+    a.q = c->q.ptr;
+    a.trace_out = c->tr[c->cur].ptr;
+    a.n_elements = c->K;
+    a.field_stride = c->Kp;
+    a.n_instances = c->n_instances;
+    if (fp32(c)) {
+        // FP32 traces are allocated the first time the form runs on this mesh.
+        const size_t count = c->tr[0].count;
+        for (auto& t : c->tr32)
+            if (t.count != count) t.allocate(count);
+        a.trace_out_f = c->tr32[c->cur].ptr;
+        check_cuda(dev::prepare_kernels_f32(c->N), "kernel attributes");
+        check_cuda(dev::launch_traces_f32(c->N, a, c->stream), "trace kernel launch");
+    } else {
+        check_cuda(dev::launch_traces(c->N, strict(c), a, c->stream), "trace kernel launch");
+    }
     ++c->launches;
     c->traces_valid = true;
 }
@@ -240,6 +270,7 @@ void set_step(ndg_ctx* c, double time, double dt, double t_end) {
 // uniform path alternates two trace buffers, so it has one graph per parity;
 // the general path has one.
 void ensure_graphs(ndg_ctx* c) {
+    require_form(c);
     const int n_graphs = c->general ? 1 : 2;
     if (c->graph[0] && (n_graphs == 1 || c->graph[1])) return;
     for (int parity = 0; parity < n_graphs; ++parity) {
@@ -365,6 +396,8 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
             if (Ne < 1 || Ne > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "element orders must lie in 1..16");
         c->tr[0].release();
         c->tr[1].release();
+        c->tr32[0].release();
+        c->tr32[1].release();
         c->gplan = build_general_plan(c->topo);
         const GeneralPlan& g = c->gplan;
         c->g_eN.upload(g.eN, c->stream);
@@ -571,9 +604,11 @@ ndg_status ndg_ctx_destroy(ndg_ctx* ctx) {
 ndg_status ndg_ctx_set_precision(ndg_ctx* ctx, int32_t precision) {
     return guarded([&] {
         if (!ctx) fail(NDG_ERR_INVALID_ARG, "ctx is NULL");
-        if (precision == NDG_FP32) fail(NDG_ERR_UNSUPPORTED, "the FP32 form is not built yet");
-        if (precision != NDG_FP64 && precision != NDG_FP64_STRICT) fail(NDG_ERR_INVALID_ARG, "unknown precision");
-        if (ctx->precision != precision) drop_graphs(ctx);
+        if (precision != NDG_FP64 && precision != NDG_FP64_STRICT && precision != NDG_FP32) fail(NDG_ERR_INVALID_ARG, "unknown precision");
+        if (ctx->precision != precision) {
+            drop_graphs(ctx);
+            ctx->traces_valid = false;  // the forms keep their traces in different buffers
+        }
         ctx->precision = precision;
     });
 }

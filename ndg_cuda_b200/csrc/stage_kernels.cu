@@ -436,6 +436,313 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) stage_kernel(StageArgs a, c
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 form of the stage (uniform order, conforming faces): traces, fluxes,
+// metrics and the volume term in FP32 with FMA contraction; q and k stay
+// FP64 in HBM and the RK update runs in FP64, so only the stage's time
+// derivative G carries FP32 rounding. Traces are stored in FP32, halving
+// their traffic.
+template <int N>
+struct CoeffsF {
+    float dhat[(N + 1) * (N + 1)];
+    float xn[N + 1], lm[N + 1], lp[N + 1], w[N + 1], iw[N + 1];
+};
+
+template <int N>
+struct TileF {
+    static constexpr int n = N + 1;
+    static constexpr int NN = n * n;
+    static constexpr int EPB = Tile<N>::EPB;
+    static constexpr int kThreads = Tile<N>::kThreads;
+    static constexpr int kNodeIters = Tile<N>::kNodeIters;
+    // the bulk-copied FP64 q tile, then FP32 arrays (offsets in floats past it)
+    static constexpr int kQd = 3 * EPB * NN;             // doubles
+    static constexpr int kQf = 0;                        // [3][EPB][NN] q in FP32
+    static constexpr int kG = kQf + 3 * EPB * NN;        // [3][EPB][NN]
+    static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n]
+    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far traces, then side fluxes
+    static constexpr int kJ = kFar + 3 * EPB * 4 * n;    // [EPB][NN] 1/J
+    static constexpr int kS = kJ + EPB * NN;             // [EPB][4]
+    static constexpr int kZ = kS + EPB * 4;              // [NN] zeros
+    static constexpr int kFloats = (kZ + NN + 3) / 4 * 4;  // keeps the mbarrier 16-byte aligned
+    static constexpr size_t kBytes = sizeof(double) * kQd + sizeof(float) * kFloats + 16;
+};
+
+// ((1 - t) d0 + (1 + t) d1) / 4 as fma(t, (d1 - d0) / 4, (d0 + d1) / 4) in FP32.
+struct MetricLineF {
+    float a, b;
+    __device__ __forceinline__ MetricLineF(float d0, float d1) : a(0.25f * (d0 + d1)), b(0.25f * (d1 - d0)) {}
+    __device__ __forceinline__ float operator()(float t) const { return fmaf(t, b, a); }
+};
+
+template <int N>
+__global__ void __launch_bounds__(TileF<N>::kThreads) stage_kernel_f32(StageArgs a, const __grid_constant__ CoeffsF<N> cf) {
+    using T = TileF<N>;
+    constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
+    extern __shared__ __align__(128) double smem[];
+    double* qs = smem;
+    float* fsm = reinterpret_cast<float*>(smem + T::kQd);
+    float* qf = fsm + T::kQf;
+    float* gs = fsm + T::kG;
+    float* own_s = fsm + T::kOwn;
+    float* far_s = fsm + T::kFar;
+    float* js = fsm + T::kJ;
+    float* ss = fsm + T::kS;
+    float* zs = fsm + T::kZ;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(fsm + T::kFloats);
+    constexpr int FS = EPB * 4 * n;
+
+    const int tid = threadIdx.x;
+    const int64_t K = a.n_elements;
+    const int64_t Kp = a.field_stride;
+    const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
+    const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
+    const int ne_copy = (ne + 1) & ~1;
+    const int64_t inst = blockIdx.y;
+    double* q = a.q + inst * 3 * Kp * NN;
+    double* k = a.k + inst * 3 * Kp * NN;
+    const float* tr_in = a.trace_in_f + inst * 3 * Kp * 4 * n;
+    float* tr_out = a.trace_out_f + inst * 3 * Kp * 4 * n;
+    const float* xn = cf.xn;
+    const float* lm = cf.lm;
+    const float* lp = cf.lp;
+    const double time = a.step[0];
+    const double dt = a.step[1];
+
+    const int f = tid / (EPB * n);
+    const int rr = tid - f * (EPB * n);
+    const int e = rr / n;
+    const int m = rr - e * n;
+    const bool active = f < 3 && e < ne;
+    const int64_t ge = e0 + e;
+
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+        const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
+        mbar_expect_tx(bar, 3 * bytes);
+        for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
+    }
+    for (int i = tid; i < NN; i += T::kThreads) zs[i] = 0.0f;
+    float x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    if (active) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int2 lk = a.link[4 * ge + s];
+            const float v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0f;
+            far_s[f * FS + (e * 4 + s) * n + m] = v;
+        }
+        const double* c = a.corners + 8 * ge;
+        x0 = static_cast<float>(c[0]); y0 = static_cast<float>(c[1]); x1 = static_cast<float>(c[2]); y1 = static_cast<float>(c[3]);
+        x2 = static_cast<float>(c[4]); y2 = static_cast<float>(c[5]); x3 = static_cast<float>(c[6]); y3 = static_cast<float>(c[7]);
+    }
+    const MetricLineF x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
+    const MetricLineF x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
+    if (active) {
+        const float tm = xn[m];
+        if (f == 2) {
+            for (int sd = m; sd < 4; sd += n) {
+                const float at = (sd == 0 || sd == 3) ? -1.0f : 1.0f;
+                const float dx = (sd == 0 || sd == 2) ? x_xi(at) : x_eta(at);
+                const float dy = (sd == 0 || sd == 2) ? y_xi(at) : y_eta(at);
+                ss[e * 4 + sd] = sqrtf(dx * dx + dy * dy);
+            }
+        }
+        const float xe = x_eta(tm), ye = y_eta(tm);
+        for (int j = f; j < n; j += 3) {
+            const float tj = xn[j];
+            js[e * NN + m * n + j] = __frcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
+        }
+    }
+    __syncthreads();
+    if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
+    for (int i = tid; i < 3 * EPB * NN; i += T::kThreads) qf[i] = static_cast<float>(qs[i]);
+    __syncthreads();
+
+    const float* Qe = qf + e * NN;
+    const float* Xe = f == 0 ? Qe + 1 * EPB * NN : (f == 1 ? Qe : zs);
+    const float* Ye = f == 0 ? Qe + 2 * EPB * NN : (f == 1 ? zs : Qe);
+    if (active) {
+        const float* Qf = Qe + f * EPB * NN;
+        float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            const float qr = Qf[m * n + j], qc = Qf[j * n + m];
+            b = fmaf(lm[j], qr, b);
+            t = fmaf(lp[j], qr, t);
+            r = fmaf(lp[j], qc, r);
+            l = fmaf(lm[j], qc, l);
+        }
+        float* o = own_s + f * FS + e * 4 * n;
+        o[0 * n + m] = b;
+        o[2 * n + (N - m)] = t;
+        o[1 * n + m] = r;
+        o[3 * n + (N - m)] = l;
+    }
+    __syncthreads();
+
+    if (active) {
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1 && f != 0) break;
+            const int s = pass == 0 ? f : 3;
+            const int2 lk = a.link[4 * ge + s];
+            const int kind = (lk.y >> 2) & 7;
+            const int role = (lk.y >> 5) & 1;
+            const double2 nvd = a.normal[4 * ge + s];
+            const float nx = static_cast<float>(nvd.x), ny = static_cast<float>(nvd.y);
+            const int o = (e * 4 + s) * n + m;
+            const float op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
+            float fp_, fu_, fv_;
+            if (kind == kInterior) {
+                fp_ = far_s[o];
+                fu_ = far_s[FS + o];
+                fv_ = far_s[2 * FS + o];
+            } else if (kind == kMirror || kind == kCopy) {
+                const float gsc = static_cast<float>(a.gscale[4 * ge + s]);
+                fp_ = op * gsc;
+                const float gu = ou * gsc, gv = ov * gsc;
+                if (kind == kMirror) {
+                    const float tx = -ny, ty = nx;
+                    const float l0 = -(gu * nx + gv * ny);
+                    const float l1 = gu * tx + gv * ty;
+                    fu_ = nx * l0 + tx * l1;
+                    fv_ = ny * l0 + ty * l1;
+                } else {
+                    fu_ = gu;
+                    fv_ = gv;
+                }
+            } else if (kind == kAnalytic) {
+                const double4 gq = a.inflow[4 * ge + s];
+                const double rr2 = (static_cast<double>(xn[N - m]) + 1.0) * 0.5;
+                double pd, ud, vd;
+                plane_wave(gq.z * rr2 + gq.x * (1.0 - rr2), gq.w * rr2 + gq.y * (1.0 - rr2), time + a.rk_b * dt, pd, ud, vd);
+                fp_ = static_cast<float>(pd);
+                fu_ = static_cast<float>(ud);
+                fv_ = static_cast<float>(vd);
+            } else {
+                fp_ = fu_ = fv_ = 0.0f;
+            }
+            const float Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
+            const float Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
+            const float wL = Lp + (Lu * nx + Lv * ny);
+            const float wR = Rp - (Ru * nx + Rv * ny);
+            const float sum = wL + wR;
+            const float sf = ss[e * 4 + s] * 0.5f;
+            far_s[o] = (role ? -(wL - wR) : (wL - wR)) * sf;
+            far_s[FS + o] = (role ? -nx : nx) * sum * sf;
+            far_s[2 * FS + o] = (role ? -ny : ny) * sum * sf;
+        }
+    }
+    __syncthreads();
+
+    const float* Dh = cf.dhat;
+    const float* iw = cf.iw;
+    const float* F = far_s + f * FS + e * 4 * n;
+    if (active) {
+        const int j = m;
+        float col[n];
+#pragma unroll
+        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * Xe[i * n + j] - x_eta(xn[i]) * Ye[i * n + j];
+        const float fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
+        float* G = gs + (f * EPB + e) * NN + j;
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[i * n + mm], col[mm], acc);
+            G[i * n] = -(acc + (fr * lp[i] + fl3 * lm[i]) * iw[i]);
+        }
+    }
+    __syncthreads();
+
+    if (active) {
+        const int i = m;
+        float line[n];
+#pragma unroll
+        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * Xe[i * n + j] + x_xi(xn[j]) * Ye[i * n + j];
+        const float ft = F[2 * n + (N - i)], fb = F[0 * n + i];
+        float* G = gs + (f * EPB + e) * NN + i * n;
+        const float* jrow = js + e * NN + i * n;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[j * n + mm], line[mm], acc);
+            G[j] = (G[j] - (acc + (ft * lp[j] + fb * lm[j]) * iw[j])) * jrow[j];
+        }
+    }
+    __syncthreads();
+
+    // RK3 update in FP64 (Solver2D_t.cpp:138-172); the new q also refreshes
+    // the FP32 tile for the traces.
+    const double gdt = a.rk_g * dt;
+    double kold[T::kNodeIters];
+#pragma unroll
+    for (int c = 0; c < T::kNodeIters; ++c) {
+        const int idx = tid + c * T::kThreads;
+        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
+        kold[c] = (!a.first && ff < 3 && r < ne * NN) ? k[(ff * Kp + e0) * NN + r] : 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < T::kNodeIters; ++c) {
+        const int idx = tid + c * T::kThreads;
+        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
+        if (ff < 3 && r < ne * NN) {
+            const double G = static_cast<double>(gs[ff * EPB * NN + r]);
+            const double kn = a.first ? G : fma(a.rk_a, kold[c], G);
+            const double qn = fma(gdt, kn, qs[ff * EPB * NN + r]);
+            const int64_t gi = (ff * Kp + e0) * NN + r;
+            k[gi] = kn;
+            q[gi] = qn;
+            qf[ff * EPB * NN + r] = static_cast<float>(qn);
+            if (a.G_out) a.G_out[inst * 3 * Kp * NN + gi] = G;
+        }
+    }
+    __syncthreads();
+
+    if (active) {
+        const float* row = qf + (f * EPB + e) * NN + m * n;
+        const float* cl = qf + (f * EPB + e) * NN + m;
+        float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            b = fmaf(lm[j], row[j], b);
+            t = fmaf(lp[j], row[j], t);
+            r = fmaf(lp[j], cl[j * n], r);
+            l = fmaf(lm[j], cl[j * n], l);
+        }
+        float* to = tr_out + (f * Kp + ge) * 4 * n;
+        to[0 * n + m] = b;
+        to[2 * n + (N - m)] = t;
+        to[1 * n + m] = r;
+        to[3 * n + (N - m)] = l;
+    }
+}
+
+// Side traces in FP32 (start of a run, or after the host changed q).
+template <int N>
+__global__ void __launch_bounds__(256) trace_kernel_f32(TraceArgs a) {
+    constexpr int n = N + 1, NN = n * n;
+    const int64_t K = a.n_elements, Kp = a.field_stride;
+    const int64_t total = static_cast<int64_t>(a.n_instances) * 3 * K * 4 * n;
+    const double* lm = c_lagrange_left + vec_offset(N);
+    const double* lp = c_lagrange_right + vec_offset(N);
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total; idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int m = static_cast<int>(idx % n);
+        const int s = static_cast<int>((idx / n) % 4);
+        const int64_t e = (idx / (4 * n)) % K;
+        const int64_t fi = idx / (4 * n * K);
+        const double* qe = a.q + (fi * Kp + e) * NN;
+        const double* l = (s == 0 || s == 3) ? lm : lp;
+        const int line = (s < 2) ? m : N - m;
+        const int base = (s == 0 || s == 2) ? line * n : line;
+        const int stride = (s == 0 || s == 2) ? 1 : n;
+        float acc = 0.0f;
+        for (int j = 0; j < n; ++j) acc = fmaf(static_cast<float>(l[j]), static_cast<float>(qe[base + j * stride]), acc);
+        a.trace_out_f[((fi * Kp + e) * 4 + s) * n + m] = acc;
+    }
+}
+
 // Side traces only (start of a run, or after the host changed q).
 template <int N, bool S>
 __global__ void __launch_bounds__(256) trace_kernel(TraceArgs a) {
@@ -589,6 +896,42 @@ static int epb_t() {
         default: break;                                                                   \
     }
 
+template <int N>
+static CoeffsF<N> make_coeffs_f() {
+    const Coeffs<N> d = make_coeffs<N>();
+    CoeffsF<N> c;
+    for (int i = 0; i < (N + 1) * (N + 1); ++i) c.dhat[i] = static_cast<float>(d.dhat[i]);
+    for (int i = 0; i <= N; ++i) {
+        c.xn[i] = static_cast<float>(d.xn[i]);
+        c.lm[i] = static_cast<float>(d.lm[i]);
+        c.lp[i] = static_cast<float>(d.lp[i]);
+        c.w[i] = static_cast<float>(d.w[i]);
+        c.iw[i] = static_cast<float>(d.iw[i]);
+    }
+    return c;
+}
+
+template <int N, bool Unused>
+static cudaError_t prepare_f32_t() {
+    return cudaFuncSetAttribute(stage_kernel_f32<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(TileF<N>::kBytes));
+}
+
+template <int N, bool Unused>
+static cudaError_t launch_stage_f32_t(const StageArgs& a, cudaStream_t stream) {
+    using T = TileF<N>;
+    const dim3 grid(static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
+    stage_kernel_f32<N><<<grid, T::kThreads, T::kBytes, stream>>>(a, make_coeffs_f<N>());
+    return cudaGetLastError();
+}
+
+template <int N, bool Unused>
+static cudaError_t launch_trace_f32_t(const TraceArgs& a, cudaStream_t stream) {
+    const int64_t total = static_cast<int64_t>(a.n_instances) * 3 * a.n_elements * 4 * (N + 1);
+    const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 32));
+    trace_kernel_f32<N><<<blocks, 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t prepare_kernels(int N, bool strict) {
     NDG_DISPATCH_ORDER(prepare_t, N, strict)
     return cudaErrorInvalidValue;
@@ -601,6 +944,21 @@ cudaError_t launch_stage(int N, bool strict, const StageArgs& a, cudaStream_t st
 
 cudaError_t launch_traces(int N, bool strict, const TraceArgs& a, cudaStream_t stream) {
     NDG_DISPATCH_ORDER(launch_trace_t, N, strict, a, stream)
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t prepare_kernels_f32(int N) {
+    NDG_DISPATCH_ORDER(prepare_f32_t, N, false)
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_stage_f32(int N, const StageArgs& a, cudaStream_t stream) {
+    NDG_DISPATCH_ORDER(launch_stage_f32_t, N, false, a, stream)
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_traces_f32(int N, const TraceArgs& a, cudaStream_t stream) {
+    NDG_DISPATCH_ORDER(launch_trace_f32_t, N, false, a, stream)
     return cudaErrorInvalidValue;
 }
 

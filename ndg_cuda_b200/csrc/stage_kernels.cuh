@@ -18,6 +18,8 @@ struct StageArgs {
     double* k;
     const double* trace_in;
     double* trace_out;
+    const float* trace_in_f;  // FP32 form: traces kept in FP32
+    float* trace_out_f;
     double* G_out;  // optional copy of the stage's time derivative
     const double* corners;
     const int2* link;
@@ -36,6 +38,7 @@ struct StageArgs {
 struct TraceArgs {
     const double* q;
     double* trace_out;
+    float* trace_out_f;  // FP32 form
     int64_t n_elements;
     int64_t field_stride;
     int n_instances;
@@ -44,6 +47,11 @@ struct TraceArgs {
 cudaError_t prepare_kernels(int N, bool strict);
 cudaError_t launch_stage(int N, bool strict, const StageArgs& a, cudaStream_t stream);
 cudaError_t launch_traces(int N, bool strict, const TraceArgs& a, cudaStream_t stream);
+// FP32 form: volume, surface and flux arithmetic in FP32, traces in FP32, the
+// RK update of q and k in FP64.
+cudaError_t prepare_kernels_f32(int N);
+cudaError_t launch_stage_f32(int N, const StageArgs& a, cudaStream_t stream);
+cudaError_t launch_traces_f32(int N, const TraceArgs& a, cudaStream_t stream);
 cudaError_t launch_initial_conditions(double* q, double* k, const double* corners, int N, int64_t K, int64_t Kp, int n_instances, cudaStream_t stream);
 cudaError_t launch_delta_t(const double* delta_xy_min, const int* elem_N, int64_t K, double cfl, double* out, cudaStream_t stream);
 cudaError_t launch_end_step(double* step, cudaStream_t stream);
