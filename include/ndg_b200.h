@@ -162,6 +162,14 @@ ndg_status ndg_mesh_get_faces(const ndg_ctx* ctx, int64_t* nodes, int64_t* eleme
                               double* normal, double* tangent, double* offset, double* scale);
 ndg_status ndg_mesh_get_elements(const ndg_ctx* ctx, int64_t* nodes, int32_t* N, double* delta_xy_min, int64_t* first_face);
 ndg_status ndg_mesh_get_boundary(const ndg_ctx* ctx, int32_t list, int64_t* out, int64_t capacity, int64_t* count);
+/* Per element (domain and ghosts): Element2D_t::split_level_, status_
+ * (Hilbert H, A, R, B = 0..3) and rotation_ (include/entities/Element2D_t.h),
+ * and the number of faces on each of its 4 sides (faces_[s].size()). Any
+ * pointer may be NULL. */
+ndg_status ndg_mesh_get_element_state(const ndg_ctx* ctx, int32_t* split_level, int32_t* status, int32_t* rotation, int32_t* n_faces_side);
+/* The faces of every element side, element by element and side by side
+ * (Element2D_t::faces_), into out[capacity]; *count = total number. */
+ndg_status ndg_mesh_get_element_faces(const ndg_ctx* ctx, int64_t* out, int64_t capacity, int64_t* count);
 ndg_status ndg_mesh_get_nodes(const ndg_ctx* ctx, double* xy);
 /* Degrees of freedom per field and instance: sum over elements of (N+1)^2. */
 ndg_status ndg_mesh_field_size(const ndg_ctx* ctx, int64_t* n_values);
@@ -208,9 +216,17 @@ ndg_status ndg_get_error(ndg_ctx* ctx, int32_t instance, double* p_error, double
  * boundary and interface ghosts and faces take their neighbours' orders
  * (adjust_boundaries, adjust_interfaces, adjust_faces, :7482-7538). Later
  * steps run the mixed-order (mortar) stage path. Needs one instance.
- * Element splitting (h-refinement, max_split_level > 0 with p_sigma_ < 1)
- * returns NDG_ERR_UNSUPPORTED. The estimate is consumed. */
+ * Elements with refine_, p_sigma_ < 1 and split_level_ < max_split_level
+ * split in four (see ndg_adapt_flags). The estimate is consumed. */
 ndg_status ndg_adapt(ndg_ctx* ctx);
+/* The same adaptation from caller-given refine_ flags and p_sigma_ decay
+ * rates, one per domain element (the element state Mesh2D_t::adapt reads).
+ * Element splitting (h-refinement) follows the reference's rules and
+ * numbering: hp_adapt, split_faces, split_boundaries and split_interfaces
+ * (src/meshes/Mesh2D_t.cpp:5186-6757); children take their solution by
+ * interpolation from the parent (Element2D_t.cpp:345-463). On a host-only
+ * context (device < 0) only the topology is adapted. */
+ndg_status ndg_adapt_flags(ndg_ctx* ctx, const int32_t* refine, const double* p_sigma);
 
 /* Benchmark aid: launches stage m n_launches times back to back (the state
  * advances), timing each launch with CUDA events on the context's stream;

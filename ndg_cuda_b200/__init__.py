@@ -76,6 +76,8 @@ def lib() -> C.CDLL:
         "ndg_mesh_get_elements": ([vp] * 5, C.c_int),
         "ndg_mesh_get_boundary": ([vp, i32, vp, i64, C.POINTER(i64)], C.c_int),
         "ndg_mesh_get_nodes": ([vp, vp], C.c_int),
+        "ndg_mesh_get_element_state": ([vp, vp, vp, vp, vp], C.c_int),
+        "ndg_mesh_get_element_faces": ([vp, vp, i64, C.POINTER(i64)], C.c_int),
         "ndg_mesh_field_size": ([vp, C.POINTER(i64)], C.c_int),
         "ndg_initial_conditions": ([vp], C.c_int),
         "ndg_set_field": ([vp, i32, i32, vp], C.c_int),
@@ -90,6 +92,7 @@ def lib() -> C.CDLL:
         "ndg_estimate_error": ([vp], C.c_int),
         "ndg_get_error": ([vp, i32, vp, vp, vp, vp], C.c_int),
         "ndg_adapt": ([vp], C.c_int),
+        "ndg_adapt_flags": ([vp, vp, vp], C.c_int),
         "ndg_delta_t_from_device": ([vp, vp, i64, dbl, vp, C.POINTER(dbl)], C.c_int),
     }
     for name, (args, res) in sigs.items():
@@ -279,9 +282,15 @@ class Mesh2D_t:
         _check(lib().ndg_get_error(self._ctx.h, instance, *[_ptr(d[k]) for k in ("p_error", "p_sigma", "refine", "coarsen")]))
         return d
 
-    def adapt(self) -> None:
-        """Mesh2D_t::adapt from the last error estimate (p-refinement)."""
-        _check(lib().ndg_adapt(self._ctx.h))
+    def adapt(self, refine: np.ndarray | None = None, p_sigma: np.ndarray | None = None) -> None:
+        """Mesh2D_t::adapt: from the last error estimate, or from the given
+        per-element refine flags and decay rates."""
+        if refine is None:
+            _check(lib().ndg_adapt(self._ctx.h))
+        else:
+            r = np.ascontiguousarray(refine, dtype=np.int32)
+            sg = np.ascontiguousarray(p_sigma, dtype=np.float64)
+            _check(lib().ndg_adapt_flags(self._ctx.h, _ptr(r), _ptr(sg)))
         counts = [C.c_int64() for _ in range(4)]
         _check(lib().ndg_mesh_counts(self._ctx.h, *[C.byref(c) for c in counts]))
         self.n_elements_, self.n_elements_total_, self.n_faces_, self.n_nodes_ = (c.value for c in counts)
@@ -318,6 +327,20 @@ class Mesh2D_t:
         d = {"nodes": np.empty(4 * E, dtype=np.int64), "N": np.empty(E, dtype=np.int32), "delta_xy_min": np.empty(E),
              "first_face": np.empty(4 * E, dtype=np.int64)}
         _check(lib().ndg_mesh_get_elements(self._ctx.h, *[_ptr(d[k]) for k in ("nodes", "N", "delta_xy_min", "first_face")]))
+        return d
+
+    def element_state(self) -> dict:
+        """split_level, status, rotation and faces per side of every element,
+        with the face lists concatenated side by side."""
+        E = self.n_elements_total_
+        d = {"split_level": np.empty(E, dtype=np.int32), "status": np.empty(E, dtype=np.int32),
+             "rotation": np.empty(E, dtype=np.int32), "n_faces_side": np.empty(4 * E, dtype=np.int32)}
+        _check(lib().ndg_mesh_get_element_state(self._ctx.h, *[_ptr(d[k]) for k in ("split_level", "status", "rotation", "n_faces_side")]))
+        cnt = C.c_int64()
+        _check(lib().ndg_mesh_get_element_faces(self._ctx.h, None, 0, C.byref(cnt)))
+        d["faces"] = np.empty(max(cnt.value, 1), dtype=np.int64)
+        _check(lib().ndg_mesh_get_element_faces(self._ctx.h, _ptr(d["faces"]), d["faces"].size, C.byref(cnt)))
+        d["faces"] = d["faces"][:cnt.value]
         return d
 
     def boundary(self, kind: int) -> np.ndarray:

@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-I", os.path.join(HERE, "..", "include")]
 CUDA_FLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr", "-Xptxas", "-v"] if os.environ.get("NDG_PTXAS_VERBOSE") else ARCH + ["-lineinfo", "--expt-relaxed-constexpr"]
 
-SOURCES = ["tables.cpp", "topology.cpp", "adapt.cpp", "stage_kernels.cu", "general_kernels.cu", "estimator.cu", "context.cu",
+SOURCES = ["tables.cpp", "topology.cpp", "adapt.cpp", "adapt_h.cpp", "stage_kernels.cu", "general_kernels.cu", "estimator.cu", "context.cu",
            "delta_t_scratch.cu"]
 
 

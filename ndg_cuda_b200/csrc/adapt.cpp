@@ -3,9 +3,73 @@
 #include "ndg_internal.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 
 namespace ndg {
+
+namespace {
+constexpr double kPi = 3.14159265358979323846;
+enum HilbertStatus : int { kH = 0, kA = 1, kR = 2, kB = 3 };
+
+// Hilbert::deduct_*_element_status (src/functions/Hilbert_splitting.cpp:3-22):
+// the curve's shape in an element from the sides it enters and leaves by.
+int first_status(int outgoing) {
+    constexpr int t[4] = {kB, kH, kA, kR};
+    return t[outgoing];
+}
+int last_status(int incoming) {
+    constexpr int t[4] = {kA, kR, kB, kH};
+    return t[incoming];
+}
+int middle_status(int incoming, int outgoing) {
+    constexpr int t[4][4] = {{kH, kH, kA, kA}, {kB, kB, kR, kR}, {kB, kB, kR, kR}, {kH, kH, kA, kA}};
+    return t[incoming][outgoing];
+}
+
+// Side of an element through which the neighbouring centre lies.
+int side_towards(double dx, double dy) {
+    if (std::abs(dy) > std::abs(dx)) return dy < 0 ? 0 : 2;
+    return dx < 0 ? 3 : 1;
+}
+}  // namespace
+
+void init_adaptivity_state(Topology& t) {
+    const size_t total = t.elem_N.size();
+    const int64_t K = t.n_domain;
+    t.elem_split.assign(total, 0);
+    t.elem_status.assign(total, kA);
+    t.elem_rotation.assign(total, 0);
+    t.ghost_sf_zero.assign(total, 0);
+    t.elem_faces.assign(total, {});
+    for (size_t e = 0; e < total; ++e)
+        for (int s = 0; s < 4; ++s) {
+            const int64_t f = t.elem_face[e][static_cast<size_t>(s)];
+            if (f >= 0 && (static_cast<int64_t>(e) < K || s == 0)) t.elem_faces[e][static_cast<size_t>(s)].push_back(f);
+        }
+    // Mesh2D_t::compute_element_status (src/meshes/Mesh2D_t.cpp:4055-4178).
+    constexpr double targets[4] = {-3 * kPi / 4, -kPi / 4, kPi / 4, 3 * kPi / 4};
+    for (int64_t e = 0; e < K; ++e) {
+        const size_t ei = static_cast<size_t>(e);
+        long rotation = 0;
+        for (size_t i = 0; i < 4; ++i) {
+            const size_t nd = static_cast<size_t>(t.elem_nodes[ei][i]);
+            const double angle = std::atan2(t.node_y[nd] - t.center[ei][1], t.node_x[nd] - t.center[ei][0]);
+            const double offset = std::atan2(std::sin(angle - targets[i]), std::cos(angle - targets[i]));
+            const long turns = std::lround(offset * 2 / kPi + 4 * (offset < 0));
+            rotation += turns * (turns < 4);
+        }
+        t.elem_rotation[ei] = static_cast<int>(rotation / 4);
+        auto toward = [&](int64_t o) {
+            const size_t oi = static_cast<size_t>(o);
+            return side_towards(t.center[oi][0] - t.center[ei][0], t.center[oi][1] - t.center[ei][1]);
+        };
+        if (K == 1) t.elem_status[ei] = kH;
+        else if (e == 0) t.elem_status[ei] = first_status(toward(e + 1));
+        else if (e == K - 1) t.elem_status[ei] = last_status(toward(e - 1));
+        else t.elem_status[ei] = middle_status(toward(e - 1), toward(e + 1));
+    }
+}
 
 bool fused_path_applies(const Topology& t) {
     if (t.n_domain <= 0) return false;
@@ -17,6 +81,7 @@ bool fused_path_applies(const Topology& t) {
     for (int64_t e = 0; e < t.n_domain; ++e) {
         const auto& nd = t.elem_nodes[static_cast<size_t>(e)];
         for (int s = 0; s < 4; ++s) {
+            if (t.elem_faces[static_cast<size_t>(e)][static_cast<size_t>(s)].size() != 1) return false;
             const int64_t f = t.elem_face[static_cast<size_t>(e)][static_cast<size_t>(s)];
             if (f < 0) return false;
             const auto& fe = t.face_elems[static_cast<size_t>(f)];
@@ -63,10 +128,9 @@ GeneralPlan build_general_plan(const Topology& t) {
     for (int64_t e = 0; e < total; ++e) {
         for (int s = 0; s < 4; ++s) {
             p.enodes[static_cast<size_t>(4 * e + s)] = t.elem_nodes[static_cast<size_t>(e)][static_cast<size_t>(s)];
-            const int64_t f = t.elem_face[static_cast<size_t>(e)][static_cast<size_t>(s)];
-            const bool has = e < K ? f >= 0 : (s == 0 && f >= 0);
-            p.sface_start[static_cast<size_t>(4 * e + s + 1)] = p.sface_start[static_cast<size_t>(4 * e + s)] + (has ? 1 : 0);
-            if (has) p.sface.push_back(f);
+            const auto& list = t.elem_faces[static_cast<size_t>(e)][static_cast<size_t>(s)];
+            p.sface_start[static_cast<size_t>(4 * e + s + 1)] = p.sface_start[static_cast<size_t>(4 * e + s)] + static_cast<int64_t>(list.size());
+            p.sface.insert(p.sface.end(), list.begin(), list.end());
         }
     }
     p.corners.resize(static_cast<size_t>(8 * K));
@@ -137,10 +201,7 @@ GeneralPlan build_general_plan(const Topology& t) {
 // scaling factor included; that is kept.
 bool p_adapt(Topology& t, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level) {
     const int64_t K = t.n_domain;
-    for (int64_t e = 0; e < K; ++e) {
-        const bool h = refine[e] && p_sigma[e] < 1.0 && 0 < max_split_level;
-        if (h) fail(NDG_ERR_UNSUPPORTED, "h-adaptation (element splitting) is not available yet; set max_split_level to 0");
-    }
+    (void)max_split_level;  // element splitting is h_adapt's branch
     bool changed = false;
     for (int64_t e = 0; e < K; ++e) {
         int& N = t.elem_N[static_cast<size_t>(e)];
@@ -152,8 +213,7 @@ bool p_adapt(Topology& t, const int32_t* refine, const double* p_sigma, int N_ma
     for (int b = 0; b < 4; ++b)
         for (int64_t g : t.boundary[static_cast<size_t>(b)]) {
             int N_el = t.elem_N[static_cast<size_t>(g)];
-            const int64_t f = t.elem_face[static_cast<size_t>(g)][0];
-            if (f >= 0) {
+            for (int64_t f : t.elem_faces[static_cast<size_t>(g)][0]) {
                 const auto& fe = t.face_elems[static_cast<size_t>(f)];
                 const int64_t src = fe[fe[0] == g ? 1 : 0];
                 N_el = std::max(N_el, t.elem_N[static_cast<size_t>(src)]);
@@ -161,6 +221,7 @@ bool p_adapt(Topology& t, const int32_t* refine, const double* p_sigma, int N_ma
             if (t.elem_N[static_cast<size_t>(g)] != N_el) {
                 t.elem_N[static_cast<size_t>(g)] = N_el;
                 t.ghost_scale[static_cast<size_t>(g)][0] = 0.0;
+                t.ghost_sf_zero[static_cast<size_t>(g)] = 1;
                 changed = true;
             }
         }
@@ -170,6 +231,7 @@ bool p_adapt(Topology& t, const int32_t* refine, const double* p_sigma, int N_ma
         if (Nd != Ns) {
             Nd = Ns;
             t.ghost_scale[static_cast<size_t>(t.if_destination[i])][0] = 0.0;
+            t.ghost_sf_zero[static_cast<size_t>(t.if_destination[i])] = 1;
             changed = true;
         }
     }

@@ -500,6 +500,7 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
         }
     }
     compute_geometry(topo, c->tables);
+    init_adaptivity_state(topo);
     c->topo = std::move(topo);
     c->params = p;
     c->n_instances = n_instances;
@@ -527,6 +528,107 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     check_cuda(cudaMemsetAsync(c->error.ptr, 0, sizeof(unsigned), c->stream), "memset");
     upload_plan(c, l);
     compute_dt_mesh(c, p.cfl);
+}
+
+// Mesh2D_t::adapt from per-element refine flags and decay rates; moves the
+// fields of a device context to the new mesh.
+void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in) {
+    const std::vector<int32_t> refine(refine_in, refine_in + ctx->topo.n_domain);
+    const std::vector<double> sigma(sigma_in, sigma_in + ctx->topo.n_domain);
+    const Layout before = layout_of(ctx->topo);
+    Topology topo = ctx->topo;
+    // Mesh2D_t::adapt: element splitting when any element splits, the
+    // p-only branch otherwise.
+    std::vector<ElementSource> sources;
+    const bool split = h_adapt(topo, ctx->tables, refine.data(), sigma.data(), ctx->params.maximum_N, ctx->params.max_split_level, sources);
+    if (!split && !p_adapt(topo, refine.data(), sigma.data(), ctx->params.maximum_N, ctx->params.max_split_level)) {
+        ctx->has_error_estimate = false;
+        return;
+    }
+    const Layout after = layout_of(topo);
+    if (ctx->device < 0) {
+        // Host-only context: the topology alone.
+        ctx->topo = std::move(topo);
+        ctx->K = ctx->topo.n_domain;
+        ctx->Kp = ctx->K + (ctx->K & 1);
+        ctx->field_size = after.field_size;
+        ctx->block = after.block;
+        ctx->has_error_estimate = false;
+        return;
+    }
+    // Per new domain element: its source element's order and offset, and
+    // for children the node coordinates in the parent.
+    const size_t K_new = static_cast<size_t>(topo.n_domain);
+    std::vector<int32_t> oNv(K_new), mode(K_new);
+    std::vector<int64_t> oOffv(K_new), coord_off(K_new, 0);
+    std::vector<double> coords;
+    for (size_t e = 0; e < K_new; ++e) {
+        const int64_t old = split ? sources[e].old : static_cast<int64_t>(e);
+        oNv[e] = before.N[static_cast<size_t>(old)];
+        oOffv[e] = before.off2[static_cast<size_t>(old)];
+        mode[e] = split ? sources[e].kind : (oNv[e] == after.N[e] ? 0 : 1);
+        if (mode[e] == 2) {
+            std::vector<double> c;
+            child_coordinates(sources[e], ctx->tables.get(NDG_TABLE_NODES, after.N[e]), c);
+            coord_off[e] = static_cast<int64_t>(coords.size());
+            coords.insert(coords.end(), c.begin(), c.end());
+        }
+    }
+    // Transfer the fields to the new elements, then switch the topology
+    // and the device plan.
+    DeviceBuffer<int32_t> oN, nN, dMode;
+    DeviceBuffer<int64_t> oOff, nOff, dCoordOff;
+    DeviceBuffer<double> dCoords;
+    oN.upload(oNv, ctx->stream);
+    nN.upload(after.N, ctx->stream);
+    oOff.upload(oOffv, ctx->stream);
+    nOff.upload(after.off2, ctx->stream);
+    dMode.upload(mode, ctx->stream);
+    dCoordOff.upload(coord_off, ctx->stream);
+    dCoords.upload(coords, ctx->stream);
+    dev::Transfer t{};
+    t.mode = dMode.ptr;
+    t.coords = dCoords.ptr;
+    t.coord_off = dCoordOff.ptr;
+    t.old_block = before.block;
+    t.new_block = after.block;
+    t.n_fields = 3;
+    t.n_instances = ctx->n_instances;
+    t.n_elements = static_cast<int64_t>(K_new);
+    t.old_N = oN.ptr;
+    t.new_N = nN.ptr;
+    t.old_off2 = oOff.ptr;
+    t.new_off2 = nOff.ptr;
+    const size_t values = static_cast<size_t>(ctx->n_instances) * 3 * static_cast<size_t>(after.block);
+    DeviceBuffer<double> q2, k2, G2;
+    q2.allocate(values);
+    k2.allocate(values);
+    check_cuda(cudaMemsetAsync(q2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
+    check_cuda(cudaMemsetAsync(k2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
+    t.src = ctx->q.ptr;
+    t.dst = q2.ptr;
+    check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
+    t.src = ctx->k.ptr;
+    t.dst = k2.ptr;
+    t.zero_changed = 1;
+    check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
+    ctx->launches += 2;
+    if (ctx->keep_derivative) {
+        G2.allocate(values);
+        check_cuda(cudaMemsetAsync(G2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
+        t.src = ctx->G.ptr;
+        t.dst = G2.ptr;
+        t.zero_changed = 0;
+        check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
+        ++ctx->launches;
+    }
+    check_cuda(cudaStreamSynchronize(ctx->stream), "transfer");
+    ctx->q.swap(q2);
+    ctx->k.swap(k2);
+    if (ctx->keep_derivative) ctx->G.swap(G2);
+    ctx->topo = std::move(topo);
+    upload_plan(ctx, after);
+    compute_dt_mesh(ctx, ctx->params.cfl);
 }
 
 template <typename F>
@@ -757,6 +859,36 @@ ndg_status ndg_mesh_get_boundary(const ndg_ctx* ctx, int32_t list, int64_t* out,
             if (capacity < static_cast<int64_t>(v->size())) fail(NDG_ERR_INVALID_ARG, "output buffer too small");
             std::memcpy(out, v->data(), v->size() * sizeof(int64_t));
         }
+    });
+}
+
+ndg_status ndg_mesh_get_element_state(const ndg_ctx* ctx, int32_t* split_level, int32_t* status, int32_t* rotation, int32_t* n_faces_side) {
+    return guarded([&] {
+        require_mesh(ctx);
+        const auto& t = ctx->topo;
+        for (size_t e = 0; e < t.elem_N.size(); ++e) {
+            if (split_level) split_level[e] = t.elem_split[e];
+            if (status) status[e] = t.elem_status[e];
+            if (rotation) rotation[e] = t.elem_rotation[e];
+            if (n_faces_side)
+                for (size_t s = 0; s < 4; ++s) n_faces_side[4 * e + s] = static_cast<int32_t>(t.elem_faces[e][s].size());
+        }
+    });
+}
+
+ndg_status ndg_mesh_get_element_faces(const ndg_ctx* ctx, int64_t* out, int64_t capacity, int64_t* count) {
+    return guarded([&] {
+        require_mesh(ctx);
+        int64_t n = 0;
+        for (const auto& sides : ctx->topo.elem_faces)
+            for (const auto& list : sides) n += static_cast<int64_t>(list.size());
+        if (count) *count = n;
+        if (!out) return;
+        if (capacity < n) fail(NDG_ERR_INVALID_ARG, "output buffer too small");
+        int64_t i = 0;
+        for (const auto& sides : ctx->topo.elem_faces)
+            for (const auto& list : sides)
+                for (int64_t f : list) out[i++] = f;
     });
 }
 
@@ -998,61 +1130,17 @@ ndg_status ndg_adapt(ndg_ctx* ctx) {
         check_cuda(cudaMemcpyAsync(refine.data(), ctx->refine.ptr, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
         check_cuda(cudaMemcpyAsync(sigma.data(), ctx->p_sigma.ptr, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
         check_cuda(cudaStreamSynchronize(ctx->stream), "flag download");
-        const Layout before = layout_of(ctx->topo);
-        Topology topo = ctx->topo;
-        if (!p_adapt(topo, refine.data(), sigma.data(), ctx->params.maximum_N, ctx->params.max_split_level)) {
-            ctx->has_error_estimate = false;
-            return;
-        }
-        const Layout after = layout_of(topo);
-        // Transfer the fields to the new orders (same element points), then
-        // switch the topology and the device plan.
-        DeviceBuffer<int32_t> oN, nN;
-        DeviceBuffer<int64_t> oOff, nOff;
-        oN.upload(before.N, ctx->stream);
-        nN.upload(after.N, ctx->stream);
-        oOff.upload(before.off2, ctx->stream);
-        nOff.upload(after.off2, ctx->stream);
-        dev::Transfer t{};
-        t.old_block = before.block;
-        t.new_block = after.block;
-        t.n_fields = 3;
-        t.n_instances = ctx->n_instances;
-        t.n_elements = ctx->K;
-        t.old_N = oN.ptr;
-        t.new_N = nN.ptr;
-        t.old_off2 = oOff.ptr;
-        t.new_off2 = nOff.ptr;
-        const size_t values = static_cast<size_t>(ctx->n_instances) * 3 * static_cast<size_t>(after.block);
-        DeviceBuffer<double> q2, k2, G2;
-        q2.allocate(values);
-        k2.allocate(values);
-        check_cuda(cudaMemsetAsync(q2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
-        check_cuda(cudaMemsetAsync(k2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
-        t.src = ctx->q.ptr;
-        t.dst = q2.ptr;
-        check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
-        t.src = ctx->k.ptr;
-        t.dst = k2.ptr;
-        t.zero_changed = 1;
-        check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
-        ctx->launches += 2;
-        if (ctx->keep_derivative) {
-            G2.allocate(values);
-            check_cuda(cudaMemsetAsync(G2.ptr, 0, values * sizeof(double), ctx->stream), "memset");
-            t.src = ctx->G.ptr;
-            t.dst = G2.ptr;
-            t.zero_changed = 0;
-            check_cuda(dev::launch_transfer(t, ctx->stream), "transfer kernel");
-            ++ctx->launches;
-        }
-        check_cuda(cudaStreamSynchronize(ctx->stream), "transfer");
-        ctx->q.swap(q2);
-        ctx->k.swap(k2);
-        if (ctx->keep_derivative) ctx->G.swap(G2);
-        ctx->topo = std::move(topo);
-        upload_plan(ctx, after);
-        compute_dt_mesh(ctx, ctx->params.cfl);
+        adapt_mesh(ctx, refine.data(), sigma.data());
+    });
+}
+
+ndg_status ndg_adapt_flags(ndg_ctx* ctx, const int32_t* refine, const double* p_sigma) {
+    return guarded([&] {
+        require_mesh(ctx);
+        if (!refine || !p_sigma) fail(NDG_ERR_INVALID_ARG, "refine and p_sigma must not be NULL");
+        if (ctx->n_instances != 1) fail(NDG_ERR_UNSUPPORTED, "adaptation needs a single instance (the mesh is shared)");
+        make_current(ctx);
+        adapt_mesh(ctx, refine, p_sigma);
     });
 }
 

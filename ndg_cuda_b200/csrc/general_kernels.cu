@@ -561,7 +561,8 @@ __global__ void __launch_bounds__(256) transfer_kernel(Transfer t, int max_nn) {
         if (node >= nn * nn) continue;
         const double* src = t.src + fi * t.old_block + t.old_off2[e];
         double* dst = t.dst + fi * t.new_block + t.new_off2[e] + node;
-        if (Nn == No) {
+        const int mode = t.mode ? t.mode[e] : (Nn == No ? 0 : 1);
+        if (mode == 0) {
             *dst = src[node];
             continue;
         }
@@ -570,7 +571,8 @@ __global__ void __launch_bounds__(256) transfer_kernel(Transfer t, int max_nn) {
             continue;
         }
         const int i = node / nn, j = node - i * nn;
-        const double x = g_nodes[gvec(Nn) + i], y = g_nodes[gvec(Nn) + j];
+        const double x = mode == 2 ? t.coords[t.coord_off[e] + 2 * node] : g_nodes[gvec(Nn) + i];
+        const double y = mode == 2 ? t.coords[t.coord_off[e] + 2 * node + 1] : g_nodes[gvec(Nn) + j];
         const double* xo = g_nodes + gvec(No);
         const double* bo = g_bary + gvec(No);
         int row = -1, col = -1;

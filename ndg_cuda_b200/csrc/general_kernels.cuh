@@ -99,6 +99,13 @@ struct Transfer {
     const int* new_N = nullptr;
     const int64_t* new_off2 = nullptr;
     int zero_changed = 0;  // 1: write zeros where the order changed (RK register)
+    // Optional, after h-adaptation: per new element 0 copy, 1 new order at the
+    // same points, 2 a child at the node coordinates coords[coord_off[e] ..]
+    // (2 per node, in the parent's reference square). Zeros replace every
+    // non-copied element when zero_changed is set.
+    const int* mode = nullptr;
+    const double* coords = nullptr;
+    const int64_t* coord_off = nullptr;
 };
 cudaError_t launch_transfer(const Transfer& t, cudaStream_t stream);
 

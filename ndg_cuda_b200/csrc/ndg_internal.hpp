@@ -57,11 +57,22 @@ struct Topology {
     std::vector<double> delta_xy_min;
     std::vector<std::array<double, 2>> center;
     std::vector<std::array<double, 4>> ghost_scale;  // scaling_factor_[s] (constant along a straight side)
+    // adaptivity state: Element2D_t::split_level_, status_ (Hilbert H, A, R,
+    // B = 0..3), rotation_, the faces of every side (faces_; ghosts use side
+    // 0), and ghosts whose boundary storage was resized without new geometry
+    // (their scaling factor stays zero, as in the reference)
+    std::vector<int> elem_split, elem_status, elem_rotation;
+    std::vector<std::array<std::vector<int64_t>, 4>> elem_faces;
+    std::vector<uint8_t> ghost_sf_zero;
 };
 
 Topology build_topology(const ndg_zone& zone, int initial_N);
 Topology read_su2(const std::string& path, int initial_N);
 void compute_geometry(Topology& topo, const Tables& tables);
+// Fills the adaptivity state of a freshly read mesh: face lists from the
+// single faces, split level 0, Hilbert status and rotation of the domain
+// elements (Mesh2D_t.cpp:4055-4178), status A and rotation 0 for ghosts.
+void init_adaptivity_state(Topology& topo);
 
 // ---------------------------------------------------------------------------
 // Device plan of one mesh for the fused stage kernels (uniform order N,
@@ -106,5 +117,22 @@ GeneralPlan build_general_plan(const Topology& t);
 // p-adaptation of the topology (orders of elements, ghosts and faces) from
 // per-element refine flags and decay rates. Returns whether an order changed.
 bool p_adapt(Topology& t, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level);
+
+// Where a domain element of an adapted mesh takes its solution from.
+struct ElementSource {
+    int64_t old = -1;  // element of the mesh before adaptation
+    int kind = 0;      // 0: same order, copied; 1: new order, same points; 2: child of a split element
+    std::array<double, 8> child{}, parent{};  // kind 2: corners x0, y0, ..., x3, y3 of the child and its parent
+};
+// h-adaptation (with the p-refinement of the same pass) of the topology.
+// Returns false, leaving t untouched, when no element splits; otherwise
+// rebuilds t, recomputes its geometry and fills sources for the new domain
+// elements.
+bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level,
+             std::vector<ElementSource>& sources);
+// Coordinates, in the parent's reference square, of the nodes of order N of
+// a child (Element2D_t::interpolate_from with quad_map and inverse_quad_map):
+// 2 (N+1)^2 values, node i*(N+1)+j.
+void child_coordinates(const ElementSource& src, const std::vector<double>& nodes_N, std::vector<double>& out);
 
 }  // namespace ndg

@@ -224,6 +224,7 @@ void compute_geometry(Topology& t, const Tables& tables) {
             t.center[e] = {(px[0] + px[1]) / 2, (py[0] + py[1]) / 2};
             const auto mb = quad_metrics(x0, -1.0, px, py);
             t.ghost_scale[e] = {std::sqrt(mb[0] * mb[0] + mb[2] * mb[2]), 0.0, 0.0, 0.0};
+            if (e < t.ghost_sf_zero.size() && t.ghost_sf_zero[e]) t.ghost_scale[e][0] = 0.0;
         }
     }
     const size_t nf = t.face_nodes.size();

@@ -70,6 +70,8 @@ def _load_ref():
         lib.ndgref_get_boundary.argtypes = [C.c_int, C.c_void_p]
         lib.ndgref_get_boundary.restype = C.c_long
         lib.ndgref_get_error.argtypes = [_dp, _dp, _ip, _ip]
+        lib.ndgref_get_element_faces.argtypes = [C.c_void_p]
+        lib.ndgref_get_element_faces.restype = C.c_long
         _ref = lib
     return _ref
 
@@ -207,6 +209,12 @@ class RefSolver(_Base):
         self.lib.ndgref_get_elements(d["nodes"], d["N"], d["split_level"], d["status"], d["rotation"],
                                      d["delta_xy_min"], d["first_face"], d["n_faces_side"])
         return d
+
+    def element_faces(self) -> np.ndarray:
+        n = self.lib.ndgref_get_element_faces(None)
+        out = np.empty(max(n, 1), dtype=np.int64)
+        self.lib.ndgref_get_element_faces(out.ctypes.data)
+        return out[:n]
 
     def nodes(self) -> np.ndarray:
         out = np.empty(2 * self.n_nodes)

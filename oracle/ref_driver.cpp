@@ -265,6 +265,19 @@ long ndgref_get_boundary(int kind, long* out) {
     return static_cast<long>(v.size());
 }
 
+// Every element's face lists, side by side (Element2D_t::faces_); returns the
+// total count, writing to out when it is not NULL.
+long ndgref_get_element_faces(long* out) {
+    long n = 0;
+    for (const auto& element : g_ref.mesh->elements_)
+        for (const auto& side : element.faces_)
+            for (size_t f : side) {
+                if (out) out[n] = static_cast<long>(f);
+                ++n;
+            }
+    return n;
+}
+
 void ndgref_estimate_error() {
     g_ref.mesh->estimate_error(g_ref.ndg->polynomials_);
 }

@@ -129,7 +129,7 @@ def test_p_adapt_all_boundary_kinds(tmp_path, ref_available):
         assert rel_l2(m.get_field(f), ref.field(f)) < TOL, f
 
 
-def test_adapt_requires_estimate_and_rejects_h_refinement():
+def test_adapt_requires_estimate_then_splits_from_device_estimate():
     zone = meshgen.uniform_zone(16, x_periodic=True, y_periodic=True)
     m = ndg.Mesh2D_t(zone, 4, maximum_N=8, max_split_level=1, tolerance_min=1e-6)
     m.initial_conditions()
@@ -137,7 +137,55 @@ def test_adapt_requires_estimate_and_rejects_h_refinement():
         m.adapt()
     ndg.Solver2D_t.run(m, 10)
     m.estimate_error()
-    if m.error()["refine"].astype(bool).any():
-        with pytest.raises(ndg.NdgError) as e:
-            m.adapt()
-        assert e.value.status == 7
+    e = m.error()
+    m.adapt()
+    splits = int(((e["refine"] == 1) & (e["p_sigma"] < 1)).sum())
+    assert m.n_elements_ == 256 + 3 * splits
+    assert splits > 0
+    ndg.Solver2D_t.run(m, 3)
+    assert np.isfinite(m.get_field("p")).all()
+
+
+@pytest.mark.parametrize("precision", [ndg.FP64_STRICT, ndg.FP64])
+@pytest.mark.parametrize("kind", ["x_periodic_walls", "periodic_jittered", "outflow"])
+def test_h_adapt_fields_and_steps(kind, precision, ref_available):
+    """Element splitting: children interpolated from their parents, then steps
+    on the nonconforming mesh (several faces per side, mortar projections),
+    against the reference after each of two adaptation rounds. The flags come
+    from the reference's estimate so that both adapt the same elements."""
+    if not ref_available:
+        pytest.skip("reference CPU build not present")
+    from oracle.pyoracle import RefSolver
+    kw = {"x_periodic_walls": dict(x_periodic=True, boundary=meshgen.WALL),
+          "periodic_jittered": dict(x_periodic=True, y_periodic=True, jitter=0.1, seed=2),
+          "outflow": dict(boundary=meshgen.OUTFLOW)}[kind]
+    zone = meshgen.uniform_zone(8, **kw)
+    ref = RefSolver(zone, 4, N_max=8, max_split_level=2, tolerance_min=1e-4, tolerance_max=1e-14)
+    m = ndg.Mesh2D_t(zone, 4, maximum_N=8, max_split_level=2, tolerance_min=1e-4, tolerance_max=1e-14, precision=precision)
+    ref.initial_conditions()
+    for f in ("p", "u", "v"):
+        m.set_field(f, ref.field(f))
+
+    def check(stage):
+        for f in ("p", "u", "v"):
+            got, want = m.get_field(f), ref.field(f)
+            if precision == ndg.FP64_STRICT:
+                assert np.array_equal(got, want), (stage, f)
+            else:
+                assert rel_l2(got, want) < TOL, (stage, f, rel_l2(got, want))
+
+    split = False
+    for rnd in range(2):
+        ref.run(10)
+        ndg.Solver2D_t.run(m, 10)
+        ref.estimate_error()
+        e = ref.error()
+        ref.adapt()
+        m.adapt(e["refine"], e["p_sigma"])
+        _check_topology(ref, m)
+        split |= m.n_elements_ > 64
+        check(f"after adapt {rnd}")
+    assert split
+    ref.run(5)
+    ndg.Solver2D_t.run(m, 5)
+    check("after steps")

@@ -122,3 +122,20 @@ def test_missing_file_and_unknown_extension():
         ndg.Mesh2D_t("mesh.cgns", 3, device=-1)
     assert e.value.status == 7
     _ = C  # ctypes is used through the package
+
+
+@pytest.mark.parametrize("res, kw", [(8, dict(x_periodic=True)), (16, dict(jitter=0.1, seed=3)),
+                                     (8, dict(order="rowmajor", x_periodic=True, y_periodic=True)), (4, {})])
+def test_element_state_bitwise_vs_reference(res, kw, ref_available):
+    """Split level, Hilbert status and rotation (Mesh2D_t::compute_element_status)
+    and per-side face lists at load, against the reference."""
+    if not ref_available:
+        pytest.skip("reference CPU build not present")
+    from oracle.pyoracle import RefSolver
+    zone = meshgen.uniform_zone(res, **kw)
+    m = ndg.Mesh2D_t(zone, 3, device=-1)
+    r = RefSolver(zone, 3)
+    sm, er = m.element_state(), r.elements()
+    for k in ("split_level", "status", "rotation", "n_faces_side"):
+        assert np.array_equal(sm[k], er[k]), k
+    assert np.array_equal(sm["faces"], r.element_faces())
