@@ -197,8 +197,10 @@ ndg_status ndg_stage(ndg_ctx* ctx, int32_t m, double time, double dt);
 /* n_steps RK3 steps, each with dt = get_delta_t; *time advances by dt per step. */
 ndg_status ndg_run(ndg_ctx* ctx, int64_t n_steps, double* time);
 /* The reference's time loop to t_end (include/solvers/Solver2D_t.tcu:7-135
- * without output or adaptivity): the last step is shortened to land on
- * t_end. *time is the start time in and the end time out. */
+ * without output): the last step is shortened to land on t_end, and with
+ * adaptivity_interval > 0 the error is estimated and the mesh adapted after
+ * every adaptivity_interval-th step. *time is the start time in and the end
+ * time out. */
 ndg_status ndg_solve(ndg_ctx* ctx, double t_end, double* time, int64_t* n_steps);
 
 /* Mesh2D_t::estimate_error (src/meshes/Mesh2D_t.cu:5158, Element2D_t::estimate_p_error,

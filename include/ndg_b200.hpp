@@ -12,7 +12,6 @@
  *   - Solver2D_t::solve takes an output callback in place of a
  *     DataWriter_t (VTK output is not part of this library);
  *   - errors throw ndg_b200::Error (the reference exits);
- *   - adaptivity (adaptivity_interval_ > 0) is not available yet and throws.
  * Header-only; link against libndg_b200.so. */
 #ifndef NDG_B200_HPP
 #define NDG_B200_HPP
@@ -202,6 +201,16 @@ public:
         check(ndg_estimate_error(ctx_), "ndg_estimate_error");
     }
 
+    // Mesh2D_t::adapt(N_max, polynomial_nodes, barycentric_weights)
+    // (src/meshes/Mesh2D_t.cpp:1644-2268) from the last error estimate.
+    void adapt(int N_max = 0, const std::vector<double>& polynomial_nodes = {}, const std::vector<double>& barycentric_weights = {}) {
+        (void)N_max;
+        (void)polynomial_nodes;
+        (void)barycentric_weights;
+        check(ndg_adapt(ctx_), "ndg_adapt");
+        refresh_counts();
+    }
+
     // Fields of one instance (instance < 0: all instances back to back), in
     // the reference's element order and node layout.
     std::vector<double> get_field(ndg_field field, int instance = 0) const {
@@ -258,18 +267,22 @@ private:
         return p;
     }
 
-    void finish_load(const ndg_mesh_params& p, int n_instances) {
+    void refresh_counts() {
         int64_t K = 0, total = 0, faces = 0, nodes = 0, size = 0;
         check(ndg_mesh_counts(ctx_, &K, &total, &faces, &nodes), "ndg_mesh_counts");
         check(ndg_mesh_field_size(ctx_, &size), "ndg_mesh_field_size");
-        initial_N_ = p.initial_N;
-        maximum_N_ = p.maximum_N;
         n_elements_ = static_cast<size_t>(K);
         n_elements_total_ = static_cast<size_t>(total);
         n_faces_ = static_cast<size_t>(faces);
         n_nodes_ = static_cast<size_t>(nodes);
-        n_instances_ = n_instances;
         field_size_ = static_cast<size_t>(size);
+    }
+
+    void finish_load(const ndg_mesh_params& p, int n_instances) {
+        refresh_counts();
+        initial_N_ = p.initial_N;
+        maximum_N_ = p.maximum_N;
+        n_instances_ = n_instances;
         adaptivity_interval_ = static_cast<size_t>(p.adaptivity_interval);
         tolerance_min_ = p.tolerance_min;
         tolerance_max_ = p.tolerance_max;
@@ -310,29 +323,41 @@ public:
     // on it. Outputs come where the reference writes them: at the start if
     // time 0 is an output time, then after the first step whose end time t
     // satisfies e <= t < e + dt for an output time e, and at the end if no
-    // output fell on the last step. Returns the number of steps.
+    // output fell on the last step. With adaptivity_interval_ > 0 the error
+    // is estimated and the mesh adapted after every adaptivity_interval_-th
+    // step, and the step size follows the new mesh. Returns the number of
+    // steps.
     template <typename Polynomial>
     size_t solve(const Entities::NDG_t<Polynomial>& NDG, Meshes::Mesh2D_t& mesh, const Output& output = {}) const {
         (void)NDG;
         if (output_times_.empty()) throw Error(NDG_ERR_INVALID_ARG, "solve: no output times");
-        if (mesh.adaptivity_interval_ > 0)
-            throw Error(NDG_ERR_UNSUPPORTED, "solve: adaptivity is not available in this library yet");
         const double t_end = output_times_.back();
-        const double dt_mesh = get_delta_t(mesh);
+        double dt_mesh = get_delta_t(mesh);
         double time = 0.0;
         for (double e : output_times_)
             if (time >= e && time < e + dt_mesh && output) output(time, mesh);
 
-        // Plan the steps as the reference takes them, then run the full
-        // steps between outputs in one call each.
+        // The reference's steps; full steps between outputs and adaptations
+        // run in one call each, the shortened last step as three stages.
         size_t steps = 0;
         int64_t pending = 0;
         double t_run = 0.0;
         bool wrote_last = false;
+        auto flush = [&] {
+            if (pending) check(ndg_run(mesh.handle(), pending, &t_run), "ndg_run");
+            pending = 0;
+        };
         while (time < t_end) {
             double dt = dt_mesh;
             const bool last = time + dt > t_end;
             if (last) dt = t_end - time;
+            if (last) {
+                flush();
+                for (int m = 0; m < 3; ++m) check(ndg_stage(mesh.handle(), m, time, dt), "ndg_stage");
+                t_run = time + dt;
+            } else {
+                ++pending;
+            }
             time += dt;
             ++steps;
             bool write = false;
@@ -342,22 +367,19 @@ public:
                     break;
                 }
             wrote_last = write;
-            if (last) {
-                if (pending) check(ndg_run(mesh.handle(), pending, &t_run), "ndg_run");
-                pending = 0;
-                int64_t n = 0;
-                check(ndg_solve(mesh.handle(), t_end, &t_run, &n), "ndg_solve");
-            } else {
-                ++pending;
-            }
             if (write) {
-                if (pending) check(ndg_run(mesh.handle(), pending, &t_run), "ndg_run");
-                pending = 0;
+                flush();
                 mesh.estimate_error();
                 if (output) output(time, mesh);
             }
+            if (mesh.adaptivity_interval_ > 0 && steps % mesh.adaptivity_interval_ == 0) {
+                flush();
+                mesh.estimate_error();
+                mesh.adapt();
+                check(ndg_get_delta_t(mesh.handle(), &dt_mesh), "ndg_get_delta_t");
+            }
         }
-        if (pending) check(ndg_run(mesh.handle(), pending, &t_run), "ndg_run");
+        flush();
         if (!wrote_last) {
             mesh.estimate_error();
             if (output) output(time, mesh);

@@ -291,6 +291,9 @@ class Mesh2D_t:
             r = np.ascontiguousarray(refine, dtype=np.int32)
             sg = np.ascontiguousarray(p_sigma, dtype=np.float64)
             _check(lib().ndg_adapt_flags(self._ctx.h, _ptr(r), _ptr(sg)))
+        self._refresh_counts()
+
+    def _refresh_counts(self) -> None:
         counts = [C.c_int64() for _ in range(4)]
         _check(lib().ndg_mesh_counts(self._ctx.h, *[C.byref(c) for c in counts]))
         self.n_elements_, self.n_elements_total_, self.n_faces_, self.n_nodes_ = (c.value for c in counts)
@@ -391,6 +394,7 @@ class Solver2D_t:
         n = C.c_int64()
         _check(lib().ndg_set_cfl(mesh.handle, float(self.CFL_)))
         _check(lib().ndg_solve(mesh.handle, float(self.output_times_[-1]), C.byref(t), C.byref(n)))
+        mesh._refresh_counts()  # the mesh may have been adapted
         return t.value, n.value
 
 

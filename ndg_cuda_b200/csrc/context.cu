@@ -631,6 +631,49 @@ void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in) 
     compute_dt_mesh(ctx, ctx->params.cfl);
 }
 
+// Legendre-decay error estimate of every element and instance
+// (Mesh2D_t::estimate_error), one launch per order group.
+void estimate(ndg_ctx* ctx) {
+    dev::EstimatorArgs a{};
+    a.q = ctx->q.ptr;
+    a.p_error = ctx->p_error.ptr;
+    a.p_sigma = ctx->p_sigma.ptr;
+    a.refine = ctx->refine.ptr;
+    a.coarsen = ctx->coarsen.ptr;
+    a.tolerance_min = ctx->params.tolerance_min;
+    a.tolerance_max = ctx->params.tolerance_max;
+    a.n_elements = ctx->K;
+    a.block = ctx->block;
+    a.n_instances = ctx->n_instances;
+    if (ctx->general) {
+        a.off2 = ctx->g_off2.ptr;
+        for (const auto& g : ctx->groups) {
+            a.N = g.N;
+            a.count = g.count;
+            a.ids = g.ids;
+            check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
+            ++ctx->launches;
+        }
+    } else {
+        a.N = ctx->N;
+        a.count = ctx->K;
+        check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
+        ++ctx->launches;
+    }
+    ctx->has_error_estimate = true;
+}
+
+// Mesh2D_t::adapt from the last estimate of instance 0.
+void adapt_from_estimate(ndg_ctx* ctx) {
+    const size_t K = static_cast<size_t>(ctx->K);
+    std::vector<int32_t> refine(K);
+    std::vector<double> sigma(K);
+    check_cuda(cudaMemcpyAsync(refine.data(), ctx->refine.ptr, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
+    check_cuda(cudaMemcpyAsync(sigma.data(), ctx->p_sigma.ptr, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "flag download");
+    adapt_mesh(ctx, refine.data(), sigma.data());
+}
+
 template <typename F>
 ndg_status guarded(F&& f) {
     try {
@@ -1019,20 +1062,33 @@ ndg_status ndg_solve(ndg_ctx* ctx, double t_end, double* time, int64_t* n_steps)
         require_mesh(ctx);
         require_device(ctx);
         make_current(ctx);
-        const double t0 = time ? *time : 0.0;
-        // Step count of the reference loop (Solver2D_t.tcu:35-42): the last
-        // step is shortened to land on t_end.
+        const int64_t interval = ctx->params.adaptivity_interval;
+        if (interval > 0 && ctx->n_instances != 1) fail(NDG_ERR_UNSUPPORTED, "adaptation needs a single instance (the mesh is shared)");
+        // The reference loop (Solver2D_t.tcu:35-110): the last step is
+        // shortened to land on t_end, and after every adaptivity_interval-th
+        // step the error is estimated and the mesh adapted. Steps between
+        // adaptations run as graph launches.
+        double t = time ? *time : 0.0;
         int64_t steps = 0;
-        double t = t0;
         while (t < t_end) {
-            double dt = ctx->dt_mesh;
-            if (t + dt > t_end) dt = t_end - t;
-            t += dt;
-            ++steps;
+            const int64_t limit = interval > 0 ? interval - steps % interval : std::numeric_limits<int64_t>::max();
+            const double c0 = t;
+            int64_t n = 0;
+            while (t < t_end && n < limit) {
+                double dt = ctx->dt_mesh;
+                if (t + dt > t_end) dt = t_end - t;
+                t += dt;
+                ++n;
+            }
+            const double dt0 = (c0 + ctx->dt_mesh > t_end) ? t_end - c0 : ctx->dt_mesh;
+            set_step(ctx, c0, dt0, t_end);
+            run_steps(ctx, n);
+            steps += n;
+            if (interval > 0 && n == limit) {
+                estimate(ctx);
+                adapt_from_estimate(ctx);
+            }
         }
-        const double dt0 = (t0 + ctx->dt_mesh > t_end) ? t_end - t0 : ctx->dt_mesh;
-        set_step(ctx, t0, dt0, t_end);
-        run_steps(ctx, steps);
         if (time) *time = t;
         if (n_steps) *n_steps = steps;
     });
@@ -1070,33 +1126,7 @@ ndg_status ndg_estimate_error(ndg_ctx* ctx) {
         require_mesh(ctx);
         require_device(ctx);
         make_current(ctx);
-        dev::EstimatorArgs a{};
-        a.q = ctx->q.ptr;
-        a.p_error = ctx->p_error.ptr;
-        a.p_sigma = ctx->p_sigma.ptr;
-        a.refine = ctx->refine.ptr;
-        a.coarsen = ctx->coarsen.ptr;
-        a.tolerance_min = ctx->params.tolerance_min;
-        a.tolerance_max = ctx->params.tolerance_max;
-        a.n_elements = ctx->K;
-        a.block = ctx->block;
-        a.n_instances = ctx->n_instances;
-        if (ctx->general) {
-            a.off2 = ctx->g_off2.ptr;
-            for (const auto& g : ctx->groups) {
-                a.N = g.N;
-                a.count = g.count;
-                a.ids = g.ids;
-                check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
-                ++ctx->launches;
-            }
-        } else {
-            a.N = ctx->N;
-            a.count = ctx->K;
-            check_cuda(dev::launch_estimate_error(a, ctx->stream), "estimator kernel launch");
-            ++ctx->launches;
-        }
-        ctx->has_error_estimate = true;
+        estimate(ctx);
     });
 }
 
@@ -1124,13 +1154,7 @@ ndg_status ndg_adapt(ndg_ctx* ctx) {
         if (!ctx->has_error_estimate) fail(NDG_ERR_INVALID_ARG, "call ndg_estimate_error first");
         if (ctx->n_instances != 1) fail(NDG_ERR_UNSUPPORTED, "adaptation needs a single instance (the mesh is shared)");
         make_current(ctx);
-        const size_t K = static_cast<size_t>(ctx->K);
-        std::vector<int32_t> refine(K);
-        std::vector<double> sigma(K);
-        check_cuda(cudaMemcpyAsync(refine.data(), ctx->refine.ptr, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
-        check_cuda(cudaMemcpyAsync(sigma.data(), ctx->p_sigma.ptr, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
-        check_cuda(cudaStreamSynchronize(ctx->stream), "flag download");
-        adapt_mesh(ctx, refine.data(), sigma.data());
+        adapt_from_estimate(ctx);
     });
 }
 

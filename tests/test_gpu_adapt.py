@@ -189,3 +189,41 @@ def test_h_adapt_fields_and_steps(kind, precision, ref_available):
     ref.run(5)
     ndg.Solver2D_t.run(m, 5)
     check("after steps")
+
+
+def test_solve_with_adaptivity_interval(ref_available):
+    """ndg_solve with adaptivity_interval > 0 follows the reference loop
+    (include/solvers/Solver2D_t.tcu:35-110): after every interval-th step the
+    error is estimated and the mesh adapted, the step size follows the new
+    mesh, and the last step is shortened to land on t_end."""
+    if not ref_available:
+        pytest.skip("reference CPU build not present")
+    from oracle.pyoracle import RefSolver
+    zone = meshgen.uniform_zone(8, x_periodic=True, boundary=meshgen.WALL)
+    kw = dict(tolerance_min=1e-4, tolerance_max=1e-14)
+    ref = RefSolver(zone, 4, N_max=8, max_split_level=1, adaptivity_interval=5, **kw)
+    m = ndg.Mesh2D_t(zone, 4, maximum_N=8, max_split_level=1, adaptivity_interval=5, precision=ndg.FP64_STRICT, **kw)
+    ref.initial_conditions()
+    for f in ("p", "u", "v"):
+        m.set_field(f, ref.field(f))
+    t_end = 12.4 * ref.delta_t()
+    t, steps = 0.0, 0
+    while t < t_end:
+        dt = ref.delta_t()
+        if t + dt > t_end:
+            dt = t_end - t
+            for s in range(3):
+                ref.stage(s, t, dt)
+            t = t + dt
+        else:
+            t = ref.run(1, t)
+        steps += 1
+        if steps % 5 == 0:
+            ref.estimate_error()
+            ref.adapt()
+    t_got, n_got = ndg.Solver2D_t(0.5, [t_end]).solve(m)
+    assert n_got == steps and t_got == t
+    _check_topology(ref, m)
+    assert m.n_elements_ > 64 or len(set(m.elements()["N"].tolist())) > 1
+    for f in ("p", "u", "v"):
+        assert np.array_equal(m.get_field(f), ref.field(f)), f
