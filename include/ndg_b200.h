@@ -254,6 +254,66 @@ ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches);
 ndg_status ndg_delta_t_from_device(const double* delta_xy_min, const int32_t* elem_N, int64_t n_elements,
                                    double cfl, void* stream, double* delta_t);
 
+/* ------------------------------------------------------------------------
+ * Discrete adjoint. No counterpart in the reference, whose wave speed is the
+ * constant c = 1 (include/helpers/constants.h:15); with c = 1 the operator
+ * below is the reference's.
+ *
+ * Operator: a wave speed c_e > 0 per domain element in
+ *   p_t + c (u_x + v_y) = 0,  u_t + c p_x = 0,  v_t + c p_y = 0:
+ * the reference's fluxes x_flux = (c u, p, 0), y_flux = (c v, 0, p)
+ * (src/solvers/Solver2D_t.cpp:31-37) become c_e (u, p, 0), c_e (v, 0, p)
+ * inside element e, and its upwind face flux (Solver2D_t.cpp:48-63, with
+ * w = p +- u.n) is multiplied by the face speed (c_left + c_right) / 2.
+ * Time stepping: the reference's low-storage RK3 with a fixed step dt.
+ * Meshes of one order with conforming faces (no adaptation since the load)
+ * and wall, symmetry, outflow or periodic boundaries (inflow sides make the
+ * step affine rather than linear and are rejected).
+ *
+ * Misfit: receivers at points (x_r, y_r) sample the pressure interpolated
+ * in their element after every step n = 1..n_steps; with targets d[n][r],
+ *   J = dt / 2 sum_n sum_r (p_r(t_n) - d[n][r])^2.
+ * ndg_adjoint_backward returns dJ/d(p0, u0, v0) (the initial fields) and
+ * dJ/dc (per element), the exact gradient of the discrete forward map (the
+ * transpose of every stage, in reverse), with dt held fixed.
+ * Memory: the forward keeps the state every checkpoint_interval steps; the
+ * backward recomputes each interval's 3 checkpoint_interval stage inputs
+ * from its checkpoint and runs the adjoint stages over it. */
+typedef struct ndg_adjoint ndg_adjoint;
+
+/* An adjoint problem on the context's mesh, with n_receivers (at most 64)
+ * receivers at receiver_xy[2 r], [2 r + 1]; the wave speed starts at 1. */
+ndg_status ndg_adjoint_create(ndg_ctx* ctx, int32_t n_receivers, const double* receiver_xy, ndg_adjoint** out);
+ndg_status ndg_adjoint_destroy(ndg_adjoint* adj);
+/* Wave speed per domain element (n_elements values, all > 0). */
+ndg_status ndg_adjoint_set_speed(ndg_adjoint* adj, const double* c);
+/* The CFL step of the variable-speed operator: min over elements of
+ * cfl * delta_xy_min / (N^2 c_e). */
+ndg_status ndg_adjoint_delta_t(ndg_adjoint* adj, double cfl, double* delta_t);
+/* Receivers: their element and reference coordinates (xi, eta); any pointer
+ * may be NULL. */
+ndg_status ndg_adjoint_receivers(const ndg_adjoint* adj, int64_t* element, double* xi_eta);
+/* Forward solve from (p0, u0, v0) (field_size values each; u0 or v0 NULL =
+ * zero) for n_steps steps of dt, keeping checkpoints every
+ * checkpoint_interval steps (0: one interval). targets: (n_steps + 1) x
+ * n_receivers values, row n for step n (row 0 unused); NULL = zero.
+ * samples (optional, same shape) receives the receivers' pressure (row 0:
+ * the initial state's). *misfit = J. */
+ndg_status ndg_adjoint_forward(ndg_adjoint* adj, const double* p0, const double* u0, const double* v0, const double* targets,
+                               double dt, int64_t n_steps, int64_t checkpoint_interval, double* samples, double* misfit);
+/* Gradient of the last forward's misfit: grad_p0, grad_u0, grad_v0
+ * (field_size values each) and grad_c (n_elements values); any may be
+ * NULL. */
+ndg_status ndg_adjoint_backward(ndg_adjoint* adj, double* grad_p0, double* grad_u0, double* grad_v0, double* grad_c);
+/* The operator and its transpose on given states (3 field_size values each,
+ * p then u then v): Lx = L(c) x, LTy = L(c)^T y, and dc[e] = d(y . L(c) x)/dc_e.
+ * Any output may be NULL. For the transpose (dot-product) test. */
+ndg_status ndg_adjoint_operator(ndg_adjoint* adj, const double* x, const double* y, double* Lx, double* LTy, double* dc);
+/* Device time (CUDA events on the context's stream) of the last forward's
+ * stepping and of the last backward's recompute + adjoint stepping, in ms,
+ * and the kernel launches of each. Any pointer may be NULL. */
+ndg_status ndg_adjoint_timings(const ndg_adjoint* adj, double* forward_ms, double* backward_ms, int64_t* forward_launches, int64_t* backward_launches);
+
 #ifdef __cplusplus
 }
 #endif

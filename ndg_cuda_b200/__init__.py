@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-__all__ = ["NdgError", "lib", "NDG_t", "Mesh2D_t", "Solver2D_t", "Zone", "LIB_PATH",
+__all__ = ["NdgError", "lib", "NDG_t", "Mesh2D_t", "Solver2D_t", "Adjoint2D_t", "Zone", "LIB_PATH",
            "FP64", "FP64_STRICT", "FP32", "tables_compute"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libndg_b200.so")
@@ -94,6 +94,15 @@ def lib() -> C.CDLL:
         "ndg_adapt": ([vp], C.c_int),
         "ndg_adapt_flags": ([vp, vp, vp], C.c_int),
         "ndg_delta_t_from_device": ([vp, vp, i64, dbl, vp, C.POINTER(dbl)], C.c_int),
+        "ndg_adjoint_create": ([vp, i32, vp, C.POINTER(vp)], C.c_int),
+        "ndg_adjoint_destroy": ([vp], C.c_int),
+        "ndg_adjoint_set_speed": ([vp, vp], C.c_int),
+        "ndg_adjoint_delta_t": ([vp, dbl, C.POINTER(dbl)], C.c_int),
+        "ndg_adjoint_receivers": ([vp, vp, vp], C.c_int),
+        "ndg_adjoint_forward": ([vp, vp, vp, vp, vp, dbl, i64, i64, vp, C.POINTER(dbl)], C.c_int),
+        "ndg_adjoint_backward": ([vp, vp, vp, vp, vp], C.c_int),
+        "ndg_adjoint_operator": ([vp, vp, vp, vp, vp, vp], C.c_int),
+        "ndg_adjoint_timings": ([vp, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64), C.POINTER(i64)], C.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
@@ -396,6 +405,105 @@ class Solver2D_t:
         _check(lib().ndg_solve(mesh.handle, float(self.output_times_[-1]), C.byref(t), C.byref(n)))
         mesh._refresh_counts()  # the mesh may have been adapted
         return t.value, n.value
+
+
+class Adjoint2D_t:
+    """Discrete adjoint of the variable-speed wave operator on a mesh of one
+    order (ndg_adjoint_*): forward solve with receivers and a misfit, its
+    exact gradient with respect to the initial fields and the per-element
+    wave speed, and the operator with its transpose.
+
+    The mesh must not be adapted while the adjoint exists."""
+
+    def __init__(self, mesh: Mesh2D_t, receivers_xy=None, speed=None):
+        xy = np.ascontiguousarray(np.zeros((0, 2)) if receivers_xy is None else receivers_xy, dtype=np.float64).reshape(-1, 2)
+        self.mesh = mesh
+        self.n_receivers = xy.shape[0]
+        self.n_elements = mesh.n_elements_
+        self.field_size = mesh.field_size
+        h = C.c_void_p()
+        _check(lib().ndg_adjoint_create(mesh.handle, self.n_receivers, _ptr(xy) if xy.size else None, C.byref(h)))
+        self.h = h
+        self.serial = 0  # changes with every forward solve and speed update
+        if speed is not None:
+            self.set_speed(speed)
+
+    def set_speed(self, c) -> None:
+        c = np.ascontiguousarray(c, dtype=np.float64).ravel()
+        if c.size != self.n_elements:
+            raise ValueError(f"expected {self.n_elements} speeds, got {c.size}")
+        _check(lib().ndg_adjoint_set_speed(self.h, _ptr(c)))
+        self.serial += 1
+
+    def delta_t(self, cfl: float) -> float:
+        dt = C.c_double()
+        _check(lib().ndg_adjoint_delta_t(self.h, cfl, C.byref(dt)))
+        return dt.value
+
+    def receivers(self) -> tuple[np.ndarray, np.ndarray]:
+        """Element and (xi, eta) of every receiver."""
+        el = np.empty(max(self.n_receivers, 1), dtype=np.int64)
+        xe = np.empty(max(2 * self.n_receivers, 1))
+        _check(lib().ndg_adjoint_receivers(self.h, _ptr(el), _ptr(xe)))
+        return el[:self.n_receivers], xe[:2 * self.n_receivers].reshape(-1, 2)
+
+    def _field(self, a):
+        if a is None:
+            return None, None
+        a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+        if a.size != self.field_size:
+            raise ValueError(f"expected {self.field_size} values, got {a.size}")
+        return a, _ptr(a)
+
+    def forward(self, p0, dt: float, n_steps: int, targets=None, u0=None, v0=None, checkpoint_interval: int = 0) -> tuple[float, np.ndarray]:
+        """Misfit J and the receivers' pressure, shape (n_steps + 1, n_receivers)."""
+        p0, pp = self._field(p0)
+        u0, pu = self._field(u0)
+        v0, pv = self._field(v0)
+        R = self.n_receivers
+        tg = None
+        if targets is not None:
+            tg = np.ascontiguousarray(targets, dtype=np.float64).reshape(n_steps + 1, R)
+        samples = np.empty((n_steps + 1, max(R, 1)))
+        J = C.c_double()
+        self.serial += 1
+        _check(lib().ndg_adjoint_forward(self.h, pp, pu, pv, None if tg is None else _ptr(tg), dt, n_steps, checkpoint_interval,
+                                         _ptr(samples), C.byref(J)))
+        return J.value, samples[:, :R]
+
+    def backward(self) -> dict:
+        """Gradients of the last forward's misfit: p0, u0, v0 and c."""
+        g = {k: np.empty(self.field_size) for k in ("p0", "u0", "v0")}
+        g["c"] = np.empty(self.n_elements)
+        _check(lib().ndg_adjoint_backward(self.h, *[_ptr(g[k]) for k in ("p0", "u0", "v0", "c")]))
+        return g
+
+    def operator(self, x, y) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(L(c) x, L(c)^T y, d(y . L(c) x)/dc) for states of 3 field_size values."""
+        x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        y = np.ascontiguousarray(y, dtype=np.float64).ravel()
+        if x.size != 3 * self.field_size or y.size != 3 * self.field_size:
+            raise ValueError("x and y hold p, u and v")
+        Lx, LTy, dc = np.empty_like(x), np.empty_like(y), np.empty(self.n_elements)
+        _check(lib().ndg_adjoint_operator(self.h, _ptr(x), _ptr(y), _ptr(Lx), _ptr(LTy), _ptr(dc)))
+        return Lx, LTy, dc
+
+    def timings(self) -> dict:
+        f, b = C.c_double(), C.c_double()
+        lf, lb = C.c_int64(), C.c_int64()
+        _check(lib().ndg_adjoint_timings(self.h, C.byref(f), C.byref(b), C.byref(lf), C.byref(lb)))
+        return {"forward_ms": f.value, "backward_ms": b.value, "forward_launches": lf.value, "backward_launches": lb.value}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().ndg_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def delta_t_from_device(delta_xy_min: int, elem_N: int, n_elements: int, cfl: float, stream: int = 0) -> float:

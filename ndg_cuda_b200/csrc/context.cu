@@ -1,7 +1,7 @@
 // C ABI of the library (include/ndg_b200.h): contexts, tables, meshes,
 // fields and time stepping. Host orchestration only; the arithmetic is in
 // stage_kernels.cu.
-#include "ndg_internal.hpp"
+#include "context.hpp"
 #include "estimator.cuh"
 #include "general_kernels.cuh"
 #include "stage_kernels.cuh"
@@ -27,118 +27,12 @@ void set_last_error(const std::string& message) { g_last_error = message; }
 
 [[noreturn]] void fail(ndg_status status, const std::string& message) { throw Error{status, message}; }
 
-namespace {
-
-void check_cuda(cudaError_t err, const char* what) {
-    if (err != cudaSuccess) {
-        const ndg_status st = (err == cudaErrorMemoryAllocation) ? NDG_ERR_OOM : NDG_ERR_CUDA;
-        fail(st, std::string(what) + ": " + cudaGetErrorString(err));
-    }
-}
-
-template <typename T>
-struct DeviceBuffer {
-    T* ptr = nullptr;
-    size_t count = 0;
-    DeviceBuffer() = default;
-    DeviceBuffer(const DeviceBuffer&) = delete;
-    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    void swap(DeviceBuffer& o) noexcept {
-        std::swap(ptr, o.ptr);
-        std::swap(count, o.count);
-    }
-    void upload(const std::vector<T>& v, cudaStream_t stream) {
-        allocate(std::max<size_t>(v.size(), 1));
-        if (!v.empty()) check_cuda(cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "mesh upload");
-    }
-    void allocate(size_t n) {
-        release();
-        if (n == 0) return;
-        check_cuda(cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)), "cudaMalloc");
-        count = n;
-    }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        count = 0;
-    }
-    ~DeviceBuffer() { release(); }
-};
-
-// Williamson low-storage RK3 coefficients (include/solvers/Solver2D_t.tpp:16-18).
-constexpr double kRkA[3] = {0, -5.0 / 9.0, -153.0 / 128.0};
-constexpr double kRkB[3] = {0, 1.0 / 3.0, 0.75};
-constexpr double kRkG[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
-
-}  // namespace
 }  // namespace ndg
-
-struct ndg_ctx {
-    int device = -1;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int precision = NDG_FP64;
-    bool keep_derivative = false;
-
-    bool has_tables = false;
-    ndg::Tables tables;
-
-    bool has_mesh = false;
-    ndg::Topology topo;
-    ndg_mesh_params params{};
-    int n_instances = 1;
-    int N = 0;
-    int64_t K = 0;
-    int64_t field_size = 0;  // values per field and instance seen through the API: K (N+1)^2
-    int64_t Kp = 0;          // elements per device field block: K rounded up to even
-    int64_t block = 0;       // values per device field block: Kp (N+1)^2
-
-    ndg::DeviceBuffer<double> q, k, G, tr[2], corners, normal, gscale, inflow, dxy, step, scratch;
-    ndg::DeviceBuffer<float> tr32[2];  // traces of the FP32 form
-    ndg::DeviceBuffer<int32_t> link, elem_N;
-    ndg::DeviceBuffer<unsigned> error;
-    ndg::DeviceBuffer<double> p_error, p_sigma;
-    ndg::DeviceBuffer<int32_t> refine, coarsen;
-    bool has_error_estimate = false;
-    int cur = 0;
-    bool traces_valid = false;
-    double dt_mesh = 0.0;
-
-    // Mixed-order meshes (after adaptation) run the general stage path.
-    bool general = false;
-    ndg::GeneralPlan gplan;
-    ndg::DeviceBuffer<int32_t> g_eN, g_fN, g_gkind, g_gsrc_side;
-    ndg::DeviceBuffer<int64_t> g_off2, g_off1, g_enodes, g_sface_start, g_sface, g_foff, g_fnodes, g_felem, g_fside, g_gsrc, g_ids;
-    ndg::DeviceBuffer<double> g_corners, g_node_xy, g_fnormal, g_ftangent, g_foffset, g_fscale, g_gscale, etr, ffl;
-    std::vector<ndg::dev::OrderGroup> groups;
-    ndg::dev::GeneralMesh gmesh;
-
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int64_t launches = 0;
-
-    ~ndg_ctx() {
-        for (auto& g : graph)
-            if (g) cudaGraphExecDestroy(g);
-        if (own_stream && stream) cudaStreamDestroy(stream);
-    }
-};
 
 namespace ndg {
 namespace {
 
 bool strict(const ndg_ctx* c) { return c->precision == NDG_FP64_STRICT; }
-
-void require_device(const ndg_ctx* c) {
-    if (c->device < 0) fail(NDG_ERR_INVALID_ARG, "this call needs a GPU context (device >= 0)");
-}
-
-void require_mesh(const ndg_ctx* c) {
-    if (!c->has_mesh) fail(NDG_ERR_INVALID_ARG, "no mesh loaded");
-}
-
-void make_current(const ndg_ctx* c) {
-    if (c->device >= 0) check_cuda(cudaSetDevice(c->device), "cudaSetDevice");
-}
 
 void drop_graphs(ndg_ctx* c) {
     for (auto& g : c->graph) {
@@ -511,6 +405,7 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     c->Kp = c->K + (c->K & 1);
     c->block = l.block;
     c->has_mesh = true;
+    ++c->mesh_version;
     c->traces_valid = false;
     c->cur = 0;
     drop_graphs(c);
@@ -546,6 +441,7 @@ void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in) 
         return;
     }
     const Layout after = layout_of(topo);
+    ++ctx->mesh_version;
     if (ctx->device < 0) {
         // Host-only context: the topology alone.
         ctx->topo = std::move(topo);
@@ -672,24 +568,6 @@ void adapt_from_estimate(ndg_ctx* ctx) {
     check_cuda(cudaMemcpyAsync(sigma.data(), ctx->p_sigma.ptr, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
     check_cuda(cudaStreamSynchronize(ctx->stream), "flag download");
     adapt_mesh(ctx, refine.data(), sigma.data());
-}
-
-template <typename F>
-ndg_status guarded(F&& f) {
-    try {
-        f();
-        set_last_error("");
-        return NDG_OK;
-    } catch (const Error& e) {
-        set_last_error(e.message);
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        set_last_error("host allocation failed");
-        return NDG_ERR_OOM;
-    } catch (const std::exception& e) {
-        set_last_error(e.what());
-        return NDG_ERR_INVALID_ARG;
-    }
 }
 
 void copy_table(const Tables& t, int32_t table, int32_t N, double* out, int64_t capacity, int64_t* count) {

@@ -56,6 +56,9 @@ cudaError_t launch_initial_conditions(double* q, double* k, const double* corner
 cudaError_t launch_delta_t(const double* delta_xy_min, const int* elem_N, int64_t K, double cfl, double* out, cudaStream_t stream);
 cudaError_t launch_end_step(double* step, cudaStream_t stream);
 cudaError_t upload_tables(const Tables& t);
+// Host copy of the order-N coefficients uploaded by upload_tables: Dhat
+// ((N+1)^2), nodes, Lagrange values at -1 and +1, weights, 1/weights.
+void host_coefficients(int N, double* dhat, double* xn, double* lm, double* lp, double* w, double* iw);
 int elements_per_block(int N);
 
 }  // namespace dev

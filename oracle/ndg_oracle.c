@@ -261,6 +261,11 @@ struct ndgo_ctx {
     int64_t* blist[4]; /* wall, symmetry, inflow, outflow */
     int64_t n_if;
     int64_t *if_origin, *if_origin_side, *if_dest;
+    /* variable-speed operator (NULL: the reference's constant c = 1):
+     * speed per domain element, and per element (ghosts included) the
+     * domain element whose speed it carries */
+    double* speed;
+    int64_t* speed_owner;
 };
 
 static void* xcalloc(size_t n, size_t sz) { return calloc(n > 0 ? n : 1, sz); }
@@ -640,7 +645,8 @@ void ndgo_destroy(ndgo_ctx* c) {
                     c->p, c->u, c->v, c->Gp, c->Gu, c->Gv, c->kp, c->ku, c->kv, c->pe, c->ue, c->ve, c->pfe, c->ufe, c->vfe, c->p_error, c->p_sigma, c->refine, c->coarsen,
                     c->fN, c->fnodes, c->felem, c->fside, c->normal, c->tangent, c->length, c->offset, c->scale, c->foff,
                     c->fp0, c->fp1, c->fu0, c->fu1, c->fv0, c->fv1, c->fluxp, c->fluxu, c->fluxv,
-                    c->blist[0], c->blist[1], c->blist[2], c->blist[3], c->if_origin, c->if_origin_side, c->if_dest};
+                    c->blist[0], c->blist[1], c->blist[2], c->blist[3], c->if_origin, c->if_origin_side, c->if_dest,
+                    c->speed, c->speed_owner};
     for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
     free(c);
 }
@@ -859,8 +865,29 @@ static void project_to_faces(ndgo_ctx* c) {
     }
 }
 
+/* Face speed of the variable-speed operator: the mean of its two sides'
+ * speeds (a ghost carries the speed of the element it stands for). */
+static double face_speed(const ndgo_ctx* c, int64_t f) {
+    return 0.5 * (c->speed[c->speed_owner[c->felem[2 * f]]] + c->speed[c->speed_owner[c->felem[2 * f + 1]]]);
+}
+
 /* src/solvers/Solver2D_t.cpp:48-63 (calculate_wave_fluxes, upwind). */
 static void calculate_wave_fluxes(ndgo_ctx* c) {
+    if (c->speed) {
+        /* variable speed: the unit-speed upwind flux times the face speed */
+        for (int64_t f = 0; f < c->n_faces; ++f) {
+            const double nxv = c->normal[2 * f], nyv = c->normal[2 * f + 1], cf = face_speed(c, f);
+            for (int i = 0; i <= c->fN[f]; ++i) {
+                const int64_t k = c->foff[f] + i;
+                const double wL = c->fp0[k] + (c->fu0[k] * nxv + c->fv0[k] * nyv);
+                const double wR = c->fp1[k] - (c->fu1[k] * nxv + c->fv1[k] * nyv);
+                c->fluxp[k] = cf * (wL - wR) / 2;
+                c->fluxu[k] = cf * nxv * (wL + wR) / 2;
+                c->fluxv[k] = cf * nyv * (wL + wR) / 2;
+            }
+        }
+        return;
+    }
     for (int64_t f = 0; f < c->n_faces; ++f) {
         const double nxv = c->normal[2 * f], nyv = c->normal[2 * f + 1];
         for (int i = 0; i <= c->fN[f]; ++i) {
@@ -948,7 +975,8 @@ static void project_to_elements(ndgo_ctx* c) {
 }
 
 /* src/solvers/Solver2D_t.cpp:66-136 (compute_dg_wave_derivative, Algorithm 114)
- * with the fluxes x_flux = (c u, p, 0), y_flux = (c v, 0, p) of :31-37. */
+ * with the fluxes x_flux = (c u, p, 0), y_flux = (c v, 0, p) of :31-37; with
+ * a speed per element, c_e (u, p, 0) and c_e (v, 0, p). */
 static void compute_dg_wave_derivative(ndgo_ctx* c) {
     double fl[3][33], fd[3][33];
     for (int64_t e = 0; e < c->n_elem; ++e) {
@@ -963,11 +991,16 @@ static void compute_dg_wave_derivative(ndgo_ctx* c) {
         const double* V = c->v + o2;
         double* G[3] = {c->Gp + o2, c->Gu + o2, c->Gv + o2};
         const double* FE[3] = {c->pfe + o1, c->ufe + o1, c->vfe + o1};
+        const double ce = c->speed ? c->speed[e] : 0.0;
         for (int j = 0; j <= N; ++j) {
             for (int i = 0; i <= N; ++i) {
                 const int k = i * n + j;
-                const double fx[3] = {C_c * U[k], P[k], 0};
-                const double fy[3] = {C_c * V[k], 0, P[k]};
+                double fx[3] = {C_c * U[k], P[k], 0};
+                double fy[3] = {C_c * V[k], 0, P[k]};
+                if (c->speed) {
+                    fx[0] = ce * U[k], fx[1] = ce * P[k];
+                    fy[0] = ce * V[k], fy[2] = ce * P[k];
+                }
                 for (int f = 0; f < 3; ++f) fl[f][i] = c->eta_y[o2 + k] * fx[f] - c->eta_x[o2 + k] * fy[f];
             }
             for (int f = 0; f < 3; ++f)
@@ -983,8 +1016,12 @@ static void compute_dg_wave_derivative(ndgo_ctx* c) {
         for (int i = 0; i <= N; ++i) {
             for (int j = 0; j <= N; ++j) {
                 const int k = i * n + j;
-                const double fx[3] = {C_c * U[k], P[k], 0};
-                const double fy[3] = {C_c * V[k], 0, P[k]};
+                double fx[3] = {C_c * U[k], P[k], 0};
+                double fy[3] = {C_c * V[k], 0, P[k]};
+                if (c->speed) {
+                    fx[0] = ce * U[k], fx[1] = ce * P[k];
+                    fy[0] = ce * V[k], fy[2] = ce * P[k];
+                }
                 for (int f = 0; f < 3; ++f) fl[f][j] = -c->xi_y[o2 + k] * fx[f] + c->xi_x[o2 + k] * fy[f];
             }
             for (int f = 0; f < 3; ++f)
@@ -1179,4 +1216,421 @@ void ndgo_get_error(const ndgo_ctx* c, double* p_error, double* p_sigma, int* re
         refine[e] = c->refine[e];
         coarsen[e] = c->coarsen[e];
     }
+}
+
+/* ------------------------------------------------------------------------
+ * Variable-speed operator and its discrete adjoint (the CPU reference
+ * gradient of the library's adjoint). Plain loops: every forward pass of
+ * ndgo_stage is transposed on its own, in reverse order, on meshes of one
+ * order with conforming faces; the c-derivative of the face flux is taken
+ * per face (both sides' owners receive half of it). */
+
+static int64_t total1(const ndgo_ctx* c) { return c->off1[c->n_elem_total - 1] + 4 * (c->eN[c->n_elem_total - 1] + 1); }
+static int64_t total_faces(const ndgo_ctx* c) { return c->n_faces ? c->foff[c->n_faces - 1] + c->fN[c->n_faces - 1] + 1 : 0; }
+static int64_t domain_size(const ndgo_ctx* c) { return c->off2[c->n_elem - 1] + (c->eN[c->n_elem - 1] + 1) * (c->eN[c->n_elem - 1] + 1); }
+
+void ndgo_set_speed(ndgo_ctx* c, const double* speed) {
+    free(c->speed);
+    free(c->speed_owner);
+    c->speed = NULL;
+    c->speed_owner = NULL;
+    if (!speed) return;
+    c->speed = (double*)xcalloc((size_t)c->n_elem, sizeof(double));
+    memcpy(c->speed, speed, (size_t)c->n_elem * sizeof(double));
+    c->speed_owner = (int64_t*)xcalloc((size_t)c->n_elem_total, sizeof(int64_t));
+    for (int64_t e = 0; e < c->n_elem_total; ++e) c->speed_owner[e] = e;
+    /* a boundary ghost carries the speed of the element across its face */
+    for (int64_t g = c->n_elem; g < c->n_elem_total; ++g) {
+        const int64_t f = c->eface[4 * g];
+        if (f >= 0) c->speed_owner[g] = c->felem[2 * f] == g ? c->felem[2 * f + 1] : c->felem[2 * f];
+    }
+    /* a periodic ghost carries the speed of the element whose trace it copies */
+    for (int64_t q = 0; q < c->n_if; ++q) c->speed_owner[c->if_dest[q]] = c->if_origin[q];
+}
+
+typedef struct {
+    double *pe, *ue, *ve;    /* adjoints of the side traces */
+    double *pfe, *ufe, *vfe; /* adjoints of the element side fluxes */
+    double *f0[3], *f1[3];   /* adjoints of the face traces (left, right) */
+    double* fl[3];           /* adjoints of the face fluxes */
+} adj_work;
+
+static void adj_work_alloc(const ndgo_ctx* c, adj_work* w) {
+    const size_t s1 = (size_t)total1(c), sf = (size_t)total_faces(c);
+    w->pe = (double*)xcalloc(s1, sizeof(double));
+    w->ue = (double*)xcalloc(s1, sizeof(double));
+    w->ve = (double*)xcalloc(s1, sizeof(double));
+    w->pfe = (double*)xcalloc(s1, sizeof(double));
+    w->ufe = (double*)xcalloc(s1, sizeof(double));
+    w->vfe = (double*)xcalloc(s1, sizeof(double));
+    for (int f = 0; f < 3; ++f) {
+        w->f0[f] = (double*)xcalloc(sf, sizeof(double));
+        w->f1[f] = (double*)xcalloc(sf, sizeof(double));
+        w->fl[f] = (double*)xcalloc(sf, sizeof(double));
+    }
+}
+
+static void adj_work_free(adj_work* w) {
+    free(w->pe), free(w->ue), free(w->ve), free(w->pfe), free(w->ufe), free(w->vfe);
+    for (int f = 0; f < 3; ++f) free(w->f0[f]), free(w->f1[f]), free(w->fl[f]);
+}
+
+static void adj_work_zero(const ndgo_ctx* c, adj_work* w) {
+    const size_t s1 = (size_t)total1(c), sf = (size_t)total_faces(c);
+    double* a1[] = {w->pe, w->ue, w->ve, w->pfe, w->ufe, w->vfe};
+    for (int k = 0; k < 6; ++k) memset(a1[k], 0, s1 * sizeof(double));
+    for (int f = 0; f < 3; ++f) {
+        memset(w->f0[f], 0, sf * sizeof(double));
+        memset(w->f1[f], 0, sf * sizeof(double));
+        memset(w->fl[f], 0, sf * sizeof(double));
+    }
+}
+
+/* The forward passes of one stage up to the element time derivative G, on
+ * the state in c->p, c->u, c->v (no RK update). */
+static void operator_passes(ndgo_ctx* c) {
+    interpolate_to_boundaries(c);
+    boundary_conditions(c, 0.0);
+    project_to_faces(c);
+    calculate_wave_fluxes(c);
+    project_to_elements(c);
+    compute_dg_wave_derivative(c);
+}
+
+/* Transpose of ghost_projection (the velocity mirror, then the projection of
+ * the neighbour's side trace), adding to the neighbour's trace adjoints and
+ * consuming the ghost's. */
+static void ghost_projection_transpose(ndgo_ctx* c, adj_work* w, int64_t ge, int mirror) {
+    const int N = c->eN[ge];
+    const double* xe = c->T.t[T_NODES][N];
+    const double* we = c->T.t[T_WEIGHTS][N];
+    const double* bwe = c->T.t[T_BARY][N];
+    double* gp = w->pe + c->off1[ge];
+    double* gu = w->ue + c->off1[ge];
+    double* gv = w->ve + c->off1[ge];
+    const double* sf = c->sf + c->off1[ge];
+    if (mirror) {
+        const int64_t f = c->eface[4 * ge];
+        const double nxv = c->normal[2 * f], nyv = c->normal[2 * f + 1];
+        const double tx = c->tangent[2 * f], ty = c->tangent[2 * f + 1];
+        for (int k = 0; k <= N; ++k) {
+            /* the mirror -n n^T + t t^T is symmetric: its own transpose */
+            const double Vx = gu[k], Vy = gv[k];
+            const double l0 = -(Vx * nxv + Vy * nyv);
+            const double l1 = Vx * tx + Vy * ty;
+            gu[k] = nxv * l0 + tx * l1;
+            gv[k] = nyv * l0 + ty * l1;
+        }
+    }
+    for (int fi = 0; fi < c->eface_cnt[4 * ge]; ++fi) {
+        const int64_t f = c->eface[4 * ge + fi];
+        const int fs = c->felem[2 * f] == ge;
+        const int64_t nb = c->felem[2 * f + fs];
+        const int64_t nbs = c->fside[2 * f + fs];
+        const int Nn = c->eN[nb], nn = Nn + 1;
+        const double* xnb = c->T.t[T_NODES][Nn];
+        const double* wnb = c->T.t[T_WEIGHTS][Nn];
+        double* np_ = w->pe + c->off1[nb] + nbs * nn;
+        double* nu_ = w->ue + c->off1[nb] + nbs * nn;
+        double* nv_ = w->ve + c->off1[nb] + nbs * nn;
+        for (int j = 0; j <= Nn; ++j) {
+            const double coord = (xnb[Nn - j] + 1) * c->scale[2 * f + fs] + 2 * c->offset[2 * f + fs] - 1;
+            int found = 0;
+            for (int i = 0; i <= N; ++i) {
+                if (almost_equal(coord, xe[i])) {
+                    np_[j] += wnb[j] / we[i] * sf[i] * gp[i];
+                    nu_[j] += wnb[j] / we[i] * sf[i] * gu[i];
+                    nv_[j] += wnb[j] / we[i] * sf[i] * gv[i];
+                    found = 1;
+                    break;
+                }
+            }
+            if (!found) {
+                double s = 0.0;
+                for (int i = 0; i <= N; ++i) s += bwe[i] / (coord - xe[i]);
+                for (int i = 0; i <= N; ++i) {
+                    const double T = bwe[i] / ((coord - xe[i]) * s);
+                    np_[j] += T * wnb[j] / we[i] * sf[i] * gp[i];
+                    nu_[j] += T * wnb[j] / we[i] * sf[i] * gu[i];
+                    nv_[j] += T * wnb[j] / we[i] * sf[i] * gv[i];
+                }
+            }
+        }
+    }
+    for (int k = 0; k <= N; ++k) gp[k] = gu[k] = gv[k] = 0.0;
+}
+
+/* lq += L(c)^T mu; dc (optional) += d(mu . L(c) q)/dc where q is the state
+ * whose forward passes were run last (its face traces and fluxes are in c).
+ * mu, lq: field blocks p, u, v of domain_size values each. Returns -1 on a
+ * non-conforming face. */
+static int operator_transpose(ndgo_ctx* c, adj_work* w, const double* mu, double* lq, double* dc) {
+    const int64_t fsz = domain_size(c);
+    adj_work_zero(c, w);
+    /* compute_dg_wave_derivative^T */
+    double lfl[3][33];
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        const int N = c->eN[e], n = N + 1;
+        const double* Dh = c->T.t[T_DHAT][N];
+        const double* lm = c->T.t[T_LL][N];
+        const double* lp = c->T.t[T_LR][N];
+        const double* wt = c->T.t[T_WEIGHTS][N];
+        const int64_t o2 = c->off2[e], o1 = c->off1[e];
+        const double ce = c->speed ? c->speed[e] : 1.0;
+        const double* P = c->p + o2;
+        const double* U = c->u + o2;
+        const double* V = c->v + o2;
+        const double* M[3] = {mu + o2, mu + fsz + o2, mu + 2 * fsz + o2};
+        double* LQ[3] = {lq + o2, lq + fsz + o2, lq + 2 * fsz + o2};
+        double* LFE[3] = {w->pfe + o1, w->ufe + o1, w->vfe + o1};
+        double dce = 0.0;
+        for (int pass = 0; pass < 2; ++pass) {
+            for (int a = 0; a <= N; ++a) {
+                /* pass 0: xi lines (column j = a); pass 1: eta lines (row i = a) */
+                double nu[3][33];
+                for (int b = 0; b <= N; ++b) {
+                    const int k = pass == 0 ? b * n + a : a * n + b;
+                    for (int f = 0; f < 3; ++f) nu[f][b] = -M[f][k] / c->jac[o2 + k];
+                }
+                for (int f = 0; f < 3; ++f)
+                    for (int m = 0; m <= N; ++m) {
+                        lfl[f][m] = 0.0;
+                        for (int b = 0; b <= N; ++b) lfl[f][m] += Dh[b * n + m] * nu[f][b];
+                    }
+                for (int f = 0; f < 3; ++f)
+                    for (int b = 0; b <= N; ++b) {
+                        if (pass == 0) {
+                            LFE[f][1 * n + a] += nu[f][b] * lp[b] / wt[b];
+                            LFE[f][3 * n + N - a] += nu[f][b] * lm[b] / wt[b];
+                        } else {
+                            LFE[f][2 * n + N - a] += nu[f][b] * lp[b] / wt[b];
+                            LFE[f][0 * n + a] += nu[f][b] * lm[b] / wt[b];
+                        }
+                    }
+                for (int m = 0; m <= N; ++m) {
+                    const int k = pass == 0 ? m * n + a : a * n + m;
+                    double lfx[3], lfy[3];
+                    for (int f = 0; f < 3; ++f) {
+                        if (pass == 0) {
+                            lfx[f] = c->eta_y[o2 + k] * lfl[f][m];
+                            lfy[f] = -c->eta_x[o2 + k] * lfl[f][m];
+                        } else {
+                            lfx[f] = -c->xi_y[o2 + k] * lfl[f][m];
+                            lfy[f] = c->xi_x[o2 + k] * lfl[f][m];
+                        }
+                    }
+                    /* fx = ce (u, p, 0), fy = ce (v, 0, p) */
+                    LQ[1][k] += ce * lfx[0];
+                    LQ[0][k] += ce * lfx[1];
+                    LQ[2][k] += ce * lfy[0];
+                    LQ[0][k] += ce * lfy[2];
+                    dce += U[k] * lfx[0] + P[k] * lfx[1] + V[k] * lfy[0] + P[k] * lfy[2];
+                }
+            }
+        }
+        if (dc) dc[e] += dce;
+    }
+    /* project_to_elements^T (conforming faces) */
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        const int N = c->eN[e], n = N + 1;
+        for (int s = 0; s < 4; ++s) {
+            const double* sf = c->sf + c->off1[e] + s * n;
+            const double* op = w->pfe + c->off1[e] + s * n;
+            const double* ou = w->ufe + c->off1[e] + s * n;
+            const double* ov = w->vfe + c->off1[e] + s * n;
+            const int64_t en0 = c->enodes[4 * e + s];
+            const int64_t en1 = c->enodes[4 * e + ((s + 1) * !(s + 1 == 4))];
+            const int64_t f0 = c->eface[4 * e + s];
+            if (c->eface_cnt[4 * e + s] != 1 || c->fN[f0] != N) return -1;
+            if (c->fnodes[2 * f0] == en0 && c->fnodes[2 * f0 + 1] == en1) {
+                for (int j = 0; j <= N; ++j) {
+                    const int64_t k = c->foff[f0] + j;
+                    w->fl[0][k] += op[j] * sf[j];
+                    w->fl[1][k] += ou[j] * sf[j];
+                    w->fl[2][k] += ov[j] * sf[j];
+                }
+            } else if (c->fnodes[2 * f0 + 1] == en0 && c->fnodes[2 * f0] == en1) {
+                for (int j = 0; j <= N; ++j) {
+                    const int64_t k = c->foff[f0] + j;
+                    w->fl[0][k] -= op[N - j] * sf[j];
+                    w->fl[1][k] -= ou[N - j] * sf[j];
+                    w->fl[2][k] -= ov[N - j] * sf[j];
+                }
+            } else {
+                return -1;
+            }
+        }
+    }
+    /* calculate_wave_fluxes^T, with the face-speed derivative */
+    for (int64_t f = 0; f < c->n_faces; ++f) {
+        const double nxv = c->normal[2 * f], nyv = c->normal[2 * f + 1];
+        const double cf = c->speed ? face_speed(c, f) : 1.0;
+        double dcf = 0.0;
+        for (int i = 0; i <= c->fN[f]; ++i) {
+            const int64_t k = c->foff[f] + i;
+            const double gp = w->fl[0][k], gu = w->fl[1][k], gv = w->fl[2][k];
+            dcf += gp * c->fluxp[k] + gu * c->fluxu[k] + gv * c->fluxv[k];
+            const double lwL = cf * (gp / 2 + (nxv * gu + nyv * gv) / 2);
+            const double lwR = cf * (-gp / 2 + (nxv * gu + nyv * gv) / 2);
+            w->f0[0][k] += lwL;
+            w->f0[1][k] += lwL * nxv;
+            w->f0[2][k] += lwL * nyv;
+            w->f1[0][k] += lwR;
+            w->f1[1][k] -= lwR * nxv;
+            w->f1[2][k] -= lwR * nyv;
+        }
+        if (dc && c->speed) {
+            dc[c->speed_owner[c->felem[2 * f]]] += 0.5 * dcf / cf;
+            dc[c->speed_owner[c->felem[2 * f + 1]]] += 0.5 * dcf / cf;
+        }
+    }
+    /* project_to_faces^T (conforming) */
+    for (int64_t f = 0; f < c->n_faces; ++f) {
+        const int Nf = c->fN[f];
+        for (int side = 0; side < 2; ++side) {
+            const int64_t e = c->felem[2 * f + side];
+            const int64_t es = c->fside[2 * f + side];
+            const int ne_ = c->eN[e] + 1;
+            double* ep = w->pe + c->off1[e] + es * ne_;
+            double* eu = w->ue + c->off1[e] + es * ne_;
+            double* ev = w->ve + c->off1[e] + es * ne_;
+            double* const* src = side == 0 ? w->f0 : w->f1;
+            for (int i = 0; i <= Nf; ++i) {
+                const int d = side == 0 ? i : Nf - i;
+                const int64_t k = c->foff[f] + d;
+                ep[i] += src[0][k];
+                eu[i] += src[1][k];
+                ev[i] += src[2][k];
+            }
+        }
+    }
+    /* boundary_conditions^T, in reverse order */
+    for (int64_t q = c->n_if - 1; q >= 0; --q) {
+        const int64_t src = c->if_origin[q], dst = c->if_dest[q], side = c->if_origin_side[q];
+        const int N = c->eN[src], n = N + 1;
+        for (int k = 0; k <= N; ++k) {
+            w->pe[c->off1[src] + side * n + k] += w->pe[c->off1[dst] + k];
+            w->ue[c->off1[src] + side * n + k] += w->ue[c->off1[dst] + k];
+            w->ve[c->off1[src] + side * n + k] += w->ve[c->off1[dst] + k];
+            w->pe[c->off1[dst] + k] = w->ue[c->off1[dst] + k] = w->ve[c->off1[dst] + k] = 0.0;
+        }
+    }
+    for (int64_t b = c->nb[3] - 1; b >= 0; --b) ghost_projection_transpose(c, w, c->blist[3][b], 0);
+    for (int64_t b = c->nb[1] - 1; b >= 0; --b) ghost_projection_transpose(c, w, c->blist[1][b], 1);
+    for (int64_t b = c->nb[0] - 1; b >= 0; --b) ghost_projection_transpose(c, w, c->blist[0][b], 1);
+    /* interpolate_to_boundaries^T */
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        const int N = c->eN[e], n = N + 1;
+        const double* lm = c->T.t[T_LL][N];
+        const double* lp = c->T.t[T_LR][N];
+        const int64_t o2 = c->off2[e], o1 = c->off1[e];
+        double* LQ[3] = {lq + o2, lq + fsz + o2, lq + 2 * fsz + o2};
+        const double* ex[3] = {w->pe + o1, w->ue + o1, w->ve + o1};
+        for (int i = 0; i <= N; ++i)
+            for (int j = 0; j <= N; ++j)
+                for (int f = 0; f < 3; ++f) {
+                    LQ[f][i * n + j] += lm[j] * ex[f][0 * n + i] + lp[j] * ex[f][2 * n + N - i];
+                    LQ[f][j * n + i] += lp[j] * ex[f][1 * n + i] + lm[j] * ex[f][3 * n + N - i];
+                }
+    }
+    return 0;
+}
+
+static void set_state(ndgo_ctx* c, const double* p, const double* u, const double* v) {
+    const size_t bytes = (size_t)domain_size(c) * sizeof(double);
+    memcpy(c->p, p, bytes);
+    if (u) memcpy(c->u, u, bytes); else memset(c->u, 0, bytes);
+    if (v) memcpy(c->v, v, bytes); else memset(c->v, 0, bytes);
+}
+
+int ndgo_operator(ndgo_ctx* c, const double* x, double* Lx) {
+    const int64_t fsz = domain_size(c);
+    set_state(c, x, x + fsz, x + 2 * fsz);
+    operator_passes(c);
+    memcpy(Lx, c->Gp, (size_t)fsz * sizeof(double));
+    memcpy(Lx + fsz, c->Gu, (size_t)fsz * sizeof(double));
+    memcpy(Lx + 2 * fsz, c->Gv, (size_t)fsz * sizeof(double));
+    return 0;
+}
+
+int ndgo_operator_transpose(ndgo_ctx* c, const double* x, const double* y, double* LTy, double* dc) {
+    const int64_t fsz = domain_size(c);
+    set_state(c, x, x + fsz, x + 2 * fsz);
+    operator_passes(c);
+    memset(LTy, 0, 3 * (size_t)fsz * sizeof(double));
+    if (dc) memset(dc, 0, (size_t)c->n_elem * sizeof(double));
+    adj_work w;
+    adj_work_alloc(c, &w);
+    const int rc = operator_transpose(c, &w, y, LTy, dc);
+    adj_work_free(&w);
+    return rc;
+}
+
+static double sample(const ndgo_ctx* c, int64_t elem, const double* wr) {
+    const int n = c->eN[elem] + 1;
+    const double* p = c->p + c->off2[elem];
+    double s = 0.0;
+    for (int i = 0; i < n * n; ++i) s += wr[i] * p[i];
+    return s;
+}
+
+double ndgo_adjoint_solve(ndgo_ctx* c, const double* p0, const double* u0, const double* v0, double dt, int64_t n_steps,
+                          int n_rec, const int64_t* rec_elem, const double* rec_w, const double* targets,
+                          double* samples, double* grad_p, double* grad_u, double* grad_v, double* grad_c) {
+    const int64_t fsz = domain_size(c);
+    const int NN = (c->eN[0] + 1) * (c->eN[0] + 1);
+    const size_t state = 3 * (size_t)fsz;
+    double* Q = (double*)xcalloc((size_t)n_steps * 3 * state, sizeof(double));
+    double* smp = (double*)xcalloc((size_t)(n_steps + 1) * (size_t)(n_rec > 0 ? n_rec : 1), sizeof(double));
+    set_state(c, p0, u0, v0);
+    for (int r = 0; r < n_rec; ++r) smp[r] = sample(c, rec_elem[r], rec_w + (size_t)r * NN);
+    double J = 0.0;
+    for (int64_t s = 1; s <= n_steps; ++s) {
+        for (int m = 0; m < 3; ++m) {
+            double* q = Q + ((size_t)(s - 1) * 3 + (size_t)m) * state;
+            memcpy(q, c->p, (size_t)fsz * sizeof(double));
+            memcpy(q + fsz, c->u, (size_t)fsz * sizeof(double));
+            memcpy(q + 2 * fsz, c->v, (size_t)fsz * sizeof(double));
+            ndgo_stage(c, m, 0.0, dt);
+        }
+        for (int r = 0; r < n_rec; ++r) {
+            smp[s * n_rec + r] = sample(c, rec_elem[r], rec_w + (size_t)r * NN);
+            const double d = smp[s * n_rec + r] - (targets ? targets[s * n_rec + r] : 0.0);
+            J += d * d;
+        }
+    }
+    J *= 0.5 * dt;
+    if (samples) memcpy(samples, smp, (size_t)(n_steps + 1) * (size_t)n_rec * sizeof(double));
+
+    /* reverse sweep */
+    double* lq = (double*)xcalloc(state, sizeof(double));
+    double* lk = (double*)xcalloc(state, sizeof(double));
+    double* mu = (double*)xcalloc(state, sizeof(double));
+    double* dc = (double*)xcalloc((size_t)c->n_elem, sizeof(double));
+    adj_work w;
+    adj_work_alloc(c, &w);
+    int rc = 0;
+    for (int64_t s = n_steps; s >= 1 && rc == 0; --s) {
+        /* the misfit's derivative at the end of step s */
+        for (int r = 0; r < n_rec; ++r) {
+            const double res = dt * (smp[s * n_rec + r] - (targets ? targets[s * n_rec + r] : 0.0));
+            const double* wr = rec_w + (size_t)r * NN;
+            for (int i = 0; i < NN; ++i) lq[c->off2[rec_elem[r]] + i] += res * wr[i];
+        }
+        for (int m = 2; m >= 0 && rc == 0; --m) {
+            const double* q = Q + ((size_t)(s - 1) * 3 + (size_t)m) * state;
+            for (size_t i = 0; i < state; ++i) mu[i] = lk[i] + RK_G[m] * dt * lq[i];
+            set_state(c, q, q + fsz, q + 2 * fsz);
+            operator_passes(c);
+            rc = operator_transpose(c, &w, mu, lq, dc);
+            for (size_t i = 0; i < state; ++i) lk[i] = RK_A[m] * mu[i];
+        }
+    }
+    if (grad_p) memcpy(grad_p, lq, (size_t)fsz * sizeof(double));
+    if (grad_u) memcpy(grad_u, lq + fsz, (size_t)fsz * sizeof(double));
+    if (grad_v) memcpy(grad_v, lq + 2 * fsz, (size_t)fsz * sizeof(double));
+    if (grad_c) memcpy(grad_c, dc, (size_t)c->n_elem * sizeof(double));
+    adj_work_free(&w);
+    free(lq), free(lk), free(mu), free(dc), free(Q), free(smp);
+    return rc == 0 ? J : NAN;
 }

@@ -59,6 +59,26 @@ int64_t ndgo_get_boundary(const ndgo_ctx* ctx, int kind, int64_t* out);
 void ndgo_estimate_error(ndgo_ctx* ctx, double tolerance_min, double tolerance_max);
 void ndgo_get_error(const ndgo_ctx* ctx, double* p_error, double* p_sigma, int* refine, int* coarsen);
 
+/* Variable-speed operator (a wave speed per domain element: fluxes
+ * c_e (u, p, 0), c_e (v, 0, p) and the upwind face flux times the mean of
+ * the two sides' speeds; NULL restores the reference's constant c = 1) and
+ * its discrete adjoint, for meshes of one order with conforming faces.
+ * States: p, u, v blocks of field-size values each. */
+void ndgo_set_speed(ndgo_ctx* ctx, const double* speed);
+/* Lx = L(c) x (one stage's time derivative; boundary time 0). */
+int ndgo_operator(ndgo_ctx* ctx, const double* x, double* Lx);
+/* LTy = L(c)^T y and dc = d(y . L(c) x)/dc. Returns -1 on a non-conforming face. */
+int ndgo_operator_transpose(ndgo_ctx* ctx, const double* x, const double* y, double* LTy, double* dc);
+/* Forward solve of n_steps RK3 steps of dt from (p0, u0, v0) (u0, v0 may be
+ * NULL) with receivers (element, (N+1)^2 interpolation weights each) sampled
+ * after every step into samples ((n_steps+1) x n_rec, row 0 the initial
+ * state), the misfit J = dt/2 sum (sample - target)^2 over steps 1..n_steps
+ * (targets of the same shape, NULL = 0), and its gradient by the discrete
+ * adjoint (every stage input kept in memory). Returns J. */
+double ndgo_adjoint_solve(ndgo_ctx* ctx, const double* p0, const double* u0, const double* v0, double dt, int64_t n_steps,
+                          int n_rec, const int64_t* rec_elem, const double* rec_w, const double* targets,
+                          double* samples, double* grad_p, double* grad_u, double* grad_v, double* grad_c);
+
 #ifdef __cplusplus
 }
 #endif

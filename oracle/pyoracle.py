@@ -106,6 +106,14 @@ def _load_oracle():
         lib.ndgo_get_boundary.restype = C.c_int64
         lib.ndgo_estimate_error.argtypes = [C.c_void_p, C.c_double, C.c_double]
         lib.ndgo_get_error.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip]
+        lib.ndgo_set_speed.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ndgo_operator.argtypes = [C.c_void_p, _dp, _dp]
+        lib.ndgo_operator.restype = C.c_int
+        lib.ndgo_operator_transpose.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        lib.ndgo_operator_transpose.restype = C.c_int
+        lib.ndgo_adjoint_solve.argtypes = [C.c_void_p, _dp, C.c_void_p, C.c_void_p, C.c_double, C.c_int64,
+                                           C.c_int, _lp, _dp, C.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        lib.ndgo_adjoint_solve.restype = C.c_double
         _orc = lib
     return _orc
 
@@ -370,3 +378,47 @@ class OracleSolver(_Base):
              "coarsen": np.empty(n, dtype=np.int32)}
         self.lib.ndgo_get_error(self.ctx, d["p_error"], d["p_sigma"], d["refine"], d["coarsen"])
         return d
+
+    # Variable-speed operator and its discrete adjoint (CPU reference gradient).
+    def set_speed(self, speed):
+        if speed is None:
+            self.lib.ndgo_set_speed(self.ctx, None)
+            return
+        self._speed = np.ascontiguousarray(speed, dtype=np.float64).ravel()
+        assert self._speed.size == self.n_elements
+        self.lib.ndgo_set_speed(self.ctx, self._speed.ctypes.data)
+
+    def operator(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        out = np.empty_like(x)
+        if self.lib.ndgo_operator(self.ctx, x, out) != 0:
+            raise ValueError("operator failed")
+        return out
+
+    def operator_transpose(self, x, y) -> tuple[np.ndarray, np.ndarray]:
+        x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        y = np.ascontiguousarray(y, dtype=np.float64).ravel()
+        lty, dc = np.empty_like(y), np.empty(self.n_elements)
+        if self.lib.ndgo_operator_transpose(self.ctx, x, y, lty, dc) != 0:
+            raise ValueError("the transpose covers conforming faces of one order")
+        return lty, dc
+
+    def adjoint_solve(self, p0, dt: float, n_steps: int, rec_elem, rec_w, targets=None, u0=None, v0=None) -> dict:
+        """Forward solve with receivers, misfit J and its gradient (p0, u0, v0, c)."""
+        fs = self._field_size()
+        p0 = np.ascontiguousarray(p0, dtype=np.float64).ravel()
+        u0 = None if u0 is None else np.ascontiguousarray(u0, dtype=np.float64).ravel()
+        v0 = None if v0 is None else np.ascontiguousarray(v0, dtype=np.float64).ravel()
+        rec_elem = np.ascontiguousarray(rec_elem, dtype=np.int64).ravel()
+        rec_w = np.ascontiguousarray(rec_w, dtype=np.float64).ravel()
+        R = rec_elem.size
+        tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.float64).reshape(n_steps + 1, R)
+        samples = np.empty((n_steps + 1, max(R, 1)))
+        g = {k: np.empty(fs) for k in ("p0", "u0", "v0")}
+        g["c"] = np.empty(self.n_elements)
+        J = self.lib.ndgo_adjoint_solve(self.ctx, p0, None if u0 is None else u0.ctypes.data, None if v0 is None else v0.ctypes.data,
+                                        dt, n_steps, R, rec_elem if R else np.zeros(1, np.int64), rec_w if R else np.zeros(1),
+                                        None if tg is None else tg.ctypes.data, samples, g["p0"], g["u0"], g["v0"], g["c"])
+        g["J"] = J
+        g["samples"] = samples[:, :R]
+        return g
