@@ -37,6 +37,11 @@ sys.path.insert(0, ROOT)
 
 RES, ORDER, CFL, CONFIG_STEPS = 256, 8, 0.5, 2000
 BYTES_PER_DOF_STAGE = 32  # read + write of q and of the RK register, FP64
+# Adjoint workload: 96 x 96 walls, N = 7, 16 receivers, 1000 steps, checkpoints every 50.
+ADJ_RES, ADJ_N, ADJ_STEPS, ADJ_INTERVAL, ADJ_RECEIVERS = 96, 7, 1000, 50, 16
+# adjoint stage: lq and lk read and written, the stage input qs read (FP64);
+# forward stage keeping its input: q, k read and written, q written once more
+ADJ_BYTES_PER_DOF_STAGE = 40
 
 
 def workload_zone():
@@ -183,6 +188,76 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def adjoint_leg(local: int, stream, peak: float, cpu_sample: bool) -> dict:
+    """Gradient of a receiver misfit with respect to the initial pressure and a
+    per-element wave speed (the library's discrete adjoint): forward solve
+    with checkpoints, then recomputation + adjoint sweep, timed on the device
+    (CUDA events inside the library) and end to end through the API with
+    host buffers."""
+    import numpy as np
+    import ndg_cuda_b200 as ndg
+    from tests import adjoint_setup as A
+    from tests import meshgen
+    zone = meshgen.uniform_zone(ADJ_RES, order="rowmajor", boundary=meshgen.WALL)
+    c = A.speed_field(zone, seed=0)
+    mesh = ndg.Mesh2D_t(zone, ADJ_N, device=local, stream=stream.cuda_stream)
+    adj = ndg.Adjoint2D_t(mesh, A.circle_receivers(ADJ_RECEIVERS, 0.7), speed=c)
+    p0 = A.gaussian_pulse(zone, ADJ_N, sigma=0.1, centre=(0.45, 0.0))
+    dt = adj.delta_t(CFL)
+    # targets: the same run with a perturbed speed
+    adj.set_speed(c * (1 + 0.05 * np.sin(4 * A.element_centres(zone)[:, 0])))
+    _, target = adj.forward(p0, dt, ADJ_STEPS, checkpoint_interval=ADJ_INTERVAL)
+    adj.set_speed(c)
+    adj.forward(p0, dt, ADJ_STEPS, targets=target, checkpoint_interval=ADJ_INTERVAL)
+    adj.backward()  # warm-up
+    reps, fwd, bwd, wall_f, wall_b = 3, [], [], [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        J, _ = adj.forward(p0, dt, ADJ_STEPS, targets=target, checkpoint_interval=ADJ_INTERVAL)
+        t1 = time.perf_counter()
+        g = adj.backward()
+        t2 = time.perf_counter()
+        tm = adj.timings()
+        fwd.append(tm["forward_ms"])
+        bwd.append(tm["backward_ms"])
+        wall_f.append(1e3 * (t1 - t0))
+        wall_b.append(1e3 * (t2 - t1))
+    kernel = {"speed_stage": adj.time_stage(0, 30), "speed_stage_keeping_input": adj.time_stage(1, 30), "adjoint_stage": adj.time_stage(2, 30)}
+    dof = 3 * mesh.field_size
+    f_ms, b_ms = statistics.median(fwd), statistics.median(bwd)
+    roof = {}
+    for name, ms in kernel.items():
+        bytes_ = (BYTES_PER_DOF_STAGE if name == "speed_stage" else ADJ_BYTES_PER_DOF_STAGE) * dof
+        roof[name] = {"achieved_GBs": bytes_ / (ms / 1e3) / 1e9, "frac": bytes_ / (ms / 1e3) / 1e9 / peak,
+                      "algorithmic_bytes_per_launch": bytes_}
+    out = {"workload": f"adjoint_wave_rk3_walls_{ADJ_RES}x{ADJ_RES}_N{ADJ_N}_{ADJ_STEPS}_steps",
+           "setup": (f"{ADJ_RES}x{ADJ_RES} uniform quads with walls, N={ADJ_N}, c = 1 + 0.2 tanh(8 seeded Gaussian bumps, sigma 0.3), "
+                     f"{ADJ_RECEIVERS} receivers on a circle r=0.7, Gaussian pressure pulse sigma 0.1 at (0.45, 0), targets from "
+                     f"c (1 + 0.05 sin 4x), {ADJ_STEPS} RK3 steps at CFL {CFL}, checkpoints every {ADJ_INTERVAL} steps"),
+           "dof": dof, "steps": ADJ_STEPS, "checkpoint_interval": ADJ_INTERVAL, "dtype": "f64",
+           "forward_ms": f_ms, "backward_ms": b_ms, "adjoint_over_forward": b_ms / f_ms,
+           "forward_dof_stage_per_s": dof * 3 * ADJ_STEPS / (f_ms / 1e3),
+           "backward_dof_stage_per_s": dof * 3 * ADJ_STEPS / (b_ms / 1e3),
+           "wall_time_per_unit_time_s": {"forward": f_ms / 1e3 / (ADJ_STEPS * dt), "forward_plus_gradient": (f_ms + b_ms) / 1e3 / (ADJ_STEPS * dt)},
+           "e2e_forward_ms": statistics.median(wall_f), "e2e_backward_ms": statistics.median(wall_b),
+           "e2e_note": "host buffers: p0 and targets uploaded, samples and the four gradients downloaded inside the timed calls",
+           "kernel_ms": kernel, "roofline": roof, "launches": {"forward": tm["forward_launches"], "backward": tm["backward_launches"]},
+           "misfit": J, "grad_norm": {"p0": float(np.linalg.norm(g["p0"])), "c": float(np.linalg.norm(g["c"]))}}
+    if cpu_sample:
+        # the oracle's CPU FP64 adjoint on a bounded sample of the same problem
+        o, el, w = A.oracle_problem(zone, ADJ_N, c, A.circle_receivers(ADJ_RECEIVERS, 0.7))
+        n_cpu = 4
+        t0 = time.perf_counter()
+        o.adjoint_solve(p0, dt, n_cpu, el, w, targets=target[:n_cpu + 1])
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": dof * 3 * n_cpu / sec, "unit": "DOF-stage updates/s (forward + adjoint)", "cores": 1, "kind": "port",
+                               "sample": f"{n_cpu} steps forward and adjoint of the same problem with the oracle's CPU FP64 adjoint, 1 core",
+                               "seconds": sec}
+    adj.close()
+    mesh.close()
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import ndg_cuda_b200 as ndg
@@ -299,6 +374,10 @@ def run_ours(args) -> None:
                 "arithmetic": "traces, fluxes, metrics and volume term in FP32; q, k and the RK update in FP64"}
         m32.close()
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_leg(local, stream, peak, rank == 0 and world == 1 and not args.no_cpu_baseline)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(float(os.environ.get("NDG_CPU_BUDGET_S", "15")), 1000, 1)
@@ -317,6 +396,7 @@ def run_ours(args) -> None:
                              "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof, "peak_source": peak_kind},
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "fp32": fp32,
+                "adjoint": adjoint,
                 "gpu_launches": launches,
                 "clocks": clocks.summary()}
         print(json.dumps(line), flush=True)
@@ -335,6 +415,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference timing (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg (profiling runs)")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-form leg (profiling runs)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -313,6 +313,12 @@ ndg_status ndg_adjoint_operator(ndg_adjoint* adj, const double* x, const double*
  * stepping and of the last backward's recompute + adjoint stepping, in ms,
  * and the kernel launches of each. Any pointer may be NULL. */
 ndg_status ndg_adjoint_timings(const ndg_adjoint* adj, double* forward_ms, double* backward_ms, int64_t* forward_launches, int64_t* backward_launches);
+/* Benchmark aid: mean duration (CUDA events) of n_launches back-to-back
+ * launches of one kernel on the current state, after a forward and a
+ * backward: which = 0 the forward stage, 1 the forward stage keeping its
+ * input (the recomputation's), 2 the adjoint stage. The state advances; run
+ * a new forward before the next backward. */
+ndg_status ndg_adjoint_time_stage(ndg_adjoint* adj, int32_t which, int32_t n_launches, double* avg_ms);
 
 #ifdef __cplusplus
 }

@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
         "ndg_adjoint_backward": ([vp, vp, vp, vp, vp], C.c_int),
         "ndg_adjoint_operator": ([vp, vp, vp, vp, vp, vp], C.c_int),
         "ndg_adjoint_timings": ([vp, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64), C.POINTER(i64)], C.c_int),
+        "ndg_adjoint_time_stage": ([vp, i32, i32, C.POINTER(dbl)], C.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
@@ -493,6 +494,13 @@ class Adjoint2D_t:
         lf, lb = C.c_int64(), C.c_int64()
         _check(lib().ndg_adjoint_timings(self.h, C.byref(f), C.byref(b), C.byref(lf), C.byref(lb)))
         return {"forward_ms": f.value, "backward_ms": b.value, "forward_launches": lf.value, "backward_launches": lb.value}
+
+    def time_stage(self, which: int, n_launches: int) -> float:
+        """Mean kernel duration in ms: 0 forward stage, 1 forward stage
+        keeping its input, 2 adjoint stage (after a forward and a backward)."""
+        ms = C.c_double()
+        _check(lib().ndg_adjoint_time_stage(self.h, which, n_launches, C.byref(ms)))
+        return ms.value
 
     def close(self) -> None:
         if getattr(self, "h", None):

@@ -520,4 +520,47 @@ ndg_status ndg_adjoint_timings(const ndg_adjoint* adj, double* forward_ms, doubl
     });
 }
 
+ndg_status ndg_adjoint_time_stage(ndg_adjoint* adj, int32_t which, int32_t n_launches, double* avg_ms) {
+    return guarded([&] {
+        require_valid(adj);
+        if (which < 0 || which > 2 || n_launches < 1 || !avg_ms) fail(NDG_ERR_INVALID_ARG, "bad stage timing request");
+        if (!(adj->dt > 0.0) || adj->seg.count == 0) fail(NDG_ERR_INVALID_ARG, "stage timing needs a forward and a backward first");
+        ndg_ctx* c = adj->ctx;
+        make_current(c);
+        cudaStream_t s = c->stream;
+        std::vector<cudaEvent_t> ev(static_cast<size_t>(2 * n_launches));
+        for (auto& e : ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+        launch_traces_of_q(adj, 0);
+        int in = 0;
+        for (int i = 0; i < n_launches; ++i) {
+            check_cuda(cudaEventRecord(ev[static_cast<size_t>(2 * i)], s), "cudaEventRecord");
+            if (which < 2) {
+                dev::SpeedStageArgs a = speed_args(adj, 1, in, adj->dt);
+                if (which == 1) a.q_save = adj->seg.ptr;
+                check_cuda(dev::launch_speed_stage(adj->N, a, s), "speed stage launch");
+            } else {
+                dev::AdjointStageArgs a = adjoint_args(adj, in);
+                a.qs = adj->seg.ptr;
+                a.rk_a = kRkA[1];
+                a.gdt = kRkG[1] * adj->dt;
+                a.gdt_next = kRkG[0] * adj->dt;
+                check_cuda(dev::launch_adjoint_stage(adj->N, a, s), "adjoint stage launch");
+            }
+            check_cuda(cudaEventRecord(ev[static_cast<size_t>(2 * i + 1)], s), "cudaEventRecord");
+            in = 1 - in;
+        }
+        check_cuda(cudaStreamSynchronize(s), "stage timing");
+        check_kernel_error(adj);
+        double total = 0.0;
+        for (int i = 0; i < n_launches; ++i) {
+            float ms = 0.0f;
+            check_cuda(cudaEventElapsedTime(&ms, ev[static_cast<size_t>(2 * i)], ev[static_cast<size_t>(2 * i + 1)]), "cudaEventElapsedTime");
+            total += ms;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        *avg_ms = total / n_launches;
+        adj->has_forward = false;  // the state advanced
+    });
+}
+
 }  // extern "C"

@@ -96,11 +96,11 @@ def locate_receivers(zone: dict, xy: np.ndarray) -> tuple[np.ndarray, np.ndarray
     elems, coords = [], []
     if len(xy) == 0:
         return np.zeros(0, np.int64), np.zeros((0, 2))
+    lo_all, hi_all = cr.min(axis=1), cr.max(axis=1)
     for px, py in xy:
-        for e, c in enumerate(cr):
-            lo, hi = c.min(axis=0), c.max(axis=0)
-            if not (lo[0] - 1e-12 <= px <= hi[0] + 1e-12 and lo[1] - 1e-12 <= py <= hi[1] + 1e-12):
-                continue
+        inside = (lo_all[:, 0] - 1e-12 <= px) & (px <= hi_all[:, 0] + 1e-12) & (lo_all[:, 1] - 1e-12 <= py) & (py <= hi_all[:, 1] + 1e-12)
+        for e in np.nonzero(inside)[0]:
+            c = cr[e]
             xi = eta = 0.0
             for _ in range(50):
                 w = np.array([(1 - xi) * (1 - eta), (1 + xi) * (1 - eta), (1 + xi) * (1 + eta), (1 - xi) * (1 + eta)]) / 4
@@ -113,7 +113,7 @@ def locate_receivers(zone: dict, xy: np.ndarray) -> tuple[np.ndarray, np.ndarray
                 if abs(d).sum() < 1e-15:
                     break
             if abs(xi) <= 1 + 1e-12 and abs(eta) <= 1 + 1e-12:
-                elems.append(e)
+                elems.append(int(e))
                 coords.append((xi, eta))
                 break
         else:
