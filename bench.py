@@ -39,6 +39,8 @@ RES, ORDER, CFL, CONFIG_STEPS = 256, 8, 0.5, 2000
 BYTES_PER_DOF_STAGE = 32  # read + write of q and of the RK register, FP64
 # Adjoint workload: 96 x 96 walls, N = 7, 16 receivers, 1000 steps, checkpoints every 50.
 ADJ_RES, ADJ_N, ADJ_STEPS, ADJ_INTERVAL, ADJ_RECEIVERS = 96, 7, 1000, 50, 16
+# Batched workload: 64 instances on one 64 x 64 walled mesh, N = 6, 1000 steps.
+BATCH_RES, BATCH_N, BATCH_INSTANCES, BATCH_STEPS = 64, 6, 64, 1000
 # adjoint stage: lq and lk read and written, the stage input qs read (FP64);
 # forward stage keeping its input: q, k read and written, q written once more
 ADJ_BYTES_PER_DOF_STAGE = 40
@@ -188,6 +190,75 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def batched_leg(local: int, stream, peak: float, dist) -> dict:
+    """Many independent runs on one mesh in one launch per stage (instances
+    as the grid's second dimension), the RK3 step as a CUDA graph, the tile
+    chosen by the autotuner per form; FP64 against the FP32 form."""
+    import numpy as np
+    import torch
+    import ndg_cuda_b200 as ndg
+    from tests import adjoint_setup as A
+    from tests import meshgen
+    zone = meshgen.uniform_zone(BATCH_RES, boundary=meshgen.WALL)
+    rng = np.random.default_rng(64)
+    centres = rng.uniform(-0.8, 0.8, size=(BATCH_INSTANCES, 2))
+    p0 = np.concatenate([A.gaussian_pulse(zone, BATCH_N, sigma=0.05, centre=c) for c in centres])
+    zeros = np.zeros_like(p0)
+    out = {"workload": f"batched_wave_rk3_walls_{BATCH_RES}x{BATCH_RES}_N{BATCH_N}_{BATCH_INSTANCES}_instances",
+           "setup": (f"{BATCH_INSTANCES} independent runs on one {BATCH_RES}x{BATCH_RES} walled mesh, N={BATCH_N}, each a radial "
+                     f"Gaussian pressure pulse sigma 0.05 at a seeded uniform centre in [-0.8,0.8]^2 (u = v = 0), "
+                     f"{BATCH_STEPS} RK3 steps at CFL {CFL}; one launch per stage for all instances, the step as a CUDA graph")}
+    meshes = {}
+    for name, prec in (("fp64", ndg.FP64), ("fp32", ndg.FP32)):
+        m = ndg.Mesh2D_t(zone, BATCH_N, cfl=CFL, n_instances=BATCH_INSTANCES, device=local, stream=stream.cuda_stream, precision=prec)
+        meshes[name] = m
+
+        def reset(m=m):
+            m.set_field("p", p0)
+            for f in ("u", "v", "k_p", "k_u", "k_v"):
+                m.set_field(f, zeros)
+
+        reset()
+        tile, tile_ms = m.autotune(20)
+        reset()
+        ndg.Solver2D_t.run(m, 3)
+        reset()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist is not None:
+            dist.barrier()
+        e0.record(stream)
+        ndg.Solver2D_t.run(m, BATCH_STEPS)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        ms = float(ms.item())
+        dof = ndg.dof_count(m)
+        world = dist.get_world_size() if dist is not None else 1
+        stage_ms = m.time_stage(1, 20)
+        out[name] = {"value": world * dof * 3 * BATCH_STEPS / (ms / 1e3), "unit": "DOF-stage updates/s", "ms_per_step": ms / BATCH_STEPS,
+                     "kernel_ms": stage_ms, "roofline_frac": BYTES_PER_DOF_STAGE * dof / (stage_ms / 1e3) / 1e9 / peak,
+                     "tile": {"elements_per_cta": tile if tile else m.tile_candidates()[1], "autotuner_choice": "candidate" if tile else "default",
+                              "candidates": m.tile_candidates()[0], "tuned_ms_per_launch": tile_ms}}
+        out["dof"] = dof
+    # FP32 against FP64 after the configuration's steps from the same state
+    for m in meshes.values():
+        m.set_field("p", p0)
+        for f in ("u", "v", "k_p", "k_u", "k_v"):
+            m.set_field(f, zeros)
+        ndg.Solver2D_t.run(m, BATCH_STEPS)
+    err = {}
+    for f in ("p", "u", "v"):
+        a64, a32 = meshes["fp64"].get_field(f), meshes["fp32"].get_field(f)
+        err[f] = float(np.linalg.norm(a32 - a64) / max(np.linalg.norm(a64), 1e-300))
+    out["fp32_rel_l2_vs_fp64"] = err
+    for m in meshes.values():
+        m.close()
+    return out
+
+
 def adjoint_leg(local: int, stream, peak: float, cpu_sample: bool) -> dict:
     """Gradient of a receiver misfit with respect to the initial pressure and a
     per-element wave speed (the library's discrete adjoint): forward solve
@@ -277,6 +348,7 @@ def run_ours(args) -> None:
     mesh.initial_conditions()
     dof = ndg.dof_count(mesh)
     assert dof == dof_count()
+    tile, _ = mesh.autotune(20)  # fields are restored by the tuner
 
     ndg.Solver2D_t.run(mesh, args.warmup)
     torch.cuda.synchronize()
@@ -348,6 +420,7 @@ def run_ours(args) -> None:
     if not args.no_fp32:
         m32 = ndg.Mesh2D_t(zone, ORDER, cfl=CFL, device=local, stream=stream.cuda_stream, precision=ndg.FP32)
         m32.initial_conditions()
+        tile32, _ = m32.autotune(20)
         ndg.Solver2D_t.run(m32, args.warmup)
         barrier()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -370,9 +443,13 @@ def run_ours(args) -> None:
         fp32 = {"value": world * dof * 3 * args.steps / (float(f_ms.item()) / 1e3), "unit": "DOF-stage updates/s",
                 "ms_per_step": float(f_ms.item()) / args.steps, "kernel": f"stage_kernel_f32<{ORDER}>", "kernel_ms": stage32_ms,
                 "roofline_frac": BYTES_PER_DOF_STAGE * dof / (stage32_ms / 1e3) / 1e9 / peak,
-                "rel_l2_vs_fp64": err, "steps_compared": CONFIG_STEPS,
+                "rel_l2_vs_fp64": err, "steps_compared": CONFIG_STEPS, "tile_elements_per_cta": tile32 or m32.tile_candidates()[1],
                 "arithmetic": "traces, fluxes, metrics and volume term in FP32; q, k and the RK update in FP64"}
         m32.close()
+
+    batched = None
+    if not args.no_batched:
+        batched = batched_leg(local, stream, peak, dist)
 
     adjoint = None
     if not args.no_adjoint:
@@ -392,10 +469,12 @@ def run_ours(args) -> None:
                         "d2h_bytes_per_step": state_bytes, "rk3_steps_per_e2e_step": CONFIG_STEPS, "e2e_steps": e2e_steps,
                         "host_wall_s": wall},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "traffic": traffic, "kernel": f"stage_kernel<{ORDER}, false>", "kernel_ms": stage_ms,
+                             "traffic": traffic, "kernel": f"stage_kernel<{ORDER}, false, {tile}>", "kernel_ms": stage_ms,
+                             "tile_elements_per_cta": tile or mesh.tile_candidates()[1], "tile_source": "autotuner",
                              "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof, "peak_source": peak_kind},
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "fp32": fp32,
+                "batched": batched,
                 "adjoint": adjoint,
                 "gpu_launches": launches,
                 "clocks": clocks.summary()}
@@ -416,6 +495,7 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg (profiling runs)")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-form leg (profiling runs)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (profiling runs)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -235,6 +235,22 @@ ndg_status ndg_adapt_flags(ndg_ctx* ctx, const int32_t* refine, const double* p_
  * *avg_ms = mean kernel duration. */
 ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* avg_ms);
 
+/* Autotuner (no reference counterpart). The uniform-order stage kernel is
+ * compiled for several tiles (elements per CTA: 2, 4, 6, 8, 12, 16 where a
+ * tile fits 512 threads and 113 KB of shared memory) besides its default.
+ * ndg_autotune times n_launches launches of each tile, and of the default,
+ * on the loaded mesh and instances in the context's current form (FP64 or
+ * FP32), keeps the fastest for later stepping and returns it (0 = the
+ * default) with its mean launch time. The fields are restored afterwards.
+ * Tiles do not change results: every element computes the same operations
+ * whatever tile holds it. Mixed-order meshes and the strict form keep their
+ * tiles (the call returns 0). Tiles reset when the mesh changes. */
+ndg_status ndg_autotune(ndg_ctx* ctx, int32_t n_launches, int32_t* elements_per_block, double* best_ms);
+/* Sets the tile of the current form by hand (0 = the default). */
+ndg_status ndg_set_tile(ndg_ctx* ctx, int32_t elements_per_block);
+/* The candidate tiles of the loaded order and current form, and the default. */
+ndg_status ndg_tile_candidates(const ndg_ctx* ctx, int32_t* out, int32_t capacity, int32_t* count, int32_t* default_tile);
+
 /* Kernel launches issued by this context so far (for launch accounting). */
 ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches);
 

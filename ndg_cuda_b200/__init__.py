@@ -94,6 +94,9 @@ def lib() -> C.CDLL:
         "ndg_adapt": ([vp], C.c_int),
         "ndg_adapt_flags": ([vp, vp, vp], C.c_int),
         "ndg_delta_t_from_device": ([vp, vp, i64, dbl, vp, C.POINTER(dbl)], C.c_int),
+        "ndg_autotune": ([vp, i32, C.POINTER(i32), C.POINTER(dbl)], C.c_int),
+        "ndg_set_tile": ([vp, i32], C.c_int),
+        "ndg_tile_candidates": ([vp, vp, i32, C.POINTER(i32), C.POINTER(i32)], C.c_int),
         "ndg_adjoint_create": ([vp, i32, vp, C.POINTER(vp)], C.c_int),
         "ndg_adjoint_destroy": ([vp], C.c_int),
         "ndg_adjoint_set_speed": ([vp, vp], C.c_int),
@@ -319,6 +322,22 @@ class Mesh2D_t:
         ms = C.c_double()
         _check(lib().ndg_time_stage(self._ctx.h, m, n_launches, C.byref(ms)))
         return ms.value
+
+    def autotune(self, n_launches: int = 20) -> tuple[int, float]:
+        """Times every candidate tile of the stage kernel on this mesh and
+        keeps the fastest: (elements per CTA, 0 = default; ms per launch)."""
+        e, ms = C.c_int32(), C.c_double()
+        _check(lib().ndg_autotune(self._ctx.h, n_launches, C.byref(e), C.byref(ms)))
+        return e.value, ms.value
+
+    def set_tile(self, elements_per_block: int) -> None:
+        _check(lib().ndg_set_tile(self._ctx.h, elements_per_block))
+
+    def tile_candidates(self) -> tuple[list[int], int]:
+        out = (C.c_int32 * 16)()
+        n, d = C.c_int32(), C.c_int32()
+        _check(lib().ndg_tile_candidates(self._ctx.h, C.cast(out, C.c_void_p), 16, C.byref(n), C.byref(d)))
+        return list(out[:n.value]), d.value
 
     def launches(self) -> int:
         n = C.c_int64()

@@ -111,7 +111,11 @@ cudaError_t issue_stage(ndg_ctx* c, int m, int in) {
         if (fp32(c)) return cudaErrorNotSupported;  // rejected by require_form before any capture
         return dev::launch_general_stage(general_args(c, m), c->groups.data(), static_cast<int>(c->groups.size()), strict(c), c->stream);
     }
-    if (fp32(c)) return dev::launch_stage_f32(c->N, stage_args(c, m, in), c->stream);
+    if (fp32(c)) {
+        if (c->tile[1]) return dev::launch_stage_variant_fp32(c->N, c->tile[1], stage_args(c, m, in), c->stream);
+        return dev::launch_stage_f32(c->N, stage_args(c, m, in), c->stream);
+    }
+    if (!strict(c) && c->tile[0]) return dev::launch_stage_variant_fp64(c->N, c->tile[0], stage_args(c, m, in), c->stream);
     return dev::launch_stage(c->N, strict(c), stage_args(c, m, in), c->stream);
 }
 
@@ -129,6 +133,23 @@ void launch_stage(ndg_ctx* c, int m) {
         c->cur = 1 - c->cur;
         ++c->launches;
     }
+}
+
+// The tile candidates of the context's form (FP64 or FP32).
+std::vector<int> tile_candidates(const ndg_ctx* c) {
+    int buf[16];
+    const int n = fp32(c) ? dev::tile_candidates_fp32(c->N, buf, 16) : dev::tile_candidates_fp64(c->N, buf, 16);
+    return std::vector<int>(buf, buf + n);
+}
+
+void set_tile(ndg_ctx* c, int epb) {
+    if (epb != 0) {
+        const std::vector<int> cand = tile_candidates(c);
+        if (std::find(cand.begin(), cand.end(), epb) == cand.end()) fail(NDG_ERR_INVALID_ARG, "not a candidate tile of this order and form");
+        check_cuda(fp32(c) ? dev::prepare_stage_variant_fp32(c->N, epb) : dev::prepare_stage_variant_fp64(c->N, epb), "kernel attributes");
+    }
+    c->tile[fp32(c) ? 1 : 0] = epb;
+    drop_graphs(c);
 }
 
 void ensure_traces(ndg_ctx* c) {
@@ -260,6 +281,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
     c->K = c->topo.n_domain;
     c->Kp = c->K + (c->K & 1);
     c->N = *std::max_element(l.N.begin(), l.N.end());
+    c->tile[0] = c->tile[1] = 0;
     const size_t K = static_cast<size_t>(c->K);
     if (!l.general) {
         if (c->N > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "orders above 16 have no compiled kernel");
@@ -996,6 +1018,89 @@ ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* a
         }
         for (auto& e : ev) cudaEventDestroy(e);
         *avg_ms = total / n_launches;
+    });
+}
+
+ndg_status ndg_tile_candidates(const ndg_ctx* ctx, int32_t* out, int32_t capacity, int32_t* count, int32_t* default_tile) {
+    return guarded([&] {
+        require_mesh(ctx);
+        if (ctx->general) fail(NDG_ERR_UNSUPPORTED, "tiles are tuned for meshes of one order");
+        const std::vector<int> cand = tile_candidates(ctx);
+        if (count) *count = static_cast<int32_t>(cand.size());
+        if (out) {
+            if (capacity < static_cast<int32_t>(cand.size())) fail(NDG_ERR_INVALID_ARG, "output buffer too small");
+            std::copy(cand.begin(), cand.end(), out);
+        }
+        if (default_tile) *default_tile = dev::elements_per_block(ctx->N);
+    });
+}
+
+ndg_status ndg_set_tile(ndg_ctx* ctx, int32_t elements_per_block) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (ctx->general) fail(NDG_ERR_UNSUPPORTED, "tiles are tuned for meshes of one order");
+        if (strict(ctx) && elements_per_block != 0) fail(NDG_ERR_UNSUPPORTED, "the strict form keeps its default tile");
+        make_current(ctx);
+        set_tile(ctx, elements_per_block);
+    });
+}
+
+ndg_status ndg_autotune(ndg_ctx* ctx, int32_t n_launches, int32_t* elements_per_block, double* best_ms) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (n_launches < 1) fail(NDG_ERR_INVALID_ARG, "n_launches must be >= 1");
+        make_current(ctx);
+        const int form = fp32(ctx) ? 1 : 0;
+        if (ctx->general || strict(ctx)) {
+            // mixed-order meshes and the strict form keep their tiles
+            if (elements_per_block) *elements_per_block = 0;
+            if (best_ms) *best_ms = 0.0;
+            return;
+        }
+        // Time on a copy of the state, then restore it.
+        const size_t values = ctx->q.count;
+        DeviceBuffer<double> q0, k0;
+        q0.allocate(values);
+        k0.allocate(values);
+        check_cuda(cudaMemcpyAsync(q0.ptr, ctx->q.ptr, values * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream), "state copy");
+        check_cuda(cudaMemcpyAsync(k0.ptr, ctx->k.ptr, values * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream), "state copy");
+        std::vector<int> cand = tile_candidates(ctx);
+        cand.insert(cand.begin(), 0);  // the default tile
+        cudaEvent_t e0, e1;
+        check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+        check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+        int best = 0;
+        double best_t = INFINITY;
+        for (int epb : cand) {
+            set_tile(ctx, epb);
+            ensure_traces(ctx);
+            launch_stage(ctx, 1);  // warm-up
+            check_cuda(cudaEventRecord(e0, ctx->stream), "cudaEventRecord");
+            for (int i = 0; i < n_launches; ++i) launch_stage(ctx, 1);
+            check_cuda(cudaEventRecord(e1, ctx->stream), "cudaEventRecord");
+            check_cuda(cudaStreamSynchronize(ctx->stream), "autotune");
+            float ms = 0.0f;
+            check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            const double t = ms / n_launches;
+            if (t < best_t) {
+                best_t = t;
+                best = epb;
+            }
+            // restart every candidate from the same state
+            check_cuda(cudaMemcpyAsync(ctx->q.ptr, q0.ptr, values * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream), "state restore");
+            check_cuda(cudaMemcpyAsync(ctx->k.ptr, k0.ptr, values * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream), "state restore");
+            ctx->traces_valid = false;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        check_device_error(ctx);
+        set_tile(ctx, best);
+        ctx->tile[form] = best;
+        check_cuda(cudaStreamSynchronize(ctx->stream), "autotune");
+        if (elements_per_block) *elements_per_block = best;
+        if (best_ms) *best_ms = best_t;
     });
 }
 

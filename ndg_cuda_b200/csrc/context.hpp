@@ -105,6 +105,9 @@ struct ndg_ctx {
     // Incremented whenever the topology or its device plan changes (load,
     // adaptation): objects built on the mesh (adjoint problems) check it.
     int64_t mesh_version = 0;
+    // Elements per CTA of the uniform stage kernel chosen by the autotuner
+    // (or by hand) for the FP64 and FP32 forms; 0 = the default tile.
+    int tile[2] = {0, 0};
 
     ~ndg_ctx() {
         for (auto& g : graph)

@@ -91,17 +91,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned* error, uint64
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 
 // ---------------------------------------------------------------------------
-template <int N>
+// Tile of the fused stage: E elements per CTA (E even), or for E = 0 the
+// default: as many as fit ~60 KB of shared memory (several CTAs per SM) and
+// 256 threads.
+template <int N, int E = 0>
 struct Tile {
     static constexpr int n = N + 1;
     static constexpr int NN = n * n;
-    // Elements per CTA: even (aligned tile copies), at most ~60 KB of shared
-    // memory so that several CTAs share an SM, at most 256 threads.
     static constexpr int per_element_doubles = 2 * 3 * NN + 2 * 3 * 4 * n + NN + 4;
     static constexpr int by_smem = (60 * 1024 / 8) / per_element_doubles;
     static constexpr int by_threads = 256 / (3 * n);
     static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
-    static constexpr int EPB = raw >= 2 ? (raw & ~1) : 2;
+    static constexpr int EPB = E > 0 ? E : (raw >= 2 ? (raw & ~1) : 2);
+    static_assert(EPB % 2 == 0, "tiles hold an even number of elements (aligned bulk copies)");
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
     // Node-wise work per thread in the RK phase: ceil(3 EPB NN / threads).
     static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;

@@ -60,6 +60,15 @@ cudaError_t upload_tables(const Tables& t);
 // ((N+1)^2), nodes, Lagrange values at -1 and +1, weights, 1/weights.
 void host_coefficients(int N, double* dhat, double* xn, double* lm, double* lp, double* w, double* iw);
 int elements_per_block(int N);
+// Candidate tiles of the autotuner (stage_variants_fp64.cu, _fp32.cu): the
+// feasible elements-per-CTA values of order N, and the stage kernel with
+// one of them (FP64 default rounding, or the FP32 form).
+int tile_candidates_fp64(int N, int* out, int max);
+int tile_candidates_fp32(int N, int* out, int max);
+cudaError_t prepare_stage_variant_fp64(int N, int epb);
+cudaError_t prepare_stage_variant_fp32(int N, int epb);
+cudaError_t launch_stage_variant_fp64(int N, int epb, const StageArgs& a, cudaStream_t stream);
+cudaError_t launch_stage_variant_fp32(int N, int epb, const StageArgs& a, cudaStream_t stream);
 
 }  // namespace dev
 }  // namespace ndg

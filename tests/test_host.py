@@ -139,3 +139,15 @@ def test_element_state_bitwise_vs_reference(res, kw, ref_available):
     for k in ("split_level", "status", "rotation", "n_faces_side"):
         assert np.array_equal(sm[k], er[k]), k
     assert np.array_equal(sm["faces"], r.element_faces())
+
+
+def test_tile_candidates_on_a_host_context():
+    """The autotuner's candidate tiles need no GPU to list: even sizes that
+    fit 512 threads and 113 KB of shared memory."""
+    zone = meshgen.uniform_zone(4, boundary=meshgen.WALL)
+    m = ndg.Mesh2D_t(zone, 8, device=-1)
+    cand, default = m.tile_candidates()
+    assert cand == [2, 4, 6, 8, 12, 16] and default == 8
+    m16 = ndg.Mesh2D_t(zone, 16, device=-1)
+    cand16, _ = m16.tile_candidates()
+    assert cand16 and max(cand16) * 3 * 17 <= 512 and all(c % 2 == 0 for c in cand16)
