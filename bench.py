@@ -314,6 +314,24 @@ def adjoint_leg(local: int, stream, peak: float, cpu_sample: bool) -> dict:
            "e2e_note": "host buffers: p0 and targets uploaded, samples and the four gradients downloaded inside the timed calls",
            "kernel_ms": kernel, "roofline": roof, "launches": {"forward": tm["forward_launches"], "backward": tm["backward_launches"]},
            "misfit": J, "grad_norm": {"p0": float(np.linalg.norm(g["p0"])), "c": float(np.linalg.norm(g["c"]))}}
+    # FP32 form of the same gradient (operator arithmetic in FP32)
+    a32 = ndg.Adjoint2D_t(mesh, A.circle_receivers(ADJ_RECEIVERS, 0.7), speed=c, precision=ndg.FP32)
+    a32.forward(p0, dt, ADJ_STEPS, targets=target, checkpoint_interval=ADJ_INTERVAL)
+    a32.backward()  # warm-up
+    f32, b32 = [], []
+    for _ in range(reps):
+        J32, _ = a32.forward(p0, dt, ADJ_STEPS, targets=target, checkpoint_interval=ADJ_INTERVAL)
+        g32 = a32.backward()
+        t32 = a32.timings()
+        f32.append(t32["forward_ms"])
+        b32.append(t32["backward_ms"])
+    k32 = {"speed_stage": a32.time_stage(0, 30), "adjoint_stage": a32.time_stage(2, 30)}
+    rel = {k: float(np.linalg.norm(g32[k] - g[k]) / max(np.linalg.norm(g[k]), 1e-300)) for k in ("p0", "c")}
+    out["fp32"] = {"forward_ms": statistics.median(f32), "backward_ms": statistics.median(b32),
+                   "adjoint_over_forward": statistics.median(b32) / statistics.median(f32), "kernel_ms": k32,
+                   "misfit_rel_diff_vs_fp64": abs(J32 - J) / max(abs(J), 1e-300), "gradient_rel_l2_vs_fp64": rel,
+                   "arithmetic": "traces, fluxes, metrics, volume term and their transposes in FP32; states, RK updates, misfit and gradient accumulation in FP64"}
+    a32.close()
     if cpu_sample:
         # the oracle's CPU FP64 adjoint on a bounded sample of the same problem
         o, el, w = A.oracle_problem(zone, ADJ_N, c, A.circle_receivers(ADJ_RECEIVERS, 0.7))

@@ -301,6 +301,10 @@ typedef struct ndg_adjoint ndg_adjoint;
  * receivers at receiver_xy[2 r], [2 r + 1]; the wave speed starts at 1. */
 ndg_status ndg_adjoint_create(ndg_ctx* ctx, int32_t n_receivers, const double* receiver_xy, ndg_adjoint** out);
 ndg_status ndg_adjoint_destroy(ndg_adjoint* adj);
+/* Arithmetic of the adjoint problem's kernels: NDG_FP64 (default) or
+ * NDG_FP32 (traces, fluxes, metrics, the volume term and their transposes
+ * in FP32; states, RK updates, misfit and gradient accumulation in FP64). */
+ndg_status ndg_adjoint_set_precision(ndg_adjoint* adj, int32_t precision);
 /* Wave speed per domain element (n_elements values, all > 0). */
 ndg_status ndg_adjoint_set_speed(ndg_adjoint* adj, const double* c);
 /* The CFL step of the variable-speed operator: min over elements of

@@ -100,6 +100,7 @@ def lib() -> C.CDLL:
         "ndg_adjoint_create": ([vp, i32, vp, C.POINTER(vp)], C.c_int),
         "ndg_adjoint_destroy": ([vp], C.c_int),
         "ndg_adjoint_set_speed": ([vp, vp], C.c_int),
+        "ndg_adjoint_set_precision": ([vp, i32], C.c_int),
         "ndg_adjoint_delta_t": ([vp, dbl, C.POINTER(dbl)], C.c_int),
         "ndg_adjoint_receivers": ([vp, vp, vp], C.c_int),
         "ndg_adjoint_forward": ([vp, vp, vp, vp, vp, dbl, i64, i64, vp, C.POINTER(dbl)], C.c_int),
@@ -435,7 +436,7 @@ class Adjoint2D_t:
 
     The mesh must not be adapted while the adjoint exists."""
 
-    def __init__(self, mesh: Mesh2D_t, receivers_xy=None, speed=None):
+    def __init__(self, mesh: Mesh2D_t, receivers_xy=None, speed=None, precision: int = FP64):
         xy = np.ascontiguousarray(np.zeros((0, 2)) if receivers_xy is None else receivers_xy, dtype=np.float64).reshape(-1, 2)
         self.mesh = mesh
         self.n_receivers = xy.shape[0]
@@ -445,6 +446,8 @@ class Adjoint2D_t:
         _check(lib().ndg_adjoint_create(mesh.handle, self.n_receivers, _ptr(xy) if xy.size else None, C.byref(h)))
         self.h = h
         self.serial = 0  # changes with every forward solve and speed update
+        if precision != FP64:
+            _check(lib().ndg_adjoint_set_precision(h, precision))
         if speed is not None:
             self.set_speed(speed)
 

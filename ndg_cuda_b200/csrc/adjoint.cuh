@@ -12,6 +12,11 @@
 // Layouts as the stage kernels: fields [field p,u,v][Kp][(N+1)^2], traces
 // and adjoint traces [field][Kp][side][N+1]; per element side link, normal
 // and gscale of the side plan; speeds [Kp] (the pad element's speed is 1).
+//
+// Two arithmetic forms. FP64: everything in FP64. FP32: traces, fluxes,
+// metrics, the volume term and their transposes in FP32 (traces and adjoint
+// traces stored in FP32); the states q, k, lq, lk, the RK updates, the
+// misfit and the gradient accumulators stay FP64.
 #pragma once
 
 #include "ndg_internal.hpp"
@@ -40,6 +45,8 @@ struct SpeedStageArgs {
     double* k;
     const double* trace_in;  // side traces of q (the previous stage's output)
     double* trace_out;       // side traces of the new q
+    const float* trace_in_f;  // the same in the FP32 form
+    float* trace_out_f;
     double* q_save;          // optional: copy of the stage input q
     double* G_out;           // optional: copy of G
     double* samples;         // optional: receivers' pressure of the new q
@@ -68,6 +75,8 @@ struct AdjointStageArgs {
     const double* qs;      // the forward stage's input
     const double* atr_in;  // neighbours' adjoint far traces of mu
     double* atr_out;       // this element's adjoint far traces of mu'
+    const float* atr_in_f;  // the same in the FP32 form
+    float* atr_out_f;
     double* acc;           // [Kp][5]
     const double* corners;
     const int2* link;
@@ -82,13 +91,13 @@ struct AdjointStageArgs {
     Receivers rec;
 };
 
-cudaError_t prepare_speed_kernels(int N);
-cudaError_t launch_speed_stage(int N, const SpeedStageArgs& a, cudaStream_t stream);
-cudaError_t launch_adjoint_stage(int N, const AdjointStageArgs& a, cudaStream_t stream);
+cudaError_t prepare_speed_kernels(int N, bool fp32);
+cudaError_t launch_speed_stage(int N, bool fp32, const SpeedStageArgs& a, cudaStream_t stream);
+cudaError_t launch_adjoint_stage(int N, bool fp32, const AdjointStageArgs& a, cudaStream_t stream);
 // grad_c[e] = acc[e][0] + sum over sides of acc[e][1+s] (boundary sides) or
 // (acc[e][1+s] + acc[nb][1+s']) / 2 (sides shared with element nb, side s').
 cudaError_t launch_speed_gradient(const double* acc, const int2* link, int64_t K, double* grad_c, cudaStream_t stream);
-int adjoint_elements_per_block(int N);
+int adjoint_elements_per_block(int N, bool fp32);
 
 }  // namespace dev
 }  // namespace ndg

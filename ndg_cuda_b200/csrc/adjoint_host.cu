@@ -23,6 +23,8 @@ struct ndg_adjoint {
     std::vector<int64_t> rec_elem;
     std::vector<double> rec_xi, rec_w;
     ndg::DeviceBuffer<double> c, q, k, G, tr[2], atr[2], lq, lk, acc, ckpt, seg, d_rec_w, targets, samples, grad;
+    ndg::DeviceBuffer<float> tr_f[2], atr_f[2];  // traces of the FP32 form
+    bool fp32 = false;
     ndg::DeviceBuffer<unsigned> error;
     ndg::dev::Receivers rec{};
     // the last forward
@@ -92,6 +94,12 @@ bool locate(const double* cr, double x, double y, double& xi, double& eta) {
     return std::fabs(xi) <= 1.0 + 1e-12 && std::fabs(eta) <= 1.0 + 1e-12;
 }
 
+// Zeroes the adjoint far traces of buffer i (both forms).
+void zero_adjoint_traces(ndg_adjoint* a, int i) {
+    check_cuda(cudaMemsetAsync(a->atr[i].ptr, 0, a->atr[i].count * sizeof(double), a->ctx->stream), "memset");
+    check_cuda(cudaMemsetAsync(a->atr_f[i].ptr, 0, a->atr_f[i].count * sizeof(float), a->ctx->stream), "memset");
+}
+
 dev::SpeedStageArgs speed_args(ndg_adjoint* a, int m, int in, double dt) {
     ndg_ctx* c = a->ctx;
     dev::SpeedStageArgs s{};
@@ -99,6 +107,8 @@ dev::SpeedStageArgs speed_args(ndg_adjoint* a, int m, int in, double dt) {
     s.k = a->k.ptr;
     s.trace_in = a->tr[in].ptr;
     s.trace_out = a->tr[1 - in].ptr;
+    s.trace_in_f = a->tr_f[in].ptr;
+    s.trace_out_f = a->tr_f[1 - in].ptr;
     s.corners = c->corners.ptr;
     s.link = reinterpret_cast<const int2*>(c->link.ptr);
     s.normal = reinterpret_cast<const double2*>(c->normal.ptr);
@@ -121,6 +131,8 @@ dev::AdjointStageArgs adjoint_args(ndg_adjoint* a, int in) {
     s.lk = a->lk.ptr;
     s.atr_in = a->atr[in].ptr;
     s.atr_out = a->atr[1 - in].ptr;
+    s.atr_in_f = a->atr_f[in].ptr;
+    s.atr_out_f = a->atr_f[1 - in].ptr;
     s.acc = a->acc.ptr;
     s.corners = c->corners.ptr;
     s.link = reinterpret_cast<const int2*>(c->link.ptr);
@@ -138,10 +150,14 @@ void launch_traces_of_q(ndg_adjoint* a, int out) {
     dev::TraceArgs t{};
     t.q = a->q.ptr;
     t.trace_out = a->tr[out].ptr;
+    t.trace_out_f = a->tr_f[out].ptr;
     t.n_elements = a->K;
     t.field_stride = a->Kp;
     t.n_instances = 1;
-    check_cuda(dev::launch_traces(a->N, false, t, a->ctx->stream), "trace kernel launch");
+    if (a->fp32)
+        check_cuda(dev::launch_traces_f32(a->N, t, a->ctx->stream), "trace kernel launch");
+    else
+        check_cuda(dev::launch_traces(a->N, false, t, a->ctx->stream), "trace kernel launch");
 }
 
 void check_kernel_error(ndg_adjoint* a) {
@@ -181,7 +197,7 @@ int run_forward(ndg_adjoint* a, int in, int64_t first, int64_t last, double* q_s
             if (q_save) s.q_save = q_save + (static_cast<size_t>(step - first) * 3 + static_cast<size_t>(m)) * state;
             if (save_every > 0 && m == 0 && (step - 1) % save_every == 0) s.q_save = a->ckpt.ptr + static_cast<size_t>((step - 1) / save_every) * state;
             if (sample && m == 2 && a->rec.n > 0) s.samples = a->samples.ptr + step * a->rec.n;
-            check_cuda(dev::launch_speed_stage(a->N, s, a->ctx->stream), "speed stage launch");
+            check_cuda(dev::launch_speed_stage(a->N, a->fp32, s, a->ctx->stream), "speed stage launch");
             ++launches;
             in = 1 - in;
         }
@@ -262,13 +278,18 @@ ndg_status ndg_adjoint_create(ndg_ctx* ctx, int32_t n_receivers, const double* r
         for (int i = 0; i < 2; ++i) {
             a->tr[i].allocate(traces);
             a->atr[i].allocate(traces);
+            a->tr_f[i].allocate(traces);
+            a->atr_f[i].allocate(traces);
             check_cuda(cudaMemsetAsync(a->tr[i].ptr, 0, traces * sizeof(double), s), "memset");
+            check_cuda(cudaMemsetAsync(a->tr_f[i].ptr, 0, traces * sizeof(float), s), "memset");
         }
         a->acc.allocate(5 * static_cast<size_t>(a->Kp));
         a->grad.allocate(static_cast<size_t>(a->Kp));
         a->error.allocate(1);
         check_cuda(cudaMemsetAsync(a->error.ptr, 0, sizeof(unsigned), s), "memset");
-        check_cuda(dev::prepare_speed_kernels(a->N), "kernel attributes");
+        check_cuda(dev::prepare_speed_kernels(a->N, false), "kernel attributes");
+        check_cuda(dev::prepare_speed_kernels(a->N, true), "kernel attributes");
+        check_cuda(dev::prepare_kernels_f32(a->N), "kernel attributes");
         check_cuda(cudaEventCreate(&a->ev[0]), "event");
         check_cuda(cudaEventCreate(&a->ev[1]), "event");
         check_cuda(cudaStreamSynchronize(s), "adjoint setup");
@@ -295,6 +316,15 @@ ndg_status ndg_adjoint_set_speed(ndg_adjoint* adj, const double* c) {
         cp.resize(static_cast<size_t>(adj->Kp), 1.0);
         check_cuda(cudaMemcpyAsync(adj->c.ptr, cp.data(), cp.size() * sizeof(double), cudaMemcpyHostToDevice, adj->ctx->stream), "speed upload");
         check_cuda(cudaStreamSynchronize(adj->ctx->stream), "speed upload");
+        adj->has_forward = false;
+    });
+}
+
+ndg_status ndg_adjoint_set_precision(ndg_adjoint* adj, int32_t precision) {
+    return guarded([&] {
+        require_valid(adj);
+        if (precision != NDG_FP64 && precision != NDG_FP32) fail(NDG_ERR_UNSUPPORTED, "the adjoint runs in NDG_FP64 or NDG_FP32");
+        adj->fp32 = precision == NDG_FP32;
         adj->has_forward = false;
     });
 }
@@ -397,11 +427,10 @@ ndg_status ndg_adjoint_backward(ndg_adjoint* adj, double* grad_p0, double* grad_
         const int64_t I = adj->interval, n = adj->n_steps, n_ckpt = (n + I - 1) / I;
         const int R = adj->rec.n;
         if (adj->seg.count != 3 * static_cast<size_t>(I) * state) adj->seg.allocate(3 * static_cast<size_t>(I) * state);
-        const size_t traces = adj->atr[0].count;
         check_cuda(cudaMemsetAsync(adj->lq.ptr, 0, state * sizeof(double), s), "memset");
         check_cuda(cudaMemsetAsync(adj->lk.ptr, 0, state * sizeof(double), s), "memset");
         check_cuda(cudaMemsetAsync(adj->acc.ptr, 0, adj->acc.count * sizeof(double), s), "memset");
-        check_cuda(cudaMemsetAsync(adj->atr[0].ptr, 0, traces * sizeof(double), s), "memset");
+        zero_adjoint_traces(adj, 0);
         int64_t launches = 0;
         int ain = 0;
         check_cuda(cudaEventRecord(adj->ev[0], s), "event");
@@ -425,7 +454,7 @@ ndg_status ndg_adjoint_backward(ndg_adjoint* adj, double* grad_p0, double* grad_
                 a.inject = R > 0;
                 a.target = adj->targets.ptr + n * R;
                 a.wdt = adj->dt;
-                check_cuda(dev::launch_adjoint_stage(adj->N, a, s), "adjoint stage launch");
+                check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, s), "adjoint stage launch");
                 ++launches;
                 ain = 1 - ain;
             }
@@ -439,7 +468,7 @@ ndg_status ndg_adjoint_backward(ndg_adjoint* adj, double* grad_p0, double* grad_
                     a.inject = (m == 0 && step - 1 >= 1 && R > 0) ? 1 : 0;
                     a.target = adj->targets.ptr + (step - 1) * R;
                     a.wdt = adj->dt;
-                    check_cuda(dev::launch_adjoint_stage(adj->N, a, s), "adjoint stage launch");
+                    check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, s), "adjoint stage launch");
                     ++launches;
                     ain = 1 - ain;
                 }
@@ -481,24 +510,23 @@ ndg_status ndg_adjoint_operator(ndg_adjoint* adj, const double* x, const double*
         dev::SpeedStageArgs f = speed_args(adj, 0, 0, 0.0);
         f.gdt = 0.0;
         f.G_out = adj->G.ptr;
-        check_cuda(dev::launch_speed_stage(adj->N, f, s), "speed stage launch");
+        check_cuda(dev::launch_speed_stage(adj->N, adj->fp32, f, s), "speed stage launch");
         // L^T y: publish the adjoint far traces of y (mu = 0, mu' = lq = y),
         // then one adjoint stage with mu = lk = y, lq = 0 and qs = x.
-        const size_t traces = adj->atr[0].count;
-        check_cuda(cudaMemsetAsync(adj->atr[0].ptr, 0, traces * sizeof(double), s), "memset");
+        zero_adjoint_traces(adj, 0);
         check_cuda(cudaMemsetAsync(adj->acc.ptr, 0, adj->acc.count * sizeof(double), s), "memset");
         upload_state(adj, adj->lq.ptr, yf);
         upload_state(adj, adj->lk.ptr, none);
         dev::AdjointStageArgs a = adjoint_args(adj, 0);
         a.qs = adj->q.ptr;
         a.gdt_next = 1.0;
-        check_cuda(dev::launch_adjoint_stage(adj->N, a, s), "adjoint stage launch");
+        check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, s), "adjoint stage launch");
         check_cuda(cudaMemsetAsync(adj->acc.ptr, 0, adj->acc.count * sizeof(double), s), "memset");
         upload_state(adj, adj->lq.ptr, none);
         upload_state(adj, adj->lk.ptr, yf);
         a = adjoint_args(adj, 1);
         a.qs = adj->q.ptr;
-        check_cuda(dev::launch_adjoint_stage(adj->N, a, s), "adjoint stage launch");
+        check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, s), "adjoint stage launch");
         check_cuda(dev::launch_speed_gradient(adj->acc.ptr, reinterpret_cast<const int2*>(c->link.ptr), adj->K, adj->grad.ptr, s), "gradient kernel");
         check_kernel_error(adj);
         for (int ff = 0; ff < 3; ++ff) {
@@ -537,14 +565,14 @@ ndg_status ndg_adjoint_time_stage(ndg_adjoint* adj, int32_t which, int32_t n_lau
             if (which < 2) {
                 dev::SpeedStageArgs a = speed_args(adj, 1, in, adj->dt);
                 if (which == 1) a.q_save = adj->seg.ptr;
-                check_cuda(dev::launch_speed_stage(adj->N, a, s), "speed stage launch");
+                check_cuda(dev::launch_speed_stage(adj->N, adj->fp32, a, s), "speed stage launch");
             } else {
                 dev::AdjointStageArgs a = adjoint_args(adj, in);
                 a.qs = adj->seg.ptr;
                 a.rk_a = kRkA[1];
                 a.gdt = kRkG[1] * adj->dt;
                 a.gdt_next = kRkG[0] * adj->dt;
-                check_cuda(dev::launch_adjoint_stage(adj->N, a, s), "adjoint stage launch");
+                check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, s), "adjoint stage launch");
             }
             check_cuda(cudaEventRecord(ev[static_cast<size_t>(2 * i + 1)], s), "cudaEventRecord");
             in = 1 - in;

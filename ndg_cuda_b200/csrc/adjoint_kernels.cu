@@ -26,7 +26,11 @@
 // (both sides' flux transposes meet in it), so the gradient gathers
 // (U_s + U_nb,s') / 2 from both elements (launch_speed_gradient).
 //
-// FP64 with FMA contraction; the RK register and the solution stay FP64.
+// Both kernels are templates over R, the type of the operator's arithmetic:
+// double (the FP64 form, FMA contraction) or float (the FP32 form: traces,
+// fluxes, metrics, contractions and their transposes in FP32, traces stored
+// in FP32). The bulk-copied states, the RK updates, the misfit and the
+// gradient accumulators are FP64 in both.
 #include "adjoint.cuh"
 #include "stage_common.cuh"
 #include "stage_kernels.cuh"
@@ -35,41 +39,100 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 namespace ndg {
 namespace dev {
 
-// Coefficients of the adjoint: Dhat, nodes, Lagrange end values and the
-// lift weights l(-1)/w, l(+1)/w.
-template <int N>
-struct AdjCoeffs {
-    double dhat[(N + 1) * (N + 1)];
-    double xn[N + 1], lm[N + 1], lp[N + 1], iw[N + 1], lmw[N + 1], lpw[N + 1];
+template <typename R>
+__device__ __forceinline__ R rcp(R x) {
+    if constexpr (std::is_same_v<R, double>)
+        return __drcp_rn(x);
+    else
+        return __frcp_rn(x);
+}
+
+// ((1 - t) d0 + (1 + t) d1) / 4 of quad_metrics as fma(t, (d1 - d0)/4, (d0 + d1)/4).
+template <typename R>
+struct LineR {
+    R d0, d1, a, b;
+    __device__ __forceinline__ LineR(R d0_, R d1_) : d0(d0_), d1(d1_), a(R(0.25) * (d0_ + d1_)), b(R(0.25) * (d1_ - d0_)) {}
+    __device__ __forceinline__ R operator()(R t) const { return fma(t, b, a); }
 };
 
-template <int N>
-static AdjCoeffs<N> make_adj_coeffs() {
+// The edge metric term of a side at t = +-1, in the reference's expression.
+template <typename R>
+__device__ __forceinline__ R edge_term(R t, R d0, R d1) {
+    return ((R(1) - t) * d0 + (R(1) + t) * d1) * R(0.25);
+}
+
+// The form's trace buffer.
+template <typename R>
+__device__ __forceinline__ const R* pick(const double* d, const float* f) {
+    if constexpr (std::is_same_v<R, double>)
+        return d;
+    else
+        return f;
+}
+template <typename R>
+__device__ __forceinline__ R* pick(double* d, float* f) {
+    if constexpr (std::is_same_v<R, double>)
+        return d;
+    else
+        return f;
+}
+
+template <int N, typename R>
+struct SpeedCoeffs {
+    R dhat[(N + 1) * (N + 1)];
+    R xn[N + 1], lm[N + 1], lp[N + 1], iw[N + 1];
+};
+
+// Coefficients of the adjoint: Dhat, nodes, Lagrange end values, 1/w and
+// the lift weights l(-1)/w, l(+1)/w.
+template <int N, typename R>
+struct AdjCoeffs {
+    R dhat[(N + 1) * (N + 1)];
+    R xn[N + 1], lm[N + 1], lp[N + 1], iw[N + 1], lmw[N + 1], lpw[N + 1];
+};
+
+template <int N, typename R>
+static SpeedCoeffs<N, R> make_speed_coeffs() {
     constexpr int n = N + 1;
-    double w[n];
-    AdjCoeffs<N> c;
-    host_coefficients(N, c.dhat, c.xn, c.lm, c.lp, w, c.iw);
+    double dh[n * n], xn[n], lm[n], lp[n], w[n], iw[n];
+    host_coefficients(N, dh, xn, lm, lp, w, iw);
+    SpeedCoeffs<N, R> c;
+    for (int i = 0; i < n * n; ++i) c.dhat[i] = static_cast<R>(dh[i]);
     for (int i = 0; i < n; ++i) {
-        c.lmw[i] = c.lm[i] * c.iw[i];
-        c.lpw[i] = c.lp[i] * c.iw[i];
+        c.xn[i] = static_cast<R>(xn[i]);
+        c.lm[i] = static_cast<R>(lm[i]);
+        c.lp[i] = static_cast<R>(lp[i]);
+        c.iw[i] = static_cast<R>(iw[i]);
     }
     return c;
 }
 
-template <int N>
-static Coeffs<N> make_speed_coeffs() {
-    Coeffs<N> c;
-    host_coefficients(N, c.dhat, c.xn, c.lm, c.lp, c.w, c.iw);
+template <int N, typename R>
+static AdjCoeffs<N, R> make_adj_coeffs() {
+    constexpr int n = N + 1;
+    double dh[n * n], xn[n], lm[n], lp[n], w[n], iw[n];
+    host_coefficients(N, dh, xn, lm, lp, w, iw);
+    AdjCoeffs<N, R> c;
+    for (int i = 0; i < n * n; ++i) c.dhat[i] = static_cast<R>(dh[i]);
+    for (int i = 0; i < n; ++i) {
+        c.xn[i] = static_cast<R>(xn[i]);
+        c.lm[i] = static_cast<R>(lm[i]);
+        c.lp[i] = static_cast<R>(lp[i]);
+        c.iw[i] = static_cast<R>(iw[i]);
+        c.lmw[i] = static_cast<R>(lm[i] * iw[i]);
+        c.lpw[i] = static_cast<R>(lp[i] * iw[i]);
+    }
     return c;
 }
 
 // Pressure at the receivers of a tile, one warp: sum of w_r . p over the
 // element's nodes, lanes striding the nodes, then a shuffle reduction in a
-// fixed order (the same result wherever it is evaluated).
+// fixed order (the same result wherever it is evaluated). FP64 in both forms.
 template <int NN>
 __device__ __forceinline__ double receiver_value(const double* __restrict__ w, const double* p, int lane) {
     double s = 0.0;
@@ -80,21 +143,37 @@ __device__ __forceinline__ double receiver_value(const double* __restrict__ w, c
 }
 
 // ---------------------------------------------------------------------------
-// Forward stage with a wave speed per element. Same tile, thread layout and
-// passes as stage_kernel<N, false> (stage_kernels.cu).
-template <int N>
-__global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedStageArgs a, const __grid_constant__ Coeffs<N> cf) {
-    using T = Tile<N>;
+// Forward stage with a wave speed per element. Same tile and thread layout
+// as stage_kernel<N, false> (stage_kernels.cu): the bulk-copied q tile in
+// FP64, then R arrays (offsets in R values past it), then the mbarrier.
+template <int N, typename R>
+struct SpeedTile {
+    using D = Tile<N>;
+    static constexpr int n = N + 1, NN = n * n, EPB = D::EPB, kThreads = D::kThreads, kNodeIters = D::kNodeIters;
+    static constexpr int kQd = 3 * EPB * NN;             // doubles: the q tile
+    static constexpr int kG = 0;                         // [3][EPB][NN] time derivative G
+    static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n] own side traces
+    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far traces, then element side fluxes
+    static constexpr int kJ = kFar + 3 * EPB * 4 * n;    // [EPB][NN] 1/J
+    static constexpr int kS = kJ + EPB * NN;             // [EPB][4] edge metric per side
+    static constexpr int kRs = kS + EPB * 4;
+    static constexpr size_t kBarOff = (sizeof(double) * kQd + sizeof(R) * kRs + 15) / 16 * 16;
+    static constexpr size_t kBytes = kBarOff + 16;
+};
+
+template <int N, typename R>
+__global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(SpeedStageArgs a, const __grid_constant__ SpeedCoeffs<N, R> cf) {
+    using T = SpeedTile<N, R>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     extern __shared__ __align__(128) double smem[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T::kBar);
-    double* qs = smem + T::kQ;
-    double* gs = smem + T::kG;
-    double* own_s = smem + T::kOwn;
-    double* far_s = smem + T::kFar;
-    double* js = smem + T::kJ;
-    double* ss = smem + T::kS;
-    double* zs = smem + T::kZ;
+    double* qs = smem;
+    R* rs = reinterpret_cast<R*>(smem + T::kQd);
+    R* gs = rs + T::kG;
+    R* own_s = rs + T::kOwn;
+    R* far_s = rs + T::kFar;
+    R* js = rs + T::kJ;
+    R* ss = rs + T::kS;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + T::kBarOff);
     constexpr int FS = EPB * 4 * n;
 
     const int tid = threadIdx.x;
@@ -105,9 +184,11 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
     const int ne_copy = (ne + 1) & ~1;
     double* q = a.q;
     double* k = a.k;
-    const double* xn = cf.xn;
-    const double* lm = cf.lm;
-    const double* lp = cf.lp;
+    const R* tr_in = pick<R>(a.trace_in, a.trace_in_f);
+    R* tr_out = pick<R>(a.trace_out, a.trace_out_f);
+    const R* xn = cf.xn;
+    const R* lm = cf.lm;
+    const R* lp = cf.lp;
 
     const int f = tid / (EPB * n);
     const int rr = tid - f * (EPB * n);
@@ -123,55 +204,57 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
         mbar_expect_tx(bar, 3 * bytes);
         for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
     }
-    for (int i = tid; i < NN; i += T::kThreads) zs[i] = 0.0;
-    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0, ce = 1.0;
+    R x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0, ce = 1;
     if (active) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const int2 lk = a.link[4 * ge + s];
-            const double v = (((lk.y >> 2) & 7) == kInterior) ? a.trace_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0;
+            const R v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : R(0);
             far_s[f * FS + (e * 4 + s) * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
-        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
-        ce = a.c[ge];
+        x0 = R(c[0]); y0 = R(c[1]); x1 = R(c[2]); y1 = R(c[3]); x2 = R(c[4]); y2 = R(c[5]); x3 = R(c[6]); y3 = R(c[7]);
+        ce = R(a.c[ge]);
     }
-    const MetricLine<false> x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
-    const MetricLine<false> x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
+    const LineR<R> x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
+    const LineR<R> x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
     if (active) {
-        const double tm = xn[m];
+        const R tm = xn[m];
         if (f == 2) {
             for (int sd = m; sd < 4; sd += n) {
-                const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
-                const double dx = (sd == 0 || sd == 2) ? metric<false>(at, x_xi.d0, x_xi.d1) : metric<false>(at, x_eta.d0, x_eta.d1);
-                const double dy = (sd == 0 || sd == 2) ? metric<false>(at, y_xi.d0, y_xi.d1) : metric<false>(at, y_eta.d0, y_eta.d1);
+                const R at = (sd == 0 || sd == 3) ? R(-1) : R(1);
+                const R dx = (sd == 0 || sd == 2) ? edge_term<R>(at, x_xi.d0, x_xi.d1) : edge_term<R>(at, x_eta.d0, x_eta.d1);
+                const R dy = (sd == 0 || sd == 2) ? edge_term<R>(at, y_xi.d0, y_xi.d1) : edge_term<R>(at, y_eta.d0, y_eta.d1);
                 ss[e * 4 + sd] = sqrt(dx * dx + dy * dy);
             }
         }
-        const double xe = x_eta(tm), ye = y_eta(tm);
+        const R xe = x_eta(tm), ye = y_eta(tm);
         for (int j = f; j < n; j += 3) {
-            const double tj = xn[j];
-            js[e * NN + m * n + j] = __drcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
+            const R tj = xn[j];
+            js[e * NN + m * n + j] = rcp<R>(x_xi(tj) * ye - xe * y_xi(tj));
         }
     }
     __syncthreads();
     if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
 
+    // Flux lines (X, Y) = (u, v), (p, 0), (0, p) for the fields p, u, v: the
+    // absent component is scaled by zero.
     const double* Qe = qs + e * NN;
-    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : (f == 1 ? Qe : zs);
-    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : (f == 1 ? zs : Qe);
+    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : Qe;
+    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : Qe;
+    const R sx = f == 2 ? R(0) : R(1), sy = f == 1 ? R(0) : R(1);
     if (active) {
         const double* Qf = Qe + f * EPB * NN;
-        double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
+        R b = 0, t = 0, r = 0, l = 0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            const double qr = Qf[m * n + j], qc = Qf[j * n + m];
+            const R qr = R(Qf[m * n + j]), qc = R(Qf[j * n + m]);
             b = fma(lm[j], qr, b);
             t = fma(lp[j], qr, t);
             r = fma(lp[j], qc, r);
             l = fma(lm[j], qc, l);
         }
-        double* o = own_s + f * FS + e * 4 * n;
+        R* o = own_s + f * FS + e * 4 * n;
         o[0 * n + m] = b;
         o[2 * n + (N - m)] = t;
         o[1 * n + m] = r;
@@ -188,59 +271,60 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
             const int2 lk = a.link[4 * ge + s];
             const int kind = (lk.y >> 2) & 7;
             const int role = (lk.y >> 5) & 1;
-            const double2 nv = a.normal[4 * ge + s];
+            const double2 nd = a.normal[4 * ge + s];
+            const R nx = R(nd.x), ny = R(nd.y);
             const int o = (e * 4 + s) * n + m;
-            const double op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
-            double fp_, fu_, fv_, cface = ce;
+            const R op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
+            R fp_, fu_, fv_, cface = ce;
             if (kind == kInterior) {
                 fp_ = far_s[o];
                 fu_ = far_s[FS + o];
                 fv_ = far_s[2 * FS + o];
-                cface = 0.5 * (ce + a.c[lk.x]);
+                cface = R(0.5) * (ce + R(a.c[lk.x]));
             } else if (kind == kMirror || kind == kCopy) {
-                const double gsc = a.gscale[4 * ge + s];
+                const R gsc = R(a.gscale[4 * ge + s]);
                 fp_ = op * gsc;
-                const double gu = ou * gsc, gv = ov * gsc;
+                const R gu = ou * gsc, gv = ov * gsc;
                 if (kind == kMirror) {
-                    const double tx = -nv.y, ty = nv.x;
-                    const double l0 = -(gu * nv.x + gv * nv.y);
-                    const double l1 = gu * tx + gv * ty;
-                    fu_ = nv.x * l0 + tx * l1;
-                    fv_ = nv.y * l0 + ty * l1;
+                    const R tx = -ny, ty = nx;
+                    const R l0 = -(gu * nx + gv * ny);
+                    const R l1 = gu * tx + gv * ty;
+                    fu_ = nx * l0 + tx * l1;
+                    fv_ = ny * l0 + ty * l1;
                 } else {
                     fu_ = gu;
                     fv_ = gv;
                 }
             } else {
-                fp_ = fu_ = fv_ = 0.0;
+                fp_ = fu_ = fv_ = R(0);
             }
-            const double Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
-            const double Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
-            const double wL = Lp + (Lu * nv.x + Lv * nv.y);
-            const double wR = Rp - (Ru * nv.x + Rv * nv.y);
-            const double sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cface;
-            const double sum = wL + wR;
-            far_s[o] = sc * ((wL - wR) * 0.5);
-            far_s[FS + o] = sc * (nv.x * sum * 0.5);
-            far_s[2 * FS + o] = sc * (nv.y * sum * 0.5);
+            const R Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
+            const R Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
+            const R wL = Lp + (Lu * nx + Lv * ny);
+            const R wR = Rp - (Ru * nx + Rv * ny);
+            const R sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cface;
+            const R sum = wL + wR;
+            far_s[o] = sc * ((wL - wR) * R(0.5));
+            far_s[FS + o] = sc * (nx * sum * R(0.5));
+            far_s[2 * FS + o] = sc * (ny * sum * R(0.5));
         }
     }
     __syncthreads();
 
-    const double* Dh = cf.dhat;
-    const double* iw = cf.iw;
-    const double* F = far_s + f * FS + e * 4 * n;
+    const R* Dh = cf.dhat;
+    const R* iw = cf.iw;
+    const R* F = far_s + f * FS + e * 4 * n;
 
     if (active) {
         const int j = m;
-        double col[n];
+        R col[n];
 #pragma unroll
-        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * Xe[i * n + j] - x_eta(xn[i]) * Ye[i * n + j];
-        const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
-        double* G = gs + (f * EPB + e) * NN + j;
+        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * (sx * R(Xe[i * n + j])) - x_eta(xn[i]) * (sy * R(Ye[i * n + j]));
+        const R fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
+        R* G = gs + (f * EPB + e) * NN + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-            double acc = 0.0;
+            R acc = 0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = fma(Dh[i * n + mm], col[mm], acc);
             G[i * n] = -fma(acc, ce, (fr * lp[i] + fl3 * lm[i]) * iw[i]);
@@ -250,15 +334,15 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
 
     if (active) {
         const int i = m;
-        double line[n];
+        R line[n];
 #pragma unroll
-        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * Xe[i * n + j] + x_xi(xn[j]) * Ye[i * n + j];
-        const double ft = F[2 * n + (N - i)], fb = F[0 * n + i];
-        double* G = gs + (f * EPB + e) * NN + i * n;
-        const double* jrow = js + e * NN + i * n;
+        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * (sx * R(Xe[i * n + j])) + x_xi(xn[j]) * (sy * R(Ye[i * n + j]));
+        const R ft = F[2 * n + (N - i)], fb = F[0 * n + i];
+        R* G = gs + (f * EPB + e) * NN + i * n;
+        const R* jrow = js + e * NN + i * n;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            double acc = 0.0;
+            R acc = 0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = fma(Dh[j * n + mm], line[mm], acc);
             G[j] = (G[j] - fma(acc, ce, (ft * lp[j] + fb * lm[j]) * iw[j])) * jrow[j];
@@ -266,6 +350,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
     }
     __syncthreads();
 
+    // RK update in FP64.
     double kold[T::kNodeIters];
 #pragma unroll
     for (int c = 0; c < T::kNodeIters; ++c) {
@@ -278,7 +363,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
         const int idx = tid + c * T::kThreads;
         const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
         if (ff < 3 && r < ne * NN) {
-            const double G = gs[ff * EPB * NN + r];
+            const double G = static_cast<double>(gs[ff * EPB * NN + r]);
             const double kn = a.first ? G : fma(a.rk_a, kold[c], G);
             const double qo = qs[ff * EPB * NN + r];
             const double qn = fma(a.gdt, kn, qo);
@@ -295,15 +380,16 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
     if (active) {
         const double* row = qs + (f * EPB + e) * NN + m * n;
         const double* cl = qs + (f * EPB + e) * NN + m;
-        double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
+        R b = 0, t = 0, r = 0, l = 0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            b = fma(lm[j], row[j], b);
-            t = fma(lp[j], row[j], t);
-            r = fma(lp[j], cl[j * n], r);
-            l = fma(lm[j], cl[j * n], l);
+            const R qr = R(row[j]), qc = R(cl[j * n]);
+            b = fma(lm[j], qr, b);
+            t = fma(lp[j], qr, t);
+            r = fma(lp[j], qc, r);
+            l = fma(lm[j], qc, l);
         }
-        double* to = a.trace_out + (f * Kp + ge) * 4 * n;
+        R* to = tr_out + (f * Kp + ge) * 4 * n;
         to[0 * n + m] = b;
         to[2 * n + (N - m)] = t;
         to[1 * n + m] = r;
@@ -321,23 +407,29 @@ __global__ void __launch_bounds__(Tile<N>::kThreads) speed_stage_kernel(SpeedSta
 
 // ---------------------------------------------------------------------------
 // Adjoint stage. Tile of EPB elements, one thread per (field, element, line)
-// as the forward. Shared memory (doubles):
-template <int N>
+// as the forward. Shared memory: FP64 arrays first (the two bulk-copied
+// tiles, the receiver residuals and masks), then R arrays, then the mbarrier.
+template <int N, typename R>
 struct AdjTile {
     static constexpr int n = N + 1;
     static constexpr int NN = n * n;
-    static constexpr int per_element_doubles = 11 * NN + 43 * n + 9;
-    static constexpr int fixed_doubles = NN + kMaxReceivers + 2;
-    static constexpr int by_smem = (60 * 1024 / 8 - fixed_doubles) / per_element_doubles;
+    static constexpr int per_element_bytes = 8 * (6 * NN + 1) + static_cast<int>(sizeof(R)) * (5 * NN + 43 * n + 8);
+    static constexpr int fixed_bytes = 8 * kMaxReceivers + 64;
+    static constexpr int by_smem = (60 * 1024 - fixed_bytes) / per_element_bytes;
     static constexpr int by_threads = 256 / (3 * n);
     static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
     static constexpr int EPB = raw >= 2 ? (raw & ~1) : 2;
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
     static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;
     static constexpr int FS = EPB * 4 * n;
+    // doubles
     static constexpr int kL = 0;                   // [3][EPB][NN] lq (bulk copy), then lq + volume transpose
     static constexpr int kQ = kL + 3 * EPB * NN;   // [3][EPB][NN] forward stage input qs (bulk copy)
-    static constexpr int kNu = kQ + 3 * EPB * NN;  // [3][EPB][NN] nu = -mu / J, later nu'
+    static constexpr int kRes = kQ + 3 * EPB * NN; // [kMaxReceivers] weighted misfit residuals
+    static constexpr int kMask = kRes + kMaxReceivers;  // [EPB] receivers of each element (bit mask)
+    static constexpr int kDoubles = kMask + EPB;
+    // R values past the doubles
+    static constexpr int kNu = 0;                  // [3][EPB][NN] nu = -mu / J, later nu'
     static constexpr int kTp = kNu + 3 * EPB * NN; // [EPB][NN] second accumulator of the pressure's transpose
     static constexpr int kJ = kTp + EPB * NN;      // [EPB][NN] 1/J
     static constexpr int kOwn = kJ + EPB * NN;     // [3][EPB][4][n] side traces of qs
@@ -347,36 +439,42 @@ struct AdjTile {
     static constexpr int kVd = kUp + FS;           // [3][EPB][n] volume part of the c-derivative per line
     static constexpr int kS = kVd + 3 * EPB * n;   // [EPB][4] edge metric
     static constexpr int kCf = kS + 4 * EPB;       // [EPB][4] face speed
-    static constexpr int kMask = kCf + 4 * EPB;    // [EPB] receivers of each element (bit mask)
-    static constexpr int kZ = kMask + EPB;         // [NN] zeros
-    static constexpr int kRes = kZ + NN;           // [kMaxReceivers] weighted residuals
-    static constexpr int kBar = kRes + kMaxReceivers;
-    static constexpr int kDoubles = kBar + 2;
-    static constexpr size_t kBytes = sizeof(double) * kDoubles;
-    static_assert(kDoubles <= EPB * per_element_doubles + fixed_doubles, "layout exceeds its budget");
+    static constexpr int kRs = kCf + 4 * EPB;
+    static constexpr size_t kBarOff = (sizeof(double) * kDoubles + sizeof(R) * kRs + 15) / 16 * 16;
+    static constexpr size_t kBytes = kBarOff + 16;
+    static_assert(kBytes <= static_cast<size_t>(EPB * per_element_bytes + fixed_bytes), "layout exceeds its budget");
 };
 
-template <int N>
-__global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(AdjointStageArgs a, const __grid_constant__ AdjCoeffs<N> cf) {
-    using T = AdjTile<N>;
+// t += c v with the form's rounding: one FMA in FP64; in the FP32 form the
+// FP32 product accumulated in the target's type.
+template <typename T, typename R>
+__device__ __forceinline__ void add_scaled(T* t, R c, R v) {
+    *t = fma(static_cast<T>(c), static_cast<T>(v), *t);
+}
+
+template <int N, typename R>
+__global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(AdjointStageArgs a, const __grid_constant__ AdjCoeffs<N, R> cf) {
+    using T = AdjTile<N, R>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB, FS = T::FS;
     extern __shared__ __align__(128) double smem[];
     double* ls = smem + T::kL;
     double* qs = smem + T::kQ;
-    double* nu = smem + T::kNu;
-    double* tp = smem + T::kTp;
-    double* js = smem + T::kJ;
-    double* own_s = smem + T::kOwn;
-    double* ell = smem + T::kEll;
-    double* far_s = smem + T::kFar;
-    double* up = smem + T::kUp;
-    double* vd = smem + T::kVd;
-    double* ss = smem + T::kS;
-    double* cfs = smem + T::kCf;
-    unsigned long long* rmask = reinterpret_cast<unsigned long long*>(smem + T::kMask);
-    double* zs = smem + T::kZ;
     double* res = smem + T::kRes;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T::kBar);
+    unsigned long long* rmask = reinterpret_cast<unsigned long long*>(smem + T::kMask);
+    R* rs = reinterpret_cast<R*>(smem + T::kDoubles);
+    R* nu = rs + T::kNu;
+    R* tp = rs + T::kTp;
+    R* js = rs + T::kJ;
+    R* own_s = rs + T::kOwn;
+    R* ell = rs + T::kEll;
+    R* far_s = rs + T::kFar;
+    R* up = rs + T::kUp;
+    R* vd = rs + T::kVd;
+    R* ss = rs + T::kS;
+    R* cfs = rs + T::kCf;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + T::kBarOff);
+    const R* atr_in = pick<R>(a.atr_in, a.atr_in_f);
+    R* atr_out = pick<R>(a.atr_out, a.atr_out_f);
 
     const int tid = threadIdx.x;
     const int64_t K = a.n_elements;
@@ -384,12 +482,12 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
     const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
     const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
     const int ne_copy = (ne + 1) & ~1;
-    const double* xn = cf.xn;
-    const double* lm = cf.lm;
-    const double* lp = cf.lp;
-    const double* lmw = cf.lmw;
-    const double* lpw = cf.lpw;
-    const double* Dh = cf.dhat;
+    const R* xn = cf.xn;
+    const R* lm = cf.lm;
+    const R* lp = cf.lp;
+    const R* lmw = cf.lmw;
+    const R* lpw = cf.lpw;
+    const R* Dh = cf.dhat;
 
     const int f = tid / (EPB * n);
     const int rr = tid - f * (EPB * n);
@@ -410,39 +508,38 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
             bulk_load(qs + ff * EPB * NN, a.qs + (ff * Kp + e0) * NN, bytes, bar);
         }
     }
-    for (int i = tid; i < NN; i += T::kThreads) zs[i] = 0.0;
-    for (int i = tid; i < EPB * NN; i += T::kThreads) tp[i] = 0.0;
+    for (int i = tid; i < EPB * NN; i += T::kThreads) tp[i] = R(0);
     if (tid < EPB) rmask[tid] = 0ull;
-    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0, ce = 1.0;
+    R x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0, ce = 1;
     if (active) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const int2 lk = a.link[4 * ge + s];
-            const double v = (((lk.y >> 2) & 7) == kInterior) ? a.atr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0;
+            const R v = (((lk.y >> 2) & 7) == kInterior) ? atr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : R(0);
             far_s[f * FS + (e * 4 + s) * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
-        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
-        ce = a.c[ge];
+        x0 = R(c[0]); y0 = R(c[1]); x1 = R(c[2]); y1 = R(c[3]); x2 = R(c[4]); y2 = R(c[5]); x3 = R(c[6]); y3 = R(c[7]);
+        ce = R(a.c[ge]);
     }
-    const MetricLine<false> x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
-    const MetricLine<false> x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
+    const LineR<R> x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
+    const LineR<R> x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
     if (active) {
-        const double tm = xn[m];
+        const R tm = xn[m];
         if (f == 2) {
             for (int sd = m; sd < 4; sd += n) {
-                const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
-                const double dx = (sd == 0 || sd == 2) ? metric<false>(at, x_xi.d0, x_xi.d1) : metric<false>(at, x_eta.d0, x_eta.d1);
-                const double dy = (sd == 0 || sd == 2) ? metric<false>(at, y_xi.d0, y_xi.d1) : metric<false>(at, y_eta.d0, y_eta.d1);
+                const R at = (sd == 0 || sd == 3) ? R(-1) : R(1);
+                const R dx = (sd == 0 || sd == 2) ? edge_term<R>(at, x_xi.d0, x_xi.d1) : edge_term<R>(at, x_eta.d0, x_eta.d1);
+                const R dy = (sd == 0 || sd == 2) ? edge_term<R>(at, y_xi.d0, y_xi.d1) : edge_term<R>(at, y_eta.d0, y_eta.d1);
                 ss[e * 4 + sd] = sqrt(dx * dx + dy * dy);
                 const int2 lk = a.link[4 * ge + sd];
-                cfs[e * 4 + sd] = (((lk.y >> 2) & 7) == kInterior) ? 0.5 * (ce + a.c[lk.x]) : ce;
+                cfs[e * 4 + sd] = (((lk.y >> 2) & 7) == kInterior) ? R(0.5) * (ce + R(a.c[lk.x])) : ce;
             }
         }
-        const double xe = x_eta(tm), ye = y_eta(tm);
+        const R xe = x_eta(tm), ye = y_eta(tm);
         for (int j = f; j < n; j += 3) {
-            const double tj = xn[j];
-            js[e * NN + m * n + j] = __drcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
+            const R tj = xn[j];
+            js[e * NN + m * n + j] = rcp<R>(x_xi(tj) * ye - xe * y_xi(tj));
         }
     }
     __syncthreads();
@@ -462,7 +559,7 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
             const double mu = fma(a.gdt, ls[ff * EPB * NN + r], a.lk[gi]);
             kn[c] = a.rk_a * mu;
             a.lk[gi] = kn[c];
-            nu[ff * EPB * NN + r] = -mu * js[r];
+            nu[ff * EPB * NN + r] = R(-mu) * js[r];
         }
     }
     if (a.inject && tid < 32) {
@@ -484,50 +581,55 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
     //   f = p: A -> lu, B -> lv;  f = u: A -> lp;  f = v: B -> lp (via tp).
     // vdot accumulates X A + Y B (the volume term's derivative in c_e).
     const double* Qe = qs + e * NN;
-    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : (f == 1 ? Qe : zs);
-    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : (f == 1 ? zs : Qe);
-    double* O1 = f == 0 ? ls + (1 * EPB + e) * NN : (f == 1 ? ls + e * NN : tp + e * NN);
-    double* O2 = ls + (2 * EPB + e) * NN;  // f = p only
-    const double* Nf = nu + (f * EPB + e) * NN;
-    double vdot = 0.0;
+    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : Qe;
+    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : Qe;
+    const R sx = f == 2 ? R(0) : R(1), sy = f == 1 ? R(0) : R(1);
+    double* O1 = f == 0 ? ls + (1 * EPB + e) * NN : ls + e * NN;  // f = p, u
+    R* O1v = tp + e * NN;                                          // f = v
+    double* O2 = ls + (2 * EPB + e) * NN;                          // f = p only
+    const R* Nf = nu + (f * EPB + e) * NN;
+    R vdot = 0;
     // xi columns (eta index j = m): alpha = Dhat^T nu(:, j); lift transpose
     // of sides 1 and 3; the side traces of qs.
     if (active) {
         const int j = m;
-        double col[n];
+        R col[n];
 #pragma unroll
         for (int i = 0; i < n; ++i) col[i] = Nf[i * n + j];
-        double l1 = 0.0, l3 = 0.0;
+        R l1 = 0, l3 = 0;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             l1 = fma(col[i], lpw[i], l1);
             l3 = fma(col[i], lmw[i], l3);
         }
-        double* L = ell + f * FS + e * 4 * n;
+        R* L = ell + f * FS + e * 4 * n;
         L[1 * n + j] = l1;
         L[3 * n + (N - j)] = l3;
 #pragma unroll
         for (int mm = 0; mm < n; ++mm) {
-            double al = 0.0;
+            R al = 0;
 #pragma unroll
             for (int i = 0; i < n; ++i) al = fma(Dh[i * n + mm], col[i], al);
-            const double A = y_eta(xn[mm]) * al, B = -x_eta(xn[mm]) * al;
+            const R A = y_eta(xn[mm]) * al, B = -x_eta(xn[mm]) * al;
             const int node = mm * n + j;
-            vdot = fma(Xe[node], A, fma(Ye[node], B, vdot));
-            O1[node] = fma(ce, f == 2 ? B : A, O1[node]);
-            if (f == 0) O2[node] = fma(ce, B, O2[node]);
+            vdot = fma(sx * R(Xe[node]), A, fma(sy * R(Ye[node]), B, vdot));
+            if (f == 2)
+                add_scaled(O1v + node, ce, B);
+            else
+                add_scaled(O1 + node, ce, A);
+            if (f == 0) add_scaled(O2 + node, ce, B);
         }
         const double* Qf = Qe + f * EPB * NN;
-        double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
+        R b = 0, t = 0, r = 0, l = 0;
 #pragma unroll
         for (int jj = 0; jj < n; ++jj) {
-            const double qr = Qf[m * n + jj], qc = Qf[jj * n + m];
+            const R qr = R(Qf[m * n + jj]), qc = R(Qf[jj * n + m]);
             b = fma(lm[jj], qr, b);
             t = fma(lp[jj], qr, t);
             r = fma(lp[jj], qc, r);
             l = fma(lm[jj], qc, l);
         }
-        double* o = own_s + f * FS + e * 4 * n;
+        R* o = own_s + f * FS + e * 4 * n;
         o[0 * n + m] = b;
         o[2 * n + (N - m)] = t;
         o[1 * n + m] = r;
@@ -539,28 +641,31 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
     // sides 2 and 0.
     if (active) {
         const int i = m;
-        double row[n];
+        R row[n];
 #pragma unroll
         for (int j = 0; j < n; ++j) row[j] = Nf[i * n + j];
-        double l2 = 0.0, l0 = 0.0;
+        R l2 = 0, l0 = 0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             l2 = fma(row[j], lpw[j], l2);
             l0 = fma(row[j], lmw[j], l0);
         }
-        double* L = ell + f * FS + e * 4 * n;
+        R* L = ell + f * FS + e * 4 * n;
         L[2 * n + (N - i)] = l2;
         L[0 * n + i] = l0;
 #pragma unroll
         for (int mm = 0; mm < n; ++mm) {
-            double be = 0.0;
+            R be = 0;
 #pragma unroll
             for (int j = 0; j < n; ++j) be = fma(Dh[j * n + mm], row[j], be);
-            const double A = -y_xi(xn[mm]) * be, B = x_xi(xn[mm]) * be;
+            const R A = -y_xi(xn[mm]) * be, B = x_xi(xn[mm]) * be;
             const int node = i * n + mm;
-            vdot = fma(Xe[node], A, fma(Ye[node], B, vdot));
-            O1[node] = fma(ce, f == 2 ? B : A, O1[node]);
-            if (f == 0) O2[node] = fma(ce, B, O2[node]);
+            vdot = fma(sx * R(Xe[node]), A, fma(sy * R(Ye[node]), B, vdot));
+            if (f == 2)
+                add_scaled(O1v + node, ce, B);
+            else
+                add_scaled(O1 + node, ce, A);
+            if (f == 0) add_scaled(O2 + node, ce, B);
         }
         vd[(f * EPB + e) * n + m] = vdot;
     }
@@ -579,31 +684,32 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
             const int2 lk = a.link[4 * ge + s];
             const int kind = (lk.y >> 2) & 7;
             const int role = (lk.y >> 5) & 1;
-            const double2 nv = a.normal[4 * ge + s];
+            const double2 nd = a.normal[4 * ge + s];
+            const R nx = R(nd.x), ny = R(nd.y);
             const int o = (e * 4 + s) * n + m;
-            const double cface = cfs[e * 4 + s];
-            const double sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cface;
-            const double pp = sc * ell[o], pu = sc * ell[FS + o], pv = sc * ell[2 * FS + o];
-            const double dn = 0.5 * (nv.x * pu + nv.y * pv);
-            const double wl = fma(0.5, pp, dn), wr = fma(-0.5, pp, dn);
+            const R cface = cfs[e * 4 + s];
+            const R sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cface;
+            const R pp = sc * ell[o], pu = sc * ell[FS + o], pv = sc * ell[2 * FS + o];
+            const R dn = R(0.5) * (nx * pu + ny * pv);
+            const R wl = fma(R(0.5), pp, dn), wr = fma(R(-0.5), pp, dn);
             // adjoints of L = (wl, wl nx, wl ny) and R = (wr, -wr nx, -wr ny)
-            const double sl = role ? -wr : wl;  // own trace: R for the right element
-            const double sf_ = role ? wl : -wr;
-            double tp_ = role ? wr : wl, tu = sl * nv.x, tv = sl * nv.y;
-            const double fp_ = role ? wl : wr, fu_ = sf_ * nv.x, fv_ = sf_ * nv.y;
+            const R sl = role ? -wr : wl;  // own trace: R for the right element
+            const R sf_ = role ? wl : -wr;
+            R tp_ = role ? wr : wl, tu = sl * nx, tv = sl * ny;
+            const R fp_ = role ? wl : wr, fu_ = sf_ * nx, fv_ = sf_ * ny;
             if (kind == kInterior) {
                 tp_ += far_s[o];
                 tu += far_s[FS + o];
                 tv += far_s[2 * FS + o];
             } else if (kind == kMirror || kind == kCopy) {
-                const double gsc = a.gscale[4 * ge + s];
-                double gu = fu_, gv = fv_;
+                const R gsc = R(a.gscale[4 * ge + s]);
+                R gu = fu_, gv = fv_;
                 if (kind == kMirror) {
-                    const double tx = -nv.y, ty = nv.x;
-                    const double l0 = -(fu_ * nv.x + fv_ * nv.y);
-                    const double l1 = fu_ * tx + fv_ * ty;
-                    gu = nv.x * l0 + tx * l1;
-                    gv = nv.y * l0 + ty * l1;
+                    const R tx = -ny, ty = nx;
+                    const R l0 = -(fu_ * nx + fv_ * ny);
+                    const R l1 = fu_ * tx + fv_ * ty;
+                    gu = nx * l0 + tx * l1;
+                    gv = ny * l0 + ty * l1;
                 }
                 tp_ = fma(gsc, fp_, tp_);
                 tu = fma(gsc, gu, tu);
@@ -627,13 +733,21 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
         if (ff < 3 && r < ne * NN) {
             const int el = r / NN, node = r - el * NN;
             const int i = node / n, j = node - i * n;
-            const double* Lo = ell + ff * FS + el * 4 * n;
+            const R* Lo = ell + ff * FS + el * 4 * n;
             double v = ls[ff * EPB * NN + r];
-            if (ff == 0) v += tp[r];
-            v = fma(lm[j], Lo[0 * n + i], v);
-            v = fma(lp[j], Lo[2 * n + (N - i)], v);
-            v = fma(lp[i], Lo[1 * n + j], v);
-            v = fma(lm[i], Lo[3 * n + (N - j)], v);
+            if (ff == 0) v += static_cast<double>(tp[r]);
+            if constexpr (std::is_same_v<R, double>) {
+                v = fma(lm[j], Lo[0 * n + i], v);
+                v = fma(lp[j], Lo[2 * n + (N - i)], v);
+                v = fma(lp[i], Lo[1 * n + j], v);
+                v = fma(lm[i], Lo[3 * n + (N - j)], v);
+            } else {
+                R t4 = lm[j] * Lo[0 * n + i];
+                t4 = fma(lp[j], Lo[2 * n + (N - i)], t4);
+                t4 = fma(lp[i], Lo[1 * n + j], t4);
+                t4 = fma(lm[i], Lo[3 * n + (N - j)], t4);
+                v += static_cast<double>(t4);
+            }
             if (ff == 0) {
                 unsigned long long mask = rmask[el];
                 while (mask) {
@@ -643,25 +757,25 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
                 }
             }
             a.lq[(ff * Kp + e0) * NN + r] = v;
-            nu[ff * EPB * NN + r] = -fma(a.gdt_next, v, kn[c]) * js[r];
+            nu[ff * EPB * NN + r] = R(-fma(a.gdt_next, v, kn[c])) * js[r];
         }
     }
     __syncthreads();
 
     // Lift transpose of nu' on the four sides (column m: sides 1, 3; row m:
-    // sides 2, 0); per element, the c-derivative accumulators.
+    // sides 2, 0); per element, the c-derivative accumulators (FP64).
     if (active) {
-        const double* Nn = nu + (f * EPB + e) * NN;
-        double l1 = 0.0, l3 = 0.0, l2 = 0.0, l0 = 0.0;
+        const R* Nn = nu + (f * EPB + e) * NN;
+        R l1 = 0, l3 = 0, l2 = 0, l0 = 0;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-            const double cv = Nn[i * n + m], rv = Nn[m * n + i];
+            const R cv = Nn[i * n + m], rv = Nn[m * n + i];
             l1 = fma(cv, lpw[i], l1);
             l3 = fma(cv, lmw[i], l3);
             l2 = fma(rv, lpw[i], l2);
             l0 = fma(rv, lmw[i], l0);
         }
-        double* L = ell + f * FS + e * 4 * n;
+        R* L = ell + f * FS + e * 4 * n;
         L[1 * n + m] = l1;
         L[3 * n + (N - m)] = l3;
         L[2 * n + (N - m)] = l2;
@@ -670,12 +784,12 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
     if (tid < ne) {
         double vsum = 0.0;
         for (int ff = 0; ff < 3; ++ff)
-            for (int i = 0; i < n; ++i) vsum += vd[(ff * EPB + tid) * n + i];
+            for (int i = 0; i < n; ++i) vsum += static_cast<double>(vd[(ff * EPB + tid) * n + i]);
         double* A = a.acc + (e0 + tid) * 5;
         A[0] += vsum;
         for (int s = 0; s < 4; ++s) {
             double us = 0.0;
-            for (int i = 0; i < n; ++i) us += up[(tid * 4 + s) * n + i];
+            for (int i = 0; i < n; ++i) us += static_cast<double>(up[(tid * 4 + s) * n + i]);
             A[1 + s] += us;
         }
     }
@@ -690,17 +804,18 @@ __global__ void __launch_bounds__(AdjTile<N>::kThreads) adjoint_stage_kernel(Adj
             const int2 lk = a.link[4 * ge + s];
             if (((lk.y >> 2) & 7) != kInterior) continue;
             const int role = (lk.y >> 5) & 1;
-            const double2 nv = a.normal[4 * ge + s];
+            const double2 nd = a.normal[4 * ge + s];
+            const R nx = R(nd.x), ny = R(nd.y);
             const int o = (e * 4 + s) * n + m;
-            const double sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cfs[e * 4 + s];
-            const double pp = sc * ell[o], pu = sc * ell[FS + o], pv = sc * ell[2 * FS + o];
-            const double dn = 0.5 * (nv.x * pu + nv.y * pv);
-            const double wl = fma(0.5, pp, dn), wr = fma(-0.5, pp, dn);
-            const double sf_ = role ? wl : -wr;
-            double* to = a.atr_out + (ge * 4 + s) * n + m;
+            const R sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cfs[e * 4 + s];
+            const R pp = sc * ell[o], pu = sc * ell[FS + o], pv = sc * ell[2 * FS + o];
+            const R dn = R(0.5) * (nx * pu + ny * pv);
+            const R wl = fma(R(0.5), pp, dn), wr = fma(R(-0.5), pp, dn);
+            const R sf_ = role ? wl : -wr;
+            R* to = atr_out + (ge * 4 + s) * n + m;
             to[0] = role ? wl : wr;
-            to[Kp * 4 * n] = sf_ * nv.x;
-            to[2 * Kp * 4 * n] = sf_ * nv.y;
+            to[Kp * 4 * n] = sf_ * nx;
+            to[2 * Kp * 4 * n] = sf_ * ny;
         }
     }
 }
@@ -720,66 +835,67 @@ __global__ void speed_gradient_kernel(const double* __restrict__ acc, const int2
 
 // ---------------------------------------------------------------------------
 // Host launchers.
-template <int N>
+template <int N, typename R>
 static cudaError_t prepare_speed_t() {
-    cudaError_t err = cudaFuncSetAttribute(speed_stage_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
+    cudaError_t err =
+        cudaFuncSetAttribute(speed_stage_kernel<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(SpeedTile<N, R>::kBytes));
     if (err != cudaSuccess) return err;
-    return cudaFuncSetAttribute(adjoint_stage_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(AdjTile<N>::kBytes));
+    return cudaFuncSetAttribute(adjoint_stage_kernel<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(AdjTile<N, R>::kBytes));
 }
 
-template <int N>
+template <int N, typename R>
 static cudaError_t launch_speed_stage_t(const SpeedStageArgs& a, cudaStream_t stream) {
-    using T = Tile<N>;
-    speed_stage_kernel<N><<<static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), T::kThreads, T::kBytes, stream>>>(a, make_speed_coeffs<N>());
+    using T = SpeedTile<N, R>;
+    speed_stage_kernel<N, R><<<static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), T::kThreads, T::kBytes, stream>>>(a, make_speed_coeffs<N, R>());
     return cudaGetLastError();
 }
 
-template <int N>
+template <int N, typename R>
 static cudaError_t launch_adjoint_stage_t(const AdjointStageArgs& a, cudaStream_t stream) {
-    using T = AdjTile<N>;
-    adjoint_stage_kernel<N><<<static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), T::kThreads, T::kBytes, stream>>>(a, make_adj_coeffs<N>());
+    using T = AdjTile<N, R>;
+    adjoint_stage_kernel<N, R><<<static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), T::kThreads, T::kBytes, stream>>>(a, make_adj_coeffs<N, R>());
     return cudaGetLastError();
 }
 
-template <int N>
+template <int N, typename R>
 static int adjoint_epb_t() {
-    return AdjTile<N>::EPB;
+    return AdjTile<N, R>::EPB;
 }
 
-#define NDG_SPEED_DISPATCH(FN, N_, ...)        \
-    switch (N_) {                              \
-        case 1: return FN<1>(__VA_ARGS__);     \
-        case 2: return FN<2>(__VA_ARGS__);     \
-        case 3: return FN<3>(__VA_ARGS__);     \
-        case 4: return FN<4>(__VA_ARGS__);     \
-        case 5: return FN<5>(__VA_ARGS__);     \
-        case 6: return FN<6>(__VA_ARGS__);     \
-        case 7: return FN<7>(__VA_ARGS__);     \
-        case 8: return FN<8>(__VA_ARGS__);     \
-        case 9: return FN<9>(__VA_ARGS__);     \
-        case 10: return FN<10>(__VA_ARGS__);   \
-        case 11: return FN<11>(__VA_ARGS__);   \
-        case 12: return FN<12>(__VA_ARGS__);   \
-        default: break;                        \
+#define NDG_SPEED_DISPATCH(FN, N_, F32_, ...)                                                   \
+    switch (N_) {                                                                               \
+        case 1: return F32_ ? FN<1, float>(__VA_ARGS__) : FN<1, double>(__VA_ARGS__);           \
+        case 2: return F32_ ? FN<2, float>(__VA_ARGS__) : FN<2, double>(__VA_ARGS__);           \
+        case 3: return F32_ ? FN<3, float>(__VA_ARGS__) : FN<3, double>(__VA_ARGS__);           \
+        case 4: return F32_ ? FN<4, float>(__VA_ARGS__) : FN<4, double>(__VA_ARGS__);           \
+        case 5: return F32_ ? FN<5, float>(__VA_ARGS__) : FN<5, double>(__VA_ARGS__);           \
+        case 6: return F32_ ? FN<6, float>(__VA_ARGS__) : FN<6, double>(__VA_ARGS__);           \
+        case 7: return F32_ ? FN<7, float>(__VA_ARGS__) : FN<7, double>(__VA_ARGS__);           \
+        case 8: return F32_ ? FN<8, float>(__VA_ARGS__) : FN<8, double>(__VA_ARGS__);           \
+        case 9: return F32_ ? FN<9, float>(__VA_ARGS__) : FN<9, double>(__VA_ARGS__);           \
+        case 10: return F32_ ? FN<10, float>(__VA_ARGS__) : FN<10, double>(__VA_ARGS__);        \
+        case 11: return F32_ ? FN<11, float>(__VA_ARGS__) : FN<11, double>(__VA_ARGS__);        \
+        case 12: return F32_ ? FN<12, float>(__VA_ARGS__) : FN<12, double>(__VA_ARGS__);        \
+        default: break;                                                                         \
     }
 
-cudaError_t prepare_speed_kernels(int N) {
-    NDG_SPEED_DISPATCH(prepare_speed_t, N)
+cudaError_t prepare_speed_kernels(int N, bool fp32) {
+    NDG_SPEED_DISPATCH(prepare_speed_t, N, fp32)
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_speed_stage(int N, const SpeedStageArgs& a, cudaStream_t stream) {
-    NDG_SPEED_DISPATCH(launch_speed_stage_t, N, a, stream)
+cudaError_t launch_speed_stage(int N, bool fp32, const SpeedStageArgs& a, cudaStream_t stream) {
+    NDG_SPEED_DISPATCH(launch_speed_stage_t, N, fp32, a, stream)
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_adjoint_stage(int N, const AdjointStageArgs& a, cudaStream_t stream) {
-    NDG_SPEED_DISPATCH(launch_adjoint_stage_t, N, a, stream)
+cudaError_t launch_adjoint_stage(int N, bool fp32, const AdjointStageArgs& a, cudaStream_t stream) {
+    NDG_SPEED_DISPATCH(launch_adjoint_stage_t, N, fp32, a, stream)
     return cudaErrorInvalidValue;
 }
 
-int adjoint_elements_per_block(int N) {
-    NDG_SPEED_DISPATCH(adjoint_epb_t, N)
+int adjoint_elements_per_block(int N, bool fp32) {
+    NDG_SPEED_DISPATCH(adjoint_epb_t, N, fp32)
     return 0;
 }
 

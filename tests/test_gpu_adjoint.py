@@ -198,3 +198,63 @@ def test_rejections():
     mesh.adapt(np.ones(K, np.int32), np.full(K, 2.0))  # p-refinement: the mesh changes
     with pytest.raises(ndg.NdgError, match="INVALID_ARG"):
         adj.forward(np.zeros(adj.field_size), 0.01, 2)
+
+
+# FP32 form: the operator's arithmetic in FP32 (states, RK updates and
+# gradient accumulation in FP64). Its gradient is compared with the FP64
+# references: the oracle's CPU adjoint and central differences of the FP64
+# forward, at FP32 accuracy.
+@pytest.mark.parametrize("kind", ["walls", "periodic", "jittered_outflow"])
+def test_fp32_operator_and_transpose(kind):
+    zone = meshgen.uniform_zone(8, **MESHES[kind])
+    c = A.speed_field(zone, seed=1)
+    mesh = ndg.Mesh2D_t(zone, 6)
+    adj = ndg.Adjoint2D_t(mesh, speed=c, precision=ndg.FP32)
+    o, _, _ = A.oracle_problem(zone, 6, c, np.zeros((0, 2)))
+    rng = np.random.default_rng(12)
+    n = 3 * mesh.field_size
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    Lx, LTy, dc = adj.operator(x, y)
+    LTy_o, dc_o = o.operator_transpose(x, y)
+    assert rel_l2(Lx, o.operator(x)) < 1e-6
+    assert rel_l2(LTy, LTy_o) < 1e-6
+    assert rel_l2(dc, dc_o) < 1e-5
+    assert abs(float(Lx @ y) - float(x @ LTy)) < 1e-6 * np.linalg.norm(Lx) * np.linalg.norm(y)
+
+
+@pytest.mark.parametrize("kind", ["walls", "periodic"])
+def test_fp32_gradient_vs_cpu_fp64_adjoint_and_differences(kind):
+    N, steps = 5, 40
+    zone = meshgen.uniform_zone(16, **MESHES[kind])
+    c = A.speed_field(zone, seed=8)
+    xy = A.circle_receivers(16, 0.7)
+    mesh = ndg.Mesh2D_t(zone, N)
+    a64 = ndg.Adjoint2D_t(mesh, xy, speed=c)
+    a32 = ndg.Adjoint2D_t(mesh, xy, speed=c, precision=ndg.FP32)
+    o, el, w = A.oracle_problem(zone, N, c, xy)
+    p0 = A.gaussian_pulse(zone, N, sigma=0.15, centre=(0.4, 0.1))
+    dt = a64.delta_t(0.5)
+    a64.set_speed(c * (1 + 0.05 * np.sin(3 * A.element_centres(zone)[:, 0])))
+    _, target = a64.forward(p0, dt, steps)
+    a64.set_speed(c)
+    J32, s32 = a32.forward(p0, dt, steps, targets=target, checkpoint_interval=9)
+    g32 = a32.backward()
+    ref = o.adjoint_solve(p0, dt, steps, el, w, targets=target)
+    assert rel_l2(s32, ref["samples"]) < 1e-6
+    assert abs(J32 - ref["J"]) < 1e-4 * ref["J"]
+    for k in ("p0", "c"):
+        assert rel_l2(g32[k], ref[k]) < 1e-4, (k, rel_l2(g32[k], ref[k]))
+    # central differences of the FP64 forward along random directions
+    rng = np.random.default_rng(6)
+    dp = rng.standard_normal(p0.size)
+    eps = 1e-4
+    Jp, _ = a64.forward(p0 + eps * dp, dt, steps, targets=target)
+    Jm, _ = a64.forward(p0 - eps * dp, dt, steps, targets=target)
+    assert _rel((Jp - Jm) / (2 * eps), float(g32["p0"] @ dp)) < 1e-4
+    dcv = rng.standard_normal(c.size)
+    eps = 1e-6
+    a64.set_speed(c + eps * dcv)
+    Jp, _ = a64.forward(p0, dt, steps, targets=target)
+    a64.set_speed(c - eps * dcv)
+    Jm, _ = a64.forward(p0, dt, steps, targets=target)
+    assert _rel((Jp - Jm) / (2 * eps), float(g32["c"] @ dcv)) < 1e-4
