@@ -47,7 +47,7 @@ ADJ_BYTES_PER_DOF_STAGE = 40
 
 
 def workload_zone():
-    from tests import meshgen
+    from ndg_cuda_b200 import meshgen
     return meshgen.uniform_zone(RES, x_periodic=True, y_periodic=True)
 
 
@@ -197,8 +197,8 @@ def batched_leg(local: int, stream, peak: float, dist) -> dict:
     import numpy as np
     import torch
     import ndg_cuda_b200 as ndg
-    from tests import adjoint_setup as A
-    from tests import meshgen
+    from ndg_cuda_b200 import workloads as A
+    from ndg_cuda_b200 import meshgen
     zone = meshgen.uniform_zone(BATCH_RES, boundary=meshgen.WALL)
     rng = np.random.default_rng(64)
     centres = rng.uniform(-0.8, 0.8, size=(BATCH_INSTANCES, 2))
@@ -267,8 +267,8 @@ def adjoint_leg(local: int, stream, peak: float, cpu_sample: bool) -> dict:
     host buffers."""
     import numpy as np
     import ndg_cuda_b200 as ndg
-    from tests import adjoint_setup as A
-    from tests import meshgen
+    from ndg_cuda_b200 import workloads as A
+    from ndg_cuda_b200 import meshgen
     zone = meshgen.uniform_zone(ADJ_RES, order="rowmajor", boundary=meshgen.WALL)
     c = A.speed_field(zone, seed=0)
     mesh = ndg.Mesh2D_t(zone, ADJ_N, device=local, stream=stream.cuda_stream)
@@ -334,7 +334,8 @@ def adjoint_leg(local: int, stream, peak: float, cpu_sample: bool) -> dict:
     a32.close()
     if cpu_sample:
         # the oracle's CPU FP64 adjoint on a bounded sample of the same problem
-        o, el, w = A.oracle_problem(zone, ADJ_N, c, A.circle_receivers(ADJ_RECEIVERS, 0.7))
+        from tests import adjoint_setup
+        o, el, w = adjoint_setup.oracle_problem(zone, ADJ_N, c, A.circle_receivers(ADJ_RECEIVERS, 0.7))
         n_cpu = 4
         t0 = time.perf_counter()
         o.adjoint_solve(p0, dt, n_cpu, el, w, targets=target[:n_cpu + 1])
