@@ -189,6 +189,44 @@ GeneralPlan build_general_plan(const Topology& t) {
     std::map<int, std::vector<int64_t>> by_order;
     for (int64_t e = 0; e < K; ++e) by_order[t.elem_N[static_cast<size_t>(e)]].push_back(e);
     for (auto& kv : by_order) p.groups.emplace_back(kv.first, std::move(kv.second));
+
+    // Mortar weight blocks for the sides and face sides that need them.
+    auto conforming = [&](int64_t f, int64_t e, int64_t es, bool left) {
+        const int64_t a = t.elem_nodes[static_cast<size_t>(e)][static_cast<size_t>(es)];
+        const int64_t b = t.elem_nodes[static_cast<size_t>(e)][static_cast<size_t>((es + 1) & 3)];
+        const auto& fn = t.face_nodes[static_cast<size_t>(f)];
+        return t.face_N[static_cast<size_t>(f)] == t.elem_N[static_cast<size_t>(e)] && (left ? (fn[0] == a && fn[1] == b) : (fn[1] == a && fn[0] == b));
+    };
+    p.sw_off.assign(p.sface.size(), -1);
+    p.sm_off.assign(p.sface.size(), -1);
+    for (int64_t e = 0; e < K; ++e)
+        for (int s = 0; s < 4; ++s) {
+            const int64_t q0 = p.sface_start[static_cast<size_t>(4 * e + s)], q1 = p.sface_start[static_cast<size_t>(4 * e + s + 1)];
+            if (q1 == q0) continue;
+            const int64_t f0 = p.sface[static_cast<size_t>(q0)];
+            if (q1 - q0 == 1 && (conforming(f0, e, s, true) || conforming(f0, e, s, false))) continue;
+            const int64_t ne_ = t.elem_N[static_cast<size_t>(e)] + 1;
+            for (int64_t q = q0; q < q1; ++q) {
+                const int64_t nf = t.face_N[static_cast<size_t>(p.sface[static_cast<size_t>(q)])] + 1;
+                p.sw_off[static_cast<size_t>(q)] = p.sw_total;
+                p.sw_total += ne_ * nf;
+                p.sm_off[static_cast<size_t>(q)] = p.sm_total;
+                p.sm_total += nf;
+            }
+        }
+    p.fw_off.assign(static_cast<size_t>(2 * F), -1);
+    p.fm_off.assign(static_cast<size_t>(2 * F), -1);
+    for (int64_t f = 0; f < F; ++f)
+        for (int side = 0; side < 2; ++side) {
+            const int64_t e = t.face_elems[static_cast<size_t>(f)][static_cast<size_t>(side)];
+            const int64_t es = t.face_sides[static_cast<size_t>(f)][static_cast<size_t>(side)];
+            if (conforming(f, e, es, side == 0)) continue;
+            const int64_t nf = t.face_N[static_cast<size_t>(f)] + 1, ne_ = t.elem_N[static_cast<size_t>(e)] + 1;
+            p.fw_off[static_cast<size_t>(2 * f + side)] = p.fw_total;
+            p.fw_total += nf * ne_ + nf;
+            p.fm_off[static_cast<size_t>(2 * f + side)] = p.fm_total;
+            p.fm_total += nf;
+        }
     return p;
 }
 

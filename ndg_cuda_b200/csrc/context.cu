@@ -337,6 +337,14 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_gscale.upload(g.gscale, c->stream);
         c->g_gsrc.upload(g.gsrc, c->stream);
         c->g_gsrc_side.upload(g.gsrc_side, c->stream);
+        c->g_sw_off.upload(g.sw_off, c->stream);
+        c->g_sm_off.upload(g.sm_off, c->stream);
+        c->g_fw_off.upload(g.fw_off, c->stream);
+        c->g_fm_off.upload(g.fm_off, c->stream);
+        c->g_sw.allocate(static_cast<size_t>(std::max<int64_t>(g.sw_total, 1)));
+        c->g_fw.allocate(static_cast<size_t>(std::max<int64_t>(g.fw_total, 1)));
+        c->g_smatch.allocate(static_cast<size_t>(std::max<int64_t>(g.sm_total, 1)));
+        c->g_fmatch.allocate(static_cast<size_t>(std::max<int64_t>(g.fm_total, 1)));
         std::vector<int64_t> ids;
         for (const auto& grp : g.groups) ids.insert(ids.end(), grp.second.begin(), grp.second.end());
         c->g_ids.upload(ids, c->stream);
@@ -385,6 +393,16 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.gscale = c->g_gscale.ptr;
         M.gsrc = c->g_gsrc.ptr;
         M.gsrc_side = c->g_gsrc_side.ptr;
+        M.sw_off = c->g_sw_off.ptr;
+        M.sm_off = c->g_sm_off.ptr;
+        M.fw_off = c->g_fw_off.ptr;
+        M.fm_off = c->g_fm_off.ptr;
+        M.sw = c->g_sw.ptr;
+        M.smatch = c->g_smatch.ptr;
+        M.fw = c->g_fw.ptr;
+        M.fmatch = c->g_fmatch.ptr;
+        check_cuda(dev::launch_general_weights(M, c->g_sw.ptr, c->g_smatch.ptr, c->g_fw.ptr, c->g_fmatch.ptr, c->stream), "mortar weights");
+        c->launches += 2;
         // The uniform-path corners also serve the initial condition of a
         // general mesh.
         c->corners.upload(g.corners, c->stream);

@@ -97,6 +97,9 @@ struct ndg_ctx {
     ndg::DeviceBuffer<int32_t> g_eN, g_fN, g_gkind, g_gsrc_side;
     ndg::DeviceBuffer<int64_t> g_off2, g_off1, g_enodes, g_sface_start, g_sface, g_foff, g_fnodes, g_felem, g_fside, g_gsrc, g_ids;
     ndg::DeviceBuffer<double> g_corners, g_node_xy, g_fnormal, g_ftangent, g_foffset, g_fscale, g_gscale, etr, ffl;
+    ndg::DeviceBuffer<int64_t> g_sw_off, g_sm_off, g_fw_off, g_fm_off;  // mortar weight offsets
+    ndg::DeviceBuffer<double> g_sw, g_fw;                              // mortar weights
+    ndg::DeviceBuffer<int32_t> g_smatch, g_fmatch;                     // mortar node matches
     std::vector<ndg::dev::OrderGroup> groups;
     ndg::dev::GeneralMesh gmesh;
 

@@ -230,27 +230,27 @@ __global__ void __launch_bounds__(256) general_faces_kernel(GeneralStage a, int 
                 val[side][1] = ep[src + ft];
                 val[side][2] = ep[src + 2 * ft];
             } else {
-                const double* xe = g_nodes + gvec(Ne);
-                const double* bwe = g_bary + gvec(Ne);
-                const double coord = mortar_coord(xf[side == 0 ? i : Nf - i], M.fscale[2 * f + side], M.foffset[2 * f + side]);
-                double pn = 0.0, un = 0.0, vn = 0.0, den = 0.0;
-                for (int j = 0; j <= Ne; ++j) {
-                    if (almost_equal(coord, xe[j])) {
-                        pn = ep[j];
-                        un = ep[j + ft];
-                        vn = ep[j + 2 * ft];
-                        den = 1.0;
-                        break;
+                // Interpolation to the face node with the plan's weights
+                // (face_weights_kernel): a matching element node is copied.
+                const int match = M.fmatch[M.fm_off[2 * f + side] + i];
+                if (match >= 0) {
+                    val[side][0] = ep[match];
+                    val[side][1] = ep[match + ft];
+                    val[side][2] = ep[match + 2 * ft];
+                } else {
+                    const double* tw = M.fw + M.fw_off[2 * f + side];
+                    const double* tj = tw + i * (Ne + 1);
+                    const double den = tw[(Nf + 1) * (Ne + 1) + i];
+                    double pn = 0.0, un = 0.0, vn = 0.0;
+                    for (int j = 0; j <= Ne; ++j) {
+                        pn = madd<S>(pn, tj[j], ep[j]);
+                        un = madd<S>(un, tj[j], ep[j + ft]);
+                        vn = madd<S>(vn, tj[j], ep[j + 2 * ft]);
                     }
-                    const double tj = S ? __ddiv_rn(bwe[j], __dsub_rn(coord, xe[j])) : bwe[j] / (coord - xe[j]);
-                    pn = madd<S>(pn, tj, ep[j]);
-                    un = madd<S>(un, tj, ep[j + ft]);
-                    vn = madd<S>(vn, tj, ep[j + 2 * ft]);
-                    den = add<S>(den, tj);
+                    val[side][0] = S ? __ddiv_rn(pn, den) : pn / den;
+                    val[side][1] = S ? __ddiv_rn(un, den) : un / den;
+                    val[side][2] = S ? __ddiv_rn(vn, den) : vn / den;
                 }
-                val[side][0] = S ? __ddiv_rn(pn, den) : pn / den;
-                val[side][1] = S ? __ddiv_rn(un, den) : un / den;
-                val[side][2] = S ? __ddiv_rn(vn, den) : vn / den;
             }
         }
         // Upwind flux with c = 1 (Solver2D_t.cpp:48-63).
@@ -265,7 +265,107 @@ __global__ void __launch_bounds__(256) general_faces_kernel(GeneralStage a, int 
     }
 }
 
+// Mortar weights of the element sides (Mesh2D_t.cpp:3895-4006, the
+// multi-face branch): per face node j the element node it matches
+// (almost_equal) or -1, and the weight of every element node i,
+// sign w_f[j] / w_e[i] at the match or sign T_i w_f[j] / w_e[i] with the
+// barycentric T_i, in the reference's rounding. Thread per domain element
+// side.
+__global__ void __launch_bounds__(128) side_weights_kernel(GeneralMesh M, double* __restrict__ sw, int* __restrict__ smatch) {
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < 4 * M.n_domain;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t e = idx / 4;
+        const int s = static_cast<int>(idx - 4 * e);
+        const int N = M.eN[e];
+        const double* xe = g_nodes + gvec(N);
+        const double* we = g_weights + gvec(N);
+        const double* bwe = g_bary + gvec(N);
+        for (int64_t q = M.sface_start[4 * e + s]; q < M.sface_start[4 * e + s + 1]; ++q) {
+            if (M.sw_off[q] < 0) continue;
+            const int64_t f = M.sface[q];
+            const int Nf = M.fN[f];
+            const double* xf = g_nodes + gvec(Nf);
+            const double* wf = g_weights + gvec(Nf);
+            const bool fwd = e == M.felem[2 * f];
+            const int fs = fwd ? 0 : 1;
+            const double sgn = fwd ? 1.0 : -1.0;
+            const double scale = M.fscale[2 * f + fs], offset = M.foffset[2 * f + fs];
+            double* W = sw + M.sw_off[q];
+            int* match = smatch + M.sm_off[q];
+            for (int j = 0; j <= Nf; ++j) {
+                const double coord = mortar_coord(xf[fwd ? j : Nf - j], scale, offset);
+                int found = -1;
+                for (int ii = 0; ii <= N; ++ii)
+                    if (almost_equal(coord, xe[ii])) {
+                        found = ii;
+                        break;
+                    }
+                match[j] = found;
+                if (found >= 0) {
+                    for (int i = 0; i <= N; ++i) W[i * (Nf + 1) + j] = (i == found) ? __ddiv_rn(__dmul_rn(sgn, wf[j]), we[i]) : 0.0;
+                } else {
+                    double sb = 0.0;
+                    for (int ii = 0; ii <= N; ++ii) sb = __dadd_rn(sb, __ddiv_rn(bwe[ii], __dsub_rn(coord, xe[ii])));
+                    for (int i = 0; i <= N; ++i) {
+                        const double T = __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), sb));
+                        W[i * (Nf + 1) + j] = __ddiv_rn(__dmul_rn(__dmul_rn(sgn, T), wf[j]), we[i]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Interpolation weights of the non-conforming face sides
+// (Mesh2D_t.cpp:3803-3893): per face node i the element node it matches or
+// -1, the barycentric terms t_j = w_j / (x - x_j) and their sum, in the
+// reference's rounding. Thread per face side.
+__global__ void __launch_bounds__(128) face_weights_kernel(GeneralMesh M, double* __restrict__ fw, int* __restrict__ fmatch) {
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < 2 * M.n_faces;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (M.fw_off[idx] < 0) continue;
+        const int64_t f = idx / 2;
+        const int side = static_cast<int>(idx - 2 * f);
+        const int Nf = M.fN[f];
+        const int64_t e = M.felem[2 * f + side];
+        const int Ne = M.eN[e];
+        const double* xf = g_nodes + gvec(Nf);
+        const double* xe = g_nodes + gvec(Ne);
+        const double* bwe = g_bary + gvec(Ne);
+        double* tw = fw + M.fw_off[idx];
+        int* match = fmatch + M.fm_off[idx];
+        for (int i = 0; i <= Nf; ++i) {
+            const double coord = mortar_coord(xf[side == 0 ? i : Nf - i], M.fscale[2 * f + side], M.foffset[2 * f + side]);
+            int found = -1;
+            double den = 0.0;
+            for (int j = 0; j <= Ne; ++j) {
+                if (almost_equal(coord, xe[j])) {
+                    found = j;
+                    break;
+                }
+                const double tj = __ddiv_rn(bwe[j], __dsub_rn(coord, xe[j]));
+                tw[i * (Ne + 1) + j] = tj;
+                den = __dadd_rn(den, tj);
+            }
+            match[i] = found;
+            tw[(Nf + 1) * (Ne + 1) + i] = den;
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, cudaStream_t stream) {
+    if (m.n_domain > 0) {
+        const int blocks = static_cast<int>(std::min<int64_t>((4 * m.n_domain + 127) / 128, 148 * 8));
+        side_weights_kernel<<<blocks, 128, 0, stream>>>(m, sw, smatch);
+    }
+    if (m.n_faces > 0) {
+        const int blocks = static_cast<int>(std::min<int64_t>((2 * m.n_faces + 127) / 128, 148 * 8));
+        face_weights_kernel<<<blocks, 128, 0, stream>>>(m, fw, fmatch);
+    }
+    return cudaGetLastError();
+}
 
 namespace {
 
@@ -318,38 +418,21 @@ __device__ __forceinline__ void element_side_flux(const GeneralStage& a, const d
         out[2] = mul<S>(-fl[2 * ff], sfv);
         return;
     }
-    const double* xe = g_nodes + gvec(N);
-    const double* we = g_weights + gvec(N);
-    const double* bwe = g_bary + gvec(N);
+    // Mortar projection with the plan's weights (side_weights_kernel): a
+    // face node that matches an element node feeds that node only.
     double acc[3] = {0.0, 0.0, 0.0};
     for (int64_t q = q0; q < q1; ++q) {
         const int64_t f = M.sface[q];
         const int Nf = M.fN[f];
-        const double* xf = g_nodes + gvec(Nf);
-        const double* wf = g_weights + gvec(Nf);
-        const bool fwd = e == M.felem[2 * f];
-        const int fs = fwd ? 0 : 1;
-        const double sgn = fwd ? 1.0 : -1.0;
-        const double scale = M.fscale[2 * f + fs], offset = M.foffset[2 * f + fs];
+        const int fs = e == M.felem[2 * f] ? 0 : 1;
+        const double scale = M.fscale[2 * f + fs];
+        const double* W = M.sw + M.sw_off[q] + i * (Nf + 1);
+        const int* match = M.smatch + M.sm_off[q];
         for (int j = 0; j <= Nf; ++j) {
-            const double coord = mortar_coord(xf[fwd ? j : Nf - j], scale, offset);
+            const int mt = match[j];
+            if (mt >= 0 && mt != i) continue;
+            const double w = W[j];
             const double* fl = ffl + M.foff[f] + j;
-            int found = -1;
-            for (int ii = 0; ii <= N; ++ii)
-                if (almost_equal(coord, xe[ii])) {
-                    found = ii;
-                    break;
-                }
-            double w;
-            if (found >= 0) {
-                if (found != i) continue;
-                w = S ? __ddiv_rn(__dmul_rn(sgn, wf[j]), we[i]) : sgn * wf[j] / we[i];
-            } else {
-                double sb = 0.0;
-                for (int ii = 0; ii <= N; ++ii) sb = add<S>(sb, S ? __ddiv_rn(bwe[ii], __dsub_rn(coord, xe[ii])) : bwe[ii] / (coord - xe[ii]));
-                const double T = S ? __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), sb)) : bwe[i] / ((coord - xe[i]) * sb);
-                w = S ? __ddiv_rn(__dmul_rn(__dmul_rn(sgn, T), wf[j]), we[i]) : sgn * T * wf[j] / we[i];
-            }
 #pragma unroll
             for (int c = 0; c < 3; ++c) acc[c] = add<S>(acc[c], mul<S>(mul<S>(mul<S>(w, fl[c * ff]), sfv), scale));
         }

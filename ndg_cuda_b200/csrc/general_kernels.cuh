@@ -50,6 +50,19 @@ struct GeneralMesh {
     const double* gscale = nullptr;     // [n_total - n_domain] side-0 scaling factor
     const int64_t* gsrc = nullptr;      // [n_total - n_domain] interface origin element
     const int* gsrc_side = nullptr;     // [n_total - n_domain] interface origin side
+    // Precomputed mortar weights (launch_general_weights): element side
+    // projections per sface entry (weights [N_e+1][N_f+1], node match per
+    // face node, -1 = barycentric) and face-side interpolations per
+    // (face, side) (weights [N_f+1][N_e+1] then N_f+1 denominators, node
+    // match per face node); offsets -1 where the fast conforming path runs.
+    const int64_t* sw_off = nullptr;
+    const int64_t* sm_off = nullptr;
+    const int64_t* fw_off = nullptr;
+    const int64_t* fm_off = nullptr;
+    const double* sw = nullptr;
+    const int* smatch = nullptr;
+    const double* fw = nullptr;
+    const int* fmatch = nullptr;
 };
 
 // One RK3 stage on a mixed-order mesh.
@@ -74,6 +87,9 @@ struct OrderGroup {
 };
 
 cudaError_t upload_general_tables(const Tables& t);
+// Fills the mortar weights of a plan (once per plan): the same arithmetic,
+// in the reference's rounding, as the per-node computation they replace.
+cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, cudaStream_t stream);
 cudaError_t prepare_general_kernels(int N);
 // Side traces, ghost traces, face fluxes, then per order group the
 // element fluxes, volume term and RK update.

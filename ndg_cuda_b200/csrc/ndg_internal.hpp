@@ -111,6 +111,14 @@ struct GeneralPlan {
     std::vector<int64_t> gsrc;
     std::vector<int32_t> gsrc_side;
     std::vector<std::pair<int, std::vector<int64_t>>> groups;  // order, its domain elements
+    // Mortar weights, filled on the device once per plan. Per entry of
+    // sface on a domain element side that is not one conforming face of the
+    // element's order: offsets of its (N_e+1) x (N_f+1) projection weights
+    // and of its N_f+1 node matches (-1 elsewhere). Per face side that is not
+    // conforming: offsets of its (N_f+1) x (N_e+1) interpolation weights
+    // followed by N_f+1 denominators, and of its N_f+1 node matches.
+    std::vector<int64_t> sw_off, sm_off, fw_off, fm_off;
+    int64_t sw_total = 0, sm_total = 0, fw_total = 0, fm_total = 0;
 };
 GeneralPlan build_general_plan(const Topology& t);
 
