@@ -3,11 +3,15 @@
     python -m ndg_cuda_b200.cases stage   --res 256 --order 8 --steps 3 [--fp32] [--tile E]
     python -m ndg_cuda_b200.cases batched --res 64 --order 6 --instances 64 --steps 3 [--fp32]
     python -m ndg_cuda_b200.cases adjoint --res 96 --order 7 --steps 20 --interval 10 [--fp32]
+    python -m ndg_cuda_b200.cases mixed   --res 128 --order 4 --rounds 3 --steps 2
 
 `stage`: the reference plane wave on a periodic res x res mesh (RK3 steps).
 `batched`: independent radial pulses on one walled mesh, one launch per stage.
 `adjoint`: forward solve with receivers and its gradient (recomputation and
 adjoint sweep) on a walled mesh with a per-element wave speed.
+`mixed`: a jittered periodic mesh whose orders are raised by 2 on a seeded
+40% of the elements in each of `rounds` p-adaptations (orders 4 to 10 for
+order 4 and 3 rounds), then steps on the mixed-order path.
 Inputs are the seeded synthetic ones of ndg_cuda_b200.workloads.
 """
 from __future__ import annotations
@@ -26,12 +30,13 @@ def _zone(res: int, **kw) -> dict:
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("case", choices=["stage", "batched", "adjoint"])
+    ap.add_argument("case", choices=["stage", "batched", "adjoint", "mixed"])
     ap.add_argument("--res", type=int, default=64)
     ap.add_argument("--order", type=int, default=6)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--instances", type=int, default=1)
     ap.add_argument("--interval", type=int, default=0, help="adjoint checkpoint interval (0: one interval)")
+    ap.add_argument("--rounds", type=int, default=3, help="p-adaptation rounds of the mixed case")
     ap.add_argument("--tile", type=int, default=0, help="elements per CTA of the stage kernel (0: default)")
     ap.add_argument("--fp32", action="store_true")
     args = ap.parse_args(argv)
@@ -52,6 +57,16 @@ def main(argv=None) -> None:
         if args.tile:
             mesh.set_tile(args.tile)
         mesh.set_field("p", p0)
+        Solver2D_t.run(mesh, args.steps)
+        print("p[0] =", mesh.get_field("p")[0])
+    elif args.case == "mixed":
+        zone = _zone(args.res, x_periodic=True, y_periodic=True, jitter=0.1, seed=1)
+        mesh = Mesh2D_t(zone, args.order, maximum_N=args.order + 2 * args.rounds, precision=prec)
+        mesh.initial_conditions()
+        rng = np.random.default_rng(0)
+        for _ in range(args.rounds):
+            K = mesh.n_elements_
+            mesh.adapt((rng.random(K) < 0.4).astype(np.int32), np.full(K, 2.0))
         Solver2D_t.run(mesh, args.steps)
         print("p[0] =", mesh.get_field("p")[0])
     else:

@@ -197,6 +197,13 @@ GeneralPlan build_general_plan(const Topology& t) {
         const auto& fn = t.face_nodes[static_cast<size_t>(f)];
         return t.face_N[static_cast<size_t>(f)] == t.elem_N[static_cast<size_t>(e)] && (left ? (fn[0] == a && fn[1] == b) : (fn[1] == a && fn[0] == b));
     };
+    for (int64_t e = 0; e < K; ++e)
+        for (int s = 0; s < 4; ++s) {
+            int64_t slots = 0;
+            for (int64_t q = p.sface_start[static_cast<size_t>(4 * e + s)]; q < p.sface_start[static_cast<size_t>(4 * e + s + 1)]; ++q)
+                slots += t.face_N[static_cast<size_t>(p.sface[static_cast<size_t>(q)])] + 1;
+            p.side_slots = std::max(p.side_slots, slots);
+        }
     p.sw_off.assign(p.sface.size(), -1);
     p.sm_off.assign(p.sface.size(), -1);
     for (int64_t e = 0; e < K; ++e)
@@ -213,6 +220,16 @@ GeneralPlan build_general_plan(const Topology& t) {
                 p.sm_off[static_cast<size_t>(q)] = p.sm_total;
                 p.sm_total += nf;
             }
+        }
+    p.fbase.resize(static_cast<size_t>(2 * F));
+    p.fsN.resize(static_cast<size_t>(2 * F));
+    for (int64_t f = 0; f < F; ++f)
+        for (int side = 0; side < 2; ++side) {
+            const int64_t e = t.face_elems[static_cast<size_t>(f)][static_cast<size_t>(side)];
+            const int64_t es = t.face_sides[static_cast<size_t>(f)][static_cast<size_t>(side)];
+            const int Ne = t.elem_N[static_cast<size_t>(e)];
+            p.fbase[static_cast<size_t>(2 * f + side)] = p.off1[static_cast<size_t>(e)] + es * (Ne + 1);
+            p.fsN[static_cast<size_t>(2 * f + side)] = Ne;
         }
     p.fw_off.assign(static_cast<size_t>(2 * F), -1);
     p.fm_off.assign(static_cast<size_t>(2 * F), -1);

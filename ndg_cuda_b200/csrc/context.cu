@@ -80,14 +80,15 @@ dev::StageArgs stage_args(ndg_ctx* c, int m, int in) {
     return a;
 }
 
-dev::GeneralStage general_args(ndg_ctx* c, int m) {
+dev::GeneralStage general_args(ndg_ctx* c, int m, int in) {
     dev::GeneralStage a{};
     a.m = c->gmesh;
     a.q = c->q.ptr;
     a.k = c->k.ptr;
     a.G_out = c->keep_derivative ? c->G.ptr : nullptr;
-    a.etr = c->etr.ptr;
-    a.ffl = c->ffl.ptr;
+    a.etr = c->getr[in].ptr;
+    a.etr_out = c->getr[1 - in].ptr;
+    a.side_slots = c->side_slots;
     a.step = c->step.ptr;
     a.rk_a = kRkA[m];
     a.rk_b = kRkB[m];
@@ -97,19 +98,55 @@ dev::GeneralStage general_args(ndg_ctx* c, int m) {
     return a;
 }
 
-// Kernel launches of one stage of the general path: side traces and volume
-// per order group, ghost traces, face fluxes.
+// Kernel launches of one stage of the general path: ghost traces, then the
+// fused stage of every order group.
 int64_t general_stage_launches(const ndg_ctx* c) {
     const int64_t ghosts = c->gmesh.n_total > c->gmesh.n_domain ? 1 : 0;
-    return 2 * static_cast<int64_t>(c->groups.size()) + ghosts + 1;
+    return static_cast<int64_t>(c->groups.size()) + ghosts;
 }
 
 bool fp32(const ndg_ctx* c) { return c->precision == NDG_FP32; }
 
+// Side streams and events for the concurrent order groups (created once,
+// before any capture).
+void ensure_aux_streams(ndg_ctx* c) {
+    const size_t want = c->groups.size() > 1 ? c->groups.size() - 1 : 0;
+    while (c->aux_streams.size() < want) {
+        cudaStream_t st;
+        check_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        c->aux_streams.push_back(st);
+    }
+    while (c->aux_events.size() < want + 1) {
+        cudaEvent_t ev;
+        check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        c->aux_events.push_back(ev);
+    }
+}
+
+// One stage of the mixed-order path: the ghost traces on the context's
+// stream, then the order groups forked onto side streams (group 0 stays on
+// the stream) and joined back.
+cudaError_t issue_general_stage(ndg_ctx* c, int m, int in) {
+    const dev::GeneralStage a = general_args(c, m, in);
+    cudaError_t err = dev::launch_general_ghosts(a, strict(c), c->stream);
+    const size_t G = c->groups.size();
+    if (err != cudaSuccess || G == 0) return err;
+    if (G > 1 && (err = cudaEventRecord(c->aux_events[0], c->stream)) != cudaSuccess) return err;
+    for (size_t g = 1; g < G && err == cudaSuccess; ++g) {
+        cudaStream_t st = c->aux_streams[g - 1];
+        if ((err = cudaStreamWaitEvent(st, c->aux_events[0], 0)) != cudaSuccess) break;
+        if ((err = dev::launch_general_group(a, c->groups[g], strict(c), st)) != cudaSuccess) break;
+        err = cudaEventRecord(c->aux_events[g], st);
+    }
+    if (err == cudaSuccess) err = dev::launch_general_group(a, c->groups[0], strict(c), c->stream);
+    for (size_t g = 1; g < G && err == cudaSuccess; ++g) err = cudaStreamWaitEvent(c->stream, c->aux_events[g], 0);
+    return err;
+}
+
 cudaError_t issue_stage(ndg_ctx* c, int m, int in) {
     if (c->general) {
         if (fp32(c)) return cudaErrorNotSupported;  // rejected by require_form before any capture
-        return dev::launch_general_stage(general_args(c, m), c->groups.data(), static_cast<int>(c->groups.size()), strict(c), c->stream);
+        return issue_general_stage(c, m, in);
     }
     if (fp32(c)) {
         if (c->tile[1]) return dev::launch_stage_variant_fp32(c->N, c->tile[1], stage_args(c, m, in), c->stream);
@@ -127,12 +164,8 @@ void require_form(const ndg_ctx* c) {
 void launch_stage(ndg_ctx* c, int m) {
     require_form(c);
     check_cuda(issue_stage(c, m, c->cur), "stage kernel launch");
-    if (c->general) {
-        c->launches += general_stage_launches(c);
-    } else {
-        c->cur = 1 - c->cur;
-        ++c->launches;
-    }
+    c->cur = 1 - c->cur;
+    c->launches += c->general ? general_stage_launches(c) : 1;
 }
 
 // The tile candidates of the context's form (FP64 or FP32).
@@ -153,7 +186,14 @@ void set_tile(ndg_ctx* c, int epb) {
 }
 
 void ensure_traces(ndg_ctx* c) {
-    if (c->traces_valid || c->general) return;
+    if (c->traces_valid) return;
+    if (c->general) {
+        dev::GeneralStage g = general_args(c, 0, c->cur);
+        check_cuda(dev::launch_general_traces(g, c->groups.data(), static_cast<int>(c->groups.size()), strict(c), c->stream), "trace kernel launch");
+        c->launches += static_cast<int64_t>(c->groups.size());
+        c->traces_valid = true;
+        return;
+    }
     dev::TraceArgs a{};
     a.q = c->q.ptr;
     a.trace_out = c->tr[c->cur].ptr;
@@ -186,7 +226,7 @@ void set_step(ndg_ctx* c, double time, double dt, double t_end) {
 // the general path has one.
 void ensure_graphs(ndg_ctx* c) {
     require_form(c);
-    const int n_graphs = c->general ? 1 : 2;
+    const int n_graphs = 2;
     if (c->graph[0] && (n_graphs == 1 || c->graph[1])) return;
     for (int parity = 0; parity < n_graphs; ++parity) {
         cudaGraph_t g = nullptr;
@@ -208,15 +248,11 @@ void ensure_graphs(ndg_ctx* c) {
 void run_steps(ndg_ctx* c, int64_t n_steps) {
     ensure_traces(c);
     ensure_graphs(c);
+    const int64_t per_step = 3 * (c->general ? general_stage_launches(c) : 1) + 1;
     for (int64_t s = 0; s < n_steps; ++s) {
-        if (c->general) {
-            check_cuda(cudaGraphLaunch(c->graph[0], c->stream), "graph launch");
-            c->launches += 3 * general_stage_launches(c) + 1;
-        } else {
-            check_cuda(cudaGraphLaunch(c->graph[c->cur], c->stream), "graph launch");
-            c->cur = 1 - c->cur;  // three stages flip the trace buffer an odd number of times
-            c->launches += 4;
-        }
+        check_cuda(cudaGraphLaunch(c->graph[c->cur], c->stream), "graph launch");
+        c->cur = 1 - c->cur;  // three stages flip the trace buffer an odd number of times
+        c->launches += per_step;
     }
 }
 
@@ -337,6 +373,8 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_gscale.upload(g.gscale, c->stream);
         c->g_gsrc.upload(g.gsrc, c->stream);
         c->g_gsrc_side.upload(g.gsrc_side, c->stream);
+        c->g_fbase.upload(g.fbase, c->stream);
+        c->g_fsN.upload(g.fsN, c->stream);
         c->g_sw_off.upload(g.sw_off, c->stream);
         c->g_sm_off.upload(g.sm_off, c->stream);
         c->g_fw_off.upload(g.fw_off, c->stream);
@@ -357,10 +395,14 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
             og.ids = c->g_ids.ptr + at;
             at += og.count;
             c->groups.push_back(og);
-            check_cuda(dev::prepare_general_kernels(og.N), "kernel attributes");
+            check_cuda(dev::prepare_general_kernels(og.N, g.side_slots), "kernel attributes");
         }
-        c->etr.allocate(inst * 3 * static_cast<size_t>(g.trace_total));
-        c->ffl.allocate(inst * 3 * static_cast<size_t>(std::max<int64_t>(g.face_total, 1)));
+        c->getr[0].allocate(inst * 3 * static_cast<size_t>(g.trace_total));
+        c->getr[1].allocate(inst * 3 * static_cast<size_t>(g.trace_total));
+        check_cuda(cudaMemsetAsync(c->getr[0].ptr, 0, c->getr[0].count * sizeof(double), c->stream), "memset");
+        check_cuda(cudaMemsetAsync(c->getr[1].ptr, 0, c->getr[1].count * sizeof(double), c->stream), "memset");
+        c->side_slots = static_cast<int>(g.side_slots);
+        ensure_aux_streams(c);
         dev::GeneralMesh& M = c->gmesh;
         M = dev::GeneralMesh{};
         M.n_domain = g.n_domain;
@@ -393,6 +435,8 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.gscale = c->g_gscale.ptr;
         M.gsrc = c->g_gsrc.ptr;
         M.gsrc_side = c->g_gsrc_side.ptr;
+        M.fbase = c->g_fbase.ptr;
+        M.fsN = c->g_fsN.ptr;
         M.sw_off = c->g_sw_off.ptr;
         M.sm_off = c->g_sm_off.ptr;
         M.fw_off = c->g_fw_off.ptr;
@@ -876,7 +920,7 @@ ndg_status ndg_initial_conditions(ndg_ctx* ctx) {
         require_device(ctx);
         make_current(ctx);
         if (ctx->general) {
-            check_cuda(dev::launch_general_initial_conditions(general_args(ctx, 0), ctx->groups.data(), static_cast<int>(ctx->groups.size()), ctx->stream),
+            check_cuda(dev::launch_general_initial_conditions(general_args(ctx, 0, ctx->cur), ctx->groups.data(), static_cast<int>(ctx->groups.size()), ctx->stream),
                        "initial condition kernel");
             ctx->launches += static_cast<int64_t>(ctx->groups.size());
         } else {

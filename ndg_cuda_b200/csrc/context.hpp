@@ -96,13 +96,20 @@ struct ndg_ctx {
     ndg::GeneralPlan gplan;
     ndg::DeviceBuffer<int32_t> g_eN, g_fN, g_gkind, g_gsrc_side;
     ndg::DeviceBuffer<int64_t> g_off2, g_off1, g_enodes, g_sface_start, g_sface, g_foff, g_fnodes, g_felem, g_fside, g_gsrc, g_ids;
-    ndg::DeviceBuffer<double> g_corners, g_node_xy, g_fnormal, g_ftangent, g_foffset, g_fscale, g_gscale, etr, ffl;
-    ndg::DeviceBuffer<int64_t> g_sw_off, g_sm_off, g_fw_off, g_fm_off;  // mortar weight offsets
+    ndg::DeviceBuffer<double> g_corners, g_node_xy, g_fnormal, g_ftangent, g_foffset, g_fscale, g_gscale;
+    ndg::DeviceBuffer<double> getr[2];  // element side traces, double-buffered between stages
+    int side_slots = 1;                 // largest sum of (face order + 1) over one element side
+    ndg::DeviceBuffer<int64_t> g_sw_off, g_sm_off, g_fw_off, g_fm_off, g_fbase;  // mortar weight offsets, face-side trace bases
+    ndg::DeviceBuffer<int32_t> g_fsN;                                            // face-side element orders
     ndg::DeviceBuffer<double> g_sw, g_fw;                              // mortar weights
     ndg::DeviceBuffer<int32_t> g_smatch, g_fmatch;                     // mortar node matches
     std::vector<ndg::dev::OrderGroup> groups;
     ndg::dev::GeneralMesh gmesh;
 
+    // Streams and events on which the order groups of a mixed-order stage
+    // run concurrently (forked from and joined to `stream`).
+    std::vector<cudaStream_t> aux_streams;
+    std::vector<cudaEvent_t> aux_events;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t launches = 0;
     // Incremented whenever the topology or its device plan changes (load,
@@ -115,6 +122,8 @@ struct ndg_ctx {
     ~ndg_ctx() {
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
+        for (auto& e : aux_events) cudaEventDestroy(e);
+        for (auto& st : aux_streams) cudaStreamDestroy(st);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };

@@ -1,22 +1,27 @@
 // Stage kernels for mixed-order meshes with nonconforming faces (sm_100a).
 //
 // After adaptation elements differ in order and faces carry mortar offsets
-// and scales, so the stage runs in the reference's own steps
-// (include/solvers/Solver2D_t.tcu:46-70), each a kernel over device arrays:
+// and scales. A stage (include/solvers/Solver2D_t.tcu:46-70) is two kinds of
+// launch over device arrays, with the element side traces double-buffered
+// between stages:
 //
-//   side traces    every domain element side, order-templated per group
-//                  (Element2D_t::interpolate_to_boundaries, Element2D_t.cpp:86-125)
 //   ghost traces   walls, symmetry planes, outflow: the neighbours' traces
 //                  projected onto the ghost; inflow: the plane wave; periodic
 //                  interfaces: the origin's side trace
 //                  (Mesh2D_t.cpp:4298-4730)
-//   face fluxes    both traces brought to the face order (copy when conforming,
-//                  barycentric interpolation otherwise), then the upwind flux
-//                  (Mesh2D_t.cpp:3803-3893, Solver2D_t.cpp:48-63)
-//   volume         per order group: the element's side fluxes gathered from
-//                  its faces (mortar projection, Mesh2D_t.cpp:3895-4006), the
-//                  derivative (Solver2D_t.cpp:66-136) and the RK3 update
-//                  (Solver2D_t.cpp:138-172), one CTA per tile of elements
+//   fused stage    per order group, one CTA per tile of elements: the face
+//                  fluxes of the elements' sides (both traces brought to the
+//                  face order, copy when conforming, interpolation otherwise;
+//                  upwind flux; Mesh2D_t.cpp:3803-3893, Solver2D_t.cpp:48-63),
+//                  the element side fluxes (mortar projection,
+//                  Mesh2D_t.cpp:3895-4006), the derivative
+//                  (Solver2D_t.cpp:66-136), the RK3 update
+//                  (Solver2D_t.cpp:138-172) and the side traces of the new
+//                  state for the next stage (Element2D_t.cpp:86-125)
+//
+// The mortar weights of the plan are computed once (side_weights_kernel,
+// face_weights_kernel). A face's flux is evaluated by each of its two
+// elements, with the same operations, so both see the same value.
 //
 // STRICT instantiations round every operation in the reference's order and
 // reproduce its CPU results bit for bit; node matching (almost_equal) is
@@ -198,73 +203,6 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
     }
 }
 
-// Face fluxes: thread per (instance, face, face node).
-template <bool S>
-__global__ void __launch_bounds__(256) general_faces_kernel(GeneralStage a, int max_n) {
-    const GeneralMesh& M = a.m;
-    const int64_t ft = M.trace_total, ff = M.face_total;
-    const int64_t per_inst = M.n_faces * max_n;
-    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < per_inst * a.n_instances;
-         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t inst = idx / per_inst;
-        const int64_t r = idx - inst * per_inst;
-        const int64_t f = r / max_n;
-        const int i = static_cast<int>(r - f * max_n);
-        const int Nf = M.fN[f];
-        if (i > Nf) continue;
-        const double* xf = g_nodes + gvec(Nf);
-        const double* tr = a.etr + inst * 3 * ft;
-        double val[2][3];
-        for (int side = 0; side < 2; ++side) {
-            const int64_t e = M.felem[2 * f + side];
-            const int64_t es = M.fside[2 * f + side];
-            const int Ne = M.eN[e];
-            const double* ep = tr + M.off1[e] + es * (Ne + 1);
-            const int64_t en0 = M.enodes[4 * e + es];
-            const int64_t en1 = M.enodes[4 * e + ((es + 1) & 3)];
-            const bool conforming = side == 0 ? (Nf == Ne && M.fnodes[2 * f] == en0 && M.fnodes[2 * f + 1] == en1)
-                                              : (Nf == Ne && M.fnodes[2 * f + 1] == en0 && M.fnodes[2 * f] == en1);
-            if (conforming) {
-                const int src = side == 0 ? i : Nf - i;
-                val[side][0] = ep[src];
-                val[side][1] = ep[src + ft];
-                val[side][2] = ep[src + 2 * ft];
-            } else {
-                // Interpolation to the face node with the plan's weights
-                // (face_weights_kernel): a matching element node is copied.
-                const int match = M.fmatch[M.fm_off[2 * f + side] + i];
-                if (match >= 0) {
-                    val[side][0] = ep[match];
-                    val[side][1] = ep[match + ft];
-                    val[side][2] = ep[match + 2 * ft];
-                } else {
-                    const double* tw = M.fw + M.fw_off[2 * f + side];
-                    const double* tj = tw + i * (Ne + 1);
-                    const double den = tw[(Nf + 1) * (Ne + 1) + i];
-                    double pn = 0.0, un = 0.0, vn = 0.0;
-                    for (int j = 0; j <= Ne; ++j) {
-                        pn = madd<S>(pn, tj[j], ep[j]);
-                        un = madd<S>(un, tj[j], ep[j + ft]);
-                        vn = madd<S>(vn, tj[j], ep[j + 2 * ft]);
-                    }
-                    val[side][0] = S ? __ddiv_rn(pn, den) : pn / den;
-                    val[side][1] = S ? __ddiv_rn(un, den) : un / den;
-                    val[side][2] = S ? __ddiv_rn(vn, den) : vn / den;
-                }
-            }
-        }
-        // Upwind flux with c = 1 (Solver2D_t.cpp:48-63).
-        const double nx = M.fnormal[2 * f], ny = M.fnormal[2 * f + 1];
-        const double wL = add<S>(val[0][0], add<S>(mul<S>(val[0][1], nx), mul<S>(val[0][2], ny)));
-        const double wR = sub<S>(val[1][0], add<S>(mul<S>(val[1][1], nx), mul<S>(val[1][2], ny)));
-        const double sum = add<S>(wL, wR);
-        double* out = a.ffl + inst * 3 * ff + M.foff[f] + i;
-        out[0] = mul<S>(sub<S>(wL, wR), 0.5);
-        out[ff] = mul<S>(mul<S>(nx, sum), 0.5);
-        out[2 * ff] = mul<S>(mul<S>(ny, sum), 0.5);
-    }
-}
-
 // Mortar weights of the element sides (Mesh2D_t.cpp:3895-4006, the
 // multi-face branch): per face node j the element node it matches
 // (almost_equal) or -1, and the weight of every element node i,
@@ -370,81 +308,71 @@ cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch
 namespace {
 
 // ---------------------------------------------------------------------------
-// Volume kernel tiles: EPB elements of one order per CTA, one thread per
-// (field, element, line) as in the uniform kernel.
+// Fused stage of one order group: the face fluxes of the elements' sides,
+// the derivative, the RK3 update and the new side traces, one CTA per tile
+// of EPB elements of the group, one thread per (field, element, line) in the
+// derivative as in the uniform kernel. Face values come from the side traces
+// of the stage's input (etr: the previous stage's output, and the ghost
+// traces of general_ghosts_kernel); the new traces go to etr_out. Every value
+// is computed with the operations, in the order, of the reference's separate
+// steps, so strict instantiations stay bit-identical to its CPU path.
+
+// Values of the three fields at face node i of side `side` of face f
+// (Mesh2D_t::project_to_faces, Mesh2D_t.cpp:3803-3893): a copy where the
+// element side matches the face, the plan's interpolation otherwise.
+template <bool S>
+__device__ __forceinline__ void face_value(const GeneralMesh& M, const double* __restrict__ tr, int64_t ft, int64_t f, int Nf, int side, int i, double v[3]) {
+    const int Ne = M.fsN[2 * f + side];
+    const double* ep = tr + M.fbase[2 * f + side];
+    if (M.fw_off[2 * f + side] < 0) {
+        const int src = side == 0 ? i : Nf - i;
+        v[0] = ep[src];
+        v[1] = ep[src + ft];
+        v[2] = ep[src + 2 * ft];
+        return;
+    }
+    const int match = M.fmatch[M.fm_off[2 * f + side] + i];
+    if (match >= 0) {
+        v[0] = ep[match];
+        v[1] = ep[match + ft];
+        v[2] = ep[match + 2 * ft];
+        return;
+    }
+    const double* tw = M.fw + M.fw_off[2 * f + side];
+    const double* tj = tw + i * (Ne + 1);
+    const double den = tw[(Nf + 1) * (Ne + 1) + i];
+    double pn = 0.0, un = 0.0, vn = 0.0;
+    for (int j = 0; j <= Ne; ++j) {
+        pn = madd<S>(pn, tj[j], ep[j]);
+        un = madd<S>(un, tj[j], ep[j + ft]);
+        vn = madd<S>(vn, tj[j], ep[j + 2 * ft]);
+    }
+    v[0] = S ? __ddiv_rn(pn, den) : pn / den;
+    v[1] = S ? __ddiv_rn(un, den) : un / den;
+    v[2] = S ? __ddiv_rn(vn, den) : vn / den;
+}
+
 template <int N>
-struct GenTile {
+struct FusedTile {
     static constexpr int n = N + 1;
     static constexpr int NN = n * n;
     static constexpr int raw = 256 / (3 * n);
     static constexpr int EPB = raw >= 1 ? raw : 1;
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
-    static constexpr int kQ = 0;                        // [3][EPB][NN] q
+    static constexpr int kQ = 0;                        // [3][EPB][NN] q, then the new q
     static constexpr int kG = kQ + 3 * EPB * NN;        // [3][EPB][NN] G
     static constexpr int kF = kG + 3 * EPB * NN;        // [3][EPB][4][n] element side fluxes
     static constexpr int kJ = kF + 3 * EPB * 4 * n;     // [EPB][NN] J (1/J in the default mode)
     static constexpr int kS = kJ + EPB * NN;            // [EPB][4] edge metric per side
-    static constexpr int kDoubles = kS + EPB * 4;
-    static constexpr size_t kBytes = sizeof(double) * kDoubles;
+    static constexpr int kSp = kS + EPB * 4;            // [4 EPB + 1] prefix sums of the sides' slot counts (ints, in 2 EPB + 1 doubles)
+    static constexpr int kOff = kSp + 2 * EPB + 1;      // [EPB] element id, [EPB] field offset, [EPB] trace offset (int64)
+    static constexpr int kFF = kOff + 3 * EPB;          // [3][EPB][4][slots] face fluxes at the side's face nodes
+    static constexpr size_t bytes(int slots) { return sizeof(double) * (kFF + 3 * EPB * 4 * slots); }
 };
 
-// Element side flux of node i of side s of element e (Mesh2D_t.cpp:3895-4006):
-// the face flux times the edge metric when one face of the same order
-// covers the side (reversed and negated for the face's right element),
-// otherwise the mortar projection of every face on the side.
-template <bool S>
-__device__ __forceinline__ void element_side_flux(const GeneralStage& a, const double* __restrict__ ffl, int64_t e, int s, int i, int N,
-                                                  double sfv, double out[3]) {
-    const GeneralMesh& M = a.m;
-    const int64_t ff = M.face_total;
-    const int64_t q0 = M.sface_start[4 * e + s], q1 = M.sface_start[4 * e + s + 1];
-    if (q1 == q0) {
-        out[0] = out[1] = out[2] = 0.0;
-        return;
-    }
-    const int64_t f0 = M.sface[q0];
-    const int64_t en0 = M.enodes[4 * e + s], en1 = M.enodes[4 * e + ((s + 1) & 3)];
-    if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0] == en0 && M.fnodes[2 * f0 + 1] == en1) {
-        const double* fl = ffl + M.foff[f0] + i;
-        out[0] = mul<S>(fl[0], sfv);
-        out[1] = mul<S>(fl[ff], sfv);
-        out[2] = mul<S>(fl[2 * ff], sfv);
-        return;
-    }
-    if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0 + 1] == en0 && M.fnodes[2 * f0] == en1) {
-        const double* fl = ffl + M.foff[f0] + (N - i);
-        out[0] = mul<S>(-fl[0], sfv);
-        out[1] = mul<S>(-fl[ff], sfv);
-        out[2] = mul<S>(-fl[2 * ff], sfv);
-        return;
-    }
-    // Mortar projection with the plan's weights (side_weights_kernel): a
-    // face node that matches an element node feeds that node only.
-    double acc[3] = {0.0, 0.0, 0.0};
-    for (int64_t q = q0; q < q1; ++q) {
-        const int64_t f = M.sface[q];
-        const int Nf = M.fN[f];
-        const int fs = e == M.felem[2 * f] ? 0 : 1;
-        const double scale = M.fscale[2 * f + fs];
-        const double* W = M.sw + M.sw_off[q] + i * (Nf + 1);
-        const int* match = M.smatch + M.sm_off[q];
-        for (int j = 0; j <= Nf; ++j) {
-            const int mt = match[j];
-            if (mt >= 0 && mt != i) continue;
-            const double w = W[j];
-            const double* fl = ffl + M.foff[f] + j;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) acc[c] = add<S>(acc[c], mul<S>(mul<S>(mul<S>(w, fl[c * ff]), sfv), scale));
-        }
-    }
-    out[0] = acc[0];
-    out[1] = acc[1];
-    out[2] = acc[2];
-}
-
 template <int N, bool S>
-__global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
-    using T = GenTile<N>;
+__global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
+    using T = FusedTile<N>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     extern __shared__ __align__(128) double smem[];
     double* qs = smem + T::kQ;
@@ -452,26 +380,90 @@ __global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(Ge
     double* fs = smem + T::kF;
     double* js = smem + T::kJ;
     double* ss = smem + T::kS;
+    double* ffs = smem + T::kFF;
+    int* sps = reinterpret_cast<int*>(smem + T::kSp);
+    int64_t* eid = reinterpret_cast<int64_t*>(smem + T::kOff);  // element numbers of the tile
+    int64_t* eo2 = eid + EPB;                                    // their first value in a field block
+    int64_t* eo1 = eo2 + EPB;                                    // their first side-trace value
     constexpr int FS = EPB * 4 * n;
+    const int SL = a.side_slots;
+    const int FFS = EPB * 4 * SL;
     const GeneralMesh& M = a.m;
     const int tid = threadIdx.x;
     const int64_t base = static_cast<int64_t>(blockIdx.x) * EPB;
     const int ne = static_cast<int>((count - base) < EPB ? (count - base) : EPB);
     const int64_t inst = blockIdx.y;
-    const int64_t fb = M.block;
+    const int64_t fb = M.block, ft = M.trace_total;
     double* q = a.q + inst * 3 * fb;
     double* k = a.k + inst * 3 * fb;
-    const double* ffl = a.ffl + inst * 3 * M.face_total;
+    const double* tr = a.etr + inst * 3 * ft;
+    double* tr_out = a.etr_out + inst * 3 * ft;
     const double* xn = g_nodes + gvec(N);
     const double* lm = g_lagrange_left + gvec(N);
     const double* lp = g_lagrange_right + gvec(N);
     const double dt = a.step[1];
 
+    if (tid < ne) {
+        const int64_t el = ids[base + tid];
+        eid[tid] = el;
+        eo2[tid] = M.off2[el];
+        eo1[tid] = M.off1[el];
+    }
+    __syncthreads();
     // q tile: coalesced within each element's blocks.
     for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
         const int f = idx / (ne * NN), r = idx - f * (ne * NN);
         const int e = r / NN, node = r - e * NN;
-        qs[(f * EPB + e) * NN + node] = q[f * fb + M.off2[ids[base + e]] + node];
+        qs[(f * EPB + e) * NN + node] = q[f * fb + eo2[e] + node];
+    }
+    // Face fluxes at every face node of every side (Mesh2D_t.cpp:3803-3893,
+    // Solver2D_t.cpp:48-63): the tile's sides' slot counts (the sum of face
+    // order + 1 over a side's faces) and their prefix sums first, then one
+    // item per (element, side, slot), the slots of a side running over its
+    // faces' nodes in face-list order.
+    for (int idx = tid; idx < ne * 4; idx += T::kThreads) {
+        const int64_t e = eid[idx / 4];
+        const int s = idx & 3;
+        int cnt = 0;
+        for (int64_t q = M.sface_start[4 * e + s]; q < M.sface_start[4 * e + s + 1]; ++q) cnt += M.fN[M.sface[q]] + 1;
+        sps[idx + 1] = cnt;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        sps[0] = 0;
+        for (int i = 1; i <= ne * 4; ++i) sps[i] += sps[i - 1];
+    }
+    __syncthreads();
+    const int n_items = sps[ne * 4];
+    for (int idx = tid; idx < n_items; idx += T::kThreads) {
+        int lo = 0, hi = ne * 4;  // the side holding item idx: sps[lo] <= idx < sps[lo + 1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (sps[mid] <= idx) lo = mid;
+            else hi = mid;
+        }
+        const int ee = lo >> 2, s = lo & 3, slot = idx - sps[lo];
+        const int64_t e = eid[ee];
+        int64_t q = M.sface_start[4 * e + s];
+        int64_t f = M.sface[q];
+        int Nf = M.fN[f];
+        int j = slot;
+        while (j > Nf) {
+            j -= Nf + 1;
+            f = M.sface[++q];
+            Nf = M.fN[f];
+        }
+        double L[3], R[3];
+        face_value<S>(M, tr, ft, f, Nf, 0, j, L);
+        face_value<S>(M, tr, ft, f, Nf, 1, j, R);
+        const double nx = M.fnormal[2 * f], ny = M.fnormal[2 * f + 1];
+        const double wL = add<S>(L[0], add<S>(mul<S>(L[1], nx), mul<S>(L[2], ny)));
+        const double wR = sub<S>(R[0], add<S>(mul<S>(R[1], nx), mul<S>(R[2], ny)));
+        const double sum = add<S>(wL, wR);
+        double* o = ffs + (ee * 4 + s) * SL + slot;
+        o[0] = mul<S>(sub<S>(wL, wR), 0.5);
+        o[FFS] = mul<S>(mul<S>(nx, sum), 0.5);
+        o[2 * FFS] = mul<S>(mul<S>(ny, sum), 0.5);
     }
 
     const int f = tid / (EPB * n);
@@ -479,7 +471,7 @@ __global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(Ge
     const int e = rr / n;
     const int m = rr - e * n;
     const bool active = f < 3 && e < ne;
-    const int64_t ge = active ? ids[base + e] : 0;
+    const int64_t ge = active ? eid[e] : 0;
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
         const double* c = M.corners + 8 * ge;
@@ -504,14 +496,47 @@ __global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(Ge
             js[e * NN + m * n + j] = S ? jac : __drcp_rn(jac);
         }
     }
-    __syncthreads();  // q tile, J, edge metrics
+    __syncthreads();  // q tile, face fluxes, J, edge metrics
 
-    // Element side fluxes: item (element, side, node), three fields each.
+    // Element side fluxes (Mesh2D_t::project_to_elements, Mesh2D_t.cpp:3895-4006):
+    // the face flux times the edge metric where one face of the element's
+    // order covers the side (reversed and negated for the face's right
+    // element), otherwise the mortar projection with the plan's weights.
     for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
         const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
         const int s = sm / n, i = sm - s * n;
-        double out[3];
-        element_side_flux<S>(a, ffl, ids[base + ee], s, i, N, ss[ee * 4 + s], out);
+        const int64_t el = eid[ee];
+        const int64_t q0 = M.sface_start[4 * el + s], q1 = M.sface_start[4 * el + s + 1];
+        const double sfv = ss[ee * 4 + s];
+        const double* fl = ffs + (ee * 4 + s) * SL;
+        double out[3] = {0.0, 0.0, 0.0};
+        if (q1 > q0) {
+            const int64_t f0 = M.sface[q0];
+            const int64_t en0 = M.enodes[4 * el + s], en1 = M.enodes[4 * el + ((s + 1) & 3)];
+            if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0] == en0 && M.fnodes[2 * f0 + 1] == en1) {
+                for (int c = 0; c < 3; ++c) out[c] = mul<S>(fl[c * FFS + i], sfv);
+            } else if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0 + 1] == en0 && M.fnodes[2 * f0] == en1) {
+                for (int c = 0; c < 3; ++c) out[c] = mul<S>(-fl[c * FFS + (N - i)], sfv);
+            } else {
+                int slot0 = 0;
+                for (int64_t qq = q0; qq < q1; ++qq) {
+                    const int64_t ff = M.sface[qq];
+                    const int Nf = M.fN[ff];
+                    const int fsd = el == M.felem[2 * ff] ? 0 : 1;
+                    const double scale = M.fscale[2 * ff + fsd];
+                    const double* W = M.sw + M.sw_off[qq] + i * (Nf + 1);
+                    const int* match = M.smatch + M.sm_off[qq];
+                    for (int j = 0; j <= Nf; ++j) {
+                        const int mt = match[j];
+                        if (mt >= 0 && mt != i) continue;
+                        const double w = W[j];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) out[c] = add<S>(out[c], mul<S>(mul<S>(mul<S>(w, fl[c * FFS + slot0 + j]), sfv), scale));
+                    }
+                    slot0 += Nf + 1;
+                }
+            }
+        }
         fs[0 * FS + idx] = out[0];
         fs[1 * FS + idx] = out[1];
         fs[2 * FS + idx] = out[2];
@@ -562,7 +587,7 @@ __global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(Ge
             else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), P[j]);
             else line[j] = mul<S>(x_xi(xn[j]), P[j]);
         }
-        const double ft = F[2 * n + (N - i)], fbm = F[0 * n + i];
+        const double ftp = F[2 * n + (N - i)], fbm = F[0 * n + i];
         double* G = gs + (f * EPB + e) * NN + i * n;
         const double* jrow = js + e * NN + i * n;
 #pragma unroll
@@ -570,7 +595,7 @@ __global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(Ge
             double acc = 0.0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[j * n + mm], line[mm]);
-            const double lift = S ? __ddiv_rn(add<S>(mul<S>(ft, lp[j]), mul<S>(fbm, lm[j])), w[j]) : (ft * lp[j] + fbm * lm[j]) * iw[j];
+            const double lift = S ? __ddiv_rn(add<S>(mul<S>(ftp, lp[j]), mul<S>(fbm, lm[j])), w[j]) : (ftp * lp[j] + fbm * lm[j]) * iw[j];
             const double num = sub<S>(G[j], add<S>(acc, lift));
             G[j] = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
         }
@@ -582,12 +607,35 @@ __global__ void __launch_bounds__(GenTile<N>::kThreads) general_volume_kernel(Ge
     for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
         const int ff = idx / (ne * NN), r = idx - ff * (ne * NN);
         const int ee = r / NN, node = r - ee * NN;
-        const int64_t gi = ff * fb + M.off2[ids[base + ee]] + node;
+        const int64_t gi = ff * fb + eo2[ee] + node;
         const double G = gs[(ff * EPB + ee) * NN + node];
         const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, k[gi]), G);
+        const double qn = add<S>(qs[(ff * EPB + ee) * NN + node], mul<S>(gdt, kn));
         k[gi] = kn;
-        q[gi] = add<S>(qs[(ff * EPB + ee) * NN + node], mul<S>(gdt, kn));
+        q[gi] = qn;
+        qs[(ff * EPB + ee) * NN + node] = qn;
         if (a.G_out) a.G_out[inst * 3 * fb + gi] = G;
+    }
+    __syncthreads();
+
+    // Side traces of the new q for the next stage (Element2D_t.cpp:86-125):
+    // item (element, side, node), three fields each.
+    for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
+        const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
+        const int s = sm / n, mm = sm - s * n;
+        const double* l = (s == 0 || s == 3) ? lm : lp;
+        const int line = (s < 2) ? mm : N - mm;
+        const int b0 = (s == 0 || s == 2) ? line * n : line;
+        const int stride = (s == 0 || s == 2) ? 1 : n;
+        double* out = tr_out + eo1[ee] + s * n + mm;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double* qe = qs + (c * EPB + ee) * NN + b0;
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], qe[j * stride]);
+            out[c * ft] = acc;
+        }
     }
 }
 
@@ -707,25 +755,25 @@ int grid_for(int64_t items, int threads) {
 }
 
 template <int N, bool S>
-cudaError_t launch_group(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
-    using T = GenTile<N>;
+cudaError_t launch_group_traces(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
     general_traces_kernel<N, S><<<grid_for(g.count * 4 * (N + 1) * a.n_instances, 256), 256, 0, stream>>>(a, g.ids, g.count);
     return cudaGetLastError();
 }
 
 template <int N, bool S>
-cudaError_t launch_volume(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
-    using T = GenTile<N>;
+cudaError_t launch_fused(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
+    using T = FusedTile<N>;
     const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
-    general_volume_kernel<N, S><<<grid, T::kThreads, T::kBytes, stream>>>(a, g.ids, g.count);
+    general_fused_kernel<N, S><<<grid, T::kThreads, T::bytes(a.side_slots), stream>>>(a, g.ids, g.count);
     return cudaGetLastError();
 }
 
 template <int N>
-cudaError_t set_attrs() {
-    cudaError_t err = cudaFuncSetAttribute(general_volume_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(GenTile<N>::kBytes));
+cudaError_t set_attrs(int side_slots) {
+    const int bytes = static_cast<int>(FusedTile<N>::bytes(side_slots));
+    cudaError_t err = cudaFuncSetAttribute(general_fused_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (err != cudaSuccess) return err;
-    return cudaFuncSetAttribute(general_volume_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(GenTile<N>::kBytes));
+    return cudaFuncSetAttribute(general_fused_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 template <int N>
@@ -787,40 +835,36 @@ cudaError_t upload_general_tables(const Tables& t) {
     return cudaMemcpyToSymbol(g_dhat, dhat.data(), sizeof(double) * kGMatTotal);
 }
 
-cudaError_t prepare_general_kernels(int N) {
-    return by_order(N, [](auto c) { return set_attrs<decltype(c)::value>(); });
+cudaError_t prepare_general_kernels(int N, int side_slots) {
+    return by_order(N, [&](auto c) { return set_attrs<decltype(c)::value>(side_slots); });
 }
 
-cudaError_t launch_general_stage(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream) {
+cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream) {
     cudaError_t err = cudaSuccess;
-    const int max_n = a.m.max_n;
     for (int g = 0; g < n_groups && err == cudaSuccess; ++g) {
         if (groups[g].count == 0) continue;
         err = by_order(groups[g].N, [&](auto c) {
             constexpr int N = decltype(c)::value;
-            return strict ? launch_group<N, true>(a, groups[g], stream) : launch_group<N, false>(a, groups[g], stream);
-        });
-    }
-    if (err != cudaSuccess) return err;
-    const int64_t n_ghosts = a.m.n_total - a.m.n_domain;
-    if (n_ghosts > 0) {
-        if (strict) general_ghosts_kernel<true><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
-        else general_ghosts_kernel<false><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
-        if ((err = cudaGetLastError()) != cudaSuccess) return err;
-    }
-    // max_n covers the largest face order.
-    const int64_t face_items = a.m.n_faces * max_n * a.n_instances;
-    if (strict) general_faces_kernel<true><<<grid_for(face_items, 256), 256, 0, stream>>>(a, max_n);
-    else general_faces_kernel<false><<<grid_for(face_items, 256), 256, 0, stream>>>(a, max_n);
-    if ((err = cudaGetLastError()) != cudaSuccess) return err;
-    for (int g = 0; g < n_groups && err == cudaSuccess; ++g) {
-        if (groups[g].count == 0) continue;
-        err = by_order(groups[g].N, [&](auto c) {
-            constexpr int N = decltype(c)::value;
-            return strict ? launch_volume<N, true>(a, groups[g], stream) : launch_volume<N, false>(a, groups[g], stream);
+            return strict ? launch_group_traces<N, true>(a, groups[g], stream) : launch_group_traces<N, false>(a, groups[g], stream);
         });
     }
     return err;
+}
+
+cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, cudaStream_t stream) {
+    const int64_t n_ghosts = a.m.n_total - a.m.n_domain;
+    if (n_ghosts == 0) return cudaSuccess;
+    if (strict) general_ghosts_kernel<true><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
+    else general_ghosts_kernel<false><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, cudaStream_t stream) {
+    if (g.count == 0) return cudaSuccess;
+    return by_order(g.N, [&](auto c) {
+        constexpr int N = decltype(c)::value;
+        return strict ? launch_fused<N, true>(a, g, stream) : launch_fused<N, false>(a, g, stream);
+    });
 }
 
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream) {

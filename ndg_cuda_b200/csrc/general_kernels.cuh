@@ -55,6 +55,8 @@ struct GeneralMesh {
     // face node, -1 = barycentric) and face-side interpolations per
     // (face, side) (weights [N_f+1][N_e+1] then N_f+1 denominators, node
     // match per face node); offsets -1 where the fast conforming path runs.
+    const int64_t* fbase = nullptr;     // [2 n_faces] first trace value of each face side's element side
+    const int* fsN = nullptr;           // [2 n_faces] order of each face side's element
     const int64_t* sw_off = nullptr;
     const int64_t* sm_off = nullptr;
     const int64_t* fw_off = nullptr;
@@ -71,8 +73,9 @@ struct GeneralStage {
     double* q = nullptr;      // [instance][field][block]
     double* k = nullptr;
     double* G_out = nullptr;  // optional copy of the stage's time derivative
-    double* etr = nullptr;    // [instance][field][trace_total] element side traces
-    double* ffl = nullptr;    // [instance][field][face_total] face fluxes
+    double* etr = nullptr;      // [instance][field][trace_total] element side traces of q (ghosts filled by the stage)
+    double* etr_out = nullptr;  // the same for the stage's output
+    int side_slots = 1;         // largest sum of (face order + 1) over the faces of one element side
     const double* step = nullptr;  // {time, dt, dt_mesh, t_end}
     double rk_a = 0, rk_b = 0, rk_g = 0;
     int first = 0;
@@ -90,10 +93,15 @@ cudaError_t upload_general_tables(const Tables& t);
 // Fills the mortar weights of a plan (once per plan): the same arithmetic,
 // in the reference's rounding, as the per-node computation they replace.
 cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, cudaStream_t stream);
-cudaError_t prepare_general_kernels(int N);
-// Side traces, ghost traces, face fluxes, then per order group the
-// element fluxes, volume term and RK update.
-cudaError_t launch_general_stage(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream);
+cudaError_t prepare_general_kernels(int N, int side_slots);
+// Side traces of q into etr (before the first stage, or after q changed).
+cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream);
+// One stage is the ghost traces into etr, then for every order group the
+// fused face fluxes, volume term, RK update and traces of the new state
+// into etr_out. The groups read only etr and write disjoint elements, so
+// they may run concurrently after the ghost launch.
+cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, cudaStream_t stream);
+cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, cudaStream_t stream);
 // The plane-wave initial condition at every node of a mixed-order mesh.
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream);
 

@@ -119,6 +119,11 @@ struct GeneralPlan {
     // followed by N_f+1 denominators, and of its N_f+1 node matches.
     std::vector<int64_t> sw_off, sm_off, fw_off, fm_off;
     int64_t sw_total = 0, sm_total = 0, fw_total = 0, fm_total = 0;
+    int64_t side_slots = 1;  // largest sum of (face order + 1) over the faces of one domain element side
+    // per face side (2 per face): first value of the element side's trace
+    // (off1 + side (N_e + 1)) and the element's order
+    std::vector<int64_t> fbase;
+    std::vector<int32_t> fsN;
 };
 GeneralPlan build_general_plan(const Topology& t);
 
