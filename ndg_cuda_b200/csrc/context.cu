@@ -88,6 +88,8 @@ dev::GeneralStage general_args(ndg_ctx* c, int m, int in) {
     a.G_out = c->keep_derivative ? c->G.ptr : nullptr;
     a.etr = c->getr[in].ptr;
     a.etr_out = c->getr[1 - in].ptr;
+    a.etr_f = c->getr32[in].ptr;
+    a.etr_out_f = c->getr32[1 - in].ptr;
     a.side_slots = c->side_slots;
     a.step = c->step.ptr;
     a.rk_a = kRkA[m];
@@ -128,26 +130,23 @@ void ensure_aux_streams(ndg_ctx* c) {
 // the stream) and joined back.
 cudaError_t issue_general_stage(ndg_ctx* c, int m, int in) {
     const dev::GeneralStage a = general_args(c, m, in);
-    cudaError_t err = dev::launch_general_ghosts(a, strict(c), c->stream);
+    cudaError_t err = dev::launch_general_ghosts(a, strict(c), fp32(c), c->stream);
     const size_t G = c->groups.size();
     if (err != cudaSuccess || G == 0) return err;
     if (G > 1 && (err = cudaEventRecord(c->aux_events[0], c->stream)) != cudaSuccess) return err;
     for (size_t g = 1; g < G && err == cudaSuccess; ++g) {
         cudaStream_t st = c->aux_streams[g - 1];
         if ((err = cudaStreamWaitEvent(st, c->aux_events[0], 0)) != cudaSuccess) break;
-        if ((err = dev::launch_general_group(a, c->groups[g], strict(c), st)) != cudaSuccess) break;
+        if ((err = dev::launch_general_group(a, c->groups[g], strict(c), fp32(c), st)) != cudaSuccess) break;
         err = cudaEventRecord(c->aux_events[g], st);
     }
-    if (err == cudaSuccess) err = dev::launch_general_group(a, c->groups[0], strict(c), c->stream);
+    if (err == cudaSuccess) err = dev::launch_general_group(a, c->groups[0], strict(c), fp32(c), c->stream);
     for (size_t g = 1; g < G && err == cudaSuccess; ++g) err = cudaStreamWaitEvent(c->stream, c->aux_events[g], 0);
     return err;
 }
 
 cudaError_t issue_stage(ndg_ctx* c, int m, int in) {
-    if (c->general) {
-        if (fp32(c)) return cudaErrorNotSupported;  // rejected by require_form before any capture
-        return issue_general_stage(c, m, in);
-    }
+    if (c->general) return issue_general_stage(c, m, in);
     if (fp32(c)) {
         if (c->tile[1]) return dev::launch_stage_variant_fp32(c->N, c->tile[1], stage_args(c, m, in), c->stream);
         return dev::launch_stage_f32(c->N, stage_args(c, m, in), c->stream);
@@ -156,9 +155,17 @@ cudaError_t issue_stage(ndg_ctx* c, int m, int in) {
     return dev::launch_stage(c->N, strict(c), stage_args(c, m, in), c->stream);
 }
 
-// The FP32 form runs the uniform-order kernels only.
-void require_form(const ndg_ctx* c) {
-    if (c->general && fp32(c)) fail(NDG_ERR_UNSUPPORTED, "the FP32 form covers meshes of one order; this mesh has been adapted");
+// The FP32 form on a mixed-order mesh allocates its trace buffers the first
+// time it runs (before any capture).
+void require_form(ndg_ctx* c) {
+    if (c->general && fp32(c)) {
+        const size_t count = c->getr[0].count;
+        for (auto& t : c->getr32)
+            if (t.count != count) {
+                t.allocate(count);
+                check_cuda(cudaMemsetAsync(t.ptr, 0, count * sizeof(float), c->stream), "memset");
+            }
+    }
 }
 
 void launch_stage(ndg_ctx* c, int m) {
@@ -188,8 +195,9 @@ void set_tile(ndg_ctx* c, int epb) {
 void ensure_traces(ndg_ctx* c) {
     if (c->traces_valid) return;
     if (c->general) {
+        require_form(c);
         dev::GeneralStage g = general_args(c, 0, c->cur);
-        check_cuda(dev::launch_general_traces(g, c->groups.data(), static_cast<int>(c->groups.size()), strict(c), c->stream), "trace kernel launch");
+        check_cuda(dev::launch_general_traces(g, c->groups.data(), static_cast<int>(c->groups.size()), strict(c), fp32(c), c->stream), "trace kernel launch");
         c->launches += static_cast<int64_t>(c->groups.size());
         c->traces_valid = true;
         return;

@@ -52,6 +52,33 @@ __constant__ double g_bary[kGVecTotal];
 __constant__ double g_lagrange_left[kGVecTotal];
 __constant__ double g_lagrange_right[kGVecTotal];
 __constant__ double g_dhat[kGMatTotal];
+// FP32 copies for the FP32 form
+__constant__ float gf_nodes[kGVecTotal];
+__constant__ float gf_weights[kGVecTotal];
+__constant__ float gf_inv_weights[kGVecTotal];
+__constant__ float gf_lagrange_left[kGVecTotal];
+__constant__ float gf_lagrange_right[kGVecTotal];
+__constant__ float gf_dhat[kGMatTotal];
+
+// The table (or trace buffer) of the arithmetic type R.
+template <typename R>
+__device__ __forceinline__ const R* tab(const double* d, const float* f) {
+    if constexpr (sizeof(R) == 8)
+        return d;
+    else
+        return f;
+}
+template <typename R>
+__device__ __forceinline__ const R* pick(const double* d, const float* f) {
+    return tab<R>(d, f);
+}
+template <typename R>
+__device__ __forceinline__ R* pick(double* d, float* f) {
+    if constexpr (sizeof(R) == 8)
+        return d;
+    else
+        return f;
+}
 
 // Mesh2D_t::almost_equal (src/meshes/Mesh2D_t.cpp:3785-3792): 2 ulp relative,
 // or an absolute difference below DBL_MIN.
@@ -69,13 +96,14 @@ __device__ __forceinline__ double mortar_coord(double xf, double scale, double o
 // ---------------------------------------------------------------------------
 // Side traces of the domain elements of one order group: thread per
 // (element, side, node), three fields each.
-template <int N, bool S>
+template <int N, bool S, typename R>
 __global__ void __launch_bounds__(256) general_traces_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
     constexpr int n = N + 1;
-    const double* lm = g_lagrange_left + gvec(N);
-    const double* lp = g_lagrange_right + gvec(N);
+    const R* lm = tab<R>(g_lagrange_left, gf_lagrange_left) + gvec(N);
+    const R* lp = tab<R>(g_lagrange_right, gf_lagrange_right) + gvec(N);
     const int64_t total = count * 4 * n;
     const int64_t fb = a.m.block, ft = a.m.trace_total;
+    R* etr = pick<R>(a.etr, a.etr_f);
     for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total * a.n_instances;
          idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int64_t inst = idx / total;
@@ -84,24 +112,24 @@ __global__ void __launch_bounds__(256) general_traces_kernel(GeneralStage a, con
         const int sm = static_cast<int>(r - le * 4 * n);
         const int s = sm / n, m = sm - s * n;
         const int64_t e = ids[le];
-        const double* l = (s == 0 || s == 3) ? lm : lp;
+        const R* l = (s == 0 || s == 3) ? lm : lp;
         const int line = (s < 2) ? m : N - m;
         const int base = (s == 0 || s == 2) ? line * n : line;
         const int stride = (s == 0 || s == 2) ? 1 : n;
         const double* q = a.q + inst * 3 * fb + a.m.off2[e] + base;
-        double* out = a.etr + inst * 3 * ft + a.m.off1[e] + s * n + m;
+        R* out = etr + inst * 3 * ft + a.m.off1[e] + s * n + m;
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
-            double acc = 0.0;
+            R acc = 0;
 #pragma unroll
-            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], q[f * fb + j * stride]);
+            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], R(q[f * fb + j * stride]));
             out[f * ft] = acc;
         }
     }
 }
 
 // Ghost traces: thread per (instance, ghost element).
-template <bool S>
+template <bool S, typename R>
 __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
     const GeneralMesh& M = a.m;
     const int64_t n_ghosts = M.n_total - M.n_domain;
@@ -114,17 +142,17 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
         const int64_t ge = M.n_domain + gi;
         const int N = M.eN[ge];
         const double* xe = g_nodes + gvec(N);
-        double* tr = a.etr + inst * 3 * ft;
-        double* gp = tr + M.off1[ge];
-        double* gu = gp + ft;
-        double* gv = gu + ft;
+        R* tr = pick<R>(a.etr, a.etr_f) + inst * 3 * ft;
+        R* gp = tr + M.off1[ge];
+        R* gu = gp + ft;
+        R* gv = gu + ft;
         const int kind = M.gkind[gi];
         if (kind == kGhostMirror || kind == kGhostCopy) {
             // Mesh2D_t.cpp:4366-4434 (multi-face branch) and 4601-4710.
             const double* we = g_weights + gvec(N);
             const double* bwe = g_bary + gvec(N);
-            const double sf = M.gscale[gi];
-            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = 0.0;
+            const R sf = R(M.gscale[gi]);
+            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = R(0);
             for (int64_t q = M.sface_start[4 * ge]; q < M.sface_start[4 * ge + 1]; ++q) {
                 const int64_t f = M.sface[q];
                 const int fs = M.felem[2 * f] == ge ? 1 : 0;
@@ -133,9 +161,9 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
                 const int Nn = M.eN[nb];
                 const double* xnb = g_nodes + gvec(Nn);
                 const double* wnb = g_weights + gvec(Nn);
-                const double* np_ = tr + M.off1[nb] + nbs * (Nn + 1);
-                const double* nu_ = np_ + ft;
-                const double* nv_ = nu_ + ft;
+                const R* np_ = tr + M.off1[nb] + nbs * (Nn + 1);
+                const R* nu_ = np_ + ft;
+                const R* nv_ = nu_ + ft;
                 const double scale = M.fscale[2 * f + fs], offset = M.foffset[2 * f + fs];
                 for (int j = 0; j <= Nn; ++j) {
                     const double coord = mortar_coord(xnb[Nn - j], scale, offset);
@@ -147,7 +175,7 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
                         }
                     if (found >= 0) {
                         const int i = found;
-                        const double w = S ? __ddiv_rn(wnb[j], we[i]) : wnb[j] / we[i];
+                        const R w = R(S ? __ddiv_rn(wnb[j], we[i]) : wnb[j] / we[i]);
                         gp[i] = add<S>(gp[i], mul<S>(mul<S>(w, np_[j]), sf));
                         gu[i] = add<S>(gu[i], mul<S>(mul<S>(w, nu_[j]), sf));
                         gv[i] = add<S>(gv[i], mul<S>(mul<S>(w, nv_[j]), sf));
@@ -156,7 +184,7 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
                         for (int i = 0; i <= N; ++i) s = add<S>(s, S ? __ddiv_rn(bwe[i], __dsub_rn(coord, xe[i])) : bwe[i] / (coord - xe[i]));
                         for (int i = 0; i <= N; ++i) {
                             const double T = S ? __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), s)) : bwe[i] / ((coord - xe[i]) * s);
-                            const double w = S ? __ddiv_rn(__dmul_rn(T, wnb[j]), we[i]) : T * wnb[j] / we[i];
+                            const R w = R(S ? __ddiv_rn(__dmul_rn(T, wnb[j]), we[i]) : T * wnb[j] / we[i]);
                             gp[i] = add<S>(gp[i], mul<S>(mul<S>(w, np_[j]), sf));
                             gu[i] = add<S>(gu[i], mul<S>(mul<S>(w, nu_[j]), sf));
                             gv[i] = add<S>(gv[i], mul<S>(mul<S>(w, nv_[j]), sf));
@@ -166,12 +194,12 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
             }
             if (kind == kGhostMirror && M.sface_start[4 * ge + 1] > M.sface_start[4 * ge]) {
                 const int64_t f = M.sface[M.sface_start[4 * ge]];
-                const double nx = M.fnormal[2 * f], ny = M.fnormal[2 * f + 1];
-                const double tx = M.ftangent[2 * f], ty = M.ftangent[2 * f + 1];
+                const R nx = R(M.fnormal[2 * f]), ny = R(M.fnormal[2 * f + 1]);
+                const R tx = R(M.ftangent[2 * f]), ty = R(M.ftangent[2 * f + 1]);
                 for (int i = 0; i <= N; ++i) {
-                    const double Vx = gu[i], Vy = gv[i];
-                    const double l0 = -add<S>(mul<S>(Vx, nx), mul<S>(Vy, ny));
-                    const double l1 = add<S>(mul<S>(Vx, tx), mul<S>(Vy, ty));
+                    const R Vx = gu[i], Vy = gv[i];
+                    const R l0 = -add<S>(mul<S>(Vx, nx), mul<S>(Vy, ny));
+                    const R l1 = add<S>(mul<S>(Vx, tx), mul<S>(Vy, ty));
                     gu[i] = add<S>(mul<S>(nx, l0), mul<S>(tx, l1));
                     gv[i] = add<S>(mul<S>(ny, l0), mul<S>(ty, l1));
                 }
@@ -185,20 +213,24 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
                 const double r = __dmul_rn(__dadd_rn(xe[i], 1.0), 0.5);
                 const double gx = __dadd_rn(__dmul_rn(p1x, r), __dmul_rn(p0x, __dsub_rn(1.0, r)));
                 const double gy = __dadd_rn(__dmul_rn(p1y, r), __dmul_rn(p0y, __dsub_rn(1.0, r)));
-                plane_wave(gx, gy, t, gp[i], gu[i], gv[i]);
+                double pw, uw, vw;
+                plane_wave(gx, gy, t, pw, uw, vw);
+                gp[i] = R(pw);
+                gu[i] = R(uw);
+                gv[i] = R(vw);
             }
         } else if (kind == kGhostInterface) {
             // Mesh2D_t.cpp:4712-4730.
             const int64_t src = M.gsrc[gi];
             const int Ns = M.eN[src];
-            const double* sp = tr + M.off1[src] + M.gsrc_side[gi] * (Ns + 1);
+            const R* sp = tr + M.off1[src] + M.gsrc_side[gi] * (Ns + 1);
             for (int i = 0; i <= Ns && i <= N; ++i) {
                 gp[i] = sp[i];
                 gu[i] = sp[i + ft];
                 gv[i] = sp[i + 2 * ft];
             }
         } else {
-            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = 0.0;
+            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = R(0);
         }
     }
 }
@@ -320,10 +352,10 @@ namespace {
 // Values of the three fields at face node i of side `side` of face f
 // (Mesh2D_t::project_to_faces, Mesh2D_t.cpp:3803-3893): a copy where the
 // element side matches the face, the plan's interpolation otherwise.
-template <bool S>
-__device__ __forceinline__ void face_value(const GeneralMesh& M, const double* __restrict__ tr, int64_t ft, int64_t f, int Nf, int side, int i, double v[3]) {
+template <bool S, typename R>
+__device__ __forceinline__ void face_value(const GeneralMesh& M, const R* __restrict__ tr, int64_t ft, int64_t f, int Nf, int side, int i, R v[3]) {
     const int Ne = M.fsN[2 * f + side];
-    const double* ep = tr + M.fbase[2 * f + side];
+    const R* ep = tr + M.fbase[2 * f + side];
     if (M.fw_off[2 * f + side] < 0) {
         const int src = side == 0 ? i : Nf - i;
         v[0] = ep[src];
@@ -340,51 +372,58 @@ __device__ __forceinline__ void face_value(const GeneralMesh& M, const double* _
     }
     const double* tw = M.fw + M.fw_off[2 * f + side];
     const double* tj = tw + i * (Ne + 1);
-    const double den = tw[(Nf + 1) * (Ne + 1) + i];
-    double pn = 0.0, un = 0.0, vn = 0.0;
+    const R den = R(tw[(Nf + 1) * (Ne + 1) + i]);
+    R pn = 0, un = 0, vn = 0;
     for (int j = 0; j <= Ne; ++j) {
-        pn = madd<S>(pn, tj[j], ep[j]);
-        un = madd<S>(un, tj[j], ep[j + ft]);
-        vn = madd<S>(vn, tj[j], ep[j + 2 * ft]);
+        const R t = R(tj[j]);
+        pn = madd<S>(pn, t, ep[j]);
+        un = madd<S>(un, t, ep[j + ft]);
+        vn = madd<S>(vn, t, ep[j + 2 * ft]);
     }
-    v[0] = S ? __ddiv_rn(pn, den) : pn / den;
-    v[1] = S ? __ddiv_rn(un, den) : un / den;
-    v[2] = S ? __ddiv_rn(vn, den) : vn / den;
+    v[0] = div<S>(pn, den);
+    v[1] = div<S>(un, den);
+    v[2] = div<S>(vn, den);
 }
 
-template <int N>
+// Tile of the fused stage: FP64 arrays (the q tile, element numbers and
+// offsets, slot prefix sums) then arrays of the arithmetic type R.
+template <int N, typename R>
 struct FusedTile {
     static constexpr int n = N + 1;
     static constexpr int NN = n * n;
     static constexpr int raw = 256 / (3 * n);
     static constexpr int EPB = raw >= 1 ? raw : 1;
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
-    static constexpr int kQ = 0;                        // [3][EPB][NN] q, then the new q
-    static constexpr int kG = kQ + 3 * EPB * NN;        // [3][EPB][NN] G
-    static constexpr int kF = kG + 3 * EPB * NN;        // [3][EPB][4][n] element side fluxes
-    static constexpr int kJ = kF + 3 * EPB * 4 * n;     // [EPB][NN] J (1/J in the default mode)
-    static constexpr int kS = kJ + EPB * NN;            // [EPB][4] edge metric per side
-    static constexpr int kSp = kS + EPB * 4;            // [4 EPB + 1] prefix sums of the sides' slot counts (ints, in 2 EPB + 1 doubles)
-    static constexpr int kOff = kSp + 2 * EPB + 1;      // [EPB] element id, [EPB] field offset, [EPB] trace offset (int64)
-    static constexpr int kFF = kOff + 3 * EPB;          // [3][EPB][4][slots] face fluxes at the side's face nodes
-    static constexpr size_t bytes(int slots) { return sizeof(double) * (kFF + 3 * EPB * 4 * slots); }
+    // doubles
+    static constexpr int kQ = 0;                   // [3][EPB][NN] q, then the new q
+    static constexpr int kOff = kQ + 3 * EPB * NN; // [EPB] element number, [EPB] field offset, [EPB] trace offset (int64)
+    static constexpr int kSp = kOff + 3 * EPB;     // [4 EPB + 1] prefix sums of the sides' slot counts (ints)
+    static constexpr int kDoubles = kSp + 2 * EPB + 1;
+    // R values past the doubles
+    static constexpr int kG = 0;                   // [3][EPB][NN] G
+    static constexpr int kF = kG + 3 * EPB * NN;   // [3][EPB][4][n] element side fluxes
+    static constexpr int kJ = kF + 3 * EPB * 4 * n;  // [EPB][NN] J (1/J in the default mode)
+    static constexpr int kS = kJ + EPB * NN;       // [EPB][4] edge metric per side
+    static constexpr int kFF = kS + EPB * 4;       // [3][EPB][4][slots] face fluxes at the side's face nodes
+    static constexpr size_t bytes(int slots) { return sizeof(double) * kDoubles + sizeof(R) * (kFF + 3 * EPB * 4 * slots); }
 };
 
-template <int N, bool S>
-__global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
-    using T = FusedTile<N>;
+template <int N, bool S, typename R>
+__global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
+    using T = FusedTile<N, R>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     extern __shared__ __align__(128) double smem[];
     double* qs = smem + T::kQ;
-    double* gs = smem + T::kG;
-    double* fs = smem + T::kF;
-    double* js = smem + T::kJ;
-    double* ss = smem + T::kS;
-    double* ffs = smem + T::kFF;
-    int* sps = reinterpret_cast<int*>(smem + T::kSp);
     int64_t* eid = reinterpret_cast<int64_t*>(smem + T::kOff);  // element numbers of the tile
     int64_t* eo2 = eid + EPB;                                    // their first value in a field block
     int64_t* eo1 = eo2 + EPB;                                    // their first side-trace value
+    int* sps = reinterpret_cast<int*>(smem + T::kSp);
+    R* rs = reinterpret_cast<R*>(smem + T::kDoubles);
+    R* gs = rs + T::kG;
+    R* fs = rs + T::kF;
+    R* js = rs + T::kJ;
+    R* ss = rs + T::kS;
+    R* ffs = rs + T::kFF;
     constexpr int FS = EPB * 4 * n;
     const int SL = a.side_slots;
     const int FFS = EPB * 4 * SL;
@@ -396,11 +435,11 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
     const int64_t fb = M.block, ft = M.trace_total;
     double* q = a.q + inst * 3 * fb;
     double* k = a.k + inst * 3 * fb;
-    const double* tr = a.etr + inst * 3 * ft;
-    double* tr_out = a.etr_out + inst * 3 * ft;
-    const double* xn = g_nodes + gvec(N);
-    const double* lm = g_lagrange_left + gvec(N);
-    const double* lp = g_lagrange_right + gvec(N);
+    const R* tr = pick<R>(a.etr, a.etr_f) + inst * 3 * ft;
+    R* tr_out = pick<R>(a.etr_out, a.etr_out_f) + inst * 3 * ft;
+    const R* xn = tab<R>(g_nodes, gf_nodes) + gvec(N);
+    const R* lm = tab<R>(g_lagrange_left, gf_lagrange_left) + gvec(N);
+    const R* lp = tab<R>(g_lagrange_right, gf_lagrange_right) + gvec(N);
     const double dt = a.step[1];
 
     if (tid < ne) {
@@ -453,17 +492,17 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
             f = M.sface[++q];
             Nf = M.fN[f];
         }
-        double L[3], R[3];
-        face_value<S>(M, tr, ft, f, Nf, 0, j, L);
-        face_value<S>(M, tr, ft, f, Nf, 1, j, R);
-        const double nx = M.fnormal[2 * f], ny = M.fnormal[2 * f + 1];
-        const double wL = add<S>(L[0], add<S>(mul<S>(L[1], nx), mul<S>(L[2], ny)));
-        const double wR = sub<S>(R[0], add<S>(mul<S>(R[1], nx), mul<S>(R[2], ny)));
-        const double sum = add<S>(wL, wR);
-        double* o = ffs + (ee * 4 + s) * SL + slot;
-        o[0] = mul<S>(sub<S>(wL, wR), 0.5);
-        o[FFS] = mul<S>(mul<S>(nx, sum), 0.5);
-        o[2 * FFS] = mul<S>(mul<S>(ny, sum), 0.5);
+        R L[3], Rv[3];
+        face_value<S, R>(M, tr, ft, f, Nf, 0, j, L);
+        face_value<S, R>(M, tr, ft, f, Nf, 1, j, Rv);
+        const R nx = R(M.fnormal[2 * f]), ny = R(M.fnormal[2 * f + 1]);
+        const R wL = add<S>(L[0], add<S>(mul<S>(L[1], nx), mul<S>(L[2], ny)));
+        const R wR = sub<S>(Rv[0], add<S>(mul<S>(Rv[1], nx), mul<S>(Rv[2], ny)));
+        const R sum = add<S>(wL, wR);
+        R* o = ffs + (ee * 4 + s) * SL + slot;
+        o[0] = mul<S>(sub<S>(wL, wR), R(0.5));
+        o[FFS] = mul<S>(mul<S>(nx, sum), R(0.5));
+        o[2 * FFS] = mul<S>(mul<S>(ny, sum), R(0.5));
     }
 
     const int f = tid / (EPB * n);
@@ -472,28 +511,28 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
     const int m = rr - e * n;
     const bool active = f < 3 && e < ne;
     const int64_t ge = active ? eid[e] : 0;
-    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    R x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
         const double* c = M.corners + 8 * ge;
-        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
+        x0 = R(c[0]); y0 = R(c[1]); x1 = R(c[2]); y1 = R(c[3]); x2 = R(c[4]); y2 = R(c[5]); x3 = R(c[6]); y3 = R(c[7]);
     }
-    const MetricLine<S> x_xi(sub<S>(x1, x0), sub<S>(x2, x3)), y_xi(sub<S>(y1, y0), sub<S>(y2, y3));
-    const MetricLine<S> x_eta(sub<S>(x3, x0), sub<S>(x2, x1)), y_eta(sub<S>(y3, y0), sub<S>(y2, y1));
+    const MetricLine<S, R> x_xi(sub<S>(x1, x0), sub<S>(x2, x3)), y_xi(sub<S>(y1, y0), sub<S>(y2, y3));
+    const MetricLine<S, R> x_eta(sub<S>(x3, x0), sub<S>(x2, x1)), y_eta(sub<S>(y3, y0), sub<S>(y2, y1));
     if (active) {
-        const double tm = xn[m];
+        const R tm = xn[m];
         if (f == 2) {
             for (int sd = m; sd < 4; sd += n) {
-                const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
-                const double dx = (sd == 0 || sd == 2) ? metric<S>(at, x_xi.d0, x_xi.d1) : metric<S>(at, x_eta.d0, x_eta.d1);
-                const double dy = (sd == 0 || sd == 2) ? metric<S>(at, y_xi.d0, y_xi.d1) : metric<S>(at, y_eta.d0, y_eta.d1);
+                const R at = (sd == 0 || sd == 3) ? R(-1) : R(1);
+                const R dx = (sd == 0 || sd == 2) ? metric<S, R>(at, x_xi.d0, x_xi.d1) : metric<S, R>(at, x_eta.d0, x_eta.d1);
+                const R dy = (sd == 0 || sd == 2) ? metric<S, R>(at, y_xi.d0, y_xi.d1) : metric<S, R>(at, y_eta.d0, y_eta.d1);
                 ss[e * 4 + sd] = sqrt(add<S>(mul<S>(dx, dx), mul<S>(dy, dy)));
             }
         }
-        const double xe = x_eta(tm), ye = y_eta(tm);
+        const R xe = x_eta(tm), ye = y_eta(tm);
         for (int j = f; j < n; j += 3) {
-            const double tj = xn[j];
-            const double jac = sub<S>(mul<S>(x_xi(tj), ye), mul<S>(xe, y_xi(tj)));
-            js[e * NN + m * n + j] = S ? jac : __drcp_rn(jac);
+            const R tj = xn[j];
+            const R jac = sub<S>(mul<S>(x_xi(tj), ye), mul<S>(xe, y_xi(tj)));
+            js[e * NN + m * n + j] = S ? jac : R(1) / jac;
         }
     }
     __syncthreads();  // q tile, face fluxes, J, edge metrics
@@ -507,9 +546,9 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
         const int s = sm / n, i = sm - s * n;
         const int64_t el = eid[ee];
         const int64_t q0 = M.sface_start[4 * el + s], q1 = M.sface_start[4 * el + s + 1];
-        const double sfv = ss[ee * 4 + s];
-        const double* fl = ffs + (ee * 4 + s) * SL;
-        double out[3] = {0.0, 0.0, 0.0};
+        const R sfv = ss[ee * 4 + s];
+        const R* fl = ffs + (ee * 4 + s) * SL;
+        R out[3] = {0, 0, 0};
         if (q1 > q0) {
             const int64_t f0 = M.sface[q0];
             const int64_t en0 = M.enodes[4 * el + s], en1 = M.enodes[4 * el + ((s + 1) & 3)];
@@ -523,13 +562,13 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
                     const int64_t ff = M.sface[qq];
                     const int Nf = M.fN[ff];
                     const int fsd = el == M.felem[2 * ff] ? 0 : 1;
-                    const double scale = M.fscale[2 * ff + fsd];
+                    const R scale = R(M.fscale[2 * ff + fsd]);
                     const double* W = M.sw + M.sw_off[qq] + i * (Nf + 1);
                     const int* match = M.smatch + M.sm_off[qq];
                     for (int j = 0; j <= Nf; ++j) {
                         const int mt = match[j];
                         if (mt >= 0 && mt != i) continue;
-                        const double w = W[j];
+                        const R w = R(W[j]);
 #pragma unroll
                         for (int c = 0; c < 3; ++c) out[c] = add<S>(out[c], mul<S>(mul<S>(mul<S>(w, fl[c * FFS + slot0 + j]), sfv), scale));
                     }
@@ -543,32 +582,32 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
     }
     __syncthreads();
 
-    const double* Dh = g_dhat + gmat(N);
-    const double* w = g_weights + gvec(N);
-    const double* iw = g_inv_weights + gvec(N);
-    const double* F = fs + f * FS + e * 4 * n;
+    const R* Dh = tab<R>(g_dhat, gf_dhat) + gmat(N);
+    const R* w = tab<R>(g_weights, gf_weights) + gvec(N);
+    const R* iw = tab<R>(g_inv_weights, gf_inv_weights) + gvec(N);
+    const R* F = fs + f * FS + e * 4 * n;
 
     // xi pass (eta index j = m): Dhat . line + lift, G = -(...) (Solver2D_t.cpp:82-101).
     if (active) {
         const int j = m;
-        double col[n];
+        R col[n];
         const double* P = qs + (0 * EPB + e) * NN + j;
         const double* U = qs + (1 * EPB + e) * NN + j;
         const double* V = qs + (2 * EPB + e) * NN + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-            if (f == 0) col[i] = sub<S>(mul<S>(y_eta(xn[i]), U[i * n]), mul<S>(x_eta(xn[i]), V[i * n]));
-            else if (f == 1) col[i] = mul<S>(y_eta(xn[i]), P[i * n]);
-            else col[i] = -mul<S>(x_eta(xn[i]), P[i * n]);
+            if (f == 0) col[i] = sub<S>(mul<S>(y_eta(xn[i]), R(U[i * n])), mul<S>(x_eta(xn[i]), R(V[i * n])));
+            else if (f == 1) col[i] = mul<S>(y_eta(xn[i]), R(P[i * n]));
+            else col[i] = -mul<S>(x_eta(xn[i]), R(P[i * n]));
         }
-        const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
-        double* G = gs + (f * EPB + e) * NN + j;
+        const R fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
+        R* G = gs + (f * EPB + e) * NN + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-            double acc = 0.0;
+            R acc = 0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[i * n + mm], col[mm]);
-            const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
+            const R lift = S ? div<S>(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
             G[i * n] = -add<S>(acc, lift);
         }
     }
@@ -577,38 +616,38 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
     // eta pass (xi index i = m): G = (G - (Dhat . line + lift)) / J (Solver2D_t.cpp:103-133).
     if (active) {
         const int i = m;
-        double line[n];
+        R line[n];
         const double* P = qs + (0 * EPB + e) * NN + i * n;
         const double* U = qs + (1 * EPB + e) * NN + i * n;
         const double* V = qs + (2 * EPB + e) * NN + i * n;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            if (f == 0) line[j] = add<S>(mul<S>(-y_xi(xn[j]), U[j]), mul<S>(x_xi(xn[j]), V[j]));
-            else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), P[j]);
-            else line[j] = mul<S>(x_xi(xn[j]), P[j]);
+            if (f == 0) line[j] = add<S>(mul<S>(-y_xi(xn[j]), R(U[j])), mul<S>(x_xi(xn[j]), R(V[j])));
+            else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), R(P[j]));
+            else line[j] = mul<S>(x_xi(xn[j]), R(P[j]));
         }
-        const double ftp = F[2 * n + (N - i)], fbm = F[0 * n + i];
-        double* G = gs + (f * EPB + e) * NN + i * n;
-        const double* jrow = js + e * NN + i * n;
+        const R ftp = F[2 * n + (N - i)], fbm = F[0 * n + i];
+        R* G = gs + (f * EPB + e) * NN + i * n;
+        const R* jrow = js + e * NN + i * n;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            double acc = 0.0;
+            R acc = 0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[j * n + mm], line[mm]);
-            const double lift = S ? __ddiv_rn(add<S>(mul<S>(ftp, lp[j]), mul<S>(fbm, lm[j])), w[j]) : (ftp * lp[j] + fbm * lm[j]) * iw[j];
-            const double num = sub<S>(G[j], add<S>(acc, lift));
-            G[j] = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
+            const R lift = S ? div<S>(add<S>(mul<S>(ftp, lp[j]), mul<S>(fbm, lm[j])), w[j]) : (ftp * lp[j] + fbm * lm[j]) * iw[j];
+            const R num = sub<S>(G[j], add<S>(acc, lift));
+            G[j] = S ? div<S>(num, jrow[j]) : num * jrow[j];
         }
     }
     __syncthreads();
 
-    // Low-storage RK3 update (Solver2D_t.cpp:138-172), node by node.
+    // Low-storage RK3 update (Solver2D_t.cpp:138-172), node by node, in FP64.
     const double gdt = mul<S>(a.rk_g, dt);
     for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
         const int ff = idx / (ne * NN), r = idx - ff * (ne * NN);
         const int ee = r / NN, node = r - ee * NN;
         const int64_t gi = ff * fb + eo2[ee] + node;
-        const double G = gs[(ff * EPB + ee) * NN + node];
+        const double G = static_cast<double>(gs[(ff * EPB + ee) * NN + node]);
         const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, k[gi]), G);
         const double qn = add<S>(qs[(ff * EPB + ee) * NN + node], mul<S>(gdt, kn));
         k[gi] = kn;
@@ -623,17 +662,17 @@ __global__ void __launch_bounds__(FusedTile<N>::kThreads) general_fused_kernel(G
     for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
         const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
         const int s = sm / n, mm = sm - s * n;
-        const double* l = (s == 0 || s == 3) ? lm : lp;
+        const R* l = (s == 0 || s == 3) ? lm : lp;
         const int line = (s < 2) ? mm : N - mm;
         const int b0 = (s == 0 || s == 2) ? line * n : line;
         const int stride = (s == 0 || s == 2) ? 1 : n;
-        double* out = tr_out + eo1[ee] + s * n + mm;
+        R* out = tr_out + eo1[ee] + s * n + mm;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const double* qe = qs + (c * EPB + ee) * NN + b0;
-            double acc = 0.0;
+            R acc = 0;
 #pragma unroll
-            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], qe[j * stride]);
+            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], R(qe[j * stride]));
             out[c * ft] = acc;
         }
     }
@@ -754,26 +793,28 @@ int grid_for(int64_t items, int threads) {
     return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32)));
 }
 
-template <int N, bool S>
+template <int N, bool S, typename R>
 cudaError_t launch_group_traces(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
-    general_traces_kernel<N, S><<<grid_for(g.count * 4 * (N + 1) * a.n_instances, 256), 256, 0, stream>>>(a, g.ids, g.count);
+    general_traces_kernel<N, S, R><<<grid_for(g.count * 4 * (N + 1) * a.n_instances, 256), 256, 0, stream>>>(a, g.ids, g.count);
     return cudaGetLastError();
 }
 
-template <int N, bool S>
+template <int N, bool S, typename R>
 cudaError_t launch_fused(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
-    using T = FusedTile<N>;
+    using T = FusedTile<N, R>;
     const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
-    general_fused_kernel<N, S><<<grid, T::kThreads, T::bytes(a.side_slots), stream>>>(a, g.ids, g.count);
+    general_fused_kernel<N, S, R><<<grid, T::kThreads, T::bytes(a.side_slots), stream>>>(a, g.ids, g.count);
     return cudaGetLastError();
 }
 
 template <int N>
 cudaError_t set_attrs(int side_slots) {
-    const int bytes = static_cast<int>(FusedTile<N>::bytes(side_slots));
-    cudaError_t err = cudaFuncSetAttribute(general_fused_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (err != cudaSuccess) return err;
-    return cudaFuncSetAttribute(general_fused_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    const int b64 = static_cast<int>(FusedTile<N, double>::bytes(side_slots));
+    const int b32 = static_cast<int>(FusedTile<N, float>::bytes(side_slots));
+    cudaError_t err = cudaFuncSetAttribute(general_fused_kernel<N, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b64);
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(general_fused_kernel<N, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b64);
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(general_fused_kernel<N, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b32);
+    return err;
 }
 
 template <int N>
@@ -832,38 +873,50 @@ cudaError_t upload_general_tables(const Tables& t) {
     if ((err = cudaMemcpyToSymbol(g_bary, bary.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
     if ((err = cudaMemcpyToSymbol(g_lagrange_left, ll.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
     if ((err = cudaMemcpyToSymbol(g_lagrange_right, lr.data(), sizeof(double) * kGVecTotal)) != cudaSuccess) return err;
-    return cudaMemcpyToSymbol(g_dhat, dhat.data(), sizeof(double) * kGMatTotal);
+    if ((err = cudaMemcpyToSymbol(g_dhat, dhat.data(), sizeof(double) * kGMatTotal)) != cudaSuccess) return err;
+    auto to_f = [](const std::vector<double>& v) { return std::vector<float>(v.begin(), v.end()); };
+    const std::vector<float> fn = to_f(nodes), fw = to_f(weights), fiw = to_f(inv_w), fll = to_f(ll), flr = to_f(lr), fd = to_f(dhat);
+    if ((err = cudaMemcpyToSymbol(gf_nodes, fn.data(), sizeof(float) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(gf_weights, fw.data(), sizeof(float) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(gf_inv_weights, fiw.data(), sizeof(float) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(gf_lagrange_left, fll.data(), sizeof(float) * kGVecTotal)) != cudaSuccess) return err;
+    if ((err = cudaMemcpyToSymbol(gf_lagrange_right, flr.data(), sizeof(float) * kGVecTotal)) != cudaSuccess) return err;
+    return cudaMemcpyToSymbol(gf_dhat, fd.data(), sizeof(float) * kGMatTotal);
 }
 
 cudaError_t prepare_general_kernels(int N, int side_slots) {
     return by_order(N, [&](auto c) { return set_attrs<decltype(c)::value>(side_slots); });
 }
 
-cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream) {
+cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, bool fp32, cudaStream_t stream) {
     cudaError_t err = cudaSuccess;
     for (int g = 0; g < n_groups && err == cudaSuccess; ++g) {
         if (groups[g].count == 0) continue;
         err = by_order(groups[g].N, [&](auto c) {
             constexpr int N = decltype(c)::value;
-            return strict ? launch_group_traces<N, true>(a, groups[g], stream) : launch_group_traces<N, false>(a, groups[g], stream);
+            if (fp32) return launch_group_traces<N, false, float>(a, groups[g], stream);
+            return strict ? launch_group_traces<N, true, double>(a, groups[g], stream) : launch_group_traces<N, false, double>(a, groups[g], stream);
         });
     }
     return err;
 }
 
-cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, cudaStream_t stream) {
+cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, bool fp32, cudaStream_t stream) {
     const int64_t n_ghosts = a.m.n_total - a.m.n_domain;
     if (n_ghosts == 0) return cudaSuccess;
-    if (strict) general_ghosts_kernel<true><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
-    else general_ghosts_kernel<false><<<grid_for(n_ghosts * a.n_instances, 128), 128, 0, stream>>>(a);
+    const int blocks = grid_for(n_ghosts * a.n_instances, 128);
+    if (fp32) general_ghosts_kernel<false, float><<<blocks, 128, 0, stream>>>(a);
+    else if (strict) general_ghosts_kernel<true, double><<<blocks, 128, 0, stream>>>(a);
+    else general_ghosts_kernel<false, double><<<blocks, 128, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, cudaStream_t stream) {
+cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream) {
     if (g.count == 0) return cudaSuccess;
     return by_order(g.N, [&](auto c) {
         constexpr int N = decltype(c)::value;
-        return strict ? launch_fused<N, true>(a, g, stream) : launch_fused<N, false>(a, g, stream);
+        if (fp32) return launch_fused<N, false, float>(a, g, stream);
+        return strict ? launch_fused<N, true, double>(a, g, stream) : launch_fused<N, false, double>(a, g, stream);
     });
 }
 

@@ -75,6 +75,8 @@ struct GeneralStage {
     double* G_out = nullptr;  // optional copy of the stage's time derivative
     double* etr = nullptr;      // [instance][field][trace_total] element side traces of q (ghosts filled by the stage)
     double* etr_out = nullptr;  // the same for the stage's output
+    float* etr_f = nullptr;     // the two trace buffers of the FP32 form
+    float* etr_out_f = nullptr;
     int side_slots = 1;         // largest sum of (face order + 1) over the faces of one element side
     const double* step = nullptr;  // {time, dt, dt_mesh, t_end}
     double rk_a = 0, rk_b = 0, rk_g = 0;
@@ -95,13 +97,15 @@ cudaError_t upload_general_tables(const Tables& t);
 cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, cudaStream_t stream);
 cudaError_t prepare_general_kernels(int N, int side_slots);
 // Side traces of q into etr (before the first stage, or after q changed).
-cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, cudaStream_t stream);
+cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, bool fp32, cudaStream_t stream);
 // One stage is the ghost traces into etr, then for every order group the
 // fused face fluxes, volume term, RK update and traces of the new state
 // into etr_out. The groups read only etr and write disjoint elements, so
 // they may run concurrently after the ghost launch.
-cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, cudaStream_t stream);
-cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, cudaStream_t stream);
+// fp32: the FP32 form (traces, fluxes and the volume term in FP32 over the
+// FP32 trace buffers; q, k and the RK update in FP64).
+cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, bool fp32, cudaStream_t stream);
+cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream);
 // The plane-wave initial condition at every node of a mixed-order mesh.
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream);
 

@@ -13,12 +13,56 @@ namespace ndg {
 namespace dev {
 
 // ---------------------------------------------------------------------------
-// Arithmetic with selectable rounding.
-template <bool S> __device__ __forceinline__ double mul(double a, double b) { return S ? __dmul_rn(a, b) : a * b; }
-template <bool S> __device__ __forceinline__ double add(double a, double b) { return S ? __dadd_rn(a, b) : a + b; }
-template <bool S> __device__ __forceinline__ double sub(double a, double b) { return S ? __dsub_rn(a, b) : a - b; }
+// Arithmetic with selectable rounding: S (strict, FP64 only) rounds every
+// operation on its own in the written order; otherwise the compiler may
+// contract, and R may be float (the FP32 forms).
+template <bool S, typename R>
+__device__ __forceinline__ R mul(R a, R b) {
+    if constexpr (S) {
+        static_assert(sizeof(R) == 8, "strict rounding is FP64");
+        return __dmul_rn(a, b);
+    } else {
+        return a * b;
+    }
+}
+template <bool S, typename R>
+__device__ __forceinline__ R add(R a, R b) {
+    if constexpr (S) {
+        static_assert(sizeof(R) == 8, "strict rounding is FP64");
+        return __dadd_rn(a, b);
+    } else {
+        return a + b;
+    }
+}
+template <bool S, typename R>
+__device__ __forceinline__ R sub(R a, R b) {
+    if constexpr (S) {
+        static_assert(sizeof(R) == 8, "strict rounding is FP64");
+        return __dsub_rn(a, b);
+    } else {
+        return a - b;
+    }
+}
 // s + a*b: two roundings in strict mode, one FMA otherwise.
-template <bool S> __device__ __forceinline__ double madd(double s, double a, double b) { return S ? __dadd_rn(s, __dmul_rn(a, b)) : fma(a, b, s); }
+template <bool S, typename R>
+__device__ __forceinline__ R madd(R s, R a, R b) {
+    if constexpr (S) {
+        static_assert(sizeof(R) == 8, "strict rounding is FP64");
+        return __dadd_rn(s, __dmul_rn(a, b));
+    } else {
+        return fma(a, b, s);
+    }
+}
+// a / b: the IEEE quotient in strict mode (and for FP32), a * (1/b) allowed otherwise by the caller.
+template <bool S, typename R>
+__device__ __forceinline__ R div(R a, R b) {
+    if constexpr (S) {
+        static_assert(sizeof(R) == 8, "strict rounding is FP64");
+        return __ddiv_rn(a, b);
+    } else {
+        return a / b;
+    }
+}
 
 // The reference plane wave g(x, t) (include/functions/analytical_solution.tpp:4-10,
 // constants of include/helpers/constants.h:15-18).
@@ -31,19 +75,19 @@ __device__ __forceinline__ void plane_wave(double x, double y, double t, double&
 }
 
 // Bilinear metric term ((1 - t) a + (1 + t) b) / 4 of quad_metrics.
-template <bool S>
-__device__ __forceinline__ double metric(double t, double a, double b) {
-    return mul<S>(add<S>(mul<S>(sub<S>(1.0, t), a), mul<S>(add<S>(1.0, t), b)), 0.25);
+template <bool S, typename R = double>
+__device__ __forceinline__ R metric(R t, R a, R b) {
+    return mul<S>(add<S>(mul<S>(sub<S>(R(1), t), a), mul<S>(add<S>(R(1), t), b)), R(0.25));
 }
 
 // Linear-in-t metric term of quad_metrics: ((1 - t) d0 + (1 + t) d1) / 4.
 // Strict mode evaluates the reference's expression; the default mode the
 // equivalent fma(t, (d1 - d0) / 4, (d0 + d1) / 4).
-template <bool S>
+template <bool S, typename R = double>
 struct MetricLine {
-    double d0, d1, a, b;
-    __device__ __forceinline__ MetricLine(double d0_, double d1_) : d0(d0_), d1(d1_), a(0.25 * (d0_ + d1_)), b(0.25 * (d1_ - d0_)) {}
-    __device__ __forceinline__ double operator()(double t) const { return S ? metric<S>(t, d0, d1) : fma(t, b, a); }
+    R d0, d1, a, b;
+    __device__ __forceinline__ MetricLine(R d0_, R d1_) : d0(d0_), d1(d1_), a(R(0.25) * (d0_ + d1_)), b(R(0.25) * (d1_ - d0_)) {}
+    __device__ __forceinline__ R operator()(R t) const { return S ? metric<S, R>(t, d0, d1) : fma(t, b, a); }
 };
 
 // ---------------------------------------------------------------------------

@@ -76,7 +76,7 @@ def test_fp32_full_size_and_batched():
     assert not np.allclose(m32.get_field("p", instance=1), m32.get_field("p", instance=0))
 
 
-def test_fp32_switch_mid_run_and_adapted_mesh_rejected():
+def test_fp32_switch_mid_run_and_after_adaptation():
     zone = meshgen.uniform_zone(16, x_periodic=True, boundary=meshgen.WALL)
     o = OracleSolver(zone, 4)
     o.initial_conditions()
@@ -92,7 +92,42 @@ def test_fp32_switch_mid_run_and_adapted_mesh_rejected():
     m.estimate_error()
     m.adapt()
     if len(set(m.elements()["N"][:m.n_elements_].tolist())) > 1:
+        # switch forms on the mixed-order path: FP32 steps against FP64 steps from the same state
+        state = {f: m.get_field(f) for f in ("p", "u", "v", "k_p", "k_u", "k_v")}
+        ndg.Solver2D_t.run(m, 5)
+        ref = {f: m.get_field(f) for f in ("p", "u", "v")}
+        for f, v in state.items():
+            m.set_field(f, v)
         m.set_precision(ndg.FP32)
-        with pytest.raises(ndg.NdgError) as e:
-            ndg.Solver2D_t.run(m, 1)
-        assert e.value.status == 7
+        ndg.Solver2D_t.run(m, 5)
+        for f in ("p", "u", "v"):
+            assert rel_l2(m.get_field(f), ref[f]) < TOL32, f
+
+
+@pytest.mark.parametrize("kind", ["periodic_jittered", "walls", "outflow"])
+def test_fp32_on_adapted_meshes(kind):
+    """The FP32 form on the mixed-order, nonconforming path (after p- and
+    h-adaptation, mortar faces): against the FP64 path on the same mesh and
+    state, 1e-6 relative L2 after 30 steps on a 16 x 16 mesh. (On a coarse
+    8 x 8 jittered mesh at N = 4 the plane wave is under-resolved and the FP32
+    form reaches 1.0e-6 after 40 steps on the uniform path as well: the
+    rounding, not the mortar path, sets that.)"""
+    kw = {"periodic_jittered": dict(x_periodic=True, y_periodic=True, jitter=0.1, seed=4),
+          "walls": dict(boundary=meshgen.WALL), "outflow": dict(boundary=meshgen.OUTFLOW)}[kind]
+    zone = meshgen.uniform_zone(16, **kw)
+    meshes = [ndg.Mesh2D_t(zone, 4, maximum_N=10, max_split_level=1, precision=p) for p in (ndg.FP64, ndg.FP32)]
+    rng = np.random.default_rng(3)
+    flags = (rng.random(256) < 0.4).astype(np.int32)
+    sigma = np.where(rng.random(256) < 0.5, 2.0, 0.5)  # p-refine or split
+    for m in meshes:
+        m.initial_conditions()
+        m.adapt(flags, sigma)
+    K = meshes[0].n_elements_
+    assert K > 256 and len(set(meshes[0].elements()["N"][:K].tolist())) > 1
+    flags2 = (rng.random(K) < 0.3).astype(np.int32)
+    for m in meshes:
+        m.adapt(flags2, np.full(K, 2.0))
+        ndg.Solver2D_t.run(m, 30)
+    for f in ("p", "u", "v"):
+        err = rel_l2(meshes[1].get_field(f), meshes[0].get_field(f))
+        assert err < TOL32, (kind, f, err)
