@@ -204,7 +204,9 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
         mbar_expect_tx(bar, 3 * bytes);
         for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
     }
-    R x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0, ce = 1;
+    // Corners in FP64: their differences are formed before rounding to R.
+    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    R ce = 1;
     if (active) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
@@ -213,11 +215,11 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
             far_s[f * FS + (e * 4 + s) * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
-        x0 = R(c[0]); y0 = R(c[1]); x1 = R(c[2]); y1 = R(c[3]); x2 = R(c[4]); y2 = R(c[5]); x3 = R(c[6]); y3 = R(c[7]);
+        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
         ce = R(a.c[ge]);
     }
-    const LineR<R> x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
-    const LineR<R> x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
+    const LineR<R> x_xi(R(x1 - x0), R(x2 - x3)), y_xi(R(y1 - y0), R(y2 - y3));
+    const LineR<R> x_eta(R(x3 - x0), R(x2 - x1)), y_eta(R(y3 - y0), R(y2 - y1));
     if (active) {
         const R tm = xn[m];
         if (f == 2) {
@@ -510,7 +512,9 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
     }
     for (int i = tid; i < EPB * NN; i += T::kThreads) tp[i] = R(0);
     if (tid < EPB) rmask[tid] = 0ull;
-    R x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0, ce = 1;
+    // Corners in FP64: their differences are formed before rounding to R.
+    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    R ce = 1;
     if (active) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
@@ -519,11 +523,11 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
             far_s[f * FS + (e * 4 + s) * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
-        x0 = R(c[0]); y0 = R(c[1]); x1 = R(c[2]); y1 = R(c[3]); x2 = R(c[4]); y2 = R(c[5]); x3 = R(c[6]); y3 = R(c[7]);
+        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
         ce = R(a.c[ge]);
     }
-    const LineR<R> x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
-    const LineR<R> x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
+    const LineR<R> x_xi(R(x1 - x0), R(x2 - x3)), y_xi(R(y1 - y0), R(y2 - y3));
+    const LineR<R> x_eta(R(x3 - x0), R(x2 - x1)), y_eta(R(y3 - y0), R(y2 - y1));
     if (active) {
         const R tm = xn[m];
         if (f == 2) {

@@ -520,6 +520,11 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
 // Mesh2D_t::adapt from per-element refine flags and decay rates; moves the
 // fields of a device context to the new mesh.
 void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in) {
+    if (std::none_of(refine_in, refine_in + ctx->topo.n_domain, [](int32_t r) { return r != 0; })) {
+        // Mesh2D_t::adapt changes nothing without a refine flag
+        ctx->has_error_estimate = false;
+        return;
+    }
     const std::vector<int32_t> refine(refine_in, refine_in + ctx->topo.n_domain);
     const std::vector<double> sigma(sigma_in, sigma_in + ctx->topo.n_domain);
     const Layout before = layout_of(ctx->topo);

@@ -128,19 +128,24 @@ __global__ void __launch_bounds__(256) general_traces_kernel(GeneralStage a, con
     }
 }
 
-// Ghost traces: thread per (instance, ghost element).
+// Ghost traces: thread per (instance, ghost element, node); each node
+// gathers the contributions the reference's loops add to it, in their order.
 template <bool S, typename R>
-__global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
+__global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a, int max_n) {
     const GeneralMesh& M = a.m;
     const int64_t n_ghosts = M.n_total - M.n_domain;
     const int64_t ft = M.trace_total;
     const double t = add<S>(a.step[0], mul<S>(a.rk_b, a.step[1]));
-    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n_ghosts * a.n_instances;
+    const int64_t per_inst = n_ghosts * max_n;
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < per_inst * a.n_instances;
          idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t inst = idx / n_ghosts;
-        const int64_t gi = idx - inst * n_ghosts;
+        const int64_t inst = idx / per_inst;
+        const int64_t r = idx - inst * per_inst;
+        const int64_t gi = r / max_n;
+        const int i = static_cast<int>(r - gi * max_n);
         const int64_t ge = M.n_domain + gi;
         const int N = M.eN[ge];
+        if (i > N) continue;
         const double* xe = g_nodes + gvec(N);
         R* tr = pick<R>(a.etr, a.etr_f) + inst * 3 * ft;
         R* gp = tr + M.off1[ge];
@@ -152,7 +157,7 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
             const double* we = g_weights + gvec(N);
             const double* bwe = g_bary + gvec(N);
             const R sf = R(M.gscale[gi]);
-            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = R(0);
+            R vp = 0, vu = 0, vv = 0;
             for (int64_t q = M.sface_start[4 * ge]; q < M.sface_start[4 * ge + 1]; ++q) {
                 const int64_t f = M.sface[q];
                 const int fs = M.felem[2 * f] == ge ? 1 : 0;
@@ -168,69 +173,63 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a) {
                 for (int j = 0; j <= Nn; ++j) {
                     const double coord = mortar_coord(xnb[Nn - j], scale, offset);
                     int found = -1;
-                    for (int i = 0; i <= N; ++i)
-                        if (almost_equal(coord, xe[i])) {
-                            found = i;
+                    for (int ii = 0; ii <= N; ++ii)
+                        if (almost_equal(coord, xe[ii])) {
+                            found = ii;
                             break;
                         }
+                    R w;
                     if (found >= 0) {
-                        const int i = found;
-                        const R w = R(S ? __ddiv_rn(wnb[j], we[i]) : wnb[j] / we[i]);
-                        gp[i] = add<S>(gp[i], mul<S>(mul<S>(w, np_[j]), sf));
-                        gu[i] = add<S>(gu[i], mul<S>(mul<S>(w, nu_[j]), sf));
-                        gv[i] = add<S>(gv[i], mul<S>(mul<S>(w, nv_[j]), sf));
+                        if (found != i) continue;
+                        w = R(S ? __ddiv_rn(wnb[j], we[i]) : wnb[j] / we[i]);
                     } else {
-                        double s = 0.0;
-                        for (int i = 0; i <= N; ++i) s = add<S>(s, S ? __ddiv_rn(bwe[i], __dsub_rn(coord, xe[i])) : bwe[i] / (coord - xe[i]));
-                        for (int i = 0; i <= N; ++i) {
-                            const double T = S ? __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), s)) : bwe[i] / ((coord - xe[i]) * s);
-                            const R w = R(S ? __ddiv_rn(__dmul_rn(T, wnb[j]), we[i]) : T * wnb[j] / we[i]);
-                            gp[i] = add<S>(gp[i], mul<S>(mul<S>(w, np_[j]), sf));
-                            gu[i] = add<S>(gu[i], mul<S>(mul<S>(w, nu_[j]), sf));
-                            gv[i] = add<S>(gv[i], mul<S>(mul<S>(w, nv_[j]), sf));
-                        }
+                        double sb = 0.0;
+                        for (int ii = 0; ii <= N; ++ii) sb = add<S>(sb, S ? __ddiv_rn(bwe[ii], __dsub_rn(coord, xe[ii])) : bwe[ii] / (coord - xe[ii]));
+                        const double T = S ? __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), sb)) : bwe[i] / ((coord - xe[i]) * sb);
+                        w = R(S ? __ddiv_rn(__dmul_rn(T, wnb[j]), we[i]) : T * wnb[j] / we[i]);
                     }
+                    vp = add<S>(vp, mul<S>(mul<S>(w, np_[j]), sf));
+                    vu = add<S>(vu, mul<S>(mul<S>(w, nu_[j]), sf));
+                    vv = add<S>(vv, mul<S>(mul<S>(w, nv_[j]), sf));
                 }
             }
             if (kind == kGhostMirror && M.sface_start[4 * ge + 1] > M.sface_start[4 * ge]) {
                 const int64_t f = M.sface[M.sface_start[4 * ge]];
                 const R nx = R(M.fnormal[2 * f]), ny = R(M.fnormal[2 * f + 1]);
                 const R tx = R(M.ftangent[2 * f]), ty = R(M.ftangent[2 * f + 1]);
-                for (int i = 0; i <= N; ++i) {
-                    const R Vx = gu[i], Vy = gv[i];
-                    const R l0 = -add<S>(mul<S>(Vx, nx), mul<S>(Vy, ny));
-                    const R l1 = add<S>(mul<S>(Vx, tx), mul<S>(Vy, ty));
-                    gu[i] = add<S>(mul<S>(nx, l0), mul<S>(tx, l1));
-                    gv[i] = add<S>(mul<S>(ny, l0), mul<S>(ty, l1));
-                }
+                const R l0 = -add<S>(mul<S>(vu, nx), mul<S>(vv, ny));
+                const R l1 = add<S>(mul<S>(vu, tx), mul<S>(vv, ty));
+                vu = add<S>(mul<S>(nx, l0), mul<S>(tx, l1));
+                vv = add<S>(mul<S>(ny, l0), mul<S>(ty, l1));
             }
+            gp[i] = vp;
+            gu[i] = vu;
+            gv[i] = vv;
         } else if (kind == kGhostAnalytic) {
             // Mesh2D_t.cpp:4575-4599.
             const int64_t n0 = M.enodes[4 * ge], n1 = M.enodes[4 * ge + 1];
             const double p0x = M.node_xy[2 * n0], p0y = M.node_xy[2 * n0 + 1];
             const double p1x = M.node_xy[2 * n1], p1y = M.node_xy[2 * n1 + 1];
-            for (int i = 0; i <= N; ++i) {
-                const double r = __dmul_rn(__dadd_rn(xe[i], 1.0), 0.5);
-                const double gx = __dadd_rn(__dmul_rn(p1x, r), __dmul_rn(p0x, __dsub_rn(1.0, r)));
-                const double gy = __dadd_rn(__dmul_rn(p1y, r), __dmul_rn(p0y, __dsub_rn(1.0, r)));
-                double pw, uw, vw;
-                plane_wave(gx, gy, t, pw, uw, vw);
-                gp[i] = R(pw);
-                gu[i] = R(uw);
-                gv[i] = R(vw);
-            }
+            const double rr = __dmul_rn(__dadd_rn(xe[i], 1.0), 0.5);
+            const double gx = __dadd_rn(__dmul_rn(p1x, rr), __dmul_rn(p0x, __dsub_rn(1.0, rr)));
+            const double gy = __dadd_rn(__dmul_rn(p1y, rr), __dmul_rn(p0y, __dsub_rn(1.0, rr)));
+            double pw, uw, vw;
+            plane_wave(gx, gy, t, pw, uw, vw);
+            gp[i] = R(pw);
+            gu[i] = R(uw);
+            gv[i] = R(vw);
         } else if (kind == kGhostInterface) {
-            // Mesh2D_t.cpp:4712-4730.
+            // Mesh2D_t.cpp:4712-4730: the origin's side trace, up to its order.
             const int64_t src = M.gsrc[gi];
             const int Ns = M.eN[src];
-            const R* sp = tr + M.off1[src] + M.gsrc_side[gi] * (Ns + 1);
-            for (int i = 0; i <= Ns && i <= N; ++i) {
+            if (i <= Ns) {
+                const R* sp = tr + M.off1[src] + M.gsrc_side[gi] * (Ns + 1);
                 gp[i] = sp[i];
                 gu[i] = sp[i + ft];
                 gv[i] = sp[i + 2 * ft];
             }
         } else {
-            for (int i = 0; i <= N; ++i) gp[i] = gu[i] = gv[i] = R(0);
+            gp[i] = gu[i] = gv[i] = R(0);
         }
     }
 }
@@ -404,7 +403,9 @@ struct FusedTile {
     static constexpr int kF = kG + 3 * EPB * NN;   // [3][EPB][4][n] element side fluxes
     static constexpr int kJ = kF + 3 * EPB * 4 * n;  // [EPB][NN] J (1/J in the default mode)
     static constexpr int kS = kJ + EPB * NN;       // [EPB][4] edge metric per side
-    static constexpr int kFF = kS + EPB * 4;       // [3][EPB][4][slots] face fluxes at the side's face nodes
+    static constexpr bool kCopy = sizeof(R) != sizeof(double);  // the FP32 form keeps an FP32 copy of the q tile
+    static constexpr int kQr = kS + EPB * 4;       // [3][EPB][NN] q in R (FP32 form only)
+    static constexpr int kFF = kQr + (kCopy ? 3 * EPB * NN : 0);  // [3][EPB][4][slots] face fluxes at the side's face nodes
     static constexpr size_t bytes(int slots) { return sizeof(double) * kDoubles + sizeof(R) * (kFF + 3 * EPB * 4 * slots); }
 };
 
@@ -424,6 +425,16 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     R* js = rs + T::kJ;
     R* ss = rs + T::kS;
     R* ffs = rs + T::kFF;
+    // q in the arithmetic type: a converted copy in the FP32 form, the tile itself in FP64
+    const R* qv;
+    R* qw;
+    if constexpr (T::kCopy) {
+        qw = rs + T::kQr;
+        qv = qw;
+    } else {
+        qw = nullptr;
+        qv = qs;
+    }
     constexpr int FS = EPB * 4 * n;
     const int SL = a.side_slots;
     const int FFS = EPB * 4 * SL;
@@ -453,7 +464,9 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
         const int f = idx / (ne * NN), r = idx - f * (ne * NN);
         const int e = r / NN, node = r - e * NN;
-        qs[(f * EPB + e) * NN + node] = q[f * fb + eo2[e] + node];
+        const double v = q[f * fb + eo2[e] + node];
+        qs[(f * EPB + e) * NN + node] = v;
+        if constexpr (T::kCopy) qw[(f * EPB + e) * NN + node] = R(v);
     }
     // Face fluxes at every face node of every side (Mesh2D_t.cpp:3803-3893,
     // Solver2D_t.cpp:48-63): the tile's sides' slot counts (the sum of face
@@ -511,13 +524,14 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     const int m = rr - e * n;
     const bool active = f < 3 && e < ne;
     const int64_t ge = active ? eid[e] : 0;
-    R x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    // Corners in FP64: their differences are formed before rounding to R.
+    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
         const double* c = M.corners + 8 * ge;
-        x0 = R(c[0]); y0 = R(c[1]); x1 = R(c[2]); y1 = R(c[3]); x2 = R(c[4]); y2 = R(c[5]); x3 = R(c[6]); y3 = R(c[7]);
+        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
     }
-    const MetricLine<S, R> x_xi(sub<S>(x1, x0), sub<S>(x2, x3)), y_xi(sub<S>(y1, y0), sub<S>(y2, y3));
-    const MetricLine<S, R> x_eta(sub<S>(x3, x0), sub<S>(x2, x1)), y_eta(sub<S>(y3, y0), sub<S>(y2, y1));
+    const MetricLine<S, R> x_xi(R(sub<S>(x1, x0)), R(sub<S>(x2, x3))), y_xi(R(sub<S>(y1, y0)), R(sub<S>(y2, y3)));
+    const MetricLine<S, R> x_eta(R(sub<S>(x3, x0)), R(sub<S>(x2, x1))), y_eta(R(sub<S>(y3, y0)), R(sub<S>(y2, y1)));
     if (active) {
         const R tm = xn[m];
         if (f == 2) {
@@ -591,14 +605,14 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     if (active) {
         const int j = m;
         R col[n];
-        const double* P = qs + (0 * EPB + e) * NN + j;
-        const double* U = qs + (1 * EPB + e) * NN + j;
-        const double* V = qs + (2 * EPB + e) * NN + j;
+        const R* P = qv + (0 * EPB + e) * NN + j;
+        const R* U = qv + (1 * EPB + e) * NN + j;
+        const R* V = qv + (2 * EPB + e) * NN + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-            if (f == 0) col[i] = sub<S>(mul<S>(y_eta(xn[i]), R(U[i * n])), mul<S>(x_eta(xn[i]), R(V[i * n])));
-            else if (f == 1) col[i] = mul<S>(y_eta(xn[i]), R(P[i * n]));
-            else col[i] = -mul<S>(x_eta(xn[i]), R(P[i * n]));
+            if (f == 0) col[i] = sub<S>(mul<S>(y_eta(xn[i]), U[i * n]), mul<S>(x_eta(xn[i]), V[i * n]));
+            else if (f == 1) col[i] = mul<S>(y_eta(xn[i]), P[i * n]);
+            else col[i] = -mul<S>(x_eta(xn[i]), P[i * n]);
         }
         const R fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
         R* G = gs + (f * EPB + e) * NN + j;
@@ -617,14 +631,14 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     if (active) {
         const int i = m;
         R line[n];
-        const double* P = qs + (0 * EPB + e) * NN + i * n;
-        const double* U = qs + (1 * EPB + e) * NN + i * n;
-        const double* V = qs + (2 * EPB + e) * NN + i * n;
+        const R* P = qv + (0 * EPB + e) * NN + i * n;
+        const R* U = qv + (1 * EPB + e) * NN + i * n;
+        const R* V = qv + (2 * EPB + e) * NN + i * n;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            if (f == 0) line[j] = add<S>(mul<S>(-y_xi(xn[j]), R(U[j])), mul<S>(x_xi(xn[j]), R(V[j])));
-            else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), R(P[j]));
-            else line[j] = mul<S>(x_xi(xn[j]), R(P[j]));
+            if (f == 0) line[j] = add<S>(mul<S>(-y_xi(xn[j]), U[j]), mul<S>(x_xi(xn[j]), V[j]));
+            else if (f == 1) line[j] = mul<S>(-y_xi(xn[j]), P[j]);
+            else line[j] = mul<S>(x_xi(xn[j]), P[j]);
         }
         const R ftp = F[2 * n + (N - i)], fbm = F[0 * n + i];
         R* G = gs + (f * EPB + e) * NN + i * n;
@@ -653,6 +667,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
         k[gi] = kn;
         q[gi] = qn;
         qs[(ff * EPB + ee) * NN + node] = qn;
+        if constexpr (T::kCopy) qw[(ff * EPB + ee) * NN + node] = R(qn);
         if (a.G_out) a.G_out[inst * 3 * fb + gi] = G;
     }
     __syncthreads();
@@ -669,10 +684,10 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
         R* out = tr_out + eo1[ee] + s * n + mm;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const double* qe = qs + (c * EPB + ee) * NN + b0;
+            const R* qe = qv + (c * EPB + ee) * NN + b0;
             R acc = 0;
 #pragma unroll
-            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], R(qe[j * stride]));
+            for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], qe[j * stride]);
             out[c * ft] = acc;
         }
     }
@@ -904,10 +919,11 @@ cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* group
 cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, bool fp32, cudaStream_t stream) {
     const int64_t n_ghosts = a.m.n_total - a.m.n_domain;
     if (n_ghosts == 0) return cudaSuccess;
-    const int blocks = grid_for(n_ghosts * a.n_instances, 128);
-    if (fp32) general_ghosts_kernel<false, float><<<blocks, 128, 0, stream>>>(a);
-    else if (strict) general_ghosts_kernel<true, double><<<blocks, 128, 0, stream>>>(a);
-    else general_ghosts_kernel<false, double><<<blocks, 128, 0, stream>>>(a);
+    const int max_n = a.m.max_n;
+    const int blocks = grid_for(n_ghosts * max_n * a.n_instances, 128);
+    if (fp32) general_ghosts_kernel<false, float><<<blocks, 128, 0, stream>>>(a, max_n);
+    else if (strict) general_ghosts_kernel<true, double><<<blocks, 128, 0, stream>>>(a, max_n);
+    else general_ghosts_kernel<false, double><<<blocks, 128, 0, stream>>>(a, max_n);
     return cudaGetLastError();
 }
 

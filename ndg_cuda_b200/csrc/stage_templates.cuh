@@ -380,7 +380,9 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
         for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
     }
     for (int i = tid; i < NN; i += T::kThreads) zs[i] = 0.0f;
-    float x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    // Corners in FP64: their differences are formed before rounding to FP32
+    // (on a fine mesh a difference is far smaller than the coordinates).
+    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
@@ -389,11 +391,10 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
             far_s[f * FS + (e * 4 + s) * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
-        x0 = static_cast<float>(c[0]); y0 = static_cast<float>(c[1]); x1 = static_cast<float>(c[2]); y1 = static_cast<float>(c[3]);
-        x2 = static_cast<float>(c[4]); y2 = static_cast<float>(c[5]); x3 = static_cast<float>(c[6]); y3 = static_cast<float>(c[7]);
+        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
     }
-    const MetricLineF x_xi(x1 - x0, x2 - x3), y_xi(y1 - y0, y2 - y3);
-    const MetricLineF x_eta(x3 - x0, x2 - x1), y_eta(y3 - y0, y2 - y1);
+    const MetricLineF x_xi(static_cast<float>(x1 - x0), static_cast<float>(x2 - x3)), y_xi(static_cast<float>(y1 - y0), static_cast<float>(y2 - y3));
+    const MetricLineF x_eta(static_cast<float>(x3 - x0), static_cast<float>(x2 - x1)), y_eta(static_cast<float>(y3 - y0), static_cast<float>(y2 - y1));
     if (active) {
         const float tm = xn[m];
         if (f == 2) {
