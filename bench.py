@@ -431,6 +431,21 @@ def adjoint_leg(local: int, stream, peak: float, cpu_sample: bool) -> dict:
     return out
 
 
+def job_rate(local_ms: float, local_units: float, dist, device: str) -> tuple[float, float]:
+    """Replicas: the slowest rank's device time (max over ranks) and the
+    whole-job rate, the units all ranks processed over that time. `dist` is
+    torch.distributed (or None for one process); tensors live on `device`
+    (cuda for NCCL, cpu for gloo)."""
+    import torch
+    ms = torch.tensor([local_ms], dtype=torch.float64, device=device)
+    units = torch.tensor([local_units], dtype=torch.float64, device=device)
+    if dist is not None and dist.is_initialized():
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        dist.all_reduce(units, op=dist.ReduceOp.SUM)
+    ms_max = float(ms.item())
+    return ms_max, float(units.item()) / (ms_max / 1e3)
+
+
 def run_ours(args) -> None:
     import torch
     import ndg_cuda_b200 as ndg
@@ -470,12 +485,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         launches = mesh.launches() - launches0
         barrier()
-    ms = start.elapsed_time(stop)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * dof * 3 * args.steps / (ms_max / 1e3)
+    ms_max, value = job_rate(start.elapsed_time(stop), dof * 3 * args.steps, dist, "cuda")
 
     # Roofline of the dominant kernel: the fused stage kernel, timed per launch.
     stage_ms = mesh.time_stage(1, 30)
