@@ -138,14 +138,16 @@ def measured_hbm_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profiled_traffic() -> float | None:
-    """DRAM bytes per stage-kernel launch from the committed ncu summary."""
+def profiled_traffic(tile: int = 0) -> float | None:
+    """DRAM bytes per stage-kernel launch of the tile in use (0: the default)
+    from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.txt")
+    key = f"N{ORDER}_res{RES}" + (f"_tile{tile}" if tile else "")
     try:
         with open(path) as f:
             for line in f:
                 parts = line.split()
-                if len(parts) == 2 and parts[0] == f"N{ORDER}_res{RES}":
+                if len(parts) == 2 and parts[0] == key:
                     return float(parts[1])
     except (OSError, ValueError):
         pass
@@ -491,7 +493,7 @@ def run_ours(args) -> None:
     stage_ms = mesh.time_stage(1, 30)
     achieved = BYTES_PER_DOF_STAGE * dof / (stage_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm_peak()
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(tile)
 
     # End to end through the C ABI with pinned host buffers.
     e2e_steps = 0 if args.no_e2e else 2
