@@ -488,6 +488,7 @@ def run_ours(args) -> None:
         launches = mesh.launches() - launches0
         barrier()
     ms_max, value = job_rate(start.elapsed_time(stop), dof * 3 * args.steps, dist, "cuda")
+    dt_step = ndg.Solver2D_t.get_delta_t(mesh)  # simulated time per RK3 step
 
     # Roofline of the dominant kernel: the fused stage kernel, timed per launch.
     stage_ms = mesh.time_stage(1, 30)
@@ -558,6 +559,7 @@ def run_ours(args) -> None:
                 "ms_per_step": float(f_ms.item()) / args.steps, "kernel": f"stage_kernel_f32<{ORDER}>", "kernel_ms": stage32_ms,
                 "roofline_frac": BYTES_PER_DOF_STAGE * dof / (stage32_ms / 1e3) / 1e9 / peak,
                 "rel_l2_vs_fp64": err, "steps_compared": CONFIG_STEPS, "tile_elements_per_cta": tile32 or m32.tile_candidates()[1],
+                "wall_time_per_unit_time_s": float(f_ms.item()) / args.steps / 1e3 / dt_step,
                 "arithmetic": "traces, fluxes, metrics and volume term in FP32; q, k and the RK update in FP64"}
         m32.close()
 
@@ -583,6 +585,9 @@ def run_ours(args) -> None:
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (reference plane-wave initial condition on a generated mesh)",
                 "config": config(),
+                "simulated_time_per_step": dt_step,
+                "wall_time_per_unit_time_s": {"device_fp64": ms_max / args.steps / 1e3 / dt_step,
+                                              "e2e_fp64": (float(e2e_t.item()) / 1e3 / (CONFIG_STEPS * e2e_steps) / dt_step) if e2e_steps else None},
                 "e2e": {"value": e2e_value, "unit": "DOF-stage updates/s", "h2d_bytes_per_step": state_bytes,
                         "d2h_bytes_per_step": state_bytes, "rk3_steps_per_e2e_step": CONFIG_STEPS, "e2e_steps": e2e_steps,
                         "host_wall_s": wall},
