@@ -236,8 +236,8 @@ ndg_status ndg_adapt_flags(ndg_ctx* ctx, const int32_t* refine, const double* p_
 ndg_status ndg_time_stage(ndg_ctx* ctx, int32_t m, int32_t n_launches, double* avg_ms);
 
 /* Autotuner (no reference counterpart). The uniform-order stage kernel is
- * compiled for several tiles (elements per CTA: 2, 4, 6, 8, 12, 16 where a
- * tile fits 512 threads and 113 KB of shared memory) besides its default.
+ * compiled for several tiles (elements per CTA: 2, 4, 8, 16 where a tile
+ * fits 512 threads and 113 KB of shared memory) besides its default.
  * ndg_autotune times n_launches launches of each tile, and of the default,
  * on the loaded mesh and instances in the context's current form (FP64 or
  * FP32), keeps the fastest for later stepping and returns it (0 = the

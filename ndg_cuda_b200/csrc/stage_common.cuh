@@ -134,10 +134,160 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned* error, uint64
 
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 
+// 8-byte asynchronous copy global -> shared (cp.async, no register staging)
+// and the wait for all of this thread's copies.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
-// Tile of the fused stage: E elements per CTA (E even), or for E = 0 the
-// default: as many as fit ~60 KB of shared memory (several CTAs per SM) and
-// 256 threads.
+// Shared-memory placement of the uniform-order stage tiles without bank
+// conflicts.
+//
+// The stage kernels order their line threads as (field f, line m, element
+// e) with e fastest, so one shared-memory wavefront's group of G threads
+// (G = 16 for 8-byte values, 32 for 4-byte values: 128 bytes either way)
+// holds G / EPB consecutive lines of every element of the tile. A row sweep
+// reads node (m, j) of each thread's element and a column sweep node
+// (j, m), with j in lockstep. Node (i, j) of element e of field f sits at
+// f QS + e ES + i P + j, and two threads of a group conflict when their
+// addresses differ by a nonzero multiple of G. So:
+//   P       the row pitch, odd: n, or n + 1 when n is even;
+//   ES      the element stride: the first value in [n P, n P + G) with the
+//           fewest wavefronts of the row and column sweeps over the groups
+//           that lie in one field;
+//   QS, Z   the field stride, in [EPB ES, EPB ES + G), and the residue of
+//           the zero array's offset, for the groups that straddle two
+//           fields (own-field sweeps and the flux-line reads of the other
+//           fields and of the zero array);
+//   SE, FS  element and field strides of the side arrays (4 n values per
+//           element, value m of side s at s n + m), the same way.
+// Every candidate's wavefront count is evaluated exactly, group by group,
+// at compile time. EPB must divide G (whole lines per group).
+namespace bank {
+
+struct Strides {
+    int P, ES, QS, Z, SE, FS;
+};
+
+enum Pattern : int { kRowOwn, kColOwn, kRowX, kColX, kRowY, kColY, kSideOwn, kSideFlux0, kSideFlux1, kSideFlux2 };
+
+// Address (in values) read by thread (f, e, m) in one instruction of a
+// pattern. The flux lines take X = u, p, 0 and Y = v, 0, p for f = 0, 1, 2;
+// the zero array starts at Z.
+constexpr int address(int pat, const Strides& L, int n, int f, int e, int m) {
+    switch (pat) {
+        case kRowOwn: return f * L.QS + e * L.ES + m * L.P;
+        case kColOwn: return f * L.QS + e * L.ES + m;
+        case kRowX: return f == 0 ? L.QS + e * L.ES + m * L.P : (f == 1 ? e * L.ES + m * L.P : L.Z + m * L.P);
+        case kColX: return f == 0 ? L.QS + e * L.ES + m : (f == 1 ? e * L.ES + m : L.Z + m);
+        case kRowY: return f == 0 ? 2 * L.QS + e * L.ES + m * L.P : (f == 1 ? L.Z + m * L.P : e * L.ES + m * L.P);
+        case kColY: return f == 0 ? 2 * L.QS + e * L.ES + m : (f == 1 ? L.Z + m : e * L.ES + m);
+        case kSideOwn: return f * L.FS + e * L.SE + m;
+        default: return (pat - kSideFlux0) * L.FS + e * L.SE + f * n + m;  // all threads read field pat - kSideFlux0 of side f
+    }
+}
+
+// Wavefronts of one instruction in the group of threads [g0, g0 + G): the
+// most distinct addresses that share a bank. Zero-array reads of elements
+// e > 0 repeat element 0's address on the same line (a broadcast) and are
+// skipped.
+constexpr int group_wavefronts(int pat, const Strides& L, int n, int EPB, int G, int g0) {
+    int bank[32] = {};
+    int worst = 0;
+    for (int t = g0; t < g0 + G; ++t) {
+        const int f = t / (EPB * n);
+        if (f >= 3) break;
+        const int rr = t - f * EPB * n, m = rr / EPB, e = rr - m * EPB;
+        const bool zero = (pat == kRowX || pat == kColX) ? f == 2 : ((pat == kRowY || pat == kColY) ? f == 1 : false);
+        if (zero && e > 0) continue;
+        const int b = address(pat, L, n, f, e, m) % G;
+        if (++bank[b] > worst) worst = bank[b];
+    }
+    return worst;
+}
+
+// Sum over the groups within one field (straddling = false) or over the (at
+// most two) groups that hold a field boundary (straddling = true).
+constexpr int wavefronts(int pat, const Strides& L, int n, int EPB, int G, bool straddling) {
+    const int field = EPB * n;
+    const int b1 = field / G * G, b2 = 2 * field / G * G;
+    const bool s1 = field % G != 0, s2 = (2 * field) % G != 0;
+    if (straddling) return (s1 ? group_wavefronts(pat, L, n, EPB, G, b1) : 0) + (s2 && b2 != b1 ? group_wavefronts(pat, L, n, EPB, G, b2) : 0);
+    int total = 0;
+    for (int g0 = 0; g0 < 3 * field; g0 += G)
+        if (!((s1 && g0 == b1) || (s2 && g0 == b2))) total += group_wavefronts(pat, L, n, EPB, G, g0);
+    return total;
+}
+
+constexpr int straddling_q_cost(const Strides& L, int n, int EPB, int G) {
+    int c = 0;
+    for (int p = kRowOwn; p <= kColOwn; ++p) c += 2 * wavefronts(p, L, n, EPB, G, true);  // traces and G sweeps
+    for (int p = kRowX; p <= kColY; ++p) c += wavefronts(p, L, n, EPB, G, true);
+    return c;
+}
+
+constexpr Strides search(int N, int EPB, int G) {
+    const int n = N + 1;
+    Strides L{n % 2 ? n : n + 1, 0, 0, 0, 0, 0};
+    int best = 1 << 30;
+    for (int s = n * L.P; s < n * L.P + G; ++s) {
+        Strides T = L;
+        T.ES = s;
+        T.QS = EPB * s;
+        const int c = wavefronts(kRowOwn, T, n, EPB, G, false) + wavefronts(kColOwn, T, n, EPB, G, false);
+        if (c < best) best = c, L.ES = s;
+    }
+    best = 1 << 30;
+    for (int s = 4 * n; s < 4 * n + G; ++s) {
+        Strides T = L;
+        T.SE = s;
+        T.FS = EPB * s;
+        const int c = wavefronts(kSideOwn, T, n, EPB, G, false);
+        if (c < best) best = c, L.SE = s;
+    }
+    best = 1 << 30;
+    for (int s = EPB * L.ES; s < EPB * L.ES + G; ++s) {
+        Strides T = L;
+        T.QS = s;
+        T.Z = 0;
+        const int c = straddling_q_cost(T, n, EPB, G);
+        if (c < best) best = c, L.QS = s;
+    }
+    best = 1 << 30;
+    for (int z = 0; z < G; ++z) {
+        Strides T = L;
+        T.Z = z;
+        const int c = straddling_q_cost(T, n, EPB, G);
+        if (c < best) best = c, L.Z = z;
+    }
+    best = 1 << 30;
+    for (int s = EPB * L.SE; s < EPB * L.SE + G; ++s) {
+        Strides T = L;
+        T.FS = s;
+        int c = wavefronts(kSideOwn, T, n, EPB, G, true);
+        for (int p = kSideFlux0; p <= kSideFlux2; ++p) c += wavefronts(p, T, n, EPB, G, true);
+        if (c < best) best = c, L.FS = s;
+    }
+    return L;
+}
+
+// First offset >= at whose residue modulo G is z.
+constexpr int place(int at, int z, int G) { return at + ((z - at % G) % G + G) % G; }
+
+constexpr int pow2_floor(int v) {
+    int p = 1;
+    while (2 * p <= v) p *= 2;
+    return p;
+}
+
+}  // namespace bank
+
+// ---------------------------------------------------------------------------
+// Tile of the fused stage: E elements per CTA (2, 4, 8 or 16), or for E = 0
+// the default: the largest power of two of elements that fits ~60 KB of
+// shared memory (several CTAs per SM) and 256 threads.
 template <int N, int E = 0>
 struct Tile {
     static constexpr int n = N + 1;
@@ -146,22 +296,38 @@ struct Tile {
     static constexpr int by_smem = (60 * 1024 / 8) / per_element_doubles;
     static constexpr int by_threads = 256 / (3 * n);
     static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
-    static constexpr int EPB = E > 0 ? E : (raw >= 2 ? (raw & ~1) : 2);
-    static_assert(EPB % 2 == 0, "tiles hold an even number of elements (aligned bulk copies)");
+    static constexpr int EPB = E > 0 ? E : bank::pow2_floor(raw >= 2 ? (raw < 16 ? raw : 16) : 2);
+    static_assert(EPB == 2 || EPB == 4 || EPB == 8 || EPB == 16, "tiles hold 2, 4, 8 or 16 elements (whole lines per wavefront group)");
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
-    // Node-wise work per thread in the RK phase: ceil(3 EPB NN / threads).
+    // Node-wise work per thread in an RK phase over the whole tile: ceil(3 EPB NN / threads).
     static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;
-    // shared memory layout (doubles); the bulk-copied q tile first
-    static constexpr int kQ = 0;                         // [3][EPB][NN] q, then q of the next stage
-    static constexpr int kG = kQ + 3 * EPB * NN;         // [3][EPB][NN] time derivative G
-    static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n] own side traces
-    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far side traces, then side fluxes
-    static constexpr int kJ = kFar + 3 * EPB * 4 * n;    // [EPB][NN] 1/J (J in strict mode)
-    static constexpr int kS = kJ + EPB * NN;             // [EPB][4] edge metric per side
-    static constexpr int kZ = kS + EPB * 4;              // [NN] zeros: the absent flux component
-    static constexpr int kBar = kZ + NN;                 // mbarrier (8 bytes)
-    static constexpr int kDoubles = kBar + 2;
+    // Node-wise phases of the stage kernels (tile copy, RK update): warp w
+    // takes the (field, element) blocks w, w + kWarps, ... and its lanes the
+    // nodes of a block, so no per-node division is needed.
+    static constexpr int kWarps = kThreads / 32;
+    static constexpr int kBlockIters = (3 * EPB + kWarps - 1) / kWarps;
+    static constexpr int kLaneIters = (NN + 31) / 32;
+    static constexpr bank::Strides L = bank::search(N, EPB, 16);
+    static constexpr int P = L.P, ES = L.ES, QS = L.QS, SE = L.SE, FS = L.FS;
+    // shared memory layout (doubles)
+    static constexpr int kQ = 0;                        // [3][QS] q, then q of the next stage
+    static constexpr int kG = kQ + 3 * QS;              // [3][QS] time derivative G
+    static constexpr int kOwn = kG + 3 * QS;            // [3][FS] own side traces
+    static constexpr int kFar = kOwn + 3 * FS;          // [3][FS] far side traces, then side fluxes
+    static constexpr int kJ = kFar + 3 * FS;            // [EPB][ES] 1/J (J in strict mode)
+    static constexpr int kS = kJ + EPB * ES;            // [EPB][4] edge metric per side
+    static constexpr int kZ = bank::place(kS + EPB * 4, L.Z, 16);  // [n P] zeros: the absent flux component
+    static constexpr int kDoubles = kZ + n * P;
     static constexpr size_t kBytes = sizeof(double) * kDoubles;
+    // Offset within an element of node nd = i n + j.
+    __device__ static __forceinline__ int node(int nd) {
+        if constexpr (P == n) {
+            return nd;
+        } else {
+            const int i = nd / n;
+            return i * P + (nd - i * n);
+        }
+    }
 };
 
 // Coefficients of order N, passed by value as a kernel parameter so that

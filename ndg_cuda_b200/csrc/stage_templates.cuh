@@ -20,8 +20,10 @@ template <int N, bool S, int E>
 __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a, const __grid_constant__ Coeffs<N> cf) {
     using T = Tile<N, E>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
+    // padded strides of the tile (Tile): row pitch, element and field strides
+    // of node arrays, element and field strides of side arrays
+    constexpr int P = T::P, ES = T::ES, QS = T::QS, SE = T::SE, FS = T::FS;
     extern __shared__ __align__(128) double smem[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T::kBar);
     double* qs = smem + T::kQ;
     double* gs = smem + T::kG;
     double* own_s = smem + T::kOwn;
@@ -29,14 +31,12 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
     double* js = smem + T::kJ;
     double* ss = smem + T::kS;
     double* zs = smem + T::kZ;
-    constexpr int FS = EPB * 4 * n;  // field stride of own_s / far_s
 
     const int tid = threadIdx.x;
     const int64_t K = a.n_elements;
     const int64_t Kp = a.field_stride;  // elements per field block (K rounded up to even)
     const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
     const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
-    const int ne_copy = (ne + 1) & ~1;  // the tile copy moves an even number of elements
     const int64_t inst = blockIdx.y;
     double* q = a.q + inst * 3 * Kp * NN;
     double* k = a.k + inst * 3 * Kp * NN;
@@ -48,23 +48,34 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
     const double time = a.step[0];
     const double dt = a.step[1];
 
-    // Line threads: (field f, element e of the tile, line or node index m).
+    // Line threads: (field f, line or node index m, element e of the tile),
+    // e fastest (the order the bank-conflict-free strides assume).
     const int f = tid / (EPB * n);
     const int rr = tid - f * (EPB * n);
-    const int e = rr / n;
-    const int m = rr - e * n;
+    const int m = rr / EPB;
+    const int e = rr - m * EPB;
     const bool active = f < 3 && e < ne;
     const int64_t ge = e0 + e;
 
-    // Prologue: one bulk copy per field brings the q tile into shared memory.
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-        const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
-        mbar_expect_tx(bar, 3 * bytes);
-        for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
+    // Prologue: 8-byte asynchronous copies place the q tile in the padded
+    // layout (coalesced reads; a padded tile is not one contiguous range).
+    // Warps take (field, element) blocks, lanes their nodes.
+    const int warp = tid >> 5, lane = tid & 31;
+    int lane_node[T::kLaneIters];  // padded offsets of this lane's nodes within an element
+#pragma unroll
+    for (int it = 0; it < T::kLaneIters; ++it) lane_node[it] = T::node(lane + 32 * it);
+#pragma unroll
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const double* src = q + (ff * Kp + e0 + el) * NN;
+            double* dst = qs + ff * QS + el * ES;
+#pragma unroll
+            for (int it = 0; it < T::kLaneIters; ++it)
+                if (lane + 32 * it < NN) cp_async8(dst + lane_node[it], src + lane + 32 * it);
+        }
     }
-    for (int i = tid; i < NN; i += T::kThreads) zs[i] = 0.0;
+    for (int i = tid; i < n * P; i += T::kThreads) zs[i] = 0.0;
     // Far traces of this thread's field at node m of the four sides (the
     // neighbour's trace of the previous stage), element metrics, edge
     // metrics and J.
@@ -74,7 +85,7 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
         for (int s = 0; s < 4; ++s) {
             const int2 lk = a.link[4 * ge + s];
             const double v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0;
-            far_s[f * FS + (e * 4 + s) * n + m] = v;
+            far_s[f * FS + e * SE + s * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
         x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
@@ -101,31 +112,31 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
         for (int j = f; j < n; j += 3) {
             const double tj = xn[j];
             const double jac = sub<S>(mul<S>(x_xi(tj), ye), mul<S>(xe, y_xi(tj)));
-            js[e * NN + m * n + j] = S ? jac : __drcp_rn(jac);
+            js[e * ES + m * P + j] = S ? jac : __drcp_rn(jac);
         }
     }
-    __syncthreads();  // mbarrier init, zeros, far traces, edge metrics, J
-    if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
+    cp_async_wait_all();
+    __syncthreads();  // q tile, zeros, far traces, edge metrics, J
 
     // Own side traces of this thread's field (Element2D_t.cpp:86-125):
     // bottom and top from row m, right and left from column m.
     // The flux lines take (X, Y) = (u, v), (p, 0), (0, p) for f = 0, 1, 2:
     // x_flux = (c u, p, 0), y_flux = (c v, 0, p) (Solver2D_t.cpp:31-37).
-    const double* Qe = qs + e * NN;
-    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : (f == 1 ? Qe : zs);
-    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : (f == 1 ? zs : Qe);
+    const double* Qe = qs + e * ES;
+    const double* Xe = f == 0 ? Qe + 1 * QS : (f == 1 ? Qe : zs);
+    const double* Ye = f == 0 ? Qe + 2 * QS : (f == 1 ? zs : Qe);
     if (active) {
-        const double* Qf = Qe + f * EPB * NN;
+        const double* Qf = Qe + f * QS;
         double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            const double qr = Qf[m * n + j], qc = Qf[j * n + m];
+            const double qr = Qf[m * P + j], qc = Qf[j * P + m];
             b = madd<S>(b, lm[j], qr);
             t = madd<S>(t, lp[j], qr);
             r = madd<S>(r, lp[j], qc);
             l = madd<S>(l, lm[j], qc);
         }
-        double* o = own_s + f * FS + e * 4 * n;
+        double* o = own_s + f * FS + e * SE;
         o[0 * n + m] = b;
         o[2 * n + (N - m)] = t;
         o[1 * n + m] = r;
@@ -146,7 +157,7 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
             const int kind = (lk.y >> 2) & 7;
             const int role = (lk.y >> 5) & 1;
             const double2 nv = a.normal[4 * ge + s];
-            const int o = (e * 4 + s) * n + m;
+            const int o = e * SE + s * n + m;
             const double op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
             double fp_, fu_, fv_;
             if (kind == kInterior) {
@@ -200,7 +211,7 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
     const double* Dh = cf.dhat;
     const double* w = cf.w;
     const double* iw = cf.iw;
-    const double* F = far_s + f * FS + e * 4 * n;  // this thread's field, element side fluxes
+    const double* F = far_s + f * FS + e * SE;  // this thread's field, element side fluxes
 
     // xi pass (eta index j = m): contravariant flux line eta_y X - eta_x Y
     // (Solver2D_t.cpp:72-80), Dhat . line + lift, G = -(...) (:82-101); G column j.
@@ -208,16 +219,16 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
         const int j = m;
         double col[n];
 #pragma unroll
-        for (int i = 0; i < n; ++i) col[i] = sub<S>(mul<S>(y_eta(xn[i]), Xe[i * n + j]), mul<S>(x_eta(xn[i]), Ye[i * n + j]));
+        for (int i = 0; i < n; ++i) col[i] = sub<S>(mul<S>(y_eta(xn[i]), Xe[i * P + j]), mul<S>(x_eta(xn[i]), Ye[i * P + j]));
         const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
-        double* G = gs + (f * EPB + e) * NN + j;
+        double* G = gs + f * QS + e * ES + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             double acc = 0.0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[i * n + mm], col[mm]);
             const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
-            G[i * n] = -add<S>(acc, lift);
+            G[i * P] = -add<S>(acc, lift);
         }
     }
     __syncthreads();
@@ -228,10 +239,10 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
         const int i = m;
         double line[n];
 #pragma unroll
-        for (int j = 0; j < n; ++j) line[j] = add<S>(mul<S>(-y_xi(xn[j]), Xe[i * n + j]), mul<S>(x_xi(xn[j]), Ye[i * n + j]));
+        for (int j = 0; j < n; ++j) line[j] = add<S>(mul<S>(-y_xi(xn[j]), Xe[i * P + j]), mul<S>(x_xi(xn[j]), Ye[i * P + j]));
         const double ft = F[2 * n + (N - i)], fb = F[0 * n + i];
-        double* G = gs + (f * EPB + e) * NN + i * n;
-        const double* jrow = js + e * NN + i * n;
+        double* G = gs + f * QS + e * ES + i * P;
+        const double* jrow = js + e * ES + i * P;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             double acc = 0.0;
@@ -245,28 +256,37 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
     __syncthreads();
 
     // Low-storage RK3 update (Solver2D_t.cpp:138-172), node by node:
-    // coalesced reads of k (prefetched) and writes of k and q.
+    // coalesced reads of k (all prefetched) and writes of k and q.
     const double gdt = mul<S>(a.rk_g, dt);
-    double kold[T::kNodeIters];
+    double kold[T::kBlockIters][T::kLaneIters];
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        kold[c] = (!a.first && ff < 3 && r < ne * NN) ? k[(ff * Kp + e0) * NN + r] : 0.0;
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        const bool live = !a.first && b < 3 * EPB && el < ne;
+        const double* kb = k + (ff * Kp + e0 + el) * NN;
+#pragma unroll
+        for (int it = 0; it < T::kLaneIters; ++it) kold[bi][it] = (live && lane + 32 * it < NN) ? kb[lane + 32 * it] : 0.0;
     }
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        if (ff < 3 && r < ne * NN) {
-            const double G = gs[ff * EPB * NN + r];
-            const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, kold[c]), G);
-            const double qn = add<S>(qs[ff * EPB * NN + r], mul<S>(gdt, kn));
-            const int64_t gi = (ff * Kp + e0) * NN + r;
-            k[gi] = kn;
-            q[gi] = qn;
-            qs[ff * EPB * NN + r] = qn;
-            if (a.G_out) a.G_out[inst * 3 * Kp * NN + gi] = G;
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const int64_t gb = (ff * Kp + e0 + el) * NN;
+            const int sb = ff * QS + el * ES;
+#pragma unroll
+            for (int it = 0; it < T::kLaneIters; ++it) {
+                const int nd = lane + 32 * it;
+                if (nd < NN) {
+                    const int sn = sb + lane_node[it];
+                    const double G = gs[sn];
+                    const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, kold[bi][it]), G);
+                    const double qn = add<S>(qs[sn], mul<S>(gdt, kn));
+                    k[gb + nd] = kn;
+                    q[gb + nd] = qn;
+                    qs[sn] = qn;
+                    if (a.G_out) a.G_out[inst * 3 * Kp * NN + gb + nd] = G;
+                }
+            }
         }
     }
     __syncthreads();
@@ -274,15 +294,15 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
     // Side traces of the new solution for the next stage: bottom/top from
     // row m, right/left from column m (Element2D_t.cpp:86-125).
     if (active) {
-        const double* row = qs + (f * EPB + e) * NN + m * n;
-        const double* cl = qs + (f * EPB + e) * NN + m;
+        const double* row = qs + f * QS + e * ES + m * P;
+        const double* cl = qs + f * QS + e * ES + m;
         double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             b = madd<S>(b, lm[j], row[j]);
             t = madd<S>(t, lp[j], row[j]);
-            r = madd<S>(r, lp[j], cl[j * n]);
-            l = madd<S>(l, lm[j], cl[j * n]);
+            r = madd<S>(r, lp[j], cl[j * P]);
+            l = madd<S>(l, lm[j], cl[j * P]);
         }
         double* to = tr_out + (f * Kp + ge) * 4 * n;
         to[0 * n + m] = b;
@@ -311,17 +331,30 @@ struct TileF {
     static constexpr int EPB = Tile<N, E>::EPB;
     static constexpr int kThreads = Tile<N, E>::kThreads;
     static constexpr int kNodeIters = Tile<N, E>::kNodeIters;
+    // bank-conflict-free strides of the FP32 arrays (32 four-byte values per wavefront)
+    static constexpr bank::Strides L = bank::search(N, EPB, 32);
+    static constexpr int P = L.P, ES = L.ES, QS = L.QS, SE = L.SE, FS = L.FS;
     // the bulk-copied FP64 q tile, then FP32 arrays (offsets in floats past it)
     static constexpr int kQd = 3 * EPB * NN;             // doubles
-    static constexpr int kQf = 0;                        // [3][EPB][NN] q in FP32
-    static constexpr int kG = kQf + 3 * EPB * NN;        // [3][EPB][NN]
-    static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n]
-    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far traces, then side fluxes
-    static constexpr int kJ = kFar + 3 * EPB * 4 * n;    // [EPB][NN] 1/J
-    static constexpr int kS = kJ + EPB * NN;             // [EPB][4]
-    static constexpr int kZ = kS + EPB * 4;              // [NN] zeros
-    static constexpr int kFloats = (kZ + NN + 3) / 4 * 4;  // keeps the mbarrier 16-byte aligned
+    static constexpr int kQf = 0;                        // [3][QS] q in FP32
+    static constexpr int kG = kQf + 3 * QS;              // [3][QS]
+    static constexpr int kOwn = kG + 3 * QS;             // [3][FS]
+    static constexpr int kFar = kOwn + 3 * FS;           // [3][FS] far traces, then side fluxes
+    static constexpr int kJ = kFar + 3 * FS;             // [EPB][ES] 1/J
+    static constexpr int kS = kJ + EPB * ES;             // [EPB][4]
+    static constexpr int kZ = bank::place(kS + EPB * 4, L.Z, 32);  // [n P] zeros
+    static constexpr int kFloats = (kZ + n * P + 3) / 4 * 4;  // keeps the mbarrier 16-byte aligned
     static constexpr size_t kBytes = sizeof(double) * kQd + sizeof(float) * kFloats + 16;
+    // Offset within a field of node r = e NN + i n + j of the tile's elements.
+    __device__ static __forceinline__ int node(int r) {
+        const int el = r / NN, nd = r - el * NN;
+        if constexpr (P == n) {
+            return el * ES + nd;
+        } else {
+            const int i = nd / n;
+            return el * ES + i * P + (nd - i * n);
+        }
+    }
 };
 
 // ((1 - t) d0 + (1 + t) d1) / 4 as fma(t, (d1 - d0) / 4, (d0 + d1) / 4) in FP32.
@@ -335,6 +368,7 @@ template <int N, int E>
 __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageArgs a, const __grid_constant__ CoeffsF<N> cf) {
     using T = TileF<N, E>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
+    constexpr int P = T::P, ES = T::ES, QS = T::QS, SE = T::SE, FS = T::FS;
     extern __shared__ __align__(128) double smem[];
     double* qs = smem;
     float* fsm = reinterpret_cast<float*>(smem + T::kQd);
@@ -346,7 +380,6 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
     float* ss = fsm + T::kS;
     float* zs = fsm + T::kZ;
     uint64_t* bar = reinterpret_cast<uint64_t*>(fsm + T::kFloats);
-    constexpr int FS = EPB * 4 * n;
 
     const int tid = threadIdx.x;
     const int64_t K = a.n_elements;
@@ -367,8 +400,8 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
 
     const int f = tid / (EPB * n);
     const int rr = tid - f * (EPB * n);
-    const int e = rr / n;
-    const int m = rr - e * n;
+    const int m = rr / EPB;
+    const int e = rr - m * EPB;
     const bool active = f < 3 && e < ne;
     const int64_t ge = e0 + e;
 
@@ -379,7 +412,7 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
         mbar_expect_tx(bar, 3 * bytes);
         for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
     }
-    for (int i = tid; i < NN; i += T::kThreads) zs[i] = 0.0f;
+    for (int i = tid; i < n * P; i += T::kThreads) zs[i] = 0.0f;
     // Corners in FP64: their differences are formed before rounding to FP32
     // (on a fine mesh a difference is far smaller than the coordinates).
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
@@ -388,7 +421,7 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
         for (int s = 0; s < 4; ++s) {
             const int2 lk = a.link[4 * ge + s];
             const float v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0f;
-            far_s[f * FS + (e * 4 + s) * n + m] = v;
+            far_s[f * FS + e * SE + s * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
         x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
@@ -408,29 +441,43 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
         const float xe = x_eta(tm), ye = y_eta(tm);
         for (int j = f; j < n; j += 3) {
             const float tj = xn[j];
-            js[e * NN + m * n + j] = __frcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
+            js[e * ES + m * P + j] = __frcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
         }
     }
     __syncthreads();
     if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
-    for (int i = tid; i < 3 * EPB * NN; i += T::kThreads) qf[i] = static_cast<float>(qs[i]);
+    // FP32 copy of the tile in the padded layout: warps take (field,
+    // element) blocks, lanes their nodes.
+    const int warp = tid >> 5, lane = tid & 31;
+    int lane_node[Tile<N, E>::kLaneIters];  // padded offsets of this lane's nodes within an element
+#pragma unroll
+    for (int it = 0; it < Tile<N, E>::kLaneIters; ++it) lane_node[it] = T::node(lane + 32 * it);
+#pragma unroll
+    for (int bi = 0; bi < Tile<N, E>::kBlockIters; ++bi) {
+        const int b = warp + bi * Tile<N, E>::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+#pragma unroll
+            for (int it = 0; it < Tile<N, E>::kLaneIters; ++it)
+                if (lane + 32 * it < NN) qf[ff * QS + el * ES + lane_node[it]] = static_cast<float>(qs[(ff * EPB + el) * NN + lane + 32 * it]);
+        }
+    }
     __syncthreads();
 
-    const float* Qe = qf + e * NN;
-    const float* Xe = f == 0 ? Qe + 1 * EPB * NN : (f == 1 ? Qe : zs);
-    const float* Ye = f == 0 ? Qe + 2 * EPB * NN : (f == 1 ? zs : Qe);
+    const float* Qe = qf + e * ES;
+    const float* Xe = f == 0 ? Qe + 1 * QS : (f == 1 ? Qe : zs);
+    const float* Ye = f == 0 ? Qe + 2 * QS : (f == 1 ? zs : Qe);
     if (active) {
-        const float* Qf = Qe + f * EPB * NN;
+        const float* Qf = Qe + f * QS;
         float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            const float qr = Qf[m * n + j], qc = Qf[j * n + m];
+            const float qr = Qf[m * P + j], qc = Qf[j * P + m];
             b = fmaf(lm[j], qr, b);
             t = fmaf(lp[j], qr, t);
             r = fmaf(lp[j], qc, r);
             l = fmaf(lm[j], qc, l);
         }
-        float* o = own_s + f * FS + e * 4 * n;
+        float* o = own_s + f * FS + e * SE;
         o[0 * n + m] = b;
         o[2 * n + (N - m)] = t;
         o[1 * n + m] = r;
@@ -447,7 +494,7 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
             const int role = (lk.y >> 5) & 1;
             const double2 nvd = a.normal[4 * ge + s];
             const float nx = static_cast<float>(nvd.x), ny = static_cast<float>(nvd.y);
-            const int o = (e * 4 + s) * n + m;
+            const int o = e * SE + s * n + m;
             const float op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
             float fp_, fu_, fv_;
             if (kind == kInterior) {
@@ -494,20 +541,20 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
 
     const float* Dh = cf.dhat;
     const float* iw = cf.iw;
-    const float* F = far_s + f * FS + e * 4 * n;
+    const float* F = far_s + f * FS + e * SE;
     if (active) {
         const int j = m;
         float col[n];
 #pragma unroll
-        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * Xe[i * n + j] - x_eta(xn[i]) * Ye[i * n + j];
+        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * Xe[i * P + j] - x_eta(xn[i]) * Ye[i * P + j];
         const float fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
-        float* G = gs + (f * EPB + e) * NN + j;
+        float* G = gs + f * QS + e * ES + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             float acc = 0.0f;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[i * n + mm], col[mm], acc);
-            G[i * n] = -(acc + (fr * lp[i] + fl3 * lm[i]) * iw[i]);
+            G[i * P] = -(acc + (fr * lp[i] + fl3 * lm[i]) * iw[i]);
         }
     }
     __syncthreads();
@@ -516,10 +563,10 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
         const int i = m;
         float line[n];
 #pragma unroll
-        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * Xe[i * n + j] + x_xi(xn[j]) * Ye[i * n + j];
+        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * Xe[i * P + j] + x_xi(xn[j]) * Ye[i * P + j];
         const float ft = F[2 * n + (N - i)], fb = F[0 * n + i];
-        float* G = gs + (f * EPB + e) * NN + i * n;
-        const float* jrow = js + e * NN + i * n;
+        float* G = gs + f * QS + e * ES + i * P;
+        const float* jrow = js + e * ES + i * P;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             float acc = 0.0f;
@@ -532,41 +579,51 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
 
     // RK3 update in FP64 (Solver2D_t.cpp:138-172); the new q also refreshes
     // the FP32 tile for the traces.
+    using U = Tile<N, E>;
     const double gdt = a.rk_g * dt;
-    double kold[T::kNodeIters];
+    double kold[U::kBlockIters][U::kLaneIters];
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        kold[c] = (!a.first && ff < 3 && r < ne * NN) ? k[(ff * Kp + e0) * NN + r] : 0.0;
+    for (int bi = 0; bi < U::kBlockIters; ++bi) {
+        const int b = warp + bi * U::kWarps, ff = b / EPB, el = b - ff * EPB;
+        const bool live = !a.first && b < 3 * EPB && el < ne;
+        const double* kb = k + (ff * Kp + e0 + el) * NN;
+#pragma unroll
+        for (int it = 0; it < U::kLaneIters; ++it) kold[bi][it] = (live && lane + 32 * it < NN) ? kb[lane + 32 * it] : 0.0;
     }
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        if (ff < 3 && r < ne * NN) {
-            const double G = static_cast<double>(gs[ff * EPB * NN + r]);
-            const double kn = a.first ? G : fma(a.rk_a, kold[c], G);
-            const double qn = fma(gdt, kn, qs[ff * EPB * NN + r]);
-            const int64_t gi = (ff * Kp + e0) * NN + r;
-            k[gi] = kn;
-            q[gi] = qn;
-            qf[ff * EPB * NN + r] = static_cast<float>(qn);
-            if (a.G_out) a.G_out[inst * 3 * Kp * NN + gi] = G;
+    for (int bi = 0; bi < U::kBlockIters; ++bi) {
+        const int b = warp + bi * U::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const int64_t gb = (ff * Kp + e0 + el) * NN;
+            const int sb = ff * QS + el * ES, db = (ff * EPB + el) * NN;
+#pragma unroll
+            for (int it = 0; it < U::kLaneIters; ++it) {
+                const int nd = lane + 32 * it;
+                if (nd < NN) {
+                    const int sn = sb + lane_node[it];
+                    const double G = static_cast<double>(gs[sn]);
+                    const double kn = a.first ? G : fma(a.rk_a, kold[bi][it], G);
+                    const double qn = fma(gdt, kn, qs[db + nd]);
+                    k[gb + nd] = kn;
+                    q[gb + nd] = qn;
+                    qf[sn] = static_cast<float>(qn);
+                    if (a.G_out) a.G_out[inst * 3 * Kp * NN + gb + nd] = G;
+                }
+            }
         }
     }
     __syncthreads();
 
     if (active) {
-        const float* row = qf + (f * EPB + e) * NN + m * n;
-        const float* cl = qf + (f * EPB + e) * NN + m;
+        const float* row = qf + f * QS + e * ES + m * P;
+        const float* cl = qf + f * QS + e * ES + m;
         float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             b = fmaf(lm[j], row[j], b);
             t = fmaf(lp[j], row[j], t);
-            r = fmaf(lp[j], cl[j * n], r);
-            l = fmaf(lm[j], cl[j * n], l);
+            r = fmaf(lp[j], cl[j * P], r);
+            l = fmaf(lm[j], cl[j * P], l);
         }
         float* to = tr_out + (f * Kp + ge) * 4 * n;
         to[0 * n + m] = b;

@@ -1,6 +1,8 @@
 // Candidate tiles of the fused stage kernels for the autotuner: every order
-// N is instantiated with E = 2, 4, 6, 8, 12 and 16 elements per CTA where
-// the tile fits 512 threads and 113 KB of shared memory (two CTAs per SM).
+// N is instantiated with E = 2, 4, 8 and 16 elements per CTA (powers of two:
+// whole element lines per shared-memory wavefront, which the bank-conflict-
+// free layout needs) where the tile fits 512 threads and 113 KB of shared
+// memory (two CTAs per SM).
 // stage_variants_fp64.cu and stage_variants_fp32.cu instantiate these
 // templates for the FP64 (default rounding) and the FP32 form.
 #pragma once
@@ -14,7 +16,7 @@
 namespace ndg {
 namespace dev {
 
-constexpr int kTileChoices[] = {2, 4, 6, 8, 12, 16};
+constexpr int kTileChoices[] = {2, 4, 8, 16};
 
 template <bool F32, int N, int E>
 struct Variant {
@@ -74,10 +76,10 @@ cudaError_t variant_launch(const StageArgs& a, cudaStream_t stream) {
 
 template <bool F32, int N>
 int variant_candidates(int* out, int max) {
-    const bool ok[] = {Variant<F32, N, 2>::feasible, Variant<F32, N, 4>::feasible, Variant<F32, N, 6>::feasible,
-                       Variant<F32, N, 8>::feasible, Variant<F32, N, 12>::feasible, Variant<F32, N, 16>::feasible};
+    const bool ok[] = {Variant<F32, N, 2>::feasible, Variant<F32, N, 4>::feasible, Variant<F32, N, 8>::feasible,
+                       Variant<F32, N, 16>::feasible};
     int count = 0;
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < 4; ++i)
         if (ok[i] && count < max) out[count++] = kTileChoices[i];
     return count;
 }
@@ -86,9 +88,7 @@ int variant_candidates(int* out, int max) {
     switch (epb) {                                        \
         case 2: return FN<F32_, N_, 2>(__VA_ARGS__);      \
         case 4: return FN<F32_, N_, 4>(__VA_ARGS__);      \
-        case 6: return FN<F32_, N_, 6>(__VA_ARGS__);      \
         case 8: return FN<F32_, N_, 8>(__VA_ARGS__);      \
-        case 12: return FN<F32_, N_, 12>(__VA_ARGS__);    \
         case 16: return FN<F32_, N_, 16>(__VA_ARGS__);    \
         default: return cudaErrorInvalidValue;            \
     }

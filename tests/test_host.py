@@ -142,12 +142,12 @@ def test_element_state_bitwise_vs_reference(res, kw, ref_available):
 
 
 def test_tile_candidates_on_a_host_context():
-    """The autotuner's candidate tiles need no GPU to list: even sizes that
-    fit 512 threads and 113 KB of shared memory."""
+    """The autotuner's candidate tiles need no GPU to list: powers of two
+    that fit 512 threads and 113 KB of shared memory."""
     zone = meshgen.uniform_zone(4, boundary=meshgen.WALL)
     m = ndg.Mesh2D_t(zone, 8, device=-1)
     cand, default = m.tile_candidates()
-    assert cand == [2, 4, 6, 8, 12, 16] and default == 8
+    assert cand == [2, 4, 8, 16] and default == 8
     m16 = ndg.Mesh2D_t(zone, 16, device=-1)
     cand16, _ = m16.tile_candidates()
-    assert cand16 and max(cand16) * 3 * 17 <= 512 and all(c % 2 == 0 for c in cand16)
+    assert cand16 and max(cand16) * 3 * 17 <= 512 and all(c in (2, 4, 8, 16) for c in cand16)
