@@ -143,13 +143,20 @@ __device__ __forceinline__ double receiver_value(const double* __restrict__ w, c
 }
 
 // ---------------------------------------------------------------------------
-// Forward stage with a wave speed per element. Same tile and thread layout
-// as stage_kernel<N, false> (stage_kernels.cu): the bulk-copied q tile in
-// FP64, then R arrays (offsets in R values past it), then the mbarrier.
+// Forward stage with a wave speed per element, one thread per (field,
+// element, line): the bulk-copied q tile in FP64, then R arrays (offsets in
+// R values past it), then the mbarrier.
 template <int N, typename R>
 struct SpeedTile {
-    using D = Tile<N>;
-    static constexpr int n = N + 1, NN = n * n, EPB = D::EPB, kThreads = D::kThreads, kNodeIters = D::kNodeIters;
+    static constexpr int n = N + 1, NN = n * n;
+    // as many elements as fit ~60 KB of shared memory and 256 threads, rounded down to a power of two
+    static constexpr int per_element_doubles = 2 * 3 * NN + 2 * 3 * 4 * n + NN + 4;
+    static constexpr int by_smem = (60 * 1024 / 8) / per_element_doubles;
+    static constexpr int by_threads = 256 / (3 * n);
+    static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
+    static constexpr int EPB = bank::pow2_floor(raw >= 2 ? (raw < 16 ? raw : 16) : 2);
+    static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
+    static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;
     static constexpr int kQd = 3 * EPB * NN;             // doubles: the q tile
     static constexpr int kG = 0;                         // [3][EPB][NN] time derivative G
     static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n] own side traces

@@ -286,17 +286,13 @@ constexpr int pow2_floor(int v) {
 
 // ---------------------------------------------------------------------------
 // Tile of the fused stage: E elements per CTA (2, 4, 8 or 16), or for E = 0
-// the default: the largest power of two of elements that fits ~60 KB of
-// shared memory (several CTAs per SM) and 256 threads.
+// the default: 4 elements up to order 10, 2 above (the autotuner's choice
+// on 256 x 256 meshes at N = 4, 6, 8 and at N = 12).
 template <int N, int E = 0>
 struct Tile {
     static constexpr int n = N + 1;
     static constexpr int NN = n * n;
-    static constexpr int per_element_doubles = 2 * 3 * NN + 2 * 3 * 4 * n + NN + 4;
-    static constexpr int by_smem = (60 * 1024 / 8) / per_element_doubles;
-    static constexpr int by_threads = 256 / (3 * n);
-    static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
-    static constexpr int EPB = E > 0 ? E : bank::pow2_floor(raw >= 2 ? (raw < 16 ? raw : 16) : 2);
+    static constexpr int EPB = E > 0 ? E : (N <= 10 ? 4 : 2);
     static_assert(EPB == 2 || EPB == 4 || EPB == 8 || EPB == 16, "tiles hold 2, 4, 8 or 16 elements (whole lines per wavefront group)");
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
     // Node-wise work per thread in an RK phase over the whole tile: ceil(3 EPB NN / threads).

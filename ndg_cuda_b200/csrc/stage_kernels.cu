@@ -7,8 +7,9 @@
 // include/solvers/Solver2D_t.tcu:46-70) become the passes of one CTA that
 // owns a tile of EPB consecutive elements:
 //
-//   prologue  one thread starts a TMA bulk copy (cp.async.bulk + mbarrier)
-//             of the tile's q = (p, u, v) into shared memory; meanwhile all
+//   prologue  8-byte asynchronous copies (cp.async) place the tile's
+//             q = (p, u, v) in shared memory, in a padded layout free of
+//             bank conflicts (Tile, stage_common.cuh); meanwhile all
 //             threads prefetch the far-side traces of their side nodes (the
 //             neighbours' traces of the previous stage) and build J and edge
 //             metrics from the four corners
@@ -20,9 +21,9 @@
 //   RK        k = a k + G, q += g dt k in FP64, node by node, coalesced
 //   traces    four side traces of the new q for the next stage
 //
-// Work is spread as one thread per (field, element, line), 3 EPB (N+1)
-// threads per CTA; shared memory carries only the q tile, G, J and the side
-// data. HBM traffic per
+// Work is spread as one thread per (field, line, element), 3 EPB (N+1)
+// threads per CTA, the element index fastest; shared memory carries only the
+// q tile, G, J and the side data. HBM traffic per
 // element and stage: q and k read and written (the algorithmic 32 B per
 // degree of freedom), one trace write and one neighbour-trace read of 4(N+1)
 // values per field, and 8 corner coordinates. Metrics are recomputed in
@@ -30,8 +31,9 @@
 // x_eta, y_eta only on xi (quad_metrics, include/functions/quad_metrics.tpp:2-7).
 //
 // Field blocks hold an even number of elements (one unused element when K is
-// odd) and tiles start on even elements, so every tile copy starts on a
-// 16-byte boundary and moves a multiple of 16 bytes, as cp.async.bulk needs.
+// odd) and tiles start on even elements, so the FP32 form's bulk copy of the
+// FP64 tile (cp.async.bulk + mbarrier) starts on a 16-byte boundary and
+// moves a multiple of 16 bytes.
 //
 // STRICT instantiations round every operation in the reference's order
 // (__dmul_rn/__dadd_rn, true divisions) and reproduce its CPU results bit

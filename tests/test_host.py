@@ -147,7 +147,7 @@ def test_tile_candidates_on_a_host_context():
     zone = meshgen.uniform_zone(4, boundary=meshgen.WALL)
     m = ndg.Mesh2D_t(zone, 8, device=-1)
     cand, default = m.tile_candidates()
-    assert cand == [2, 4, 8, 16] and default == 8
+    assert cand == [2, 4, 8, 16] and default == 4
     m16 = ndg.Mesh2D_t(zone, 16, device=-1)
     cand16, _ = m16.tile_candidates()
     assert cand16 and max(cand16) * 3 * 17 <= 512 and all(c in (2, 4, 8, 16) for c in cand16)
