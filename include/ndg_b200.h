@@ -271,6 +271,80 @@ ndg_status ndg_delta_t_from_device(const double* delta_xy_min, const int32_t* el
                                    double cfl, void* stream, double* delta_t);
 
 /* ------------------------------------------------------------------------
+ * Solution output. */
+
+/* Mesh2D_t::get_solution and get_complete_solution (src/meshes/Mesh2D_t.cpp:4237-4296;
+ * Element2D_t::interpolate_solution and interpolate_complete_solution,
+ * src/entities/Element2D_t.cpp:580-646) for one instance, on the device:
+ * every domain element's fields on an n x n grid of equispaced reference
+ * points xi_i = i / (n - 1) * 2 - 1, n = the mesh's n_interpolation_points
+ * (>= 2). Each array holds n_elements n^2 values, point (i, j) of element e
+ * at e n^2 + i n + j; any pointer may be NULL. x, y: physical coordinates
+ * (quad_map); p, u, v: the fields interpolated with the order's
+ * interpolation matrix; dp_dt, du_dt, dv_dt: the last stage's time
+ * derivative (needs ndg_ctx_keep_derivative before stepping);
+ * *_analytical_error: sum_mn |g(x_mn, time) - q_mn| I_im I_jn over the Gauss
+ * nodes, g the reference plane wave. Rounded in the reference's order: x, y,
+ * the fields and the derivatives equal its CPU output bit for bit, the
+ * analytic error to the rounding of the exponential. */
+typedef struct ndg_solution_output {
+    double *x, *y, *p, *u, *v;
+    double *dp_dt, *du_dt, *dv_dt;
+    double *p_analytical_error, *u_analytical_error, *v_analytical_error;
+} ndg_solution_output;
+ndg_status ndg_get_solution(ndg_ctx* ctx, int32_t instance, double time, const ndg_solution_output* out);
+
+/* Output files in the role of DataWriter_t (src/helpers/DataWriter_t.cpp,
+ * include/helpers/DataWriter_t.h; VTK is not needed): per output time a
+ * parallel unstructured grid <stem>_t<time, 9 decimals, '.' -> '_'>s<ext>
+ * (PUnstructuredGrid summary) with its piece <that name without ext>_0.vtu
+ * (base64 binary arrays), and for the complete output the element grid
+ * <stem>_element_t...s<ext>; time series <output_filename>.series and
+ * <stem>_element<ext>.series (JSON), created empty by ndg_writer_create
+ * (DataWriter_t::DataWriter_t) and extended at every write. Array names,
+ * components and cell layout are the reference's (see writer.cpp). */
+typedef struct ndg_writer ndg_writer;
+ndg_status ndg_writer_create(const char* output_filename, ndg_writer** writer);
+ndg_status ndg_writer_destroy(ndg_writer* writer);
+/* DataWriter_t::write_data (complete = 0: x, y, p, u, v) and
+ * write_complete_data (complete = 1: also the derivatives, analytic errors
+ * and the per-element arrays; NULL ones are written as zeros) from host
+ * arrays: point arrays of n_elements n_interp^2 values as ndg_get_solution
+ * returns them, element arrays of n_elements values. No GPU needed. */
+typedef struct ndg_output_arrays {
+    int32_t complete;
+    const double *x, *y, *p, *u, *v;
+    const double *dp_dt, *du_dt, *dv_dt;
+    const double *p_analytical_error, *u_analytical_error, *v_analytical_error;
+    const int32_t* N;
+    const int32_t *status, *rotation;
+    int32_t rank;
+    const double *p_error, *u_error, *v_error, *p_sigma, *u_sigma, *v_sigma;
+    const int32_t *refine, *coarsen, *split_level;
+} ndg_output_arrays;
+ndg_status ndg_writer_write_arrays(ndg_writer* writer, double time, int64_t n_elements, int64_t n_interp, const ndg_output_arrays* arrays);
+/* Mesh2D_t::write_data / write_complete_data (src/meshes/Mesh2D_t.cpp:1601-1642)
+ * for one instance of a context: ndg_get_solution at `time`, and for the
+ * complete output the element orders, Hilbert status and rotation, split
+ * levels and the last error estimate (zeros when none is held, as the
+ * reference's elements hold before their first estimate; the reference
+ * estimates only the pressure, so the velocity errors and decay rates are
+ * zeros). The time derivative is written as zeros unless the context keeps
+ * it (ndg_ctx_keep_derivative). */
+ndg_status ndg_writer_write(ndg_writer* writer, ndg_ctx* ctx, int32_t instance, double time, int32_t complete);
+
+/* Solver2D_t::pre_condition and pre_condition_iterative
+ * (include/solvers/Solver2D_t.tpp:136-334): RK3 steps of dt = get_delta_t
+ * (never shortened) from time 0; after every pre_condition_interval-th step
+ * the error is estimated and the mesh adapted, n_adaptivity_steps times.
+ * iterative = 0 (sequential): the initial conditions are set once at the
+ * end, on the adapted mesh; iterative = 1: after every adaptation the
+ * initial conditions are set again and the time restarts from 0.
+ * pre_condition_interval = 0 is rejected (the reference exits with 77).
+ * Needs one instance. *n_steps (may be NULL) = the steps taken. */
+ndg_status ndg_pre_condition(ndg_ctx* ctx, int64_t n_adaptivity_steps, int64_t pre_condition_interval, int32_t iterative, int64_t* n_steps);
+
+/* ------------------------------------------------------------------------
  * Discrete adjoint. No counterpart in the reference, whose wave speed is the
  * constant c = 1 (include/helpers/constants.h:15); with c = 1 the operator
  * below is the reference's.

@@ -9,8 +9,9 @@
  * after swapping `SEM::Device` for `ndg_b200`. Differences a caller sees:
  *   - tables are host vectors in the device NDG_t's packed layout (the
  *     library keeps its own device copies);
- *   - Solver2D_t::solve takes an output callback in place of a
- *     DataWriter_t (VTK output is not part of this library);
+ *   - Helpers::DataWriter_t writes the reference's files without VTK (a
+ *     parallel unstructured grid per output time and the .series files);
+ *     Solver2D_t::solve takes it, or any output callback;
  *   - errors throw ndg_b200::Error (the reference exits);
  * Header-only; link against libndg_b200.so. */
 #ifndef NDG_B200_HPP
@@ -113,6 +114,29 @@ private:
 
 }  // namespace Entities
 
+namespace Helpers {
+
+// DataWriter_t (include/helpers/DataWriter_t.h, src/helpers/DataWriter_t.cpp):
+// creates the empty time series files; Mesh2D_t::write_data and
+// write_complete_data add output times.
+class DataWriter_t {
+public:
+    explicit DataWriter_t(const std::filesystem::path& output_filename) {
+        check(ndg_writer_create(output_filename.string().c_str(), &w_), "ndg_writer_create");
+    }
+    DataWriter_t(const DataWriter_t&) = delete;
+    DataWriter_t& operator=(const DataWriter_t&) = delete;
+    ~DataWriter_t() {
+        if (w_) ndg_writer_destroy(w_);
+    }
+    ndg_writer* handle() const noexcept { return w_; }
+
+private:
+    ndg_writer* w_ = nullptr;
+};
+
+}  // namespace Helpers
+
 namespace Meshes {
 
 // Mesh2D_t (include/meshes/Mesh2D_t.cuh:23-182): the mesh, its fields and
@@ -167,6 +191,7 @@ public:
         field_size_ = other.field_size_;
         adaptivity_interval_ = other.adaptivity_interval_;
         load_balancing_interval_ = other.load_balancing_interval_;
+        n_interpolation_points_ = other.n_interpolation_points_;
         tolerance_min_ = other.tolerance_min_;
         tolerance_max_ = other.tolerance_max_;
         return *this;
@@ -185,6 +210,7 @@ public:
     size_t field_size_ = 0;  // values per field and instance: sum of (N+1)^2
     size_t adaptivity_interval_ = 0;
     size_t load_balancing_interval_ = 0;
+    size_t n_interpolation_points_ = 0;
     double tolerance_min_ = 0.0;
     double tolerance_max_ = 0.0;
 
@@ -244,9 +270,45 @@ public:
         return N;
     }
 
+    // Mesh2D_t::get_solution / get_complete_solution (src/meshes/Mesh2D_t.cpp:4237-4296):
+    // the arrays of ndg_get_solution, n_elements_ n_interpolation_points^2
+    // values each; the derivatives only when the mesh keeps them.
+    struct Solution {
+        std::vector<double> x, y, p, u, v, dp_dt, du_dt, dv_dt, p_analytical_error, u_analytical_error, v_analytical_error;
+    };
+    Solution get_solution(double time = 0.0, bool complete = false, bool with_derivative = false, int instance = 0) const {
+        const size_t n = n_elements_ * n_interpolation_points_ * n_interpolation_points_;
+        Solution s;
+        ndg_solution_output o{};
+        for (auto* v : {&s.x, &s.y, &s.p, &s.u, &s.v}) v->resize(n);
+        o.x = s.x.data(), o.y = s.y.data(), o.p = s.p.data(), o.u = s.u.data(), o.v = s.v.data();
+        if (complete) {
+            for (auto* v : {&s.p_analytical_error, &s.u_analytical_error, &s.v_analytical_error}) v->resize(n);
+            o.p_analytical_error = s.p_analytical_error.data();
+            o.u_analytical_error = s.u_analytical_error.data();
+            o.v_analytical_error = s.v_analytical_error.data();
+            if (with_derivative) {
+                for (auto* v : {&s.dp_dt, &s.du_dt, &s.dv_dt}) v->resize(n);
+                o.dp_dt = s.dp_dt.data(), o.du_dt = s.du_dt.data(), o.dv_dt = s.dv_dt.data();
+            }
+        }
+        check(ndg_get_solution(ctx_, instance, time, &o), "ndg_get_solution");
+        return s;
+    }
+
+    // Mesh2D_t::write_data / write_complete_data (src/meshes/Mesh2D_t.cpp:1601-1642).
+    void write_data(double time, const Helpers::DataWriter_t& data_writer, int instance = 0) const {
+        check(ndg_writer_write(data_writer.handle(), ctx_, instance, time, 0), "ndg_writer_write");
+    }
+    void write_complete_data(double time, const Helpers::DataWriter_t& data_writer, int instance = 0) const {
+        check(ndg_writer_write(data_writer.handle(), ctx_, instance, time, 1), "ndg_writer_write");
+    }
+
     void synchronize() const { check(ndg_ctx_synchronize(ctx_), "ndg_ctx_synchronize"); }
 
     ndg_ctx* handle() const noexcept { return ctx_; }
+    // Re-reads the counts after a call that may adapt the mesh.
+    void refresh() { refresh_counts(); }
 
 private:
     Mesh2D_t(int device, CUstream_st* stream) {
@@ -284,6 +346,7 @@ private:
         maximum_N_ = p.maximum_N;
         n_instances_ = n_instances;
         adaptivity_interval_ = static_cast<size_t>(p.adaptivity_interval);
+        n_interpolation_points_ = static_cast<size_t>(p.n_interpolation_points);
         tolerance_min_ = p.tolerance_min;
         tolerance_max_ = p.tolerance_max;
     }
@@ -385,6 +448,35 @@ public:
             if (output) output(time, mesh);
         }
         return steps;
+    }
+
+    // The reference's signature: write_complete_data to data_writer at the output times.
+    template <typename Polynomial>
+    size_t solve(const Entities::NDG_t<Polynomial>& NDG, Meshes::Mesh2D_t& mesh, const Helpers::DataWriter_t& data_writer) const {
+        return solve(NDG, mesh, Output([&data_writer](double time, Meshes::Mesh2D_t& m) { m.write_complete_data(time, data_writer); }));
+    }
+
+    // Solver2D_t::pre_condition and pre_condition_iterative
+    // (include/solvers/Solver2D_t.tpp:136-334) at this solver's CFL.
+    // Returns the number of steps.
+    template <typename Polynomial>
+    size_t pre_condition(const Entities::NDG_t<Polynomial>& NDG, Meshes::Mesh2D_t& mesh, size_t n_adaptivity_steps, size_t pre_condition_interval) const {
+        return pre_condition_run(NDG, mesh, n_adaptivity_steps, pre_condition_interval, 0);
+    }
+    template <typename Polynomial>
+    size_t pre_condition_iterative(const Entities::NDG_t<Polynomial>& NDG, Meshes::Mesh2D_t& mesh, size_t n_adaptivity_steps, size_t pre_condition_interval) const {
+        return pre_condition_run(NDG, mesh, n_adaptivity_steps, pre_condition_interval, 1);
+    }
+
+private:
+    template <typename Polynomial>
+    size_t pre_condition_run(const Entities::NDG_t<Polynomial>& NDG, Meshes::Mesh2D_t& mesh, size_t n, size_t interval, int iterative) const {
+        (void)NDG;
+        (void)get_delta_t(mesh);  // sets the CFL
+        int64_t steps = 0;
+        check(ndg_pre_condition(mesh.handle(), static_cast<int64_t>(n), static_cast<int64_t>(interval), iterative, &steps), "ndg_pre_condition");
+        mesh.refresh();
+        return static_cast<size_t>(steps);
     }
 };
 

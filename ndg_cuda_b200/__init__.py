@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-__all__ = ["NdgError", "lib", "NDG_t", "Mesh2D_t", "Solver2D_t", "Adjoint2D_t", "Zone", "LIB_PATH",
+__all__ = ["NdgError", "lib", "NDG_t", "Mesh2D_t", "Solver2D_t", "Adjoint2D_t", "DataWriter_t", "Zone", "LIB_PATH",
            "FP64", "FP64_STRICT", "FP32", "tables_compute"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libndg_b200.so")
@@ -45,6 +45,22 @@ class _Params(C.Structure):
     _fields_ = [("initial_N", C.c_int32), ("maximum_N", C.c_int32), ("n_interpolation_points", C.c_int64),
                 ("max_split_level", C.c_int32), ("adaptivity_interval", C.c_int64),
                 ("tolerance_min", C.c_double), ("tolerance_max", C.c_double), ("cfl", C.c_double)]
+
+
+# arrays of ndg_get_solution / ndg_solution_output, in its field order
+SOLUTION_NAMES = ("x", "y", "p", "u", "v", "dp_dt", "du_dt", "dv_dt",
+                  "p_analytical_error", "u_analytical_error", "v_analytical_error")
+
+
+class _SolutionOutput(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in SOLUTION_NAMES]
+
+
+class _OutputArrays(C.Structure):
+    _fields_ = ([("complete", C.c_int32)] + [(k, C.c_void_p) for k in SOLUTION_NAMES]
+                + [("N", C.c_void_p), ("status", C.c_void_p), ("rotation", C.c_void_p), ("rank", C.c_int32)]
+                + [(k, C.c_void_p) for k in ("p_error", "u_error", "v_error", "p_sigma", "u_sigma", "v_sigma",
+                                             "refine", "coarsen", "split_level")])
 
 
 _lib = None
@@ -92,6 +108,12 @@ def lib() -> C.CDLL:
         "ndg_estimate_error": ([vp], C.c_int),
         "ndg_get_error": ([vp, i32, vp, vp, vp, vp], C.c_int),
         "ndg_adapt": ([vp], C.c_int),
+        "ndg_get_solution": ([vp, i32, dbl, C.POINTER(_SolutionOutput)], C.c_int),
+        "ndg_writer_create": ([C.c_char_p, C.POINTER(vp)], C.c_int),
+        "ndg_writer_destroy": ([vp], C.c_int),
+        "ndg_writer_write_arrays": ([vp, dbl, i64, i64, C.POINTER(_OutputArrays)], C.c_int),
+        "ndg_writer_write": ([vp, vp, i32, dbl, i32], C.c_int),
+        "ndg_pre_condition": ([vp, i64, i64, i32, C.POINTER(i64)], C.c_int),
         "ndg_adapt_flags": ([vp, vp, vp], C.c_int),
         "ndg_delta_t_from_device": ([vp, vp, i64, dbl, vp, C.POINTER(dbl)], C.c_int),
         "ndg_autotune": ([vp, i32, C.POINTER(i32), C.POINTER(dbl)], C.c_int),
@@ -238,6 +260,8 @@ class Mesh2D_t:
         self.initial_N_ = initial_N
         self.maximum_N_ = maximum_N if maximum_N is not None else initial_N
         self.adaptivity_interval_ = adaptivity_interval
+        self.n_interpolation_points_ = n_interpolation_points
+        self.keep_derivative_ = keep_derivative
         self.n_instances = n_instances
         self._ctx = _Context(device, stream)
         h = self._ctx.h
@@ -388,8 +412,76 @@ class Mesh2D_t:
         _check(lib().ndg_mesh_get_nodes(self._ctx.h, _ptr(out)))
         return out.reshape(-1, 2)
 
+    # Mesh2D_t::get_solution / get_complete_solution (src/meshes/Mesh2D_t.cpp:4237-4296)
+    def get_solution(self, time: float = 0.0, complete: bool = False, instance: int = 0) -> dict:
+        """Fields on the n_interpolation_points^2 output grid of every element
+        (ndg_get_solution): x, y, p, u, v, and with `complete` the analytic
+        errors at `time` and, when the mesh keeps them, the time derivatives.
+        Element e's point (i, j) is entry e n^2 + i n + j."""
+        names = ["x", "y", "p", "u", "v"]
+        if complete:
+            if self.keep_derivative_:
+                names += ["dp_dt", "du_dt", "dv_dt"]
+            names += ["p_analytical_error", "u_analytical_error", "v_analytical_error"]
+        P = self.n_interpolation_points_
+        arrays = {k: np.empty(self.n_elements_ * P * P) for k in names}
+        o = _SolutionOutput(**{k: arrays[k].ctypes.data for k in names})
+        _check(lib().ndg_get_solution(self._ctx.h, instance, float(time), C.byref(o)))
+        return arrays
+
+    def get_complete_solution(self, time: float, instance: int = 0) -> dict:
+        return self.get_solution(time, complete=True, instance=instance)
+
+    # Mesh2D_t::write_data / write_complete_data (src/meshes/Mesh2D_t.cpp:1601-1642)
+    def write_data(self, time: float, data_writer: "DataWriter_t", instance: int = 0) -> None:
+        _check(lib().ndg_writer_write(data_writer.handle, self._ctx.h, instance, float(time), 0))
+
+    def write_complete_data(self, time: float, data_writer: "DataWriter_t", instance: int = 0) -> None:
+        _check(lib().ndg_writer_write(data_writer.handle, self._ctx.h, instance, float(time), 1))
+
     def close(self) -> None:
         self._ctx.close()
+
+
+class DataWriter_t:
+    """DataWriter_t(output_filename) (include/helpers/DataWriter_t.h,
+    src/helpers/DataWriter_t.cpp), without VTK: per output time a parallel
+    unstructured grid <stem>_t<time>s<ext> with its piece <...>_0.vtu, the
+    element grid <stem>_element_t<time>s<ext> for complete outputs, and the
+    time series files <output_filename>.series and <stem>_element<ext>.series
+    (created empty here)."""
+
+    def __init__(self, output_filename):
+        h = C.c_void_p()
+        _check(lib().ndg_writer_create(os.fspath(output_filename).encode(), C.byref(h)))
+        self.handle = h.value
+
+    def write_arrays(self, time: float, n_elements: int, n_interp: int, arrays: dict, complete: bool = False,
+                     rank: int = 0) -> None:
+        """Writes host arrays (the names of Mesh2D_t.get_solution, plus the
+        element arrays N, status, rotation, p_error, u_error, v_error, p_sigma,
+        u_sigma, v_sigma, refine, coarsen, split_level); missing ones are
+        zeros. Needs no GPU."""
+        keep = {}
+        fields = {}
+        for k, v in arrays.items():
+            dt = np.int32 if k in ("N", "status", "rotation", "refine", "coarsen", "split_level") else np.float64
+            keep[k] = np.ascontiguousarray(v, dtype=dt)
+            fields[k] = keep[k].ctypes.data
+        a = _OutputArrays(complete=1 if complete else 0, rank=rank, **fields)
+        _check(lib().ndg_writer_write_arrays(self.handle, float(time), n_elements, n_interp, C.byref(a)))
+        del keep
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().ndg_writer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Solver2D_t:
@@ -417,15 +509,83 @@ class Solver2D_t:
         _check(lib().ndg_run(mesh.handle, n_steps, C.byref(t)))
         return t.value
 
-    def solve(self, mesh: Mesh2D_t, time: float = 0.0) -> tuple[float, int]:
+    def solve(self, mesh: Mesh2D_t, time: float = 0.0, data_writer: DataWriter_t | None = None,
+              output=None) -> tuple[float, int]:
         """Steps to output_times_[-1] with the reference's shortened last step,
-        at this solver's CFL."""
-        t = C.c_double(time)
+        at this solver's CFL. With a data_writer (write_complete_data) or an
+        output(time, mesh) callback, outputs come where the reference's
+        Solver2D_t::solve (include/solvers/Solver2D_t.tpp:7-133) writes them:
+        at the start if the start time is an output time, after the first step
+        whose end time t has e <= t < e + dt for an output time e (after an
+        error estimate), and at the end if the last step wrote none."""
+        _check(lib().ndg_set_cfl(mesh.handle, float(self.CFL_)))
+        if data_writer is None and output is None:
+            t = C.c_double(time)
+            n = C.c_int64()
+            _check(lib().ndg_solve(mesh.handle, float(self.output_times_[-1]), C.byref(t), C.byref(n)))
+            mesh._refresh_counts()  # the mesh may have been adapted
+            return t.value, n.value
+        emit = output if output is not None else (lambda tt, m: m.write_complete_data(tt, data_writer))
+        t_end = float(self.output_times_[-1])
+        dt_mesh = self.get_delta_t(mesh)
+        for e in self.output_times_:
+            if e <= time < e + dt_mesh:
+                emit(time, mesh)
+        steps, pending, t_run, wrote_last = 0, 0, time, False
+
+        def flush():
+            nonlocal pending, t_run
+            if pending:
+                t_run = self.run(mesh, pending, t_run)
+            pending = 0
+
+        while time < t_end:
+            dt = dt_mesh
+            last = time + dt > t_end
+            if last:
+                dt = t_end - time
+                flush()
+                for m in range(3):
+                    self.stage(mesh, m, time, dt)
+                t_run = time + dt
+            else:
+                pending += 1
+            time += dt
+            steps += 1
+            wrote_last = any(e <= time < e + dt for e in self.output_times_)
+            if wrote_last:
+                flush()
+                mesh.estimate_error()
+                emit(time, mesh)
+            if mesh.adaptivity_interval_ > 0 and steps % mesh.adaptivity_interval_ == 0:
+                flush()
+                mesh.estimate_error()
+                mesh.adapt()
+                dt_mesh = self.get_delta_t(mesh)
+        flush()
+        if not wrote_last:
+            mesh.estimate_error()
+            emit(time, mesh)
+        return time, steps
+
+    def _pre_condition(self, mesh: Mesh2D_t, n_adaptivity_steps: int, pre_condition_interval: int, iterative: int) -> int:
         n = C.c_int64()
         _check(lib().ndg_set_cfl(mesh.handle, float(self.CFL_)))
-        _check(lib().ndg_solve(mesh.handle, float(self.output_times_[-1]), C.byref(t), C.byref(n)))
-        mesh._refresh_counts()  # the mesh may have been adapted
-        return t.value, n.value
+        _check(lib().ndg_pre_condition(mesh.handle, n_adaptivity_steps, pre_condition_interval, iterative, C.byref(n)))
+        mesh._refresh_counts()
+        return n.value
+
+    # Solver2D_t::pre_condition / pre_condition_iterative (include/solvers/Solver2D_t.tpp:136-334)
+    def pre_condition(self, mesh: Mesh2D_t, n_adaptivity_steps: int, pre_condition_interval: int) -> int:
+        """Steps and adapts n_adaptivity_steps times, every
+        pre_condition_interval steps, then sets the initial conditions on the
+        adapted mesh. Returns the number of steps."""
+        return self._pre_condition(mesh, n_adaptivity_steps, pre_condition_interval, 0)
+
+    def pre_condition_iterative(self, mesh: Mesh2D_t, n_adaptivity_steps: int, pre_condition_interval: int) -> int:
+        """As pre_condition, with the initial conditions set again (and the
+        time restarted) after every adaptation."""
+        return self._pre_condition(mesh, n_adaptivity_steps, pre_condition_interval, 1)
 
 
 class Adjoint2D_t:

@@ -679,6 +679,22 @@ void copy_table(const Tables& t, int32_t table, int32_t N, double* out, int64_t 
 }
 
 }  // namespace
+
+// Mesh2D_t::initial_conditions on every instance (the device must be current).
+void set_initial_conditions(ndg_ctx* ctx) {
+    if (ctx->general) {
+        check_cuda(dev::launch_general_initial_conditions(general_args(ctx, 0, ctx->cur), ctx->groups.data(), static_cast<int>(ctx->groups.size()), ctx->stream),
+                   "initial condition kernel");
+        ctx->launches += static_cast<int64_t>(ctx->groups.size());
+    } else {
+        check_cuda(dev::launch_initial_conditions(ctx->q.ptr, ctx->k.ptr, ctx->corners.ptr, ctx->N, ctx->K, ctx->Kp, ctx->n_instances, ctx->stream),
+                   "initial condition kernel");
+        ++ctx->launches;
+    }
+    if (ctx->keep_derivative) check_cuda(cudaMemsetAsync(ctx->G.ptr, 0, ctx->G.count * sizeof(double), ctx->stream), "memset");
+    ctx->traces_valid = false;
+}
+
 }  // namespace ndg
 
 using namespace ndg;
@@ -927,22 +943,13 @@ ndg_status ndg_mesh_field_size(const ndg_ctx* ctx, int64_t* n_values) {
     });
 }
 
+
 ndg_status ndg_initial_conditions(ndg_ctx* ctx) {
     return guarded([&] {
         require_mesh(ctx);
         require_device(ctx);
         make_current(ctx);
-        if (ctx->general) {
-            check_cuda(dev::launch_general_initial_conditions(general_args(ctx, 0, ctx->cur), ctx->groups.data(), static_cast<int>(ctx->groups.size()), ctx->stream),
-                       "initial condition kernel");
-            ctx->launches += static_cast<int64_t>(ctx->groups.size());
-        } else {
-            check_cuda(dev::launch_initial_conditions(ctx->q.ptr, ctx->k.ptr, ctx->corners.ptr, ctx->N, ctx->K, ctx->Kp, ctx->n_instances, ctx->stream),
-                       "initial condition kernel");
-            ++ctx->launches;
-        }
-        if (ctx->keep_derivative) check_cuda(cudaMemsetAsync(ctx->G.ptr, 0, ctx->G.count * sizeof(double), ctx->stream), "memset");
-        ctx->traces_valid = false;
+        set_initial_conditions(ctx);
     });
 }
 
@@ -1065,6 +1072,37 @@ ndg_status ndg_solve(ndg_ctx* ctx, double t_end, double* time, int64_t* n_steps)
             }
         }
         if (time) *time = t;
+        if (n_steps) *n_steps = steps;
+    });
+}
+
+ndg_status ndg_pre_condition(ndg_ctx* ctx, int64_t n_adaptivity_steps, int64_t pre_condition_interval, int32_t iterative, int64_t* n_steps) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (pre_condition_interval <= 0) fail(NDG_ERR_INVALID_ARG, "pre-condition needs a positive pre_condition_interval");
+        if (n_adaptivity_steps < 0) fail(NDG_ERR_INVALID_ARG, "n_adaptivity_steps must be >= 0");
+        if (n_adaptivity_steps > 0 && ctx->n_instances != 1) fail(NDG_ERR_UNSUPPORTED, "adaptation needs a single instance (the mesh is shared)");
+        make_current(ctx);
+        // Solver2D_t.tpp:136-334: full steps of the current mesh's dt; an
+        // estimate and an adaptation after every pre_condition_interval-th
+        // step; the initial conditions once at the end (sequential) or after
+        // every adaptation with the time restarted (iterative).
+        double t = 0.0;
+        int64_t steps = 0;
+        for (int64_t a = 0; a < n_adaptivity_steps; ++a) {
+            set_step(ctx, t, ctx->dt_mesh, std::numeric_limits<double>::infinity());
+            run_steps(ctx, pre_condition_interval);
+            for (int64_t s = 0; s < pre_condition_interval; ++s) t += ctx->dt_mesh;
+            steps += pre_condition_interval;
+            estimate(ctx);
+            adapt_from_estimate(ctx);
+            if (iterative) {
+                set_initial_conditions(ctx);
+                t = 0.0;
+            }
+        }
+        if (!iterative) set_initial_conditions(ctx);
         if (n_steps) *n_steps = steps;
     });
 }

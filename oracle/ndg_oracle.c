@@ -1634,3 +1634,56 @@ double ndgo_adjoint_solve(ndgo_ctx* c, const double* p0, const double* u0, const
     free(lq), free(lk), free(mu), free(dc), free(Q), free(smp);
     return rc == 0 ? J : NAN;
 }
+
+/* Mesh2D_t::get_complete_solution (src/meshes/Mesh2D_t.cpp:4251-4296) with
+ * Element2D_t::interpolate_complete_solution (src/entities/Element2D_t.cpp:606-646):
+ * per domain element, on the n_interp x n_interp grid of reference points
+ * i / (n_interp - 1) * 2 - 1, the coordinates (quad_map), the fields and
+ * their time derivatives interpolated with the order's interpolation
+ * matrix, and the interpolated |g(x_mn, time) - q_mn| over the Gauss nodes,
+ * each sum in the reference's order. out[11] = x, y, p, u, v, dp/dt, du/dt,
+ * dv/dt, p/u/v analytic error, n_elements n_interp^2 values each (any may
+ * be NULL). Returns 0, or -1 when the tables cannot be built. */
+int ndgo_complete_solution(const ndgo_ctx* c, int64_t n_interp, double time, double** out) {
+    ndgo_tables T;
+    if (n_interp < 2 || tables_build(&T, c->T.N_max, n_interp) != 0) return -1;
+    const int64_t PP = n_interp * n_interp;
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        const int N = c->eN[e], n = N + 1;
+        const int64_t o2 = c->off2[e];
+        double px[4], py[4];
+        for (int k = 0; k < 4; ++k) {
+            px[k] = c->nx[c->enodes[4 * e + k]];
+            py[k] = c->ny[c->enodes[4 * e + k]];
+        }
+        const double* I = T.t[T_INTERP][N];
+        const double* xn = T.t[T_NODES][N];
+        const double* q[6] = {c->p + o2, c->u + o2, c->v + o2, c->Gp + o2, c->Gu + o2, c->Gv + o2};
+        for (int64_t i = 0; i < n_interp; ++i) {
+            for (int64_t j = 0; j < n_interp; ++j) {
+                const int64_t o = e * PP + i * n_interp + j;
+                const double xi = (double)i / (double)(n_interp - 1) * 2 - 1;
+                const double eta = (double)j / (double)(n_interp - 1) * 2 - 1;
+                double gx, gy;
+                quad_map(xi, eta, px, py, &gx, &gy);
+                double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                for (int m = 0; m < n; ++m) {
+                    for (int nn = 0; nn < n; ++nn) {
+                        const double im = I[i * n + m], jn = I[j * n + nn];
+                        for (int f = 0; f < 6; ++f) acc[f] += q[f][m * n + nn] * im * jn;
+                        double nxg, nyg, g[3];
+                        quad_map(xn[m], xn[nn], px, py, &nxg, &nyg);
+                        analytic_g(nxg, nyg, time, &g[0], &g[1], &g[2]);
+                        for (int f = 0; f < 3; ++f) acc[6 + f] += fabs(g[f] - q[f][m * n + nn]) * im * jn;
+                    }
+                }
+                if (out[0]) out[0][o] = gx;
+                if (out[1]) out[1][o] = gy;
+                for (int f = 0; f < 9; ++f)
+                    if (out[2 + f]) out[2 + f][o] = acc[f];
+            }
+        }
+    }
+    tables_free(&T);
+    return 0;
+}

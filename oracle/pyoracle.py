@@ -72,6 +72,8 @@ def _load_ref():
         lib.ndgref_get_error.argtypes = [_dp, _dp, _ip, _ip]
         lib.ndgref_get_element_faces.argtypes = [C.c_void_p]
         lib.ndgref_get_element_faces.restype = C.c_long
+        lib.ndgref_complete_solution.argtypes = [C.c_double, C.POINTER(C.c_void_p)]
+        lib.ndgref_pre_condition.argtypes = [C.c_long, C.c_long, C.c_int]
         _ref = lib
     return _ref
 
@@ -114,11 +116,22 @@ def _load_oracle():
         lib.ndgo_adjoint_solve.argtypes = [C.c_void_p, _dp, C.c_void_p, C.c_void_p, C.c_double, C.c_int64,
                                            C.c_int, _lp, _dp, C.c_void_p, _dp, _dp, _dp, _dp, _dp]
         lib.ndgo_adjoint_solve.restype = C.c_double
+        lib.ndgo_complete_solution.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]
+        lib.ndgo_complete_solution.restype = C.c_int
         _orc = lib
     return _orc
 
 
 FIELDS = {"p": 0, "u": 1, "v": 2, "Gp": 3, "Gu": 4, "Gv": 5, "kp": 6, "ku": 7, "kv": 8}
+# arrays of Mesh2D_t::get_complete_solution, in the checkers' output order
+OUTPUT_NAMES = ("x", "y", "p", "u", "v", "dp_dt", "du_dt", "dv_dt",
+                "p_analytical_error", "u_analytical_error", "v_analytical_error")
+
+
+def _output_arrays(count: int) -> tuple[dict, C.Array]:
+    arrays = {k: np.zeros(count) for k in OUTPUT_NAMES}
+    ptrs = (C.c_void_p * len(OUTPUT_NAMES))(*[a.ctypes.data for a in arrays.values()])
+    return arrays, ptrs
 
 
 class _Base:
@@ -144,6 +157,7 @@ class RefSolver(_Base):
                  tolerance_min: float = 1e-6, tolerance_max: float = 1e-14):
         lib = _load_ref()
         self.lib = lib
+        self.n_interp = n_interp
         if isinstance(zone, str):
             lib.ndgref_create_file(zone.encode(), N, N_max if N_max is not None else N, n_interp, cfl)
             self._refresh_counts()
@@ -248,6 +262,17 @@ class RefSolver(_Base):
 
     def adapt(self):
         self.lib.ndgref_adapt()
+        self._refresh_counts()
+
+    def complete_solution(self, time: float) -> dict:
+        """Mesh2D_t::get_complete_solution at `time` (the reference's own code)."""
+        arrays, ptrs = _output_arrays(self.n_elements * self.n_interp * self.n_interp)
+        self.lib.ndgref_complete_solution(time, ptrs)
+        return arrays
+
+    def pre_condition(self, n_adaptivity_steps: int, pre_condition_interval: int, iterative: bool = False):
+        """Solver2D_t::pre_condition / pre_condition_iterative (prints the reference's progress bar)."""
+        self.lib.ndgref_pre_condition(n_adaptivity_steps, pre_condition_interval, 1 if iterative else 0)
         self._refresh_counts()
 
 
@@ -371,6 +396,13 @@ class OracleSolver(_Base):
 
     def estimate_error(self):
         self.lib.ndgo_estimate_error(self.ctx, *self.tolerance)
+
+    def complete_solution(self, n_interp: int, time: float) -> dict:
+        """Restatement of Mesh2D_t::get_complete_solution on n_interp^2 points per element."""
+        arrays, ptrs = _output_arrays(self.n_elements * n_interp * n_interp)
+        if self.lib.ndgo_complete_solution(self.ctx, n_interp, time, ptrs) != 0:
+            raise ValueError("bad output request")
+        return arrays
 
     def error(self) -> dict:
         n = self.n_elements

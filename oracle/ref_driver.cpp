@@ -296,4 +296,31 @@ void ndgref_adapt() {
     g_ref.mesh->adapt(g_ref.ndg->N_max_, g_ref.ndg->nodes_, g_ref.ndg->barycentric_weights_);
 }
 
+// Mesh2D_t::get_complete_solution (src/meshes/Mesh2D_t.cpp:4251-4296) at
+// `time` through the reference's public interface: point arrays of
+// n_elements n_interpolation_points^2 values, in the order x, y, p, u, v,
+// dp_dt, du_dt, dv_dt, p/u/v analytical error (out[11], any may be NULL).
+void ndgref_complete_solution(double time, double** out) {
+    Mesh2D_t& mesh = *g_ref.mesh;
+    NDG& ndg = *g_ref.ndg;
+    const size_t K = mesh.n_elements_, PP = mesh.n_interpolation_points_ * mesh.n_interpolation_points_;
+    std::vector<int> N(K), refine(K), coarsen(K), split(K), status(K), rotation(K);
+    std::vector<double> pe(K), ue(K), ve(K), ps(K), us(K), vs(K);
+    std::vector<double> d[6];
+    for (auto& v : d) v.assign(K * PP, 0.0);
+    mesh.get_complete_solution(time, ndg.nodes_, ndg.interpolation_matrices_, N, d[0], d[1], d[2], pe, ue, ve, ps, us, vs, refine, coarsen, split, d[3], d[4], d[5], status, rotation);
+    const std::vector<double>* src[11] = {&mesh.x_output_, &mesh.y_output_, &mesh.p_output_, &mesh.u_output_, &mesh.v_output_, &d[0], &d[1], &d[2], &d[3], &d[4], &d[5]};
+    for (int i = 0; i < 11; ++i)
+        if (out[i]) std::memcpy(out[i], src[i]->data(), K * PP * sizeof(double));
+}
+
+// Solver2D_t::pre_condition (iterative = 0) or pre_condition_iterative
+// (include/solvers/Solver2D_t.tpp:136-334); the progress bar goes to stdout.
+void ndgref_pre_condition(long n_adaptivity_steps, long pre_condition_interval, int iterative) {
+    if (iterative)
+        g_ref.solver->pre_condition_iterative(*g_ref.ndg, *g_ref.mesh, static_cast<size_t>(n_adaptivity_steps), static_cast<size_t>(pre_condition_interval));
+    else
+        g_ref.solver->pre_condition(*g_ref.ndg, *g_ref.mesh, static_cast<size_t>(n_adaptivity_steps), static_cast<size_t>(pre_condition_interval));
+}
+
 }  // extern "C"

@@ -4,6 +4,9 @@
 //
 //   api_driver host  <mesh.su2> <N>                        tables and counts as JSON (no GPU)
 //   api_driver solve <mesh.su2> <N> <CFL> <out.bin> <t_1> ... <t_end>
+//   api_driver write <mesh.su2> <N> <CFL> <output.pvtu> <n_adapt> <interval> <t_1> ... <t_end>
+//       pre_condition (n_adapt adaptations every interval steps, N_max = N + 4,
+//       one split level) then solve with a DataWriter_t; prints the steps of both as JSON
 //
 // solve writes, little-endian: int64 steps, int64 outputs, int64 field_size,
 // double dt, then per output: double time and the p, u, v fields.
@@ -66,6 +69,19 @@ int solve_mode(const std::string& path, int N, double CFL, const std::string& ou
     return 0;
 }
 
+int write_mode(const std::string& path, int N, double CFL, const std::string& output, size_t n_adapt, size_t interval,
+               std::vector<double> times) {
+    ndg_b200::Entities::NDG_t<> NDG(N + 4, 3);
+    ndg_b200::Meshes::Mesh2D_t mesh(path, N, N + 4, 3, 1, 0, 0, 1e-6, 1e-14, 0.0, NDG.nodes_, {}, nullptr, 0);
+    mesh.initial_conditions(NDG.nodes_);
+    ndg_b200::Solvers::Solver2D_t solver(CFL, times, 0.0);
+    const size_t pre = solver.pre_condition(NDG, mesh, n_adapt, interval);
+    ndg_b200::Helpers::DataWriter_t writer(output);
+    const size_t steps = solver.solve(NDG, mesh, writer);
+    std::printf("{\"pre_condition_steps\": %zu, \"steps\": %zu, \"n_elements\": %zu}\n", pre, steps, mesh.n_elements_);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -77,7 +93,14 @@ int main(int argc, char** argv) {
             for (int i = 6; i < argc; ++i) times.push_back(std::strtod(argv[i], nullptr));
             return solve_mode(argv[2], std::atoi(argv[3]), std::strtod(argv[4], nullptr), argv[5], times);
         }
-        std::fprintf(stderr, "usage: api_driver host <mesh> <N> | solve <mesh> <N> <CFL> <out> <t_1> ... <t_end>\n");
+        if (mode == "write" && argc >= 9) {
+            std::vector<double> times;
+            for (int i = 8; i < argc; ++i) times.push_back(std::strtod(argv[i], nullptr));
+            return write_mode(argv[2], std::atoi(argv[3]), std::strtod(argv[4], nullptr), argv[5],
+                              static_cast<size_t>(std::atol(argv[6])), static_cast<size_t>(std::atol(argv[7])), times);
+        }
+        std::fprintf(stderr, "usage: api_driver host <mesh> <N> | solve <mesh> <N> <CFL> <out> <t_1> ... <t_end> | "
+                             "write <mesh> <N> <CFL> <output> <n_adapt> <interval> <t_1> ... <t_end>\n");
         return 1;
     } catch (const ndg_b200::Error& e) {
         std::fprintf(stderr, "ndg_b200 error %d: %s\n", static_cast<int>(e.status()), e.what());

@@ -118,3 +118,25 @@ def test_solve_matches_reference_steps_and_fields(driver, su2_mesh, tmp_path, re
         for i, f in enumerate(("p", "u", "v")):
             w = ref.field(f)
             assert np.linalg.norm(fields[i] - w) <= TOL * np.linalg.norm(w), (t_out, f)
+
+
+@pytest.mark.gpu
+def test_pre_condition_and_data_writer_through_the_cpp_api(driver, su2_mesh, tmp_path):
+    """Solver2D_t::pre_condition then solve with a Helpers::DataWriter_t, the
+    reference's driver sequence (src/main.cu:346-390): the writer's series
+    lists one complete output per output time, each file readable, and the
+    mesh is the pre-conditioned (adapted) one."""
+    from tests.vtu import read_grid
+    out = tmp_path / "wave.pvtu"
+    N, cfl = 3, 0.5
+    res = subprocess.run([driver, "write", su2_mesh, str(N), repr(cfl), str(out), "2", "4", "0.0", "0.02", "0.05"],
+                         check=True, capture_output=True, text=True)
+    d = json.loads(res.stdout)
+    assert d["pre_condition_steps"] == 8 and d["steps"] > 0
+    series = json.loads((tmp_path / "wave.pvtu.series").read_text())["files"]
+    elements = json.loads((tmp_path / "wave_element.pvtu.series").read_text())["files"]
+    assert [f["time"] for f in series][0] == 0.0 and series[-1]["time"] == 0.05 and len(series) == len(elements) >= 3
+    g = read_grid(str(tmp_path / series[-1]["name"]))
+    eg = read_grid(str(tmp_path / elements[-1]["name"]))
+    assert eg["n_cells"] == d["n_elements"] and g["n_points"] == 9 * d["n_elements"]
+    assert np.isfinite(g["point_data"]["Pressure"]).all() and (eg["cell_data"]["N"] >= N).all()
