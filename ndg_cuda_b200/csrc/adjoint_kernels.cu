@@ -133,10 +133,12 @@ static AdjCoeffs<N, R> make_adj_coeffs() {
 // Pressure at the receivers of a tile, one warp: sum of w_r . p over the
 // element's nodes, lanes striding the nodes, then a shuffle reduction in a
 // fixed order (the same result wherever it is evaluated). FP64 in both forms.
-template <int NN>
+// Receiver sample sum_i w_i p_i over an element's nodes, with the element's
+// tile block p laid out in rows of pitch P (node i of n per row).
+template <int n, int P>
 __device__ __forceinline__ double receiver_value(const double* __restrict__ w, const double* p, int lane) {
     double s = 0.0;
-    for (int i = lane; i < NN; i += 32) s = fma(w[i], p[i], s);
+    for (int i = lane; i < n * n; i += 32) s = fma(w[i], p[(i / n) * P + i % n], s);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     return s;
@@ -144,8 +146,11 @@ __device__ __forceinline__ double receiver_value(const double* __restrict__ w, c
 
 // ---------------------------------------------------------------------------
 // Forward stage with a wave speed per element, one thread per (field,
-// element, line): the bulk-copied q tile in FP64, then R arrays (offsets in
-// R values past it), then the mbarrier.
+// element, line), the line fastest: the FP64 q tile, then R arrays
+// (offsets in R values past it). Node arrays have rows of pitch P and
+// element strides chosen by bank::search for this thread order (for even n,
+// e.g. N = 7: pitch 9, element stride 72, both sweeps conflict-free); the q
+// tile arrives by 8-byte cp.async copies into that layout.
 template <int N, typename R>
 struct SpeedTile {
     static constexpr int n = N + 1, NN = n * n;
@@ -156,22 +161,36 @@ struct SpeedTile {
     static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
     static constexpr int EPB = bank::pow2_floor(raw >= 2 ? (raw < 16 ? raw : 16) : 2);
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
-    static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;
-    static constexpr int kQd = 3 * EPB * NN;             // doubles: the q tile
-    static constexpr int kG = 0;                         // [3][EPB][NN] time derivative G
-    static constexpr int kOwn = kG + 3 * EPB * NN;       // [3][EPB][4][n] own side traces
-    static constexpr int kFar = kOwn + 3 * EPB * 4 * n;  // [3][EPB][4][n] far traces, then element side fluxes
-    static constexpr int kJ = kFar + 3 * EPB * 4 * n;    // [EPB][NN] 1/J
-    static constexpr int kS = kJ + EPB * NN;             // [EPB][4] edge metric per side
+    static constexpr int kWarps = kThreads / 32;
+    static constexpr int kBlockIters = (3 * EPB + kWarps - 1) / kWarps;
+    static constexpr int kLaneIters = (NN + 31) / 32;
+    static constexpr bank::Strides Ld = bank::search(N, EPB, 16, false);                              // FP64 tile
+    static constexpr bank::Strides Lr = bank::search(N, EPB, static_cast<int>(128 / sizeof(R)), false);  // R arrays
+    static constexpr int P = Ld.P, ESd = Ld.ES, QSd = Ld.QS, ESr = Lr.ES, QSr = Lr.QS, SE = Lr.SE, FS = Lr.FS;
+    static constexpr int kQd = 3 * QSd;              // doubles: the q tile
+    static constexpr int kG = 0;                     // [3][QSr] time derivative G
+    static constexpr int kOwn = kG + 3 * QSr;        // [3][FS] own side traces
+    static constexpr int kFar = kOwn + 3 * FS;       // [3][FS] far traces, then element side fluxes
+    static constexpr int kJ = kFar + 3 * FS;         // [EPB][ESr] 1/J
+    static constexpr int kS = kJ + EPB * ESr;        // [EPB][4] edge metric per side
     static constexpr int kRs = kS + EPB * 4;
-    static constexpr size_t kBarOff = (sizeof(double) * kQd + sizeof(R) * kRs + 15) / 16 * 16;
-    static constexpr size_t kBytes = kBarOff + 16;
+    static constexpr size_t kBytes = sizeof(double) * kQd + sizeof(R) * kRs;
+    // Offset within an element of node nd = i n + j.
+    __device__ static __forceinline__ int node(int nd) {
+        if constexpr (P == n) {
+            return nd;
+        } else {
+            const int i = nd / n;
+            return i * P + (nd - i * n);
+        }
+    }
 };
 
 template <int N, typename R>
 __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(SpeedStageArgs a, const __grid_constant__ SpeedCoeffs<N, R> cf) {
     using T = SpeedTile<N, R>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
+    constexpr int P = T::P, ESd = T::ESd, QSd = T::QSd, ESr = T::ESr, QSr = T::QSr, SE = T::SE, FS = T::FS;
     extern __shared__ __align__(128) double smem[];
     double* qs = smem;
     R* rs = reinterpret_cast<R*>(smem + T::kQd);
@@ -180,15 +199,12 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
     R* far_s = rs + T::kFar;
     R* js = rs + T::kJ;
     R* ss = rs + T::kS;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + T::kBarOff);
-    constexpr int FS = EPB * 4 * n;
 
     const int tid = threadIdx.x;
     const int64_t K = a.n_elements;
     const int64_t Kp = a.field_stride;
     const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
     const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
-    const int ne_copy = (ne + 1) & ~1;
     double* q = a.q;
     double* k = a.k;
     const R* tr_in = pick<R>(a.trace_in, a.trace_in_f);
@@ -204,12 +220,21 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
     const bool active = f < 3 && e < ne;
     const int64_t ge = e0 + e;
 
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-        const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
-        mbar_expect_tx(bar, 3 * bytes);
-        for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
+    // q tile: warps take (field, element) blocks, lanes their nodes.
+    const int warp = tid >> 5, lane = tid & 31;
+    int lane_node[T::kLaneIters];
+#pragma unroll
+    for (int it = 0; it < T::kLaneIters; ++it) lane_node[it] = T::node(lane + 32 * it);
+#pragma unroll
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const double* src = q + (ff * Kp + e0 + el) * NN;
+            double* dst = qs + ff * QSd + el * ESd;
+#pragma unroll
+            for (int it = 0; it < T::kLaneIters; ++it)
+                if (lane + 32 * it < NN) cp_async8(dst + lane_node[it], src + lane + 32 * it);
+        }
     }
     // Corners in FP64: their differences are formed before rounding to R.
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
@@ -219,7 +244,7 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
         for (int s = 0; s < 4; ++s) {
             const int2 lk = a.link[4 * ge + s];
             const R v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : R(0);
-            far_s[f * FS + (e * 4 + s) * n + m] = v;
+            far_s[f * FS + e * SE + s * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
         x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
@@ -240,30 +265,30 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
         const R xe = x_eta(tm), ye = y_eta(tm);
         for (int j = f; j < n; j += 3) {
             const R tj = xn[j];
-            js[e * NN + m * n + j] = rcp<R>(x_xi(tj) * ye - xe * y_xi(tj));
+            js[e * ESr + m * P + j] = rcp<R>(x_xi(tj) * ye - xe * y_xi(tj));
         }
     }
+    cp_async_wait_all();
     __syncthreads();
-    if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
 
     // Flux lines (X, Y) = (u, v), (p, 0), (0, p) for the fields p, u, v: the
     // absent component is scaled by zero.
-    const double* Qe = qs + e * NN;
-    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : Qe;
-    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : Qe;
+    const double* Qe = qs + e * ESd;
+    const double* Xe = f == 0 ? Qe + 1 * QSd : Qe;
+    const double* Ye = f == 0 ? Qe + 2 * QSd : Qe;
     const R sx = f == 2 ? R(0) : R(1), sy = f == 1 ? R(0) : R(1);
     if (active) {
-        const double* Qf = Qe + f * EPB * NN;
+        const double* Qf = Qe + f * QSd;
         R b = 0, t = 0, r = 0, l = 0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            const R qr = R(Qf[m * n + j]), qc = R(Qf[j * n + m]);
+            const R qr = R(Qf[m * P + j]), qc = R(Qf[j * P + m]);
             b = fma(lm[j], qr, b);
             t = fma(lp[j], qr, t);
             r = fma(lp[j], qc, r);
             l = fma(lm[j], qc, l);
         }
-        R* o = own_s + f * FS + e * 4 * n;
+        R* o = own_s + f * FS + e * SE;
         o[0 * n + m] = b;
         o[2 * n + (N - m)] = t;
         o[1 * n + m] = r;
@@ -282,7 +307,7 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
             const int role = (lk.y >> 5) & 1;
             const double2 nd = a.normal[4 * ge + s];
             const R nx = R(nd.x), ny = R(nd.y);
-            const int o = (e * 4 + s) * n + m;
+            const int o = e * SE + s * n + m;
             const R op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
             R fp_, fu_, fv_, cface = ce;
             if (kind == kInterior) {
@@ -322,21 +347,21 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
 
     const R* Dh = cf.dhat;
     const R* iw = cf.iw;
-    const R* F = far_s + f * FS + e * 4 * n;
+    const R* F = far_s + f * FS + e * SE;
 
     if (active) {
         const int j = m;
         R col[n];
 #pragma unroll
-        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * (sx * R(Xe[i * n + j])) - x_eta(xn[i]) * (sy * R(Ye[i * n + j]));
+        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * (sx * R(Xe[i * P + j])) - x_eta(xn[i]) * (sy * R(Ye[i * P + j]));
         const R fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
-        R* G = gs + (f * EPB + e) * NN + j;
+        R* G = gs + f * QSr + e * ESr + j;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             R acc = 0;
 #pragma unroll
             for (int mm = 0; mm < n; ++mm) acc = fma(Dh[i * n + mm], col[mm], acc);
-            G[i * n] = -fma(acc, ce, (fr * lp[i] + fl3 * lm[i]) * iw[i]);
+            G[i * P] = -fma(acc, ce, (fr * lp[i] + fl3 * lm[i]) * iw[i]);
         }
     }
     __syncthreads();
@@ -345,10 +370,10 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
         const int i = m;
         R line[n];
 #pragma unroll
-        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * (sx * R(Xe[i * n + j])) + x_xi(xn[j]) * (sy * R(Ye[i * n + j]));
+        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * (sx * R(Xe[i * P + j])) + x_xi(xn[j]) * (sy * R(Ye[i * P + j]));
         const R ft = F[2 * n + (N - i)], fb = F[0 * n + i];
-        R* G = gs + (f * EPB + e) * NN + i * n;
-        const R* jrow = js + e * NN + i * n;
+        R* G = gs + f * QSr + e * ESr + i * P;
+        const R* jrow = js + e * ESr + i * P;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             R acc = 0;
@@ -359,40 +384,48 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
     }
     __syncthreads();
 
-    // RK update in FP64.
-    double kold[T::kNodeIters];
+    // RK update in FP64: warps take (field, element) blocks, lanes their nodes.
+    double kold[T::kBlockIters][T::kLaneIters];
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        kold[c] = (!a.first && ff < 3 && r < ne * NN) ? k[(ff * Kp + e0) * NN + r] : 0.0;
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        const bool live = !a.first && b < 3 * EPB && el < ne;
+        const double* kb = k + (ff * Kp + e0 + el) * NN;
+#pragma unroll
+        for (int it = 0; it < T::kLaneIters; ++it) kold[bi][it] = (live && lane + 32 * it < NN) ? kb[lane + 32 * it] : 0.0;
     }
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        if (ff < 3 && r < ne * NN) {
-            const double G = static_cast<double>(gs[ff * EPB * NN + r]);
-            const double kn = a.first ? G : fma(a.rk_a, kold[c], G);
-            const double qo = qs[ff * EPB * NN + r];
-            const double qn = fma(a.gdt, kn, qo);
-            const int64_t gi = (ff * Kp + e0) * NN + r;
-            if (a.q_save) a.q_save[gi] = qo;
-            k[gi] = kn;
-            q[gi] = qn;
-            qs[ff * EPB * NN + r] = qn;
-            if (a.G_out) a.G_out[gi] = G;
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const int64_t gb = (ff * Kp + e0 + el) * NN;
+#pragma unroll
+            for (int it = 0; it < T::kLaneIters; ++it) {
+                const int nd = lane + 32 * it;
+                if (nd < NN) {
+                    const int sd = ff * QSd + el * ESd + lane_node[it];
+                    const double G = static_cast<double>(gs[ff * QSr + el * ESr + lane_node[it]]);
+                    const double kn = a.first ? G : fma(a.rk_a, kold[bi][it], G);
+                    const double qo = qs[sd];
+                    const double qn = fma(a.gdt, kn, qo);
+                    if (a.q_save) a.q_save[gb + nd] = qo;
+                    k[gb + nd] = kn;
+                    q[gb + nd] = qn;
+                    qs[sd] = qn;
+                    if (a.G_out) a.G_out[gb + nd] = G;
+                }
+            }
         }
     }
     __syncthreads();
 
     if (active) {
-        const double* row = qs + (f * EPB + e) * NN + m * n;
-        const double* cl = qs + (f * EPB + e) * NN + m;
+        const double* row = qs + f * QSd + e * ESd + m * P;
+        const double* cl = qs + f * QSd + e * ESd + m;
         R b = 0, t = 0, r = 0, l = 0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
-            const R qr = R(row[j]), qc = R(cl[j * n]);
+            const R qr = R(row[j]), qc = R(cl[j * P]);
             b = fma(lm[j], qr, b);
             t = fma(lp[j], qr, t);
             r = fma(lp[j], qc, r);
@@ -408,7 +441,7 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
         for (int r = 0; r < a.rec.n; ++r) {
             const int64_t el = a.rec.elem[r] - e0;
             if (el < 0 || el >= ne) continue;
-            const double v = receiver_value<NN>(a.rec.w + static_cast<int64_t>(r) * NN, qs + el * NN, tid);
+            const double v = receiver_value<n, P>(a.rec.w + static_cast<int64_t>(r) * NN, qs + el * ESd, tid);
             if (tid == 0) a.samples[r] = v;
         }
     }
@@ -416,8 +449,10 @@ __global__ void __launch_bounds__(SpeedTile<N, R>::kThreads) speed_stage_kernel(
 
 // ---------------------------------------------------------------------------
 // Adjoint stage. Tile of EPB elements, one thread per (field, element, line)
-// as the forward. Shared memory: FP64 arrays first (the two bulk-copied
-// tiles, the receiver residuals and masks), then R arrays, then the mbarrier.
+// as the forward. Shared memory: FP64 arrays first (the lq and qs tiles,
+// copied by 8-byte cp.async into rows of pitch P, the receiver residuals
+// and masks), then R arrays; node and side arrays use the strides
+// bank::search finds for this thread order.
 template <int N, typename R>
 struct AdjTile {
     static constexpr int n = N + 1;
@@ -429,29 +464,40 @@ struct AdjTile {
     static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
     static constexpr int EPB = raw >= 2 ? (raw & ~1) : 2;
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
-    static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;
-    static constexpr int FS = EPB * 4 * n;
+    static constexpr int kWarps = kThreads / 32;
+    static constexpr int kBlockIters = (3 * EPB + kWarps - 1) / kWarps;
+    static constexpr int kLaneIters = (NN + 31) / 32;
+    static constexpr bank::Strides Ld = bank::search(N, EPB, 16, false);                              // FP64 tiles
+    static constexpr bank::Strides Lr = bank::search(N, EPB, static_cast<int>(128 / sizeof(R)), false);  // R arrays
+    static constexpr int P = Ld.P, ESd = Ld.ES, QSd = Ld.QS, ESr = Lr.ES, QSr = Lr.QS, SE = Lr.SE, FS = Lr.FS;
     // doubles
-    static constexpr int kL = 0;                   // [3][EPB][NN] lq (bulk copy), then lq + volume transpose
-    static constexpr int kQ = kL + 3 * EPB * NN;   // [3][EPB][NN] forward stage input qs (bulk copy)
-    static constexpr int kRes = kQ + 3 * EPB * NN; // [kMaxReceivers] weighted misfit residuals
+    static constexpr int kL = 0;                    // [3][QSd] lq, then lq + volume transpose
+    static constexpr int kQ = kL + 3 * QSd;         // [3][QSd] forward stage input qs
+    static constexpr int kRes = kQ + 3 * QSd;       // [kMaxReceivers] weighted misfit residuals
     static constexpr int kMask = kRes + kMaxReceivers;  // [EPB] receivers of each element (bit mask)
     static constexpr int kDoubles = kMask + EPB;
     // R values past the doubles
-    static constexpr int kNu = 0;                  // [3][EPB][NN] nu = -mu / J, later nu'
-    static constexpr int kTp = kNu + 3 * EPB * NN; // [EPB][NN] second accumulator of the pressure's transpose
-    static constexpr int kJ = kTp + EPB * NN;      // [EPB][NN] 1/J
-    static constexpr int kOwn = kJ + EPB * NN;     // [3][EPB][4][n] side traces of qs
-    static constexpr int kEll = kOwn + 3 * FS;     // [3][EPB][4][n] lift transpose, then own-trace adjoint, then next lift transpose
-    static constexpr int kFar = kEll + 3 * FS;     // [3][EPB][4][n] neighbours' adjoint far traces
-    static constexpr int kUp = kFar + 3 * FS;      // [EPB][4][n] flux part of the c-derivative per side node
-    static constexpr int kVd = kUp + FS;           // [3][EPB][n] volume part of the c-derivative per line
-    static constexpr int kS = kVd + 3 * EPB * n;   // [EPB][4] edge metric
-    static constexpr int kCf = kS + 4 * EPB;       // [EPB][4] face speed
+    static constexpr int kNu = 0;                   // [3][QSr] nu = -mu / J, later nu'
+    static constexpr int kTp = kNu + 3 * QSr;       // [EPB][ESr] second accumulator of the pressure's transpose
+    static constexpr int kJ = kTp + EPB * ESr;      // [EPB][ESr] 1/J
+    static constexpr int kOwn = kJ + EPB * ESr;     // [3][FS] side traces of qs
+    static constexpr int kEll = kOwn + 3 * FS;      // [3][FS] lift transpose, then own-trace adjoint, then next lift transpose
+    static constexpr int kFar = kEll + 3 * FS;      // [3][FS] neighbours' adjoint far traces
+    static constexpr int kUp = kFar + 3 * FS;       // [EPB][SE] flux part of the c-derivative per side node
+    static constexpr int kVd = kUp + EPB * SE;      // [3][EPB][n] volume part of the c-derivative per line
+    static constexpr int kS = kVd + 3 * EPB * n;    // [EPB][4] edge metric
+    static constexpr int kCf = kS + 4 * EPB;        // [EPB][4] face speed
     static constexpr int kRs = kCf + 4 * EPB;
-    static constexpr size_t kBarOff = (sizeof(double) * kDoubles + sizeof(R) * kRs + 15) / 16 * 16;
-    static constexpr size_t kBytes = kBarOff + 16;
-    static_assert(kBytes <= static_cast<size_t>(EPB * per_element_bytes + fixed_bytes), "layout exceeds its budget");
+    static constexpr size_t kBytes = sizeof(double) * kDoubles + sizeof(R) * kRs;
+    // Offset within an element of node nd = i n + j.
+    __device__ static __forceinline__ int node(int nd) {
+        if constexpr (P == n) {
+            return nd;
+        } else {
+            const int i = nd / n;
+            return i * P + (nd - i * n);
+        }
+    }
 };
 
 // t += c v with the form's rounding: one FMA in FP64; in the FP32 form the
@@ -465,6 +511,7 @@ template <int N, typename R>
 __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(AdjointStageArgs a, const __grid_constant__ AdjCoeffs<N, R> cf) {
     using T = AdjTile<N, R>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB, FS = T::FS;
+    constexpr int P = T::P, ESd = T::ESd, QSd = T::QSd, ESr = T::ESr, QSr = T::QSr, SE = T::SE;
     extern __shared__ __align__(128) double smem[];
     double* ls = smem + T::kL;
     double* qs = smem + T::kQ;
@@ -481,7 +528,6 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
     R* vd = rs + T::kVd;
     R* ss = rs + T::kS;
     R* cfs = rs + T::kCf;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + T::kBarOff);
     const R* atr_in = pick<R>(a.atr_in, a.atr_in_f);
     R* atr_out = pick<R>(a.atr_out, a.atr_out_f);
 
@@ -490,7 +536,6 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
     const int64_t Kp = a.field_stride;
     const int64_t e0 = static_cast<int64_t>(blockIdx.x) * EPB;
     const int ne = static_cast<int>((K - e0) < EPB ? (K - e0) : EPB);
-    const int ne_copy = (ne + 1) & ~1;
     const R* xn = cf.xn;
     const R* lm = cf.lm;
     const R* lp = cf.lp;
@@ -505,19 +550,28 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
     const bool active = f < 3 && e < ne;
     const int64_t ge = e0 + e;
 
-    // Prologue: bulk copies of the lq and qs tiles; adjoint far traces of
-    // the neighbours, metrics, J, edge metrics and face speeds.
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-        const uint32_t bytes = static_cast<uint32_t>(ne_copy * NN * sizeof(double));
-        mbar_expect_tx(bar, 6 * bytes);
-        for (int ff = 0; ff < 3; ++ff) {
-            bulk_load(ls + ff * EPB * NN, a.lq + (ff * Kp + e0) * NN, bytes, bar);
-            bulk_load(qs + ff * EPB * NN, a.qs + (ff * Kp + e0) * NN, bytes, bar);
+    // Prologue: asynchronous copies of the lq and qs tiles (warps take
+    // (field, element) blocks, lanes their nodes); adjoint far traces of the
+    // neighbours, metrics, J, edge metrics and face speeds.
+    const int warp = tid >> 5, lane = tid & 31;
+    int lane_node[T::kLaneIters];
+#pragma unroll
+    for (int it = 0; it < T::kLaneIters; ++it) lane_node[it] = T::node(lane + 32 * it);
+#pragma unroll
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const int64_t gb = (ff * Kp + e0 + el) * NN;
+            const int sb = ff * QSd + el * ESd;
+#pragma unroll
+            for (int it = 0; it < T::kLaneIters; ++it)
+                if (lane + 32 * it < NN) {
+                    cp_async8(ls + sb + lane_node[it], a.lq + gb + lane + 32 * it);
+                    cp_async8(qs + sb + lane_node[it], a.qs + gb + lane + 32 * it);
+                }
         }
     }
-    for (int i = tid; i < EPB * NN; i += T::kThreads) tp[i] = R(0);
+    for (int i = tid; i < EPB * ESr; i += T::kThreads) tp[i] = R(0);
     if (tid < EPB) rmask[tid] = 0ull;
     // Corners in FP64: their differences are formed before rounding to R.
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
@@ -527,7 +581,7 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
         for (int s = 0; s < 4; ++s) {
             const int2 lk = a.link[4 * ge + s];
             const R v = (((lk.y >> 2) & 7) == kInterior) ? atr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : R(0);
-            far_s[f * FS + (e * 4 + s) * n + m] = v;
+            far_s[f * FS + e * SE + s * n + m] = v;
         }
         const double* c = a.corners + 8 * ge;
         x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
@@ -550,34 +604,39 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
         const R xe = x_eta(tm), ye = y_eta(tm);
         for (int j = f; j < n; j += 3) {
             const R tj = xn[j];
-            js[e * NN + m * n + j] = rcp<R>(x_xi(tj) * ye - xe * y_xi(tj));
+            js[e * ESr + m * P + j] = rcp<R>(x_xi(tj) * ye - xe * y_xi(tj));
         }
     }
+    cp_async_wait_all();
     __syncthreads();
-    if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
 
     // Node pass: mu = lk + gdt lq; lk = a mu (kept in registers for mu');
     // nu = -mu / J. One warp evaluates the misfit residuals of the
     // receivers in the tile at the state qs.
-    double kn[T::kNodeIters];
+    double kn[T::kBlockIters][T::kLaneIters];
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        kn[c] = 0.0;
-        if (ff < 3 && r < ne * NN) {
-            const int64_t gi = (ff * Kp + e0) * NN + r;
-            const double mu = fma(a.gdt, ls[ff * EPB * NN + r], a.lk[gi]);
-            kn[c] = a.rk_a * mu;
-            a.lk[gi] = kn[c];
-            nu[ff * EPB * NN + r] = R(-mu) * js[r];
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        const bool live = b < 3 * EPB && el < ne;
+        const int64_t gb = (ff * Kp + e0 + el) * NN;
+#pragma unroll
+        for (int it = 0; it < T::kLaneIters; ++it) {
+            const int nd = lane + 32 * it;
+            kn[bi][it] = 0.0;
+            if (live && nd < NN) {
+                const int64_t gi = gb + nd;
+                const double mu = fma(a.gdt, ls[ff * QSd + el * ESd + lane_node[it]], a.lk[gi]);
+                kn[bi][it] = a.rk_a * mu;
+                a.lk[gi] = kn[bi][it];
+                nu[ff * QSr + el * ESr + lane_node[it]] = R(-mu) * js[el * ESr + lane_node[it]];
+            }
         }
     }
     if (a.inject && tid < 32) {
         for (int r = 0; r < a.rec.n; ++r) {
             const int64_t el = a.rec.elem[r] - e0;
             if (el < 0 || el >= ne) continue;
-            const double v = receiver_value<NN>(a.rec.w + static_cast<int64_t>(r) * NN, qs + el * NN, tid);
+            const double v = receiver_value<n, P>(a.rec.w + static_cast<int64_t>(r) * NN, qs + el * ESd, tid);
             if (tid == 0) {
                 res[r] = a.wdt * (v - a.target[r]);
                 rmask[el] |= 1ull << r;
@@ -591,14 +650,14 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
     // line adjoints A (of X) and B (of Y) back to those fields:
     //   f = p: A -> lu, B -> lv;  f = u: A -> lp;  f = v: B -> lp (via tp).
     // vdot accumulates X A + Y B (the volume term's derivative in c_e).
-    const double* Qe = qs + e * NN;
-    const double* Xe = f == 0 ? Qe + 1 * EPB * NN : Qe;
-    const double* Ye = f == 0 ? Qe + 2 * EPB * NN : Qe;
+    const double* Qe = qs + e * ESd;
+    const double* Xe = f == 0 ? Qe + 1 * QSd : Qe;
+    const double* Ye = f == 0 ? Qe + 2 * QSd : Qe;
     const R sx = f == 2 ? R(0) : R(1), sy = f == 1 ? R(0) : R(1);
-    double* O1 = f == 0 ? ls + (1 * EPB + e) * NN : ls + e * NN;  // f = p, u
-    R* O1v = tp + e * NN;                                          // f = v
-    double* O2 = ls + (2 * EPB + e) * NN;                          // f = p only
-    const R* Nf = nu + (f * EPB + e) * NN;
+    double* O1 = f == 0 ? ls + 1 * QSd + e * ESd : ls + e * ESd;  // f = p, u
+    R* O1v = tp + e * ESr;                                          // f = v
+    double* O2 = ls + 2 * QSd + e * ESd;                            // f = p only
+    const R* Nf = nu + f * QSr + e * ESr;
     R vdot = 0;
     // xi columns (eta index j = m): alpha = Dhat^T nu(:, j); lift transpose
     // of sides 1 and 3; the side traces of qs.
@@ -606,14 +665,14 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
         const int j = m;
         R col[n];
 #pragma unroll
-        for (int i = 0; i < n; ++i) col[i] = Nf[i * n + j];
+        for (int i = 0; i < n; ++i) col[i] = Nf[i * P + j];
         R l1 = 0, l3 = 0;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             l1 = fma(col[i], lpw[i], l1);
             l3 = fma(col[i], lmw[i], l3);
         }
-        R* L = ell + f * FS + e * 4 * n;
+        R* L = ell + f * FS + e * SE;
         L[1 * n + j] = l1;
         L[3 * n + (N - j)] = l3;
 #pragma unroll
@@ -622,7 +681,7 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
 #pragma unroll
             for (int i = 0; i < n; ++i) al = fma(Dh[i * n + mm], col[i], al);
             const R A = y_eta(xn[mm]) * al, B = -x_eta(xn[mm]) * al;
-            const int node = mm * n + j;
+            const int node = mm * P + j;
             vdot = fma(sx * R(Xe[node]), A, fma(sy * R(Ye[node]), B, vdot));
             if (f == 2)
                 add_scaled(O1v + node, ce, B);
@@ -630,17 +689,17 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
                 add_scaled(O1 + node, ce, A);
             if (f == 0) add_scaled(O2 + node, ce, B);
         }
-        const double* Qf = Qe + f * EPB * NN;
+        const double* Qf = Qe + f * QSd;
         R b = 0, t = 0, r = 0, l = 0;
 #pragma unroll
         for (int jj = 0; jj < n; ++jj) {
-            const R qr = R(Qf[m * n + jj]), qc = R(Qf[jj * n + m]);
+            const R qr = R(Qf[m * P + jj]), qc = R(Qf[jj * P + m]);
             b = fma(lm[jj], qr, b);
             t = fma(lp[jj], qr, t);
             r = fma(lp[jj], qc, r);
             l = fma(lm[jj], qc, l);
         }
-        R* o = own_s + f * FS + e * 4 * n;
+        R* o = own_s + f * FS + e * SE;
         o[0 * n + m] = b;
         o[2 * n + (N - m)] = t;
         o[1 * n + m] = r;
@@ -654,14 +713,14 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
         const int i = m;
         R row[n];
 #pragma unroll
-        for (int j = 0; j < n; ++j) row[j] = Nf[i * n + j];
+        for (int j = 0; j < n; ++j) row[j] = Nf[i * P + j];
         R l2 = 0, l0 = 0;
 #pragma unroll
         for (int j = 0; j < n; ++j) {
             l2 = fma(row[j], lpw[j], l2);
             l0 = fma(row[j], lmw[j], l0);
         }
-        R* L = ell + f * FS + e * 4 * n;
+        R* L = ell + f * FS + e * SE;
         L[2 * n + (N - i)] = l2;
         L[0 * n + i] = l0;
 #pragma unroll
@@ -670,7 +729,7 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
 #pragma unroll
             for (int j = 0; j < n; ++j) be = fma(Dh[j * n + mm], row[j], be);
             const R A = -y_xi(xn[mm]) * be, B = x_xi(xn[mm]) * be;
-            const int node = i * n + mm;
+            const int node = i * P + mm;
             vdot = fma(sx * R(Xe[node]), A, fma(sy * R(Ye[node]), B, vdot));
             if (f == 2)
                 add_scaled(O1v + node, ce, B);
@@ -697,7 +756,7 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
             const int role = (lk.y >> 5) & 1;
             const double2 nd = a.normal[4 * ge + s];
             const R nx = R(nd.x), ny = R(nd.y);
-            const int o = (e * 4 + s) * n + m;
+            const int o = e * SE + s * n + m;
             const R cface = cfs[e * 4 + s];
             const R sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cface;
             const R pp = sc * ell[o], pu = sc * ell[FS + o], pv = sc * ell[2 * FS + o];
@@ -738,15 +797,18 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
     // side-trace adjoints back to the nodes), the misfit injection, then
     // nu' = -(lk' + gdt_next lq') / J for the next stage.
 #pragma unroll
-    for (int c = 0; c < T::kNodeIters; ++c) {
-        const int idx = tid + c * T::kThreads;
-        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
-        if (ff < 3 && r < ne * NN) {
-            const int el = r / NN, node = r - el * NN;
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (!(b < 3 * EPB && el < ne)) continue;
+        const int64_t gb = (ff * Kp + e0 + el) * NN;
+#pragma unroll
+        for (int it = 0; it < T::kLaneIters; ++it) {
+            const int node = lane + 32 * it;
+            if (node >= NN) continue;
             const int i = node / n, j = node - i * n;
-            const R* Lo = ell + ff * FS + el * 4 * n;
-            double v = ls[ff * EPB * NN + r];
-            if (ff == 0) v += static_cast<double>(tp[r]);
+            const R* Lo = ell + ff * FS + el * SE;
+            double v = ls[ff * QSd + el * ESd + lane_node[it]];
+            if (ff == 0) v += static_cast<double>(tp[el * ESr + lane_node[it]]);
             if constexpr (std::is_same_v<R, double>) {
                 v = fma(lm[j], Lo[0 * n + i], v);
                 v = fma(lp[j], Lo[2 * n + (N - i)], v);
@@ -767,8 +829,8 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
                     v = fma(res[rc], a.rec.w[static_cast<int64_t>(rc) * NN + node], v);
                 }
             }
-            a.lq[(ff * Kp + e0) * NN + r] = v;
-            nu[ff * EPB * NN + r] = R(-fma(a.gdt_next, v, kn[c])) * js[r];
+            a.lq[gb + node] = v;
+            nu[ff * QSr + el * ESr + lane_node[it]] = R(-fma(a.gdt_next, v, kn[bi][it])) * js[el * ESr + lane_node[it]];
         }
     }
     __syncthreads();
@@ -776,17 +838,17 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
     // Lift transpose of nu' on the four sides (column m: sides 1, 3; row m:
     // sides 2, 0); per element, the c-derivative accumulators (FP64).
     if (active) {
-        const R* Nn = nu + (f * EPB + e) * NN;
+        const R* Nn = nu + f * QSr + e * ESr;
         R l1 = 0, l3 = 0, l2 = 0, l0 = 0;
 #pragma unroll
         for (int i = 0; i < n; ++i) {
-            const R cv = Nn[i * n + m], rv = Nn[m * n + i];
+            const R cv = Nn[i * P + m], rv = Nn[m * P + i];
             l1 = fma(cv, lpw[i], l1);
             l3 = fma(cv, lmw[i], l3);
             l2 = fma(rv, lpw[i], l2);
             l0 = fma(rv, lmw[i], l0);
         }
-        R* L = ell + f * FS + e * 4 * n;
+        R* L = ell + f * FS + e * SE;
         L[1 * n + m] = l1;
         L[3 * n + (N - m)] = l3;
         L[2 * n + (N - m)] = l2;
@@ -800,7 +862,7 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
         A[0] += vsum;
         for (int s = 0; s < 4; ++s) {
             double us = 0.0;
-            for (int i = 0; i < n; ++i) us += static_cast<double>(up[(tid * 4 + s) * n + i]);
+            for (int i = 0; i < n; ++i) us += static_cast<double>(up[tid * SE + s * n + i]);
             A[1 + s] += us;
         }
     }
@@ -817,7 +879,7 @@ __global__ void __launch_bounds__(AdjTile<N, R>::kThreads) adjoint_stage_kernel(
             const int role = (lk.y >> 5) & 1;
             const double2 nd = a.normal[4 * ge + s];
             const R nx = R(nd.x), ny = R(nd.y);
-            const int o = (e * 4 + s) * n + m;
+            const int o = e * SE + s * n + m;
             const R sc = (role ? -ss[e * 4 + s] : ss[e * 4 + s]) * cfs[e * 4 + s];
             const R pp = sc * ell[o], pu = sc * ell[FS + o], pv = sc * ell[2 * FS + o];
             const R dn = R(0.5) * (nx * pu + ny * pv);

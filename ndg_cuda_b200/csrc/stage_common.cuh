@@ -164,7 +164,11 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //   SE, FS  element and field strides of the side arrays (4 n values per
 //           element, value m of side s at s n + m), the same way.
 // Every candidate's wavefront count is evaluated exactly, group by group,
-// at compile time. EPB must divide G (whole lines per group).
+// at compile time. EPB must divide G (whole lines per group). The search
+// also serves kernels that order their threads (field, element, line), line
+// fastest (element_fast = false); there an odd row pitch and an element
+// stride that puts consecutive elements half a group apart make both sweeps
+// conflict-free when n divides G.
 namespace bank {
 
 struct Strides {
@@ -190,18 +194,24 @@ constexpr int address(int pat, const Strides& L, int n, int f, int e, int m) {
 }
 
 // Wavefronts of one instruction in the group of threads [g0, g0 + G): the
-// most distinct addresses that share a bank. Zero-array reads of elements
-// e > 0 repeat element 0's address on the same line (a broadcast) and are
-// skipped.
-constexpr int group_wavefronts(int pat, const Strides& L, int n, int EPB, int G, int g0) {
+// most distinct addresses that share a bank. Zero-array reads of a line
+// already read by another element of the group repeat its address (a
+// broadcast) and are skipped.
+constexpr int group_wavefronts(int pat, const Strides& L, int n, int EPB, int G, int g0, bool element_fast) {
     int bank[32] = {};
+    bool seen_zero[32] = {};
     int worst = 0;
     for (int t = g0; t < g0 + G; ++t) {
         const int f = t / (EPB * n);
         if (f >= 3) break;
-        const int rr = t - f * EPB * n, m = rr / EPB, e = rr - m * EPB;
+        const int rr = t - f * EPB * n;
+        const int m = element_fast ? rr / EPB : rr - (rr / n) * n;
+        const int e = element_fast ? rr - m * EPB : rr / n;
         const bool zero = (pat == kRowX || pat == kColX) ? f == 2 : ((pat == kRowY || pat == kColY) ? f == 1 : false);
-        if (zero && e > 0) continue;
+        if (zero) {
+            if (seen_zero[m]) continue;  // another element's read of this line: a broadcast
+            seen_zero[m] = true;
+        }
         const int b = address(pat, L, n, f, e, m) % G;
         if (++bank[b] > worst) worst = bank[b];
     }
@@ -210,25 +220,27 @@ constexpr int group_wavefronts(int pat, const Strides& L, int n, int EPB, int G,
 
 // Sum over the groups within one field (straddling = false) or over the (at
 // most two) groups that hold a field boundary (straddling = true).
-constexpr int wavefronts(int pat, const Strides& L, int n, int EPB, int G, bool straddling) {
+constexpr int wavefronts(int pat, const Strides& L, int n, int EPB, int G, bool straddling, bool element_fast) {
     const int field = EPB * n;
     const int b1 = field / G * G, b2 = 2 * field / G * G;
     const bool s1 = field % G != 0, s2 = (2 * field) % G != 0;
-    if (straddling) return (s1 ? group_wavefronts(pat, L, n, EPB, G, b1) : 0) + (s2 && b2 != b1 ? group_wavefronts(pat, L, n, EPB, G, b2) : 0);
+    if (straddling)
+        return (s1 ? group_wavefronts(pat, L, n, EPB, G, b1, element_fast) : 0) +
+               (s2 && b2 != b1 ? group_wavefronts(pat, L, n, EPB, G, b2, element_fast) : 0);
     int total = 0;
     for (int g0 = 0; g0 < 3 * field; g0 += G)
-        if (!((s1 && g0 == b1) || (s2 && g0 == b2))) total += group_wavefronts(pat, L, n, EPB, G, g0);
+        if (!((s1 && g0 == b1) || (s2 && g0 == b2))) total += group_wavefronts(pat, L, n, EPB, G, g0, element_fast);
     return total;
 }
 
-constexpr int straddling_q_cost(const Strides& L, int n, int EPB, int G) {
+constexpr int straddling_q_cost(const Strides& L, int n, int EPB, int G, bool ef) {
     int c = 0;
-    for (int p = kRowOwn; p <= kColOwn; ++p) c += 2 * wavefronts(p, L, n, EPB, G, true);  // traces and G sweeps
-    for (int p = kRowX; p <= kColY; ++p) c += wavefronts(p, L, n, EPB, G, true);
+    for (int p = kRowOwn; p <= kColOwn; ++p) c += 2 * wavefronts(p, L, n, EPB, G, true, ef);  // traces and G sweeps
+    for (int p = kRowX; p <= kColY; ++p) c += wavefronts(p, L, n, EPB, G, true, ef);
     return c;
 }
 
-constexpr Strides search(int N, int EPB, int G) {
+constexpr Strides search(int N, int EPB, int G, bool ef = true) {
     const int n = N + 1;
     Strides L{n % 2 ? n : n + 1, 0, 0, 0, 0, 0};
     int best = 1 << 30;
@@ -236,7 +248,7 @@ constexpr Strides search(int N, int EPB, int G) {
         Strides T = L;
         T.ES = s;
         T.QS = EPB * s;
-        const int c = wavefronts(kRowOwn, T, n, EPB, G, false) + wavefronts(kColOwn, T, n, EPB, G, false);
+        const int c = wavefronts(kRowOwn, T, n, EPB, G, false, ef) + wavefronts(kColOwn, T, n, EPB, G, false, ef);
         if (c < best) best = c, L.ES = s;
     }
     best = 1 << 30;
@@ -244,7 +256,7 @@ constexpr Strides search(int N, int EPB, int G) {
         Strides T = L;
         T.SE = s;
         T.FS = EPB * s;
-        const int c = wavefronts(kSideOwn, T, n, EPB, G, false);
+        const int c = wavefronts(kSideOwn, T, n, EPB, G, false, ef);
         if (c < best) best = c, L.SE = s;
     }
     best = 1 << 30;
@@ -252,22 +264,22 @@ constexpr Strides search(int N, int EPB, int G) {
         Strides T = L;
         T.QS = s;
         T.Z = 0;
-        const int c = straddling_q_cost(T, n, EPB, G);
+        const int c = straddling_q_cost(T, n, EPB, G, ef);
         if (c < best) best = c, L.QS = s;
     }
     best = 1 << 30;
     for (int z = 0; z < G; ++z) {
         Strides T = L;
         T.Z = z;
-        const int c = straddling_q_cost(T, n, EPB, G);
+        const int c = straddling_q_cost(T, n, EPB, G, ef);
         if (c < best) best = c, L.Z = z;
     }
     best = 1 << 30;
     for (int s = EPB * L.SE; s < EPB * L.SE + G; ++s) {
         Strides T = L;
         T.FS = s;
-        int c = wavefronts(kSideOwn, T, n, EPB, G, true);
-        for (int p = kSideFlux0; p <= kSideFlux2; ++p) c += wavefronts(p, T, n, EPB, G, true);
+        int c = wavefronts(kSideOwn, T, n, EPB, G, true, ef);
+        for (int p = kSideFlux0; p <= kSideFlux2; ++p) c += wavefronts(p, T, n, EPB, G, true, ef);
         if (c < best) best = c, L.FS = s;
     }
     return L;
