@@ -366,9 +366,11 @@ ndg_status ndg_pre_condition(ndg_ctx* ctx, int64_t n_adaptivity_steps, int64_t p
  * ndg_adjoint_backward returns dJ/d(p0, u0, v0) (the initial fields) and
  * dJ/dc (per element), the exact gradient of the discrete forward map (the
  * transpose of every stage, in reverse), with dt held fixed.
- * Memory: the forward keeps the state every checkpoint_interval steps; the
- * backward recomputes each interval's 3 checkpoint_interval stage inputs
- * from its checkpoint and runs the adjoint stages over it. */
+ * Memory: the forward keeps the state every checkpoint_interval steps and
+ * the 3 checkpoint_interval stage inputs of its last interval; the backward
+ * recomputes each earlier interval's stage inputs from its checkpoint, the
+ * recomputation of interval j - 1 overlapping the adjoint stages over
+ * interval j (two interval buffers when the memory allows, one otherwise). */
 typedef struct ndg_adjoint ndg_adjoint;
 
 /* An adjoint problem on the context's mesh, with n_receivers (at most 64)

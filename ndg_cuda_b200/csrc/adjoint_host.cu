@@ -23,6 +23,17 @@ struct ndg_adjoint {
     std::vector<int64_t> rec_elem;
     std::vector<double> rec_xi, rec_w;
     ndg::DeviceBuffer<double> c, q, k, G, tr[2], atr[2], lq, lk, acc, ckpt, seg, d_rec_w, targets, samples, grad;
+    // The backward recomputes interval j - 1 (on rstream, into seg2 or seg)
+    // while the adjoint sweeps interval j (on the context's stream); qfinal
+    // keeps the final state for the first adjoint stage.
+    ndg::DeviceBuffer<double> seg2, qfinal;
+    // The forward keeps its last interval's stage inputs in seg and its final
+    // state in q; the first backward after it starts from them.
+    bool last_kept = false;
+    // streams of the adjoint sweep and of the recomputation, both joined to
+    // the context's stream
+    cudaStream_t rstream = nullptr, astream = nullptr;
+    cudaEvent_t evr[2] = {nullptr, nullptr}, eva[2] = {nullptr, nullptr}, evs = nullptr;
     ndg::DeviceBuffer<float> tr_f[2], atr_f[2];  // traces of the FP32 form
     bool fp32 = false;
     ndg::DeviceBuffer<unsigned> error;
@@ -37,6 +48,10 @@ struct ndg_adjoint {
     ~ndg_adjoint() {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto* e : {&evr[0], &evr[1], &eva[0], &eva[1], &evs})
+            if (*e) cudaEventDestroy(*e);
+        if (rstream) cudaStreamDestroy(rstream);
+        if (astream) cudaStreamDestroy(astream);
     }
 };
 
@@ -146,7 +161,8 @@ dev::AdjointStageArgs adjoint_args(ndg_adjoint* a, int in) {
     return s;
 }
 
-void launch_traces_of_q(ndg_adjoint* a, int out) {
+void launch_traces_of_q(ndg_adjoint* a, int out, cudaStream_t stream = nullptr) {
+    if (!stream) stream = a->ctx->stream;
     dev::TraceArgs t{};
     t.q = a->q.ptr;
     t.trace_out = a->tr[out].ptr;
@@ -155,9 +171,9 @@ void launch_traces_of_q(ndg_adjoint* a, int out) {
     t.field_stride = a->Kp;
     t.n_instances = 1;
     if (a->fp32)
-        check_cuda(dev::launch_traces_f32(a->N, t, a->ctx->stream), "trace kernel launch");
+        check_cuda(dev::launch_traces_f32(a->N, t, stream), "trace kernel launch");
     else
-        check_cuda(dev::launch_traces(a->N, false, t, a->ctx->stream), "trace kernel launch");
+        check_cuda(dev::launch_traces(a->N, false, t, stream), "trace kernel launch");
 }
 
 void check_kernel_error(ndg_adjoint* a) {
@@ -189,7 +205,9 @@ void download_field(ndg_adjoint* a, const double* src, double* out) {
 // are in tr[in]; q_save (optional) receives each stage input (3 states per
 // step), sample_rows (optional) the receivers' pressure after each step.
 // Returns the trace buffer holding the final traces.
-int run_forward(ndg_adjoint* a, int in, int64_t first, int64_t last, double* q_save, bool sample, int64_t save_every, int64_t& launches) {
+int run_forward(ndg_adjoint* a, int in, int64_t first, int64_t last, double* q_save, bool sample, int64_t save_every, int64_t& launches,
+                cudaStream_t stream = nullptr) {
+    if (!stream) stream = a->ctx->stream;
     const size_t state = 3 * static_cast<size_t>(a->block);
     for (int64_t step = first; step <= last; ++step) {
         for (int m = 0; m < 3; ++m) {
@@ -197,7 +215,7 @@ int run_forward(ndg_adjoint* a, int in, int64_t first, int64_t last, double* q_s
             if (q_save) s.q_save = q_save + (static_cast<size_t>(step - first) * 3 + static_cast<size_t>(m)) * state;
             if (save_every > 0 && m == 0 && (step - 1) % save_every == 0) s.q_save = a->ckpt.ptr + static_cast<size_t>((step - 1) / save_every) * state;
             if (sample && m == 2 && a->rec.n > 0) s.samples = a->samples.ptr + step * a->rec.n;
-            check_cuda(dev::launch_speed_stage(a->N, a->fp32, s, a->ctx->stream), "speed stage launch");
+            check_cuda(dev::launch_speed_stage(a->N, a->fp32, s, stream), "speed stage launch");
             ++launches;
             in = 1 - in;
         }
@@ -377,11 +395,25 @@ ndg_status ndg_adjoint_forward(ndg_adjoint* adj, const double* p0, const double*
         adj->dt = dt;
         adj->n_steps = n_steps;
         adj->interval = interval;
+        const size_t seg_values = 3 * static_cast<size_t>(interval) * state;
+        if (adj->seg.count != seg_values) adj->seg.allocate(seg_values);
         int64_t launches = 0;
         check_cuda(cudaEventRecord(adj->ev[0], s), "event");
         launch_traces_of_q(adj, 0);
         ++launches;
-        run_forward(adj, 0, 1, n_steps, nullptr, true, interval, launches);
+        // Checkpoints at the starts of the intervals before the last; the
+        // last interval keeps every stage input (the backward needs them
+        // first, and a stage that keeps its input costs no more).
+        const int64_t last_first = (n_ckpt - 1) * interval + 1;
+        int in = 0;
+        if (last_first > 1) in = run_forward(adj, 0, 1, last_first - 1, nullptr, true, interval, launches);
+        run_forward(adj, in, last_first, n_steps, adj->seg.ptr, true, 0, launches);
+        // its checkpoint too (a later backward recomputes from it): the
+        // interval's first stage input
+        check_cuda(cudaMemcpyAsync(adj->ckpt.ptr + static_cast<size_t>(n_ckpt - 1) * state, adj->seg.ptr, state * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, s),
+                   "checkpoint");
+        adj->last_kept = true;
         check_cuda(cudaEventRecord(adj->ev[1], s), "event");
         check_kernel_error(adj);
         float ms = 0.0f;
@@ -426,7 +458,36 @@ ndg_status ndg_adjoint_backward(ndg_adjoint* adj, double* grad_p0, double* grad_
         const size_t state = 3 * static_cast<size_t>(adj->block);
         const int64_t I = adj->interval, n = adj->n_steps, n_ckpt = (n + I - 1) / I;
         const int R = adj->rec.n;
-        if (adj->seg.count != 3 * static_cast<size_t>(I) * state) adj->seg.allocate(3 * static_cast<size_t>(I) * state);
+        const size_t seg_values = 3 * static_cast<size_t>(I) * state;
+        if (adj->seg.count != seg_values) adj->seg.allocate(seg_values);
+        if (adj->qfinal.count != state) adj->qfinal.allocate(state);
+        // A second interval buffer lets the recomputation of interval j - 1
+        // overlap the adjoint sweep of interval j; without the memory for it
+        // the intervals run one after the other on one buffer.
+        bool overlap = n_ckpt > 1;
+        if (overlap && adj->seg2.count != seg_values) {
+            try {
+                adj->seg2.allocate(seg_values);
+            } catch (const Error&) {
+                cudaGetLastError();
+                overlap = false;
+            }
+        }
+        if (!adj->rstream) {
+            check_cuda(cudaStreamCreateWithFlags(&adj->rstream, cudaStreamNonBlocking), "cudaStreamCreate");
+            check_cuda(cudaStreamCreateWithFlags(&adj->astream, cudaStreamNonBlocking), "cudaStreamCreate");
+            for (auto* e : {&adj->evr[0], &adj->evr[1], &adj->eva[0], &adj->eva[1], &adj->evs})
+                check_cuda(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        cudaStream_t r = overlap ? adj->rstream : s;
+        cudaStream_t as = overlap ? adj->astream : s;
+        // the last interval's buffer is seg (where the forward kept it)
+        const int last_buf = static_cast<int>((n_ckpt - 1) % 2);
+        double* buf[2];
+        buf[last_buf] = adj->seg.ptr;
+        buf[1 - last_buf] = overlap ? adj->seg2.ptr : adj->seg.ptr;
+        const bool kept = adj->last_kept;
+        adj->last_kept = false;  // this backward overwrites seg and q
         check_cuda(cudaMemsetAsync(adj->lq.ptr, 0, state * sizeof(double), s), "memset");
         check_cuda(cudaMemsetAsync(adj->lk.ptr, 0, state * sizeof(double), s), "memset");
         check_cuda(cudaMemsetAsync(adj->acc.ptr, 0, adj->acc.count * sizeof(double), s), "memset");
@@ -434,45 +495,78 @@ ndg_status ndg_adjoint_backward(ndg_adjoint* adj, double* grad_p0, double* grad_
         int64_t launches = 0;
         int ain = 0;
         check_cuda(cudaEventRecord(adj->ev[0], s), "event");
+        if (kept) check_cuda(cudaMemcpyAsync(adj->qfinal.ptr, adj->q.ptr, state * sizeof(double), cudaMemcpyDeviceToDevice, s), "final state");
+        if (overlap) {
+            check_cuda(cudaEventRecord(adj->evs, s), "event");
+            check_cuda(cudaStreamWaitEvent(r, adj->evs, 0), "stream wait");
+            check_cuda(cudaStreamWaitEvent(as, adj->evs, 0), "stream wait");
+        }
+        // Recomputes interval j from its checkpoint, keeping every stage
+        // input, into buf[j % 2] (on stream r).
+        auto recompute = [&](int64_t j) {
+            const int64_t first = j * I + 1, last = std::min((j + 1) * I, n);
+            check_cuda(cudaMemcpyAsync(adj->q.ptr, adj->ckpt.ptr + static_cast<size_t>(j) * state, state * sizeof(double), cudaMemcpyDeviceToDevice, r),
+                       "checkpoint restore");
+            launch_traces_of_q(adj, 0, r);
+            ++launches;
+            run_forward(adj, 0, first, last, buf[j % 2], false, 0, launches, r);
+            if (j == n_ckpt - 1)
+                check_cuda(cudaMemcpyAsync(adj->qfinal.ptr, adj->q.ptr, state * sizeof(double), cudaMemcpyDeviceToDevice, r), "final state");
+            if (overlap) check_cuda(cudaEventRecord(adj->evr[j % 2], r), "event");
+        };
+        if (kept) {
+            if (overlap) check_cuda(cudaEventRecord(adj->evr[(n_ckpt - 1) % 2], s), "event");
+        } else {
+            recompute(n_ckpt - 1);
+        }
         for (int64_t j = n_ckpt - 1; j >= 0; --j) {
             const int64_t first = j * I + 1, last = std::min((j + 1) * I, n);
-            // Recompute the interval from its checkpoint, keeping every
-            // stage input.
-            check_cuda(cudaMemcpyAsync(adj->q.ptr, adj->ckpt.ptr + static_cast<size_t>(j) * state, state * sizeof(double), cudaMemcpyDeviceToDevice, s),
-                       "checkpoint restore");
-            launch_traces_of_q(adj, 0);
-            ++launches;
-            run_forward(adj, 0, first, last, adj->seg.ptr, false, 0, launches);
+            if (overlap) {
+                if (j >= 1) {
+                    // interval j - 1 reuses the buffer of interval j + 1
+                    if (j + 1 <= n_ckpt - 1) check_cuda(cudaStreamWaitEvent(r, adj->eva[(j + 1) % 2], 0), "stream wait");
+                    recompute(j - 1);
+                }
+                check_cuda(cudaStreamWaitEvent(as, adj->evr[j % 2], 0), "stream wait");
+            } else if (j < n_ckpt - 1) {
+                recompute(j);
+            }
             if (j == n_ckpt - 1) {
                 // The misfit's derivative at the final state, and the first
                 // adjoint far traces.
                 dev::AdjointStageArgs a = adjoint_args(adj, ain);
-                a.qs = adj->q.ptr;
+                a.qs = adj->qfinal.ptr;
                 a.rk_a = 0.0;
                 a.gdt = 0.0;
                 a.gdt_next = kRkG[2] * adj->dt;
                 a.inject = R > 0;
                 a.target = adj->targets.ptr + n * R;
                 a.wdt = adj->dt;
-                check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, s), "adjoint stage launch");
+                check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, as), "adjoint stage launch");
                 ++launches;
                 ain = 1 - ain;
             }
             for (int64_t step = last; step >= first; --step) {
                 for (int m = 2; m >= 0; --m) {
                     dev::AdjointStageArgs a = adjoint_args(adj, ain);
-                    a.qs = adj->seg.ptr + (static_cast<size_t>(step - first) * 3 + static_cast<size_t>(m)) * state;
+                    a.qs = buf[j % 2] + (static_cast<size_t>(step - first) * 3 + static_cast<size_t>(m)) * state;
                     a.rk_a = kRkA[m];
                     a.gdt = kRkG[m] * adj->dt;
                     a.gdt_next = kRkG[m > 0 ? m - 1 : 2] * adj->dt;
                     a.inject = (m == 0 && step - 1 >= 1 && R > 0) ? 1 : 0;
                     a.target = adj->targets.ptr + (step - 1) * R;
                     a.wdt = adj->dt;
-                    check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, s), "adjoint stage launch");
+                    check_cuda(dev::launch_adjoint_stage(adj->N, adj->fp32, a, as), "adjoint stage launch");
                     ++launches;
                     ain = 1 - ain;
                 }
             }
+            if (overlap) check_cuda(cudaEventRecord(adj->eva[j % 2], as), "event");
+        }
+        if (overlap) {
+            // the adjoint stream's last event covers the recomputations it waited for
+            check_cuda(cudaEventRecord(adj->evs, as), "event");
+            check_cuda(cudaStreamWaitEvent(s, adj->evs, 0), "stream wait");
         }
         check_cuda(dev::launch_speed_gradient(adj->acc.ptr, reinterpret_cast<const int2*>(c->link.ptr), adj->K, adj->grad.ptr, s), "gradient kernel");
         ++launches;

@@ -462,7 +462,7 @@ struct AdjTile {
     static constexpr int by_smem = (60 * 1024 - fixed_bytes) / per_element_bytes;
     static constexpr int by_threads = 256 / (3 * n);
     static constexpr int raw = by_smem < by_threads ? by_smem : by_threads;
-    static constexpr int EPB = raw >= 2 ? (raw & ~1) : 2;
+    static constexpr int EPB = raw >= 4 ? 4 : (raw >= 2 ? (raw & ~1) : 2);
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
     static constexpr int kWarps = kThreads / 32;
     static constexpr int kBlockIters = (3 * EPB + kWarps - 1) / kWarps;
