@@ -511,7 +511,11 @@ def run_ours(args) -> None:
     mesh.initial_conditions()
     dof = ndg.dof_count(mesh)
     assert dof == dof_count()
-    tile, _ = mesh.autotune(20)  # fields are restored by the tuner
+    if args.tile is None:
+        tile, _ = mesh.autotune(20)  # fields are restored by the tuner
+    else:
+        tile = args.tile  # fixed by hand (profiler runs, where the tuner's timings are distorted)
+        mesh.set_tile(tile)
 
     ndg.Solver2D_t.run(mesh, args.warmup)
     torch.cuda.synchronize()
@@ -637,7 +641,8 @@ def run_ours(args) -> None:
                         "host_wall_s": wall},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "traffic": traffic, "kernel": f"stage_kernel<{ORDER}, false, {tile}>", "kernel_ms": stage_ms,
-                             "tile_elements_per_cta": tile or mesh.tile_candidates()[1], "tile_source": "autotuner",
+                             "tile_elements_per_cta": tile or mesh.tile_candidates()[1],
+                             "tile_source": "autotuner" if args.tile is None else "--tile",
                              "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof, "peak_source": peak_kind},
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "fp32": fp32,
@@ -665,6 +670,8 @@ def main() -> None:
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances leg (profiling runs)")
     ap.add_argument("--no-hp", action="store_true", help="skip the hp-adaptive leg (profiling runs)")
+    ap.add_argument("--tile", type=int, default=None,
+                    help="elements per CTA of the main leg's stage kernel instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
