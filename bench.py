@@ -201,6 +201,35 @@ def _available_memory_kb() -> float | None:
     return None
 
 
+def config1_leg(local: int, stream) -> dict:
+    """The reference's own CPU-runnable case (16 x 16 periodic, N = 4, 200 RK3
+    steps of the plane wave): the L2 error against the analytic solution of
+    the reference's CPU path (its restatement in the oracle, bit-identical to
+    it) and of the device path in every form, from the same initial fields."""
+    import numpy as np
+
+    import ndg_cuda_b200 as ndg
+    from ndg_cuda_b200 import meshgen
+    from oracle.pyoracle import OracleSolver
+    zone = meshgen.uniform_zone(16, x_periodic=True, y_periodic=True)
+    o = OracleSolver(zone, 4, cfl=CFL)
+    o.initial_conditions()
+    ic = {f: o.field(f) for f in ("p", "u", "v")}
+    t_ref = o.run(200)
+    out = {"workload": "dg_wave_rk3_periodic_16x16_N4_plane_wave_200_steps", "time": t_ref,
+           "l2_vs_analytic": {"reference_cpu": dict(zip("puv", map(float, o.l2_error(t_ref))))}, "rel_l2_vs_reference": {}}
+    for name, prec in (("fp64_strict", ndg.FP64_STRICT), ("fp64", ndg.FP64), ("fp32", ndg.FP32)):
+        m = ndg.Mesh2D_t(zone, 4, cfl=CFL, device=local, stream=stream.cuda_stream, precision=prec)
+        for f in ("p", "u", "v"):
+            m.set_field(f, ic[f])
+        t = ndg.Solver2D_t.run(m, 200)
+        out["l2_vs_analytic"][name] = dict(zip("puv", map(float, m.l2_error(t))))
+        out["rel_l2_vs_reference"][name] = {f: float(np.linalg.norm(m.get_field(f) - o.field(f)) / np.linalg.norm(o.field(f)))
+                                            for f in ("p", "u", "v")}
+        m.close()
+    return out
+
+
 def run_reference_arm(args) -> None:
     """The reference's CPU path on all the host cores it can use: its stepping
     is single-threaded and its MPI domain decomposition is not built here, so
@@ -597,8 +626,10 @@ def run_ours(args) -> None:
         stage32_ms = m32.time_stage(1, 30)
         m32.initial_conditions()
         mesh.initial_conditions()
-        ndg.Solver2D_t.run(m32, CONFIG_STEPS)
-        ndg.Solver2D_t.run(mesh, CONFIG_STEPS)
+        t32 = ndg.Solver2D_t.run(m32, CONFIG_STEPS)
+        t64 = ndg.Solver2D_t.run(mesh, CONFIG_STEPS)
+        l2_analytic = {"time": t64, "fp64": dict(zip("puv", map(float, mesh.l2_error(t64)))),
+                       "fp32": dict(zip("puv", map(float, m32.l2_error(t32))))}
         err = {}
         for f in ("p", "u", "v"):
             a64, a32 = mesh.get_field(f), m32.get_field(f)
@@ -607,6 +638,7 @@ def run_ours(args) -> None:
                 "ms_per_step": float(f_ms.item()) / args.steps, "kernel": f"stage_kernel_f32<{ORDER}>", "kernel_ms": stage32_ms,
                 "roofline_frac": BYTES_PER_DOF_STAGE * dof / (stage32_ms / 1e3) / 1e9 / peak,
                 "rel_l2_vs_fp64": err, "steps_compared": CONFIG_STEPS, "tile_elements_per_cta": tile32 or m32.tile_candidates()[1],
+                "l2_vs_analytic": l2_analytic,
                 "wall_time_per_unit_time_s": float(f_ms.item()) / args.steps / 1e3 / dt_step,
                 "arithmetic": "traces, fluxes, metrics and volume term in FP32; q, k and the RK update in FP64"}
         m32.close()
@@ -614,6 +646,8 @@ def run_ours(args) -> None:
     hp = None
     if not args.no_hp and world == 1:
         hp = hp_leg(local, stream)
+
+    config1 = config1_leg(local, stream) if not args.no_fp32 and world == 1 else None
 
     batched = None
     if not args.no_batched:
@@ -646,6 +680,7 @@ def run_ours(args) -> None:
                              "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof, "peak_source": peak_kind},
                 "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "fp32": fp32,
+                "config1_analytic": config1,
                 "hp_adaptive": hp,
                 "batched": batched,
                 "adjoint": adjoint,

@@ -294,6 +294,14 @@ typedef struct ndg_solution_output {
 } ndg_solution_output;
 ndg_status ndg_get_solution(ndg_ctx* ctx, int32_t instance, double time, const ndg_solution_output* out);
 
+/* L2 error of one instance against the reference plane wave g(x, time)
+ * (include/functions/analytical_solution.tpp:4-10), per field:
+ * l2[f] = sqrt(sum_e sum_ij w_i w_j J_ij (q_ij - g_ij)^2), w the Gauss
+ * weights and J the Jacobian of the element map (Element2D_t.cpp:743-777).
+ * The reference writes only the pointwise |g - q| (get_complete_solution);
+ * this is the norm of it over the domain, the same formula as the oracle's. */
+ndg_status ndg_l2_error(ndg_ctx* ctx, int32_t instance, double time, double* l2);
+
 /* Output files in the role of DataWriter_t (src/helpers/DataWriter_t.cpp,
  * include/helpers/DataWriter_t.h; VTK is not needed): per output time a
  * parallel unstructured grid <stem>_t<time, 9 decimals, '.' -> '_'>s<ext>

@@ -114,6 +114,7 @@ def lib() -> C.CDLL:
         "ndg_writer_write_arrays": ([vp, dbl, i64, i64, C.POINTER(_OutputArrays)], C.c_int),
         "ndg_writer_write": ([vp, vp, i32, dbl, i32], C.c_int),
         "ndg_pre_condition": ([vp, i64, i64, i32, C.POINTER(i64)], C.c_int),
+        "ndg_l2_error": ([vp, i32, dbl, vp], C.c_int),
         "ndg_adapt_flags": ([vp, vp, vp], C.c_int),
         "ndg_delta_t_from_device": ([vp, vp, i64, dbl, vp, C.POINTER(dbl)], C.c_int),
         "ndg_autotune": ([vp, i32, C.POINTER(i32), C.POINTER(dbl)], C.c_int),
@@ -431,6 +432,13 @@ class Mesh2D_t:
 
     def get_complete_solution(self, time: float, instance: int = 0) -> dict:
         return self.get_solution(time, complete=True, instance=instance)
+
+    def l2_error(self, time: float, instance: int = 0) -> np.ndarray:
+        """L2 error of p, u, v against the reference plane wave at `time`
+        (ndg_l2_error): sqrt(sum w_i w_j J (q - g)^2) per field."""
+        out = np.zeros(3)
+        _check(lib().ndg_l2_error(self._ctx.h, instance, float(time), _ptr(out)))
+        return out
 
     # Mesh2D_t::write_data / write_complete_data (src/meshes/Mesh2D_t.cpp:1601-1642)
     def write_data(self, time: float, data_writer: "DataWriter_t", instance: int = 0) -> None:

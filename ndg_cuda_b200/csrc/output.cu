@@ -20,6 +20,9 @@
 // node-wise |g - q| (evaluated once per node rather than once per output
 // point; the values are the same) are staged in shared memory, then the
 // block's threads take the output points.
+//
+// Also here: the L2 error against the plane wave (l2_error_kernel), per
+// element in a fixed reduction order; the host adds the elements in order.
 #include "output.cuh"
 #include "stage_common.cuh"
 
@@ -110,7 +113,60 @@ __global__ void __launch_bounds__(128) output_kernel(OutputArgs a) {
     }
 }
 
+// Per element: sum over nodes of w_i w_j J_ij (q - g)^2 for p, u, v, with
+// J = x_xi y_eta - x_eta y_xi of the bilinear map in the reference's
+// expression (Element2D_t.cpp:743-777) and g the reference plane wave.
+__global__ void __launch_bounds__(128) l2_error_kernel(L2Args a) {
+    __shared__ double red[3][128];
+    for (int64_t e = blockIdx.x; e < a.K; e += gridDim.x) {
+        const int N = a.N[e], n = N + 1, NN = n * n;
+        const double* c = a.corners + 8 * e;
+        const double* xn = a.nodes + a.vec_off[N];
+        const double* w = a.weights + a.vec_off[N];
+        const int64_t o2 = a.off2[e];
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int t = threadIdx.x; t < NN; t += blockDim.x) {
+            const int i = t / n, j = t - i * n;
+            const double xi = xn[i], eta = xn[j];
+            const double m00 = metric<true>(eta, __dsub_rn(c[2], c[0]), __dsub_rn(c[4], c[6]));
+            const double m01 = metric<true>(xi, __dsub_rn(c[6], c[0]), __dsub_rn(c[4], c[2]));
+            const double m10 = metric<true>(eta, __dsub_rn(c[3], c[1]), __dsub_rn(c[5], c[7]));
+            const double m11 = metric<true>(xi, __dsub_rn(c[7], c[1]), __dsub_rn(c[5], c[3]));
+            const double J = __dsub_rn(__dmul_rn(m00, m11), __dmul_rn(m01, m10));
+            double gx, gy, g[3];
+            quad_map(c, xi, eta, gx, gy);
+            plane_wave(gx, gy, a.time, g[0], g[1], g[2]);
+            const double ww = __dmul_rn(__dmul_rn(w[i], w[j]), J);
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                const double d = __dsub_rn(a.q[f * a.block + o2 + t], g[f]);
+                s[f] = fma(ww * d, d, s[f]);
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) red[f][threadIdx.x] = s[f];
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h)
+#pragma unroll
+                for (int f = 0; f < 3; ++f) red[f][threadIdx.x] += red[f][threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int f = 0; f < 3; ++f) a.partial[3 * e + f] = red[f][0];
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_l2_error(const L2Args& a, cudaStream_t stream) {
+    if (a.K == 0) return cudaSuccess;
+    const int blocks = static_cast<int>(a.K < 148 * 16 ? a.K : 148 * 16);
+    l2_error_kernel<<<blocks, 128, 0, stream>>>(a);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_output(const OutputArgs& a, int max_N, cudaStream_t stream) {
     if (a.K == 0) return cudaSuccess;

@@ -30,5 +30,23 @@ struct OutputArgs {
 
 cudaError_t launch_output(const OutputArgs& a, int max_N, cudaStream_t stream);
 
+// L2 error against the reference plane wave at `time`: per domain element
+// and field, sum_ij w_i w_j J_ij (q_ij - g_ij)^2 into partial[3 e + f].
+struct L2Args {
+    const double* q;          // field blocks of p, u, v of one instance
+    int64_t block;
+    const int32_t* N;
+    const int64_t* off2;
+    const double* corners;    // [K][8]
+    const double* nodes;      // Gauss nodes, order by order
+    const double* weights;    // Gauss weights, order by order
+    const int64_t* vec_off;   // [N_max + 1] first node of order N in nodes / weights
+    int64_t K;
+    double time;
+    double* partial;          // [K][3]
+};
+
+cudaError_t launch_l2_error(const L2Args& a, cudaStream_t stream);
+
 }  // namespace dev
 }  // namespace ndg

@@ -1,15 +1,45 @@
-// C ABI of the output interpolation (ndg_get_solution): gathers the per
-// element orders, value offsets and corners and the order's tables, runs
-// output_kernel (output.cu) on the context's stream and copies the requested
-// arrays to the caller.
+// C ABI of the output interpolation (ndg_get_solution) and of the L2 error
+// against the plane wave (ndg_l2_error): gathers the per element orders,
+// value offsets and corners and the orders' tables, runs the kernels of
+// output.cu on the context's stream and copies the results to the caller.
 #include "context.hpp"
 #include "output.cuh"
 
 #include <array>
+#include <cmath>
 #include <cstdint>
 #include <vector>
 
 using namespace ndg;
+
+namespace {
+
+// Per domain element: order, first value within a field block, corners
+// (x0, y0, ..., x3, y3). Returns the largest order.
+int gather_elements(const ndg_ctx* ctx, std::vector<int32_t>& N, std::vector<int64_t>& off2, std::vector<double>& corners) {
+    const Topology& t = ctx->topo;
+    const int64_t K = t.n_domain;
+    N.resize(static_cast<size_t>(K));
+    off2.resize(static_cast<size_t>(K));
+    corners.resize(static_cast<size_t>(8 * K));
+    int64_t o = 0;
+    int max_N = 0;
+    for (int64_t e = 0; e < K; ++e) {
+        const size_t se = static_cast<size_t>(e);
+        N[se] = t.elem_N[se];
+        off2[se] = o;
+        o += static_cast<int64_t>(N[se] + 1) * (N[se] + 1);
+        max_N = std::max(max_N, N[se]);
+        for (int v = 0; v < 4; ++v) {
+            const size_t node = static_cast<size_t>(t.elem_nodes[se][static_cast<size_t>(v)]);
+            corners[8 * se + 2 * static_cast<size_t>(v)] = t.node_x[node];
+            corners[8 * se + 2 * static_cast<size_t>(v) + 1] = t.node_y[node];
+        }
+    }
+    return max_N;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -30,25 +60,11 @@ ndg_status ndg_get_solution(ndg_ctx* ctx, int32_t instance, double time, const n
         }
         make_current(ctx);
 
-        const Topology& t = ctx->topo;
-        const int64_t K = t.n_domain;
-        std::vector<int32_t> N(static_cast<size_t>(K));
-        std::vector<int64_t> off2(static_cast<size_t>(K));
-        std::vector<double> corners(static_cast<size_t>(8 * K));
-        int64_t o = 0;
-        int max_N = 0;
-        for (int64_t e = 0; e < K; ++e) {
-            const size_t se = static_cast<size_t>(e);
-            N[se] = t.elem_N[se];
-            off2[se] = o;
-            o += static_cast<int64_t>(N[se] + 1) * (N[se] + 1);
-            max_N = std::max(max_N, N[se]);
-            for (int v = 0; v < 4; ++v) {
-                const size_t node = static_cast<size_t>(t.elem_nodes[se][static_cast<size_t>(v)]);
-                corners[8 * se + 2 * static_cast<size_t>(v)] = t.node_x[node];
-                corners[8 * se + 2 * static_cast<size_t>(v) + 1] = t.node_y[node];
-            }
-        }
+        const int64_t K = ctx->topo.n_domain;
+        std::vector<int32_t> N;
+        std::vector<int64_t> off2;
+        std::vector<double> corners;
+        const int max_N = gather_elements(ctx, N, off2, corners);
         if (max_N > ctx->tables.N_max) fail(NDG_ERR_INVALID_ARG, "element order above the tables' N_max");
         std::vector<double> interp, nodes;
         std::vector<int64_t> interp_off(static_cast<size_t>(max_N + 1)), nodes_off(static_cast<size_t>(max_N + 1));
@@ -107,6 +123,62 @@ ndg_status ndg_get_solution(ndg_ctx* ctx, int32_t instance, double time, const n
             if (host[i] && count)
                 check_cuda(cudaMemcpyAsync(host[i], d[i], count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "output download");
         check_cuda(cudaStreamSynchronize(ctx->stream), "output");
+    });
+}
+
+ndg_status ndg_l2_error(ndg_ctx* ctx, int32_t instance, double time, double* l2) {
+    return guarded([&] {
+        require_mesh(ctx);
+        require_device(ctx);
+        if (!l2) fail(NDG_ERR_INVALID_ARG, "l2 is NULL");
+        if (instance < 0 || instance >= ctx->n_instances) fail(NDG_ERR_INVALID_ARG, "instance out of range");
+        make_current(ctx);
+        const int64_t K = ctx->topo.n_domain;
+        std::vector<int32_t> N;
+        std::vector<int64_t> off2;
+        std::vector<double> corners;
+        const int max_N = gather_elements(ctx, N, off2, corners);
+        if (max_N > ctx->tables.N_max) fail(NDG_ERR_INVALID_ARG, "element order above the tables' N_max");
+        std::vector<double> nodes, weights;
+        std::vector<int64_t> vec_off(static_cast<size_t>(max_N + 1));
+        for (int n = 0; n <= max_N; ++n) {
+            vec_off[static_cast<size_t>(n)] = static_cast<int64_t>(nodes.size());
+            const auto& x = ctx->tables.get(NDG_TABLE_NODES, n);
+            const auto& w = ctx->tables.get(NDG_TABLE_WEIGHTS, n);
+            nodes.insert(nodes.end(), x.begin(), x.end());
+            weights.insert(weights.end(), w.begin(), w.end());
+        }
+        DeviceBuffer<int32_t> dN;
+        DeviceBuffer<int64_t> doff2, dvoff;
+        DeviceBuffer<double> dcorners, dnodes, dweights, dpartial;
+        dN.upload(N, ctx->stream);
+        doff2.upload(off2, ctx->stream);
+        dcorners.upload(corners, ctx->stream);
+        dnodes.upload(nodes, ctx->stream);
+        dweights.upload(weights, ctx->stream);
+        dvoff.upload(vec_off, ctx->stream);
+        dpartial.allocate(static_cast<size_t>(std::max<int64_t>(3 * K, 1)));
+        dev::L2Args a{};
+        a.q = ctx->q.ptr + instance * 3 * ctx->block;
+        a.block = ctx->block;
+        a.N = dN.ptr;
+        a.off2 = doff2.ptr;
+        a.corners = dcorners.ptr;
+        a.nodes = dnodes.ptr;
+        a.weights = dweights.ptr;
+        a.vec_off = dvoff.ptr;
+        a.K = K;
+        a.time = time;
+        a.partial = dpartial.ptr;
+        check_cuda(dev::launch_l2_error(a, ctx->stream), "l2 error kernel launch");
+        ++ctx->launches;
+        std::vector<double> partial(static_cast<size_t>(3 * K));
+        if (K) check_cuda(cudaMemcpyAsync(partial.data(), dpartial.ptr, partial.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "l2 download");
+        check_cuda(cudaStreamSynchronize(ctx->stream), "l2");
+        double sum[3] = {0.0, 0.0, 0.0};
+        for (int64_t e = 0; e < K; ++e)
+            for (int f = 0; f < 3; ++f) sum[f] += partial[static_cast<size_t>(3 * e + f)];
+        for (int f = 0; f < 3; ++f) l2[f] = std::sqrt(sum[f]);
     });
 }
 

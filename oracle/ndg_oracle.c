@@ -1687,3 +1687,36 @@ int ndgo_complete_solution(const ndgo_ctx* c, int64_t n_interp, double time, dou
     tables_free(&T);
     return 0;
 }
+
+/* The L2 error against the reference plane wave g(x, time) per field:
+ * sqrt(sum_e sum_ij w_i w_j J_ij (q_ij - g_ij)^2), with the weights of the
+ * element's order and J as compute_geometry forms it (Element2D_t.cpp:743-777);
+ * elements, then nodes, in order. */
+void ndgo_l2_error(const ndgo_ctx* c, double time, double* out) {
+    double s[3] = {0, 0, 0};
+    const double* q[3] = {c->p, c->u, c->v};
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        const int N = c->eN[e], n = N + 1;
+        const double* xn = c->T.t[T_NODES][N];
+        const double* w = c->T.t[T_WEIGHTS][N];
+        double px[4], py[4];
+        for (int k = 0; k < 4; ++k) {
+            px[k] = c->nx[c->enodes[4 * e + k]];
+            py[k] = c->ny[c->enodes[4 * e + k]];
+        }
+        for (int i = 0; i < n; ++i) {
+            for (int j = 0; j < n; ++j) {
+                const int64_t k = c->off2[e] + i * n + j;
+                double gx, gy, g[3];
+                quad_map(xn[i], xn[j], px, py, &gx, &gy);
+                analytic_g(gx, gy, time, &g[0], &g[1], &g[2]);
+                const double ww = w[i] * w[j] * c->jac[k];
+                for (int f = 0; f < 3; ++f) {
+                    const double d = q[f][k] - g[f];
+                    s[f] += ww * d * d;
+                }
+            }
+        }
+    }
+    for (int f = 0; f < 3; ++f) out[f] = sqrt(s[f]);
+}

@@ -61,6 +61,8 @@ void ndgo_get_error(const ndgo_ctx* ctx, double* p_error, double* p_sigma, int* 
 /* Mesh2D_t::get_complete_solution: out[11] = x, y, p, u, v, dp/dt, du/dt,
  * dv/dt, p/u/v analytic error on n_interp^2 points per element. */
 int ndgo_complete_solution(const ndgo_ctx* ctx, int64_t n_interp, double time, double** out);
+/* L2 error against the plane wave at `time`: out[3] for p, u, v. */
+void ndgo_l2_error(const ndgo_ctx* ctx, double time, double* out);
 
 /* Variable-speed operator (a wave speed per domain element: fluxes
  * c_e (u, p, 0), c_e (v, 0, p) and the upwind face flux times the mean of

@@ -118,6 +118,7 @@ def _load_oracle():
         lib.ndgo_adjoint_solve.restype = C.c_double
         lib.ndgo_complete_solution.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]
         lib.ndgo_complete_solution.restype = C.c_int
+        lib.ndgo_l2_error.argtypes = [C.c_void_p, C.c_double, _dp]
         _orc = lib
     return _orc
 
@@ -396,6 +397,12 @@ class OracleSolver(_Base):
 
     def estimate_error(self):
         self.lib.ndgo_estimate_error(self.ctx, *self.tolerance)
+
+    def l2_error(self, time: float) -> np.ndarray:
+        """L2 error of p, u, v against the plane wave at `time`."""
+        out = np.zeros(3)
+        self.lib.ndgo_l2_error(self.ctx, time, out)
+        return out
 
     def complete_solution(self, n_interp: int, time: float) -> dict:
         """Restatement of Mesh2D_t::get_complete_solution on n_interp^2 points per element."""
