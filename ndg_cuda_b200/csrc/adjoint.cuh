@@ -55,7 +55,6 @@ struct SpeedStageArgs {
     const double2* normal;
     const double* gscale;
     const double* c;
-    unsigned* error;
     double rk_a, gdt;
     int first;
     int64_t n_elements, field_stride;
@@ -84,7 +83,6 @@ struct AdjointStageArgs {
     const double* gscale;
     const double* c;
     const double* target;  // [n receivers], when inject
-    unsigned* error;
     double rk_a, gdt, gdt_next, wdt;
     int inject;
     int64_t n_elements, field_stride;

@@ -2,7 +2,8 @@
 //
 // speed_stage_kernel  one low-storage RK3 stage of L(c) (the operator of
 //                     adjoint.cuh), fused like the uniform-order stage kernel:
-//                     bulk copy of the q tile, own traces, upwind flux with
+//                     cp.async copy of the q tile into a padded shared
+//                     layout free of bank conflicts, own traces, upwind flux with
 //                     the face speed, volume term times c_e, RK update,
 //                     traces of the new q; optionally it keeps the stage
 //                     input (for the adjoint's c-gradient) and samples the
@@ -29,8 +30,8 @@
 // Both kernels are templates over R, the type of the operator's arithmetic:
 // double (the FP64 form, FMA contraction) or float (the FP32 form: traces,
 // fluxes, metrics, contractions and their transposes in FP32, traces stored
-// in FP32). The bulk-copied states, the RK updates, the misfit and the
-// gradient accumulators are FP64 in both.
+// in FP32). The states copied into shared memory, the RK updates, the
+// misfit and the gradient accumulators are FP64 in both.
 #include "adjoint.cuh"
 #include "stage_common.cuh"
 #include "stage_kernels.cuh"

@@ -307,8 +307,6 @@ struct Tile {
     static constexpr int EPB = E > 0 ? E : (N <= 10 ? 4 : 2);
     static_assert(EPB == 2 || EPB == 4 || EPB == 8 || EPB == 16, "tiles hold 2, 4, 8 or 16 elements (whole lines per wavefront group)");
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
-    // Node-wise work per thread in an RK phase over the whole tile: ceil(3 EPB NN / threads).
-    static constexpr int kNodeIters = (3 * EPB * NN + kThreads - 1) / kThreads;
     // Node-wise phases of the stage kernels (tile copy, RK update): warp w
     // takes the (field, element) blocks w, w + kWarps, ... and its lanes the
     // nodes of a block, so no per-node division is needed.

@@ -330,7 +330,6 @@ struct TileF {
     static constexpr int NN = n * n;
     static constexpr int EPB = Tile<N, E>::EPB;
     static constexpr int kThreads = Tile<N, E>::kThreads;
-    static constexpr int kNodeIters = Tile<N, E>::kNodeIters;
     // bank-conflict-free strides of the FP32 arrays (32 four-byte values per wavefront)
     static constexpr bank::Strides L = bank::search(N, EPB, 32);
     static constexpr int P = L.P, ES = L.ES, QS = L.QS, SE = L.SE, FS = L.FS;
