@@ -244,6 +244,39 @@ GeneralPlan build_general_plan(const Topology& t) {
             p.fm_off[static_cast<size_t>(2 * f + side)] = p.fm_total;
             p.fm_total += nf;
         }
+
+    // Slots and side modes in group-list order, so that the sides of one
+    // tile of a group own one contiguous slot range.
+    p.pslot_start.assign(static_cast<size_t>(4 * K + 1), 0);
+    p.pside_mode.assign(static_cast<size_t>(4 * K), 0);
+    int64_t pos = 0, slot = 0;
+    for (const auto& grp : p.groups)
+        for (int64_t e : grp.second) {
+            const int Ne = t.elem_N[static_cast<size_t>(e)];
+            for (int s = 0; s < 4; ++s) {
+                const size_t ps = static_cast<size_t>(4 * pos + s);
+                p.pslot_start[ps] = slot;
+                const int64_t q0 = p.sface_start[static_cast<size_t>(4 * e + s)], q1 = p.sface_start[static_cast<size_t>(4 * e + s + 1)];
+                for (int64_t q = q0; q < q1; ++q) {
+                    const int64_t f = p.sface[static_cast<size_t>(q)];
+                    for (int j = 0; j <= t.face_N[static_cast<size_t>(f)]; ++j) {
+                        p.slot_desc.push_back(32 * f + j);
+                        p.slot_normal.push_back(t.face_normal[static_cast<size_t>(f)][0]);
+                        p.slot_normal.push_back(t.face_normal[static_cast<size_t>(f)][1]);
+                        ++slot;
+                    }
+                }
+                if (q1 == q0) continue;
+                const int64_t f0 = p.sface[static_cast<size_t>(q0)];
+                const auto& fn = t.face_nodes[static_cast<size_t>(f0)];
+                const int64_t en0 = p.enodes[static_cast<size_t>(4 * e + s)], en1 = p.enodes[static_cast<size_t>(4 * e + ((s + 1) & 3))];
+                const bool one = q1 - q0 == 1 && t.face_N[static_cast<size_t>(f0)] == Ne;
+                p.pside_mode[ps] = one && fn[0] == en0 && fn[1] == en1 ? 1 : one && fn[1] == en0 && fn[0] == en1 ? 2 : 3;
+            }
+            ++pos;
+        }
+    p.pslot_start[static_cast<size_t>(4 * K)] = slot;
+    p.n_slots = slot;
     return p;
 }
 

@@ -391,6 +391,11 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_fw.allocate(static_cast<size_t>(std::max<int64_t>(g.fw_total, 1)));
         c->g_smatch.allocate(static_cast<size_t>(std::max<int64_t>(g.sm_total, 1)));
         c->g_fmatch.allocate(static_cast<size_t>(std::max<int64_t>(g.fm_total, 1)));
+        c->g_pslot_start.upload(g.pslot_start, c->stream);
+        c->g_slot_desc.upload(g.slot_desc, c->stream);
+        c->g_slot_normal.upload(g.slot_normal, c->stream);
+        c->g_pside_mode.upload(g.pside_mode, c->stream);
+        c->g_slot_src.allocate(static_cast<size_t>(std::max<int64_t>(2 * g.n_slots, 1)));
         std::vector<int64_t> ids;
         for (const auto& grp : g.groups) ids.insert(ids.end(), grp.second.begin(), grp.second.end());
         c->g_ids.upload(ids, c->stream);
@@ -401,6 +406,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
             og.N = grp.first;
             og.count = static_cast<int64_t>(grp.second.size());
             og.ids = c->g_ids.ptr + at;
+            og.first = at;
             at += og.count;
             c->groups.push_back(og);
             check_cuda(dev::prepare_general_kernels(og.N, g.side_slots), "kernel attributes");
@@ -453,8 +459,15 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.smatch = c->g_smatch.ptr;
         M.fw = c->g_fw.ptr;
         M.fmatch = c->g_fmatch.ptr;
-        check_cuda(dev::launch_general_weights(M, c->g_sw.ptr, c->g_smatch.ptr, c->g_fw.ptr, c->g_fmatch.ptr, c->stream), "mortar weights");
-        c->launches += 2;
+        M.n_slots = g.n_slots;
+        M.pslot_start = c->g_pslot_start.ptr;
+        M.slot_desc = c->g_slot_desc.ptr;
+        M.slot_normal = c->g_slot_normal.ptr;
+        M.slot_src = c->g_slot_src.ptr;
+        M.pside_mode = c->g_pside_mode.ptr;
+        check_cuda(dev::launch_general_weights(M, c->g_sw.ptr, c->g_smatch.ptr, c->g_fw.ptr, c->g_fmatch.ptr, c->g_slot_src.ptr, c->stream),
+                   "mortar weights");
+        c->launches += 3;
         // The uniform-path corners also serve the initial condition of a
         // general mesh.
         c->corners.upload(g.corners, c->stream);

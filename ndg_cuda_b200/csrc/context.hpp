@@ -104,6 +104,9 @@ struct ndg_ctx {
     ndg::DeviceBuffer<int32_t> g_fsN;                                            // face-side element orders
     ndg::DeviceBuffer<double> g_sw, g_fw;                              // mortar weights
     ndg::DeviceBuffer<int32_t> g_smatch, g_fmatch;                     // mortar node matches
+    ndg::DeviceBuffer<int64_t> g_pslot_start, g_slot_desc, g_slot_src;  // face-node slots of the sides, list order
+    ndg::DeviceBuffer<double> g_slot_normal;
+    ndg::DeviceBuffer<int32_t> g_pside_mode;
     std::vector<ndg::dev::OrderGroup> groups;
     ndg::dev::GeneralMesh gmesh;
 

@@ -322,9 +322,33 @@ __global__ void __launch_bounds__(128) face_weights_kernel(GeneralMesh M, double
     }
 }
 
+// Trace value each face-node slot reads on each face side, as face_value
+// picks it: the element side's node (side 0) or its mirror (side 1) where the
+// face side is conforming, the matched node where the face node coincides
+// with an element node, -1 where face_value interpolates.
+__global__ void __launch_bounds__(128) slot_sources_kernel(GeneralMesh M, int64_t* __restrict__ src) {
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < 2 * M.n_slots;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t slot = idx / 2;
+        const int side = static_cast<int>(idx - 2 * slot);
+        const int64_t d = M.slot_desc[slot];
+        const int64_t f = d / 32;
+        const int j = static_cast<int>(d - 32 * f);
+        const int64_t b = M.fbase[2 * f + side];
+        int64_t v;
+        if (M.fw_off[2 * f + side] < 0) {
+            v = b + (side == 0 ? j : M.fN[f] - j);
+        } else {
+            const int match = M.fmatch[M.fm_off[2 * f + side] + j];
+            v = match >= 0 ? b + match : -1;
+        }
+        src[idx] = v;
+    }
+}
+
 }  // namespace
 
-cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, cudaStream_t stream) {
+cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, int64_t* slot_src, cudaStream_t stream) {
     if (m.n_domain > 0) {
         const int blocks = static_cast<int>(std::min<int64_t>((4 * m.n_domain + 127) / 128, 148 * 8));
         side_weights_kernel<<<blocks, 128, 0, stream>>>(m, sw, smatch);
@@ -332,6 +356,10 @@ cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch
     if (m.n_faces > 0) {
         const int blocks = static_cast<int>(std::min<int64_t>((2 * m.n_faces + 127) / 128, 148 * 8));
         face_weights_kernel<<<blocks, 128, 0, stream>>>(m, fw, fmatch);
+    }
+    if (m.n_slots > 0) {
+        const int blocks = static_cast<int>(std::min<int64_t>((2 * m.n_slots + 127) / 128, 148 * 8));
+        slot_sources_kernel<<<blocks, 128, 0, stream>>>(m, slot_src);
     }
     return cudaGetLastError();
 }
@@ -384,41 +412,49 @@ __device__ __forceinline__ void face_value(const GeneralMesh& M, const R* __rest
     v[2] = div<S>(vn, den);
 }
 
-// Tile of the fused stage: FP64 arrays (the q tile, element numbers and
-// offsets, slot prefix sums) then arrays of the arithmetic type R.
+// Tile of the fused stage: FP64 arrays (the q and k tiles, element numbers
+// and offsets, the sides' slot ranges and flux modes) then arrays of the
+// arithmetic type R. About 128 threads per CTA: the stage's time on a small
+// order group is one CTA's dependent chain, so tiles are kept short.
 template <int N, typename R>
 struct FusedTile {
     static constexpr int n = N + 1;
     static constexpr int NN = n * n;
-    static constexpr int raw = 256 / (3 * n);
+    static constexpr int raw = 128 / (3 * n);
     static constexpr int EPB = raw >= 1 ? raw : 1;
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
+    static constexpr int kVals = 3 * EPB * NN;     // values of a [3][EPB][NN] field tile
+    static_assert(4 * EPB < kThreads, "one thread per tile side and one more");
     // doubles
     static constexpr int kQ = 0;                   // [3][EPB][NN] q, then the new q
-    static constexpr int kOff = kQ + 3 * EPB * NN; // [EPB] element number, [EPB] field offset, [EPB] trace offset (int64)
-    static constexpr int kSp = kOff + 3 * EPB;     // [4 EPB + 1] prefix sums of the sides' slot counts (ints)
-    static constexpr int kDoubles = kSp + 2 * EPB + 1;
+    static constexpr int kK = kQ + kVals;          // [3][EPB][NN] k of the stage's input
+    static constexpr int kOff = kK + kVals;        // [EPB] element number, [EPB] field offset, [EPB] trace offset,
+                                                   // [4 EPB + 1] first slot of each side, then the end (int64)
+    static constexpr int kMode = kOff + 7 * EPB + 1;  // [4 EPB] side flux modes (ints)
+    static constexpr int kDoubles = kMode + 2 * EPB;
     // R values past the doubles
-    static constexpr int kG = 0;                   // [3][EPB][NN] G
-    static constexpr int kF = kG + 3 * EPB * NN;   // [3][EPB][4][n] element side fluxes
+    static constexpr int kF = 0;                   // [3][EPB][4][n] element side fluxes
     static constexpr int kJ = kF + 3 * EPB * 4 * n;  // [EPB][NN] J (1/J in the default mode)
     static constexpr int kS = kJ + EPB * NN;       // [EPB][4] edge metric per side
     static constexpr bool kCopy = sizeof(R) != sizeof(double);  // the FP32 form keeps an FP32 copy of the q tile
     static constexpr int kQr = kS + EPB * 4;       // [3][EPB][NN] q in R (FP32 form only)
-    static constexpr int kFF = kQr + (kCopy ? 3 * EPB * NN : 0);  // [3][EPB][4][slots] face fluxes at the side's face nodes
+    static constexpr int kG = kQr + (kCopy ? kVals : 0);  // [3][EPB][NN] G
+    static constexpr int kFF = kG + kVals;         // [3][EPB][4][slots] face fluxes at the sides' face nodes
     static constexpr size_t bytes(int slots) { return sizeof(double) * kDoubles + sizeof(R) * (kFF + 3 * EPB * 4 * slots); }
 };
 
 template <int N, bool S, typename R>
-__global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kernel(GeneralStage a, const int64_t* __restrict__ ids, int64_t count) {
+__global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kernel(GeneralStage a, OrderGroup grp) {
     using T = FusedTile<N, R>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     extern __shared__ __align__(128) double smem[];
     double* qs = smem + T::kQ;
+    double* ks = smem + T::kK;
     int64_t* eid = reinterpret_cast<int64_t*>(smem + T::kOff);  // element numbers of the tile
     int64_t* eo2 = eid + EPB;                                    // their first value in a field block
     int64_t* eo1 = eo2 + EPB;                                    // their first side-trace value
-    int* sps = reinterpret_cast<int*>(smem + T::kSp);
+    int64_t* sst = eo1 + EPB;                                    // first slot of each tile side, then the end
+    int* smode = reinterpret_cast<int*>(smem + T::kMode);
     R* rs = reinterpret_cast<R*>(smem + T::kDoubles);
     R* gs = rs + T::kG;
     R* fs = rs + T::kF;
@@ -441,7 +477,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     const GeneralMesh& M = a.m;
     const int tid = threadIdx.x;
     const int64_t base = static_cast<int64_t>(blockIdx.x) * EPB;
-    const int ne = static_cast<int>((count - base) < EPB ? (count - base) : EPB);
+    const int ne = static_cast<int>((grp.count - base) < EPB ? (grp.count - base) : EPB);
     const int64_t inst = blockIdx.y;
     const int64_t fb = M.block, ft = M.trace_total;
     double* q = a.q + inst * 3 * fb;
@@ -453,66 +489,68 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     const R* lp = tab<R>(g_lagrange_right, gf_lagrange_right) + gvec(N);
     const double dt = a.step[1];
 
-    if (tid < ne) {
-        const int64_t el = ids[base + tid];
-        eid[tid] = el;
-        eo2[tid] = M.off2[el];
-        eo1[tid] = M.off1[el];
+    // The tile's sides: slot ranges and flux modes (plan arrays in list
+    // order), and per element its number and offsets.
+    if (tid <= 4 * ne) {
+        const int64_t ps = 4 * (grp.first + base) + tid;
+        sst[tid] = M.pslot_start[ps];
+        if (tid < 4 * ne) smode[tid] = M.pside_mode[ps];
+        if (tid < ne) {
+            const int64_t el = grp.ids[base + tid];
+            eid[tid] = el;
+            eo2[tid] = M.off2[el];
+            eo1[tid] = M.off1[el];
+        }
     }
     __syncthreads();
-    // q tile: coalesced within each element's blocks.
-    for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
-        const int f = idx / (ne * NN), r = idx - f * (ne * NN);
+    // q and k tiles: asynchronous copies, waited for before the volume terms.
+    for (int idx = tid; idx < T::kVals; idx += T::kThreads) {
+        const int f = idx / (EPB * NN), r = idx - f * (EPB * NN);
         const int e = r / NN, node = r - e * NN;
-        const double v = q[f * fb + eo2[e] + node];
-        qs[(f * EPB + e) * NN + node] = v;
-        if constexpr (T::kCopy) qw[(f * EPB + e) * NN + node] = R(v);
+        if (e < ne) {
+            const int64_t gi = f * fb + eo2[e] + node;
+            cp_async8(qs + idx, q + gi);
+            if (!a.first) cp_async8(ks + idx, k + gi);
+        }
     }
     // Face fluxes at every face node of every side (Mesh2D_t.cpp:3803-3893,
-    // Solver2D_t.cpp:48-63): the tile's sides' slot counts (the sum of face
-    // order + 1 over a side's faces) and their prefix sums first, then one
-    // item per (element, side, slot), the slots of a side running over its
-    // faces' nodes in face-list order.
-    for (int idx = tid; idx < ne * 4; idx += T::kThreads) {
-        const int64_t e = eid[idx / 4];
-        const int s = idx & 3;
-        int cnt = 0;
-        for (int64_t q = M.sface_start[4 * e + s]; q < M.sface_start[4 * e + s + 1]; ++q) cnt += M.fN[M.sface[q]] + 1;
-        sps[idx + 1] = cnt;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        sps[0] = 0;
-        for (int i = 1; i <= ne * 4; ++i) sps[i] += sps[i - 1];
-    }
-    __syncthreads();
-    const int n_items = sps[ne * 4];
+    // Solver2D_t.cpp:48-63): one item per slot of the tile's contiguous slot
+    // range, the side found by bisection of the slot starts.
+    const int64_t g0 = sst[0];
+    const int n_items = static_cast<int>(sst[4 * ne] - g0);
     for (int idx = tid; idx < n_items; idx += T::kThreads) {
-        int lo = 0, hi = ne * 4;  // the side holding item idx: sps[lo] <= idx < sps[lo + 1]
+        const int64_t g = g0 + idx;
+        int lo = 0, hi = ne * 4;  // the side holding slot g: sst[lo] <= g < sst[lo + 1]
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (sps[mid] <= idx) lo = mid;
+            if (sst[mid] <= g) lo = mid;
             else hi = mid;
         }
-        const int ee = lo >> 2, s = lo & 3, slot = idx - sps[lo];
-        const int64_t e = eid[ee];
-        int64_t q = M.sface_start[4 * e + s];
-        int64_t f = M.sface[q];
-        int Nf = M.fN[f];
-        int j = slot;
-        while (j > Nf) {
-            j -= Nf + 1;
-            f = M.sface[++q];
-            Nf = M.fN[f];
-        }
+        const int slot = static_cast<int>(g - sst[lo]);
+        const int64_t d = M.slot_desc[g];
+        const int64_t src0 = M.slot_src[2 * g], src1 = M.slot_src[2 * g + 1];
+        const R nx = R(M.slot_normal[2 * g]), ny = R(M.slot_normal[2 * g + 1]);
         R L[3], Rv[3];
-        face_value<S, R>(M, tr, ft, f, Nf, 0, j, L);
-        face_value<S, R>(M, tr, ft, f, Nf, 1, j, Rv);
-        const R nx = R(M.fnormal[2 * f]), ny = R(M.fnormal[2 * f + 1]);
+        if (src0 >= 0) {
+            L[0] = tr[src0];
+            L[1] = tr[src0 + ft];
+            L[2] = tr[src0 + 2 * ft];
+        } else {
+            const int64_t fc = d / 32;
+            face_value<S, R>(M, tr, ft, fc, M.fN[fc], 0, static_cast<int>(d - 32 * fc), L);
+        }
+        if (src1 >= 0) {
+            Rv[0] = tr[src1];
+            Rv[1] = tr[src1 + ft];
+            Rv[2] = tr[src1 + 2 * ft];
+        } else {
+            const int64_t fc = d / 32;
+            face_value<S, R>(M, tr, ft, fc, M.fN[fc], 1, static_cast<int>(d - 32 * fc), Rv);
+        }
         const R wL = add<S>(L[0], add<S>(mul<S>(L[1], nx), mul<S>(L[2], ny)));
         const R wR = sub<S>(Rv[0], add<S>(mul<S>(Rv[1], nx), mul<S>(Rv[2], ny)));
         const R sum = add<S>(wL, wR);
-        R* o = ffs + (ee * 4 + s) * SL + slot;
+        R* o = ffs + lo * SL + slot;
         o[0] = mul<S>(sub<S>(wL, wR), R(0.5));
         o[FFS] = mul<S>(mul<S>(nx, sum), R(0.5));
         o[2 * FFS] = mul<S>(mul<S>(ny, sum), R(0.5));
@@ -549,7 +587,12 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
             js[e * NN + m * n + j] = S ? jac : R(1) / jac;
         }
     }
-    __syncthreads();  // q tile, face fluxes, J, edge metrics
+    // Each thread converts the q values it copied (FP32 form).
+    cp_async_wait_all();
+    if constexpr (T::kCopy) {
+        for (int idx = tid; idx < T::kVals; idx += T::kThreads) qw[idx] = R(qs[idx]);
+    }
+    __syncthreads();  // q and k tiles, face fluxes, J, edge metrics
 
     // Element side fluxes (Mesh2D_t::project_to_elements, Mesh2D_t.cpp:3895-4006):
     // the face flux times the edge metric where one face of the element's
@@ -558,36 +601,33 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
         const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
         const int s = sm / n, i = sm - s * n;
-        const int64_t el = eid[ee];
-        const int64_t q0 = M.sface_start[4 * el + s], q1 = M.sface_start[4 * el + s + 1];
+        const int mode = smode[ee * 4 + s];
         const R sfv = ss[ee * 4 + s];
         const R* fl = ffs + (ee * 4 + s) * SL;
         R out[3] = {0, 0, 0};
-        if (q1 > q0) {
-            const int64_t f0 = M.sface[q0];
-            const int64_t en0 = M.enodes[4 * el + s], en1 = M.enodes[4 * el + ((s + 1) & 3)];
-            if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0] == en0 && M.fnodes[2 * f0 + 1] == en1) {
-                for (int c = 0; c < 3; ++c) out[c] = mul<S>(fl[c * FFS + i], sfv);
-            } else if (q1 - q0 == 1 && M.fN[f0] == N && M.fnodes[2 * f0 + 1] == en0 && M.fnodes[2 * f0] == en1) {
-                for (int c = 0; c < 3; ++c) out[c] = mul<S>(-fl[c * FFS + (N - i)], sfv);
-            } else {
-                int slot0 = 0;
-                for (int64_t qq = q0; qq < q1; ++qq) {
-                    const int64_t ff = M.sface[qq];
-                    const int Nf = M.fN[ff];
-                    const int fsd = el == M.felem[2 * ff] ? 0 : 1;
-                    const R scale = R(M.fscale[2 * ff + fsd]);
-                    const double* W = M.sw + M.sw_off[qq] + i * (Nf + 1);
-                    const int* match = M.smatch + M.sm_off[qq];
-                    for (int j = 0; j <= Nf; ++j) {
-                        const int mt = match[j];
-                        if (mt >= 0 && mt != i) continue;
-                        const R w = R(W[j]);
+        if (mode == 1) {
+            for (int c = 0; c < 3; ++c) out[c] = mul<S>(fl[c * FFS + i], sfv);
+        } else if (mode == 2) {
+            for (int c = 0; c < 3; ++c) out[c] = mul<S>(-fl[c * FFS + (N - i)], sfv);
+        } else if (mode == 3) {
+            const int64_t el = eid[ee];
+            const int64_t q0 = M.sface_start[4 * el + s], q1 = M.sface_start[4 * el + s + 1];
+            int slot0 = 0;
+            for (int64_t qq = q0; qq < q1; ++qq) {
+                const int64_t ff = M.sface[qq];
+                const int Nf = M.fN[ff];
+                const int fsd = el == M.felem[2 * ff] ? 0 : 1;
+                const R scale = R(M.fscale[2 * ff + fsd]);
+                const double* W = M.sw + M.sw_off[qq] + i * (Nf + 1);
+                const int* match = M.smatch + M.sm_off[qq];
+                for (int j = 0; j <= Nf; ++j) {
+                    const int mt = match[j];
+                    if (mt >= 0 && mt != i) continue;
+                    const R w = R(W[j]);
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) out[c] = add<S>(out[c], mul<S>(mul<S>(mul<S>(w, fl[c * FFS + slot0 + j]), sfv), scale));
-                    }
-                    slot0 += Nf + 1;
+                    for (int c = 0; c < 3; ++c) out[c] = add<S>(out[c], mul<S>(mul<S>(mul<S>(w, fl[c * FFS + slot0 + j]), sfv), scale));
                 }
+                slot0 += Nf + 1;
             }
         }
         fs[0 * FS + idx] = out[0];
@@ -657,17 +697,18 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
 
     // Low-storage RK3 update (Solver2D_t.cpp:138-172), node by node, in FP64.
     const double gdt = mul<S>(a.rk_g, dt);
-    for (int idx = tid; idx < 3 * ne * NN; idx += T::kThreads) {
-        const int ff = idx / (ne * NN), r = idx - ff * (ne * NN);
+    for (int idx = tid; idx < T::kVals; idx += T::kThreads) {
+        const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
         const int ee = r / NN, node = r - ee * NN;
+        if (ee >= ne) continue;
         const int64_t gi = ff * fb + eo2[ee] + node;
-        const double G = static_cast<double>(gs[(ff * EPB + ee) * NN + node]);
-        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, k[gi]), G);
-        const double qn = add<S>(qs[(ff * EPB + ee) * NN + node], mul<S>(gdt, kn));
+        const double G = static_cast<double>(gs[idx]);
+        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, ks[idx]), G);
+        const double qn = add<S>(qs[idx], mul<S>(gdt, kn));
         k[gi] = kn;
         q[gi] = qn;
-        qs[(ff * EPB + ee) * NN + node] = qn;
-        if constexpr (T::kCopy) qw[(ff * EPB + ee) * NN + node] = R(qn);
+        qs[idx] = qn;
+        if constexpr (T::kCopy) qw[idx] = R(qn);
         if (a.G_out) a.G_out[inst * 3 * fb + gi] = G;
     }
     __syncthreads();
@@ -818,7 +859,7 @@ template <int N, bool S, typename R>
 cudaError_t launch_fused(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
     using T = FusedTile<N, R>;
     const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
-    general_fused_kernel<N, S, R><<<grid, T::kThreads, T::bytes(a.side_slots), stream>>>(a, g.ids, g.count);
+    general_fused_kernel<N, S, R><<<grid, T::kThreads, T::bytes(a.side_slots), stream>>>(a, g);
     return cudaGetLastError();
 }
 

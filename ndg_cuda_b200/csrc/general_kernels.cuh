@@ -65,6 +65,18 @@ struct GeneralMesh {
     const int* smatch = nullptr;
     const double* fw = nullptr;
     const int* fmatch = nullptr;
+    // Face-node slots of the domain element sides in group-list order (side
+    // s of list position p owns [pslot_start[4 p + s], pslot_start[4 p + s + 1])):
+    // per slot the face and node (32 f + j), the face normal, and per face
+    // side the trace value the slot reads (first of the three fields; -1
+    // where the face side interpolates); per position side its flux mode (0
+    // no face, 1 one conforming face, 2 the same reversed, 3 mortar).
+    int64_t n_slots = 0;
+    const int64_t* pslot_start = nullptr;  // [4 n_domain + 1]
+    const int64_t* slot_desc = nullptr;    // [n_slots]
+    const double* slot_normal = nullptr;   // [2 n_slots]
+    const int64_t* slot_src = nullptr;     // [2 n_slots], filled by launch_general_weights
+    const int* pside_mode = nullptr;       // [4 n_domain]
 };
 
 // One RK3 stage on a mixed-order mesh.
@@ -89,12 +101,14 @@ struct OrderGroup {
     int N = 0;
     int64_t count = 0;
     const int64_t* ids = nullptr;  // device, element numbers
+    int64_t first = 0;             // list position of the group's first element
 };
 
 cudaError_t upload_general_tables(const Tables& t);
 // Fills the mortar weights of a plan (once per plan): the same arithmetic,
 // in the reference's rounding, as the per-node computation they replace.
-cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, cudaStream_t stream);
+// Then the trace sources of the face-node slots (slot_src).
+cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, int64_t* slot_src, cudaStream_t stream);
 cudaError_t prepare_general_kernels(int N, int side_slots);
 // Side traces of q into etr (before the first stage, or after q changed).
 cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* groups, int n_groups, bool strict, bool fp32, cudaStream_t stream);

@@ -124,6 +124,18 @@ struct GeneralPlan {
     // (off1 + side (N_e + 1)) and the element's order
     std::vector<int64_t> fbase;
     std::vector<int32_t> fsN;
+    // Face-node slots of the domain element sides, numbered in the order of
+    // the group lists (position p = index of the element in the
+    // concatenated lists): side s of position p owns slots
+    // [pslot_start[4 p + s], pslot_start[4 p + s + 1]), running over the
+    // side's faces in list order and each face's nodes; per slot the face and
+    // node as 32 f + j and the face normal (2 values). pside_mode per position
+    // side: 0 no face, 1 one face of the element's order from the side's
+    // first to its second node, 2 the same face reversed, 3 mortar.
+    std::vector<int64_t> pslot_start, slot_desc;
+    std::vector<double> slot_normal;
+    std::vector<int32_t> pside_mode;
+    int64_t n_slots = 0;
 };
 GeneralPlan build_general_plan(const Topology& t);
 
