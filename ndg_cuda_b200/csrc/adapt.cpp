@@ -245,6 +245,39 @@ GeneralPlan build_general_plan(const Topology& t) {
             p.fm_total += nf;
         }
 
+    // Ghost side-0 gathers, for the ghosts whose trace is projected from
+    // their neighbours (mirror and copy kinds).
+    p.gq_start.assign(static_cast<size_t>(G + 1), 0);
+    p.gframe.assign(static_cast<size_t>(4 * G), 0.0);
+    for (int64_t g = K; g < total; ++g) {
+        const size_t gi = static_cast<size_t>(g - K);
+        p.gq_start[gi] = static_cast<int64_t>(p.gq_face.size());
+        if (p.gkind[gi] != 0 && p.gkind[gi] != 2) continue;
+        const int Ng = t.elem_N[static_cast<size_t>(g)];
+        const int64_t q0 = p.sface_start[static_cast<size_t>(4 * g)], q1 = p.sface_start[static_cast<size_t>(4 * g + 1)];
+        for (int64_t q = q0; q < q1; ++q) {
+            const int64_t f = p.sface[static_cast<size_t>(q)];
+            const int fs = t.face_elems[static_cast<size_t>(f)][0] == g ? 1 : 0;
+            const int Nn = p.fsN[static_cast<size_t>(2 * f + fs)];
+            p.gq_face.push_back(f);
+            p.gq_fs.push_back(fs);
+            p.gq_base.push_back(p.fbase[static_cast<size_t>(2 * f + fs)]);
+            p.gq_N.push_back(Nn);
+            p.gq_woff.push_back(p.sw_total);
+            p.sw_total += static_cast<int64_t>(Ng + 1) * (Nn + 1);
+            p.gq_moff.push_back(p.sm_total);
+            p.sm_total += Nn + 1;
+        }
+        if (q1 > q0) {
+            const size_t f0 = static_cast<size_t>(p.sface[static_cast<size_t>(q0)]);
+            p.gframe[4 * gi] = t.face_normal[f0][0];
+            p.gframe[4 * gi + 1] = t.face_normal[f0][1];
+            p.gframe[4 * gi + 2] = t.face_tangent[f0][0];
+            p.gframe[4 * gi + 3] = t.face_tangent[f0][1];
+        }
+    }
+    p.gq_start[static_cast<size_t>(G)] = static_cast<int64_t>(p.gq_face.size());
+
     // Slots and side modes in group-list order, so that the sides of one
     // tile of a group own one contiguous slot range.
     p.pslot_start.assign(static_cast<size_t>(4 * K + 1), 0);

@@ -396,6 +396,14 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_slot_normal.upload(g.slot_normal, c->stream);
         c->g_pside_mode.upload(g.pside_mode, c->stream);
         c->g_slot_src.allocate(static_cast<size_t>(std::max<int64_t>(2 * g.n_slots, 1)));
+        c->g_gq_start.upload(g.gq_start, c->stream);
+        c->g_gq_face.upload(g.gq_face, c->stream);
+        c->g_gq_fs.upload(g.gq_fs, c->stream);
+        c->g_gq_base.upload(g.gq_base, c->stream);
+        c->g_gq_N.upload(g.gq_N, c->stream);
+        c->g_gq_woff.upload(g.gq_woff, c->stream);
+        c->g_gq_moff.upload(g.gq_moff, c->stream);
+        c->g_gframe.upload(g.gframe, c->stream);
         std::vector<int64_t> ids;
         for (const auto& grp : g.groups) ids.insert(ids.end(), grp.second.begin(), grp.second.end());
         c->g_ids.upload(ids, c->stream);
@@ -465,9 +473,17 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.slot_normal = c->g_slot_normal.ptr;
         M.slot_src = c->g_slot_src.ptr;
         M.pside_mode = c->g_pside_mode.ptr;
+        M.gq_start = c->g_gq_start.ptr;
+        M.gq_face = c->g_gq_face.ptr;
+        M.gq_fs = c->g_gq_fs.ptr;
+        M.gq_base = c->g_gq_base.ptr;
+        M.gq_N = c->g_gq_N.ptr;
+        M.gq_woff = c->g_gq_woff.ptr;
+        M.gq_moff = c->g_gq_moff.ptr;
+        M.gframe = c->g_gframe.ptr;
         check_cuda(dev::launch_general_weights(M, c->g_sw.ptr, c->g_smatch.ptr, c->g_fw.ptr, c->g_fmatch.ptr, c->g_slot_src.ptr, c->stream),
                    "mortar weights");
-        c->launches += 3;
+        c->launches += 4;
         // The uniform-path corners also serve the initial condition of a
         // general mesh.
         c->corners.upload(g.corners, c->stream);

@@ -153,50 +153,30 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a, int
         R* gv = gu + ft;
         const int kind = M.gkind[gi];
         if (kind == kGhostMirror || kind == kGhostCopy) {
-            // Mesh2D_t.cpp:4366-4434 (multi-face branch) and 4601-4710.
-            const double* we = g_weights + gvec(N);
-            const double* bwe = g_bary + gvec(N);
+            // Mesh2D_t.cpp:4366-4434 (multi-face branch) and 4601-4710, with
+            // the plan's weights (ghost_weights_kernel).
             const R sf = R(M.gscale[gi]);
             R vp = 0, vu = 0, vv = 0;
-            for (int64_t q = M.sface_start[4 * ge]; q < M.sface_start[4 * ge + 1]; ++q) {
-                const int64_t f = M.sface[q];
-                const int fs = M.felem[2 * f] == ge ? 1 : 0;
-                const int64_t nb = M.felem[2 * f + fs];
-                const int64_t nbs = M.fside[2 * f + fs];
-                const int Nn = M.eN[nb];
-                const double* xnb = g_nodes + gvec(Nn);
-                const double* wnb = g_weights + gvec(Nn);
-                const R* np_ = tr + M.off1[nb] + nbs * (Nn + 1);
+            const int64_t e0 = M.gq_start[gi], e1 = M.gq_start[gi + 1];
+            for (int64_t qe = e0; qe < e1; ++qe) {
+                const int Nn = M.gq_N[qe];
+                const R* np_ = tr + M.gq_base[qe];
                 const R* nu_ = np_ + ft;
                 const R* nv_ = nu_ + ft;
-                const double scale = M.fscale[2 * f + fs], offset = M.foffset[2 * f + fs];
+                const double* W = M.sw + M.gq_woff[qe] + i * (Nn + 1);
+                const int* match = M.smatch + M.gq_moff[qe];
                 for (int j = 0; j <= Nn; ++j) {
-                    const double coord = mortar_coord(xnb[Nn - j], scale, offset);
-                    int found = -1;
-                    for (int ii = 0; ii <= N; ++ii)
-                        if (almost_equal(coord, xe[ii])) {
-                            found = ii;
-                            break;
-                        }
-                    R w;
-                    if (found >= 0) {
-                        if (found != i) continue;
-                        w = R(S ? __ddiv_rn(wnb[j], we[i]) : wnb[j] / we[i]);
-                    } else {
-                        double sb = 0.0;
-                        for (int ii = 0; ii <= N; ++ii) sb = add<S>(sb, S ? __ddiv_rn(bwe[ii], __dsub_rn(coord, xe[ii])) : bwe[ii] / (coord - xe[ii]));
-                        const double T = S ? __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), sb)) : bwe[i] / ((coord - xe[i]) * sb);
-                        w = R(S ? __ddiv_rn(__dmul_rn(T, wnb[j]), we[i]) : T * wnb[j] / we[i]);
-                    }
+                    const int mt = match[j];
+                    if (mt >= 0 && mt != i) continue;
+                    const R w = R(W[j]);
                     vp = add<S>(vp, mul<S>(mul<S>(w, np_[j]), sf));
                     vu = add<S>(vu, mul<S>(mul<S>(w, nu_[j]), sf));
                     vv = add<S>(vv, mul<S>(mul<S>(w, nv_[j]), sf));
                 }
             }
-            if (kind == kGhostMirror && M.sface_start[4 * ge + 1] > M.sface_start[4 * ge]) {
-                const int64_t f = M.sface[M.sface_start[4 * ge]];
-                const R nx = R(M.fnormal[2 * f]), ny = R(M.fnormal[2 * f + 1]);
-                const R tx = R(M.ftangent[2 * f]), ty = R(M.ftangent[2 * f + 1]);
+            if (kind == kGhostMirror && e1 > e0) {
+                const R nx = R(M.gframe[4 * gi]), ny = R(M.gframe[4 * gi + 1]);
+                const R tx = R(M.gframe[4 * gi + 2]), ty = R(M.gframe[4 * gi + 3]);
                 const R l0 = -add<S>(mul<S>(vu, nx), mul<S>(vv, ny));
                 const R l1 = add<S>(mul<S>(vu, tx), mul<S>(vv, ty));
                 vu = add<S>(mul<S>(nx, l0), mul<S>(tx, l1));
@@ -322,6 +302,52 @@ __global__ void __launch_bounds__(128) face_weights_kernel(GeneralMesh M, double
     }
 }
 
+// Weights of the ghost side-0 gathers (Mesh2D_t.cpp:4366-4434, 4601-4710):
+// per neighbour node j the ghost node it matches (almost_equal) or -1, and
+// the weight of every ghost node i, w_n[j] / w_g[i] at the match or
+// T_i w_n[j] / w_g[i] with the barycentric T_i, in the reference's rounding.
+// Thread per ghost.
+__global__ void __launch_bounds__(128) ghost_weights_kernel(GeneralMesh M, double* __restrict__ sw, int* __restrict__ smatch) {
+    const int64_t n_ghosts = M.n_total - M.n_domain;
+    for (int64_t gi = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; gi < n_ghosts;
+         gi += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int N = M.eN[M.n_domain + gi];
+        const double* xe = g_nodes + gvec(N);
+        const double* we = g_weights + gvec(N);
+        const double* bwe = g_bary + gvec(N);
+        for (int64_t qe = M.gq_start[gi]; qe < M.gq_start[gi + 1]; ++qe) {
+            const int64_t f = M.gq_face[qe];
+            const int fs = M.gq_fs[qe];
+            const int Nn = M.gq_N[qe];
+            const double* xnb = g_nodes + gvec(Nn);
+            const double* wnb = g_weights + gvec(Nn);
+            const double scale = M.fscale[2 * f + fs], offset = M.foffset[2 * f + fs];
+            double* W = sw + M.gq_woff[qe];
+            int* match = smatch + M.gq_moff[qe];
+            for (int j = 0; j <= Nn; ++j) {
+                const double coord = mortar_coord(xnb[Nn - j], scale, offset);
+                int found = -1;
+                for (int ii = 0; ii <= N; ++ii)
+                    if (almost_equal(coord, xe[ii])) {
+                        found = ii;
+                        break;
+                    }
+                match[j] = found;
+                if (found >= 0) {
+                    for (int i = 0; i <= N; ++i) W[i * (Nn + 1) + j] = (i == found) ? __ddiv_rn(wnb[j], we[i]) : 0.0;
+                } else {
+                    double sb = 0.0;
+                    for (int ii = 0; ii <= N; ++ii) sb = __dadd_rn(sb, __ddiv_rn(bwe[ii], __dsub_rn(coord, xe[ii])));
+                    for (int i = 0; i <= N; ++i) {
+                        const double T = __ddiv_rn(bwe[i], __dmul_rn(__dsub_rn(coord, xe[i]), sb));
+                        W[i * (Nn + 1) + j] = __ddiv_rn(__dmul_rn(T, wnb[j]), we[i]);
+                    }
+                }
+            }
+        }
+    }
+}
+
 // Trace value each face-node slot reads on each face side, as face_value
 // picks it: the element side's node (side 0) or its mirror (side 1) where the
 // face side is conforming, the matched node where the face node coincides
@@ -356,6 +382,10 @@ cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch
     if (m.n_faces > 0) {
         const int blocks = static_cast<int>(std::min<int64_t>((2 * m.n_faces + 127) / 128, 148 * 8));
         face_weights_kernel<<<blocks, 128, 0, stream>>>(m, fw, fmatch);
+    }
+    if (m.n_total > m.n_domain) {
+        const int blocks = static_cast<int>(std::min<int64_t>((m.n_total - m.n_domain + 127) / 128, 148 * 8));
+        ghost_weights_kernel<<<blocks, 128, 0, stream>>>(m, sw, smatch);
     }
     if (m.n_slots > 0) {
         const int blocks = static_cast<int>(std::min<int64_t>((2 * m.n_slots + 127) / 128, 148 * 8));

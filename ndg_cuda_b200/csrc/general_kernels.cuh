@@ -77,6 +77,19 @@ struct GeneralMesh {
     const double* slot_normal = nullptr;   // [2 n_slots]
     const int64_t* slot_src = nullptr;     // [2 n_slots], filled by launch_general_weights
     const int* pside_mode = nullptr;       // [4 n_domain]
+    // Ghost side-0 gathers of the mirror and copy ghosts (ghost g - n_domain
+    // owns entries [gq_start[.], gq_start[. + 1])): per entry the face and the
+    // neighbour's face side, the neighbour side's trace base and order, and
+    // the offsets of its weights and node matches in sw / smatch; gframe is
+    // the normal and tangent of each ghost's first face.
+    const int64_t* gq_start = nullptr;     // [n_total - n_domain + 1]
+    const int64_t* gq_face = nullptr;
+    const int* gq_fs = nullptr;
+    const int64_t* gq_base = nullptr;
+    const int* gq_N = nullptr;
+    const int64_t* gq_woff = nullptr;
+    const int64_t* gq_moff = nullptr;
+    const double* gframe = nullptr;        // [4 (n_total - n_domain)]
 };
 
 // One RK3 stage on a mixed-order mesh.
@@ -107,7 +120,8 @@ struct OrderGroup {
 cudaError_t upload_general_tables(const Tables& t);
 // Fills the mortar weights of a plan (once per plan): the same arithmetic,
 // in the reference's rounding, as the per-node computation they replace.
-// Then the trace sources of the face-node slots (slot_src).
+// Then the ghost gathers' weights (into sw, smatch) and the trace sources of
+// the face-node slots (slot_src).
 cudaError_t launch_general_weights(const GeneralMesh& m, double* sw, int* smatch, double* fw, int* fmatch, int64_t* slot_src, cudaStream_t stream);
 cudaError_t prepare_general_kernels(int N, int side_slots);
 // Side traces of q into etr (before the first stage, or after q changed).

@@ -136,6 +136,16 @@ struct GeneralPlan {
     std::vector<double> slot_normal;
     std::vector<int32_t> pside_mode;
     int64_t n_slots = 0;
+    // Ghost side-0 gathers (wall, symmetry and outflow ghosts): ghost g (from
+    // n_domain) owns entries [gq_start[g - n_domain], gq_start[g - n_domain + 1]),
+    // one per face of its side 0 in list order, each with the face and the
+    // neighbour's face side, the neighbour side's trace base and order, and
+    // the offsets of its weights [(N_g+1) x (N_n+1)] and node matches [N_n+1]
+    // in the side-weight arrays (filled on the device). gframe: normal and
+    // tangent of the ghost's first face (4 per ghost).
+    std::vector<int64_t> gq_start, gq_face, gq_base, gq_woff, gq_moff;
+    std::vector<int32_t> gq_fs, gq_N;
+    std::vector<double> gframe;
 };
 GeneralPlan build_general_plan(const Topology& t);
 
