@@ -45,6 +45,14 @@ ADJ_RES, ADJ_N, ADJ_STEPS, ADJ_INTERVAL, ADJ_RECEIVERS = 96, 7, 1000, 50, 16
 HP_RES, HP_N0, HP_NMAX, HP_SPLITS, HP_INTERVAL, HP_STEPS = 128, 4, 12, 2, 20, 3000
 # Batched workload: 64 instances on one 64 x 64 walled mesh, N = 6, 1000 steps.
 BATCH_RES, BATCH_N, BATCH_INSTANCES, BATCH_STEPS = 64, 6, 64, 1000
+# The reference's published order sweep (thesis/Chapter_results/code/plots.py:152-153,
+# setup thesis/Chapter_results/results.tex:64-97 and 664-676): a 64 x 64 mesh on a
+# unit square, the plane wave with boundaries held to the analytic solution, CFL
+# 0.5, 1000 RK3 iterations with an error estimate and adaptation every 100 that
+# never refines; ms per iteration on one A100 40 GB and on one AMD Milan 7413 core.
+SWEEP_RES, SWEEP_STEPS, SWEEP_INTERVAL = 64, 1000, 100
+SWEEP_A100_MS = {4: 2.149, 6: 4.136, 8: 8.075, 10: 12.71, 12: 18.22, 14: 26.06, 16: 33.39}
+SWEEP_CPU_CORE_MS = {4: 40.11, 6: 71.50, 8: 108.4, 10: 166.6, 12: 257.5, 14: 349.0, 16: 490.1}
 # adjoint stage: lq and lk read and written, the stage input qs read (FP64);
 # forward stage keeping its input: q, k read and written, q written once more
 ADJ_BYTES_PER_DOF_STAGE = 40
@@ -324,6 +332,50 @@ def hp_run(local: int, stream, tolerance: float, steps: int, precision: int = 0,
     fields = {f: m.get_field(f) for f in ("p", "u", "v")}
     m.close()
     return out, flags, fields
+
+
+def order_sweep_leg(local: int, stream) -> dict:
+    """The reference's published order sweep, run the same way here: per
+    order, 1000 RK3 steps with an error estimate and an adaptation every 100
+    (maximum order and split level held at the start, so that nothing
+    refines, as in the published runs). ms per iteration is the host wall
+    time of the whole loop (estimates, flag downloads and adaptation calls
+    included) over the iterations; the device time of the same loop is
+    reported beside it."""
+    import torch
+    import ndg_cuda_b200 as ndg
+    from ndg_cuda_b200 import meshgen
+    zone = meshgen.uniform_zone(SWEEP_RES, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, boundary=meshgen.INFLOW)
+    orders = {}
+    for N in sorted(SWEEP_A100_MS):
+        m = ndg.Mesh2D_t(zone, N, maximum_N=N, max_split_level=0, cfl=CFL, device=local, stream=stream.cuda_stream)
+        m.initial_conditions()
+        tile, _ = m.autotune(10)
+        ndg.Solver2D_t.run(m, 5)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(SWEEP_STEPS // SWEEP_INTERVAL):
+            ndg.Solver2D_t.run(m, SWEEP_INTERVAL)
+            m.estimate_error()
+            m.adapt()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        ms = 1e3 * wall / SWEEP_STEPS
+        dof = ndg.dof_count(m)
+        orders[str(N)] = {"ms_per_iteration": ms, "device_ms_per_iteration": e0.elapsed_time(e1) / SWEEP_STEPS,
+                          "dof": dof, "value": dof * 3 * SWEEP_STEPS / wall, "unit": "DOF-stage updates/s",
+                          "reference_a100_ms": SWEEP_A100_MS[N], "speedup_vs_reference_a100": SWEEP_A100_MS[N] / ms,
+                          "reference_cpu_core_ms": SWEEP_CPU_CORE_MS[N], "elements_after": m.n_elements_,
+                          "tile_elements_per_cta": tile or m.tile_candidates()[1]}
+        m.close()
+    return {"workload": f"dg_wave_rk3_inflow_{SWEEP_RES}x{SWEEP_RES}_unit_square_plane_wave_N4to16",
+            "setup": (f"{SWEEP_RES}x{SWEEP_RES} quads on [0,1]^2, boundaries held to the analytic plane wave, CFL {CFL}, FP64, "
+                      f"{SWEEP_STEPS} RK3 steps with an error estimate and adaptation every {SWEEP_INTERVAL} (nothing refines)"),
+            "reference_numbers": "published ms per iteration of the reference (thesis plots.py:152-153): one A100 40 GB, one AMD Milan 7413 core",
+            "orders": orders}
 
 
 def hp_leg(local: int, stream) -> dict:
@@ -649,6 +701,8 @@ def run_ours(args) -> None:
 
     config1 = config1_leg(local, stream) if not args.no_fp32 and world == 1 else None
 
+    sweep = order_sweep_leg(local, stream) if not args.no_sweep and world == 1 else None
+
     batched = None
     if not args.no_batched:
         batched = batched_leg(local, stream, peak, dist)
@@ -682,6 +736,7 @@ def run_ours(args) -> None:
                 "fp32": fp32,
                 "config1_analytic": config1,
                 "hp_adaptive": hp,
+                "order_sweep": sweep,
                 "batched": batched,
                 "adjoint": adjoint,
                 "gpu_launches": launches,
@@ -705,6 +760,7 @@ def main() -> None:
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances leg (profiling runs)")
     ap.add_argument("--no-hp", action="store_true", help="skip the hp-adaptive leg (profiling runs)")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the order sweep on the reference's published 64 x 64 case")
     ap.add_argument("--tile", type=int, default=None,
                     help="elements per CTA of the main leg's stage kernel instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
