@@ -53,6 +53,12 @@ BATCH_RES, BATCH_N, BATCH_INSTANCES, BATCH_STEPS = 64, 6, 64, 1000
 SWEEP_RES, SWEEP_STEPS, SWEEP_INTERVAL = 64, 1000, 100
 SWEEP_A100_MS = {4: 2.149, 6: 4.136, 8: 8.075, 10: 12.71, 12: 18.22, 14: 26.06, 16: 33.39}
 SWEEP_CPU_CORE_MS = {4: 40.11, 6: 71.50, 8: 108.4, 10: 166.6, 12: 257.5, 14: 349.0, 16: 490.1}
+# The reference's published full runs of the same plane wave to t = 2 s with no
+# adaptivity (thesis/Chapter_results/code/plots.py:22 and 101-104; setup
+# thesis/Chapter_results/results.tex:23-35, 164-171, 323-333): mesh, order,
+# published steps, published wall seconds, hardware.
+PUBLISHED_RUNS = [(128, 10, 51200, 1136.14, "A100 40 GB"), (32, 10, 12800, 48.36, "A100 40 GB"),
+                  (256, 4, 16384, 4036.09, "V100 SXM2 16 GB")]
 # adjoint stage: lq and lk read and written, the stage input qs read (FP64);
 # forward stage keeping its input: q, k read and written, q written once more
 ADJ_BYTES_PER_DOF_STAGE = 40
@@ -376,6 +382,43 @@ def order_sweep_leg(local: int, stream) -> dict:
                       f"{SWEEP_STEPS} RK3 steps with an error estimate and adaptation every {SWEEP_INTERVAL} (nothing refines)"),
             "reference_numbers": "published ms per iteration of the reference (thesis plots.py:152-153): one A100 40 GB, one AMD Milan 7413 core",
             "orders": orders}
+
+
+def published_runs_leg(local: int, stream) -> dict:
+    """The reference's published full runs, end to end: the plane wave on a
+    unit square with boundaries held to the analytic solution, CFL 0.5, from
+    t = 0 to t = 2 s through Solver2D_t.solve (the last step shortened to land
+    on t = 2), no adaptivity. Wall time from the initial condition on the
+    device to the final state, and the L2 error against the analytic
+    solution at t = 2."""
+    import torch
+    import ndg_cuda_b200 as ndg
+    from ndg_cuda_b200 import meshgen
+    runs = []
+    for res, N, ref_steps, ref_s, hardware in PUBLISHED_RUNS:
+        zone = meshgen.uniform_zone(res, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, boundary=meshgen.INFLOW)
+        m = ndg.Mesh2D_t(zone, N, cfl=CFL, device=local, stream=stream.cuda_stream)
+        m.initial_conditions()
+        tile, _ = m.autotune(10)
+        solver = ndg.Solver2D_t(CFL, output_times=(2.0,))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        e0.record(stream)
+        m.initial_conditions()
+        t, steps = solver.solve(m)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        dof = ndg.dof_count(m)
+        runs.append({"mesh": f"{res}x{res}", "N": N, "dof": dof, "steps": steps, "reference_steps": ref_steps, "time": t,
+                     "wall_s": wall, "device_s": e0.elapsed_time(e1) / 1e3, "value": dof * 3 * steps / wall,
+                     "unit": "DOF-stage updates/s", "reference_wall_s": ref_s, "reference_hardware": hardware,
+                     "speedup_vs_reference": ref_s / wall, "l2_vs_analytic": dict(zip("puv", map(float, m.l2_error(t)))),
+                     "tile_elements_per_cta": tile or m.tile_candidates()[1]})
+        m.close()
+    return {"setup": f"unit square, boundaries held to the analytic plane wave, CFL {CFL}, FP64, t = 0 to 2 s, no adaptivity",
+            "reference_numbers": "published wall times of the reference (thesis plots.py:22, 101-104)", "runs": runs}
 
 
 def hp_leg(local: int, stream) -> dict:
@@ -702,6 +745,7 @@ def run_ours(args) -> None:
     config1 = config1_leg(local, stream) if not args.no_fp32 and world == 1 else None
 
     sweep = order_sweep_leg(local, stream) if not args.no_sweep and world == 1 else None
+    published = published_runs_leg(local, stream) if not args.no_sweep and world == 1 else None
 
     batched = None
     if not args.no_batched:
@@ -737,6 +781,7 @@ def run_ours(args) -> None:
                 "config1_analytic": config1,
                 "hp_adaptive": hp,
                 "order_sweep": sweep,
+                "published_runs": published,
                 "batched": batched,
                 "adjoint": adjoint,
                 "gpu_launches": launches,
@@ -760,7 +805,7 @@ def main() -> None:
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances leg (profiling runs)")
     ap.add_argument("--no-hp", action="store_true", help="skip the hp-adaptive leg (profiling runs)")
-    ap.add_argument("--no-sweep", action="store_true", help="skip the order sweep on the reference's published 64 x 64 case")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the legs on the reference's published cases (order sweep, full runs)")
     ap.add_argument("--tile", type=int, default=None,
                     help="elements per CTA of the main leg's stage kernel instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
