@@ -282,6 +282,7 @@ GeneralPlan build_general_plan(const Topology& t) {
     // tile of a group own one contiguous slot range.
     p.pslot_start.assign(static_cast<size_t>(4 * K + 1), 0);
     p.pside_mode.assign(static_cast<size_t>(4 * K), 0);
+    p.pq_start.assign(static_cast<size_t>(4 * K + 1), 0);
     int64_t pos = 0, slot = 0;
     for (const auto& grp : p.groups)
         for (int64_t e : grp.second) {
@@ -289,6 +290,7 @@ GeneralPlan build_general_plan(const Topology& t) {
             for (int s = 0; s < 4; ++s) {
                 const size_t ps = static_cast<size_t>(4 * pos + s);
                 p.pslot_start[ps] = slot;
+                p.pq_start[ps] = static_cast<int64_t>(p.pq_N.size());
                 const int64_t q0 = p.sface_start[static_cast<size_t>(4 * e + s)], q1 = p.sface_start[static_cast<size_t>(4 * e + s + 1)];
                 for (int64_t q = q0; q < q1; ++q) {
                     const int64_t f = p.sface[static_cast<size_t>(q)];
@@ -305,10 +307,20 @@ GeneralPlan build_general_plan(const Topology& t) {
                 const int64_t en0 = p.enodes[static_cast<size_t>(4 * e + s)], en1 = p.enodes[static_cast<size_t>(4 * e + ((s + 1) & 3))];
                 const bool one = q1 - q0 == 1 && t.face_N[static_cast<size_t>(f0)] == Ne;
                 p.pside_mode[ps] = one && fn[0] == en0 && fn[1] == en1 ? 1 : one && fn[1] == en0 && fn[0] == en1 ? 2 : 3;
+                if (p.pside_mode[ps] != 3) continue;
+                for (int64_t q = q0; q < q1; ++q) {
+                    const size_t f = static_cast<size_t>(p.sface[static_cast<size_t>(q)]);
+                    const int fsd = t.face_elems[f][0] == e ? 0 : 1;
+                    p.pq_N.push_back(t.face_N[f]);
+                    p.pq_scale.push_back(t.face_scale[f][static_cast<size_t>(fsd)]);
+                    p.pq_woff.push_back(p.sw_off[static_cast<size_t>(q)]);
+                    p.pq_moff.push_back(p.sm_off[static_cast<size_t>(q)]);
+                }
             }
             ++pos;
         }
     p.pslot_start[static_cast<size_t>(4 * K)] = slot;
+    p.pq_start[static_cast<size_t>(4 * K)] = static_cast<int64_t>(p.pq_N.size());
     p.n_slots = slot;
     return p;
 }

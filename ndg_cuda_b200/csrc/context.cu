@@ -396,6 +396,11 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_slot_normal.upload(g.slot_normal, c->stream);
         c->g_pside_mode.upload(g.pside_mode, c->stream);
         c->g_slot_src.allocate(static_cast<size_t>(std::max<int64_t>(2 * g.n_slots, 1)));
+        c->g_pq_start.upload(g.pq_start, c->stream);
+        c->g_pq_N.upload(g.pq_N, c->stream);
+        c->g_pq_scale.upload(g.pq_scale, c->stream);
+        c->g_pq_woff.upload(g.pq_woff, c->stream);
+        c->g_pq_moff.upload(g.pq_moff, c->stream);
         c->g_gq_start.upload(g.gq_start, c->stream);
         c->g_gq_face.upload(g.gq_face, c->stream);
         c->g_gq_fs.upload(g.gq_fs, c->stream);
@@ -473,6 +478,11 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.slot_normal = c->g_slot_normal.ptr;
         M.slot_src = c->g_slot_src.ptr;
         M.pside_mode = c->g_pside_mode.ptr;
+        M.pq_start = c->g_pq_start.ptr;
+        M.pq_N = c->g_pq_N.ptr;
+        M.pq_scale = c->g_pq_scale.ptr;
+        M.pq_woff = c->g_pq_woff.ptr;
+        M.pq_moff = c->g_pq_moff.ptr;
         M.gq_start = c->g_gq_start.ptr;
         M.gq_face = c->g_gq_face.ptr;
         M.gq_fs = c->g_gq_fs.ptr;

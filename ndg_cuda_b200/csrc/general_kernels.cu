@@ -348,10 +348,11 @@ __global__ void __launch_bounds__(128) ghost_weights_kernel(GeneralMesh M, doubl
     }
 }
 
-// Trace value each face-node slot reads on each face side, as face_value
-// picks it: the element side's node (side 0) or its mirror (side 1) where the
-// face side is conforming, the matched node where the face node coincides
-// with an element node, -1 where face_value interpolates.
+// Trace value each face-node slot reads on each face side
+// (Mesh2D_t::project_to_faces, Mesh2D_t.cpp:3803-3893): the element side's
+// node (side 0) or its mirror (side 1) where the face side is conforming, the
+// matched node where the face node coincides with an element node, otherwise
+// -1 - (32 (2 f + side) + j): the face side and node to interpolate at.
 __global__ void __launch_bounds__(128) slot_sources_kernel(GeneralMesh M, int64_t* __restrict__ src) {
     for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < 2 * M.n_slots;
          idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(128) slot_sources_kernel(GeneralMesh M, int64_
             v = b + (side == 0 ? j : M.fN[f] - j);
         } else {
             const int match = M.fmatch[M.fm_off[2 * f + side] + j];
-            v = match >= 0 ? b + match : -1;
+            v = match >= 0 ? b + match : -1 - (32 * (2 * f + side) + j);
         }
         src[idx] = v;
     }
@@ -406,36 +407,25 @@ namespace {
 // is computed with the operations, in the order, of the reference's separate
 // steps, so strict instantiations stay bit-identical to its CPU path.
 
-// Values of the three fields at face node i of side `side` of face f
-// (Mesh2D_t::project_to_faces, Mesh2D_t.cpp:3803-3893): a copy where the
-// element side matches the face, the plan's interpolation otherwise.
+// Values of the three fields at node j of face side fs2 = 2 f + side whose
+// element side is interpolated to the face (Mesh2D_t::project_to_faces,
+// Mesh2D_t.cpp:3803-3893): the barycentric sum with the plan's weights over
+// its denominator. code = 32 fs2 + j.
 template <bool S, typename R>
-__device__ __forceinline__ void face_value(const GeneralMesh& M, const R* __restrict__ tr, int64_t ft, int64_t f, int Nf, int side, int i, R v[3]) {
-    const int Ne = M.fsN[2 * f + side];
-    const R* ep = tr + M.fbase[2 * f + side];
-    if (M.fw_off[2 * f + side] < 0) {
-        const int src = side == 0 ? i : Nf - i;
-        v[0] = ep[src];
-        v[1] = ep[src + ft];
-        v[2] = ep[src + 2 * ft];
-        return;
-    }
-    const int match = M.fmatch[M.fm_off[2 * f + side] + i];
-    if (match >= 0) {
-        v[0] = ep[match];
-        v[1] = ep[match + ft];
-        v[2] = ep[match + 2 * ft];
-        return;
-    }
-    const double* tw = M.fw + M.fw_off[2 * f + side];
-    const double* tj = tw + i * (Ne + 1);
-    const R den = R(tw[(Nf + 1) * (Ne + 1) + i]);
+__device__ __forceinline__ void slot_interp(const GeneralMesh& M, const R* __restrict__ tr, int64_t ft, int64_t code, R v[3]) {
+    const int64_t fs2 = code / 32;
+    const int j = static_cast<int>(code - 32 * fs2);
+    const int Ne = M.fsN[fs2], Nf = M.fN[fs2 / 2];
+    const R* ep = tr + M.fbase[fs2];
+    const double* tw = M.fw + M.fw_off[fs2];
+    const double* tj = tw + j * (Ne + 1);
+    const R den = R(tw[(Nf + 1) * (Ne + 1) + j]);
     R pn = 0, un = 0, vn = 0;
-    for (int j = 0; j <= Ne; ++j) {
-        const R t = R(tj[j]);
-        pn = madd<S>(pn, t, ep[j]);
-        un = madd<S>(un, t, ep[j + ft]);
-        vn = madd<S>(vn, t, ep[j + 2 * ft]);
+    for (int i = 0; i <= Ne; ++i) {
+        const R t = R(tj[i]);
+        pn = madd<S>(pn, t, ep[i]);
+        un = madd<S>(un, t, ep[i + ft]);
+        vn = madd<S>(vn, t, ep[i + 2 * ft]);
     }
     v[0] = div<S>(pn, den);
     v[1] = div<S>(un, den);
@@ -459,8 +449,9 @@ struct FusedTile {
     static constexpr int kQ = 0;                   // [3][EPB][NN] q, then the new q
     static constexpr int kK = kQ + kVals;          // [3][EPB][NN] k of the stage's input
     static constexpr int kOff = kK + kVals;        // [EPB] element number, [EPB] field offset, [EPB] trace offset,
-                                                   // [4 EPB + 1] first slot of each side, then the end (int64)
-    static constexpr int kMode = kOff + 7 * EPB + 1;  // [4 EPB] side flux modes (ints)
+                                                   // [4 EPB + 1] first slot of each side, then the end,
+                                                   // [4 EPB + 1] first mortar entry of each side, then the end (int64)
+    static constexpr int kMode = kOff + 11 * EPB + 2;  // [4 EPB] side flux modes (ints)
     static constexpr int kDoubles = kMode + 2 * EPB;
     // R values past the doubles
     static constexpr int kF = 0;                   // [3][EPB][4][n] element side fluxes
@@ -484,6 +475,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     int64_t* eo2 = eid + EPB;                                    // their first value in a field block
     int64_t* eo1 = eo2 + EPB;                                    // their first side-trace value
     int64_t* sst = eo1 + EPB;                                    // first slot of each tile side, then the end
+    int64_t* sqs = sst + 4 * EPB + 1;                            // first mortar entry of each tile side, then the end
     int* smode = reinterpret_cast<int*>(smem + T::kMode);
     R* rs = reinterpret_cast<R*>(smem + T::kDoubles);
     R* gs = rs + T::kG;
@@ -524,6 +516,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     if (tid <= 4 * ne) {
         const int64_t ps = 4 * (grp.first + base) + tid;
         sst[tid] = M.pslot_start[ps];
+        sqs[tid] = M.pq_start[ps];
         if (tid < 4 * ne) smode[tid] = M.pside_mode[ps];
         if (tid < ne) {
             const int64_t el = grp.ids[base + tid];
@@ -557,7 +550,6 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
             else hi = mid;
         }
         const int slot = static_cast<int>(g - sst[lo]);
-        const int64_t d = M.slot_desc[g];
         const int64_t src0 = M.slot_src[2 * g], src1 = M.slot_src[2 * g + 1];
         const R nx = R(M.slot_normal[2 * g]), ny = R(M.slot_normal[2 * g + 1]);
         R L[3], Rv[3];
@@ -566,16 +558,14 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
             L[1] = tr[src0 + ft];
             L[2] = tr[src0 + 2 * ft];
         } else {
-            const int64_t fc = d / 32;
-            face_value<S, R>(M, tr, ft, fc, M.fN[fc], 0, static_cast<int>(d - 32 * fc), L);
+            slot_interp<S, R>(M, tr, ft, -1 - src0, L);
         }
         if (src1 >= 0) {
             Rv[0] = tr[src1];
             Rv[1] = tr[src1 + ft];
             Rv[2] = tr[src1 + 2 * ft];
         } else {
-            const int64_t fc = d / 32;
-            face_value<S, R>(M, tr, ft, fc, M.fN[fc], 1, static_cast<int>(d - 32 * fc), Rv);
+            slot_interp<S, R>(M, tr, ft, -1 - src1, Rv);
         }
         const R wL = add<S>(L[0], add<S>(mul<S>(L[1], nx), mul<S>(L[2], ny)));
         const R wR = sub<S>(Rv[0], add<S>(mul<S>(Rv[1], nx), mul<S>(Rv[2], ny)));
@@ -640,16 +630,13 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
         } else if (mode == 2) {
             for (int c = 0; c < 3; ++c) out[c] = mul<S>(-fl[c * FFS + (N - i)], sfv);
         } else if (mode == 3) {
-            const int64_t el = eid[ee];
-            const int64_t q0 = M.sface_start[4 * el + s], q1 = M.sface_start[4 * el + s + 1];
+            const int64_t q0 = sqs[ee * 4 + s], q1 = sqs[ee * 4 + s + 1];
             int slot0 = 0;
             for (int64_t qq = q0; qq < q1; ++qq) {
-                const int64_t ff = M.sface[qq];
-                const int Nf = M.fN[ff];
-                const int fsd = el == M.felem[2 * ff] ? 0 : 1;
-                const R scale = R(M.fscale[2 * ff + fsd]);
-                const double* W = M.sw + M.sw_off[qq] + i * (Nf + 1);
-                const int* match = M.smatch + M.sm_off[qq];
+                const int Nf = M.pq_N[qq];
+                const R scale = R(M.pq_scale[qq]);
+                const double* W = M.sw + M.pq_woff[qq] + i * (Nf + 1);
+                const int* match = M.smatch + M.pq_moff[qq];
                 for (int j = 0; j <= Nf; ++j) {
                     const int mt = match[j];
                     if (mt >= 0 && mt != i) continue;

@@ -68,15 +68,25 @@ struct GeneralMesh {
     // Face-node slots of the domain element sides in group-list order (side
     // s of list position p owns [pslot_start[4 p + s], pslot_start[4 p + s + 1])):
     // per slot the face and node (32 f + j), the face normal, and per face
-    // side the trace value the slot reads (first of the three fields; -1
-    // where the face side interpolates); per position side its flux mode (0
-    // no face, 1 one conforming face, 2 the same reversed, 3 mortar).
+    // side the trace value the slot reads (first of the three fields), or,
+    // where the face side interpolates, -1 - (32 (2 f + side) + j); per
+    // position side its flux mode (0 no face, 1 one conforming face, 2 the
+    // same reversed, 3 mortar).
     int64_t n_slots = 0;
     const int64_t* pslot_start = nullptr;  // [4 n_domain + 1]
     const int64_t* slot_desc = nullptr;    // [n_slots]
     const double* slot_normal = nullptr;   // [2 n_slots]
     const int64_t* slot_src = nullptr;     // [2 n_slots], filled by launch_general_weights
     const int* pside_mode = nullptr;       // [4 n_domain]
+    // Mortar sides (mode 3) in list order: side s of list position p owns
+    // entries [pq_start[4 p + s], pq_start[4 p + s + 1]), one per face, with
+    // the face order, the element's scaling factor on the face and the
+    // offsets of its weights and node matches in sw / smatch.
+    const int64_t* pq_start = nullptr;     // [4 n_domain + 1]
+    const int* pq_N = nullptr;
+    const double* pq_scale = nullptr;
+    const int64_t* pq_woff = nullptr;
+    const int64_t* pq_moff = nullptr;
     // Ghost side-0 gathers of the mirror and copy ghosts (ghost g - n_domain
     // owns entries [gq_start[.], gq_start[. + 1])): per entry the face and the
     // neighbour's face side, the neighbour side's trace base and order, and

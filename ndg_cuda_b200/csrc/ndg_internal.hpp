@@ -136,6 +136,13 @@ struct GeneralPlan {
     std::vector<double> slot_normal;
     std::vector<int32_t> pside_mode;
     int64_t n_slots = 0;
+    // Mortar sides (mode 3) in list order: side s of position p owns face
+    // entries [pq_start[4 p + s], pq_start[4 p + s + 1]), one per face in list
+    // order, each with the face order, the element's scaling factor on the
+    // face, and the offsets of its weights and node matches (sw_off, sm_off).
+    std::vector<int64_t> pq_start, pq_woff, pq_moff;
+    std::vector<int32_t> pq_N;
+    std::vector<double> pq_scale;
     // Ghost side-0 gathers (wall, symmetry and outflow ghosts): ghost g (from
     // n_domain) owns entries [gq_start[g - n_domain], gq_start[g - n_domain + 1]),
     // one per face of its side 0 in list order, each with the face and the
