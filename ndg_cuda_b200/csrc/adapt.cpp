@@ -287,6 +287,9 @@ GeneralPlan build_general_plan(const Topology& t) {
     for (const auto& grp : p.groups)
         for (int64_t e : grp.second) {
             const int Ne = t.elem_N[static_cast<size_t>(e)];
+            p.poff2.push_back(p.off2[static_cast<size_t>(e)]);
+            p.poff1.push_back(p.off1[static_cast<size_t>(e)]);
+            p.pcorners.insert(p.pcorners.end(), p.corners.begin() + 8 * e, p.corners.begin() + 8 * e + 8);
             for (int s = 0; s < 4; ++s) {
                 const size_t ps = static_cast<size_t>(4 * pos + s);
                 p.pslot_start[ps] = slot;

@@ -401,6 +401,9 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_pq_scale.upload(g.pq_scale, c->stream);
         c->g_pq_woff.upload(g.pq_woff, c->stream);
         c->g_pq_moff.upload(g.pq_moff, c->stream);
+        c->g_poff2.upload(g.poff2, c->stream);
+        c->g_poff1.upload(g.poff1, c->stream);
+        c->g_pcorners.upload(g.pcorners, c->stream);
         c->g_gq_start.upload(g.gq_start, c->stream);
         c->g_gq_face.upload(g.gq_face, c->stream);
         c->g_gq_fs.upload(g.gq_fs, c->stream);
@@ -483,6 +486,9 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.pq_scale = c->g_pq_scale.ptr;
         M.pq_woff = c->g_pq_woff.ptr;
         M.pq_moff = c->g_pq_moff.ptr;
+        M.poff2 = c->g_poff2.ptr;
+        M.poff1 = c->g_poff1.ptr;
+        M.pcorners = c->g_pcorners.ptr;
         M.gq_start = c->g_gq_start.ptr;
         M.gq_face = c->g_gq_face.ptr;
         M.gq_fs = c->g_gq_fs.ptr;

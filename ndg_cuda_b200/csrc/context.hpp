@@ -110,6 +110,8 @@ struct ndg_ctx {
     ndg::DeviceBuffer<int64_t> g_pq_start, g_pq_woff, g_pq_moff;        // mortar side entries, list order
     ndg::DeviceBuffer<int32_t> g_pq_N;
     ndg::DeviceBuffer<double> g_pq_scale;
+    ndg::DeviceBuffer<int64_t> g_poff2, g_poff1;                       // offsets and corners in list order
+    ndg::DeviceBuffer<double> g_pcorners;
     ndg::DeviceBuffer<int64_t> g_gq_start, g_gq_face, g_gq_base, g_gq_woff, g_gq_moff;  // ghost side-0 gathers
     ndg::DeviceBuffer<int32_t> g_gq_fs, g_gq_N;
     ndg::DeviceBuffer<double> g_gframe;

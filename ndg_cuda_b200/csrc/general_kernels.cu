@@ -448,10 +448,10 @@ struct FusedTile {
     // doubles
     static constexpr int kQ = 0;                   // [3][EPB][NN] q, then the new q
     static constexpr int kK = kQ + kVals;          // [3][EPB][NN] k of the stage's input
-    static constexpr int kOff = kK + kVals;        // [EPB] element number, [EPB] field offset, [EPB] trace offset,
+    static constexpr int kOff = kK + kVals;        // [EPB] field offset, [EPB] trace offset,
                                                    // [4 EPB + 1] first slot of each side, then the end,
                                                    // [4 EPB + 1] first mortar entry of each side, then the end (int64)
-    static constexpr int kMode = kOff + 11 * EPB + 2;  // [4 EPB] side flux modes (ints)
+    static constexpr int kMode = kOff + 10 * EPB + 2;  // [4 EPB] side flux modes (ints)
     static constexpr int kDoubles = kMode + 2 * EPB;
     // R values past the doubles
     static constexpr int kF = 0;                   // [3][EPB][4][n] element side fluxes
@@ -471,8 +471,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     extern __shared__ __align__(128) double smem[];
     double* qs = smem + T::kQ;
     double* ks = smem + T::kK;
-    int64_t* eid = reinterpret_cast<int64_t*>(smem + T::kOff);  // element numbers of the tile
-    int64_t* eo2 = eid + EPB;                                    // their first value in a field block
+    int64_t* eo2 = reinterpret_cast<int64_t*>(smem + T::kOff);  // first value of the tile's elements in a field block
     int64_t* eo1 = eo2 + EPB;                                    // their first side-trace value
     int64_t* sst = eo1 + EPB;                                    // first slot of each tile side, then the end
     int64_t* sqs = sst + 4 * EPB + 1;                            // first mortar entry of each tile side, then the end
@@ -511,18 +510,16 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     const R* lp = tab<R>(g_lagrange_right, gf_lagrange_right) + gvec(N);
     const double dt = a.step[1];
 
-    // The tile's sides: slot ranges and flux modes (plan arrays in list
-    // order), and per element its number and offsets.
+    // The tile's sides: slot ranges, mortar entries and flux modes, and per
+    // element its offsets (plan arrays in list order).
     if (tid <= 4 * ne) {
         const int64_t ps = 4 * (grp.first + base) + tid;
         sst[tid] = M.pslot_start[ps];
         sqs[tid] = M.pq_start[ps];
         if (tid < 4 * ne) smode[tid] = M.pside_mode[ps];
         if (tid < ne) {
-            const int64_t el = grp.ids[base + tid];
-            eid[tid] = el;
-            eo2[tid] = M.off2[el];
-            eo1[tid] = M.off1[el];
+            eo2[tid] = M.poff2[grp.first + base + tid];
+            eo1[tid] = M.poff1[grp.first + base + tid];
         }
     }
     __syncthreads();
@@ -581,11 +578,11 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     const int e = rr / n;
     const int m = rr - e * n;
     const bool active = f < 3 && e < ne;
-    const int64_t ge = active ? eid[e] : 0;
+    const int64_t pe = active ? grp.first + base + e : 0;
     // Corners in FP64: their differences are formed before rounding to R.
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
-        const double* c = M.corners + 8 * ge;
+        const double* c = M.pcorners + 8 * pe;
         x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
     }
     const MetricLine<S, R> x_xi(R(sub<S>(x1, x0)), R(sub<S>(x2, x3))), y_xi(R(sub<S>(y1, y0)), R(sub<S>(y2, y3)));

@@ -87,6 +87,9 @@ struct GeneralMesh {
     const double* pq_scale = nullptr;
     const int64_t* pq_woff = nullptr;
     const int64_t* pq_moff = nullptr;
+    const int64_t* poff2 = nullptr;        // [n_domain] off2 in list order
+    const int64_t* poff1 = nullptr;        // [n_domain] off1 in list order
+    const double* pcorners = nullptr;      // [8 n_domain] corners in list order
     // Ghost side-0 gathers of the mirror and copy ghosts (ghost g - n_domain
     // owns entries [gq_start[.], gq_start[. + 1])): per entry the face and the
     // neighbour's face side, the neighbour side's trace base and order, and

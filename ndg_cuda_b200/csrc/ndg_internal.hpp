@@ -143,6 +143,9 @@ struct GeneralPlan {
     std::vector<int64_t> pq_start, pq_woff, pq_moff;
     std::vector<int32_t> pq_N;
     std::vector<double> pq_scale;
+    // off2, off1 and corners of the domain elements in list order.
+    std::vector<int64_t> poff2, poff1;
+    std::vector<double> pcorners;
     // Ghost side-0 gathers (wall, symmetry and outflow ghosts): ghost g (from
     // n_domain) owns entries [gq_start[g - n_domain], gq_start[g - n_domain + 1]),
     // one per face of its side 0 in list order, each with the face and the
