@@ -279,7 +279,9 @@ GeneralPlan build_general_plan(const Topology& t) {
     p.gq_start[static_cast<size_t>(G)] = static_cast<int64_t>(p.gq_face.size());
 
     // Slots and side modes in group-list order, so that the sides of one
-    // tile of a group own one contiguous slot range.
+    // tile of a group own one contiguous slot range. A slot stores its face
+    // node j as 32 f + j, and the kernels decode it with the same base.
+    static_assert(kMaxOrder < 32, "face node index of a slot must fit below 32");
     p.pslot_start.assign(static_cast<size_t>(4 * K + 1), 0);
     p.pside_mode.assign(static_cast<size_t>(4 * K), 0);
     p.pq_start.assign(static_cast<size_t>(4 * K + 1), 0);
