@@ -459,9 +459,16 @@ struct FusedTile {
     static constexpr int kS = kJ + EPB * NN;       // [EPB][4] edge metric per side
     static constexpr bool kCopy = sizeof(R) != sizeof(double);  // the FP32 form keeps an FP32 copy of the q tile
     static constexpr int kQr = kS + EPB * 4;       // [3][EPB][NN] q in R (FP32 form only)
-    static constexpr int kG = kQr + (kCopy ? kVals : 0);  // [3][EPB][NN] G
-    static constexpr int kFF = kG + kVals;         // [3][EPB][4][slots] face fluxes at the sides' face nodes
-    static constexpr size_t bytes(int slots) { return sizeof(double) * kDoubles + sizeof(R) * (kFF + 3 * EPB * 4 * slots); }
+    // [3][EPB][NN] G and [3][EPB][4][slots] face fluxes at the sides' face
+    // nodes. In the FP32 form G takes the face fluxes' place once they are
+    // dead (after the element side fluxes), which fits more CTAs per SM; in
+    // FP64 that measured slower, so there G has a place of its own.
+    static constexpr int kG = kQr + (kCopy ? kVals : 0);
+    static constexpr int kFF = kCopy ? kG : kG + kVals;
+    static constexpr size_t bytes(int slots) {
+        const size_t ff = static_cast<size_t>(3 * EPB * 4) * static_cast<size_t>(slots);
+        return sizeof(double) * kDoubles + sizeof(R) * (kFF + (kCopy ? (ff > kVals ? ff : static_cast<size_t>(kVals)) : ff));
+    }
 };
 
 template <int N, bool S, typename R>
