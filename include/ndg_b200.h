@@ -47,8 +47,9 @@ typedef struct ndg_ctx ndg_ctx;
  *   CPU path on the same inputs.
  * NDG_FP32: traces, fluxes, metrics and the volume term in FP32 (traces
  *   stored in FP32); the solution, the RK register and the RK update stay
- *   FP64. Meshes of one order; after adaptation stepping returns
- *   NDG_ERR_UNSUPPORTED. */
+ *   FP64. Every mesh: uniform meshes use the fused FP32 stage kernel;
+ *   mixed-order and nonconforming meshes after adaptation run the mixed-order
+ *   kernels in FP32 (mortar interpolation and projection included). */
 typedef enum ndg_precision { NDG_FP64 = 0, NDG_FP64_STRICT = 1, NDG_FP32 = 2 } ndg_precision;
 
 /* Tables of NDG_t (include/entities/NDG_t.cuh:11-29). */
@@ -264,9 +265,12 @@ ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches);
  * the device-wide synchronisation of cudaMalloc/cudaFree. The partial minima go to one fixed 33 KB scratch array
  * per device, so n_elements is at most 4,194,304 (NDG_ERR_INVALID_ARG
  * beyond), and calls that overlap in time on one device race on that array:
- * serialise them. The first call on each device looks up the array's
- * address; make it before any stream capture begins. stream is a
- * cudaStream_t of the current device (NULL: the default stream). */
+ * serialise them. Each call looks up the array's address on the current
+ * device (nothing is cached between calls); the first call on a device also
+ * loads the library's kernels there, so make it before any stream capture
+ * begins on that device. Every call synchronises its stream before it
+ * returns. stream is a cudaStream_t of the current device (NULL: the default
+ * stream); a stream of another device is refused with NDG_ERR_INVALID_ARG. */
 ndg_status ndg_delta_t_from_device(const double* delta_xy_min, const int32_t* elem_N, int64_t n_elements,
                                    double cfl, void* stream, double* delta_t);
 

@@ -21,16 +21,19 @@
 //    calls on the same device that overlap in time (from different host
 //    threads, or on different streams) race on the array; callers must
 //    serialise them;
-//  * the first call on each device looks up the array's device address
-//    (which loads the library's kernels onto that device); make that first
-//    call before any stream capture begins.
+//  * every call looks up the array's device address for the current device
+//    (cudaGetSymbolAddress), so no address is kept between calls: after the
+//    device's context is torn down and rebuilt, the next call finds the
+//    array where the reloaded module put it. The first lookup on a device
+//    also loads the library's kernels there; make that first call before any
+//    stream capture begins on the device;
+//  * every call waits for its stream (cudaStreamSynchronize) before it
+//    returns, since the result is returned in host memory.
 #include "ndg_internal.hpp"
 
 #include <cuda_runtime.h>
 
-#include <atomic>
 #include <cstdint>
-#include <mutex>
 
 namespace {
 
@@ -43,7 +46,6 @@ constexpr int64_t kMaxElements = kElementsPerBlock * kMaxBlocks;
 // double 1 the result. The partial minima follow.
 constexpr int kHeaderDoubles = 32;
 constexpr int kScratchDoubles = kHeaderDoubles + kMaxBlocks;  // 33,024 bytes
-constexpr int kMaxDevices = 64;
 
 }  // namespace
 
@@ -53,9 +55,6 @@ static __device__ __align__(256) double g_delta_t_scratch[kScratchDoubles];
 
 namespace ndg {
 namespace {
-
-std::atomic<double*> g_scratch_ptr[kMaxDevices];
-std::mutex g_setup_mutex;
 
 __device__ __forceinline__ double warp_min(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -107,22 +106,13 @@ __global__ void __launch_bounds__(kThreads) delta_t_scratch_kernel(const double*
     }
 }
 
-// Once per device, with that device current: the device address of the
-// scratch array.
+// The device address of the scratch array on the current device, looked up
+// on every call: a cached address could outlive the context it came from.
 double* scratch_for_current_device() {
-    int device = -1;
-    cudaError_t err = cudaGetDevice(&device);
-    if (err != cudaSuccess) fail(NDG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(err));
-    if (device < 0 || device >= kMaxDevices) fail(NDG_ERR_UNSUPPORTED, "device ordinal above 63");
-    double* ptr = g_scratch_ptr[device].load(std::memory_order_acquire);
-    if (ptr) return ptr;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    ptr = g_scratch_ptr[device].load(std::memory_order_relaxed);
-    if (ptr) return ptr;
-    err = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_delta_t_scratch);
+    double* ptr = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_delta_t_scratch);
     if (err != cudaSuccess || !ptr)
         fail(NDG_ERR_CUDA, std::string("scratch address lookup: ") + cudaGetErrorString(err));
-    g_scratch_ptr[device].store(ptr, std::memory_order_release);
     return ptr;
 }
 
@@ -150,13 +140,20 @@ extern "C" ndg_status ndg_delta_t_from_device(const double* delta_xy_min, const 
         if (n_elements < 1) fail(NDG_ERR_INVALID_ARG, "n_elements must be at least 1");
         if (n_elements > kMaxElements)
             fail(NDG_ERR_INVALID_ARG, "n_elements exceeds the scratch limit of 4194304 elements per call");
-        double* scratch = scratch_for_current_device();
         int device = -1;
-        cudaGetDevice(&device);
+        cudaError_t err = cudaGetDevice(&device);
+        if (err != cudaSuccess) fail(NDG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(err));
         require_device_pointer(delta_xy_min, device, "delta_xy_min");
         require_device_pointer(elem_N, device, "elem_N");
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
-        cudaError_t err = cudaMemsetAsync(scratch, 0, kHeaderDoubles * sizeof(double), s);
+        if (s) {
+            int stream_device = -1;
+            err = cudaStreamGetDevice(s, &stream_device);
+            if (err != cudaSuccess) fail(NDG_ERR_INVALID_ARG, std::string("stream: ") + cudaGetErrorString(err));
+            if (stream_device != device) fail(NDG_ERR_INVALID_ARG, "stream belongs to another device than the current one");
+        }
+        double* scratch = scratch_for_current_device();
+        err = cudaMemsetAsync(scratch, 0, kHeaderDoubles * sizeof(double), s);
         if (err != cudaSuccess) fail(NDG_ERR_CUDA, std::string("scratch clear: ") + cudaGetErrorString(err));
         const unsigned blocks = static_cast<unsigned>((n_elements + kElementsPerBlock - 1) / kElementsPerBlock);
         delta_t_scratch_kernel<<<blocks, kThreads, 0, s>>>(delta_xy_min, elem_N, n_elements, cfl, scratch);

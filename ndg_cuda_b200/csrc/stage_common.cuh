@@ -112,9 +112,9 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Waits for phase 0 of an mbarrier, giving up after `limit_ns`: the error
-// word is then set and false returned so that the CTA stops.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned* error, uint64_t limit_ns) {
+// Polls phase 0 of an mbarrier until it completes or `limit_ns` has passed;
+// true when it completed.
+__device__ __forceinline__ bool mbar_poll(uint64_t* bar, uint64_t limit_ns) {
     const uint32_t a = smem_addr(bar);
     uint32_t done = 0;
     const uint64_t t0 = global_ns();
@@ -125,11 +125,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned* error, uint64
             : "r"(a)
             : "memory");
         if (done) return true;
-        if (global_ns() - t0 > limit_ns) {
-            atomicOr(error, 1u);
-            return false;
-        }
+        if (global_ns() - t0 > limit_ns) return false;
     }
+}
+
+// Waits for phase 0 of an mbarrier with a CTA-wide decision; every thread of
+// the CTA calls it (it is also a __syncthreads). Each thread polls with the
+// time limit, then the CTA gives up together if any thread timed out: the
+// error word is set, thread 0 waits once more (bounded) so that a copy that
+// was about to land is not left writing into an exited CTA, and false is
+// returned to every thread so that the CTA stops as one.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned* error, uint64_t limit_ns) {
+    const bool ok = mbar_poll(bar, limit_ns);
+    if (!__syncthreads_or(!ok)) return true;
+    if (threadIdx.x == 0) {
+        atomicOr(error, 1u);
+        mbar_poll(bar, limit_ns);
+    }
+    __syncthreads();
+    return false;
 }
 
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s

@@ -443,8 +443,7 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
             js[e * ES + m * P + j] = __frcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
         }
     }
-    __syncthreads();
-    if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;
+    if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;  // also the barrier for zeros, far traces, edge metrics and J
     // FP32 copy of the tile in the padded layout: warps take (field,
     // element) blocks, lanes their nodes.
     const int warp = tid >> 5, lane = tid & 31;

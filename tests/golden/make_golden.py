@@ -1,6 +1,7 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference.
 
-Run in a container that has the reference sources (default /root/reference)
+Run where the reference sources are present (--reference, or the environment
+variable NDG_REFERENCE_DIR)
 after `make -C oracle`:
 
     python tests/golden/make_golden.py [--reference /path/to/NDG_cuda]
@@ -52,8 +53,11 @@ def legendre_literals(reference: str) -> dict:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("NDG_REFERENCE_DIR"),
+                    help="root of the reference checkout (default: $NDG_REFERENCE_DIR)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("the reference checkout is needed: --reference or NDG_REFERENCE_DIR")
     with open(os.path.join(HERE, "legendre_n16.json"), "w") as f:
         json.dump(legendre_literals(args.reference), f, indent=1)
     if not pyoracle.ref_available():

@@ -9,6 +9,10 @@ left behind.
 from __future__ import annotations
 
 import ctypes as C
+import os
+import subprocess
+import sys
+import textwrap
 
 import numpy as np
 import pytest
@@ -69,3 +73,78 @@ def test_largest_size_and_rejection():
     out = C.c_double()
     st = ndg.lib().ndg_delta_t_from_device(host.ctypes.data, elem_N.data_ptr(), 16, cfl, None, C.byref(out))
     assert st == 1 and b"not device-accessible" in ndg.lib().ndg_last_error()
+
+
+def test_allocates_no_device_memory():
+    """The entry point's defining property: free device memory (cudaMemGetInfo,
+    which also sees allocations outside torch's allocator) is the same before
+    and after a batch of calls, once the first call has loaded the kernels."""
+    mesh = ndg.Mesh2D_t(meshgen.uniform_zone(64, x_periodic=True, y_periodic=True, jitter=0.1, seed=2), 5, cfl=0.4)
+    want = ndg.Solver2D_t.get_delta_t(mesh)
+    el = mesh.elements()
+    K = mesh.n_elements_
+    dxy = torch.tensor(el["delta_xy_min"][:K], dtype=torch.float64, device="cuda")
+    elem_N = torch.tensor(el["N"][:K], dtype=torch.int32, device="cuda")
+    mesh.close()
+    st, got = _call(dxy, elem_N, K, 0.4)  # warm-up: module load
+    assert st == 0 and got == want
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(50):
+        st, got = _call(dxy, elem_N, K, 0.4)
+        assert st == 0 and got == want
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+_RESET_SCRIPT = textwrap.dedent("""
+    import ctypes as C, glob, os, sys
+    import numpy as np
+    sys.path.insert(0, os.environ["NDG_ROOT"])
+    import ndg_cuda_b200 as ndg
+    lib = ndg.lib()
+    cands = sorted(glob.glob("/usr/local/cuda/lib64/libcudart.so*"))
+    rt = C.CDLL(cands[0])
+    rt.cudaMalloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+    rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    rt.cudaFree.argtypes = [C.c_void_p]
+    K = 3000
+    rng = np.random.default_rng(5)
+    dxy = rng.uniform(1e-3, 2e-2, K)
+    N = rng.integers(1, 13, K).astype(np.int32)
+    want = float((0.5 * dxy / (N.astype(np.float64) * N)).min())
+
+    def one_call():
+        assert rt.cudaSetDevice(0) == 0
+        a, b = C.c_void_p(), C.c_void_p()
+        assert rt.cudaMalloc(C.byref(a), K * 8) == 0 and rt.cudaMalloc(C.byref(b), K * 4) == 0
+        assert rt.cudaMemcpy(a, dxy.ctypes.data, K * 8, 1) == 0 and rt.cudaMemcpy(b, N.ctypes.data, K * 4, 1) == 0
+        out = C.c_double(-1.0)
+        st = lib.ndg_delta_t_from_device(a, b, K, 0.5, None, C.byref(out))
+        msg = lib.ndg_last_error()
+        rt.cudaFree(a)
+        rt.cudaFree(b)
+        return st, out.value, msg
+
+    st, got, msg = one_call()
+    assert st == 0 and got == want, (st, got, msg)
+    assert rt.cudaDeviceReset() == 0
+    st, got, msg = one_call()
+    print("after-reset", st, got == want, msg)
+""")
+
+
+def test_call_after_device_reset():
+    """A call, a reset of the device's primary context by another CUDA runtime
+    in the same process, and a second call: the second call must not reuse a
+    device address from the first context. It either returns the right step
+    (the library's runtime rebuilt its context) or reports a CUDA error
+    status; it never launches on a stale address. Runs in a fresh process so
+    the reset touches no other test's state."""
+    env = dict(os.environ, NDG_ROOT=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    res = subprocess.run([sys.executable, "-c", _RESET_SCRIPT], env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    line = [ln for ln in res.stdout.splitlines() if ln.startswith("after-reset")][-1].split(" ", 3)
+    st, ok = int(line[1]), line[2] == "True"
+    assert (st == 0 and ok) or st == 3, line  # NDG_OK with the right step, or NDG_ERR_CUDA
