@@ -89,21 +89,27 @@ struct Work {
 
 namespace {
 
-// Index of a refined face's new node, or of the second half of a refined face:
-// base + number of refined faces before face f.
-int64_t refined_before(const std::vector<Face>& fa, int64_t f) {
-    int64_t n = 0;
-    for (int64_t j = 0; j < f; ++j) n += fa[static_cast<size_t>(j)].refine ? 1 : 0;
-    return n;
+// Exclusive prefix count of a flag: out[i] = number of set flags before i
+// (out has one more entry, the total). The reference numbers new faces,
+// nodes and elements by these counts (its serial loops over j < i,
+// src/meshes/Mesh2D_t.cpp:5204-5209 and the split_* functions); one scan
+// gives every count at once.
+template <typename Flag>
+std::vector<int64_t> exclusive_count(size_t n, Flag flag) {
+    std::vector<int64_t> out(n + 1, 0);
+    for (size_t i = 0; i < n; ++i) out[i + 1] = out[i] + (flag(i) ? 1 : 0);
+    return out;
 }
 
 // A side's face list with every refined face followed by its second half
-// (the move and p-refine branches of hp_adapt, :5576-5605 and :5617-5646).
-std::vector<int64_t> expand_side(const std::vector<Face>& fa, const std::vector<int64_t>& side, int64_t second_half_base) {
+// (the move and p-refine branches of hp_adapt, :5576-5605 and :5617-5646);
+// refined_before[f] is the number of refined faces before face f.
+std::vector<int64_t> expand_side(const std::vector<Face>& fa, const std::vector<int64_t>& refined_before,
+                                 const std::vector<int64_t>& side, int64_t second_half_base) {
     std::vector<int64_t> out;
     for (int64_t f : side) {
         out.push_back(f);
-        if (fa[static_cast<size_t>(f)].refine) out.push_back(second_half_base + refined_before(fa, f));
+        if (fa[static_cast<size_t>(f)].refine) out.push_back(second_half_base + refined_before[static_cast<size_t>(f)]);
     }
     return out;
 }
@@ -217,6 +223,13 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
         }
     }
 
+    // Index of a refined face's new node, or of the second half of a refined
+    // face: base + number of refined faces before it.
+    const std::vector<int64_t> refined_prefix = exclusive_count(w.fa.size(), [&](size_t f) { return w.fa[f].refine; });
+    auto refined_before = [&](int64_t f) { return refined_prefix[static_cast<size_t>(f)]; };
+    // Splitting domain elements before element j: element j moves to j + 3 * that.
+    const std::vector<int64_t> split_prefix = exclusive_count(static_cast<size_t>(w.K), [&](size_t e) { return w.would_h(w.el[e]); });
+
     // Sizes of the new arrays (:2091-2151).
     std::array<int64_t, 4> n_split_b{};
     for (int b = 0; b < 4; ++b)
@@ -253,7 +266,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                     const int64_t f = x.faces[static_cast<size_t>(s)][0];
                     const Face& fc = w.fa[static_cast<size_t>(f)];
                     side_xy[static_cast<size_t>(s)] = (w.node(fc.nodes[0]) + w.node(fc.nodes[1])) / 2;
-                    side_node[static_cast<size_t>(s)] = split_node_base + refined_before(w.fa, f);
+                    side_node[static_cast<size_t>(s)] = split_node_base + refined_before(f);
                 } else {
                     const V2 mid = (w.node(x.nodes[static_cast<size_t>(s)]) + w.node(x.nodes[static_cast<size_t>((s + 1) % 4)])) / 2;
                     for (int64_t f : x.faces[static_cast<size_t>(s)]) {
@@ -293,7 +306,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                     if (x.add[static_cast<size_t>(ps)]) {
                         const int64_t f = x.faces[static_cast<size_t>(ps)][0];
                         const bool forward = i == w.fa[static_cast<size_t>(f)].elems[0];
-                        const int64_t second = split_face_base + refined_before(w.fa, f);
+                        const int64_t second = split_face_base + refined_before(f);
                         out = {(half == 0) == forward ? f : second};
                         continue;
                     }
@@ -310,7 +323,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                             const double C = dot(w.node(fc.nodes[0]) - A, AB) * inv, D = dot(fm - A, AB) * inv,
                                          E = dot(w.node(fc.nodes[1]) - A, AB) * inv;
                             if (on_side(C, D)) out.push_back(f);
-                            if (on_side(D, E)) out.push_back(split_face_base + refined_before(w.fa, f));
+                            if (on_side(D, E)) out.push_back(split_face_base + refined_before(f));
                         } else {
                             const double C = dot(w.node(fc.nodes[0]) - A, AB) * inv, D = dot(w.node(fc.nodes[1]) - A, AB) * inv;
                             if (on_side(C, D)) out.push_back(f);
@@ -353,7 +366,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                 y.refine = false;
                 src.kind = 1;
             }
-            for (int s = 0; s < 4; ++s) y.faces[static_cast<size_t>(s)] = expand_side(w.fa, x.faces[static_cast<size_t>(s)], split_face_base);
+            for (int s = 0; s < 4; ++s) y.faces[static_cast<size_t>(s)] = expand_side(w.fa, refined_prefix, x.faces[static_cast<size_t>(s)], split_face_base);
             ne[static_cast<size_t>(at)] = std::move(y);
         }
     }
@@ -375,8 +388,8 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
             const bool splits = dst.faces[0].size() == 1 && w.fa[static_cast<size_t>(dst.faces[0][0])].refine;
             if (splits) {
                 const int64_t f = dst.faces[0][0];
-                const int64_t mid_node = split_node_base + refined_before(w.fa, f);
-                const int64_t second = split_face_base + refined_before(w.fa, f);
+                const int64_t mid_node = split_node_base + refined_before(f);
+                const int64_t second = split_face_base + refined_before(f);
                 out[static_cast<size_t>(nb)] = at;
                 out[static_cast<size_t>(nb + 1)] = at + 1;
                 for (int h = 0; h < 2; ++h) {
@@ -424,8 +437,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
             const Elem& src = w.el[static_cast<size_t>(si)];
             Elem& dst = w.el[static_cast<size_t>(di)];
             const int side = static_cast<int>(w.if_origin_side[ii]);
-            int64_t src_new = si;
-            for (int64_t j = 0; j < si; ++j) src_new += 3 * (w.would_h(w.el[static_cast<size_t>(j)]) ? 1 : 0);
+            const int64_t src_new = si + 3 * split_prefix[static_cast<size_t>(si)];
             const int64_t nii = static_cast<int64_t>(ii) + shift;
             const int64_t at = offset + nii;
             new_index[static_cast<size_t>(di)] = at;
@@ -442,7 +454,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                 if (dst.add[0]) {
                     const int64_t f = dst.faces[0][0];
                     mid = (w.node(w.fa[static_cast<size_t>(f)].nodes[0]) + w.node(w.fa[static_cast<size_t>(f)].nodes[1])) / 2;
-                    mid_node = split_node_base + refined_before(w.fa, f);
+                    mid_node = split_node_base + refined_before(f);
                 } else {
                     const V2 m2 = (w.node(dst.nodes[0]) + w.node(dst.nodes[1])) / 2;
                     for (int64_t f : dst.faces[0]) {
@@ -471,7 +483,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                 }
                 if (dst.add[0]) {
                     const int64_t f = dst.faces[0][0];
-                    ne[static_cast<size_t>(at)].faces[0] = {split_face_base + refined_before(w.fa, f)};
+                    ne[static_cast<size_t>(at)].faces[0] = {split_face_base + refined_before(f)};
                     ne[static_cast<size_t>(at + 1)].faces[0] = {f};
                 } else {
                     const V2 n0 = w.node(dst.nodes[0]), n1 = w.node(dst.nodes[1]);
@@ -483,7 +495,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                     for (int64_t f : dst.faces[0]) {
                         const Face& fc = w.fa[static_cast<size_t>(f)];
                         if (fc.refine) {
-                            const int64_t second = split_face_base + refined_before(w.fa, f);
+                            const int64_t second = split_face_base + refined_before(f);
                             const V2 fm = (w.node(fc.nodes[0]) + w.node(fc.nodes[1])) / 2;
                             double C[2], D[2], E[2];
                             for (int h = 0; h < 2; ++h) {
@@ -517,7 +529,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                     dst.sf_zero = false;
                 }
                 Elem y = dst;
-                y.faces[0] = expand_side(w.fa, dst.faces[0], split_face_base);
+                y.faces[0] = expand_side(w.fa, refined_prefix, dst.faces[0], split_face_base);
                 ne[static_cast<size_t>(at)] = std::move(y);
             }
         }
@@ -556,8 +568,8 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
         const int face_N = std::max(L.N + 2 * (w.would_p(L) ? 1 : 0), R.N + 2 * (w.would_p(R) ? 1 : 0));
         const V2 p0 = w.node(fc.nodes[0]), p2 = w.node(fc.nodes[1]);
         if (fc.refine) {
-            const int64_t mid_node = split_node_base + refined_before(w.fa, fi);
-            const int64_t second = split_face_base + refined_before(w.fa, fi);
+            const int64_t mid_node = split_node_base + refined_before(fi);
+            const int64_t second = split_face_base + refined_before(fi);
             const V2 p1 = (p0 + p2) / 2;
             w.nd[static_cast<size_t>(mid_node)] = p1;
             std::array<int64_t, 2> e1{Ln, Rn}, e2{Ln, Rn};
