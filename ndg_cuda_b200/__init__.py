@@ -20,6 +20,9 @@ __all__ = ["NdgError", "lib", "NDG_t", "Mesh2D_t", "Solver2D_t", "Adjoint2D_t", 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libndg_b200.so")
 
 FP64, FP64_STRICT, FP32 = 0, 1, 2
+# Tile codes at or above TENSOR_TILE select the stage kernel whose contraction
+# passes run on the tensor cores, with (code - TENSOR_TILE) elements per CTA.
+TENSOR_TILE = 100
 _STATUS = {0: "OK", 1: "INVALID_ARG", 2: "MESH", 3: "CUDA", 4: "NONFINITE", 5: "OOM", 6: "TIMEOUT", 7: "UNSUPPORTED"}
 FIELDS = {"p": 0, "u": 1, "v": 2, "G_p": 3, "G_u": 4, "G_v": 5, "k_p": 6, "k_u": 7, "k_v": 8}
 TABLES = ["nodes", "weights", "barycentric_weights", "lagrange_interpolant_left", "lagrange_interpolant_right",

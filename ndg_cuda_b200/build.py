@@ -22,7 +22,7 @@ COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contra
 CUDA_FLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr", "-Xptxas", "-v"] if os.environ.get("NDG_PTXAS_VERBOSE") else ARCH + ["-lineinfo", "--expt-relaxed-constexpr"]
 
 SOURCES = ["tables.cpp", "topology.cpp", "adapt.cpp", "adapt_h.cpp", "stage_kernels.cu", "general_kernels.cu", "estimator.cu", "context.cu",
-           "adjoint_kernels.cu", "adjoint_host.cu", "stage_variants_fp64.cu", "stage_variants_fp32.cu",
+           "adjoint_kernels.cu", "adjoint_host.cu", "stage_variants_fp64.cu", "stage_variants_fp32.cu", "stage_variants_tc64.cu", "stage_variants_tc32.cu",
            "delta_t_scratch.cu", "output.cu", "output_host.cu", "writer.cpp"]
 
 

@@ -4,6 +4,7 @@
     python -m ndg_cuda_b200.cases batched --res 64 --order 6 --instances 64 --steps 3 [--fp32]
     python -m ndg_cuda_b200.cases adjoint --res 96 --order 7 --steps 20 --interval 10 [--fp32]
     python -m ndg_cuda_b200.cases mixed   --res 128 --order 4 --rounds 3 --steps 2
+    python -m ndg_cuda_b200.cases tiles   --res 256 --order 8 [--fp32]
 
 `stage`: the reference plane wave on a periodic res x res mesh (RK3 steps).
 `batched`: independent radial pulses on one walled mesh, one launch per stage.
@@ -12,6 +13,10 @@ adjoint sweep) on a walled mesh with a per-element wave speed.
 `mixed`: a jittered periodic mesh whose orders are raised by 2 on a seeded
 40% of the elements in each of `rounds` p-adaptations (orders 4 to 10 for
 order 4 and 3 rounds), then steps on the mixed-order path.
+`tiles`: the plane wave on a periodic res x res mesh; every candidate tile
+of the stage kernel (SIMT and tensor-core codes) and the default, timed by
+CUDA events (best of the second and third RK stages, two rounds, 20 launches
+each); one line per tile in µs per launch.
 Inputs are the seeded synthetic ones of ndg_cuda_b200.workloads.
 """
 from __future__ import annotations
@@ -30,7 +35,7 @@ def _zone(res: int, **kw) -> dict:
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("case", choices=["stage", "batched", "adjoint", "mixed"])
+    ap.add_argument("case", choices=["stage", "batched", "adjoint", "mixed", "tiles"])
     ap.add_argument("--res", type=int, default=64)
     ap.add_argument("--order", type=int, default=6)
     ap.add_argument("--steps", type=int, default=3)
@@ -59,6 +64,19 @@ def main(argv=None) -> None:
         mesh.set_field("p", p0)
         Solver2D_t.run(mesh, args.steps)
         print("p[0] =", mesh.get_field("p")[0])
+    elif args.case == "tiles":
+        mesh = Mesh2D_t(_zone(args.res, x_periodic=True, y_periodic=True), args.order, precision=prec)
+        mesh.initial_conditions()
+        cand, _ = mesh.tile_candidates()
+        best: dict[int, float] = {}
+        for _ in range(2):
+            for t in [0] + cand:
+                mesh.set_tile(t)
+                Solver2D_t.run(mesh, 1)
+                ms = min(mesh.time_stage(1, 20), mesh.time_stage(2, 20))
+                best[t] = min(best.get(t, ms), ms)
+        for t, ms in best.items():
+            print(f"tile {t:4d}: {1e3 * ms:8.1f} us per launch")
     elif args.case == "mixed":
         zone = _zone(args.res, x_periodic=True, y_periodic=True, jitter=0.1, seed=1)
         mesh = Mesh2D_t(zone, args.order, maximum_N=args.order + 2 * args.rounds, precision=prec)

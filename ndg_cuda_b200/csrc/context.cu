@@ -77,6 +77,8 @@ dev::StageArgs stage_args(ndg_ctx* c, int m, int in) {
     a.field_stride = c->Kp;
     a.n_instances = c->n_instances;
     a.error = c->error.ptr;
+    a.tc64 = c->tc64.ptr;
+    a.tc32 = c->tc32.ptr;
     return a;
 }
 
@@ -348,6 +350,8 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->gscale.upload(plan.gscale, c->stream);
         c->inflow.upload(plan.inflow_xy, c->stream);
         c->link.upload(plan.link, c->stream);
+        c->tc64.upload(dev::tc_lane_table_fp64(c->N), c->stream);
+        c->tc32.upload(dev::tc_lane_table_fp32(c->N), c->stream);
         check_cuda(dev::prepare_kernels(c->N, false), "kernel attributes");
         check_cuda(dev::prepare_kernels(c->N, true), "kernel attributes");
         c->groups.clear();

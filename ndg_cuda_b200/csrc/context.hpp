@@ -82,6 +82,8 @@ struct ndg_ctx {
 
     ndg::DeviceBuffer<double> q, k, G, tr[2], corners, normal, gscale, inflow, dxy, step, scratch;
     ndg::DeviceBuffer<float> tr32[2];  // traces of the FP32 form
+    ndg::DeviceBuffer<double> tc64;    // per-lane tables of the tensor-core stage passes (order N)
+    ndg::DeviceBuffer<float> tc32;
     ndg::DeviceBuffer<int32_t> link, elem_N;
     ndg::DeviceBuffer<unsigned> error;
     ndg::DeviceBuffer<double> p_error, p_sigma;

@@ -156,6 +156,54 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
+// Warp-level tensor-core products (PTX ISA: mma.sync). Fragments, with
+// g = lane / 4 and t = lane % 4:
+//   f64 m16n8k4:  A rows g, g + 8 at column t (a0, a1); B row t, column g
+//                 (b0); C rows g, g + 8 at columns 2t, 2t + 1 (c0 c1, c2 c3).
+//   tf32 m16n8k8: A (g, t), (g + 8, t), (g, t + 4), (g + 8, t + 4); B (t, g),
+//                 (t + 4, g); C as for f64.
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+    asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, {%0, %1, %2, %3};"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+__device__ __forceinline__ void tf32mma_16x8x8(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// Round to TF32 (nearest, ties away from zero), kept in a 32-bit register.
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// Per-lane tables of the tensor-core contraction passes of order N, built
+// on the host (tc_lane_table_fp64 / _fp32) and read once per CTA, coalesced:
+// lane-dependent entries would otherwise be divergent constant loads.
+//   FP64 (m16n8k4): B[s][u][lane] = Dhat[8u + g][4s + t] (0 outside n x n);
+//     LPW[u][h][lane], LMW[u][h][lane] = l(+1)[i] / w[i], l(-1)[i] / w[i] at
+//     i = 8u + 2t + h (0 for i >= n); XK[s][lane] = node 4s + t (0 beyond).
+//   FP32 (3xTF32 m16n8k8): B[s][u][lane][4] = TF32 high and low parts of
+//     Dhat[8u + g][8s + t] and Dhat[8u + g][8s + t + 4]; LPW, LMW as FP64's
+//     in float; XK[s][lane][2] = nodes 8s + t and 8s + t + 4.
+template <int N>
+struct TcTable64 {
+    static constexpr int n = N + 1;
+    static constexpr int KS = (n + 3) / 4;  // k-steps of 4
+    static constexpr int NT = (n + 7) / 8;  // n-tiles of 8 output nodes
+    static constexpr int kB = 0, kLPW = KS * NT * 32, kLMW = kLPW + NT * 64, kXK = kLMW + NT * 64, kSize = kXK + KS * 32;
+};
+template <int N>
+struct TcTable32 {
+    static constexpr int n = N + 1;
+    static constexpr int KS = (n + 7) / 8;  // k-steps of 8
+    static constexpr int NT = (n + 7) / 8;
+    static constexpr int kB = 0, kLPW = KS * NT * 128, kLMW = kLPW + NT * 64, kXK = kLMW + NT * 64, kSize = kXK + KS * 64;
+};
+
+// ---------------------------------------------------------------------------
 // Shared-memory placement of the uniform-order stage tiles without bank
 // conflicts.
 //

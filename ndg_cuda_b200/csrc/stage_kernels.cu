@@ -48,6 +48,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 namespace ndg {
@@ -217,6 +218,78 @@ void host_coefficients(int N, double* dhat, double* xn, double* lm, double* lp, 
         iw[i] = h_inv_weights[static_cast<size_t>(vec_offset(N) + i)];
     }
     for (int i = 0; i < n * n; ++i) dhat[i] = h_dhat[static_cast<size_t>(mat_offset(N) + i)];
+}
+
+std::vector<double> tc_lane_table_fp64(int N) {
+    const int n = N + 1, KS = (n + 3) / 4, NT = (n + 7) / 8;
+    const int kLPW = KS * NT * 32, kLMW = kLPW + NT * 64, kXK = kLMW + NT * 64, kSize = kXK + KS * 32;
+    std::vector<double> dh(static_cast<size_t>(n * n)), xn(n), lm(n), lp(n), w(n), iw(n);
+    host_coefficients(N, dh.data(), xn.data(), lm.data(), lp.data(), w.data(), iw.data());
+    std::vector<double> t(static_cast<size_t>(kSize), 0.0);
+    for (int lane = 0; lane < 32; ++lane) {
+        const int g = lane >> 2, tt = lane & 3;
+        for (int s = 0; s < KS; ++s)
+            for (int u = 0; u < NT; ++u) {
+                const int i = 8 * u + g, k = 4 * s + tt;
+                t[static_cast<size_t>((s * NT + u) * 32 + lane)] = (i < n && k < n) ? dh[static_cast<size_t>(i * n + k)] : 0.0;
+            }
+        for (int u = 0; u < NT; ++u)
+            for (int h = 0; h < 2; ++h) {
+                const int i = 8 * u + 2 * tt + h;
+                t[static_cast<size_t>(kLPW + (u * 2 + h) * 32 + lane)] = i < n ? lp[static_cast<size_t>(i)] * iw[static_cast<size_t>(i)] : 0.0;
+                t[static_cast<size_t>(kLMW + (u * 2 + h) * 32 + lane)] = i < n ? lm[static_cast<size_t>(i)] * iw[static_cast<size_t>(i)] : 0.0;
+            }
+        for (int s = 0; s < KS; ++s) {
+            const int k = 4 * s + tt;
+            t[static_cast<size_t>(kXK + s * 32 + lane)] = k < n ? xn[static_cast<size_t>(k)] : 0.0;
+        }
+    }
+    return t;
+}
+
+namespace {
+// TF32 rounding of the host (nearest, ties away from zero on the magnitude:
+// cvt.rna.tf32.f32), as a float whose low 13 mantissa bits are zero.
+float tf32_round(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, sizeof b);
+    if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0x1000u) & 0xffffe000u;
+    float r;
+    std::memcpy(&r, &b, sizeof r);
+    return r;
+}
+}  // namespace
+
+std::vector<float> tc_lane_table_fp32(int N) {
+    const int n = N + 1, KS = (n + 7) / 8, NT = (n + 7) / 8;
+    const int kLPW = KS * NT * 128, kLMW = kLPW + NT * 64, kXK = kLMW + NT * 64, kSize = kXK + KS * 64;
+    std::vector<double> dh(static_cast<size_t>(n * n)), xn(n), lm(n), lp(n), w(n), iw(n);
+    host_coefficients(N, dh.data(), xn.data(), lm.data(), lp.data(), w.data(), iw.data());
+    std::vector<float> t(static_cast<size_t>(kSize), 0.0f);
+    for (int lane = 0; lane < 32; ++lane) {
+        const int g = lane >> 2, tt = lane & 3;
+        for (int s = 0; s < KS; ++s)
+            for (int u = 0; u < NT; ++u)
+                for (int r = 0; r < 2; ++r) {
+                    const int i = 8 * u + g, k = 8 * s + tt + 4 * r;
+                    const float v = (i < n && k < n) ? static_cast<float>(dh[static_cast<size_t>(i * n + k)]) : 0.0f;
+                    const float hi = tf32_round(v), lo = tf32_round(v - hi);
+                    t[static_cast<size_t>(((s * NT + u) * 32 + lane) * 4 + r)] = hi;
+                    t[static_cast<size_t>(((s * NT + u) * 32 + lane) * 4 + 2 + r)] = lo;
+                }
+        for (int u = 0; u < NT; ++u)
+            for (int h = 0; h < 2; ++h) {
+                const int i = 8 * u + 2 * tt + h;
+                t[static_cast<size_t>(kLPW + (u * 2 + h) * 32 + lane)] = i < n ? static_cast<float>(lp[static_cast<size_t>(i)] * iw[static_cast<size_t>(i)]) : 0.0f;
+                t[static_cast<size_t>(kLMW + (u * 2 + h) * 32 + lane)] = i < n ? static_cast<float>(lm[static_cast<size_t>(i)] * iw[static_cast<size_t>(i)]) : 0.0f;
+            }
+        for (int s = 0; s < KS; ++s)
+            for (int r = 0; r < 2; ++r) {
+                const int k = 8 * s + tt + 4 * r;
+                t[static_cast<size_t>(kXK + (s * 32 + lane) * 2 + r)] = k < n ? static_cast<float>(xn[static_cast<size_t>(k)]) : 0.0f;
+            }
+    }
+    return t;
 }
 
 // ---------------------------------------------------------------------------

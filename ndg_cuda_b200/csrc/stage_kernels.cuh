@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace ndg {
 namespace dev {
 
@@ -28,6 +30,8 @@ struct StageArgs {
     const double4* inflow;
     const double* step;  // {time, dt, dt_mesh, t_end}
     unsigned* error;     // set when a bounded wait gives up
+    const double* tc64;  // per-lane tables of the tensor-core passes (TcTable64 / TcTable32 of the order)
+    const float* tc32;
     double rk_a, rk_b, rk_g;
     int first;
     int64_t n_elements;
@@ -69,6 +73,12 @@ cudaError_t prepare_stage_variant_fp64(int N, int epb);
 cudaError_t prepare_stage_variant_fp32(int N, int epb);
 cudaError_t launch_stage_variant_fp64(int N, int epb, const StageArgs& a, cudaStream_t stream);
 cudaError_t launch_stage_variant_fp32(int N, int epb, const StageArgs& a, cudaStream_t stream);
+// Tile codes at or above kTensorTile select the tensor-core contraction
+// variant with (code - kTensorTile) elements per CTA.
+constexpr int kTensorTile = 100;
+// Per-lane tables of the tensor-core passes of order N (stage_common.cuh).
+std::vector<double> tc_lane_table_fp64(int N);
+std::vector<float> tc_lane_table_fp32(int N);
 
 }  // namespace dev
 }  // namespace ndg

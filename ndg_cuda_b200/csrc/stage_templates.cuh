@@ -16,8 +16,27 @@
 namespace ndg {
 namespace dev {
 
-template <int N, bool S, int E>
+// Tensor-core form of the two contraction passes (TC = true; FP64 with DMMA
+// m16n8k4, the FP32 form with 3xTF32 m16n8k8). The tile's 3 EPB (N+1) flux
+// lines, in the threads' (field, line, element) order with the element
+// fastest, are the M rows of 16-row MMA tiles; the node index along the line
+// is K and the output node is N, both padded with zeros:
+// out[line][i] = sum_k line[k] Dhat[i][k], so B holds Dhat transposed and
+// stays in registers for both passes. With EPB dividing 8, rows g and g + 8
+// of lane 4g + t belong to element g mod EPB in every MMA tile, so a lane
+// evaluates the metric terms of its lines' element once. Warps take the MMA
+// tiles round robin. The line values are formed in registers from the
+// shared q tile as in the SIMT passes, and the lift, the sign, 1/J and the
+// stores to G follow from the accumulator fragments.
+template <int N, int EPB>
+struct TcLines {
+    static_assert(EPB == 2 || EPB == 4 || EPB == 8, "the tensor-core passes need EPB dividing 8");
+    static constexpr int kTiles = (3 * EPB * (N + 1) + 15) / 16;
+};
+
+template <int N, bool S, int E, bool TC = false>
 __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a, const __grid_constant__ Coeffs<N> cf) {
+    static_assert(!(TC && S), "the strict form rounds every operation in the reference's order: no tensor cores");
     using T = Tile<N, E>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     // padded strides of the tile (Tile): row pitch, element and field strides
@@ -213,9 +232,83 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
     const double* iw = cf.iw;
     const double* F = far_s + f * FS + e * SE;  // this thread's field, element side fluxes
 
+    // Tensor-core passes: the lane's fragments of Dhat transposed, its lift
+    // weights and the metric terms of its rows' element.
+    using TT = TcTable64<N>;
+    [[maybe_unused]] double tb[TT::KS][TT::NT], tlpw[TT::NT][2], tlmw[TT::NT][2], tcx[8];
+    [[maybe_unused]] const int tg = lane >> 2, tt = lane & 3, tel = tg % (EPB < 8 ? EPB : 8);
+    [[maybe_unused]] const bool tlive = tel < ne;
+    if constexpr (TC) {
+        const double* tab = a.tc64;
+#pragma unroll
+        for (int s = 0; s < TT::KS; ++s)
+#pragma unroll
+            for (int u = 0; u < TT::NT; ++u) tb[s][u] = tab[TT::kB + (s * TT::NT + u) * 32 + lane];
+#pragma unroll
+        for (int u = 0; u < TT::NT; ++u)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                tlpw[u][h] = tab[TT::kLPW + (u * 2 + h) * 32 + lane];
+                tlmw[u][h] = tab[TT::kLMW + (u * 2 + h) * 32 + lane];
+            }
+        const double* cc = a.corners + 8 * (e0 + tel);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) tcx[k] = tlive ? cc[k] : 0.0;
+    }
+
     // xi pass (eta index j = m): contravariant flux line eta_y X - eta_x Y
     // (Solver2D_t.cpp:72-80), Dhat . line + lift, G = -(...) (:82-101); G column j.
-    if (active) {
+    if constexpr (TC) {
+        const MetricLine<false> mx_eta(tcx[6] - tcx[0], tcx[4] - tcx[2]), my_eta(tcx[7] - tcx[1], tcx[5] - tcx[3]);
+        double ka[TT::KS], kb[TT::KS];  // eta_y, eta_x at the lane's nodes k = 4s + t (0 beyond N)
+#pragma unroll
+        for (int s = 0; s < TT::KS; ++s) {
+            const double xv = a.tc64[TT::kXK + s * 32 + lane];
+            const bool kv = 4 * s + tt < n;
+            ka[s] = kv ? my_eta(xv) : 0.0;
+            kb[s] = kv ? mx_eta(xv) : 0.0;
+        }
+        for (int mt = warp; mt < TcLines<N, EPB>::kTiles; mt += T::kWarps) {
+            int rf[2], rj[2];
+            bool rv[2];
+            double av[2][TT::KS];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int qq = (16 * mt + tg + 8 * h) / EPB;
+                rf[h] = qq / n;
+                rj[h] = qq - rf[h] * n;
+                rv[h] = tlive && rf[h] < 3;
+                const double* Xr = rf[h] == 0 ? qs + QS + tel * ES : (rf[h] == 1 ? qs + tel * ES : zs);
+                const double* Yr = rf[h] == 0 ? qs + 2 * QS + tel * ES : (rf[h] == 1 ? zs : qs + tel * ES);
+#pragma unroll
+                for (int s = 0; s < TT::KS; ++s) {
+                    const int k = 4 * s + tt;
+                    av[h][s] = (rv[h] && k < n) ? ka[s] * Xr[k * P + rj[h]] - kb[s] * Yr[k * P + rj[h]] : 0.0;
+                }
+            }
+            double acc[TT::NT][4];
+#pragma unroll
+            for (int u = 0; u < TT::NT; ++u) {
+                acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+#pragma unroll
+                for (int s = 0; s < TT::KS; ++s) dmma_16x8x4(acc[u], av[0][s], av[1][s], tb[s][u]);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!rv[h]) continue;
+                const double* Fr = far_s + rf[h] * FS + tel * SE;
+                const double fr = Fr[1 * n + rj[h]], fl3 = Fr[3 * n + (N - rj[h])];
+                double* G = gs + rf[h] * QS + tel * ES + rj[h];
+#pragma unroll
+                for (int u = 0; u < TT::NT; ++u)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int i = 8 * u + 2 * tt + c;
+                        if (i < n) G[i * P] = -(acc[u][2 * h + c] + fr * tlpw[u][c] + fl3 * tlmw[u][c]);
+                    }
+            }
+        }
+    } else if (active) {
         const int j = m;
         double col[n];
 #pragma unroll
@@ -235,7 +328,58 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
 
     // eta pass (xi index i = m): line -xi_y X + xi_x Y (Solver2D_t.cpp:103-113),
     // G = (G - (Dhat . line + lift)) / J (:114-133); G row i.
-    if (active) {
+    if constexpr (TC) {
+        const MetricLine<false> mx_xi(tcx[2] - tcx[0], tcx[4] - tcx[6]), my_xi(tcx[3] - tcx[1], tcx[5] - tcx[7]);
+        double ka[TT::KS], kb[TT::KS];  // -xi_y, xi_x at the lane's nodes k = 4s + t (0 beyond N)
+#pragma unroll
+        for (int s = 0; s < TT::KS; ++s) {
+            const double xv = a.tc64[TT::kXK + s * 32 + lane];
+            const bool kv = 4 * s + tt < n;
+            ka[s] = kv ? -my_xi(xv) : 0.0;
+            kb[s] = kv ? mx_xi(xv) : 0.0;
+        }
+        for (int mt = warp; mt < TcLines<N, EPB>::kTiles; mt += T::kWarps) {
+            int rf[2], ri[2];
+            bool rv[2];
+            double av[2][TT::KS];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int qq = (16 * mt + tg + 8 * h) / EPB;
+                rf[h] = qq / n;
+                ri[h] = qq - rf[h] * n;
+                rv[h] = tlive && rf[h] < 3;
+                const double* Xr = rf[h] == 0 ? qs + QS + tel * ES : (rf[h] == 1 ? qs + tel * ES : zs);
+                const double* Yr = rf[h] == 0 ? qs + 2 * QS + tel * ES : (rf[h] == 1 ? zs : qs + tel * ES);
+#pragma unroll
+                for (int s = 0; s < TT::KS; ++s) {
+                    const int k = 4 * s + tt;
+                    av[h][s] = (rv[h] && k < n) ? ka[s] * Xr[ri[h] * P + k] + kb[s] * Yr[ri[h] * P + k] : 0.0;
+                }
+            }
+            double acc[TT::NT][4];
+#pragma unroll
+            for (int u = 0; u < TT::NT; ++u) {
+                acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+#pragma unroll
+                for (int s = 0; s < TT::KS; ++s) dmma_16x8x4(acc[u], av[0][s], av[1][s], tb[s][u]);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!rv[h]) continue;
+                const double* Fr = far_s + rf[h] * FS + tel * SE;
+                const double ft = Fr[2 * n + (N - ri[h])], fb = Fr[0 * n + ri[h]];
+                double* G = gs + rf[h] * QS + tel * ES + ri[h] * P;
+                const double* jrow = js + tel * ES + ri[h] * P;
+#pragma unroll
+                for (int u = 0; u < TT::NT; ++u)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int j = 8 * u + 2 * tt + c;
+                        if (j < n) G[j] = (G[j] - (acc[u][2 * h + c] + ft * tlpw[u][c] + fb * tlmw[u][c])) * jrow[j];
+                    }
+            }
+        }
+    } else if (active) {
         const int i = m;
         double line[n];
 #pragma unroll
@@ -363,7 +507,22 @@ struct MetricLineF {
     __device__ __forceinline__ float operator()(float t) const { return fmaf(t, b, a); }
 };
 
-template <int N, int E>
+// One 3xTF32 product accumulation: c += a b with a = a_hi + a_lo split in
+// TF32 and b's parts (b_hi, b_lo) from the lane table, the small terms first:
+// c += a_lo b_hi, c += a_hi b_lo, c += a_hi b_hi.
+__device__ __forceinline__ void tf32x3_mma(float (&c)[4], const float (&a)[4], const float (&b)[4]) {
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        hi[r] = to_tf32(a[r]);
+        lo[r] = to_tf32(a[r] - __uint_as_float(hi[r]));
+    }
+    tf32mma_16x8x8(c, lo, __float_as_uint(b[0]), __float_as_uint(b[1]));
+    tf32mma_16x8x8(c, hi, __float_as_uint(b[2]), __float_as_uint(b[3]));
+    tf32mma_16x8x8(c, hi, __float_as_uint(b[0]), __float_as_uint(b[1]));
+}
+
+template <int N, int E, bool TC = false>
 __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageArgs a, const __grid_constant__ CoeffsF<N> cf) {
     using T = TileF<N, E>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
@@ -540,7 +699,94 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
     const float* Dh = cf.dhat;
     const float* iw = cf.iw;
     const float* F = far_s + f * FS + e * SE;
-    if (active) {
+    // Tensor-core passes (3xTF32): the lane's fragments of Dhat transposed
+    // (high and low TF32 parts), its lift weights and the corners of its
+    // rows' element.
+    using TT = TcTable32<N>;
+    constexpr int EPBc = Tile<N, E>::EPB;
+    [[maybe_unused]] float tb[TT::KS][TT::NT][4], tlpw[TT::NT][2], tlmw[TT::NT][2];
+    [[maybe_unused]] double tcx[8];
+    [[maybe_unused]] const int tg = lane >> 2, tt = lane & 3, tel = tg % (EPBc < 8 ? EPBc : 8);
+    [[maybe_unused]] const bool tlive = tel < ne;
+    if constexpr (TC) {
+        const float* tab = a.tc32;
+#pragma unroll
+        for (int s = 0; s < TT::KS; ++s)
+#pragma unroll
+            for (int u = 0; u < TT::NT; ++u)
+#pragma unroll
+                for (int r = 0; r < 4; ++r) tb[s][u][r] = tab[TT::kB + ((s * TT::NT + u) * 32 + lane) * 4 + r];
+#pragma unroll
+        for (int u = 0; u < TT::NT; ++u)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                tlpw[u][h] = tab[TT::kLPW + (u * 2 + h) * 32 + lane];
+                tlmw[u][h] = tab[TT::kLMW + (u * 2 + h) * 32 + lane];
+            }
+        const double* cc = a.corners + 8 * (e0 + tel);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) tcx[k] = tlive ? cc[k] : 0.0;
+    }
+    if constexpr (TC) {
+        // xi pass: rows (field, eta line j, element), K along xi.
+        const MetricLineF mx_eta(static_cast<float>(tcx[6] - tcx[0]), static_cast<float>(tcx[4] - tcx[2]));
+        const MetricLineF my_eta(static_cast<float>(tcx[7] - tcx[1]), static_cast<float>(tcx[5] - tcx[3]));
+        float ka[TT::KS][2], kb[TT::KS][2];
+#pragma unroll
+        for (int s = 0; s < TT::KS; ++s)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const float xv = a.tc32[TT::kXK + (s * 32 + lane) * 2 + r];
+                const bool kv = 8 * s + tt + 4 * r < n;
+                ka[s][r] = kv ? my_eta(xv) : 0.0f;
+                kb[s][r] = kv ? mx_eta(xv) : 0.0f;
+            }
+        for (int mt = warp; mt < TcLines<N, EPBc>::kTiles; mt += Tile<N, E>::kWarps) {
+            int rf[2], rj[2];
+            bool rv[2];
+            const float* Xr[2];
+            const float* Yr[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int qq = (16 * mt + tg + 8 * h) / EPBc;
+                rf[h] = qq / n;
+                rj[h] = qq - rf[h] * n;
+                rv[h] = tlive && rf[h] < 3;
+                Xr[h] = rf[h] == 0 ? qf + QS + tel * ES : (rf[h] == 1 ? qf + tel * ES : zs);
+                Yr[h] = rf[h] == 0 ? qf + 2 * QS + tel * ES : (rf[h] == 1 ? zs : qf + tel * ES);
+            }
+            float acc[TT::NT][4];
+#pragma unroll
+            for (int u = 0; u < TT::NT; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0f;
+#pragma unroll
+            for (int s = 0; s < TT::KS; ++s) {
+                float av[4];  // (row h, column r) at fragment register h + 2r
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int k = 8 * s + tt + 4 * r;
+                        av[h + 2 * r] = (rv[h] && k < n) ? ka[s][r] * Xr[h][k * P + rj[h]] - kb[s][r] * Yr[h][k * P + rj[h]] : 0.0f;
+                    }
+#pragma unroll
+                for (int u = 0; u < TT::NT; ++u) tf32x3_mma(acc[u], av, tb[s][u]);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!rv[h]) continue;
+                const float* Fr = far_s + rf[h] * FS + tel * SE;
+                const float fr = Fr[1 * n + rj[h]], fl3 = Fr[3 * n + (N - rj[h])];
+                float* G = gs + rf[h] * QS + tel * ES + rj[h];
+#pragma unroll
+                for (int u = 0; u < TT::NT; ++u)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int i = 8 * u + 2 * tt + c;
+                        if (i < n) G[i * P] = -(acc[u][2 * h + c] + fr * tlpw[u][c] + fl3 * tlmw[u][c]);
+                    }
+            }
+        }
+    } else if (active) {
         const int j = m;
         float col[n];
 #pragma unroll
@@ -557,7 +803,67 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
     }
     __syncthreads();
 
-    if (active) {
+    if constexpr (TC) {
+        // eta pass: rows (field, xi line i, element), K along eta.
+        const MetricLineF mx_xi(static_cast<float>(tcx[2] - tcx[0]), static_cast<float>(tcx[4] - tcx[6]));
+        const MetricLineF my_xi(static_cast<float>(tcx[3] - tcx[1]), static_cast<float>(tcx[5] - tcx[7]));
+        float ka[TT::KS][2], kb[TT::KS][2];
+#pragma unroll
+        for (int s = 0; s < TT::KS; ++s)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const float xv = a.tc32[TT::kXK + (s * 32 + lane) * 2 + r];
+                const bool kv = 8 * s + tt + 4 * r < n;
+                ka[s][r] = kv ? -my_xi(xv) : 0.0f;
+                kb[s][r] = kv ? mx_xi(xv) : 0.0f;
+            }
+        for (int mt = warp; mt < TcLines<N, EPBc>::kTiles; mt += Tile<N, E>::kWarps) {
+            int rf[2], ri[2];
+            bool rv[2];
+            const float* Xr[2];
+            const float* Yr[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int qq = (16 * mt + tg + 8 * h) / EPBc;
+                rf[h] = qq / n;
+                ri[h] = qq - rf[h] * n;
+                rv[h] = tlive && rf[h] < 3;
+                Xr[h] = rf[h] == 0 ? qf + QS + tel * ES : (rf[h] == 1 ? qf + tel * ES : zs);
+                Yr[h] = rf[h] == 0 ? qf + 2 * QS + tel * ES : (rf[h] == 1 ? zs : qf + tel * ES);
+            }
+            float acc[TT::NT][4];
+#pragma unroll
+            for (int u = 0; u < TT::NT; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0f;
+#pragma unroll
+            for (int s = 0; s < TT::KS; ++s) {
+                float av[4];
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int k = 8 * s + tt + 4 * r;
+                        av[h + 2 * r] = (rv[h] && k < n) ? ka[s][r] * Xr[h][ri[h] * P + k] + kb[s][r] * Yr[h][ri[h] * P + k] : 0.0f;
+                    }
+#pragma unroll
+                for (int u = 0; u < TT::NT; ++u) tf32x3_mma(acc[u], av, tb[s][u]);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!rv[h]) continue;
+                const float* Fr = far_s + rf[h] * FS + tel * SE;
+                const float ft = Fr[2 * n + (N - ri[h])], fb = Fr[0 * n + ri[h]];
+                float* G = gs + rf[h] * QS + tel * ES + ri[h] * P;
+                const float* jrow = js + tel * ES + ri[h] * P;
+#pragma unroll
+                for (int u = 0; u < TT::NT; ++u)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int j = 8 * u + 2 * tt + c;
+                        if (j < n) G[j] = (G[j] - (acc[u][2 * h + c] + ft * tlpw[u][c] + fb * tlmw[u][c])) * jrow[j];
+                    }
+            }
+        }
+    } else if (active) {
         const int i = m;
         float line[n];
 #pragma unroll

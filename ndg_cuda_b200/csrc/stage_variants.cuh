@@ -18,10 +18,14 @@ namespace dev {
 
 constexpr int kTileChoices[] = {2, 4, 8, 16};
 
-template <bool F32, int N, int E>
+// Orders with tensor-core variants (the contraction passes on the tensor
+// cores pay once the lines are long: N >= 6).
+constexpr int kTensorMinOrder = 6;
+
+template <bool F32, int N, int E, bool TC = false>
 struct Variant {
     using T = std::conditional_t<F32, TileF<N, E>, Tile<N, E>>;
-    static constexpr bool feasible = T::kThreads <= 512 && T::kBytes <= 113 * 1024;
+    static constexpr bool feasible = T::kThreads <= 512 && T::kBytes <= 113 * 1024 && (!TC || (E <= 8 && N >= kTensorMinOrder));
 };
 
 template <int N>
@@ -46,61 +50,63 @@ CoeffsF<N> variant_coeffs_f() {
     return c;
 }
 
-template <bool F32, int N, int E>
+template <bool F32, int N, int E, bool TC>
 cudaError_t variant_prepare() {
-    if constexpr (Variant<F32, N, E>::feasible) {
-        using T = typename Variant<F32, N, E>::T;
+    if constexpr (Variant<F32, N, E, TC>::feasible) {
+        using T = typename Variant<F32, N, E, TC>::T;
         if constexpr (F32)
-            return cudaFuncSetAttribute(stage_kernel_f32<N, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(T::kBytes));
+            return cudaFuncSetAttribute(stage_kernel_f32<N, E, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(T::kBytes));
         else
-            return cudaFuncSetAttribute(stage_kernel<N, false, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(T::kBytes));
+            return cudaFuncSetAttribute(stage_kernel<N, false, E, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(T::kBytes));
     } else {
         return cudaErrorInvalidValue;
     }
 }
 
-template <bool F32, int N, int E>
+template <bool F32, int N, int E, bool TC>
 cudaError_t variant_launch(const StageArgs& a, cudaStream_t stream) {
-    if constexpr (Variant<F32, N, E>::feasible) {
-        using T = typename Variant<F32, N, E>::T;
+    if constexpr (Variant<F32, N, E, TC>::feasible) {
+        using T = typename Variant<F32, N, E, TC>::T;
         const dim3 grid(static_cast<unsigned>((a.n_elements + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
         if constexpr (F32)
-            stage_kernel_f32<N, E><<<grid, T::kThreads, T::kBytes, stream>>>(a, variant_coeffs_f<N>());
+            stage_kernel_f32<N, E, TC><<<grid, T::kThreads, T::kBytes, stream>>>(a, variant_coeffs_f<N>());
         else
-            stage_kernel<N, false, E><<<grid, T::kThreads, T::kBytes, stream>>>(a, variant_coeffs<N>());
+            stage_kernel<N, false, E, TC><<<grid, T::kThreads, T::kBytes, stream>>>(a, variant_coeffs<N>());
         return cudaGetLastError();
     } else {
         return cudaErrorInvalidValue;
     }
 }
 
-template <bool F32, int N>
+// Tile codes of order N: E for the SIMT passes, kTensorTile + E for the
+// tensor-core passes (TC true), each where feasible.
+template <bool F32, int N, bool TC>
 int variant_candidates(int* out, int max) {
-    const bool ok[] = {Variant<F32, N, 2>::feasible, Variant<F32, N, 4>::feasible, Variant<F32, N, 8>::feasible,
-                       Variant<F32, N, 16>::feasible};
+    const bool ok[] = {Variant<F32, N, 2, TC>::feasible, Variant<F32, N, 4, TC>::feasible, Variant<F32, N, 8, TC>::feasible,
+                       Variant<F32, N, 16, TC>::feasible};
     int count = 0;
     for (int i = 0; i < 4; ++i)
-        if (ok[i] && count < max) out[count++] = kTileChoices[i];
+        if (ok[i] && count < max) out[count++] = kTileChoices[i] + (TC ? kTensorTile : 0);
     return count;
 }
 
-#define NDG_VARIANT_TILES(FN, F32_, N_, ...)             \
-    switch (epb) {                                        \
-        case 2: return FN<F32_, N_, 2>(__VA_ARGS__);      \
-        case 4: return FN<F32_, N_, 4>(__VA_ARGS__);      \
-        case 8: return FN<F32_, N_, 8>(__VA_ARGS__);      \
-        case 16: return FN<F32_, N_, 16>(__VA_ARGS__);    \
-        default: return cudaErrorInvalidValue;            \
+#define NDG_VARIANT_TILES(FN, F32_, N_, TC_, ...)            \
+    switch (epb) {                                            \
+        case 2: return FN<F32_, N_, 2, TC_>(__VA_ARGS__);     \
+        case 4: return FN<F32_, N_, 4, TC_>(__VA_ARGS__);     \
+        case 8: return FN<F32_, N_, 8, TC_>(__VA_ARGS__);     \
+        case 16: return FN<F32_, N_, 16, TC_>(__VA_ARGS__);   \
+        default: return cudaErrorInvalidValue;                \
     }
 
-template <bool F32, int N>
+template <bool F32, int N, bool TC>
 cudaError_t variant_prepare_n(int epb) {
-    NDG_VARIANT_TILES(variant_prepare, F32, N)
+    NDG_VARIANT_TILES(variant_prepare, F32, N, TC)
 }
 
-template <bool F32, int N>
+template <bool F32, int N, bool TC>
 cudaError_t variant_launch_n(int epb, const StageArgs& a, cudaStream_t stream) {
-    NDG_VARIANT_TILES(variant_launch, F32, N, a, stream)
+    NDG_VARIANT_TILES(variant_launch, F32, N, TC, a, stream)
 }
 
 #define NDG_VARIANT_ORDERS(CALL)  \

@@ -143,11 +143,16 @@ def test_element_state_bitwise_vs_reference(res, kw, ref_available):
 
 def test_tile_candidates_on_a_host_context():
     """The autotuner's candidate tiles need no GPU to list: powers of two
-    that fit 512 threads and 113 KB of shared memory."""
+    that fit 512 threads and 113 KB of shared memory, then the tensor-core
+    tiles (TENSOR_TILE + 2, 4, 8) from order 6 up."""
     zone = meshgen.uniform_zone(4, boundary=meshgen.WALL)
     m = ndg.Mesh2D_t(zone, 8, device=-1)
     cand, default = m.tile_candidates()
-    assert cand == [2, 4, 8, 16] and default == 4
+    T = ndg.TENSOR_TILE
+    assert cand == [2, 4, 8, 16, T + 2, T + 4, T + 8] and default == 4
+    m4 = ndg.Mesh2D_t(zone, 4, device=-1)
+    assert all(t < T for t in m4.tile_candidates()[0])
     m16 = ndg.Mesh2D_t(zone, 16, device=-1)
     cand16, _ = m16.tile_candidates()
-    assert cand16 and max(cand16) * 3 * 17 <= 512 and all(c in (2, 4, 8, 16) for c in cand16)
+    simt16 = [c % T for c in cand16]
+    assert cand16 and max(simt16) * 3 * 17 <= 512 and all(c in (2, 4, 8, 16) for c in simt16)
