@@ -140,6 +140,17 @@ ndg_status ndg_ctx_synchronize(ndg_ctx* ctx);
 /* Keep a copy of each stage's time derivative G (Element2D_t::G_p_ ...) so
  * that ndg_get_field can return it; off by default (it costs HBM traffic). */
 ndg_status ndg_ctx_keep_derivative(ndg_ctx* ctx, int32_t enable);
+/* How a stage runs on a mixed-order mesh (after adaptation), replacing the
+ * reference's per-stage launch chain (include/solvers/Solver2D_t.tcu:44-70):
+ * mode 0 (default) one launch per order group, as concurrent branches of
+ * the step graph, each with its order's own tile, registers and shared
+ * memory; mode 1 one launch per stage whose CTAs take the tiles of every
+ * order group from one queue, largest order first, each running its tile's
+ * order. Each tile computes the same operations either way (bit-identical
+ * in NDG_FP64_STRICT; the compiler may contract differently otherwise).
+ * Mode 0 is the faster on the meshes measured; meshes of one order are not
+ * affected. */
+ndg_status ndg_set_mixed_launch(ndg_ctx* ctx, int32_t mode);
 
 /* NDG_t<LegendrePolynomial_t>(N_max, n_interpolation_points, stream)
  * (include/entities/NDG_t.cuh:11, include/entities/NDG_t.tcu:13-72). */

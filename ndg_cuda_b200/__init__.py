@@ -84,6 +84,7 @@ def lib() -> C.CDLL:
         "ndg_ctx_destroy": ([vp], C.c_int),
         "ndg_ctx_set_precision": ([vp, i32], C.c_int),
         "ndg_ctx_keep_derivative": ([vp, i32], C.c_int),
+        "ndg_set_mixed_launch": ([vp, i32], C.c_int),
         "ndg_ctx_synchronize": ([vp], C.c_int),
         "ndg_tables_build": ([vp, i32, i64], C.c_int),
         "ndg_tables_get": ([vp, i32, i32, vp, i64, C.POINTER(i64)], C.c_int),
@@ -295,6 +296,10 @@ class Mesh2D_t:
 
     def set_precision(self, precision: int) -> None:
         _check(lib().ndg_ctx_set_precision(self._ctx.h, precision))
+
+    def set_mixed_launch(self, mode: int) -> None:
+        """Mixed-order meshes: 0 one launch per order group (default), 1 one queue launch per stage."""
+        _check(lib().ndg_set_mixed_launch(self._ctx.h, mode))
 
     # Mesh2D_t::initial_conditions (src/meshes/Mesh2D_t.cu:5030)
     def initial_conditions(self) -> None:

@@ -44,6 +44,9 @@ def main(argv=None) -> None:
     ap.add_argument("--rounds", type=int, default=3, help="p-adaptation rounds of the mixed case")
     ap.add_argument("--tile", type=int, default=0, help="elements per CTA of the stage kernel (0: default)")
     ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--launch", type=int, default=0, choices=[0, 1],
+                    help="mixed case: 0 one launch per order group, 1 one queue launch per stage")
+    ap.add_argument("--time", type=int, default=0, help="mixed case: then time this many steps (wall clock after a synchronise)")
     args = ap.parse_args(argv)
     prec = FP32 if args.fp32 else FP64
     if args.case == "stage":
@@ -85,8 +88,17 @@ def main(argv=None) -> None:
         for _ in range(args.rounds):
             K = mesh.n_elements_
             mesh.adapt((rng.random(K) < 0.4).astype(np.int32), np.full(K, 2.0))
+        mesh.set_mixed_launch(args.launch)
         Solver2D_t.run(mesh, args.steps)
         print("p[0] =", mesh.get_field("p")[0])
+        if args.time:
+            import time
+            for _ in range(2):
+                mesh.synchronize()
+                t0 = time.perf_counter()
+                Solver2D_t.run(mesh, args.time)
+                mesh.synchronize()
+                print(f"launch mode {args.launch}: {1e3 * (time.perf_counter() - t0) / args.time:.4f} ms per RK3 step")
     else:
         zone = _zone(args.res, boundary=meshgen.WALL)
         c = workloads.speed_field(zone, seed=0)

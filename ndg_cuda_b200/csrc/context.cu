@@ -106,6 +106,7 @@ dev::GeneralStage general_args(ndg_ctx* c, int m, int in) {
 // fused stage of every order group.
 int64_t general_stage_launches(const ndg_ctx* c) {
     const int64_t ghosts = c->gmesh.n_total > c->gmesh.n_domain ? 1 : 0;
+    if (c->mixed_launch == 1) return (c->queue.n_tiles > 0 ? 1 : 0) + ghosts;
     return static_cast<int64_t>(c->groups.size()) + ghosts;
 }
 
@@ -133,6 +134,7 @@ void ensure_aux_streams(ndg_ctx* c) {
 cudaError_t issue_general_stage(ndg_ctx* c, int m, int in) {
     const dev::GeneralStage a = general_args(c, m, in);
     cudaError_t err = dev::launch_general_ghosts(a, strict(c), fp32(c), c->stream);
+    if (c->mixed_launch == 1) return err == cudaSuccess ? dev::launch_general_queue(a, c->queue, strict(c), fp32(c), c->stream) : err;
     const size_t G = c->groups.size();
     if (err != cudaSuccess || G == 0) return err;
     if (G > 1 && (err = cudaEventRecord(c->aux_events[0], c->stream)) != cudaSuccess) return err;
@@ -430,6 +432,26 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
             at += og.count;
             c->groups.push_back(og);
             check_cuda(dev::prepare_general_kernels(og.N, g.side_slots), "kernel attributes");
+        }
+        // The stage queue: the groups' tiles, largest order first, and the
+        // shared memory of the largest tile in either form.
+        {
+            std::vector<const dev::OrderGroup*> by_N;
+            for (const auto& og : c->groups) by_N.push_back(&og);
+            std::stable_sort(by_N.begin(), by_N.end(), [](const dev::OrderGroup* x, const dev::OrderGroup* y) { return x->N > y->N; });
+            std::vector<dev::QueueTile> tiles;
+            size_t smem = 0;
+            for (const dev::OrderGroup* og : by_N) {
+                const int epb = dev::general_tile_elements(og->N);
+                for (int64_t b = 0; b < og->count; b += epb) tiles.push_back(dev::QueueTile{og->N, og->first, og->count, b});
+                smem = std::max({smem, dev::general_tile_bytes(og->N, g.side_slots, false), dev::general_tile_bytes(og->N, g.side_slots, true)});
+            }
+            c->g_queue.upload(tiles, c->stream);
+            c->queue = dev::StageQueue{};
+            c->queue.tiles = c->g_queue.ptr;
+            c->queue.n_tiles = static_cast<int64_t>(tiles.size());
+            c->queue.smem_bytes = smem;
+            check_cuda(dev::prepare_general_queue(smem), "queue kernel attributes");
         }
         c->getr[0].allocate(inst * 3 * static_cast<size_t>(g.trace_total));
         c->getr[1].allocate(inst * 3 * static_cast<size_t>(g.trace_total));
@@ -795,6 +817,15 @@ ndg_status ndg_ctx_set_precision(ndg_ctx* ctx, int32_t precision) {
             ctx->traces_valid = false;  // the forms keep their traces in different buffers
         }
         ctx->precision = precision;
+    });
+}
+
+ndg_status ndg_set_mixed_launch(ndg_ctx* ctx, int32_t mode) {
+    return guarded([&] {
+        if (!ctx) fail(NDG_ERR_INVALID_ARG, "ctx is NULL");
+        if (mode != 0 && mode != 1) fail(NDG_ERR_INVALID_ARG, "mode is 0 (one launch per order group) or 1 (one queue launch per stage)");
+        ctx->mixed_launch = mode;
+        drop_graphs(ctx);
     });
 }
 

@@ -119,6 +119,12 @@ struct ndg_ctx {
     ndg::DeviceBuffer<double> g_gframe;
     std::vector<ndg::dev::OrderGroup> groups;
     ndg::dev::GeneralMesh gmesh;
+    // Mixed-order stages: one launch per order group as concurrent graph
+    // branches (mixed_launch 0, the default), or one launch per stage over
+    // the stage queue, every tile of every group (mixed_launch 1).
+    ndg::DeviceBuffer<ndg::dev::QueueTile> g_queue;
+    ndg::dev::StageQueue queue;
+    int mixed_launch = 0;
 
     // Streams and events on which the order groups of a mixed-order stage
     // run concurrently (forked from and joined to `stream`).

@@ -471,11 +471,16 @@ struct FusedTile {
     }
 };
 
-template <int N, bool S, typename R>
-__global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kernel(GeneralStage a, OrderGroup grp) {
+// One tile of EPB elements of an order group: list positions
+// first + base .. first + base + EPB - 1 (at most count - base of them), of
+// instance inst, by THREADS threads (at least the tile's own kThreads; the
+// extra threads take part in the strided loops and the barriers only).
+template <int N, bool S, typename R, int THREADS>
+__device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t first, const int64_t count, const int64_t base,
+                                           const int64_t inst, double* smem) {
     using T = FusedTile<N, R>;
+    static_assert(T::kThreads <= THREADS, "a tile needs at least its own threads");
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
-    extern __shared__ __align__(128) double smem[];
     double* qs = smem + T::kQ;
     double* ks = smem + T::kK;
     int64_t* eo2 = reinterpret_cast<int64_t*>(smem + T::kOff);  // first value of the tile's elements in a field block
@@ -504,9 +509,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     const int FFS = EPB * 4 * SL;
     const GeneralMesh& M = a.m;
     const int tid = threadIdx.x;
-    const int64_t base = static_cast<int64_t>(blockIdx.x) * EPB;
-    const int ne = static_cast<int>((grp.count - base) < EPB ? (grp.count - base) : EPB);
-    const int64_t inst = blockIdx.y;
+    const int ne = static_cast<int>((count - base) < EPB ? (count - base) : EPB);
     const int64_t fb = M.block, ft = M.trace_total;
     double* q = a.q + inst * 3 * fb;
     double* k = a.k + inst * 3 * fb;
@@ -520,18 +523,18 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     // The tile's sides: slot ranges, mortar entries and flux modes, and per
     // element its offsets (plan arrays in list order).
     if (tid <= 4 * ne) {
-        const int64_t ps = 4 * (grp.first + base) + tid;
+        const int64_t ps = 4 * (first + base) + tid;
         sst[tid] = M.pslot_start[ps];
         sqs[tid] = M.pq_start[ps];
         if (tid < 4 * ne) smode[tid] = M.pside_mode[ps];
         if (tid < ne) {
-            eo2[tid] = M.poff2[grp.first + base + tid];
-            eo1[tid] = M.poff1[grp.first + base + tid];
+            eo2[tid] = M.poff2[first + base + tid];
+            eo1[tid] = M.poff1[first + base + tid];
         }
     }
     __syncthreads();
     // q and k tiles: asynchronous copies, waited for before the volume terms.
-    for (int idx = tid; idx < T::kVals; idx += T::kThreads) {
+    for (int idx = tid; idx < T::kVals; idx += THREADS) {
         const int f = idx / (EPB * NN), r = idx - f * (EPB * NN);
         const int e = r / NN, node = r - e * NN;
         if (e < ne) {
@@ -545,7 +548,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     // range, the side found by bisection of the slot starts.
     const int64_t g0 = sst[0];
     const int n_items = static_cast<int>(sst[4 * ne] - g0);
-    for (int idx = tid; idx < n_items; idx += T::kThreads) {
+    for (int idx = tid; idx < n_items; idx += THREADS) {
         const int64_t g = g0 + idx;
         int lo = 0, hi = ne * 4;  // the side holding slot g: sst[lo] <= g < sst[lo + 1]
         while (hi - lo > 1) {
@@ -585,7 +588,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     const int e = rr / n;
     const int m = rr - e * n;
     const bool active = f < 3 && e < ne;
-    const int64_t pe = active ? grp.first + base + e : 0;
+    const int64_t pe = active ? first + base + e : 0;
     // Corners in FP64: their differences are formed before rounding to R.
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
@@ -614,7 +617,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     // Each thread converts the q values it copied (FP32 form).
     cp_async_wait_all();
     if constexpr (T::kCopy) {
-        for (int idx = tid; idx < T::kVals; idx += T::kThreads) qw[idx] = R(qs[idx]);
+        for (int idx = tid; idx < T::kVals; idx += THREADS) qw[idx] = R(qs[idx]);
     }
     __syncthreads();  // q and k tiles, face fluxes, J, edge metrics
 
@@ -622,7 +625,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
     // the face flux times the edge metric where one face of the element's
     // order covers the side (reversed and negated for the face's right
     // element), otherwise the mortar projection with the plan's weights.
-    for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
+    for (int idx = tid; idx < ne * 4 * n; idx += THREADS) {
         const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
         const int s = sm / n, i = sm - s * n;
         const int mode = smode[ee * 4 + s];
@@ -718,7 +721,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
 
     // Low-storage RK3 update (Solver2D_t.cpp:138-172), node by node, in FP64.
     const double gdt = mul<S>(a.rk_g, dt);
-    for (int idx = tid; idx < T::kVals; idx += T::kThreads) {
+    for (int idx = tid; idx < T::kVals; idx += THREADS) {
         const int ff = idx / (EPB * NN), r = idx - ff * (EPB * NN);
         const int ee = r / NN, node = r - ee * NN;
         if (ee >= ne) continue;
@@ -736,7 +739,7 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
 
     // Side traces of the new q for the next stage (Element2D_t.cpp:86-125):
     // item (element, side, node), three fields each.
-    for (int idx = tid; idx < ne * 4 * n; idx += T::kThreads) {
+    for (int idx = tid; idx < ne * 4 * n; idx += THREADS) {
         const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
         const int s = sm / n, mm = sm - s * n;
         const R* l = (s == 0 || s == 3) ? lm : lp;
@@ -752,6 +755,47 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
             for (int j = 0; j < n; ++j) acc = madd<S>(acc, l[j], qe[j * stride]);
             out[c * ft] = acc;
         }
+    }
+}
+
+// Fused stage of one order group: one CTA per tile.
+template <int N, bool S, typename R>
+__global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kernel(GeneralStage a, OrderGroup grp) {
+    extern __shared__ __align__(128) double smem[];
+    fused_tile<N, S, R, FusedTile<N, R>::kThreads>(a, grp.first, grp.count, static_cast<int64_t>(blockIdx.x) * FusedTile<N, R>::EPB,
+                                                   blockIdx.y, smem);
+}
+
+// Fused stage of every order group in one launch: one CTA of kQueueThreads
+// threads per entry of the stage queue (the tiles of every group, largest
+// order first, then the next instance), which names the tile's order; the
+// CTA runs that order's tile. The block scheduler hands out the entries in
+// queue order as CTAs retire, so the long high-order tiles start first.
+// One order's tile as a function of its own (not inlined), so that each
+// order is register-allocated on its own rather than the sixteen together;
+// the stage arguments reach it through a restrict pointer to the kernel's
+// parameter, so the mesh arrays' addresses stay in registers across the
+// tile's stores.
+template <int N, bool S, typename R>
+__device__ __noinline__ void queue_tile(const GeneralStage* __restrict__ ap, int64_t first, int64_t count, int64_t base, int64_t inst,
+                                        double* smem) {
+    fused_tile<N, S, R, kQueueThreads>(*ap, first, count, base, inst, smem);
+}
+
+template <bool S, typename R>
+__global__ void __launch_bounds__(kQueueThreads, 6) general_stage_kernel(const __grid_constant__ GeneralStage a, StageQueue wq) {
+    extern __shared__ __align__(128) double smem[];
+    const int64_t it = blockIdx.x;
+    const int64_t inst = it / wq.n_tiles;
+    const QueueTile w = wq.tiles[it - inst * wq.n_tiles];
+    switch (w.N) {
+#define NDG_TILE_CASE(n_) \
+    case n_: queue_tile<n_, S, R>(&a, w.first, w.count, w.base, inst, smem); break;
+        NDG_TILE_CASE(1) NDG_TILE_CASE(2) NDG_TILE_CASE(3) NDG_TILE_CASE(4) NDG_TILE_CASE(5) NDG_TILE_CASE(6)
+        NDG_TILE_CASE(7) NDG_TILE_CASE(8) NDG_TILE_CASE(9) NDG_TILE_CASE(10) NDG_TILE_CASE(11) NDG_TILE_CASE(12)
+        NDG_TILE_CASE(13) NDG_TILE_CASE(14) NDG_TILE_CASE(15) NDG_TILE_CASE(16)
+#undef NDG_TILE_CASE
+        default: break;
     }
 }
 
@@ -884,6 +928,14 @@ cudaError_t launch_fused(const GeneralStage& a, const OrderGroup& g, cudaStream_
     return cudaGetLastError();
 }
 
+template <bool S, typename R>
+cudaError_t launch_queue_t(const GeneralStage& a, const StageQueue& wq, cudaStream_t stream) {
+    const int64_t ctas = wq.n_tiles * a.n_instances;
+    if (ctas > 0x7fffffff) return cudaErrorInvalidValue;
+    general_stage_kernel<S, R><<<static_cast<unsigned>(ctas), kQueueThreads, wq.smem_bytes, stream>>>(a, wq);
+    return cudaGetLastError();
+}
+
 template <int N>
 cudaError_t set_attrs(int side_slots) {
     const int b64 = static_cast<int>(FusedTile<N, double>::bytes(side_slots));
@@ -996,6 +1048,39 @@ cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, boo
         if (fp32) return launch_fused<N, false, float>(a, g, stream);
         return strict ? launch_fused<N, true, double>(a, g, stream) : launch_fused<N, false, double>(a, g, stream);
     });
+}
+
+size_t general_tile_bytes(int N, int side_slots, bool fp32) {
+    size_t b = 0;
+    by_order(N, [&](auto c) {
+        constexpr int n_ = decltype(c)::value;
+        b = fp32 ? FusedTile<n_, float>::bytes(side_slots) : FusedTile<n_, double>::bytes(side_slots);
+        return cudaSuccess;
+    });
+    return b;
+}
+
+int general_tile_elements(int N) {
+    int e = 0;
+    by_order(N, [&](auto c) {
+        e = FusedTile<decltype(c)::value, double>::EPB;
+        return cudaSuccess;
+    });
+    return e;
+}
+
+cudaError_t prepare_general_queue(size_t smem_bytes) {
+    const int b = static_cast<int>(smem_bytes);
+    cudaError_t err = cudaFuncSetAttribute(general_stage_kernel<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(general_stage_kernel<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(general_stage_kernel<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return err;
+}
+
+cudaError_t launch_general_queue(const GeneralStage& a, const StageQueue& wq, bool strict, bool fp32, cudaStream_t stream) {
+    if (wq.n_tiles == 0) return cudaSuccess;
+    if (fp32) return launch_queue_t<false, float>(a, wq, stream);
+    return strict ? launch_queue_t<true, double>(a, wq, stream) : launch_queue_t<false, double>(a, wq, stream);
 }
 
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream) {

@@ -130,6 +130,22 @@ struct OrderGroup {
     int64_t first = 0;             // list position of the group's first element
 };
 
+// The stage queue of a mixed-order mesh: every tile of every order group
+// (largest order first), one CTA each in one launch per stage
+// (launch_general_queue).
+constexpr int kQueueThreads = 128;
+struct QueueTile {
+    int N = 0;
+    int64_t first = 0;  // list position of the group's first element
+    int64_t count = 0;  // elements of the group
+    int64_t base = 0;   // the tile's first element within the group
+};
+struct StageQueue {
+    const QueueTile* tiles = nullptr;
+    int64_t n_tiles = 0;    // per instance
+    size_t smem_bytes = 0;  // the largest tile of the orders present
+};
+
 cudaError_t upload_general_tables(const Tables& t);
 // Fills the mortar weights of a plan (once per plan): the same arithmetic,
 // in the reference's rounding, as the per-node computation they replace.
@@ -147,6 +163,13 @@ cudaError_t launch_general_traces(const GeneralStage& a, const OrderGroup* group
 // FP32 trace buffers; q, k and the RK update in FP64).
 cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, bool fp32, cudaStream_t stream);
 cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream);
+// Shared memory and elements of the fused tile of order N.
+size_t general_tile_bytes(int N, int side_slots, bool fp32);
+int general_tile_elements(int N);
+// Opts the queue kernels into smem_bytes of dynamic shared memory.
+cudaError_t prepare_general_queue(size_t smem_bytes);
+// The fused stage of every order group in one launch (after the ghosts).
+cudaError_t launch_general_queue(const GeneralStage& a, const StageQueue& wq, bool strict, bool fp32, cudaStream_t stream);
 // The plane-wave initial condition at every node of a mixed-order mesh.
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream);
 
