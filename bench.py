@@ -454,6 +454,7 @@ def hp_leg(local: int, stream) -> dict:
     # Parity at the configuration's scale: three adaptation rounds in
     # lockstep with the reference's CPU path (outside every timed region).
     lockstep = hp_lockstep_check(local, stream)
+    adapt_cost = adapt_cost_leg(local, stream)
     return {"workload": f"hp_adaptive_wave_rk3_walls_{HP_RES}x{HP_RES}_jitter0.1_N{HP_N0}to{HP_NMAX}",
             "setup": (f"{HP_RES}x{HP_RES} walled quads, interior nodes jittered by U(-0.1h, 0.1h) (seed 7), N {HP_N0} up to {HP_NMAX}, "
                       f"up to {HP_SPLITS} splits, estimate + adapt every {HP_INTERVAL} steps (Legendre decay), two crossing "
@@ -466,7 +467,39 @@ def hp_leg(local: int, stream) -> dict:
             "note": ("at the configuration's threshold 1e-4 the estimate never exceeds it on this mesh (largest error at N=4 "
                      "is 3.4e-6), so nothing refines; the 1e-9 runs exercise p-refinement, splitting to level 2 and the mortar path"),
             "flags_parity": lockstep["flags_parity"],
-            "lockstep": lockstep}
+            "lockstep": lockstep,
+            "adapt_cost": adapt_cost}
+
+
+def adapt_cost_leg(local: int, stream) -> dict:
+    """Wall time of one adaptation (Mesh2D_t::adapt: decisions and counts on
+    the device, topology rebuild on the host, device plan and field
+    transfer) on the hp mesh family at 128 x 128 and 512 x 512: seeded flags
+    on 10% of the elements, half of them splitting, three rounds each."""
+    import numpy as np
+    import ndg_cuda_b200 as ndg
+    from ndg_cuda_b200 import meshgen
+    out = {}
+    for res in (HP_RES, 4 * HP_RES):
+        zone = meshgen.uniform_zone(res, boundary=meshgen.WALL, jitter=0.1, seed=7)
+        m = ndg.Mesh2D_t(zone, HP_N0, maximum_N=HP_NMAX, max_split_level=HP_SPLITS, cfl=CFL, device=local, stream=stream.cuda_stream)
+        m.initial_conditions()
+        ndg.Solver2D_t.run(m, 1)
+        rng = np.random.default_rng(res)
+        rounds = []
+        for _ in range(3):
+            K = m.n_elements_
+            refine = (rng.random(K) < 0.1).astype(np.int32)
+            sigma = np.where(rng.random(K) < 0.5, 0.5, 2.0)
+            m.synchronize()
+            t0 = time.perf_counter()
+            m.adapt(refine, sigma)
+            m.synchronize()
+            rounds.append({"elements_before": K, "elements_after": m.n_elements_, "faces_after": m.n_faces_,
+                           "ms": 1e3 * (time.perf_counter() - t0), "phases_ms": m.adapt_timings()})
+        out[f"{res}x{res}"] = {"rounds": rounds, "ms_per_adaptation": statistics.median(r["ms"] for r in rounds)}
+        m.close()
+    return out
 
 
 def hp_lockstep_check(local: int, stream) -> dict:

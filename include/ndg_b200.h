@@ -263,6 +263,14 @@ ndg_status ndg_set_tile(ndg_ctx* ctx, int32_t elements_per_block);
 /* The candidate tiles of the loaded order and current form, and the default. */
 ndg_status ndg_tile_candidates(const ndg_ctx* ctx, int32_t* out, int32_t capacity, int32_t* count, int32_t* default_tile);
 
+/* No counterpart in the reference. Host wall time of the last adaptation
+ * (ndg_adapt or ndg_adapt_flags) by phase, in ms: ms[0] the decisions and
+ * renumbering counts on the device (with the upload of the topology they
+ * read and the download of their results), ms[1] the rebuild of the
+ * topology on the host, ms[2] the field transfer to the new elements,
+ * ms[3] the device plan of the new mesh. */
+ndg_status ndg_adapt_timings(const ndg_ctx* ctx, double* ms);
+
 /* Kernel launches issued by this context so far (for launch accounting). */
 ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches);
 

@@ -85,6 +85,7 @@ def lib() -> C.CDLL:
         "ndg_ctx_set_precision": ([vp, i32], C.c_int),
         "ndg_ctx_keep_derivative": ([vp, i32], C.c_int),
         "ndg_set_mixed_launch": ([vp, i32], C.c_int),
+        "ndg_adapt_timings": ([vp, C.POINTER(dbl)], C.c_int),
         "ndg_ctx_synchronize": ([vp], C.c_int),
         "ndg_tables_build": ([vp, i32, i64], C.c_int),
         "ndg_tables_get": ([vp, i32, i32, vp, i64, C.POINTER(i64)], C.c_int),
@@ -296,6 +297,12 @@ class Mesh2D_t:
 
     def set_precision(self, precision: int) -> None:
         _check(lib().ndg_ctx_set_precision(self._ctx.h, precision))
+
+    def adapt_timings(self) -> dict:
+        """Host wall time (ms) of the last adaptation by phase."""
+        ms = (C.c_double * 4)()
+        _check(lib().ndg_adapt_timings(self._ctx.h, ms))
+        return dict(zip(("device_decisions", "topology", "transfer", "plan"), ms))
 
     def set_mixed_launch(self, mode: int) -> None:
         """Mixed-order meshes: 0 one launch per order group (default), 1 one queue launch per stage."""

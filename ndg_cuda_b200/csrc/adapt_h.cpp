@@ -117,7 +117,7 @@ std::vector<int64_t> expand_side(const std::vector<Face>& fa, const std::vector<
 }  // namespace
 
 bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level,
-             std::vector<ElementSource>& sources) {
+             std::vector<ElementSource>& sources, const AdaptDecisions* dec) {
     Work w;
     w.K = t.n_domain;
     w.max_split = max_split_level;
@@ -157,12 +157,27 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
     w.if_destination = t.if_destination;
 
     int64_t n_split = 0;
-    for (int64_t e = 0; e < w.K; ++e) n_split += w.would_h(w.el[static_cast<size_t>(e)]) ? 1 : 0;
-    if (n_split == 0) return false;
+    if (dec) {
+        // The device's decisions: every element's flags (ghosts holding
+        // their source's), new-node flags, face splits and counts.
+        n_split = dec->split_prefix[static_cast<size_t>(w.K)];
+        if (n_split == 0) return false;
+        for (int64_t e = 0; e < total; ++e) {
+            Elem& x = w.el[static_cast<size_t>(e)];
+            const uint8_t c = dec->code[static_cast<size_t>(e)];
+            x.refine = (c & 1u) != 0;
+            x.sigma = (c & 2u) ? 1.0 : 0.0;
+            for (size_t s = 0; s < 4; ++s) x.add[s] = dec->add[static_cast<size_t>(4 * e) + s] != 0;
+        }
+        for (int64_t f = 0; f < F; ++f) w.fa[static_cast<size_t>(f)].refine = dec->face_split[static_cast<size_t>(f)] != 0;
+    } else {
+        for (int64_t e = 0; e < w.K; ++e) n_split += w.would_h(w.el[static_cast<size_t>(e)]) ? 1 : 0;
+        if (n_split == 0) return false;
+    }
 
     // find_nodes (:5987-6014): a splitting element needs a new node on a side
     // unless a face of that side already ends at the side's midpoint.
-    for (int64_t e = 0; e < w.K; ++e) {
+    for (int64_t e = 0; !dec && e < w.K; ++e) {
         Elem& x = w.el[static_cast<size_t>(e)];
         x.add = {false, false, false, false};
         if (!w.would_h(x)) continue;
@@ -179,14 +194,14 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
         }
     }
     // copy_interfaces_error (:6054-6077), then copy_boundaries_error (:6025-6053).
-    for (size_t i = 0; i < w.if_origin.size(); ++i) {
+    for (size_t i = 0; !dec && i < w.if_origin.size(); ++i) {
         const Elem src = w.el[static_cast<size_t>(w.if_origin[i])];
         Elem& dst = w.el[static_cast<size_t>(w.if_destination[i])];
         dst.add[0] = src.add[static_cast<size_t>(w.if_origin_side[i])];
         dst.refine = src.refine;
         dst.sigma = src.sigma;
     }
-    for (int b = 0; b < 4; ++b)
+    for (int b = 0; !dec && b < 4; ++b)
         for (int64_t g : w.boundary[static_cast<size_t>(b)]) {
             Elem& dst = w.el[static_cast<size_t>(g)];
             if (dst.faces[0].size() != 1) continue;
@@ -199,8 +214,9 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
         }
     // Faces that split: a new node on the side of one of their elements and
     // both halves of the side cover part of the face (:1917-2090).
-    int64_t n_split_faces = 0;
+    int64_t n_split_faces = dec ? dec->split_face_prefix[static_cast<size_t>(F)] : 0;
     for (Face& fc : w.fa) {
+        if (dec) break;
         fc.refine = false;
         for (int side = 0; side < 2; ++side) {
             if (side == 1 && fc.refine) break;
@@ -225,10 +241,12 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
 
     // Index of a refined face's new node, or of the second half of a refined
     // face: base + number of refined faces before it.
-    const std::vector<int64_t> refined_prefix = exclusive_count(w.fa.size(), [&](size_t f) { return w.fa[f].refine; });
+    const std::vector<int64_t> refined_prefix =
+        dec ? dec->split_face_prefix : exclusive_count(w.fa.size(), [&](size_t f) { return w.fa[f].refine; });
     auto refined_before = [&](int64_t f) { return refined_prefix[static_cast<size_t>(f)]; };
     // Splitting domain elements before element j: element j moves to j + 3 * that.
-    const std::vector<int64_t> split_prefix = exclusive_count(static_cast<size_t>(w.K), [&](size_t e) { return w.would_h(w.el[e]); });
+    const std::vector<int64_t> split_prefix =
+        dec ? dec->split_prefix : exclusive_count(static_cast<size_t>(w.K), [&](size_t e) { return w.would_h(w.el[e]); });
 
     // Sizes of the new arrays (:2091-2151).
     std::array<int64_t, 4> n_split_b{};

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -367,60 +368,60 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->gplan = build_general_plan(c->topo);
         const GeneralPlan& g = c->gplan;
         c->g_eN.upload(g.eN, c->stream);
-        c->g_off2.upload(g.off2, c->stream);
-        c->g_off1.upload(g.off1, c->stream);
-        c->g_enodes.upload(g.enodes, c->stream);
-        c->g_sface_start.upload(g.sface_start, c->stream);
-        c->g_sface.upload(g.sface, c->stream);
-        c->g_corners.upload(g.corners, c->stream);
-        c->g_node_xy.upload(g.node_xy, c->stream);
+        c->g_off2.upload_reuse(g.off2, c->stream);
+        c->g_off1.upload_reuse(g.off1, c->stream);
+        c->g_enodes.upload_reuse(g.enodes, c->stream);
+        c->g_sface_start.upload_reuse(g.sface_start, c->stream);
+        c->g_sface.upload_reuse(g.sface, c->stream);
+        c->g_corners.upload_reuse(g.corners, c->stream);
+        c->g_node_xy.upload_reuse(g.node_xy, c->stream);
         c->g_fN.upload(g.fN, c->stream);
-        c->g_foff.upload(g.foff, c->stream);
-        c->g_fnodes.upload(g.fnodes, c->stream);
-        c->g_felem.upload(g.felem, c->stream);
-        c->g_fside.upload(g.fside, c->stream);
-        c->g_fnormal.upload(g.fnormal, c->stream);
-        c->g_ftangent.upload(g.ftangent, c->stream);
-        c->g_foffset.upload(g.foffset, c->stream);
-        c->g_fscale.upload(g.fscale, c->stream);
-        c->g_gkind.upload(g.gkind, c->stream);
-        c->g_gscale.upload(g.gscale, c->stream);
-        c->g_gsrc.upload(g.gsrc, c->stream);
-        c->g_gsrc_side.upload(g.gsrc_side, c->stream);
-        c->g_fbase.upload(g.fbase, c->stream);
+        c->g_foff.upload_reuse(g.foff, c->stream);
+        c->g_fnodes.upload_reuse(g.fnodes, c->stream);
+        c->g_felem.upload_reuse(g.felem, c->stream);
+        c->g_fside.upload_reuse(g.fside, c->stream);
+        c->g_fnormal.upload_reuse(g.fnormal, c->stream);
+        c->g_ftangent.upload_reuse(g.ftangent, c->stream);
+        c->g_foffset.upload_reuse(g.foffset, c->stream);
+        c->g_fscale.upload_reuse(g.fscale, c->stream);
+        c->g_gkind.upload_reuse(g.gkind, c->stream);
+        c->g_gscale.upload_reuse(g.gscale, c->stream);
+        c->g_gsrc.upload_reuse(g.gsrc, c->stream);
+        c->g_gsrc_side.upload_reuse(g.gsrc_side, c->stream);
+        c->g_fbase.upload_reuse(g.fbase, c->stream);
         c->g_fsN.upload(g.fsN, c->stream);
-        c->g_sw_off.upload(g.sw_off, c->stream);
-        c->g_sm_off.upload(g.sm_off, c->stream);
-        c->g_fw_off.upload(g.fw_off, c->stream);
-        c->g_fm_off.upload(g.fm_off, c->stream);
-        c->g_sw.allocate(static_cast<size_t>(std::max<int64_t>(g.sw_total, 1)));
-        c->g_fw.allocate(static_cast<size_t>(std::max<int64_t>(g.fw_total, 1)));
-        c->g_smatch.allocate(static_cast<size_t>(std::max<int64_t>(g.sm_total, 1)));
-        c->g_fmatch.allocate(static_cast<size_t>(std::max<int64_t>(g.fm_total, 1)));
-        c->g_pslot_start.upload(g.pslot_start, c->stream);
-        c->g_slot_desc.upload(g.slot_desc, c->stream);
-        c->g_slot_normal.upload(g.slot_normal, c->stream);
-        c->g_pside_mode.upload(g.pside_mode, c->stream);
-        c->g_slot_src.allocate(static_cast<size_t>(std::max<int64_t>(2 * g.n_slots, 1)));
-        c->g_pq_start.upload(g.pq_start, c->stream);
+        c->g_sw_off.upload_reuse(g.sw_off, c->stream);
+        c->g_sm_off.upload_reuse(g.sm_off, c->stream);
+        c->g_fw_off.upload_reuse(g.fw_off, c->stream);
+        c->g_fm_off.upload_reuse(g.fm_off, c->stream);
+        c->g_sw.reserve(static_cast<size_t>(std::max<int64_t>(g.sw_total, 1)));
+        c->g_fw.reserve(static_cast<size_t>(std::max<int64_t>(g.fw_total, 1)));
+        c->g_smatch.reserve(static_cast<size_t>(std::max<int64_t>(g.sm_total, 1)));
+        c->g_fmatch.reserve(static_cast<size_t>(std::max<int64_t>(g.fm_total, 1)));
+        c->g_pslot_start.upload_reuse(g.pslot_start, c->stream);
+        c->g_slot_desc.upload_reuse(g.slot_desc, c->stream);
+        c->g_slot_normal.upload_reuse(g.slot_normal, c->stream);
+        c->g_pside_mode.upload_reuse(g.pside_mode, c->stream);
+        c->g_slot_src.reserve(static_cast<size_t>(std::max<int64_t>(2 * g.n_slots, 1)));
+        c->g_pq_start.upload_reuse(g.pq_start, c->stream);
         c->g_pq_N.upload(g.pq_N, c->stream);
-        c->g_pq_scale.upload(g.pq_scale, c->stream);
-        c->g_pq_woff.upload(g.pq_woff, c->stream);
-        c->g_pq_moff.upload(g.pq_moff, c->stream);
-        c->g_poff2.upload(g.poff2, c->stream);
-        c->g_poff1.upload(g.poff1, c->stream);
-        c->g_pcorners.upload(g.pcorners, c->stream);
-        c->g_gq_start.upload(g.gq_start, c->stream);
-        c->g_gq_face.upload(g.gq_face, c->stream);
-        c->g_gq_fs.upload(g.gq_fs, c->stream);
-        c->g_gq_base.upload(g.gq_base, c->stream);
+        c->g_pq_scale.upload_reuse(g.pq_scale, c->stream);
+        c->g_pq_woff.upload_reuse(g.pq_woff, c->stream);
+        c->g_pq_moff.upload_reuse(g.pq_moff, c->stream);
+        c->g_poff2.upload_reuse(g.poff2, c->stream);
+        c->g_poff1.upload_reuse(g.poff1, c->stream);
+        c->g_pcorners.upload_reuse(g.pcorners, c->stream);
+        c->g_gq_start.upload_reuse(g.gq_start, c->stream);
+        c->g_gq_face.upload_reuse(g.gq_face, c->stream);
+        c->g_gq_fs.upload_reuse(g.gq_fs, c->stream);
+        c->g_gq_base.upload_reuse(g.gq_base, c->stream);
         c->g_gq_N.upload(g.gq_N, c->stream);
-        c->g_gq_woff.upload(g.gq_woff, c->stream);
-        c->g_gq_moff.upload(g.gq_moff, c->stream);
-        c->g_gframe.upload(g.gframe, c->stream);
+        c->g_gq_woff.upload_reuse(g.gq_woff, c->stream);
+        c->g_gq_moff.upload_reuse(g.gq_moff, c->stream);
+        c->g_gframe.upload_reuse(g.gframe, c->stream);
         std::vector<int64_t> ids;
         for (const auto& grp : g.groups) ids.insert(ids.end(), grp.second.begin(), grp.second.end());
-        c->g_ids.upload(ids, c->stream);
+        c->g_ids.upload_reuse(ids, c->stream);
         c->groups.clear();
         int64_t at = 0;
         for (const auto& grp : g.groups) {
@@ -446,7 +447,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
                 for (int64_t b = 0; b < og->count; b += epb) tiles.push_back(dev::QueueTile{og->N, og->first, og->count, b});
                 smem = std::max({smem, dev::general_tile_bytes(og->N, g.side_slots, false), dev::general_tile_bytes(og->N, g.side_slots, true)});
             }
-            c->g_queue.upload(tiles, c->stream);
+            c->g_queue.upload_reuse(tiles, c->stream);
             c->queue = dev::StageQueue{};
             c->queue.tiles = c->g_queue.ptr;
             c->queue.n_tiles = static_cast<int64_t>(tiles.size());
@@ -588,9 +589,110 @@ void load_mesh(ndg_ctx* c, Topology&& topo, const ndg_mesh_params& p, int32_t n_
     compute_dt_mesh(c, p.cfl);
 }
 
+// The adaptation's decisions on the device (adapt_device.cu), from the
+// estimate in ctx->refine / ctx->p_sigma (instance 0): uploads the topology
+// the kernels read, runs them and downloads their compact results.
+AdaptDecisions device_decisions(ndg_ctx* c) {
+    const Topology& t = c->topo;
+    const int64_t E = static_cast<int64_t>(t.elem_N.size()), K = t.n_domain, F = static_cast<int64_t>(t.face_N.size());
+    std::vector<int64_t> enodes(static_cast<size_t>(4 * E)), sstart(static_cast<size_t>(4 * E + 1), 0), sface;
+    for (int64_t e = 0; e < E; ++e)
+        for (size_t s = 0; s < 4; ++s) {
+            enodes[static_cast<size_t>(4 * e) + s] = t.elem_nodes[static_cast<size_t>(e)][s];
+            const auto& l = t.elem_faces[static_cast<size_t>(e)][s];
+            sface.insert(sface.end(), l.begin(), l.end());
+            sstart[static_cast<size_t>(4 * e) + s + 1] = static_cast<int64_t>(sface.size());
+        }
+    std::vector<int64_t> fnodes(static_cast<size_t>(2 * F)), felem(static_cast<size_t>(2 * F)), fside(static_cast<size_t>(2 * F));
+    for (int64_t f = 0; f < F; ++f)
+        for (size_t k = 0; k < 2; ++k) {
+            fnodes[static_cast<size_t>(2 * f) + k] = t.face_nodes[static_cast<size_t>(f)][k];
+            felem[static_cast<size_t>(2 * f) + k] = t.face_elems[static_cast<size_t>(f)][k];
+            fside[static_cast<size_t>(2 * f) + k] = t.face_sides[static_cast<size_t>(f)][k];
+        }
+    const size_t n_if = t.if_origin.size();
+    std::vector<int64_t> ifs(3 * n_if), bnd;
+    for (size_t i = 0; i < n_if; ++i) {
+        ifs[i] = t.if_origin[i];
+        ifs[n_if + i] = t.if_origin_side[i];
+        ifs[2 * n_if + i] = t.if_destination[i];
+    }
+    for (const auto& l : t.boundary) bnd.insert(bnd.end(), l.begin(), l.end());
+    std::vector<double> xy(2 * t.node_x.size());
+    for (size_t i = 0; i < t.node_x.size(); ++i) {
+        xy[2 * i] = t.node_x[i];
+        xy[2 * i + 1] = t.node_y[i];
+    }
+    const std::vector<int32_t> split(t.elem_split.begin(), t.elem_split.begin() + K);
+    c->av_split.upload_reuse(split, c->stream);
+    c->av_enodes.upload_reuse(enodes, c->stream);
+    c->av_sface_start.upload_reuse(sstart, c->stream);
+    c->av_sface.upload_reuse(sface, c->stream);
+    c->av_fnodes.upload_reuse(fnodes, c->stream);
+    c->av_felem.upload_reuse(felem, c->stream);
+    c->av_fside.upload_reuse(fside, c->stream);
+    c->av_if.upload_reuse(ifs, c->stream);
+    c->av_boundary.upload_reuse(bnd, c->stream);
+    c->av_node_xy.upload_reuse(xy, c->stream);
+    c->ad_code.reserve(static_cast<size_t>(E));
+    c->ad_add.reserve(static_cast<size_t>(4 * E));
+    c->ad_frefine.reserve(static_cast<size_t>(std::max<int64_t>(F, 1)));
+    c->ad_split_flags.reserve(static_cast<size_t>(std::max<int64_t>(K, 1)));
+    c->ad_split_prefix.reserve(static_cast<size_t>(K + 1));
+    c->ad_refined_prefix.reserve(static_cast<size_t>(F + 1));
+    c->ad_scan.reserve(static_cast<size_t>(dev::adapt_scan_scratch(std::max(K, F))));
+    dev::AdaptView v;
+    v.n_domain = K;
+    v.n_total = E;
+    v.n_faces = F;
+    v.n_interfaces = static_cast<int64_t>(n_if);
+    v.n_boundary = static_cast<int64_t>(bnd.size());
+    v.max_split = c->params.max_split_level;
+    v.split = c->av_split.ptr;
+    v.enodes = c->av_enodes.ptr;
+    v.sface_start = c->av_sface_start.ptr;
+    v.sface = c->av_sface.ptr;
+    v.fnodes = c->av_fnodes.ptr;
+    v.felem = c->av_felem.ptr;
+    v.fside = c->av_fside.ptr;
+    v.if_origin = c->av_if.ptr;
+    v.if_origin_side = c->av_if.ptr + n_if;
+    v.if_destination = c->av_if.ptr + 2 * n_if;
+    v.boundary = c->av_boundary.ptr;
+    v.node_xy = c->av_node_xy.ptr;
+    dev::AdaptOutputs o;
+    o.code = c->ad_code.ptr;
+    o.add = c->ad_add.ptr;
+    o.frefine = c->ad_frefine.ptr;
+    o.split_flags = c->ad_split_flags.ptr;
+    o.split_prefix = c->ad_split_prefix.ptr;
+    o.refined_prefix = c->ad_refined_prefix.ptr;
+    o.scan_sums = c->ad_scan.ptr;
+    check_cuda(dev::launch_adapt_decisions(v, c->refine.ptr, c->p_sigma.ptr, o, c->stream), "adaptation decision kernels");
+    c->launches += 9;
+    AdaptDecisions d;
+    d.code.resize(static_cast<size_t>(E));
+    d.add.resize(static_cast<size_t>(4 * E));
+    d.face_split.resize(static_cast<size_t>(F));
+    d.split_prefix.resize(static_cast<size_t>(K + 1));
+    d.split_face_prefix.resize(static_cast<size_t>(F + 1));
+    check_cuda(cudaMemcpyAsync(d.code.data(), o.code, d.code.size(), cudaMemcpyDeviceToHost, c->stream), "decision download");
+    check_cuda(cudaMemcpyAsync(d.add.data(), o.add, d.add.size(), cudaMemcpyDeviceToHost, c->stream), "decision download");
+    if (F > 0) check_cuda(cudaMemcpyAsync(d.face_split.data(), o.frefine, d.face_split.size(), cudaMemcpyDeviceToHost, c->stream), "decision download");
+    check_cuda(cudaMemcpyAsync(d.split_prefix.data(), o.split_prefix, d.split_prefix.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream),
+               "decision download");
+    check_cuda(cudaMemcpyAsync(d.split_face_prefix.data(), o.refined_prefix, d.split_face_prefix.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                               c->stream),
+               "decision download");
+    check_cuda(cudaStreamSynchronize(c->stream), "adaptation decisions");
+    return d;
+}
+
 // Mesh2D_t::adapt from per-element refine flags and decay rates; moves the
-// fields of a device context to the new mesh.
-void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in) {
+// fields of a device context to the new mesh. With `dec` (device contexts)
+// the flags are dec's bits and the topology rebuild takes dec's decisions
+// and counts.
+void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in, const AdaptDecisions* dec = nullptr) {
     if (std::none_of(refine_in, refine_in + ctx->topo.n_domain, [](int32_t r) { return r != 0; })) {
         // Mesh2D_t::adapt changes nothing without a refine flag
         ctx->has_error_estimate = false;
@@ -598,18 +700,22 @@ void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in) 
     }
     const std::vector<int32_t> refine(refine_in, refine_in + ctx->topo.n_domain);
     const std::vector<double> sigma(sigma_in, sigma_in + ctx->topo.n_domain);
+    const auto t_topo = std::chrono::steady_clock::now();
+    if (!dec) ctx->adapt_ms[0] = 0.0;
     const Layout before = layout_of(ctx->topo);
     Topology topo = ctx->topo;
     // Mesh2D_t::adapt: element splitting when any element splits, the
     // p-only branch otherwise.
     std::vector<ElementSource> sources;
-    const bool split = h_adapt(topo, ctx->tables, refine.data(), sigma.data(), ctx->params.maximum_N, ctx->params.max_split_level, sources);
+    const bool split = h_adapt(topo, ctx->tables, refine.data(), sigma.data(), ctx->params.maximum_N, ctx->params.max_split_level, sources, dec);
     if (!split && !p_adapt(topo, refine.data(), sigma.data(), ctx->params.maximum_N, ctx->params.max_split_level)) {
         ctx->has_error_estimate = false;
         return;
     }
     const Layout after = layout_of(topo);
     ++ctx->mesh_version;
+    const auto t_transfer = std::chrono::steady_clock::now();
+    ctx->adapt_ms[1] = std::chrono::duration<double, std::milli>(t_transfer - t_topo).count();
     if (ctx->device < 0) {
         // Host-only context: the topology alone.
         ctx->topo = std::move(topo);
@@ -690,9 +796,12 @@ void adapt_mesh(ndg_ctx* ctx, const int32_t* refine_in, const double* sigma_in) 
     ctx->q.swap(q2);
     ctx->k.swap(k2);
     if (ctx->keep_derivative) ctx->G.swap(G2);
+    const auto t_plan = std::chrono::steady_clock::now();
+    ctx->adapt_ms[2] = std::chrono::duration<double, std::milli>(t_plan - t_transfer).count();
     ctx->topo = std::move(topo);
     upload_plan(ctx, after);
     compute_dt_mesh(ctx, ctx->params.cfl);
+    ctx->adapt_ms[3] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_plan).count();
 }
 
 // Legendre-decay error estimate of every element and instance
@@ -727,15 +836,20 @@ void estimate(ndg_ctx* ctx) {
     ctx->has_error_estimate = true;
 }
 
-// Mesh2D_t::adapt from the last estimate of instance 0.
+// Mesh2D_t::adapt from the last estimate of instance 0 (or flags the caller
+// placed there): the decisions on the device, the topology rebuilt from them.
 void adapt_from_estimate(ndg_ctx* ctx) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const AdaptDecisions dec = device_decisions(ctx);
+    ctx->adapt_ms[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     const size_t K = static_cast<size_t>(ctx->K);
     std::vector<int32_t> refine(K);
     std::vector<double> sigma(K);
-    check_cuda(cudaMemcpyAsync(refine.data(), ctx->refine.ptr, K * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
-    check_cuda(cudaMemcpyAsync(sigma.data(), ctx->p_sigma.ptr, K * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "flag download");
-    check_cuda(cudaStreamSynchronize(ctx->stream), "flag download");
-    adapt_mesh(ctx, refine.data(), sigma.data());
+    for (size_t e = 0; e < K; ++e) {
+        refine[e] = dec.code[e] & 1u;
+        sigma[e] = (dec.code[e] & 2u) ? 1.0 : 0.0;  // only its comparison with 1 decides
+    }
+    adapt_mesh(ctx, refine.data(), sigma.data(), &dec);
 }
 
 void copy_table(const Tables& t, int32_t table, int32_t N, double* out, int64_t capacity, int64_t* count) {
@@ -1340,7 +1454,23 @@ ndg_status ndg_adapt_flags(ndg_ctx* ctx, const int32_t* refine, const double* p_
         if (!refine || !p_sigma) fail(NDG_ERR_INVALID_ARG, "refine and p_sigma must not be NULL");
         if (ctx->n_instances != 1) fail(NDG_ERR_UNSUPPORTED, "adaptation needs a single instance (the mesh is shared)");
         make_current(ctx);
-        adapt_mesh(ctx, refine, p_sigma);
+        if (ctx->device < 0) {
+            adapt_mesh(ctx, refine, p_sigma);  // host-only context: the topology alone, decided on the host
+            return;
+        }
+        // Device contexts take the caller's flags through the device decisions.
+        const size_t K = static_cast<size_t>(ctx->K);
+        check_cuda(cudaMemcpyAsync(ctx->refine.ptr, refine, K * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream), "flag upload");
+        check_cuda(cudaMemcpyAsync(ctx->p_sigma.ptr, p_sigma, K * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "flag upload");
+        adapt_from_estimate(ctx);
+        ctx->has_error_estimate = false;
+    });
+}
+
+ndg_status ndg_adapt_timings(const ndg_ctx* ctx, double* ms) {
+    return guarded([&] {
+        if (!ctx || !ms) fail(NDG_ERR_INVALID_ARG, "NULL argument");
+        for (int i = 0; i < 4; ++i) ms[i] = ctx->adapt_ms[i];
     });
 }
 

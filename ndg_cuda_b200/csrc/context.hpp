@@ -39,6 +39,16 @@ struct DeviceBuffer {
         allocate(std::max<size_t>(v.size(), 1));
         if (!v.empty()) check_cuda(cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "mesh upload");
     }
+    // At least n values, keeping the allocation when it is large enough
+    // (scratch reused from call to call; grows by half again when it is not).
+    void reserve(size_t n) {
+        if (n <= count && ptr) return;
+        allocate(std::max<size_t>(n + n / 2, 1));
+    }
+    void upload_reuse(const std::vector<T>& v, cudaStream_t stream) {
+        reserve(std::max<size_t>(v.size(), 1));
+        if (!v.empty()) check_cuda(cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "mesh upload");
+    }
     void allocate(size_t n) {
         release();
         if (n == 0) return;
@@ -88,6 +98,16 @@ struct ndg_ctx {
     ndg::DeviceBuffer<unsigned> error;
     ndg::DeviceBuffer<double> p_error, p_sigma;
     ndg::DeviceBuffer<int32_t> refine, coarsen;
+    // The adaptation's decisions on the device (adapt_device.cu): a copy of
+    // the topology they read, uploaded at each adaptation, and their outputs.
+    ndg::DeviceBuffer<int32_t> av_split;
+    ndg::DeviceBuffer<int64_t> av_enodes, av_sface_start, av_sface, av_fnodes, av_felem, av_fside, av_if, av_boundary;
+    ndg::DeviceBuffer<double> av_node_xy;
+    ndg::DeviceBuffer<uint8_t> ad_code, ad_add, ad_frefine, ad_split_flags;
+    ndg::DeviceBuffer<int64_t> ad_split_prefix, ad_refined_prefix, ad_scan;
+    // Host wall time of the last adaptation by phase, in ms: decisions on
+    // the device, topology rebuild, field transfer, device plan.
+    double adapt_ms[4] = {0, 0, 0, 0};
     bool has_error_estimate = false;
     int cur = 0;
     bool traces_valid = false;

@@ -4,6 +4,8 @@
 
 #include "../../include/ndg_b200.h"
 
+#include <cuda_runtime_api.h>
+
 #include <array>
 #include <cstdint>
 #include <string>
@@ -169,12 +171,55 @@ struct ElementSource {
     int kind = 0;      // 0: same order, copied; 1: new order, same points; 2: child of a split element
     std::array<double, 8> child{}, parent{};  // kind 2: corners x0, y0, ..., x3, y3 of the child and its parent
 };
+// Decisions of one adaptation computed on the device (adapt_device.cu):
+// per element (domain and ghosts) bit 0 refine and bit 1 sigma >= 1, ghosts
+// holding their source's (copy_interfaces_error, copy_boundaries_error); per
+// element side whether it gets a new node (find_nodes); per face whether it
+// splits; the exclusive counts of splitting domain elements (n_domain + 1
+// values) and of split faces (n_faces + 1 values).
+struct AdaptDecisions {
+    std::vector<uint8_t> code, add, face_split;
+    std::vector<int64_t> split_prefix, split_face_prefix;
+};
 // h-adaptation (with the p-refinement of the same pass) of the topology.
 // Returns false, leaving t untouched, when no element splits; otherwise
 // rebuilds t, recomputes its geometry and fills sources for the new domain
-// elements.
+// elements. With `dec` the new-node flags, face splits and counts are the
+// device's (refine and p_sigma then carry dec's bits); without, the host
+// computes them.
 bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level,
-             std::vector<ElementSource>& sources);
+             std::vector<ElementSource>& sources, const AdaptDecisions* dec = nullptr);
+
+namespace dev {
+// Device copy of the topology that the decisions read (adapt_device.cu).
+struct AdaptView {
+    int64_t n_domain = 0, n_total = 0, n_faces = 0, n_interfaces = 0, n_boundary = 0;
+    int max_split = 0;
+    const int* split = nullptr;               // [n_domain] split levels
+    const int64_t* enodes = nullptr;          // [4 n_total]
+    const int64_t* sface_start = nullptr;     // [4 n_total + 1]
+    const int64_t* sface = nullptr;
+    const int64_t* fnodes = nullptr;          // [2 n_faces]
+    const int64_t* felem = nullptr;
+    const int64_t* fside = nullptr;
+    const int64_t* if_origin = nullptr;       // [n_interfaces]
+    const int64_t* if_origin_side = nullptr;
+    const int64_t* if_destination = nullptr;
+    const int64_t* boundary = nullptr;        // [n_boundary] the ghosts of the four boundary lists
+    const double* node_xy = nullptr;          // [2 n_nodes]
+};
+struct AdaptOutputs {
+    uint8_t* code = nullptr;         // [n_total]
+    uint8_t* add = nullptr;          // [4 n_total]
+    uint8_t* frefine = nullptr;      // [n_faces]
+    uint8_t* split_flags = nullptr;  // [n_domain]
+    int64_t* split_prefix = nullptr;      // [n_domain + 1]
+    int64_t* refined_prefix = nullptr;    // [n_faces + 1]
+    int64_t* scan_sums = nullptr;         // [adapt_scan_scratch(max(n_domain, n_faces))]
+};
+int64_t adapt_scan_scratch(int64_t n);
+cudaError_t launch_adapt_decisions(const AdaptView& v, const int32_t* refine, const double* sigma, const AdaptOutputs& o, cudaStream_t stream);
+}  // namespace dev
 // Coordinates, in the parent's reference square, of the nodes of order N of
 // a child (Element2D_t::interpolate_from with quad_map and inverse_quad_map):
 // 2 (N+1)^2 values, node i*(N+1)+j.

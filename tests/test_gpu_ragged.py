@@ -7,7 +7,8 @@ The last CTA of a launch holds fewer elements than its tile; its copies,
 traces, fluxes and RK updates must stop at the last element, and the
 padding element between instances must never leak into a neighbour's
 fields. Bars: bit-exact in FP64_STRICT (default tile), 1e-12 relative L2
-in FP64 (every tile, bit-identical across tiles), 1e-6 in FP32.
+in FP64 (every tile; the SIMT tiles bit-identical to each other), 1e-6 in
+FP32.
 """
 from __future__ import annotations
 
@@ -67,7 +68,7 @@ def test_odd_element_counts_every_tile(res, N, kind):
                     assert rel_l2(b, -want[f]) < tol and rel_l2(c, 0.5 * want[f]) < tol, (tile, f)
             if first is None:
                 first = got
-            else:
+            elif tile < ndg.TENSOR_TILE:  # tensor-core tiles sum in another order: held to tol above
                 for f in ("p", "u", "v"):
                     assert np.array_equal(got[f], first[f]), (precision, tile, f)
         m.close()
