@@ -118,6 +118,17 @@ std::vector<int64_t> expand_side(const std::vector<Face>& fa, const std::vector<
 
 bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const double* p_sigma, int N_max, int max_split_level,
              std::vector<ElementSource>& sources, const AdaptDecisions* dec) {
+    // Splitting elements first: without one, t stays untouched.
+    int64_t n_split = 0;
+    if (dec) {
+        n_split = dec->split_prefix[static_cast<size_t>(t.n_domain)];
+    } else {
+        for (int64_t e = 0; e < t.n_domain; ++e)
+            n_split += (refine[e] != 0 && p_sigma[e] < 1.0 && t.elem_split[static_cast<size_t>(e)] < max_split_level) ? 1 : 0;
+    }
+    if (n_split == 0) return false;
+
+    // The working copy takes t's face lists (t is rebuilt at the end).
     Work w;
     w.K = t.n_domain;
     w.max_split = max_split_level;
@@ -134,7 +145,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
         x.status = t.elem_status[ei];
         x.rotation = t.elem_rotation[ei];
         x.nodes = t.elem_nodes[ei];
-        x.faces = t.elem_faces[ei];
+        x.faces = std::move(t.elem_faces[ei]);
         x.sf_zero = t.ghost_sf_zero[ei] != 0;
         if (e < w.K) {
             x.refine = refine[e] != 0;
@@ -156,12 +167,9 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
     w.if_origin_side = t.if_origin_side;
     w.if_destination = t.if_destination;
 
-    int64_t n_split = 0;
     if (dec) {
         // The device's decisions: every element's flags (ghosts holding
         // their source's), new-node flags, face splits and counts.
-        n_split = dec->split_prefix[static_cast<size_t>(w.K)];
-        if (n_split == 0) return false;
         for (int64_t e = 0; e < total; ++e) {
             Elem& x = w.el[static_cast<size_t>(e)];
             const uint8_t c = dec->code[static_cast<size_t>(e)];
@@ -170,9 +178,6 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
             for (size_t s = 0; s < 4; ++s) x.add[s] = dec->add[static_cast<size_t>(4 * e) + s] != 0;
         }
         for (int64_t f = 0; f < F; ++f) w.fa[static_cast<size_t>(f)].refine = dec->face_split[static_cast<size_t>(f)] != 0;
-    } else {
-        for (int64_t e = 0; e < w.K; ++e) n_split += w.would_h(w.el[static_cast<size_t>(e)]) ? 1 : 0;
-        if (n_split == 0) return false;
     }
 
     // find_nodes (:5987-6014): a splitting element needs a new node on a side
@@ -195,7 +200,7 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
     }
     // copy_interfaces_error (:6054-6077), then copy_boundaries_error (:6025-6053).
     for (size_t i = 0; !dec && i < w.if_origin.size(); ++i) {
-        const Elem src = w.el[static_cast<size_t>(w.if_origin[i])];
+        const Elem& src = w.el[static_cast<size_t>(w.if_origin[i])];
         Elem& dst = w.el[static_cast<size_t>(w.if_destination[i])];
         dst.add[0] = src.add[static_cast<size_t>(w.if_origin_side[i])];
         dst.refine = src.refine;
@@ -375,7 +380,18 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
             }
             ++before;
         } else {
-            Elem y = x;
+            // The element moves (its face lists are rebuilt below; the
+            // old lists are read no more).
+            Elem y;
+            y.N = x.N;
+            y.split = x.split;
+            y.status = x.status;
+            y.rotation = x.rotation;
+            y.nodes = x.nodes;
+            y.refine = x.refine;
+            y.sigma = x.sigma;
+            y.add = x.add;
+            y.sf_zero = x.sf_zero;
             ElementSource& src = sources[static_cast<size_t>(at)];
             src.old = i;
             src.kind = 0;
@@ -436,7 +452,8 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                     dst.N = N_el;
                     dst.sf_zero = false;  // resized with its geometry recomputed
                 }
-                ne[static_cast<size_t>(at)] = dst;
+                // Moved: split_faces reads only its order, flags and nodes.
+                ne[static_cast<size_t>(at)] = std::move(dst);
             }
         }
         offset += static_cast<int64_t>(list.size()) + n_split_b[static_cast<size_t>(b)];
@@ -632,11 +649,11 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
     t.elem_rotation.resize(E);
     t.ghost_sf_zero.assign(E, 0);
     for (size_t e = 0; e < E; ++e) {
-        const Elem& x = ne[e];
+        Elem& x = ne[e];
         t.elem_N[e] = x.N;
         t.elem_nodes[e] = x.nodes;
-        t.elem_faces[e] = x.faces;
-        for (size_t s = 0; s < 4; ++s) t.elem_face[e][s] = x.faces[s].empty() ? -1 : x.faces[s][0];
+        t.elem_faces[e] = std::move(x.faces);
+        for (size_t s = 0; s < 4; ++s) t.elem_face[e][s] = t.elem_faces[e][s].empty() ? -1 : t.elem_faces[e][s][0];
         t.elem_split[e] = x.split;
         t.elem_status[e] = x.status;
         t.elem_rotation[e] = x.rotation;
