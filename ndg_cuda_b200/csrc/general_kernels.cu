@@ -432,7 +432,7 @@ __device__ __forceinline__ void slot_interp(const GeneralMesh& M, const R* __res
     v[2] = div<S>(vn, den);
 }
 
-// Tile of the fused stage: FP64 arrays (the q and k tiles, element numbers
+// Tile of the fused stage: FP64 arrays (the q tile, element numbers
 // and offsets, the sides' slot ranges and flux modes) then arrays of the
 // arithmetic type R. About 128 threads per CTA: the stage's time on a small
 // order group is one CTA's dependent chain, so tiles are kept short.
@@ -445,10 +445,11 @@ struct FusedTile {
     static constexpr int kThreads = (3 * EPB * n + 31) / 32 * 32;
     static constexpr int kVals = 3 * EPB * NN;     // values of a [3][EPB][NN] field tile
     static_assert(4 * EPB < kThreads, "one thread per tile side and one more");
-    // doubles
+    // doubles (the RK register k is read from global memory in the update:
+    // a k tile here measured 3.4% slower per step, its shared memory costing
+    // a CTA per SM)
     static constexpr int kQ = 0;                   // [3][EPB][NN] q, then the new q
-    static constexpr int kK = kQ + kVals;          // [3][EPB][NN] k of the stage's input
-    static constexpr int kOff = kK + kVals;        // [EPB] field offset, [EPB] trace offset,
+    static constexpr int kOff = kQ + kVals;        // [EPB] field offset, [EPB] trace offset,
                                                    // [4 EPB + 1] first slot of each side, then the end,
                                                    // [4 EPB + 1] first mortar entry of each side, then the end (int64)
     static constexpr int kMode = kOff + 10 * EPB + 2;  // [4 EPB] side flux modes (ints)
@@ -482,7 +483,6 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
     static_assert(T::kThreads <= THREADS, "a tile needs at least its own threads");
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     double* qs = smem + T::kQ;
-    double* ks = smem + T::kK;
     int64_t* eo2 = reinterpret_cast<int64_t*>(smem + T::kOff);  // first value of the tile's elements in a field block
     int64_t* eo1 = eo2 + EPB;                                    // their first side-trace value
     int64_t* sst = eo1 + EPB;                                    // first slot of each tile side, then the end
@@ -533,14 +533,13 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
         }
     }
     __syncthreads();
-    // q and k tiles: asynchronous copies, waited for before the volume terms.
+    // q tile: asynchronous copies, waited for before the volume terms.
     for (int idx = tid; idx < T::kVals; idx += THREADS) {
         const int f = idx / (EPB * NN), r = idx - f * (EPB * NN);
         const int e = r / NN, node = r - e * NN;
         if (e < ne) {
             const int64_t gi = f * fb + eo2[e] + node;
             cp_async8(qs + idx, q + gi);
-            if (!a.first) cp_async8(ks + idx, k + gi);
         }
     }
     // Face fluxes at every face node of every side (Mesh2D_t.cpp:3803-3893,
@@ -619,7 +618,7 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
     if constexpr (T::kCopy) {
         for (int idx = tid; idx < T::kVals; idx += THREADS) qw[idx] = R(qs[idx]);
     }
-    __syncthreads();  // q and k tiles, face fluxes, J, edge metrics
+    __syncthreads();  // q tile, face fluxes, J, edge metrics
 
     // Element side fluxes (Mesh2D_t::project_to_elements, Mesh2D_t.cpp:3895-4006):
     // the face flux times the edge metric where one face of the element's
@@ -727,7 +726,7 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
         if (ee >= ne) continue;
         const int64_t gi = ff * fb + eo2[ee] + node;
         const double G = static_cast<double>(gs[idx]);
-        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, ks[idx]), G);
+        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, k[gi]), G);
         const double qn = add<S>(qs[idx], mul<S>(gdt, kn));
         k[gi] = kn;
         q[gi] = qn;
