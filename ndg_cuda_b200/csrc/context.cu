@@ -210,6 +210,7 @@ void ensure_traces(ndg_ctx* c) {
     dev::TraceArgs a{};
     a.q = c->q.ptr;
     a.trace_out = c->tr[c->cur].ptr;
+    a.link = reinterpret_cast<const int2*>(c->link.ptr);  // far-slot layout of the stage kernels
     a.n_elements = c->K;
     a.field_stride = c->Kp;
     a.n_instances = c->n_instances;

@@ -130,7 +130,8 @@ __device__ __forceinline__ bool mbar_poll(uint64_t* bar, uint64_t limit_ns) {
 }
 
 // Waits for phase 0 of an mbarrier with a CTA-wide decision; every thread of
-// the CTA calls it (it is also a __syncthreads). Each thread polls with the
+// the CTA calls it (it is also a __syncthreads), after a barrier that orders
+// the mbarrier's initialisation before every poll. Each thread polls with the
 // time limit, then the CTA gives up together if any thread timed out: the
 // error word is set, thread 0 waits once more (bounded) so that a copy that
 // was about to land is not left writing into an exited CTA, and false is
@@ -152,6 +153,9 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 // and the wait for all of this thread's copies.
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 

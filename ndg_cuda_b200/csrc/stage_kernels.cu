@@ -9,24 +9,27 @@
 //
 //   prologue  8-byte asynchronous copies (cp.async) place the tile's
 //             q = (p, u, v) in shared memory, in a padded layout free of
-//             bank conflicts (Tile, stage_common.cuh); meanwhile all
-//             threads prefetch the far-side traces of their side nodes (the
-//             neighbours' traces of the previous stage) and build J and edge
-//             metrics from the four corners
+//             bank conflicts (Tile, stage_common.cuh), and the far-side
+//             traces of its sides (the neighbours' traces of the previous
+//             stage, which they wrote into this element's far slots);
+//             meanwhile all threads build J and edge metrics from the four
+//             corners
 //   rows      bottom/top own traces
 //   columns   xi-direction flux lines (kept in registers), right/left own traces
 //   flux      upwind flux of every side node, times the edge metric
 //   xi pass   Dhat . line + lift                       -> G (columns)
 //   eta pass  eta-direction flux lines, Dhat . line + lift, then /J -> G (rows)
 //   RK        k = a k + G, q += g dt k in FP64, node by node, coalesced
-//   traces    four side traces of the new q for the next stage
+//   traces    four side traces of the new q for the next stage, written
+//             into the far slots of the neighbour across each interior side
 //
 // Work is spread as one thread per (field, line, element), 3 EPB (N+1)
 // threads per CTA, the element index fastest; shared memory carries only the
 // q tile, G, J and the side data. HBM traffic per
 // element and stage: q and k read and written (the algorithmic 32 B per
-// degree of freedom), one trace write and one neighbour-trace read of 4(N+1)
-// values per field, and 8 corner coordinates. Metrics are recomputed in
+// degree of freedom), one trace write (into the neighbours' far slots) and
+// one contiguous far-trace read of 4(N+1) values per field, and 8 corner
+// coordinates. Metrics are recomputed in
 // registers: on straight-sided quads x_xi, y_xi depend only on eta and
 // x_eta, y_eta only on xi (quad_metrics, include/functions/quad_metrics.tpp:2-7).
 //
@@ -104,7 +107,12 @@ __global__ void __launch_bounds__(256) trace_kernel_f32(TraceArgs a) {
         const int stride = (s == 0 || s == 2) ? 1 : n;
         float acc = 0.0f;
         for (int j = 0; j < n; ++j) acc = fmaf(static_cast<float>(l[j]), static_cast<float>(qe[base + j * stride]), acc);
-        a.trace_out_f[((fi * Kp + e) * 4 + s) * n + m] = acc;
+        if (a.link) {
+            const int2 lk = a.link[4 * e + s];
+            if (((lk.y >> 2) & 7) == kInterior) a.trace_out_f[((fi * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] = acc;
+        } else {
+            a.trace_out_f[((fi * Kp + e) * 4 + s) * n + m] = acc;
+        }
     }
 }
 
@@ -120,7 +128,13 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceArgs a) {
         const int64_t e = (idx / (4 * n)) % K;
         const int64_t fi = idx / (4 * n * K);  // instance * 3 + field
         const double* qf = a.q + (fi * Kp + e) * NN;
-        a.trace_out[((fi * Kp + e) * 4 + s) * n + m] = side_trace<N, S>(qf, s, m);
+        const double v = side_trace<N, S>(qf, s, m);
+        if (a.link) {
+            const int2 lk = a.link[4 * e + s];
+            if (((lk.y >> 2) & 7) == kInterior) a.trace_out[((fi * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] = v;
+        } else {
+            a.trace_out[((fi * Kp + e) * 4 + s) * n + m] = v;
+        }
     }
 }
 

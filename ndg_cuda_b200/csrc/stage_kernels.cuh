@@ -39,6 +39,10 @@ struct StageArgs {
     int n_instances;
 };
 
+// Side traces of q. With link (the side plan of the uniform stage kernels)
+// each interior side's trace goes into the far slots of the neighbour across
+// it (neighbour side lk.y & 3, node N - m), the layout the stage kernels
+// read; without, into the element's own slots [element][side][node].
 struct TraceArgs {
     const double* q;
     double* trace_out;
@@ -46,6 +50,7 @@ struct TraceArgs {
     int64_t n_elements;
     int64_t field_stride;
     int n_instances;
+    const int2* link = nullptr;
 };
 
 cudaError_t prepare_kernels(int N, bool strict);

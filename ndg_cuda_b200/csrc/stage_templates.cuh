@@ -94,18 +94,25 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
                 if (lane + 32 * it < NN) cp_async8(dst + lane_node[it], src + lane + 32 * it);
         }
     }
+    // Far traces: the previous stage wrote each neighbour's trace into this
+    // element's far slots ([field][element][side][node], 4 (N+1) contiguous
+    // values per field and element), so they arrive like the q tile, with
+    // no link to follow.
+#pragma unroll
+    for (int bi = 0; bi < T::kBlockIters; ++bi) {
+        const int b = warp + bi * T::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const double* src = tr_in + (ff * Kp + e0 + el) * 4 * n;
+            double* dst = far_s + ff * FS + el * SE;
+#pragma unroll
+            for (int it = 0; it < (4 * n + 31) / 32; ++it)
+                if (lane + 32 * it < 4 * n) cp_async8(dst + lane + 32 * it, src + lane + 32 * it);
+        }
+    }
     for (int i = tid; i < n * P; i += T::kThreads) zs[i] = 0.0;
-    // Far traces of this thread's field at node m of the four sides (the
-    // neighbour's trace of the previous stage), element metrics, edge
-    // metrics and J.
+    // Element metrics, edge metrics and J.
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const int2 lk = a.link[4 * ge + s];
-            const double v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0;
-            far_s[f * FS + e * SE + s * n + m] = v;
-        }
         const double* c = a.corners + 8 * ge;
         x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
     }
@@ -135,7 +142,7 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
         }
     }
     cp_async_wait_all();
-    __syncthreads();  // q tile, zeros, far traces, edge metrics, J
+    __syncthreads();  // q tile, far traces, zeros, edge metrics, J
 
     // Own side traces of this thread's field (Element2D_t.cpp:86-125):
     // bottom and top from row m, right and left from column m.
@@ -436,7 +443,9 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
     __syncthreads();
 
     // Side traces of the new solution for the next stage: bottom/top from
-    // row m, right/left from column m (Element2D_t.cpp:86-125).
+    // row m, right/left from column m (Element2D_t.cpp:86-125), written into
+    // the far slots of the neighbour across each interior side (its side
+    // lk.y & 3, node N - k for this side's node k; links are reciprocal).
     if (active) {
         const double* row = qs + f * QS + e * ES + m * P;
         const double* cl = qs + f * QS + e * ES + m;
@@ -448,11 +457,13 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
             r = madd<S>(r, lp[j], cl[j * P]);
             l = madd<S>(l, lm[j], cl[j * P]);
         }
-        double* to = tr_out + (f * Kp + ge) * 4 * n;
-        to[0 * n + m] = b;
-        to[2 * n + (N - m)] = t;
-        to[1 * n + m] = r;
-        to[3 * n + (N - m)] = l;
+        const double v[4] = {b, r, t, l};
+        const int at[4] = {N - m, N - m, m, m};  // N - (own node of side s)
+#pragma unroll
+        for (int sd = 0; sd < 4; ++sd) {
+            const int2 lk = a.link[4 * ge + sd];
+            if (((lk.y >> 2) & 7) == kInterior) tr_out[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + at[sd]] = v[sd];
+        }
     }
 }
 
@@ -570,17 +581,28 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
         mbar_expect_tx(bar, 3 * bytes);
         for (int ff = 0; ff < 3; ++ff) bulk_load(qs + ff * EPB * NN, q + (ff * Kp + e0) * NN, bytes, bar);
     }
+    // Far traces (written into this element's far slots by its neighbours
+    // in the previous stage): 4-byte asynchronous copies of the contiguous
+    // [field][element] blocks.
+    {
+        const int warp0 = tid >> 5, lane0 = tid & 31;
+#pragma unroll
+        for (int bi = 0; bi < Tile<N, E>::kBlockIters; ++bi) {
+            const int b = warp0 + bi * Tile<N, E>::kWarps, ff = b / EPB, el = b - ff * EPB;
+            if (b < 3 * EPB && el < ne) {
+                const float* src = tr_in + (ff * Kp + e0 + el) * 4 * n;
+                float* dst = far_s + ff * FS + el * SE;
+#pragma unroll
+                for (int it = 0; it < (4 * n + 31) / 32; ++it)
+                    if (lane0 + 32 * it < 4 * n) cp_async4(dst + lane0 + 32 * it, src + lane0 + 32 * it);
+            }
+        }
+    }
     for (int i = tid; i < n * P; i += T::kThreads) zs[i] = 0.0f;
     // Corners in FP64: their differences are formed before rounding to FP32
     // (on a fine mesh a difference is far smaller than the coordinates).
     double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
     if (active) {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const int2 lk = a.link[4 * ge + s];
-            const float v = (((lk.y >> 2) & 7) == kInterior) ? tr_in[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + (N - m)] : 0.0f;
-            far_s[f * FS + e * SE + s * n + m] = v;
-        }
         const double* c = a.corners + 8 * ge;
         x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
     }
@@ -602,6 +624,10 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
             js[e * ES + m * P + j] = __frcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
         }
     }
+    cp_async_wait_all();
+    // Every thread waits on the mbarrier only after thread 0 initialised it
+    // (polling an uninitialised mbarrier is undefined).
+    __syncthreads();
     if (!mbar_wait(bar, a.error, kWaitLimitNs)) return;  // also the barrier for zeros, far traces, edge metrics and J
     // FP32 copy of the tile in the padded layout: warps take (field,
     // element) blocks, lanes their nodes.
@@ -929,11 +955,14 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageA
             r = fmaf(lp[j], cl[j * P], r);
             l = fmaf(lm[j], cl[j * P], l);
         }
-        float* to = tr_out + (f * Kp + ge) * 4 * n;
-        to[0 * n + m] = b;
-        to[2 * n + (N - m)] = t;
-        to[1 * n + m] = r;
-        to[3 * n + (N - m)] = l;
+        // into the neighbours' far slots (as the FP64 kernel)
+        const float v[4] = {b, r, t, l};
+        const int at[4] = {N - m, N - m, m, m};
+#pragma unroll
+        for (int sd = 0; sd < 4; ++sd) {
+            const int2 lk = a.link[4 * ge + sd];
+            if (((lk.y >> 2) & 7) == kInterior) tr_out[((f * Kp + lk.x) * 4 + (lk.y & 3)) * n + at[sd]] = v[sd];
+        }
     }
 }
 
