@@ -322,13 +322,26 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
         for (int i = 0; i < n; ++i) col[i] = sub<S>(mul<S>(y_eta(xn[i]), Xe[i * P + j]), mul<S>(x_eta(xn[i]), Ye[i * P + j]));
         const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
         double* G = gs + f * QS + e * ES + j;
+        // Up to 9 outputs accumulate side by side (independent FMA chains);
+        // each output's terms are summed in the same order as one at a time.
+        constexpr int GR = n < 9 ? n : 9;
 #pragma unroll
-        for (int i = 0; i < n; ++i) {
-            double acc = 0.0;
+        for (int i0 = 0; i0 < n; i0 += GR) {
+            double acc[GR];
 #pragma unroll
-            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[i * n + mm], col[mm]);
-            const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
-            G[i * P] = -add<S>(acc, lift);
+            for (int g = 0; g < GR; ++g) acc[g] = 0.0;
+#pragma unroll
+            for (int mm = 0; mm < n; ++mm)
+#pragma unroll
+                for (int g = 0; g < GR; ++g)
+                    if (i0 + g < n) acc[g] = madd<S>(acc[g], Dh[(i0 + g) * n + mm], col[mm]);
+#pragma unroll
+            for (int g = 0; g < GR; ++g) {
+                const int i = i0 + g;
+                if (i >= n) break;
+                const double lift = S ? __ddiv_rn(add<S>(mul<S>(fr, lp[i]), mul<S>(fl3, lm[i])), w[i]) : (fr * lp[i] + fl3 * lm[i]) * iw[i];
+                G[i * P] = -add<S>(acc[g], lift);
+            }
         }
     }
     __syncthreads();
@@ -394,14 +407,25 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a
         const double ft = F[2 * n + (N - i)], fb = F[0 * n + i];
         double* G = gs + f * QS + e * ES + i * P;
         const double* jrow = js + e * ES + i * P;
+        constexpr int GR = n < 9 ? n : 9;  // outputs side by side, as in the xi pass
 #pragma unroll
-        for (int j = 0; j < n; ++j) {
-            double acc = 0.0;
+        for (int j0 = 0; j0 < n; j0 += GR) {
+            double acc[GR];
 #pragma unroll
-            for (int mm = 0; mm < n; ++mm) acc = madd<S>(acc, Dh[j * n + mm], line[mm]);
-            const double lift = S ? __ddiv_rn(add<S>(mul<S>(ft, lp[j]), mul<S>(fb, lm[j])), w[j]) : (ft * lp[j] + fb * lm[j]) * iw[j];
-            const double num = sub<S>(G[j], add<S>(acc, lift));
-            G[j] = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
+            for (int g = 0; g < GR; ++g) acc[g] = 0.0;
+#pragma unroll
+            for (int mm = 0; mm < n; ++mm)
+#pragma unroll
+                for (int g = 0; g < GR; ++g)
+                    if (j0 + g < n) acc[g] = madd<S>(acc[g], Dh[(j0 + g) * n + mm], line[mm]);
+#pragma unroll
+            for (int g = 0; g < GR; ++g) {
+                const int j = j0 + g;
+                if (j >= n) break;
+                const double lift = S ? __ddiv_rn(add<S>(mul<S>(ft, lp[j]), mul<S>(fb, lm[j])), w[j]) : (ft * lp[j] + fb * lm[j]) * iw[j];
+                const double num = sub<S>(G[j], add<S>(acc[g], lift));
+                G[j] = S ? __ddiv_rn(num, jrow[j]) : num * jrow[j];
+            }
         }
     }
     __syncthreads();
