@@ -248,12 +248,26 @@ def config1_leg(local: int, stream) -> dict:
     t_ref = o.run(200)
     out = {"workload": "dg_wave_rk3_periodic_16x16_N4_plane_wave_200_steps", "time": t_ref,
            "l2_vs_analytic": {"reference_cpu": dict(zip("puv", map(float, o.l2_error(t_ref))))}, "rel_l2_vs_reference": {}}
+    import torch
+    out["device_rate"] = {}
     for name, prec in (("fp64_strict", ndg.FP64_STRICT), ("fp64", ndg.FP64), ("fp32", ndg.FP32)):
         m = ndg.Mesh2D_t(zone, 4, cfl=CFL, device=local, stream=stream.cuda_stream, precision=prec)
         for f in ("p", "u", "v"):
             m.set_field(f, ic[f])
         t = ndg.Solver2D_t.run(m, 200)
         out["l2_vs_analytic"][name] = dict(zip("puv", map(float, m.l2_error(t))))
+        # the configuration's 200 steps timed on the device (CUDA events; the
+        # step graphs are built by the run above)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ndg.Solver2D_t.run(m, 200, t)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out["device_rate"][name] = {"ms_200_steps": ms, "value": ndg.dof_count(m) * 3 * 200 / (ms / 1e3), "unit": "DOF-stage updates/s"}
+        for f in ("p", "u", "v"):
+            m.set_field(f, ic[f])
+        ndg.Solver2D_t.run(m, 200)
         out["rel_l2_vs_reference"][name] = {f: float(np.linalg.norm(m.get_field(f) - o.field(f)) / np.linalg.norm(o.field(f)))
                                             for f in ("p", "u", "v")}
         m.close()

@@ -19,6 +19,7 @@
 
 #include "ndg_b200.h"
 
+#include <array>
 #include <cstddef>
 #include <cstdint>
 #include <filesystem>
@@ -235,6 +236,25 @@ public:
         (void)barycentric_weights;
         check(ndg_adapt(ctx_), "ndg_adapt");
         refresh_counts();
+    }
+
+    // Library-side tuning (no counterpart in the reference): the autotuner
+    // of the uniform stage kernel's tile (returns the tile kept, 0 = the
+    // default), the launch structure of mixed-order stages (0 one launch per
+    // order group, 1 one launch over the queue of every group's tiles), and
+    // the last adaptation's host wall time by phase (ms: device decisions,
+    // topology rebuild, field transfer, device plan).
+    int autotune(int n_launches = 20) {
+        int32_t tile = 0;
+        double ms = 0.0;
+        check(ndg_autotune(ctx_, n_launches, &tile, &ms), "ndg_autotune");
+        return tile;
+    }
+    void set_mixed_launch(int mode) { check(ndg_set_mixed_launch(ctx_, mode), "ndg_set_mixed_launch"); }
+    std::array<double, 4> adapt_timings() const {
+        std::array<double, 4> ms{};
+        check(ndg_adapt_timings(ctx_, ms.data()), "ndg_adapt_timings");
+        return ms;
     }
 
     // Fields of one instance (instance < 0: all instances back to back), in
