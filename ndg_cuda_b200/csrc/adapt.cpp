@@ -125,6 +125,12 @@ GeneralPlan build_general_plan(const Topology& t) {
     p.trace_total = o1;
     p.enodes.resize(static_cast<size_t>(4 * total));
     p.sface_start.assign(static_cast<size_t>(4 * total + 1), 0);
+    {
+        size_t n_entries = 0;  // the side face lists' total, so that sface grows once
+        for (const auto& sides : t.elem_faces)
+            for (const auto& list : sides) n_entries += list.size();
+        p.sface.reserve(n_entries);
+    }
     for (int64_t e = 0; e < total; ++e) {
         for (int s = 0; s < 4; ++s) {
             p.enodes[static_cast<size_t>(4 * e + s)] = t.elem_nodes[static_cast<size_t>(e)][static_cast<size_t>(s)];
@@ -249,6 +255,9 @@ GeneralPlan build_general_plan(const Topology& t) {
     // their neighbours (mirror and copy kinds).
     p.gq_start.assign(static_cast<size_t>(G + 1), 0);
     p.gframe.assign(static_cast<size_t>(4 * G), 0.0);
+    for (auto* v : {&p.gq_face, &p.gq_base, &p.gq_woff, &p.gq_moff}) v->reserve(static_cast<size_t>(G));
+    p.gq_fs.reserve(static_cast<size_t>(G));
+    p.gq_N.reserve(static_cast<size_t>(G));
     for (int64_t g = K; g < total; ++g) {
         const size_t gi = static_cast<size_t>(g - K);
         p.gq_start[gi] = static_cast<int64_t>(p.gq_face.size());
@@ -285,6 +294,22 @@ GeneralPlan build_general_plan(const Topology& t) {
     p.pslot_start.assign(static_cast<size_t>(4 * K + 1), 0);
     p.pside_mode.assign(static_cast<size_t>(4 * K), 0);
     p.pq_start.assign(static_cast<size_t>(4 * K + 1), 0);
+    {
+        // Sizes first, so that the slot and list-order arrays grow once.
+        size_t n_slots = 0;
+        for (int64_t q = 0; q < p.sface_start[static_cast<size_t>(4 * K)]; ++q)
+            n_slots += static_cast<size_t>(t.face_N[static_cast<size_t>(p.sface[static_cast<size_t>(q)])] + 1);
+        p.slot_desc.reserve(n_slots);
+        p.slot_normal.reserve(2 * n_slots);
+        const size_t n_q = static_cast<size_t>(p.sface_start[static_cast<size_t>(4 * K)]);
+        p.pq_N.reserve(n_q);
+        p.pq_scale.reserve(n_q);
+        p.pq_woff.reserve(n_q);
+        p.pq_moff.reserve(n_q);
+        p.poff2.reserve(static_cast<size_t>(K));
+        p.poff1.reserve(static_cast<size_t>(K));
+        p.pcorners.reserve(static_cast<size_t>(8 * K));
+    }
     int64_t pos = 0, slot = 0;
     for (const auto& grp : p.groups)
         for (int64_t e : grp.second) {

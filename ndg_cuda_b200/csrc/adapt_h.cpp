@@ -400,7 +400,12 @@ bool h_adapt(Topology& t, const Tables& tables, const int32_t* refine, const dou
                 y.refine = false;
                 src.kind = 1;
             }
-            for (int s = 0; s < 4; ++s) y.faces[static_cast<size_t>(s)] = expand_side(w.fa, refined_prefix, x.faces[static_cast<size_t>(s)], split_face_base);
+            for (int s = 0; s < 4; ++s) {
+                auto& list = x.faces[static_cast<size_t>(s)];
+                const bool any_split = std::any_of(list.begin(), list.end(), [&](int64_t f) { return w.fa[static_cast<size_t>(f)].refine; });
+                // A side without a split face keeps its list (moved: x is read no more).
+                y.faces[static_cast<size_t>(s)] = any_split ? expand_side(w.fa, refined_prefix, list, split_face_base) : std::move(list);
+            }
             ne[static_cast<size_t>(at)] = std::move(y);
         }
     }
