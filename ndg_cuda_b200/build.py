@@ -32,7 +32,7 @@ def _compile(src: str) -> str:
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(path), *(os.path.getmtime(os.path.join(CSRC, h)) for h in os.listdir(CSRC) if h.endswith((".hpp", ".cuh")))) \
             and os.path.getmtime(obj) >= os.path.getmtime(os.path.join(HERE, "..", "include", "ndg_b200.h")):
         return obj
-    flags = COMMON + (CUDA_FLAGS if src.endswith(".cu") else ["-x", "c++"])
+    flags = COMMON + (CUDA_FLAGS if src.endswith(".cu") else ["-x", "c++", "-Wno-deprecated-gpu-targets"])
     cmd = [NVCC] + flags + ["-c", path, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:

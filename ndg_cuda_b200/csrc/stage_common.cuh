@@ -363,6 +363,32 @@ constexpr int pow2_floor(int v) {
 }  // namespace bank
 
 // ---------------------------------------------------------------------------
+// Occupancy of the fused stage tiles. The target is as many CTAs per SM as
+// fit in 200 KB of shared memory (the rest of the SM's 256 KB stays L1 for
+// the side plan, corner and RK-register loads) and in `min_regs` registers
+// per thread, at most 32. ptxas gives these kernels about 72 registers when
+// it is free to choose; the target becomes a launch bound (bound_blocks)
+// only where its register budget (allocated in steps of 8) is below that,
+// i.e. where it raises the CTAs per SM. Measured on 256 x 256 meshes (best
+// tile per order, against the free choice everywhere): FP64 N = 4 and 6
+// 2.9% and 1.9% faster per launch, the FP32 form N = 6 7.6% and N = 10 1.2%;
+// N = 8 and 12 keep their allocation. A bound everywhere (a budget of 80
+// registers at the same 5 CTAs per SM for FP64 N = 10) lost 2.4% there.
+constexpr int occupancy_target(size_t bytes, int threads, int min_regs) {
+    const int by_smem = static_cast<int>(204800 / (bytes + 1024));
+    const int by_regs = 65536 / (min_regs * threads);
+    const int t = by_smem < by_regs ? by_smem : by_regs;
+    return t < 1 ? 1 : (t > 32 ? 32 : t);
+}
+constexpr int register_budget(int blocks, int threads) { return 65536 / (blocks * threads) / 8 * 8; }
+// The launch bound's CTAs per SM, or 0 (no bound: a zero minimum leaves
+// ptxas its free choice).
+constexpr int bound_blocks(size_t bytes, int threads, int min_regs) {
+    const int t = occupancy_target(bytes, threads, min_regs);
+    return register_budget(t, threads) < 72 ? t : 0;
+}
+
+// ---------------------------------------------------------------------------
 // Tile of the fused stage: E elements per CTA (2, 4, 8 or 16), or for E = 0
 // the default: 4 elements up to order 10, 2 above (the autotuner's choice
 // on 256 x 256 meshes at N = 4, 6, 8 and at N = 12).
@@ -391,6 +417,8 @@ struct Tile {
     static constexpr int kZ = bank::place(kS + EPB * 4, L.Z, 16);  // [n P] zeros: the absent flux component
     static constexpr int kDoubles = kZ + n * P;
     static constexpr size_t kBytes = sizeof(double) * kDoubles;
+    // CTAs per SM of the kernel's launch bound (occupancy_target; 0: none).
+    static constexpr int kMinBlocks = bound_blocks(kBytes, kThreads, 64);
     // Offset within an element of node nd = i n + j.
     __device__ static __forceinline__ int node(int nd) {
         if constexpr (P == n) {

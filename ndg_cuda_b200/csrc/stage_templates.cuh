@@ -35,7 +35,7 @@ struct TcLines {
 };
 
 template <int N, bool S, int E, bool TC = false>
-__global__ void __launch_bounds__(Tile<N, E>::kThreads) stage_kernel(StageArgs a, const __grid_constant__ Coeffs<N> cf) {
+__global__ void __launch_bounds__(Tile<N, E>::kThreads, TC ? 0 : Tile<N, E>::kMinBlocks) stage_kernel(StageArgs a, const __grid_constant__ Coeffs<N> cf) {
     static_assert(!(TC && S), "the strict form rounds every operation in the reference's order: no tensor cores");
     using T = Tile<N, E>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
@@ -523,6 +523,8 @@ struct TileF {
     static constexpr int kZ = bank::place(kS + EPB * 4, L.Z, 32);  // [n P] zeros
     static constexpr int kFloats = (kZ + n * P + 3) / 4 * 4;  // keeps the mbarrier 16-byte aligned
     static constexpr size_t kBytes = sizeof(double) * kQd + sizeof(float) * kFloats + 16;
+    // CTAs per SM of the launch bound (occupancy_target at 56 registers; 0: none)
+    static constexpr int kMinBlocks = bound_blocks(kBytes, kThreads, 56);
     // Offset within a field of node r = e NN + i n + j of the tile's elements.
     __device__ static __forceinline__ int node(int r) {
         const int el = r / NN, nd = r - el * NN;
@@ -558,7 +560,7 @@ __device__ __forceinline__ void tf32x3_mma(float (&c)[4], const float (&a)[4], c
 }
 
 template <int N, int E, bool TC = false>
-__global__ void __launch_bounds__(TileF<N, E>::kThreads) stage_kernel_f32(StageArgs a, const __grid_constant__ CoeffsF<N> cf) {
+__global__ void __launch_bounds__(TileF<N, E>::kThreads, TC ? 0 : TileF<N, E>::kMinBlocks) stage_kernel_f32(StageArgs a, const __grid_constant__ CoeffsF<N> cf) {
     using T = TileF<N, E>;
     constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
     constexpr int P = T::P, ES = T::ES, QS = T::QS, SE = T::SE, FS = T::FS;
