@@ -363,6 +363,77 @@ constexpr int pow2_floor(int v) {
 }  // namespace bank
 
 // ---------------------------------------------------------------------------
+// D-hat times a line by the even-odd decomposition (A. Solomonoff, "A fast
+// algorithm for spectral differentiation", J. Comput. Phys. 98, 1992). The
+// nodes are symmetric about 0, so D-hat is centro-antisymmetric:
+// dhat[n-1-i][n-1-j] = -dhat[i][j]. With e_j = x_j + x_{n-1-j} and
+// o_j = x_j - x_{n-1-j} (j < H = n / 2), and e_H = x_H for odd n, the part
+// of y = dhat x that is odd under reversal is A_i = sum_j ea[i][j] e_j
+// (i < H) and the even part S_i = sum_j so[i][j] o_j (i < HO = n - H); then
+// y_i = S_i + A_i and y_{n-1-i} = S_i - A_i (y_H = S_H for odd n). That is
+// H HO + HO H multiply-adds (40 at n = 9) instead of n^2 (81), and half the
+// coefficient loads. The sums round differently from the plain product, so
+// the strict form keeps the plain one. `out(i, y_i)` takes each output; the
+// pairs go in chunks of up to 5, so at most 10 accumulators are live.
+template <int n, typename R, typename Out>
+__device__ __forceinline__ void dhat_even_odd(const R* ea, const R* so, const R (&x)[n], Out&& out) {
+    constexpr int H = n / 2, HO = n - H, C = HO < 5 ? HO : 5;
+    R e[HO], o[H];
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        e[j] = x[j] + x[n - 1 - j];
+        o[j] = x[j] - x[n - 1 - j];
+    }
+    if constexpr (HO > H) e[H] = x[H];
+#pragma unroll
+    for (int i0 = 0; i0 < HO; i0 += C) {
+        R A[C], Sv[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (i0 + c < H) A[c] = ea[(i0 + c) * HO] * e[0];
+            if (i0 + c < HO) Sv[c] = so[(i0 + c) * H] * o[0];
+        }
+#pragma unroll
+        for (int j = 1; j < HO; ++j)
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                if (i0 + c < H) A[c] = fma(ea[(i0 + c) * HO + j], e[j], A[c]);
+                if (i0 + c < HO && j < H) Sv[c] = fma(so[(i0 + c) * H + j], o[j], Sv[c]);
+            }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const int i = i0 + c;
+            if (i < H) {
+                out(i, Sv[c] + A[c]);
+                out(n - 1 - i, Sv[c] - A[c]);
+            } else if (i < HO) {
+                out(i, Sv[c]);
+            }
+        }
+    }
+}
+
+// Lowest orders at which the stage kernels contract by dhat_even_odd,
+// measured per order on 256 x 256 meshes (best tile of each, against the
+// plain product). FP32 form: N = 7 to 16 gain 2-10% per launch (N = 8:
+// 135.7 -> 129.2 us), N <= 5 are even, N = 6 loses 3%. FP64 (not strict):
+// N = 11 to 16 gain 2-5%, N <= 9 are even (the FP64 kernel there is bound by
+// shared-memory traffic, not by its multiply-adds) and N = 10 loses 4.6%.
+constexpr int kEvenOddMinOrder64 = 11;
+constexpr int kEvenOddMinOrder32 = 7;
+
+// Host: the even-odd halves of an n x n D-hat (dhat_even_odd), rounded to R.
+template <typename R>
+inline void even_odd_halves(int n, const double* dhat, R* ea, R* so) {
+    const int H = n / 2, HO = n - H;
+    for (int i = 0; i < H; ++i)
+        for (int j = 0; j < HO; ++j)
+            ea[i * HO + j] = static_cast<R>(j < H ? 0.5 * (dhat[i * n + j] + dhat[i * n + n - 1 - j]) : dhat[i * n + j]);
+    for (int i = 0; i < HO; ++i)
+        for (int j = 0; j < H; ++j) so[i * H + j] = static_cast<R>(0.5 * (dhat[i * n + j] - dhat[i * n + n - 1 - j]));
+}
+
+// ---------------------------------------------------------------------------
 // Occupancy of the fused stage tiles. The target is as many CTAs per SM as
 // fit in 200 KB of shared memory (the rest of the SM's 256 KB stays L1 for
 // the side plan, corner and RK-register loads) and in `min_regs` registers
@@ -434,8 +505,15 @@ struct Tile {
 // every use is a constant-bank operand with a compile-time offset.
 template <int N>
 struct Coeffs {
-    double dhat[(N + 1) * (N + 1)];
-    double xn[N + 1], lm[N + 1], lp[N + 1], w[N + 1], iw[N + 1];
+    static constexpr int n = N + 1, H = n / 2, HO = n - n / 2;
+    double dhat[n * n];
+    double xn[n], lm[n], lp[n], w[n], iw[n];
+    double ea[H * HO], so[HO * H];  // even-odd halves of dhat (fill_even_odd)
+    // The even-odd halves of dhat used by dhat_even_odd: ea[i][j] =
+    // (dhat[i][j] + dhat[i][n-1-j]) / 2 for i < H, j < H, and ea[i][H] =
+    // dhat[i][H] for odd n; so[i][j] = (dhat[i][j] - dhat[i][n-1-j]) / 2 for
+    // i < HO, j < H.
+    void fill_even_odd() { even_odd_halves(n, dhat, ea, so); }
 };
 
 }  // namespace dev

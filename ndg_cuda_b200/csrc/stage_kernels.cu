@@ -219,6 +219,7 @@ Coeffs<N> make_coeffs() {
         c.iw[i] = h_inv_weights[static_cast<size_t>(vec_offset(N) + i)];
     }
     for (int i = 0; i < n * n; ++i) c.dhat[i] = h_dhat[static_cast<size_t>(mat_offset(N) + i)];
+    c.fill_even_odd();
     return c;
 }
 
@@ -371,6 +372,7 @@ static CoeffsF<N> make_coeffs_f() {
         c.w[i] = static_cast<float>(d.w[i]);
         c.iw[i] = static_cast<float>(d.iw[i]);
     }
+    even_odd_halves(N + 1, d.dhat, c.ea, c.so);
     return c;
 }
 

@@ -322,11 +322,16 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads, TC ? 0 : Tile<N, E>::kMi
         for (int i = 0; i < n; ++i) col[i] = sub<S>(mul<S>(y_eta(xn[i]), Xe[i * P + j]), mul<S>(x_eta(xn[i]), Ye[i * P + j]));
         const double fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
         double* G = gs + f * QS + e * ES + j;
-        // Up to 9 outputs accumulate side by side (independent FMA chains);
-        // each output's terms are summed in the same order as one at a time.
+        constexpr bool EO = !S && N >= kEvenOddMinOrder64;
+        if constexpr (EO) {
+            dhat_even_odd<n>(cf.ea, cf.so, col, [&](int i, double y) { G[i * P] = -(y + (fr * lp[i] + fl3 * lm[i]) * iw[i]); });
+        }
+        // Otherwise the plain product (in the reference's order in the strict
+        // form), up to 9 outputs accumulating side by side (independent FMA
+        // chains).
         constexpr int GR = n < 9 ? n : 9;
 #pragma unroll
-        for (int i0 = 0; i0 < n; i0 += GR) {
+        for (int i0 = 0; i0 < (EO ? 0 : n); i0 += GR) {
             double acc[GR];
 #pragma unroll
             for (int g = 0; g < GR; ++g) acc[g] = 0.0;
@@ -407,9 +412,13 @@ __global__ void __launch_bounds__(Tile<N, E>::kThreads, TC ? 0 : Tile<N, E>::kMi
         const double ft = F[2 * n + (N - i)], fb = F[0 * n + i];
         double* G = gs + f * QS + e * ES + i * P;
         const double* jrow = js + e * ES + i * P;
-        constexpr int GR = n < 9 ? n : 9;  // outputs side by side, as in the xi pass
+        constexpr bool EO = !S && N >= kEvenOddMinOrder64;
+        if constexpr (EO) {
+            dhat_even_odd<n>(cf.ea, cf.so, line, [&](int j, double y) { G[j] = (G[j] - (y + (ft * lp[j] + fb * lm[j]) * iw[j])) * jrow[j]; });
+        }
+        constexpr int GR = n < 9 ? n : 9;  // otherwise as in the xi pass
 #pragma unroll
-        for (int j0 = 0; j0 < n; j0 += GR) {
+        for (int j0 = 0; j0 < (EO ? 0 : n); j0 += GR) {
             double acc[GR];
 #pragma unroll
             for (int g = 0; g < GR; ++g) acc[g] = 0.0;
@@ -501,6 +510,7 @@ template <int N>
 struct CoeffsF {
     float dhat[(N + 1) * (N + 1)];
     float xn[N + 1], lm[N + 1], lp[N + 1], w[N + 1], iw[N + 1];
+    float ea[Coeffs<N>::H * Coeffs<N>::HO], so[Coeffs<N>::HO * Coeffs<N>::H];  // as Coeffs
 };
 
 template <int N, int E>
@@ -845,12 +855,16 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads, TC ? 0 : TileF<N, E>::k
         for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * Xe[i * P + j] - x_eta(xn[i]) * Ye[i * P + j];
         const float fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
         float* G = gs + f * QS + e * ES + j;
+        if constexpr (N >= kEvenOddMinOrder32) {
+            dhat_even_odd<n>(cf.ea, cf.so, col, [&](int i, float y) { G[i * P] = -(y + (fr * lp[i] + fl3 * lm[i]) * iw[i]); });
+        } else {
 #pragma unroll
-        for (int i = 0; i < n; ++i) {
-            float acc = 0.0f;
+            for (int i = 0; i < n; ++i) {
+                float acc = 0.0f;
 #pragma unroll
-            for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[i * n + mm], col[mm], acc);
-            G[i * P] = -(acc + (fr * lp[i] + fl3 * lm[i]) * iw[i]);
+                for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[i * n + mm], col[mm], acc);
+                G[i * P] = -(acc + (fr * lp[i] + fl3 * lm[i]) * iw[i]);
+            }
         }
     }
     __syncthreads();
@@ -923,12 +937,16 @@ __global__ void __launch_bounds__(TileF<N, E>::kThreads, TC ? 0 : TileF<N, E>::k
         const float ft = F[2 * n + (N - i)], fb = F[0 * n + i];
         float* G = gs + f * QS + e * ES + i * P;
         const float* jrow = js + e * ES + i * P;
+        if constexpr (N >= kEvenOddMinOrder32) {
+            dhat_even_odd<n>(cf.ea, cf.so, line, [&](int j, float y) { G[j] = (G[j] - (y + (ft * lp[j] + fb * lm[j]) * iw[j])) * jrow[j]; });
+        } else {
 #pragma unroll
-        for (int j = 0; j < n; ++j) {
-            float acc = 0.0f;
+            for (int j = 0; j < n; ++j) {
+                float acc = 0.0f;
 #pragma unroll
-            for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[j * n + mm], line[mm], acc);
-            G[j] = (G[j] - (acc + (ft * lp[j] + fb * lm[j]) * iw[j])) * jrow[j];
+                for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[j * n + mm], line[mm], acc);
+                G[j] = (G[j] - (acc + (ft * lp[j] + fb * lm[j]) * iw[j])) * jrow[j];
+            }
         }
     }
     __syncthreads();

@@ -32,6 +32,7 @@ template <int N>
 Coeffs<N> variant_coeffs() {
     Coeffs<N> c;
     host_coefficients(N, c.dhat, c.xn, c.lm, c.lp, c.w, c.iw);
+    c.fill_even_odd();
     return c;
 }
 
@@ -47,6 +48,7 @@ CoeffsF<N> variant_coeffs_f() {
         c.w[i] = static_cast<float>(d.w[i]);
         c.iw[i] = static_cast<float>(d.iw[i]);
     }
+    even_odd_halves(N + 1, d.dhat, c.ea, c.so);
     return c;
 }
 
