@@ -301,6 +301,7 @@ GeneralPlan build_general_plan(const Topology& t) {
             n_slots += static_cast<size_t>(t.face_N[static_cast<size_t>(p.sface[static_cast<size_t>(q)])] + 1);
         p.slot_desc.reserve(n_slots);
         p.slot_normal.reserve(2 * n_slots);
+        p.slot_side.reserve(n_slots);
         const size_t n_q = static_cast<size_t>(p.sface_start[static_cast<size_t>(4 * K)]);
         p.pq_N.reserve(n_q);
         p.pq_scale.reserve(n_q);
@@ -328,6 +329,7 @@ GeneralPlan build_general_plan(const Topology& t) {
                         p.slot_desc.push_back(32 * f + j);
                         p.slot_normal.push_back(t.face_normal[static_cast<size_t>(f)][0]);
                         p.slot_normal.push_back(t.face_normal[static_cast<size_t>(f)][1]);
+                        p.slot_side.push_back(static_cast<int32_t>(ps));
                         ++slot;
                     }
                 }

@@ -366,6 +366,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->tr[1].release();
         c->tr32[0].release();
         c->tr32[1].release();
+        if (4 * c->topo.n_domain >= (int64_t{1} << 31)) fail(NDG_ERR_UNSUPPORTED, "mixed-order meshes hold fewer than 2^29 elements");
         c->gplan = build_general_plan(c->topo);
         const GeneralPlan& g = c->gplan;
         c->g_eN.upload(g.eN, c->stream);
@@ -403,6 +404,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_slot_desc.upload_reuse(g.slot_desc, c->stream);
         c->g_slot_normal.upload_reuse(g.slot_normal, c->stream);
         c->g_pside_mode.upload_reuse(g.pside_mode, c->stream);
+        c->g_slot_side.upload_reuse(g.slot_side, c->stream);
         c->g_slot_src.reserve(static_cast<size_t>(std::max<int64_t>(2 * g.n_slots, 1)));
         c->g_pq_start.upload_reuse(g.pq_start, c->stream);
         c->g_pq_N.upload(g.pq_N, c->stream);
@@ -509,6 +511,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.slot_normal = c->g_slot_normal.ptr;
         M.slot_src = c->g_slot_src.ptr;
         M.pside_mode = c->g_pside_mode.ptr;
+        M.slot_side = c->g_slot_side.ptr;
         M.pq_start = c->g_pq_start.ptr;
         M.pq_N = c->g_pq_N.ptr;
         M.pq_scale = c->g_pq_scale.ptr;

@@ -128,7 +128,7 @@ struct ndg_ctx {
     ndg::DeviceBuffer<int32_t> g_smatch, g_fmatch;                     // mortar node matches
     ndg::DeviceBuffer<int64_t> g_pslot_start, g_slot_desc, g_slot_src;  // face-node slots of the sides, list order
     ndg::DeviceBuffer<double> g_slot_normal;
-    ndg::DeviceBuffer<int32_t> g_pside_mode;
+    ndg::DeviceBuffer<int32_t> g_pside_mode, g_slot_side;
     ndg::DeviceBuffer<int64_t> g_pq_start, g_pq_woff, g_pq_moff;        // mortar side entries, list order
     ndg::DeviceBuffer<int32_t> g_pq_N;
     ndg::DeviceBuffer<double> g_pq_scale;

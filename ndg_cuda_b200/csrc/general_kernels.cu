@@ -544,17 +544,13 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
     }
     // Face fluxes at every face node of every side (Mesh2D_t.cpp:3803-3893,
     // Solver2D_t.cpp:48-63): one item per slot of the tile's contiguous slot
-    // range, the side found by bisection of the slot starts.
+    // range; the plan names each slot's position side (slot_side).
     const int64_t g0 = sst[0];
     const int n_items = static_cast<int>(sst[4 * ne] - g0);
+    const int64_t side0 = 4 * (first + base);
     for (int idx = tid; idx < n_items; idx += THREADS) {
         const int64_t g = g0 + idx;
-        int lo = 0, hi = ne * 4;  // the side holding slot g: sst[lo] <= g < sst[lo + 1]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (sst[mid] <= g) lo = mid;
-            else hi = mid;
-        }
+        const int lo = static_cast<int>(M.slot_side[g] - side0);
         const int slot = static_cast<int>(g - sst[lo]);
         const int64_t src0 = M.slot_src[2 * g], src1 = M.slot_src[2 * g + 1];
         const R nx = R(M.slot_normal[2 * g]), ny = R(M.slot_normal[2 * g + 1]);

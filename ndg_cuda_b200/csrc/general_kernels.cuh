@@ -78,6 +78,7 @@ struct GeneralMesh {
     const double* slot_normal = nullptr;   // [2 n_slots]
     const int64_t* slot_src = nullptr;     // [2 n_slots], filled by launch_general_weights
     const int* pside_mode = nullptr;       // [4 n_domain]
+    const int* slot_side = nullptr;        // [n_slots] the position side 4 p + s owning each slot
     // Mortar sides (mode 3) in list order: side s of list position p owns
     // entries [pq_start[4 p + s], pq_start[4 p + s + 1]), one per face, with
     // the face order, the element's scaling factor on the face and the

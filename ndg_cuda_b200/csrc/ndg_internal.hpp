@@ -131,12 +131,13 @@ struct GeneralPlan {
     // concatenated lists): side s of position p owns slots
     // [pslot_start[4 p + s], pslot_start[4 p + s + 1]), running over the
     // side's faces in list order and each face's nodes; per slot the face and
-    // node as 32 f + j and the face normal (2 values). pside_mode per position
+    // node as 32 f + j, the face normal (2 values) and the position side
+    // 4 p + s that owns the slot (slot_side). pside_mode per position
     // side: 0 no face, 1 one face of the element's order from the side's
     // first to its second node, 2 the same face reversed, 3 mortar.
     std::vector<int64_t> pslot_start, slot_desc;
     std::vector<double> slot_normal;
-    std::vector<int32_t> pside_mode;
+    std::vector<int32_t> pside_mode, slot_side;
     int64_t n_slots = 0;
     // Mortar sides (mode 3) in list order: side s of position p owns face
     // entries [pq_start[4 p + s], pq_start[4 p + s + 1]), one per face in list
