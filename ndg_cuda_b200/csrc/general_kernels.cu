@@ -542,6 +542,16 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
             cp_async8(qs + idx, q + gi);
         }
     }
+    // The RK register of the tile into L2 while the stage runs (the update
+    // reads it last, after the CTA's longest chains of dependent loads).
+    if (!a.first) {
+        constexpr int kLines = (NN + 15) / 16 + 1;  // 128-byte lines an element's NN values can touch
+        for (int idx = tid; idx < 3 * ne * kLines; idx += THREADS) {
+            const int f = idx / (ne * kLines), r = idx - f * (ne * kLines);
+            const int e = r / kLines, l = r - e * kLines;
+            prefetch_l2(k + f * fb + eo2[e] + (16 * l < NN ? 16 * l : NN - 1));
+        }
+    }
     // Face fluxes at every face node of every side (Mesh2D_t.cpp:3803-3893,
     // Solver2D_t.cpp:48-63): one item per slot of the tile's contiguous slot
     // range; the plan names each slot's position side (slot_side).
