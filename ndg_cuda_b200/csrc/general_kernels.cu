@@ -165,13 +165,17 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a, int
                 const R* nv_ = nu_ + ft;
                 const double* W = M.sw + M.gq_woff[qe] + i * (Nn + 1);
                 const int* match = M.smatch + M.gq_moff[qe];
+                // Every node's loads are issued before its match decides
+                // whether it adds (the sums keep their order), so that
+                // unrolled iterations overlap their loads.
+#pragma unroll 4
                 for (int j = 0; j <= Nn; ++j) {
                     const int mt = match[j];
+                    const R w = R(W[j]), xp = np_[j], xu = nu_[j], xv = nv_[j];
                     if (mt >= 0 && mt != i) continue;
-                    const R w = R(W[j]);
-                    vp = add<S>(vp, mul<S>(mul<S>(w, np_[j]), sf));
-                    vu = add<S>(vu, mul<S>(mul<S>(w, nu_[j]), sf));
-                    vv = add<S>(vv, mul<S>(mul<S>(w, nv_[j]), sf));
+                    vp = add<S>(vp, mul<S>(mul<S>(w, xp), sf));
+                    vu = add<S>(vu, mul<S>(mul<S>(w, xu), sf));
+                    vv = add<S>(vv, mul<S>(mul<S>(w, xv), sf));
                 }
             }
             if (kind == kGhostMirror && e1 > e0) {
@@ -651,8 +655,8 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
                 const int* match = M.smatch + M.pq_moff[qq];
                 for (int j = 0; j <= Nf; ++j) {
                     const int mt = match[j];
+                    const R w = R(W[j]);  // loaded with the match (the sums keep their order)
                     if (mt >= 0 && mt != i) continue;
-                    const R w = R(W[j]);
 #pragma unroll
                     for (int c = 0; c < 3; ++c) out[c] = add<S>(out[c], mul<S>(mul<S>(mul<S>(w, fl[c * FFS + slot0 + j]), sfv), scale));
                 }
