@@ -5,6 +5,7 @@
     python -m ndg_cuda_b200.cases adjoint --res 96 --order 7 --steps 20 --interval 10 [--fp32]
     python -m ndg_cuda_b200.cases mixed   --res 128 --order 4 --rounds 3 --steps 2
     python -m ndg_cuda_b200.cases tiles   --res 256 --order 8 [--fp32]
+    python -m ndg_cuda_b200.cases hp      --res 128 --order 4 --steps 600 [--fp32]
 
 `stage`: the reference plane wave on a periodic res x res mesh (RK3 steps).
 `batched`: independent radial pulses on one walled mesh, one launch per stage.
@@ -17,6 +18,12 @@ order 4 and 3 rounds), then steps on the mixed-order path.
 of the stage kernel (SIMT and tensor-core codes) and the default, timed by
 CUDA events (best of the second and third RK stages, two rounds, 20 launches
 each); one line per tile in µs per launch.
+`hp`: the hp-adaptive refining run (walled res x res mesh, interior nodes
+jittered by 0.1 h with seed 7, orders up to 12, two split levels, the
+Legendre-decay estimate and adapt every 20 steps at threshold 1e-9, two
+crossing pulses) for `steps` steps; then the final mesh's stage time by
+CUDA events on a stream of its own, and 3 steps inside a profiler range
+(cudaProfilerStart/Stop: `ncu --profile-from-start off` captures only them).
 Inputs are the seeded synthetic ones of ndg_cuda_b200.workloads.
 """
 from __future__ import annotations
@@ -35,7 +42,7 @@ def _zone(res: int, **kw) -> dict:
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("case", choices=["stage", "batched", "adjoint", "mixed", "tiles"])
+    ap.add_argument("case", choices=["stage", "batched", "adjoint", "mixed", "tiles", "hp"])
     ap.add_argument("--res", type=int, default=64)
     ap.add_argument("--order", type=int, default=6)
     ap.add_argument("--steps", type=int, default=3)
@@ -99,6 +106,37 @@ def main(argv=None) -> None:
                 Solver2D_t.run(mesh, args.time)
                 mesh.synchronize()
                 print(f"launch mode {args.launch}: {1e3 * (time.perf_counter() - t0) / args.time:.4f} ms per RK3 step")
+    elif args.case == "hp":
+        import torch
+        zone = meshgen.uniform_zone(args.res, boundary=meshgen.WALL, jitter=0.1, seed=7)
+        stream = torch.cuda.Stream()
+        mesh = Mesh2D_t(zone, args.order, maximum_N=12, max_split_level=2, tolerance_min=1e-9, tolerance_max=1e-14, cfl=0.5,
+                        stream=stream.cuda_stream, precision=prec)
+        k1, k2 = np.array([1.0, 1.0]) / np.sqrt(2), np.array([-1.0, 1.0]) / np.sqrt(2)
+        pa = workloads.gaussian_pulse(zone, args.order, sigma=0.1, centre=(-0.4, -0.4))
+        pb = workloads.gaussian_pulse(zone, args.order, sigma=0.1, centre=(0.4, -0.4))
+        mesh.set_field("p", pa + pb)
+        mesh.set_field("u", k1[0] * pa + k2[0] * pb)
+        mesh.set_field("v", k1[1] * pa + k2[1] * pb)
+        for _ in range(args.steps // 20):
+            Solver2D_t.run(mesh, 20)
+            mesh.estimate_error()
+            e = mesh.error()
+            mesh.adapt(e["refine"], e["p_sigma"])
+        N = mesh.elements()["N"][:mesh.n_elements_]
+        print("final mesh:", mesh.n_elements_, "elements, orders", {int(k): int(c) for k, c in zip(*np.unique(N, return_counts=True))})
+        Solver2D_t.run(mesh, 0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            e0.record(stream)
+            Solver2D_t.run(mesh, 20)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            print(f"final mesh: {1e3 * e0.elapsed_time(e1) / 60:.1f} us per RK stage")
+        torch.cuda.profiler.start()
+        Solver2D_t.run(mesh, 3)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
     else:
         zone = _zone(args.res, boundary=meshgen.WALL)
         c = workloads.speed_field(zone, seed=0)
