@@ -23,7 +23,7 @@ CUDA_FLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr", "-Xptxas", "-v"] i
 
 SOURCES = ["tables.cpp", "topology.cpp", "adapt.cpp", "adapt_h.cpp", "stage_kernels.cu", "general_kernels.cu", "estimator.cu", "context.cu",
            "adjoint_kernels.cu", "adjoint_host.cu", "stage_variants_fp64.cu", "stage_variants_fp32.cu", "stage_variants_tc64.cu", "stage_variants_tc32.cu",
-           "delta_t_scratch.cu", "adapt_device.cu", "output.cu", "output_host.cu", "writer.cpp"]
+           "delta_t_scratch.cu", "adapt_device.cu", "conforming_kernels.cu", "output.cu", "output_host.cu", "writer.cpp"]
 
 
 def _compile(src: str) -> str:

@@ -203,6 +203,49 @@ GeneralPlan build_general_plan(const Topology& t) {
         const auto& fn = t.face_nodes[static_cast<size_t>(f)];
         return t.face_N[static_cast<size_t>(f)] == t.elem_N[static_cast<size_t>(e)] && (left ? (fn[0] == a && fn[1] == b) : (fn[1] == a && fn[0] == b));
     };
+    // Conforming elements (conforming_stage_kernel): on each side one face
+    // of the element's order from the side's first to its second node (or
+    // reversed, for the face's right element), whose other element (a domain
+    // element or a ghost) sees it the same way. Where they are at least half
+    // of their order group they go last in it (the rest, whose tiles take
+    // longest, first) and form a group of their own at run time; elsewhere
+    // the group keeps its order and runs as one.
+    auto conforming_side = [&](int64_t e, int s, int64_t& nb, int32_t& role, int64_t& face) {
+        const auto& list = t.elem_faces[static_cast<size_t>(e)][static_cast<size_t>(s)];
+        if (list.size() != 1) return false;
+        const int64_t f = list[0];
+        const auto& fe = t.face_elems[static_cast<size_t>(f)];
+        const auto& fs = t.face_sides[static_cast<size_t>(f)];
+        const bool left = fe[0] == e && fs[0] == s, right = fe[1] == e && fs[1] == s;
+        if (left == right) return false;
+        const size_t oi = left ? 1 : 0;
+        const int64_t o = fe[oi], os = fs[oi];
+        if (o >= K && os != 0) return false;  // a ghost's only trace is its side 0
+        if (!conforming(f, e, s, left) || !conforming(f, o, os, !left)) return false;
+        nb = p.off1[static_cast<size_t>(o)] + os * (t.elem_N[static_cast<size_t>(o)] + 1);
+        role = left ? 0 : 1;
+        face = f;
+        return true;
+    };
+    std::vector<char> conf(static_cast<size_t>(K), 0);
+    for (int64_t e = 0; e < K; ++e) {
+        bool ok = true;
+        for (int s = 0; s < 4 && ok; ++s) {
+            int64_t nb, face;
+            int32_t role;
+            ok = conforming_side(e, s, nb, role, face);
+        }
+        conf[static_cast<size_t>(e)] = ok ? 1 : 0;
+    }
+    p.group_conforming.assign(p.groups.size(), 0);
+    for (size_t gi = 0; gi < p.groups.size(); ++gi) {
+        auto& list = p.groups[gi].second;
+        int64_t nconf = 0;
+        for (int64_t e : list) nconf += conf[static_cast<size_t>(e)];
+        if (2 * nconf < static_cast<int64_t>(list.size())) continue;
+        std::stable_partition(list.begin(), list.end(), [&](int64_t e) { return conf[static_cast<size_t>(e)] == 0; });
+        p.group_conforming[gi] = nconf;
+    }
     for (int64_t e = 0; e < K; ++e)
         for (int s = 0; s < 4; ++s) {
             int64_t slots = 0;
@@ -308,6 +351,9 @@ GeneralPlan build_general_plan(const Topology& t) {
         p.pq_woff.reserve(n_q);
         p.pq_moff.reserve(n_q);
         p.poff2.reserve(static_cast<size_t>(K));
+        p.cnb.reserve(static_cast<size_t>(4 * K));
+        p.crole.reserve(static_cast<size_t>(4 * K));
+        p.cnormal.reserve(static_cast<size_t>(8 * K));
         p.poff1.reserve(static_cast<size_t>(K));
         p.pcorners.reserve(static_cast<size_t>(8 * K));
     }
@@ -319,6 +365,13 @@ GeneralPlan build_general_plan(const Topology& t) {
             p.poff1.push_back(p.off1[static_cast<size_t>(e)]);
             p.pcorners.insert(p.pcorners.end(), p.corners.begin() + 8 * e, p.corners.begin() + 8 * e + 8);
             for (int s = 0; s < 4; ++s) {
+                int64_t nb = 0, face = -1;
+                int32_t role = 0;
+                if (!conf[static_cast<size_t>(e)] || !conforming_side(e, s, nb, role, face)) nb = 0, role = 0, face = -1;
+                p.cnb.push_back(nb);
+                p.crole.push_back(role);
+                p.cnormal.push_back(face >= 0 ? t.face_normal[static_cast<size_t>(face)][0] : 0.0);
+                p.cnormal.push_back(face >= 0 ? t.face_normal[static_cast<size_t>(face)][1] : 0.0);
                 const size_t ps = static_cast<size_t>(4 * pos + s);
                 p.pslot_start[ps] = slot;
                 p.pq_start[ps] = static_cast<int64_t>(p.pq_N.size());

@@ -105,18 +105,23 @@ dev::GeneralStage general_args(ndg_ctx* c, int m, int in) {
 
 // Kernel launches of one stage of the general path: ghost traces, then the
 // fused stage of every order group.
+bool fp32(const ndg_ctx* c) { return c->precision == NDG_FP32; }
+
+// The order groups a stage launches: in the FP32 form, which has no
+// conforming kernel, one per order.
+const std::vector<dev::OrderGroup>& stage_groups(const ndg_ctx* c) { return fp32(c) ? c->whole_groups : c->groups; }
+
 int64_t general_stage_launches(const ndg_ctx* c) {
     const int64_t ghosts = c->gmesh.n_total > c->gmesh.n_domain ? 1 : 0;
     if (c->mixed_launch == 1) return (c->queue.n_tiles > 0 ? 1 : 0) + ghosts;
-    return static_cast<int64_t>(c->groups.size()) + ghosts;
+    return static_cast<int64_t>(stage_groups(c).size()) + ghosts;
 }
-
-bool fp32(const ndg_ctx* c) { return c->precision == NDG_FP32; }
 
 // Side streams and events for the concurrent order groups (created once,
 // before any capture).
 void ensure_aux_streams(ndg_ctx* c) {
-    const size_t want = c->groups.size() > 1 ? c->groups.size() - 1 : 0;
+    const size_t most = std::max(c->groups.size(), c->whole_groups.size());
+    const size_t want = most > 1 ? most - 1 : 0;
     while (c->aux_streams.size() < want) {
         cudaStream_t st;
         check_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -136,16 +141,23 @@ cudaError_t issue_general_stage(ndg_ctx* c, int m, int in) {
     const dev::GeneralStage a = general_args(c, m, in);
     cudaError_t err = dev::launch_general_ghosts(a, strict(c), fp32(c), c->stream);
     if (c->mixed_launch == 1) return err == cudaSuccess ? dev::launch_general_queue(a, c->queue, strict(c), fp32(c), c->stream) : err;
-    const size_t G = c->groups.size();
+    const std::vector<dev::OrderGroup>& groups = stage_groups(c);
+    const size_t G = groups.size();
     if (err != cudaSuccess || G == 0) return err;
+    // Group 0 goes before the forks in the FP64 forms and after them in the
+    // FP32 form: the order in which the branches reach the GPU changes how
+    // their CTAs share the SMs, and these were the faster orders on the
+    // hp-adaptive and the mixed p-adapted meshes.
+    const bool first0 = !fp32(c);
     if (G > 1 && (err = cudaEventRecord(c->aux_events[0], c->stream)) != cudaSuccess) return err;
+    if (first0 && (err = dev::launch_general_group(a, groups[0], strict(c), fp32(c), c->stream)) != cudaSuccess) return err;
     for (size_t g = 1; g < G && err == cudaSuccess; ++g) {
         cudaStream_t st = c->aux_streams[g - 1];
         if ((err = cudaStreamWaitEvent(st, c->aux_events[0], 0)) != cudaSuccess) break;
-        if ((err = dev::launch_general_group(a, c->groups[g], strict(c), fp32(c), st)) != cudaSuccess) break;
+        if ((err = dev::launch_general_group(a, groups[g], strict(c), fp32(c), st)) != cudaSuccess) break;
         err = cudaEventRecord(c->aux_events[g], st);
     }
-    if (err == cudaSuccess) err = dev::launch_general_group(a, c->groups[0], strict(c), fp32(c), c->stream);
+    if (!first0 && err == cudaSuccess) err = dev::launch_general_group(a, groups[0], strict(c), fp32(c), c->stream);
     for (size_t g = 1; g < G && err == cudaSuccess; ++g) err = cudaStreamWaitEvent(c->stream, c->aux_events[g], 0);
     return err;
 }
@@ -202,8 +214,9 @@ void ensure_traces(ndg_ctx* c) {
     if (c->general) {
         require_form(c);
         dev::GeneralStage g = general_args(c, 0, c->cur);
-        check_cuda(dev::launch_general_traces(g, c->groups.data(), static_cast<int>(c->groups.size()), strict(c), fp32(c), c->stream), "trace kernel launch");
-        c->launches += static_cast<int64_t>(c->groups.size());
+        check_cuda(dev::launch_general_traces(g, c->whole_groups.data(), static_cast<int>(c->whole_groups.size()), strict(c), fp32(c), c->stream),
+                   "trace kernel launch");
+        c->launches += static_cast<int64_t>(c->whole_groups.size());
         c->traces_valid = true;
         return;
     }
@@ -359,6 +372,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         check_cuda(dev::prepare_kernels(c->N, false), "kernel attributes");
         check_cuda(dev::prepare_kernels(c->N, true), "kernel attributes");
         c->groups.clear();
+        c->whole_groups.clear();
     } else {
         for (int Ne : c->topo.elem_N)
             if (Ne < 1 || Ne > kMaxOrder) fail(NDG_ERR_UNSUPPORTED, "element orders must lie in 1..16");
@@ -405,6 +419,9 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_slot_normal.upload_reuse(g.slot_normal, c->stream);
         c->g_pside_mode.upload_reuse(g.pside_mode, c->stream);
         c->g_slot_side.upload_reuse(g.slot_side, c->stream);
+        c->g_cnb.upload_reuse(g.cnb, c->stream);
+        c->g_crole.upload_reuse(g.crole, c->stream);
+        c->g_cnormal.upload_reuse(g.cnormal, c->stream);
         c->g_slot_src.reserve(static_cast<size_t>(std::max<int64_t>(2 * g.n_slots, 1)));
         c->g_pq_start.upload_reuse(g.pq_start, c->stream);
         c->g_pq_N.upload(g.pq_N, c->stream);
@@ -425,23 +442,41 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         std::vector<int64_t> ids;
         for (const auto& grp : g.groups) ids.insert(ids.end(), grp.second.begin(), grp.second.end());
         c->g_ids.upload_reuse(ids, c->stream);
+        // Where most of an order's elements are conforming (the plan lists
+        // them last), they and the rest are groups of their own, run by their
+        // own kernels as concurrent branches; the rest, latency-bound on
+        // their dependent loads, come first in the list. Where few are, the split
+        // only adds a branch beside the fused launch (measured slower), and
+        // the order stays one group (group_conforming 0). The FP32 form, which
+        // has no conforming kernel, runs one group per order.
         c->groups.clear();
+        c->whole_groups.clear();
+        std::vector<dev::OrderGroup> conforming_parts;
         int64_t at = 0;
-        for (const auto& grp : g.groups) {
+        for (size_t gi = 0; gi < g.groups.size(); ++gi) {
+            const int64_t total = static_cast<int64_t>(g.groups[gi].second.size()), nconf = g.group_conforming[gi];
             dev::OrderGroup og;
-            og.N = grp.first;
-            og.count = static_cast<int64_t>(grp.second.size());
+            og.N = g.groups[gi].first;
             og.ids = c->g_ids.ptr + at;
             og.first = at;
-            at += og.count;
-            c->groups.push_back(og);
-            check_cuda(dev::prepare_general_kernels(og.N, g.side_slots), "kernel attributes");
+            og.count = total;
+            if (total > 0) c->whole_groups.push_back(og);
+            og.count = total - nconf;
+            if (og.count > 0) c->groups.push_back(og);
+            og.ids += total - nconf;
+            og.first += total - nconf;
+            og.count = nconf;
+            og.conforming = 1;
+            if (nconf > 0) conforming_parts.push_back(og);
+            at += total;
+            check_cuda(dev::prepare_general_kernels(g.groups[gi].first, g.side_slots), "kernel attributes");
         }
+        c->groups.insert(c->groups.end(), conforming_parts.begin(), conforming_parts.end());
         // The stage queue: the groups' tiles, largest order first, and the
         // shared memory of the largest tile in either form.
         {
             std::vector<const dev::OrderGroup*> by_N;
-            for (const auto& og : c->groups) by_N.push_back(&og);
+            for (const auto& og : c->whole_groups) by_N.push_back(&og);
             std::stable_sort(by_N.begin(), by_N.end(), [](const dev::OrderGroup* x, const dev::OrderGroup* y) { return x->N > y->N; });
             std::vector<dev::QueueTile> tiles;
             size_t smem = 0;
@@ -512,6 +547,9 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.slot_src = c->g_slot_src.ptr;
         M.pside_mode = c->g_pside_mode.ptr;
         M.slot_side = c->g_slot_side.ptr;
+        M.cnb = c->g_cnb.ptr;
+        M.crole = c->g_crole.ptr;
+        M.cnormal = c->g_cnormal.ptr;
         M.pq_start = c->g_pq_start.ptr;
         M.pq_N = c->g_pq_N.ptr;
         M.pq_scale = c->g_pq_scale.ptr;

@@ -129,6 +129,9 @@ struct ndg_ctx {
     ndg::DeviceBuffer<int64_t> g_pslot_start, g_slot_desc, g_slot_src;  // face-node slots of the sides, list order
     ndg::DeviceBuffer<double> g_slot_normal;
     ndg::DeviceBuffer<int32_t> g_pside_mode, g_slot_side;
+    ndg::DeviceBuffer<int64_t> g_cnb;  // conforming position sides: neighbour trace base, role, face normal
+    ndg::DeviceBuffer<int32_t> g_crole;
+    ndg::DeviceBuffer<double> g_cnormal;
     ndg::DeviceBuffer<int64_t> g_pq_start, g_pq_woff, g_pq_moff;        // mortar side entries, list order
     ndg::DeviceBuffer<int32_t> g_pq_N;
     ndg::DeviceBuffer<double> g_pq_scale;
@@ -137,7 +140,8 @@ struct ndg_ctx {
     ndg::DeviceBuffer<int64_t> g_gq_start, g_gq_face, g_gq_base, g_gq_woff, g_gq_moff;  // ghost side-0 gathers
     ndg::DeviceBuffer<int32_t> g_gq_fs, g_gq_N;
     ndg::DeviceBuffer<double> g_gframe;
-    std::vector<ndg::dev::OrderGroup> groups;
+    std::vector<ndg::dev::OrderGroup> groups;        // FP64 forms: mostly-conforming orders split (conforming parts last)
+    std::vector<ndg::dev::OrderGroup> whole_groups;  // one group per order: the FP32 form and the stage queue
     ndg::dev::GeneralMesh gmesh;
     // Mixed-order stages: one launch per order group as concurrent graph
     // branches (mixed_launch 0, the default), or one launch per stage over

@@ -19,6 +19,11 @@
 //                  (Solver2D_t.cpp:138-172) and the side traces of the new
 //                  state for the next stage (Element2D_t.cpp:86-125)
 //
+// Each order group's conforming elements (one same-order face per side,
+// shared with a same-order neighbour) come first in the plan's lists and run
+// conforming_stage_kernel (conforming_kernels.cu) instead of the fused
+// stage; the two parts are separate groups and concurrent branches.
+//
 // The mortar weights of the plan are computed once (side_weights_kernel,
 // face_weights_kernel). A face's flux is evaluated by each of its two
 // elements, with the same operations, so both see the same value.
@@ -1023,6 +1028,8 @@ cudaError_t upload_general_tables(const Tables& t) {
 }
 
 cudaError_t prepare_general_kernels(int N, int side_slots) {
+    const cudaError_t err = prepare_conforming_kernels(N);
+    if (err != cudaSuccess) return err;
     return by_order(N, [&](auto c) { return set_attrs<decltype(c)::value>(side_slots); });
 }
 
@@ -1052,6 +1059,7 @@ cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, bool fp32,
 
 cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream) {
     if (g.count == 0) return cudaSuccess;
+    if (g.conforming && !fp32) return launch_conforming_group(a, g, strict, stream);
     return by_order(g.N, [&](auto c) {
         constexpr int N = decltype(c)::value;
         if (fp32) return launch_fused<N, false, float>(a, g, stream);

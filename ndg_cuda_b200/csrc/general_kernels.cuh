@@ -79,6 +79,12 @@ struct GeneralMesh {
     const int64_t* slot_src = nullptr;     // [2 n_slots], filled by launch_general_weights
     const int* pside_mode = nullptr;       // [4 n_domain]
     const int* slot_side = nullptr;        // [n_slots] the position side 4 p + s owning each slot
+    // Conforming position sides (conforming_stage_kernel): the first trace
+    // value of the neighbour's side, 1 when the element is the face's right
+    // element, and the face normal.
+    const int64_t* cnb = nullptr;          // [4 n_domain]
+    const int* crole = nullptr;            // [4 n_domain]
+    const double* cnormal = nullptr;       // [8 n_domain]
     // Mortar sides (mode 3) in list order: side s of list position p owns
     // entries [pq_start[4 p + s], pq_start[4 p + s + 1]), one per face, with
     // the face order, the element's scaling factor on the face and the
@@ -129,6 +135,7 @@ struct OrderGroup {
     int64_t count = 0;
     const int64_t* ids = nullptr;  // device, element numbers
     int64_t first = 0;             // list position of the group's first element
+    int conforming = 0;            // 1: every side one same-order face with a same-order neighbour (conforming_stage_kernel)
 };
 
 // The stage queue of a mixed-order mesh: every tile of every order group
@@ -171,6 +178,11 @@ int general_tile_elements(int N);
 cudaError_t prepare_general_queue(size_t smem_bytes);
 // The fused stage of every order group in one launch (after the ghosts).
 cudaError_t launch_general_queue(const GeneralStage& a, const StageQueue& wq, bool strict, bool fp32, cudaStream_t stream);
+// Stage kernel of a group of conforming elements (conforming_kernels.cu):
+// the uniform-order stage with the neighbour traces gathered by the plan.
+// FP64 only; the FP32 form runs such groups through the general kernel.
+cudaError_t prepare_conforming_kernels(int N);
+cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, cudaStream_t stream);
 // The plane-wave initial condition at every node of a mixed-order mesh.
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream);
 

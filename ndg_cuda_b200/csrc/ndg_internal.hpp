@@ -113,6 +113,18 @@ struct GeneralPlan {
     std::vector<int64_t> gsrc;
     std::vector<int32_t> gsrc_side;
     std::vector<std::pair<int, std::vector<int64_t>>> groups;  // order, its domain elements
+    // Per group, how many of its last elements are conforming and run the
+    // conforming stage kernel (0 where they are fewer than half the group,
+    // which then keeps its order): on each side one face of the element's
+    // order whose nodes are the side's, shared with a neighbour (or ghost) of
+    // the same order. Per position side: the first
+    // trace value of the neighbour's side, 1 when the element is the face's
+    // right element, the face normal (2 values); meaningful for conforming
+    // positions only.
+    std::vector<int64_t> group_conforming;
+    std::vector<int64_t> cnb;
+    std::vector<int32_t> crole;
+    std::vector<double> cnormal;
     // Mortar weights, filled on the device once per plan. Per entry of
     // sface on a domain element side that is not one conforming face of the
     // element's order: offsets of its (N_e+1) x (N_f+1) projection weights
