@@ -10,16 +10,21 @@
 // gathered into it (each side's trace base comes from the plan), the upwind
 // flux, both contraction passes, the RK update and the new side traces into
 // the element's own trace slots, which the general kernels and the ghost
-// kernel read. The plan lists these elements first in each order group; the
-// rest of the group runs general_fused_kernel.
+// kernel read. Where they are at least half of an order group the plan
+// lists them last in it and they run here as a group of their own; the rest
+// of the group runs general_fused_kernel.
 //
 // Every value is computed with the operations, in the order, of the general
 // kernel's conforming branches, so STRICT instantiations reproduce the
 // reference's CPU results bit for bit; the default form contracts by the
 // even-odd decomposition where the uniform kernels do (kEvenOddMinOrder64).
+// The FP32 form (conforming_stage_kernel_f32) follows the uniform FP32
+// kernel: traces, fluxes and the volume term in FP32 over FP32 trace
+// buffers, q, k and the RK update in FP64.
 #include "general_kernels.cuh"
 #include "stage_common.cuh"
 #include "stage_kernels.cuh"
+#include "stage_templates.cuh"
 
 #include <cuda_runtime.h>
 
@@ -314,6 +319,252 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
     }
 }
 
+// FP32 form. The FP64 q tile arrives unpadded by 8-byte copies (warps over
+// (field, element) blocks, as above) and each thread converts the values it
+// copied into the padded FP32 tile once its own copies have landed.
+template <int N>
+__global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks)
+    conforming_stage_kernel_f32(GeneralStage a, OrderGroup grp, const __grid_constant__ CoeffsF<N> cf) {
+    using T = TileF<N, 0>;
+    using U = Tile<N, 0>;
+    constexpr int n = T::n, NN = T::NN, EPB = T::EPB;
+    constexpr int P = T::P, ES = T::ES, QS = T::QS, SE = T::SE, FS = T::FS;
+    extern __shared__ __align__(128) double smem[];
+    double* qs = smem;  // [3][EPB][NN] FP64 q, unpadded
+    float* fsm = reinterpret_cast<float*>(smem + T::kQd);
+    float* qf = fsm + T::kQf;
+    float* gs = fsm + T::kG;
+    float* own_s = fsm + T::kOwn;
+    float* far_s = fsm + T::kFar;
+    float* js = fsm + T::kJ;
+    float* ss = fsm + T::kS;
+    float* zs = fsm + T::kZ;
+
+    const GeneralMesh& M = a.m;
+    const int tid = threadIdx.x;
+    const int64_t base = static_cast<int64_t>(blockIdx.x) * EPB;
+    const int64_t p0 = grp.first + base;
+    const int ne = static_cast<int>((grp.count - base) < EPB ? (grp.count - base) : EPB);
+    const int64_t inst = blockIdx.y;
+    const int64_t fb = M.block, ft = M.trace_total;
+    double* q = a.q + inst * 3 * fb;
+    double* k = a.k + inst * 3 * fb;
+    const float* tr_in = a.etr_f + inst * 3 * ft;
+    float* tr_out = a.etr_out_f + inst * 3 * ft;
+    const float* xn = cf.xn;
+    const float* lm = cf.lm;
+    const float* lp = cf.lp;
+    const double dt = a.step[1];
+
+    const int f = tid / (EPB * n);
+    const int rr = tid - f * (EPB * n);
+    const int m = rr / EPB;
+    const int e = rr - m * EPB;
+    const bool active = f < 3 && e < ne;
+    const int64_t pe = p0 + e;
+
+    const int warp = tid >> 5, lane = tid & 31;
+    int lane_node[U::kLaneIters];
+#pragma unroll
+    for (int it = 0; it < U::kLaneIters; ++it) lane_node[it] = T::node(lane + 32 * it);
+#pragma unroll
+    for (int bi = 0; bi < U::kBlockIters; ++bi) {
+        const int b = warp + bi * U::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const double* src = q + ff * fb + M.poff2[p0 + el];
+#pragma unroll
+            for (int it = 0; it < U::kLaneIters; ++it)
+                if (lane + 32 * it < NN) cp_async8(qs + b * NN + lane + 32 * it, src + lane + 32 * it);
+        }
+    }
+#pragma unroll
+    for (int bi = 0; bi < U::kBlockIters; ++bi) {
+        const int b = warp + bi * U::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            float* dst = far_s + ff * FS + el * SE;
+#pragma unroll
+            for (int it = 0; it < (4 * n + 31) / 32; ++it) {
+                const int idx = lane + 32 * it;
+                if (idx < 4 * n) {
+                    const int sd = idx / n, kk = idx - sd * n;
+                    cp_async4(dst + idx, tr_in + ff * ft + M.cnb[4 * (p0 + el) + sd] + (N - kk));
+                }
+            }
+        }
+    }
+    for (int i = tid; i < n * P; i += T::kThreads) zs[i] = 0.0f;
+    double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0;
+    if (active) {
+        const double* c = M.pcorners + 8 * pe;
+        x0 = c[0]; y0 = c[1]; x1 = c[2]; y1 = c[3]; x2 = c[4]; y2 = c[5]; x3 = c[6]; y3 = c[7];
+    }
+    const MetricLineF x_xi(static_cast<float>(x1 - x0), static_cast<float>(x2 - x3)), y_xi(static_cast<float>(y1 - y0), static_cast<float>(y2 - y3));
+    const MetricLineF x_eta(static_cast<float>(x3 - x0), static_cast<float>(x2 - x1)), y_eta(static_cast<float>(y3 - y0), static_cast<float>(y2 - y1));
+    if (active) {
+        const float tm = xn[m];
+        if (f == 2) {
+            for (int sd = m; sd < 4; sd += n) {
+                const float at = (sd == 0 || sd == 3) ? -1.0f : 1.0f;
+                const float dx = (sd == 0 || sd == 2) ? x_xi(at) : x_eta(at);
+                const float dy = (sd == 0 || sd == 2) ? y_xi(at) : y_eta(at);
+                ss[e * 4 + sd] = sqrtf(dx * dx + dy * dy);
+            }
+        }
+        const float xe = x_eta(tm), ye = y_eta(tm);
+        for (int j = f; j < n; j += 3) {
+            const float tj = xn[j];
+            js[e * ES + m * P + j] = __frcp_rn(x_xi(tj) * ye - xe * y_xi(tj));
+        }
+    }
+    cp_async_wait_all();
+#pragma unroll
+    for (int bi = 0; bi < U::kBlockIters; ++bi) {
+        const int b = warp + bi * U::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+#pragma unroll
+            for (int it = 0; it < U::kLaneIters; ++it)
+                if (lane + 32 * it < NN) qf[ff * QS + el * ES + lane_node[it]] = static_cast<float>(qs[b * NN + lane + 32 * it]);
+        }
+    }
+    __syncthreads();  // FP32 q tile, neighbour traces, zeros, edge metrics, J
+
+    const float* Qe = qf + e * ES;
+    const float* Xe = f == 0 ? Qe + 1 * QS : (f == 1 ? Qe : zs);
+    const float* Ye = f == 0 ? Qe + 2 * QS : (f == 1 ? zs : Qe);
+    if (active) {
+        const float* Qf = Qe + f * QS;
+        float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            const float qr = Qf[m * P + j], qc = Qf[j * P + m];
+            b = fmaf(lm[j], qr, b);
+            t = fmaf(lp[j], qr, t);
+            r = fmaf(lp[j], qc, r);
+            l = fmaf(lm[j], qc, l);
+        }
+        float* o = own_s + f * FS + e * SE;
+        o[0 * n + m] = b;
+        o[2 * n + (N - m)] = t;
+        o[1 * n + m] = r;
+        o[3 * n + (N - m)] = l;
+    }
+    __syncthreads();
+
+    if (active) {
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1 && f != 0) break;
+            const int s = pass == 0 ? f : 3;
+            const int role = M.crole[4 * pe + s];
+            const float nx = static_cast<float>(M.cnormal[2 * (4 * pe + s)]), ny = static_cast<float>(M.cnormal[2 * (4 * pe + s) + 1]);
+            const int o = e * SE + s * n + m;
+            const float op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
+            const float fp_ = far_s[o], fu_ = far_s[FS + o], fv_ = far_s[2 * FS + o];
+            const float Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
+            const float Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
+            const float wL = Lp + (Lu * nx + Lv * ny);
+            const float wR = Rp - (Ru * nx + Rv * ny);
+            const float sum = wL + wR;
+            const float sf = ss[e * 4 + s] * 0.5f;
+            far_s[o] = (role ? -(wL - wR) : (wL - wR)) * sf;
+            far_s[FS + o] = (role ? -nx : nx) * sum * sf;
+            far_s[2 * FS + o] = (role ? -ny : ny) * sum * sf;
+        }
+    }
+    __syncthreads();
+
+    const float* Dh = cf.dhat;
+    const float* iw = cf.iw;
+    const float* F = far_s + f * FS + e * SE;
+    if (active) {
+        const int j = m;
+        float col[n];
+#pragma unroll
+        for (int i = 0; i < n; ++i) col[i] = y_eta(xn[i]) * Xe[i * P + j] - x_eta(xn[i]) * Ye[i * P + j];
+        const float fr = F[1 * n + j], fl3 = F[3 * n + (N - j)];
+        float* G = gs + f * QS + e * ES + j;
+        if constexpr (N >= kEvenOddMinOrder32) {
+            dhat_even_odd<n>(cf.ea, cf.so, col, [&](int i, float y) { G[i * P] = -(y + (fr * lp[i] + fl3 * lm[i]) * iw[i]); });
+        } else {
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                float acc = 0.0f;
+#pragma unroll
+                for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[i * n + mm], col[mm], acc);
+                G[i * P] = -(acc + (fr * lp[i] + fl3 * lm[i]) * iw[i]);
+            }
+        }
+    }
+    __syncthreads();
+    if (active) {
+        const int i = m;
+        float line[n];
+#pragma unroll
+        for (int j = 0; j < n; ++j) line[j] = -y_xi(xn[j]) * Xe[i * P + j] + x_xi(xn[j]) * Ye[i * P + j];
+        const float ftp = F[2 * n + (N - i)], fbm = F[0 * n + i];
+        float* G = gs + f * QS + e * ES + i * P;
+        const float* jrow = js + e * ES + i * P;
+        if constexpr (N >= kEvenOddMinOrder32) {
+            dhat_even_odd<n>(cf.ea, cf.so, line, [&](int j, float y) { G[j] = (G[j] - (y + (ftp * lp[j] + fbm * lm[j]) * iw[j])) * jrow[j]; });
+        } else {
+#pragma unroll
+            for (int j = 0; j < n; ++j) {
+                float acc = 0.0f;
+#pragma unroll
+                for (int mm = 0; mm < n; ++mm) acc = fmaf(Dh[j * n + mm], line[mm], acc);
+                G[j] = (G[j] - (acc + (ftp * lp[j] + fbm * lm[j]) * iw[j])) * jrow[j];
+            }
+        }
+    }
+    __syncthreads();
+
+    // RK update in FP64; the new state also into the FP32 tile for the traces.
+    const double gdt = a.rk_g * dt;
+#pragma unroll
+    for (int bi = 0; bi < U::kBlockIters; ++bi) {
+        const int b = warp + bi * U::kWarps, ff = b / EPB, el = b - ff * EPB;
+        if (b < 3 * EPB && el < ne) {
+            const int64_t gb = ff * fb + M.poff2[p0 + el];
+            const int sb = ff * QS + el * ES, db = b * NN;
+            double kold[U::kLaneIters];
+#pragma unroll
+            for (int it = 0; it < U::kLaneIters; ++it) kold[it] = (!a.first && lane + 32 * it < NN) ? k[gb + lane + 32 * it] : 0.0;
+#pragma unroll
+            for (int it = 0; it < U::kLaneIters; ++it) {
+                const int nd = lane + 32 * it;
+                if (nd < NN) {
+                    const int sn = sb + lane_node[it];
+                    const double G = static_cast<double>(gs[sn]);
+                    const double kn = a.first ? G : fma(a.rk_a, kold[it], G);
+                    const double qn = fma(gdt, kn, qs[db + nd]);
+                    k[gb + nd] = kn;
+                    q[gb + nd] = qn;
+                    qf[sn] = static_cast<float>(qn);
+                    if (a.G_out) a.G_out[inst * 3 * fb + gb + nd] = G;
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    if (active) {
+        const float* row = qf + f * QS + e * ES + m * P;
+        const float* cl = qf + f * QS + e * ES + m;
+        float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+            b = fmaf(lm[j], row[j], b);
+            t = fmaf(lp[j], row[j], t);
+            r = fmaf(lp[j], cl[j * P], r);
+            l = fmaf(lm[j], cl[j * P], l);
+        }
+        float* o = tr_out + f * ft + M.poff1[pe];
+        o[0 * n + m] = b;
+        o[1 * n + m] = r;
+        o[2 * n + (N - m)] = t;
+        o[3 * n + (N - m)] = l;
+    }
+}
+
 template <int N>
 Coeffs<N> conforming_coeffs() {
     Coeffs<N> c;
@@ -331,10 +582,36 @@ cudaError_t launch_t(const GeneralStage& a, const OrderGroup& g, cudaStream_t st
 }
 
 template <int N>
+CoeffsF<N> conforming_coeffs_f() {
+    const Coeffs<N> d = conforming_coeffs<N>();
+    CoeffsF<N> c;
+    for (int i = 0; i < (N + 1) * (N + 1); ++i) c.dhat[i] = static_cast<float>(d.dhat[i]);
+    for (int i = 0; i <= N; ++i) {
+        c.xn[i] = static_cast<float>(d.xn[i]);
+        c.lm[i] = static_cast<float>(d.lm[i]);
+        c.lp[i] = static_cast<float>(d.lp[i]);
+        c.w[i] = static_cast<float>(d.w[i]);
+        c.iw[i] = static_cast<float>(d.iw[i]);
+    }
+    even_odd_halves(N + 1, d.dhat, c.ea, c.so);
+    return c;
+}
+
+template <int N>
+cudaError_t launch_f32_t(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
+    using T = TileF<N, 0>;
+    const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
+    conforming_stage_kernel_f32<N><<<grid, T::kThreads, T::kBytes, stream>>>(a, g, conforming_coeffs_f<N>());
+    return cudaGetLastError();
+}
+
+template <int N>
 cudaError_t prepare_t() {
     cudaError_t err = cudaFuncSetAttribute(conforming_stage_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
     if (err == cudaSuccess)
         err = cudaFuncSetAttribute(conforming_stage_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(conforming_stage_kernel_f32<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(TileF<N, 0>::kBytes));
     return err;
 }
 
@@ -352,11 +629,11 @@ cudaError_t prepare_conforming_kernels(int N) {
     }
 }
 
-cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, cudaStream_t stream) {
+cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream) {
     if (g.count <= 0) return cudaSuccess;
     switch (g.N) {
 #define NDG_CASE(n_) \
-    case n_: return strict ? launch_t<n_, true>(a, g, stream) : launch_t<n_, false>(a, g, stream);
+    case n_: return fp32 ? launch_f32_t<n_>(a, g, stream) : (strict ? launch_t<n_, true>(a, g, stream) : launch_t<n_, false>(a, g, stream));
         NDG_CONFORMING_ORDERS(NDG_CASE)
 #undef NDG_CASE
         default: return cudaErrorInvalidValue;

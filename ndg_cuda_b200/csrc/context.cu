@@ -107,9 +107,8 @@ dev::GeneralStage general_args(ndg_ctx* c, int m, int in) {
 // fused stage of every order group.
 bool fp32(const ndg_ctx* c) { return c->precision == NDG_FP32; }
 
-// The order groups a stage launches: in the FP32 form, which has no
-// conforming kernel, one per order.
-const std::vector<dev::OrderGroup>& stage_groups(const ndg_ctx* c) { return fp32(c) ? c->whole_groups : c->groups; }
+// The order groups a stage launches.
+const std::vector<dev::OrderGroup>& stage_groups(const ndg_ctx* c) { return c->groups; }
 
 int64_t general_stage_launches(const ndg_ctx* c) {
     const int64_t ghosts = c->gmesh.n_total > c->gmesh.n_domain ? 1 : 0;
@@ -447,8 +446,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         // own kernels as concurrent branches; the rest, latency-bound on
         // their dependent loads, come first in the list. Where few are, the split
         // only adds a branch beside the fused launch (measured slower), and
-        // the order stays one group (group_conforming 0). The FP32 form, which
-        // has no conforming kernel, runs one group per order.
+        // the order stays one group (group_conforming 0).
         c->groups.clear();
         c->whole_groups.clear();
         std::vector<dev::OrderGroup> conforming_parts;

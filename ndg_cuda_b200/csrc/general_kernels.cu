@@ -19,10 +19,11 @@
 //                  (Solver2D_t.cpp:138-172) and the side traces of the new
 //                  state for the next stage (Element2D_t.cpp:86-125)
 //
-// Each order group's conforming elements (one same-order face per side,
-// shared with a same-order neighbour) come first in the plan's lists and run
-// conforming_stage_kernel (conforming_kernels.cu) instead of the fused
-// stage; the two parts are separate groups and concurrent branches.
+// Where at least half of an order group's elements are conforming (one
+// same-order face per side, shared with a same-order neighbour), they come
+// last in the plan's list and run conforming_stage_kernel
+// (conforming_kernels.cu) instead of the fused stage; the two parts are
+// separate groups and concurrent branches.
 //
 // The mortar weights of the plan are computed once (side_weights_kernel,
 // face_weights_kernel). A face's flux is evaluated by each of its two
@@ -1059,7 +1060,7 @@ cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, bool fp32,
 
 cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream) {
     if (g.count == 0) return cudaSuccess;
-    if (g.conforming && !fp32) return launch_conforming_group(a, g, strict, stream);
+    if (g.conforming) return launch_conforming_group(a, g, strict, fp32, stream);
     return by_order(g.N, [&](auto c) {
         constexpr int N = decltype(c)::value;
         if (fp32) return launch_fused<N, false, float>(a, g, stream);

@@ -179,10 +179,10 @@ cudaError_t prepare_general_queue(size_t smem_bytes);
 // The fused stage of every order group in one launch (after the ghosts).
 cudaError_t launch_general_queue(const GeneralStage& a, const StageQueue& wq, bool strict, bool fp32, cudaStream_t stream);
 // Stage kernel of a group of conforming elements (conforming_kernels.cu):
-// the uniform-order stage with the neighbour traces gathered by the plan.
-// FP64 only; the FP32 form runs such groups through the general kernel.
+// the uniform-order stage with the neighbour traces gathered by the plan, in
+// FP64 (strict or not) or in the FP32 form.
 cudaError_t prepare_conforming_kernels(int N);
-cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, cudaStream_t stream);
+cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream);
 // The plane-wave initial condition at every node of a mixed-order mesh.
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream);
 
