@@ -465,6 +465,14 @@ def hp_leg(local: int, stream) -> dict:
     refining32, _, f32 = hp_run(local, stream, HP_REFINING_TOL, HP_REFINING_STEPS, precision=ndg.FP32, replay=flags)
     refining32["rel_l2_vs_fp64"] = {f: float(np.linalg.norm(f32[f] - f64[f]) / max(np.linalg.norm(f64[f]), 1e-300)) for f in f64}
     refining32["note"] = "the same meshes as the FP64 run (its refine flags replayed); FP32 traces, fluxes, mortar and volume arithmetic, FP64 q, k and RK update"
+    # Roofline of the mixed-order path: the whole stage (ghost kernel and the
+    # order groups' kernels) at the 32 B per DOF-stage of the uniform path's
+    # convention, over the run's device stepping time.
+    peak, peak_src = measured_hbm_peak()
+    for run in (as_configured, refining, refining32):
+        achieved = run["value"] * BYTES_PER_DOF_STAGE / 1e9
+        run["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                           "peak_source": peak_src, "scope": "whole stage: ghost traces and every order group's kernel, 32 B per DOF-stage"}
     # Parity at the configuration's scale: three adaptation rounds in
     # lockstep with the reference's CPU path (outside every timed region).
     lockstep = hp_lockstep_check(local, stream)
@@ -476,8 +484,9 @@ def hp_leg(local: int, stream) -> dict:
             "as_configured": as_configured,
             "refining": refining,
             "refining_fp32": refining32,
-            "launch_structure": ("one CUDA graph per RK3 step; per stage a ghost-trace kernel, then one fused kernel per order group, "
-                                 "the groups forked onto side streams as parallel graph branches"),
+            "launch_structure": ("one CUDA graph per RK3 step; per stage a ghost-trace kernel, then per order group the fused kernel, "
+                                 "or, where at least half its elements are conforming, the conforming-element kernel for those and "
+                                 "the fused kernel for the rest; the groups forked onto side streams as parallel graph branches"),
             "note": ("at the configuration's threshold 1e-4 the estimate never exceeds it on this mesh (largest error at N=4 "
                      "is 3.4e-6), so nothing refines; the 1e-9 runs exercise p-refinement, splitting to level 2 and the mortar path"),
             "flags_parity": lockstep["flags_parity"],
