@@ -97,7 +97,7 @@ bool fused_path_applies(const Topology& t) {
     return true;
 }
 
-GeneralPlan build_general_plan(const Topology& t) {
+GeneralPlan build_general_plan(const Topology& t, const Tables* tab) {
     GeneralPlan p;
     const int64_t K = t.n_domain;
     const int64_t total = static_cast<int64_t>(t.elem_N.size());
@@ -298,6 +298,7 @@ GeneralPlan build_general_plan(const Topology& t) {
     // their neighbours (mirror and copy kinds).
     p.gq_start.assign(static_cast<size_t>(G + 1), 0);
     p.gframe.assign(static_cast<size_t>(4 * G), 0.0);
+    p.gdirect.assign(static_cast<size_t>(G), -1);
     for (auto* v : {&p.gq_face, &p.gq_base, &p.gq_woff, &p.gq_moff}) v->reserve(static_cast<size_t>(G));
     p.gq_fs.reserve(static_cast<size_t>(G));
     p.gq_N.reserve(static_cast<size_t>(G));
@@ -319,6 +320,25 @@ GeneralPlan build_general_plan(const Topology& t) {
             p.sw_total += static_cast<int64_t>(Ng + 1) * (Nn + 1);
             p.gq_moff.push_back(p.sm_total);
             p.sm_total += Nn + 1;
+        }
+        if (q1 - q0 == 1 && tab != nullptr) {
+            // Direct gather: ghost_weights_kernel would match neighbour node j
+            // to ghost node N - j with weight w_n[j] / w_g[N - j] == 1.
+            const int64_t f = p.sface[static_cast<size_t>(q0)];
+            const int fs = p.gq_fs.back(), Nn = p.gq_N.back();
+            bool direct = Nn == Ng;
+            const auto& x = tab->get(NDG_TABLE_NODES, Ng);
+            const auto& w = tab->get(NDG_TABLE_WEIGHTS, Ng);
+            const double scale = t.face_scale[static_cast<size_t>(f)][static_cast<size_t>(fs)];
+            const double offset = t.face_offset[static_cast<size_t>(f)][static_cast<size_t>(fs)];
+            for (int j = 0; j <= Nn && direct; ++j) {
+                const double coord = ((x[static_cast<size_t>(Nn - j)] + 1.0) * scale + 2.0 * offset) - 1.0;  // mortar_coord
+                int found = -1;
+                for (int ii = 0; ii <= Ng && found < 0; ++ii)
+                    if (almost_equal(coord, x[static_cast<size_t>(ii)])) found = ii;
+                direct = found == Ng - j && w[static_cast<size_t>(j)] == w[static_cast<size_t>(Ng - j)];
+            }
+            if (direct) p.gdirect[gi] = p.gq_base.back();
         }
         if (q1 > q0) {
             const size_t f0 = static_cast<size_t>(p.sface[static_cast<size_t>(q0)]);

@@ -381,7 +381,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->tr32[0].release();
         c->tr32[1].release();
         if (4 * c->topo.n_domain >= (int64_t{1} << 31)) fail(NDG_ERR_UNSUPPORTED, "mixed-order meshes hold fewer than 2^29 elements");
-        c->gplan = build_general_plan(c->topo);
+        c->gplan = build_general_plan(c->topo, c->has_tables ? &c->tables : nullptr);
         const GeneralPlan& g = c->gplan;
         c->g_eN.upload(g.eN, c->stream);
         c->g_off2.upload_reuse(g.off2, c->stream);
@@ -439,6 +439,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         c->g_gq_woff.upload_reuse(g.gq_woff, c->stream);
         c->g_gq_moff.upload_reuse(g.gq_moff, c->stream);
         c->g_gframe.upload_reuse(g.gframe, c->stream);
+        c->g_gdirect.upload_reuse(g.gdirect, c->stream);
         std::vector<int64_t> ids;
         for (const auto& grp : g.groups) ids.insert(ids.end(), grp.second.begin(), grp.second.end());
         c->g_ids.upload_reuse(ids, c->stream);
@@ -565,6 +566,7 @@ void upload_plan(ndg_ctx* c, const Layout& l) {
         M.gq_woff = c->g_gq_woff.ptr;
         M.gq_moff = c->g_gq_moff.ptr;
         M.gframe = c->g_gframe.ptr;
+        M.gdirect = c->g_gdirect.ptr;
         check_cuda(dev::launch_general_weights(M, c->g_sw.ptr, c->g_smatch.ptr, c->g_fw.ptr, c->g_fmatch.ptr, c->g_slot_src.ptr, c->stream),
                    "mortar weights");
         c->launches += 4;

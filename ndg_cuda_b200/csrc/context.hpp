@@ -140,6 +140,7 @@ struct ndg_ctx {
     ndg::DeviceBuffer<int64_t> g_gq_start, g_gq_face, g_gq_base, g_gq_woff, g_gq_moff;  // ghost side-0 gathers
     ndg::DeviceBuffer<int32_t> g_gq_fs, g_gq_N;
     ndg::DeviceBuffer<double> g_gframe;
+    ndg::DeviceBuffer<int64_t> g_gdirect;
     std::vector<ndg::dev::OrderGroup> groups;        // mostly-conforming orders split (conforming parts last)
     std::vector<ndg::dev::OrderGroup> whole_groups;  // one group per order: first traces and the stage queue
     ndg::dev::GeneralMesh gmesh;

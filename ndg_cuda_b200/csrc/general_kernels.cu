@@ -164,7 +164,16 @@ __global__ void __launch_bounds__(128) general_ghosts_kernel(GeneralStage a, int
             const R sf = R(M.gscale[gi]);
             R vp = 0, vu = 0, vv = 0;
             const int64_t e0 = M.gq_start[gi], e1 = M.gq_start[gi + 1];
-            for (int64_t qe = e0; qe < e1; ++qe) {
+            const int64_t direct = M.gdirect[gi];
+            if (direct >= 0) {
+                // The one term of the loop below (neighbour node N - i, weight
+                // exactly 1), without its chain of plan loads.
+                const R* np_ = tr + direct + (N - i);
+                vp = add<S>(vp, mul<S>(mul<S>(R(1), np_[0]), sf));
+                vu = add<S>(vu, mul<S>(mul<S>(R(1), np_[ft]), sf));
+                vv = add<S>(vv, mul<S>(mul<S>(R(1), np_[2 * ft]), sf));
+            }
+            for (int64_t qe = (direct >= 0 ? e1 : e0); qe < e1; ++qe) {
                 const int Nn = M.gq_N[qe];
                 const R* np_ = tr + M.gq_base[qe];
                 const R* nu_ = np_ + ft;

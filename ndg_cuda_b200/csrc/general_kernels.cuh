@@ -110,6 +110,7 @@ struct GeneralMesh {
     const int64_t* gq_woff = nullptr;
     const int64_t* gq_moff = nullptr;
     const double* gframe = nullptr;        // [4 (n_total - n_domain)]
+    const int64_t* gdirect = nullptr;      // [n_total - n_domain] trace base of a direct one-face gather, or -1
 };
 
 // One RK3 stage on a mixed-order mesh.

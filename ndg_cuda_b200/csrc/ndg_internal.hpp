@@ -167,12 +167,17 @@ struct GeneralPlan {
     // neighbour's face side, the neighbour side's trace base and order, and
     // the offsets of its weights [(N_g+1) x (N_n+1)] and node matches [N_n+1]
     // in the side-weight arrays (filled on the device). gframe: normal and
-    // tangent of the ghost's first face (4 per ghost).
-    std::vector<int64_t> gq_start, gq_face, gq_base, gq_woff, gq_moff;
+    // tangent of the ghost's first face (4 per ghost). gdirect: where the
+    // ghost's gather is one face of its own order whose every node matches
+    // the reversed neighbour node with weight exactly 1 (checked with the
+    // gather's arithmetic), the neighbour side's trace base; -1 elsewhere.
+    std::vector<int64_t> gq_start, gq_face, gq_base, gq_woff, gq_moff, gdirect;
     std::vector<int32_t> gq_fs, gq_N;
     std::vector<double> gframe;
 };
-GeneralPlan build_general_plan(const Topology& t);
+// tab: the host tables of the context (node matching of the direct ghost
+// gathers; without them no gather is direct).
+GeneralPlan build_general_plan(const Topology& t, const Tables* tab = nullptr);
 
 // p-adaptation of the topology (orders of elements, ghosts and faces) from
 // per-element refine flags and decay rates. Returns whether an order changed.
