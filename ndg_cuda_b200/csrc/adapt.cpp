@@ -321,7 +321,7 @@ GeneralPlan build_general_plan(const Topology& t, const Tables* tab) {
             p.gq_moff.push_back(p.sm_total);
             p.sm_total += Nn + 1;
         }
-        if (q1 - q0 == 1 && tab != nullptr) {
+        if (q1 - q0 == 1 && tab != nullptr && Ng <= tab->N_max) {
             // Direct gather: ghost_weights_kernel would match neighbour node j
             // to ghost node N - j with weight w_n[j] / w_g[N - j] == 1.
             const int64_t f = p.sface[static_cast<size_t>(q0)];
