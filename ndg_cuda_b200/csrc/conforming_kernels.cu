@@ -80,6 +80,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
     // likewise, node N - k of the neighbour's side for node k of this side
     // (two elements traverse a shared side in opposite directions).
     const int warp = tid >> 5, lane = tid & 31;
+    const uint64_t stream_policy = evict_first_policy();  // q and k: read and rewritten once per stage
     int lane_node[T::kLaneIters];
 #pragma unroll
     for (int it = 0; it < T::kLaneIters; ++it) lane_node[it] = T::node(lane + 32 * it);
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
             double* dst = qs + ff * QS + el * ES;
 #pragma unroll
             for (int it = 0; it < T::kLaneIters; ++it)
-                if (lane + 32 * it < NN) cp_async8(dst + lane_node[it], src + lane + 32 * it);
+                if (lane + 32 * it < NN) cp_async8_stream(dst + lane_node[it], src + lane + 32 * it, stream_policy);
         }
     }
 #pragma unroll
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
             const int sb = ff * QS + el * ES;
             double kold[T::kLaneIters];
 #pragma unroll
-            for (int it = 0; it < T::kLaneIters; ++it) kold[it] = (!a.first && lane + 32 * it < NN) ? k[gb + lane + 32 * it] : 0.0;
+            for (int it = 0; it < T::kLaneIters; ++it) kold[it] = (!a.first && lane + 32 * it < NN) ? __ldcs(k + gb + lane + 32 * it) : 0.0;
 #pragma unroll
             for (int it = 0; it < T::kLaneIters; ++it) {
                 const int nd = lane + 32 * it;
@@ -288,8 +289,8 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
                     const double G = gs[sn];
                     const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, kold[it]), G);
                     const double qn = add<S>(qs[sn], mul<S>(gdt, kn));
-                    k[gb + nd] = kn;
-                    q[gb + nd] = qn;
+                    __stcs(k + gb + nd, kn);
+                    __stcs(q + gb + nd, qn);
                     qs[sn] = qn;
                     if (a.G_out) a.G_out[inst * 3 * fb + gb + nd] = G;
                 }
@@ -364,6 +365,7 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
     const int64_t pe = p0 + e;
 
     const int warp = tid >> 5, lane = tid & 31;
+    const uint64_t stream_policy = evict_first_policy();  // q and k: read and rewritten once per stage
     int lane_node[U::kLaneIters];
 #pragma unroll
     for (int it = 0; it < U::kLaneIters; ++it) lane_node[it] = T::node(lane + 32 * it);
@@ -374,7 +376,7 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
             const double* src = q + ff * fb + M.poff2[p0 + el];
 #pragma unroll
             for (int it = 0; it < U::kLaneIters; ++it)
-                if (lane + 32 * it < NN) cp_async8(qs + b * NN + lane + 32 * it, src + lane + 32 * it);
+                if (lane + 32 * it < NN) cp_async8_stream(qs + b * NN + lane + 32 * it, src + lane + 32 * it, stream_policy);
         }
     }
 #pragma unroll
@@ -527,7 +529,7 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
             const int sb = ff * QS + el * ES, db = b * NN;
             double kold[U::kLaneIters];
 #pragma unroll
-            for (int it = 0; it < U::kLaneIters; ++it) kold[it] = (!a.first && lane + 32 * it < NN) ? k[gb + lane + 32 * it] : 0.0;
+            for (int it = 0; it < U::kLaneIters; ++it) kold[it] = (!a.first && lane + 32 * it < NN) ? __ldcs(k + gb + lane + 32 * it) : 0.0;
 #pragma unroll
             for (int it = 0; it < U::kLaneIters; ++it) {
                 const int nd = lane + 32 * it;
@@ -536,8 +538,8 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
                     const double G = static_cast<double>(gs[sn]);
                     const double kn = a.first ? G : fma(a.rk_a, kold[it], G);
                     const double qn = fma(gdt, kn, qs[db + nd]);
-                    k[gb + nd] = kn;
-                    q[gb + nd] = qn;
+                    __stcs(k + gb + nd, kn);
+                    __stcs(q + gb + nd, qn);
                     qf[sn] = static_cast<float>(qn);
                     if (a.G_out) a.G_out[inst * 3 * fb + gb + nd] = G;
                 }

@@ -552,13 +552,15 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
         }
     }
     __syncthreads();
-    // q tile: asynchronous copies, waited for before the volume terms.
+    // q tile: asynchronous copies, waited for before the volume terms. The
+    // state is read and rewritten once per stage, evict-first in L2.
+    const uint64_t stream_policy = evict_first_policy();
     for (int idx = tid; idx < T::kVals; idx += THREADS) {
         const int f = idx / (EPB * NN), r = idx - f * (EPB * NN);
         const int e = r / NN, node = r - e * NN;
         if (e < ne) {
             const int64_t gi = f * fb + eo2[e] + node;
-            cp_async8(qs + idx, q + gi);
+            cp_async8_stream(qs + idx, q + gi, stream_policy);
         }
     }
     // The RK register of the tile into L2 while the stage runs (the update
@@ -751,10 +753,10 @@ __device__ __forceinline__ void fused_tile(const GeneralStage& a, const int64_t 
         if (ee >= ne) continue;
         const int64_t gi = ff * fb + eo2[ee] + node;
         const double G = static_cast<double>(gs[idx]);
-        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, k[gi]), G);
+        const double kn = a.first ? G : add<S>(mul<S>(a.rk_a, __ldcs(k + gi)), G);
         const double qn = add<S>(qs[idx], mul<S>(gdt, kn));
-        k[gi] = kn;
-        q[gi] = qn;
+        __stcs(k + gi, kn);
+        __stcs(q + gi, qn);
         qs[idx] = qn;
         if constexpr (T::kCopy) qw[idx] = R(qn);
         if (a.G_out) a.G_out[inst * 3 * fb + gi] = G;
