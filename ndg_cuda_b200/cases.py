@@ -51,8 +51,9 @@ def main(argv=None) -> None:
     ap.add_argument("--rounds", type=int, default=3, help="p-adaptation rounds of the mixed case")
     ap.add_argument("--tile", type=int, default=0, help="elements per CTA of the stage kernel (0: default)")
     ap.add_argument("--fp32", action="store_true")
-    ap.add_argument("--launch", type=int, default=0, choices=[0, 1],
-                    help="mixed case: 0 one launch per order group, 1 one queue launch per stage")
+    ap.add_argument("--launch", type=int, default=0, choices=[0, 1, 2],
+                    help="mixed case: 0 one launch per order group, 1 one queue launch per stage, "
+                    "2 order groups split into side fluxes and element tiles")
     ap.add_argument("--time", type=int, default=0, help="mixed case: then time this many steps (wall clock after a synchronise)")
     args = ap.parse_args(argv)
     prec = FP32 if args.fp32 else FP64

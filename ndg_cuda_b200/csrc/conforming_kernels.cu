@@ -21,6 +21,11 @@
 // The FP32 form (conforming_stage_kernel_f32) follows the uniform FP32
 // kernel: traces, fluxes and the volume term in FP32 over FP32 trace
 // buffers, q, k and the RK update in FP64.
+//
+// PRE forms: the element side fluxes arrive precomputed (side_flux_kernel,
+// general_kernels.cu, in the trace layout of sflux), so that any element,
+// conforming or not, runs the tile: it copies them where the neighbour
+// traces go and skips its own traces, the edge metrics and the flux pass.
 #include "general_kernels.cuh"
 #include "stage_common.cuh"
 #include "stage_kernels.cuh"
@@ -35,7 +40,7 @@ namespace dev {
 
 namespace {
 
-template <int N, bool S>
+template <int N, bool S, bool PRE>
 __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
     conforming_stage_kernel(GeneralStage a, OrderGroup grp, const __grid_constant__ Coeffs<N> cf) {
     using T = Tile<N>;
@@ -61,6 +66,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
     double* k = a.k + inst * 3 * fb;
     const double* tr_in = a.etr + inst * 3 * ft;
     double* tr_out = a.etr_out + inst * 3 * ft;
+    const double* sf_in = PRE ? a.sflux + inst * 3 * ft : nullptr;  // element side fluxes (PRE)
     const double* xn = cf.xn;
     const double* lm = cf.lm;
     const double* lp = cf.lp;
@@ -104,8 +110,12 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
             for (int it = 0; it < (4 * n + 31) / 32; ++it) {
                 const int idx = lane + 32 * it;
                 if (idx < 4 * n) {
-                    const int sd = idx / n, kk = idx - sd * n;
-                    cp_async8(dst + idx, tr_in + ff * ft + M.cnb[4 * (p0 + el) + sd] + (N - kk));
+                    if constexpr (PRE) {
+                        cp_async8(dst + idx, sf_in + ff * ft + M.poff1[p0 + el] + idx);
+                    } else {
+                        const int sd = idx / n, kk = idx - sd * n;
+                        cp_async8(dst + idx, tr_in + ff * ft + M.cnb[4 * (p0 + el) + sd] + (N - kk));
+                    }
                 }
             }
         }
@@ -120,7 +130,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
     const MetricLine<S> x_eta(sub<S>(x3, x0), sub<S>(x2, x1)), y_eta(sub<S>(y3, y0), sub<S>(y2, y1));
     if (active) {
         const double tm = xn[m];
-        if (f == 2) {
+        if (!PRE && f == 2) {
             // Edge metric of each side (Element2D_t.cpp:756-769).
             for (int sd = m; sd < 4; sd += n) {
                 const double at = (sd == 0 || sd == 3) ? -1.0 : 1.0;
@@ -147,54 +157,56 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
     const double* Qe = qs + e * ES;
     const double* Xe = f == 0 ? Qe + 1 * QS : (f == 1 ? Qe : zs);
     const double* Ye = f == 0 ? Qe + 2 * QS : (f == 1 ? zs : Qe);
-    if (active) {
-        const double* Qf = Qe + f * QS;
-        double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
-#pragma unroll
-        for (int j = 0; j < n; ++j) {
-            const double qr = Qf[m * P + j], qc = Qf[j * P + m];
-            b = madd<S>(b, lm[j], qr);
-            t = madd<S>(t, lp[j], qr);
-            r = madd<S>(r, lp[j], qc);
-            l = madd<S>(l, lm[j], qc);
+    if constexpr (!PRE) {
+        if (active) {
+            const double* Qf = Qe + f * QS;
+            double b = 0.0, t = 0.0, r = 0.0, l = 0.0;
+    #pragma unroll
+            for (int j = 0; j < n; ++j) {
+                const double qr = Qf[m * P + j], qc = Qf[j * P + m];
+                b = madd<S>(b, lm[j], qr);
+                t = madd<S>(t, lp[j], qr);
+                r = madd<S>(r, lp[j], qc);
+                l = madd<S>(l, lm[j], qc);
+            }
+            double* o = own_s + f * FS + e * SE;
+            o[0 * n + m] = b;
+            o[2 * n + (N - m)] = t;
+            o[1 * n + m] = r;
+            o[3 * n + (N - m)] = l;
         }
-        double* o = own_s + f * FS + e * SE;
-        o[0 * n + m] = b;
-        o[2 * n + (N - m)] = t;
-        o[1 * n + m] = r;
-        o[3 * n + (N - m)] = l;
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // Flux pass: side nodes m of side f, and of side 3 for f = 0. The upwind
-    // flux in the face's own left/right order (Solver2D_t.cpp:48-63), then
-    // the element's view of it: times the edge metric, negated for the
-    // face's right element, whose side runs against the face's nodes
-    // (Mesh2D_t.cpp:3895-3929).
-    if (active) {
-        for (int pass = 0; pass < 2; ++pass) {
-            if (pass == 1 && f != 0) break;
-            const int s = pass == 0 ? f : 3;
-            const int role = M.crole[4 * pe + s];
-            const double nx = M.cnormal[2 * (4 * pe + s)], ny = M.cnormal[2 * (4 * pe + s) + 1];
-            const int o = e * SE + s * n + m;
-            const double op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
-            const double fp_ = far_s[o], fu_ = far_s[FS + o], fv_ = far_s[2 * FS + o];
-            const double Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
-            const double Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
-            const double wL = add<S>(Lp, add<S>(mul<S>(Lu, nx), mul<S>(Lv, ny)));
-            const double wR = sub<S>(Rp, add<S>(mul<S>(Ru, nx), mul<S>(Rv, ny)));
-            const double flp = mul<S>(sub<S>(wL, wR), 0.5);
-            const double sum = add<S>(wL, wR);
-            const double flu = mul<S>(mul<S>(nx, sum), 0.5);
-            const double flv = mul<S>(mul<S>(ny, sum), 0.5);
-            const double sf = ss[e * 4 + s];
-            far_s[o] = mul<S>(role ? -flp : flp, sf);
-            far_s[FS + o] = mul<S>(role ? -flu : flu, sf);
-            far_s[2 * FS + o] = mul<S>(role ? -flv : flv, sf);
+        // Flux pass: side nodes m of side f, and of side 3 for f = 0. The upwind
+        // flux in the face's own left/right order (Solver2D_t.cpp:48-63), then
+        // the element's view of it: times the edge metric, negated for the
+        // face's right element, whose side runs against the face's nodes
+        // (Mesh2D_t.cpp:3895-3929).
+        if (active) {
+            for (int pass = 0; pass < 2; ++pass) {
+                if (pass == 1 && f != 0) break;
+                const int s = pass == 0 ? f : 3;
+                const int role = M.crole[4 * pe + s];
+                const double nx = M.cnormal[2 * (4 * pe + s)], ny = M.cnormal[2 * (4 * pe + s) + 1];
+                const int o = e * SE + s * n + m;
+                const double op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
+                const double fp_ = far_s[o], fu_ = far_s[FS + o], fv_ = far_s[2 * FS + o];
+                const double Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
+                const double Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
+                const double wL = add<S>(Lp, add<S>(mul<S>(Lu, nx), mul<S>(Lv, ny)));
+                const double wR = sub<S>(Rp, add<S>(mul<S>(Ru, nx), mul<S>(Rv, ny)));
+                const double flp = mul<S>(sub<S>(wL, wR), 0.5);
+                const double sum = add<S>(wL, wR);
+                const double flu = mul<S>(mul<S>(nx, sum), 0.5);
+                const double flv = mul<S>(mul<S>(ny, sum), 0.5);
+                const double sf = ss[e * 4 + s];
+                far_s[o] = mul<S>(role ? -flp : flp, sf);
+                far_s[FS + o] = mul<S>(role ? -flu : flu, sf);
+                far_s[2 * FS + o] = mul<S>(role ? -flv : flv, sf);
+            }
         }
+        __syncthreads();
     }
-    __syncthreads();
 
     const double* Dh = cf.dhat;
     const double* w = cf.w;
@@ -323,7 +335,7 @@ __global__ void __launch_bounds__(Tile<N>::kThreads, Tile<N>::kMinBlocks)
 // FP32 form. The FP64 q tile arrives unpadded by 8-byte copies (warps over
 // (field, element) blocks, as above) and each thread converts the values it
 // copied into the padded FP32 tile once its own copies have landed.
-template <int N>
+template <int N, bool PRE>
 __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks)
     conforming_stage_kernel_f32(GeneralStage a, OrderGroup grp, const __grid_constant__ CoeffsF<N> cf) {
     using T = TileF<N, 0>;
@@ -352,6 +364,7 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
     double* k = a.k + inst * 3 * fb;
     const float* tr_in = a.etr_f + inst * 3 * ft;
     float* tr_out = a.etr_out_f + inst * 3 * ft;
+    const float* sf_in = PRE ? a.sflux_f + inst * 3 * ft : nullptr;  // element side fluxes (PRE)
     const float* xn = cf.xn;
     const float* lm = cf.lm;
     const float* lp = cf.lp;
@@ -388,8 +401,12 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
             for (int it = 0; it < (4 * n + 31) / 32; ++it) {
                 const int idx = lane + 32 * it;
                 if (idx < 4 * n) {
-                    const int sd = idx / n, kk = idx - sd * n;
-                    cp_async4(dst + idx, tr_in + ff * ft + M.cnb[4 * (p0 + el) + sd] + (N - kk));
+                    if constexpr (PRE) {
+                        cp_async4(dst + idx, sf_in + ff * ft + M.poff1[p0 + el] + idx);
+                    } else {
+                        const int sd = idx / n, kk = idx - sd * n;
+                        cp_async4(dst + idx, tr_in + ff * ft + M.cnb[4 * (p0 + el) + sd] + (N - kk));
+                    }
                 }
             }
         }
@@ -404,7 +421,7 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
     const MetricLineF x_eta(static_cast<float>(x3 - x0), static_cast<float>(x2 - x1)), y_eta(static_cast<float>(y3 - y0), static_cast<float>(y2 - y1));
     if (active) {
         const float tm = xn[m];
-        if (f == 2) {
+        if (!PRE && f == 2) {
             for (int sd = m; sd < 4; sd += n) {
                 const float at = (sd == 0 || sd == 3) ? -1.0f : 1.0f;
                 const float dx = (sd == 0 || sd == 2) ? x_xi(at) : x_eta(at);
@@ -433,46 +450,48 @@ __global__ void __launch_bounds__(TileF<N, 0>::kThreads, TileF<N, 0>::kMinBlocks
     const float* Qe = qf + e * ES;
     const float* Xe = f == 0 ? Qe + 1 * QS : (f == 1 ? Qe : zs);
     const float* Ye = f == 0 ? Qe + 2 * QS : (f == 1 ? zs : Qe);
-    if (active) {
-        const float* Qf = Qe + f * QS;
-        float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
-#pragma unroll
-        for (int j = 0; j < n; ++j) {
-            const float qr = Qf[m * P + j], qc = Qf[j * P + m];
-            b = fmaf(lm[j], qr, b);
-            t = fmaf(lp[j], qr, t);
-            r = fmaf(lp[j], qc, r);
-            l = fmaf(lm[j], qc, l);
+    if constexpr (!PRE) {
+        if (active) {
+            const float* Qf = Qe + f * QS;
+            float b = 0.0f, t = 0.0f, r = 0.0f, l = 0.0f;
+    #pragma unroll
+            for (int j = 0; j < n; ++j) {
+                const float qr = Qf[m * P + j], qc = Qf[j * P + m];
+                b = fmaf(lm[j], qr, b);
+                t = fmaf(lp[j], qr, t);
+                r = fmaf(lp[j], qc, r);
+                l = fmaf(lm[j], qc, l);
+            }
+            float* o = own_s + f * FS + e * SE;
+            o[0 * n + m] = b;
+            o[2 * n + (N - m)] = t;
+            o[1 * n + m] = r;
+            o[3 * n + (N - m)] = l;
         }
-        float* o = own_s + f * FS + e * SE;
-        o[0 * n + m] = b;
-        o[2 * n + (N - m)] = t;
-        o[1 * n + m] = r;
-        o[3 * n + (N - m)] = l;
-    }
-    __syncthreads();
+        __syncthreads();
 
-    if (active) {
-        for (int pass = 0; pass < 2; ++pass) {
-            if (pass == 1 && f != 0) break;
-            const int s = pass == 0 ? f : 3;
-            const int role = M.crole[4 * pe + s];
-            const float nx = static_cast<float>(M.cnormal[2 * (4 * pe + s)]), ny = static_cast<float>(M.cnormal[2 * (4 * pe + s) + 1]);
-            const int o = e * SE + s * n + m;
-            const float op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
-            const float fp_ = far_s[o], fu_ = far_s[FS + o], fv_ = far_s[2 * FS + o];
-            const float Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
-            const float Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
-            const float wL = Lp + (Lu * nx + Lv * ny);
-            const float wR = Rp - (Ru * nx + Rv * ny);
-            const float sum = wL + wR;
-            const float sf = ss[e * 4 + s] * 0.5f;
-            far_s[o] = (role ? -(wL - wR) : (wL - wR)) * sf;
-            far_s[FS + o] = (role ? -nx : nx) * sum * sf;
-            far_s[2 * FS + o] = (role ? -ny : ny) * sum * sf;
+        if (active) {
+            for (int pass = 0; pass < 2; ++pass) {
+                if (pass == 1 && f != 0) break;
+                const int s = pass == 0 ? f : 3;
+                const int role = M.crole[4 * pe + s];
+                const float nx = static_cast<float>(M.cnormal[2 * (4 * pe + s)]), ny = static_cast<float>(M.cnormal[2 * (4 * pe + s) + 1]);
+                const int o = e * SE + s * n + m;
+                const float op = own_s[o], ou = own_s[FS + o], ov = own_s[2 * FS + o];
+                const float fp_ = far_s[o], fu_ = far_s[FS + o], fv_ = far_s[2 * FS + o];
+                const float Lp = role ? fp_ : op, Lu = role ? fu_ : ou, Lv = role ? fv_ : ov;
+                const float Rp = role ? op : fp_, Ru = role ? ou : fu_, Rv = role ? ov : fv_;
+                const float wL = Lp + (Lu * nx + Lv * ny);
+                const float wR = Rp - (Ru * nx + Rv * ny);
+                const float sum = wL + wR;
+                const float sf = ss[e * 4 + s] * 0.5f;
+                far_s[o] = (role ? -(wL - wR) : (wL - wR)) * sf;
+                far_s[FS + o] = (role ? -nx : nx) * sum * sf;
+                far_s[2 * FS + o] = (role ? -ny : ny) * sum * sf;
+            }
         }
+        __syncthreads();
     }
-    __syncthreads();
 
     const float* Dh = cf.dhat;
     const float* iw = cf.iw;
@@ -575,11 +594,11 @@ Coeffs<N> conforming_coeffs() {
     return c;
 }
 
-template <int N, bool S>
+template <int N, bool S, bool PRE>
 cudaError_t launch_t(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
     using T = Tile<N>;
     const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
-    conforming_stage_kernel<N, S><<<grid, T::kThreads, T::kBytes, stream>>>(a, g, conforming_coeffs<N>());
+    conforming_stage_kernel<N, S, PRE><<<grid, T::kThreads, T::kBytes, stream>>>(a, g, conforming_coeffs<N>());
     return cudaGetLastError();
 }
 
@@ -599,22 +618,27 @@ CoeffsF<N> conforming_coeffs_f() {
     return c;
 }
 
-template <int N>
+template <int N, bool PRE>
 cudaError_t launch_f32_t(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
     using T = TileF<N, 0>;
     const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
-    conforming_stage_kernel_f32<N><<<grid, T::kThreads, T::kBytes, stream>>>(a, g, conforming_coeffs_f<N>());
+    conforming_stage_kernel_f32<N, PRE><<<grid, T::kThreads, T::kBytes, stream>>>(a, g, conforming_coeffs_f<N>());
     return cudaGetLastError();
 }
 
+template <int N, bool PRE>
+cudaError_t prepare_form() {
+    cudaError_t err = cudaFuncSetAttribute(conforming_stage_kernel<N, false, PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(conforming_stage_kernel<N, true, PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(conforming_stage_kernel_f32<N, PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(TileF<N, 0>::kBytes));
+    return err;
+}
 template <int N>
 cudaError_t prepare_t() {
-    cudaError_t err = cudaFuncSetAttribute(conforming_stage_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
-    if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(conforming_stage_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Tile<N>::kBytes));
-    if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(conforming_stage_kernel_f32<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(TileF<N, 0>::kBytes));
-    return err;
+    const cudaError_t err = prepare_form<N, false>();
+    return err == cudaSuccess ? prepare_form<N, true>() : err;
 }
 
 #define NDG_CONFORMING_ORDERS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
@@ -631,11 +655,13 @@ cudaError_t prepare_conforming_kernels(int N) {
     }
 }
 
-cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream) {
+cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream, bool pre) {
     if (g.count <= 0) return cudaSuccess;
     switch (g.N) {
-#define NDG_CASE(n_) \
-    case n_: return fp32 ? launch_f32_t<n_>(a, g, stream) : (strict ? launch_t<n_, true>(a, g, stream) : launch_t<n_, false>(a, g, stream));
+#define NDG_CASE(n_)                                                                                                          \
+    case n_:                                                                                                                  \
+        if (pre) return fp32 ? launch_f32_t<n_, true>(a, g, stream) : (strict ? launch_t<n_, true, true>(a, g, stream) : launch_t<n_, false, true>(a, g, stream)); \
+        return fp32 ? launch_f32_t<n_, false>(a, g, stream) : (strict ? launch_t<n_, true, false>(a, g, stream) : launch_t<n_, false, false>(a, g, stream));
         NDG_CONFORMING_ORDERS(NDG_CASE)
 #undef NDG_CASE
         default: return cudaErrorInvalidValue;

@@ -93,6 +93,8 @@ dev::GeneralStage general_args(ndg_ctx* c, int m, int in) {
     a.etr_out = c->getr[1 - in].ptr;
     a.etr_f = c->getr32[in].ptr;
     a.etr_out_f = c->getr32[1 - in].ptr;
+    a.sflux = c->gsflux.ptr;
+    a.sflux_f = c->gsflux32.ptr;
     a.side_slots = c->side_slots;
     a.step = c->step.ptr;
     a.rk_a = kRkA[m];
@@ -110,10 +112,31 @@ bool fp32(const ndg_ctx* c) { return c->precision == NDG_FP32; }
 // The order groups a stage launches.
 const std::vector<dev::OrderGroup>& stage_groups(const ndg_ctx* c) { return c->groups; }
 
+// Whether an order group runs split (side_flux_kernel, then the
+// conforming-element kernel over its side fluxes) rather than fused: always
+// in launch mode 2; in mode 0 in the FP32 form, where the group (times the
+// instances) has at least kSplitMinElements elements and its order has no
+// conforming part. Measured (ms per step, DOF-stage updates/s), fused
+// against split by this rule: the mixed p-adapted 128² mesh FP64 0.2705 →
+// 0.2572, FP32 0.2092 → 0.2045; the hp refining run (about 30 meshes) FP64
+// 4.72e10 → 4.60e10, FP32 6.16e10 → 6.27e10. FP64 stays fused by default
+// for the hp run; splitting every group there cost 4% (FP64) and 5% (FP32).
+constexpr int64_t kSplitMinElements = 2048;
+bool split_group(const ndg_ctx* c, const dev::OrderGroup& og) {
+    if (og.conforming || c->mixed_launch == 1) return false;
+    if (c->mixed_launch == 2) return true;
+    if (!fp32(c)) return false;
+    const bool has_conforming_part =
+        std::any_of(c->groups.begin(), c->groups.end(), [&](const dev::OrderGroup& other) { return other.conforming && other.N == og.N; });
+    return !has_conforming_part && og.count * c->n_instances >= kSplitMinElements;
+}
+
 int64_t general_stage_launches(const ndg_ctx* c) {
     const int64_t ghosts = c->gmesh.n_total > c->gmesh.n_domain ? 1 : 0;
     if (c->mixed_launch == 1) return (c->queue.n_tiles > 0 ? 1 : 0) + ghosts;
-    return static_cast<int64_t>(stage_groups(c).size()) + ghosts;
+    const auto& groups = stage_groups(c);
+    const int64_t split = std::count_if(groups.begin(), groups.end(), [&](const dev::OrderGroup& og) { return split_group(c, og); });
+    return static_cast<int64_t>(groups.size()) + split + ghosts;
 }
 
 // Side streams and events for the concurrent order groups (created once,
@@ -150,14 +173,21 @@ cudaError_t issue_general_stage(ndg_ctx* c, int m, int in) {
     // the mixed p-adapted mesh (FP32: 0.220 against 0.257 ms per step).
     const bool first0 = !fp32(c) || std::any_of(groups.begin(), groups.end(), [](const dev::OrderGroup& og) { return og.conforming != 0; });
     if (G > 1 && (err = cudaEventRecord(c->aux_events[0], c->stream)) != cudaSuccess) return err;
-    if (first0 && (err = dev::launch_general_group(a, groups[0], strict(c), fp32(c), c->stream)) != cudaSuccess) return err;
+    // A split group runs its element side fluxes first (side_flux_kernel),
+    // then the conforming-element kernel over them (split_group).
+    const auto group = [&](size_t g) {
+        dev::OrderGroup og = groups[g];
+        og.split = split_group(c, og) ? 1 : 0;
+        return og;
+    };
+    if (first0 && (err = dev::launch_general_group(a, group(0), strict(c), fp32(c), c->stream)) != cudaSuccess) return err;
     for (size_t g = 1; g < G && err == cudaSuccess; ++g) {
         cudaStream_t st = c->aux_streams[g - 1];
         if ((err = cudaStreamWaitEvent(st, c->aux_events[0], 0)) != cudaSuccess) break;
-        if ((err = dev::launch_general_group(a, groups[g], strict(c), fp32(c), st)) != cudaSuccess) break;
+        if ((err = dev::launch_general_group(a, group(g), strict(c), fp32(c), st)) != cudaSuccess) break;
         err = cudaEventRecord(c->aux_events[g], st);
     }
-    if (!first0 && err == cudaSuccess) err = dev::launch_general_group(a, groups[0], strict(c), fp32(c), c->stream);
+    if (!first0 && err == cudaSuccess) err = dev::launch_general_group(a, group(0), strict(c), fp32(c), c->stream);
     for (size_t g = 1; g < G && err == cudaSuccess; ++g) err = cudaStreamWaitEvent(c->stream, c->aux_events[g], 0);
     return err;
 }
@@ -175,6 +205,12 @@ cudaError_t issue_stage(ndg_ctx* c, int m, int in) {
 // The FP32 form on a mixed-order mesh allocates its trace buffers the first
 // time it runs (before any capture).
 void require_form(ndg_ctx* c) {
+    if (c->general && std::any_of(c->groups.begin(), c->groups.end(), [&](const dev::OrderGroup& og) { return split_group(c, og); })) {
+        // The split groups' side fluxes, written before they are read in every stage.
+        const size_t count = c->getr[0].count;
+        if (c->gsflux.count != count) c->gsflux.allocate(count);
+        if (fp32(c) && c->gsflux32.count != count) c->gsflux32.allocate(count);
+    }
     if (c->general && fp32(c)) {
         const size_t count = c->getr[0].count;
         for (auto& t : c->getr32)
@@ -980,7 +1016,8 @@ ndg_status ndg_ctx_set_precision(ndg_ctx* ctx, int32_t precision) {
 ndg_status ndg_set_mixed_launch(ndg_ctx* ctx, int32_t mode) {
     return guarded([&] {
         if (!ctx) fail(NDG_ERR_INVALID_ARG, "ctx is NULL");
-        if (mode != 0 && mode != 1) fail(NDG_ERR_INVALID_ARG, "mode is 0 (one launch per order group) or 1 (one queue launch per stage)");
+        if (mode < 0 || mode > 2)
+            fail(NDG_ERR_INVALID_ARG, "mode is 0 (one launch per order group), 1 (one queue launch per stage) or 2 (order groups split into side fluxes and element tiles)");
         ctx->mixed_launch = mode;
         drop_graphs(ctx);
     });

@@ -121,6 +121,8 @@ struct ndg_ctx {
     ndg::DeviceBuffer<double> g_corners, g_node_xy, g_fnormal, g_ftangent, g_foffset, g_fscale, g_gscale;
     ndg::DeviceBuffer<double> getr[2];  // element side traces, double-buffered between stages
     ndg::DeviceBuffer<float> getr32[2]; // the same in the FP32 form (allocated when it first runs)
+    ndg::DeviceBuffer<double> gsflux;   // element side fluxes of the split launch (mixed launch 2, allocated when it first runs)
+    ndg::DeviceBuffer<float> gsflux32;
     int side_slots = 1;                 // largest sum of (face order + 1) over one element side
     ndg::DeviceBuffer<int64_t> g_sw_off, g_sm_off, g_fw_off, g_fm_off, g_fbase;  // mortar weight offsets, face-side trace bases
     ndg::DeviceBuffer<int32_t> g_fsN;                                            // face-side element orders

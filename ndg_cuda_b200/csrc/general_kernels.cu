@@ -792,6 +792,148 @@ __global__ void __launch_bounds__(FusedTile<N, R>::kThreads) general_fused_kerne
                                                    blockIdx.y, smem);
 }
 
+// Element side fluxes of one order group for its split form: the fused
+// tile's face-flux and element-side-flux phases, with the same operations
+// in the same order, written to sflux in the trace layout (field, then the
+// element's four sides of N + 1 values) for conforming_stage_kernel's PRE
+// form, which runs the rest of the stage on the uniform kernels' tile. Tiles
+// of about 32 side nodes a field (128 threads), with no q tile, so that many
+// short tiles share an SM and hide the gathers' latency.
+template <int N, typename R>
+struct FluxTile {
+    static constexpr int n = N + 1;
+    static constexpr int EPB = 32 / n >= 1 ? 32 / n : 1;
+    static constexpr int kThreads = 128;
+    // FP64: at most 40 registers, for warps to hide the gathers' latency (the
+    // FP32 form fits 10 CTAs at its free 48 registers; bound to 40 it spills)
+    static constexpr int kMinBlocks = sizeof(R) == 8 ? 12 : 0;
+    // doubles: [EPB] trace offsets, [4 EPB + 1] first slot of each side and
+    // the end, the same for mortar entries (int64), [4 EPB] flux modes (ints)
+    static constexpr int kDoubles = EPB + 2 * (4 * EPB + 1) + 2 * EPB;
+    // then R: [EPB][4] edge metrics, [3][EPB][4][slots] face fluxes
+    static constexpr size_t bytes(int slots) {
+        return sizeof(double) * kDoubles + sizeof(R) * (4 * EPB + static_cast<size_t>(3 * EPB * 4) * static_cast<size_t>(slots));
+    }
+};
+
+template <int N, bool S, typename R>
+__global__ void __launch_bounds__(FluxTile<N, R>::kThreads, FluxTile<N, R>::kMinBlocks) side_flux_kernel(GeneralStage a, OrderGroup grp) {
+    using T = FluxTile<N, R>;
+    constexpr int n = T::n, EPB = T::EPB, THREADS = T::kThreads;
+    extern __shared__ __align__(128) double smem[];
+    int64_t* eo1 = reinterpret_cast<int64_t*>(smem);
+    int64_t* sst = eo1 + EPB;
+    int64_t* sqs = sst + 4 * EPB + 1;
+    int* smode = reinterpret_cast<int*>(sqs + 4 * EPB + 1);
+    R* ss = reinterpret_cast<R*>(smem + T::kDoubles);
+    R* ffs = ss + 4 * EPB;
+    const GeneralMesh& M = a.m;
+    const int tid = threadIdx.x;
+    const int64_t first = grp.first;
+    const int64_t base = static_cast<int64_t>(blockIdx.x) * EPB;
+    const int ne = static_cast<int>((grp.count - base) < EPB ? (grp.count - base) : EPB);
+    const int64_t inst = blockIdx.y;
+    const int64_t ft = M.trace_total;
+    const R* tr = pick<R>(a.etr, a.etr_f) + inst * 3 * ft;
+    R* out_flux = pick<R>(a.sflux, a.sflux_f) + inst * 3 * ft;
+    const int SL = a.side_slots;
+    const int FFS = EPB * 4 * SL;
+
+    if (tid <= 4 * ne) {
+        const int64_t ps = 4 * (first + base) + tid;
+        sst[tid] = M.pslot_start[ps];
+        sqs[tid] = M.pq_start[ps];
+        if (tid < 4 * ne) smode[tid] = M.pside_mode[ps];
+        if (tid < ne) eo1[tid] = M.poff1[first + base + tid];
+    }
+    // Edge metric of each side (Element2D_t.cpp:756-769), thread per side.
+    if (tid < 4 * ne) {
+        const int ee = tid / 4, sd = tid - 4 * ee;
+        const double* c = M.pcorners + 8 * (first + base + ee);
+        const double x0 = c[0], y0 = c[1], x1 = c[2], y1 = c[3], x2 = c[4], y2 = c[5], x3 = c[6], y3 = c[7];
+        const MetricLine<S, R> x_xi(R(sub<S>(x1, x0)), R(sub<S>(x2, x3))), y_xi(R(sub<S>(y1, y0)), R(sub<S>(y2, y3)));
+        const MetricLine<S, R> x_eta(R(sub<S>(x3, x0)), R(sub<S>(x2, x1))), y_eta(R(sub<S>(y3, y0)), R(sub<S>(y2, y1)));
+        const R at = (sd == 0 || sd == 3) ? R(-1) : R(1);
+        const R dx = (sd == 0 || sd == 2) ? metric<S, R>(at, x_xi.d0, x_xi.d1) : metric<S, R>(at, x_eta.d0, x_eta.d1);
+        const R dy = (sd == 0 || sd == 2) ? metric<S, R>(at, y_xi.d0, y_xi.d1) : metric<S, R>(at, y_eta.d0, y_eta.d1);
+        ss[tid] = sqrt(add<S>(mul<S>(dx, dx), mul<S>(dy, dy)));
+    }
+    __syncthreads();
+
+    // Face fluxes at every face node of the tile's sides (Mesh2D_t.cpp:3803-3893,
+    // Solver2D_t.cpp:48-63), as in fused_tile.
+    const int64_t g0 = sst[0];
+    const int n_items = static_cast<int>(sst[4 * ne] - g0);
+    const int64_t side0 = 4 * (first + base);
+    for (int idx = tid; idx < n_items; idx += THREADS) {
+        const int64_t g = g0 + idx;
+        const int lo = static_cast<int>(M.slot_side[g] - side0);
+        const int slot = static_cast<int>(g - sst[lo]);
+        const int64_t src0 = M.slot_src[2 * g], src1 = M.slot_src[2 * g + 1];
+        const R nx = R(M.slot_normal[2 * g]), ny = R(M.slot_normal[2 * g + 1]);
+        R L[3], Rv[3];
+        if (src0 >= 0) {
+            L[0] = tr[src0];
+            L[1] = tr[src0 + ft];
+            L[2] = tr[src0 + 2 * ft];
+        } else {
+            slot_interp<S, R>(M, tr, ft, -1 - src0, L);
+        }
+        if (src1 >= 0) {
+            Rv[0] = tr[src1];
+            Rv[1] = tr[src1 + ft];
+            Rv[2] = tr[src1 + 2 * ft];
+        } else {
+            slot_interp<S, R>(M, tr, ft, -1 - src1, Rv);
+        }
+        const R wL = add<S>(L[0], add<S>(mul<S>(L[1], nx), mul<S>(L[2], ny)));
+        const R wR = sub<S>(Rv[0], add<S>(mul<S>(Rv[1], nx), mul<S>(Rv[2], ny)));
+        const R sum = add<S>(wL, wR);
+        R* o = ffs + lo * SL + slot;
+        o[0] = mul<S>(sub<S>(wL, wR), R(0.5));
+        o[FFS] = mul<S>(mul<S>(nx, sum), R(0.5));
+        o[2 * FFS] = mul<S>(mul<S>(ny, sum), R(0.5));
+    }
+    __syncthreads();
+
+    // Element side fluxes (Mesh2D_t::project_to_elements, Mesh2D_t.cpp:3895-4006),
+    // as in fused_tile, into the element's trace-layout slots of sflux.
+    for (int idx = tid; idx < ne * 4 * n; idx += THREADS) {
+        const int ee = idx / (4 * n), sm = idx - ee * 4 * n;
+        const int s = sm / n, i = sm - s * n;
+        const int mode = smode[ee * 4 + s];
+        const R sfv = ss[ee * 4 + s];
+        const R* fl = ffs + (ee * 4 + s) * SL;
+        R out[3] = {0, 0, 0};
+        if (mode == 1) {
+            for (int c = 0; c < 3; ++c) out[c] = mul<S>(fl[c * FFS + i], sfv);
+        } else if (mode == 2) {
+            for (int c = 0; c < 3; ++c) out[c] = mul<S>(-fl[c * FFS + (N - i)], sfv);
+        } else if (mode == 3) {
+            const int64_t q0 = sqs[ee * 4 + s], q1 = sqs[ee * 4 + s + 1];
+            int slot0 = 0;
+            for (int64_t qq = q0; qq < q1; ++qq) {
+                const int Nf = M.pq_N[qq];
+                const R scale = R(M.pq_scale[qq]);
+                const double* W = M.sw + M.pq_woff[qq] + i * (Nf + 1);
+                const int* match = M.smatch + M.pq_moff[qq];
+                for (int j = 0; j <= Nf; ++j) {
+                    const int mt = match[j];
+                    const R w = R(W[j]);  // loaded with the match (the sums keep their order)
+                    if (mt >= 0 && mt != i) continue;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) out[c] = add<S>(out[c], mul<S>(mul<S>(mul<S>(w, fl[c * FFS + slot0 + j]), sfv), scale));
+                }
+                slot0 += Nf + 1;
+            }
+        }
+        R* o = out_flux + eo1[ee] + sm;
+        o[0] = out[0];
+        o[ft] = out[1];
+        o[2 * ft] = out[2];
+    }
+}
+
 // Fused stage of every order group in one launch: one CTA of kQueueThreads
 // threads per entry of the stage queue (the tiles of every group, largest
 // order first, then the next instance), which names the tile's order; the
@@ -969,7 +1111,20 @@ cudaError_t set_attrs(int side_slots) {
     cudaError_t err = cudaFuncSetAttribute(general_fused_kernel<N, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b64);
     if (err == cudaSuccess) err = cudaFuncSetAttribute(general_fused_kernel<N, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b64);
     if (err == cudaSuccess) err = cudaFuncSetAttribute(general_fused_kernel<N, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b32);
+    const int f64 = static_cast<int>(FluxTile<N, double>::bytes(side_slots));
+    const int f32 = static_cast<int>(FluxTile<N, float>::bytes(side_slots));
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(side_flux_kernel<N, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, f64);
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(side_flux_kernel<N, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, f64);
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(side_flux_kernel<N, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, f32);
     return err;
+}
+
+template <int N, bool S, typename R>
+cudaError_t launch_side_fluxes(const GeneralStage& a, const OrderGroup& g, cudaStream_t stream) {
+    using T = FluxTile<N, R>;
+    const dim3 grid(static_cast<unsigned>((g.count + T::EPB - 1) / T::EPB), static_cast<unsigned>(a.n_instances));
+    side_flux_kernel<N, S, R><<<grid, T::kThreads, T::bytes(a.side_slots), stream>>>(a, g);
+    return cudaGetLastError();
 }
 
 template <int N>
@@ -1072,6 +1227,14 @@ cudaError_t launch_general_ghosts(const GeneralStage& a, bool strict, bool fp32,
 cudaError_t launch_general_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream) {
     if (g.count == 0) return cudaSuccess;
     if (g.conforming) return launch_conforming_group(a, g, strict, fp32, stream);
+    if (g.split) {
+        const cudaError_t err = by_order(g.N, [&](auto c) {
+            constexpr int N = decltype(c)::value;
+            if (fp32) return launch_side_fluxes<N, false, float>(a, g, stream);
+            return strict ? launch_side_fluxes<N, true, double>(a, g, stream) : launch_side_fluxes<N, false, double>(a, g, stream);
+        });
+        return err == cudaSuccess ? launch_conforming_group(a, g, strict, fp32, stream, true) : err;
+    }
     return by_order(g.N, [&](auto c) {
         constexpr int N = decltype(c)::value;
         if (fp32) return launch_fused<N, false, float>(a, g, stream);

@@ -123,6 +123,8 @@ struct GeneralStage {
     double* etr_out = nullptr;  // the same for the stage's output
     float* etr_f = nullptr;     // the two trace buffers of the FP32 form
     float* etr_out_f = nullptr;
+    double* sflux = nullptr;    // [instance][field][trace_total] element side fluxes of a split group
+    float* sflux_f = nullptr;   // the same in the FP32 form
     int side_slots = 1;         // largest sum of (face order + 1) over the faces of one element side
     const double* step = nullptr;  // {time, dt, dt_mesh, t_end}
     double rk_a = 0, rk_b = 0, rk_g = 0;
@@ -137,6 +139,7 @@ struct OrderGroup {
     const int64_t* ids = nullptr;  // device, element numbers
     int64_t first = 0;             // list position of the group's first element
     int conforming = 0;            // 1: every side one same-order face with a same-order neighbour (conforming_stage_kernel)
+    int split = 0;                 // 1: side_flux_kernel, then conforming_stage_kernel over its side fluxes
 };
 
 // The stage queue of a mixed-order mesh: every tile of every order group
@@ -183,7 +186,8 @@ cudaError_t launch_general_queue(const GeneralStage& a, const StageQueue& wq, bo
 // the uniform-order stage with the neighbour traces gathered by the plan, in
 // FP64 (strict or not) or in the FP32 form.
 cudaError_t prepare_conforming_kernels(int N);
-cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream);
+// pre: the group's element side fluxes are in sflux (sflux_f) already.
+cudaError_t launch_conforming_group(const GeneralStage& a, const OrderGroup& g, bool strict, bool fp32, cudaStream_t stream, bool pre = false);
 // The plane-wave initial condition at every node of a mixed-order mesh.
 cudaError_t launch_general_initial_conditions(const GeneralStage& a, const OrderGroup* groups, int n_groups, cudaStream_t stream);
 

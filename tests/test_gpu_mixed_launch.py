@@ -1,7 +1,9 @@
-"""The two launch structures of a stage on a mixed-order mesh: one launch
-per order group as concurrent graph branches (the default) and one launch
-per stage over a queue of every order group's tiles. Each tile runs the same
-operations in either, so the fields must be bit-identical in FP64_STRICT;
+"""The three launch structures of a stage on a mixed-order mesh: one launch
+per order group as concurrent graph branches (the default), one launch
+per stage over a queue of every order group's tiles, and the groups split
+into a side-flux launch and an element-tile launch (the conforming-element
+kernel over the side fluxes). Each computes the same operations, so the
+fields must be bit-identical in FP64_STRICT;
 in FP64 and FP32 the two compilations may contract multiply-adds
 differently, so they are held to 1e-12 and 1e-6 relative L2. Meshes after
 p-adaptation (mortar faces between orders) and after element splitting
@@ -52,18 +54,19 @@ def test_queue_and_group_launches_agree(kind, precision):
     assert len(set(N.tolist())) >= 2
     state = {f: m.get_field(f) for f in ("p", "u", "v", "k_p", "k_u", "k_v")}
     out = []
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         m.set_mixed_launch(mode)
         for f, v in state.items():
             m.set_field(f, v)
         launches0 = m.launches()
         ndg.Solver2D_t.run(m, 6)
         out.append(({f: m.get_field(f) for f in ("p", "u", "v")}, m.launches() - launches0))
-    (a, _), (b, launches_queue) = out
+    (a, _), (b, launches_queue), (c, _) = out
     tol = {ndg.FP64_STRICT: 0.0, ndg.FP64: 1e-12, ndg.FP32: 1e-6}[precision]
-    for f in ("p", "u", "v"):
-        assert np.linalg.norm(a[f] - b[f]) <= tol * np.linalg.norm(a[f]), f
-        assert np.isfinite(b[f]).all()
+    for other in (b, c):
+        for f in ("p", "u", "v"):
+            assert np.linalg.norm(a[f] - other[f]) <= tol * np.linalg.norm(a[f]), f
+            assert np.isfinite(other[f]).all()
     ghosts = 1 if m.n_elements_total_ > m.n_elements_ else 0
     # per step: 3 stages x (ghosts + queue) + the time update; then the first
     # traces, one launch per order's conforming part and per its other part
