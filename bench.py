@@ -486,8 +486,8 @@ def hp_leg(local: int, stream) -> dict:
             "refining_fp32": refining32,
             "launch_structure": ("one CUDA graph per RK3 step; per stage a ghost-trace kernel, then per order group the fused kernel, "
                                  "or, where at least half its elements are conforming, the conforming-element kernel for those and "
-                                 "the fused kernel for the rest (in the FP32 form an order of at least 2,048 elements with no "
-                                 "conforming part runs split: its side fluxes, then the conforming-element kernel over them); "
+                                 "the fused kernel for the rest (an order of at least 2,048 elements with no conforming part "
+                                 "runs split: its side fluxes, then the conforming-element kernel over them); "
                                  "the groups forked onto side streams as parallel graph branches"),
             "note": ("at the configuration's threshold 1e-4 the estimate never exceeds it on this mesh (largest error at N=4 "
                      "is 3.4e-6), so nothing refines; the 1e-9 runs exercise p-refinement, splitting to level 2 and the mortar path"),

@@ -149,9 +149,9 @@ ndg_status ndg_ctx_keep_derivative(ndg_ctx* ctx, int32_t enable);
  * order; mode 2 as mode 0, but every order group that is not all
  * conforming elements runs in two launches: its element side fluxes (face
  * fluxes and mortar projections), then the uniform-style element tile over
- * them. Mode 0 runs a group that way in the FP32 form where it has at
- * least 2,048 elements (times the instances) and its order no conforming
- * part, else fused. Each computes the same operations
+ * them. Mode 0 runs a group that way where it has at least 2,048
+ * elements (times the instances) and its order no conforming part, else
+ * fused. Each computes the same operations
  * either way (bit-identical in NDG_FP64_STRICT; the compiler may contract
  * differently otherwise). Meshes of one order are not affected. */
 ndg_status ndg_set_mixed_launch(ndg_ctx* ctx, int32_t mode);

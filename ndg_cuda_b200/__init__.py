@@ -305,9 +305,9 @@ class Mesh2D_t:
         return dict(zip(("device_decisions", "topology", "transfer", "plan"), ms))
 
     def set_mixed_launch(self, mode: int) -> None:
-        """Mixed-order meshes: 0 one launch per order group, in the FP32 form groups of at least
-        2,048 elements whose order has no conforming part split into a side-flux launch and an
-        element-tile launch (default); 1 one queue launch per stage;
+        """Mixed-order meshes: 0 one launch per order group, groups of at least 2,048 elements whose
+        order has no conforming part split into a side-flux launch and an element-tile launch
+        (default); 1 one queue launch per stage;
         2 as 0 with every group that is not all conforming elements split."""
         _check(lib().ndg_set_mixed_launch(self._ctx.h, mode))
 

@@ -114,18 +114,19 @@ const std::vector<dev::OrderGroup>& stage_groups(const ndg_ctx* c) { return c->g
 
 // Whether an order group runs split (side_flux_kernel, then the
 // conforming-element kernel over its side fluxes) rather than fused: always
-// in launch mode 2; in mode 0 in the FP32 form, where the group (times the
-// instances) has at least kSplitMinElements elements and its order has no
-// conforming part. Measured (ms per step, DOF-stage updates/s), fused
-// against split by this rule: the mixed p-adapted 128² mesh FP64 0.2705 →
-// 0.2572, FP32 0.2092 → 0.2045; the hp refining run (about 30 meshes) FP64
-// 4.72e10 → 4.60e10, FP32 6.16e10 → 6.27e10. FP64 stays fused by default
-// for the hp run; splitting every group there cost 4% (FP64) and 5% (FP32).
+// in launch mode 2; in mode 0 where the group (times the instances) has at
+// least kSplitMinElements elements and its order has no conforming part. A
+// remainder beside a conforming part runs in parallel with it, which hides
+// its latency, and small groups are one short wave either way. Measured
+// (ms per step, DOF-stage updates/s), fused against split by this rule:
+// the mixed p-adapted 128² mesh FP64 0.2709 → 0.2502, FP32 0.2092 →
+// 0.2045; the hp refining run (about 30 meshes) FP64 4.71e10 → 4.81e10,
+// FP32 6.16e10 → 6.27e10. Splitting every group cost the hp run 4% (FP64)
+// and 5% (FP32).
 constexpr int64_t kSplitMinElements = 2048;
 bool split_group(const ndg_ctx* c, const dev::OrderGroup& og) {
     if (og.conforming || c->mixed_launch == 1) return false;
     if (c->mixed_launch == 2) return true;
-    if (!fp32(c)) return false;
     const bool has_conforming_part =
         std::any_of(c->groups.begin(), c->groups.end(), [&](const dev::OrderGroup& other) { return other.conforming && other.N == og.N; });
     return !has_conforming_part && og.count * c->n_instances >= kSplitMinElements;

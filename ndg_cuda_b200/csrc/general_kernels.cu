@@ -804,9 +804,6 @@ struct FluxTile {
     static constexpr int n = N + 1;
     static constexpr int EPB = 32 / n >= 1 ? 32 / n : 1;
     static constexpr int kThreads = 128;
-    // FP64: at most 40 registers, for warps to hide the gathers' latency (the
-    // FP32 form fits 10 CTAs at its free 48 registers; bound to 40 it spills)
-    static constexpr int kMinBlocks = sizeof(R) == 8 ? 12 : 0;
     // doubles: [EPB] trace offsets, [4 EPB + 1] first slot of each side and
     // the end, the same for mortar entries (int64), [4 EPB] flux modes (ints)
     static constexpr int kDoubles = EPB + 2 * (4 * EPB + 1) + 2 * EPB;
@@ -817,7 +814,7 @@ struct FluxTile {
 };
 
 template <int N, bool S, typename R>
-__global__ void __launch_bounds__(FluxTile<N, R>::kThreads, FluxTile<N, R>::kMinBlocks) side_flux_kernel(GeneralStage a, OrderGroup grp) {
+__global__ void __launch_bounds__(FluxTile<N, R>::kThreads) side_flux_kernel(GeneralStage a, OrderGroup grp) {
     using T = FluxTile<N, R>;
     constexpr int n = T::n, EPB = T::EPB, THREADS = T::kThreads;
     extern __shared__ __align__(128) double smem[];
