@@ -804,6 +804,11 @@ struct FluxTile {
     static constexpr int n = N + 1;
     static constexpr int EPB = 32 / n >= 1 ? 32 / n : 1;
     static constexpr int kThreads = 128;
+    // FP64: 8 CTAs per SM (64 registers, 24 bytes of spills) rather than the
+    // free allocation's 7 at 66: mixed 128² step 0.2545 → 0.2507 ms, the hp
+    // refining run unchanged. Bounds of 10 and 12 CTAs spill 80-108 bytes and
+    // cost the hp run 2-3%; the FP32 form fits 10 at its free 48 registers.
+    static constexpr int kMinBlocks = sizeof(R) == 8 ? 8 : 0;
     // doubles: [EPB] trace offsets, [4 EPB + 1] first slot of each side and
     // the end, the same for mortar entries (int64), [4 EPB] flux modes (ints)
     static constexpr int kDoubles = EPB + 2 * (4 * EPB + 1) + 2 * EPB;
@@ -814,7 +819,7 @@ struct FluxTile {
 };
 
 template <int N, bool S, typename R>
-__global__ void __launch_bounds__(FluxTile<N, R>::kThreads) side_flux_kernel(GeneralStage a, OrderGroup grp) {
+__global__ void __launch_bounds__(FluxTile<N, R>::kThreads, FluxTile<N, R>::kMinBlocks) side_flux_kernel(GeneralStage a, OrderGroup grp) {
     using T = FluxTile<N, R>;
     constexpr int n = T::n, EPB = T::EPB, THREADS = T::kThreads;
     extern __shared__ __align__(128) double smem[];
