@@ -23,7 +23,10 @@
 // same-order face per side, shared with a same-order neighbour), they come
 // last in the plan's list and run conforming_stage_kernel
 // (conforming_kernels.cu) instead of the fused stage; the two parts are
-// separate groups and concurrent branches.
+// separate groups and concurrent branches. A large group whose order has no
+// conforming part runs split instead of fused: side_flux_kernel (the fused
+// stage's face and element-side fluxes, into a trace-layout buffer), then
+// conforming_stage_kernel's PRE form over those side fluxes.
 //
 // The mortar weights of the plan are computed once (side_weights_kernel,
 // face_weights_kernel). A face's flux is evaluated by each of its two
