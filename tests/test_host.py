@@ -156,3 +156,19 @@ def test_tile_candidates_on_a_host_context():
     cand16, _ = m16.tile_candidates()
     simt16 = [c % T for c in cand16]
     assert cand16 and max(simt16) * 3 * 17 <= 512 and all(c in (2, 4, 8, 16) for c in simt16)
+
+
+def test_mixed_launch_modes_on_a_host_context():
+    """ndg_set_mixed_launch takes 0 (one launch per order group, large
+    non-conforming orders split), 1 (one queue launch per stage) and 2 (every
+    group split into side fluxes and element tiles); other modes are an
+    invalid argument, reported as a status."""
+    zone = meshgen.uniform_zone(4, x_periodic=True, y_periodic=True)
+    m = ndg.Mesh2D_t(zone, 4, device=-1)
+    for mode in (0, 1, 2):
+        m.set_mixed_launch(mode)
+    for mode in (-1, 3):
+        with pytest.raises(ndg.NdgError) as e:
+            m.set_mixed_launch(mode)
+        assert e.value.status == 1
+        assert "mode is 0" in ndg.lib().ndg_last_error().decode()
