@@ -290,9 +290,11 @@ ndg_status ndg_launch_count(const ndg_ctx* ctx, int64_t* launches);
  * beyond), and calls that overlap in time on one device race on that array:
  * serialise them. Each call looks up the array's address on the current
  * device (nothing is cached between calls); the first call on a device also
- * loads the library's kernels there, so make it before any stream capture
- * begins on that device. Every call synchronises its stream before it
- * returns. stream is a cudaStream_t of the current device (NULL: the default
+ * loads the library's kernels there. Every call copies the result to the
+ * host and synchronises its stream before it returns, so it can never be
+ * captured into a graph: do not make it on a capturing stream, nor while
+ * another thread runs a global-mode capture on the device. stream is a
+ * cudaStream_t of the current device (NULL: the default
  * stream); a stream of another device is refused with NDG_ERR_INVALID_ARG. */
 ndg_status ndg_delta_t_from_device(const double* delta_xy_min, const int32_t* elem_N, int64_t n_elements,
                                    double cfl, void* stream, double* delta_t);
